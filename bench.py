@@ -1,0 +1,453 @@
+"""Benchmark of the electrostatic PIC time step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the MCC configuration): 513x513 nodes (512^2 cells, dx = 1e-4 m),
+4M electrons + 4M ions, left wall 100 V, multigrid to a 1e-8 relative
+residual, null-collision MCC against an argon-like gas (1e21 m^-3, 300 K,
+elastic / excitation / ionisation / charge exchange), dt = 1e-11 s.  Inputs
+are synthetic and seeded.  One step = kick + MCC + drift + absorb + deposit,
+the Poisson solve and E.  The metric is particle-steps/s; `value` times K
+steps with the state resident in HBM (particle arrays 8M x 20 B = 160 MB,
+larger than the 126 MB L2).  `e2e` times the public API from pinned host
+arrays: load, init, K steps, read back particles and phi.  `poisson` times
+the large workload's solve (2049^2, 64M + 64M particles, Gaussian blob) to a
+1e-10 relative residual, mixed precision against plain FP64.
+
+Multi-GPU (torchrun): independent replicas, one per GPU (the path does not
+shard); the time is the max over ranks and `value` sums all ranks' work.
+--impl reference runs the reference's own kernels (compiled for the CPU by
+oracle/ref_build.py) on the host cores for the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s/GPU at 512², 8M ptcl; mixed vs FP64 multigrid at 1e-10 residual"
+UNIT = "particle-steps/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--sort-interval", type=int, default=20)
+    ap.add_argument("--particles", type=int, default=4_000_000, help="per species")
+    ap.add_argument("--no-poisson", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-collisionless", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.rows.append([c.strip() for c in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 4 + k and "Active" in r[4 + k]
+                          and "Not" not in r[4 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------
+# our implementation
+# ---------------------------------------------------------------------------
+
+def peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per k_push launch from the committed ncu summary (profiles/), or None."""
+    p = os.path.join(ROOT, "profiles", "k_push_traffic.txt")
+    try:
+        for line in open(p):
+            if line.startswith("bytes_per_launch:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+def make_sim(w, rank, sort_interval, mcc=True):
+    from pic_b200 import Consts, workloads
+    from pic_b200.simulation import PICSimulation
+
+    mask, phi_bc = workloads.dirichlet(w)
+    species = [dict(name="e", charge=-Consts.qe, mass=Consts.me, np2c=w.np2c(w.n_e), capacity=int(w.n_e * 1.25)),
+               dict(name="i", charge=Consts.qe, mass=workloads.ION_MASS, np2c=w.np2c(w.n_i),
+                    capacity=int(w.n_i * 1.25))]
+    tables = workloads.mcc_tables(w) if mcc else None
+    return PICSimulation(w.nodes, w.nodes, w.dx, w.dx, w.dt, species, mask, phi_bc, tol=w.tol, max_cycles=50,
+                         sort_interval=sort_interval, mcc=tables, seed=1000 + rank)
+
+
+def gen_arrays(w, rank):
+    from pic_b200 import workloads
+
+    rng = np.random.Generator(np.random.Philox(w.seed + 17 * rank))
+    return [workloads.species_arrays(w, "e", rng), workloads.species_arrays(w, "i", rng)]
+
+
+def live_count(sim):
+    return sum(sim.counters()["count"])
+
+
+def time_steps(sim, K, world):
+    import torch
+    import torch.distributed as dist
+
+    stream = torch.cuda.current_stream()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    n0 = live_count(sim)
+    l0 = sim.kernel_launches()
+    sim.set_profiling(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.step(K)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    prof = sim.read_profile()
+    sim.set_profiling(False)
+    n1 = live_count(sim)
+    return ms, prof, sim.kernel_launches() - l0, n0, n1
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    import torch.distributed as dist
+
+    from pic_b200 import workloads
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local))
+    w = workloads.scaled(workloads.MCC, n=args.particles)
+    arrays = gen_arrays(w, rank)
+    sim = make_sim(w, rank, args.sort_interval, mcc=True)
+    for s, a in enumerate(arrays):
+        sim.load(s, *a)
+    sim.init()
+    sim.step(args.warmup)
+    with ClockSampler(local) as clk:
+        ms, prof, launches, n0, n1 = time_steps(sim, args.steps, world)
+    clocks = clk.summary()
+    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    work = torch.tensor([0.5 * (n0 + n1) * args.steps], device="cuda", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(work)
+    value = float(work.item()) / (ms_max / 1e3)
+    counters = sim.counters()
+
+    # roofline of the fused particle kernel: 16 B read + 16 B written per
+    # particle (x, y, vx, vy), + 8 B (vz read and written) for species with
+    # collisions -- here both -- plus the E tile read (8 B/node) and the
+    # charge flush (4 B/node) per step.
+    G = w.nodes * w.nodes
+    push = prof["push"]
+    push_ms = push["ms"] / max(1, push["count"])
+    bytes_per_launch = 0.5 * (n0 + n1) * 40.0 + G * 12.0
+    achieved = bytes_per_launch / (push_ms / 1e3) / 1e9
+    peak, peak_kind = peak_hbm()
+    traffic = ncu_traffic()
+    roofline = {"bound": "hbm", "kernel": "k_push", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
+                "bytes_per_launch": bytes_per_launch, "ms_per_launch": round(push_ms, 5)}
+    phases = {k: round(v["ms"] / args.steps, 4) for k, v in prof.items() if isinstance(v, dict)}
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 particles / f64 Poisson residual", "data": "synthetic (seeded Philox)",
+        "config": {"workload": "mcc: 513x513 nodes (512^2 cells), dx 1e-4 m, "
+                               f"{w.n_e} e- + {w.n_i} ions (40 amu), Te 2 eV, Ti 0.03 eV, n0 1e14, left wall 100 V, "
+                               "argon-like gas 1e21 m^-3 300 K, elastic/excitation/ionisation/charge exchange, "
+                               "dt 1e-11 s, multigrid tol 1e-8",
+                   "global_batch": int(0.5 * (n0 + n1)) * world, "parallelism": f"replicas{world}",
+                   "sort_interval": args.sort_interval,
+                   "l2": "inputs larger than L2 (particle arrays 160 MB > 126 MB)"},
+        "phase_ms_per_step": phases,
+        "mg_cycles_per_step": prof["mg_cycles"] / args.steps,
+        "counters": {k: counters[k] for k in ("absorbed", "collisions", "born", "count", "last_rel_res")},
+        "roofline": roofline,
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    sim.close()
+    del sim
+    torch.cuda.empty_cache()
+
+    if not args.no_collisionless:
+        sim = make_sim(w, rank, args.sort_interval, mcc=False)
+        for s, a in enumerate(arrays):
+            sim.load(s, *a)
+        sim.init()
+        sim.step(args.warmup)
+        ms2, prof2, _, m0, m1 = time_steps(sim, args.steps, world)
+        t2 = torch.tensor([ms2], device="cuda", dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+        p2 = prof2["push"]["ms"] / max(1, prof2["push"]["count"])
+        out["collisionless"] = {"value": world * 0.5 * (m0 + m1) * args.steps / (float(t2.item()) / 1e3),
+                                "ms_per_step": float(t2.item()) / args.steps,
+                                "push_ms": round(p2, 5),
+                                "push_frac_of_peak": round((0.5 * (m0 + m1) * 40.0 + G * 12.0) / (p2 / 1e3) / 1e9
+                                                           / peak, 4),
+                                "mg_cycles_per_step": prof2["mg_cycles"] / args.steps}
+        sim.close()
+        del sim
+        torch.cuda.empty_cache()
+
+    if not args.no_e2e:
+        out["e2e"] = run_e2e(w, arrays, args, world, rank)
+    if not args.no_poisson and rank == 0:
+        out["poisson"] = run_poisson()
+    if not args.no_cpu_baseline and rank == 0 and world == 1:
+        out["cpu_baseline"] = run_cpu_baseline(w, arrays, args.cpu_steps)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_e2e(w, arrays, args, world, rank):
+    """Public API from pinned host arrays: load, init, K steps, read back particles and phi."""
+    import torch
+    import torch.distributed as dist
+
+    pinned = [[torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in sp] for sp in arrays]
+    sim = make_sim(w, rank, args.sort_interval, mcc=True)
+    stream = torch.cuda.current_stream()
+    outs = None
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for s, a in enumerate(pinned):
+        sim.load(s, *[t.numpy() for t in a])
+    sim.init()
+    sim.step(args.steps)
+    sim.sync()
+    outs = [[t.to("cpu", non_blocking=False) for t in sim.species_arrays(s)] for s in range(2)]
+    phi = sim.fields()[0].to("cpu")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    n = sum(len(a[0]) for a in arrays)
+    h2d = sum(a.numel() * 4 for sp in pinned for a in sp)
+    d2h = sum(a.numel() * 4 for sp in outs for a in sp) + phi.numel() * 8
+    sim.close()
+    return {"value": world * n * args.steps / (float(t.item()) / 1e3), "unit": UNIT,
+            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+            "ms_total": float(t.item()), "includes": "H2D of all particles from pinned host memory, init, "
+                                                     f"{args.steps} steps, D2H of particles and phi"}
+
+
+def run_poisson():
+    """Large workload: deposit 64M + 64M particles on 2049^2 nodes, solve to 1e-10 from phi = 0."""
+    import torch
+
+    from pic_b200 import Consts, _lib, workloads
+    from pic_b200.multigrid import MultigridSolver
+
+    w = workloads.LARGE
+    n = w.nodes
+    G = n * n
+    g = torch.Generator(device="cuda")
+    g.manual_seed(2)
+    rho = torch.zeros(G, dtype=torch.float32, device="cuda")
+    top = float(n - 1)
+    chunk = 16_000_000
+    for which, count in (("e", w.n_e), ("i", w.n_i)):
+        q = -Consts.qe if which == "e" else Consts.qe
+        scale = q * w.np2c(count) / (w.dx * w.dx)
+        done = 0
+        while done < count:
+            k = min(chunk, count - done)
+            if which == "e" and done < count // 2:
+                k = min(k, count // 2 - done)
+                c = 0.5 * top
+                x = torch.randn(k, generator=g, device="cuda") * (0.2 * top) + c
+                y = torch.randn(k, generator=g, device="cuda") * (0.2 * top) + c
+                x = x.clamp(0, top - 1e-3)
+                y = y.clamp(0, top - 1e-3)
+            else:
+                x = torch.rand(k, generator=g, device="cuda") * (top - 1e-3)
+                y = torch.rand(k, generator=g, device="cuda") * (top - 1e-3)
+            _lib.call("pic_deposit", _lib.ptr(x), _lib.ptr(y), k, float(scale), _lib.ptr(rho), n, n,
+                      _lib.stream_ptr())
+            done += k
+    mask, _ = workloads.dirichlet(w)
+    mask_t = torch.as_tensor(mask, device="cuda")
+    f = torch.zeros(G, dtype=torch.float64, device="cuda")
+    _lib.call("pic_form_rhs", _lib.ptr(rho), _lib.ptr(mask_t), Consts.eps0, _lib.ptr(f), n, n, _lib.stream_ptr())
+    res = {"workload": "large: 2049x2049 nodes, 64M e- (half in a sigma=0.2L blob) + 64M ions, tol 1e-10, phi0 = 0"}
+    for prec in ("mixed", "fp64"):
+        mg = MultigridSolver(mask, n, n, w.dx, precision=prec)
+        phi = torch.zeros(G, dtype=torch.float64, device="cuda")
+        mg.solve(phi, f, tol=1e-10, max_cycles=60)  # warm-up (allocations, caches)
+        best = None
+        for _ in range(3):
+            phi.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            _, (cycles, rel) = mg.solve(phi, f, tol=1e-10, max_cycles=60)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None or ms < best else best
+        res[prec] = {"ms": round(best, 3), "cycles": cycles, "rel_res": rel}
+        del mg
+    res["speedup_mixed_vs_fp64"] = round(res["fp64"]["ms"] / res["mixed"]["ms"], 3)
+    return res
+
+
+def run_cpu_baseline(w, arrays, steps):
+    from oracle import oracle as O
+    from oracle import refstep
+    from pic_b200 import workloads
+
+    if not O.ref_available():
+        return {"value": None, "unavailable": "oracle/_ref/libpicref.so not built"}
+    E, el, *_ = workloads.cross_sections()
+    ref = refstep.ReferenceCPU(w.nodes, w.dx, w.dt, arrays[0], arrays[1], w.np2c(w.n_e), workloads.ION_MASS,
+                               left_V=w.left_V, tol=w.tol, mcc_table=(E, el), gas_density=w.gas_density)
+    dt, cycles = refstep.time_steps(ref, steps, warmup=1)
+    n = ref.N
+    ref.close()
+    return {"value": n * steps / dt, "unit": UNIT, "cores": ref.threads, "kind": "reference",
+            "sample": f"{steps} full steps of the same workload ({n} particles, 513^2) after 1 warm-up step; "
+                      f"multigrid cycles {cycles}", "cpu": refstep.cpu_model()}
+
+
+# ---------------------------------------------------------------------------
+# reference arm
+# ---------------------------------------------------------------------------
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from oracle import refstep
+    from pic_b200 import workloads
+
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libpicref.so not built"}))
+        return
+    w = workloads.scaled(workloads.MCC, n=args.particles)
+    arrays = gen_arrays(w, 0)
+    E, el, *_ = workloads.cross_sections()
+    ref = refstep.ReferenceCPU(w.nodes, w.dx, w.dt, arrays[0], arrays[1], w.np2c(w.n_e), workloads.ION_MASS,
+                               left_V=w.left_V, tol=w.tol, mcc_table=(E, el), gas_density=w.gas_density)
+    steps = max(1, args.steps)
+    dt, cycles = refstep.time_steps(ref, steps, warmup=max(0, args.warmup))
+    value = ref.N * steps / dt
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Philox)",
+        "config": {"workload": "mcc: 513x513 nodes, "
+                               f"{w.n_e} e- + {w.n_i} ions, left wall 100 V, multigrid tol 1e-8, MCC (elastic table)",
+                   "global_batch": ref.N, "parallelism": "host cores"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": ref.threads, "kind": "reference",
+                         "sample": f"{steps} full steps after {args.warmup} warm-up steps; multigrid cycles {cycles}",
+                         "cpu": refstep.cpu_model()},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    ref.close()
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,323 @@
+/*
+ * picb200.h -- C ABI of libpicb200.so, the B200 (sm_100a) implementation of
+ * the electrostatic PIC time step of dimad285/PIC: CIC charge deposition,
+ * the multigrid Poisson solve, field gather fused with the leapfrog push and
+ * wall absorption, cell sorting, and null-collision Monte-Carlo collisions.
+ *
+ * The reference has no C interface: its operator API is the set of Python
+ * classes that src/simulation.py calls (Particles2D, Grid2D, Solver,
+ * MultigridSolver, Boundaries, MCC).  Each entry point below names the
+ * reference function it replaces; the Python shims in pic_b200/ bind these
+ * symbols with ctypes and keep the reference's call signatures.
+ *
+ * Conventions
+ *  - Every function returns a pic_status; 0 is success.  pic_last_error()
+ *    returns a message for the last failing call on the calling thread.
+ *  - Pointers named d_* are device pointers; h_* are host pointers.
+ *  - Grid arrays are flat row-major, index = j*nx + i, nx = number of nodes
+ *    in x (src/Grid.py:140-143).  Grids are given in NODES (Grid2D(m, n, ...)).
+ *  - Particle arrays are SoA float32.  Positions are in grid units
+ *    (x/dx, y/dy); velocities in m/s.  A dead (absorbed) slot holds NaN in x.
+ *  - `stream` is a cudaStream_t passed as void*; NULL is the legacy stream.
+ *    All calls are asynchronous on that stream unless they say otherwise.
+ *  - Objects (pic_mg, pic_sorter, pic_sim) are not thread-safe; use one per
+ *    host thread or serialise calls.
+ */
+#ifndef PICB200_H
+#define PICB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PIC_ABI_VERSION 1
+#define PIC_MAX_SPECIES 4
+#define PIC_MAX_PROCESSES 4
+
+typedef enum pic_status {
+    PIC_OK = 0,
+    PIC_ERR_BAD_ARG = 1,
+    PIC_ERR_CUDA = 2,
+    PIC_ERR_NOT_CONVERGED = 3,
+    PIC_ERR_TIMEOUT = 4,
+    PIC_ERR_OUT_OF_CAPACITY = 5,
+    PIC_ERR_NUMERIC = 6
+} pic_status;
+
+int pic_abi_version(void);
+/* Message of the last failing call on this host thread ("" if none). */
+const char* pic_last_error(void);
+
+/* ------------------------------------------------------------------ */
+/* Stateless particle and grid operators                               */
+/* ------------------------------------------------------------------ */
+
+/* Particles2D.update_R (src/Particles.py:359-367, kernel :251-264):
+ * x += vx*dtdx, y += vy*dtdy for live slots [0, n).  dtdx = dt/dx.
+ * d_x_old/d_y_old (optional, may be NULL) receive the positions before the move. */
+int pic_update_R(float* d_x, float* d_y, const float* d_vx, const float* d_vy, int n, float dtdx, float dtdy,
+                 float* d_x_old, float* d_y_old, void* stream);
+
+/* Wall absorption, the predicate of collisions.remove_out_of_bounds
+ * (src/collisions.py:177-215) on all four walls: a live particle outside
+ * [0, nx-1] x [0, ny-1] (grid units) is marked dead.  Replaces
+ * Particles2D.update_axis (src/Particles.py:369-376), which reflects at y < 0.
+ * *d_absorbed (device, uint64) is incremented by the number absorbed. */
+int pic_absorb(float* d_x, float* d_y, int n, int nx, int ny, unsigned long long* d_absorbed, void* stream);
+
+/* Particles2D.update_V (src/Particles.py:378-410, kernel :117-180): bilinear
+ * gather of (Ex, Ey) at each live particle, v += kq*E with kq = dt*q/m. */
+int pic_update_V(const float* d_x, const float* d_y, float* d_vx, float* d_vy, int n, const float* d_Ex,
+                 const float* d_Ey, int nx, int ny, float kq, void* stream);
+
+/* Grid2D.update_density, Cartesian (src/Grid.py:246-294, kernel :96-154):
+ * adds scale*w (scale = q*np2c/(dx*dy)) of each live particle to the four
+ * surrounding nodes of d_rho (float32, nx*ny).  The caller zeroes d_rho
+ * once before depositing all species. */
+int pic_deposit(const float* d_x, const float* d_y, int n, float scale, float* d_rho, int nx, int ny,
+                void* stream);
+
+/* Grid2D.update_E (src/Grid.py:232-243, kernel :157-196): E = -grad(phi),
+ * central differences inside, one-sided at the edges, computed in FP64 and
+ * stored as float32 planes d_Ex, d_Ey (nx*ny each). */
+int pic_update_E(const double* d_phi, float* d_Ex, float* d_Ey, int nx, int ny, double dx, double dy,
+                 void* stream);
+
+/* Solver.solve right-hand side (src/Solvers.py:271-276): d_f = -rho/eps0 on
+ * free nodes, d_f = 0 on Dirichlet nodes (d_dirichlet: uint8, 1 = Dirichlet).
+ * The reference's extra dx^2 factor is not applied: the multigrid applies h^2. */
+int pic_form_rhs(const float* d_rho, const uint8_t* d_dirichlet, double eps0, double* d_f, int nx, int ny,
+                 void* stream);
+
+/* ------------------------------------------------------------------ */
+/* Multigrid Poisson solver (src/multigrid.py:277-455, src/Solvers.py:258-299) */
+/* ------------------------------------------------------------------ */
+
+typedef struct pic_mg pic_mg;
+
+typedef enum pic_mg_precision {
+    PIC_MG_MIXED = 0, /* FP32 V-cycles inside an FP64 iterative-refinement loop */
+    PIC_MG_FP64 = 1   /* the same V-cycle in FP64 throughout                    */
+} pic_mg_precision;
+
+typedef struct pic_mg_options {
+    int precision;    /* pic_mg_precision */
+    int pre_sweeps;   /* red-black Gauss-Seidel sweeps before restriction (default 2) */
+    int post_sweeps;  /* sweeps after prolongation (default 2) */
+    double omega;     /* over-relaxation of the smoother (default 1.0) */
+    int coarsest_max; /* coarsen while both node counts exceed this (default 9) */
+} pic_mg_options;
+
+typedef struct pic_mg_info {
+    int cycles;        /* V-cycles run */
+    double rel_res;    /* final ||f - A phi|| / ||f|| over free nodes (FP64) */
+    double rhs_norm;   /* ||f|| */
+    int converged;     /* 1 if rel_res < tol */
+} pic_mg_info;
+
+/* MultigridSolver.__init__ (src/multigrid.py:278-309).  h_dirichlet: host
+ * uint8 mask nx*ny (1 = Dirichlet: the bc_lookup of src/Boundaries.py:9-10).
+ * Grid spacings dx, dy; (nx-1) and (ny-1) must be divisible by 2 down to
+ * the coarsest level (nodes 2^k*c+1, as the reference requires).  opts may
+ * be NULL for defaults.  Allocates device memory. */
+int pic_mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_dirichlet, const pic_mg_options* opts,
+                  pic_mg** out);
+int pic_mg_destroy(pic_mg* mg);
+
+/* MultigridSolver.solve (src/multigrid.py:445-455): iterate V-cycles until
+ * ||f - A phi||/||f|| < tol or max_cycles.  d_phi (FP64, nx*ny) holds the
+ * initial guess and the Dirichlet values on Dirichlet nodes (never changed);
+ * d_f (FP64) is the right-hand side (-rho/eps0).  Synchronises `stream` once
+ * per cycle to test convergence.  Returns PIC_ERR_NOT_CONVERGED (with *info
+ * filled) if max_cycles is reached first. */
+int pic_mg_solve(pic_mg* mg, double* d_phi, const double* d_f, double tol, int max_cycles, pic_mg_info* info,
+                 void* stream);
+
+/* Device-resident solve for graph capture: runs exactly `cycles` V-cycles
+ * with no host synchronisation; each cycle after convergence is skipped on
+ * the device (the kernels test a device flag).  Read the outcome with
+ * pic_mg_read_info after synchronising the stream. */
+int pic_mg_solve_async(pic_mg* mg, double* d_phi, const double* d_f, double tol, int cycles, void* stream);
+int pic_mg_read_info(pic_mg* mg, double tol, pic_mg_info* info);
+
+/* ------------------------------------------------------------------ */
+/* Cell sort (replaces Particles2D.sort_particles_sparse, src/Particles.py:550-632) */
+/* ------------------------------------------------------------------ */
+
+typedef struct pic_sorter pic_sorter;
+
+/* Scratch for sorting up to `capacity` particles on an nx*ny-node grid whose
+ * cells are grouped in tile x tile tiles (tile-major cell keys). */
+int pic_sorter_create(int capacity, int nx, int ny, int tile, pic_sorter** out);
+int pic_sorter_destroy(pic_sorter* s);
+
+/* Stable counting sort by tile-major cell key.  Dead slots sort last and are
+ * dropped.  Writes d_perm[k] = source slot of the k-th live particle in key
+ * order (bit-identical to a stable argsort of the keys), gathers the five
+ * arrays into the *_out arrays, writes the live count to *d_count_out
+ * (device int) and, if d_tile_start is not NULL, the first sorted slot of
+ * each tile (ntiles+1 ints).  Deterministic. */
+int pic_sort(pic_sorter* s, const float* d_x, const float* d_y, const float* d_vx, const float* d_vy,
+             const float* d_vz, int n, float* d_x_out, float* d_y_out, float* d_vx_out, float* d_vy_out,
+             float* d_vz_out, uint32_t* d_perm, int* d_count_out, int* d_tile_start, void* stream);
+
+/* ------------------------------------------------------------------ */
+/* Null-collision Monte-Carlo collisions (src/MCC.py:308-415)          */
+/* ------------------------------------------------------------------ */
+
+typedef enum pic_process_type {
+    PIC_ELASTIC = 0,        /* isotropic, with the 2m/M recoil loss           */
+    PIC_EXCITATION = 1,     /* isotropic, loses the threshold energy          */
+    PIC_IONIZATION = 2,     /* loses the threshold, splits the rest U(0.2,0.8) with a new electron, adds an ion */
+    PIC_CHARGE_EXCHANGE = 3 /* ion takes a neutral Maxwellian velocity        */
+} pic_process_type;
+
+/* Cross-section tables of one species on a shared log-spaced energy grid
+ * (h_energy[0..ne-1], eV, geometric); h_sigma[k] has ne values (m^2). */
+typedef struct pic_mcc_species_desc {
+    int nproc;
+    int type[PIC_MAX_PROCESSES];
+    double threshold[PIC_MAX_PROCESSES]; /* eV */
+    const double* h_sigma[PIC_MAX_PROCESSES];
+    int born_electron_species;           /* ionisation: species index of the new electron */
+    int born_ion_species;                /* ionisation: species index of the new ion */
+} pic_mcc_species_desc;
+
+typedef struct pic_mcc_desc {
+    int ne;
+    const double* h_energy;              /* eV, log-spaced */
+    double gas_density;                  /* m^-3 */
+    double gas_temperature;              /* K */
+    double gas_mass;                     /* kg */
+    pic_mcc_species_desc species[PIC_MAX_SPECIES]; /* nproc = 0: no collisions */
+} pic_mcc_desc;
+
+/* Birth buffer for ionisation products: positions (grid units) and
+ * velocities of new particles with their species; *count (device int) is
+ * advanced atomically and may exceed capacity (the excess is dropped and
+ * counted). */
+typedef struct pic_birth_buffer {
+    float *x, *y, *vx, *vy, *vz;
+    int* species;
+    int* count;
+    int capacity;
+} pic_birth_buffer;
+
+typedef struct pic_mcc pic_mcc;
+
+/* Uploads the tables; species_mass[s] in kg (m_type), dt in s.  Computes the
+ * null-collision frequency nu' = n_g max_E sigma_T(E) v(E) per species. */
+int pic_mcc_create(const pic_mcc_desc* desc, int nspecies, const double* species_mass, double dt, pic_mcc** out);
+int pic_mcc_destroy(pic_mcc* m);
+/* nu' (1/s), P_null = 1 - exp(-nu' dt) and 1/log(1 - P_null) of species s. */
+int pic_mcc_query(pic_mcc* m, int s, double* nu_max, double* p_null, double* inv_log1m_p);
+
+/* MCC.null_collision_method (src/MCC.py:308-415) on the n slots of species s,
+ * after their kick: selects null-collision candidates from the Philox stream
+ * (seed, step) and scatters them; ionisation products go to *births.
+ * d_counters: 30 uint64 counters, see pic_sim_counters for the meaning;
+ * index s*4+k = collisions of process k, 16+s = candidates, 20 = dropped
+ * births, 21 = nu' overflow. */
+int pic_mcc_apply(pic_mcc* m, int s, const float* d_x, const float* d_y, float* d_vx, float* d_vy, float* d_vz, int n,
+                  unsigned long long seed, unsigned int step, const pic_birth_buffer* births,
+                  unsigned long long* d_counters, void* stream);
+
+/* ------------------------------------------------------------------ */
+/* Fused time step (SimulationManager._init_step / _step, src/simulation.py:622-660) */
+/* ------------------------------------------------------------------ */
+
+typedef struct pic_sim pic_sim;
+
+typedef struct pic_species_desc {
+    int capacity;    /* slots allocated for this species */
+    double charge;   /* C (q_type) */
+    double mass;     /* kg (m_type) */
+    double np2c;     /* physical particles per macro-particle */
+} pic_species_desc;
+
+typedef struct pic_sim_desc {
+    int nx, ny;                 /* nodes */
+    double dx, dy;              /* m */
+    double dt;                  /* s */
+    double eps0;                /* F/m */
+    int nspecies;
+    pic_species_desc species[PIC_MAX_SPECIES];
+    const uint8_t* h_dirichlet; /* nx*ny, 1 = Dirichlet node */
+    const double* h_phi_bc;     /* nx*ny, potential on Dirichlet nodes (V) */
+    double tol;                 /* multigrid relative residual */
+    int max_cycles;
+    pic_mg_options mg;
+    int sort_interval;          /* steps between cell sorts (0 = never) */
+    int tile;                   /* cells per tile side (16) */
+    const pic_mcc_desc* mcc;    /* NULL: collisionless */
+    unsigned long long seed;    /* Philox key */
+    int use_graph;              /* capture the step in a CUDA graph */
+} pic_sim_desc;
+
+typedef struct pic_sim_counters {
+    unsigned long long absorbed[PIC_MAX_SPECIES];
+    unsigned long long collisions[PIC_MAX_SPECIES][PIC_MAX_PROCESSES];
+    unsigned long long null_candidates[PIC_MAX_SPECIES];
+    unsigned long long born[PIC_MAX_SPECIES];
+    unsigned long long dropped_births;
+    unsigned long long nu_overflow;
+    int count[PIC_MAX_SPECIES];   /* slots in use */
+    int last_cycles;              /* V-cycles of the last solve */
+    double last_rel_res;
+    long long steps;
+} pic_sim_counters;
+
+int pic_sim_create(const pic_sim_desc* desc, void* stream, pic_sim** out);
+int pic_sim_destroy(pic_sim* sim);
+
+/* Copy n particles of species s (device or host arrays, grid units, m/s). */
+int pic_sim_load_species(pic_sim* sim, int s, const float* x, const float* y, const float* vx, const float* vy,
+                         const float* vz, int n, int from_host, void* stream);
+
+/* _init_step: deposit, solve, E, and the half kick v -= q/m E dt/2. */
+int pic_sim_init(pic_sim* sim, void* stream);
+
+/* n_steps reference steps (_step: drift, deposit, solve, E, kick, MCC).
+ * The kick+MCC of the last step is left pending until the next step or
+ * pic_sim_sync; the state then equals the reference's after the same steps. */
+int pic_sim_step(pic_sim* sim, int n_steps, void* stream);
+int pic_sim_sync(pic_sim* sim, void* stream);
+
+/* Current device arrays of species s (the sort swaps buffers). */
+int pic_sim_species_arrays(pic_sim* sim, int s, float** x, float** y, float** vx, float** vy, float** vz);
+/* Device pointers of phi (FP64), rho (float32, last deposit), Ex, Ey (float32). */
+int pic_sim_fields(pic_sim* sim, double** phi, float** rho, float** Ex, float** Ey);
+/* Synchronises `stream` and reads counters. */
+int pic_sim_read_counters(pic_sim* sim, pic_sim_counters* out, void* stream);
+/* Kernel launches issued by this object since creation (all phases). */
+long long pic_sim_kernel_launches(pic_sim* sim);
+
+/* Per-phase device timing with CUDA events recorded on the launch stream. */
+enum {
+    PIC_PHASE_BUILD = 0, /* work items, step counter           */
+    PIC_PHASE_PUSH = 1,  /* the fused particle kernel           */
+    PIC_PHASE_MERGE = 2, /* ionisation products                 */
+    PIC_PHASE_RHS = 3,   /* rho -> f                            */
+    PIC_PHASE_SOLVE = 4, /* multigrid                           */
+    PIC_PHASE_EFIELD = 5,/* E = -grad(phi)                      */
+    PIC_PHASE_SORT = 6,  /* cell sort                           */
+    PIC_NUM_PHASES = 7
+};
+typedef struct pic_sim_profile {
+    double ms[PIC_NUM_PHASES];         /* summed device time per phase */
+    long long count[PIC_NUM_PHASES];   /* timed intervals per phase */
+    long long mg_cycles;               /* V-cycles in the timed steps */
+} pic_sim_profile;
+/* enable = 1 starts recording (and clears what was recorded), 0 stops. */
+int pic_sim_set_profiling(pic_sim* sim, int enable);
+/* Synchronises the device and sums the recorded intervals. */
+int pic_sim_read_profile(pic_sim* sim, pic_sim_profile* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PICB200_H */

@@ -1,0 +1,55 @@
+"""Solver: drop-in for src/Solvers.py:198-299, multigrid branch.
+
+``solve(grid)`` forms b = -rho/eps0 on free nodes (without the reference's
+extra dx^2, src/Solvers.py:271, which its multigrid then applies a second
+time), keeps the Dirichlet values in phi, and runs the GPU multigrid.
+The direct/cg/gmres/inverse branches use cupyx library solvers in the
+reference and are not part of this build.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import Consts, _lib
+from .multigrid import MultigridSolver
+
+
+class Solver:
+    def __init__(self, solver_type, grid, cylindrical=False, boundaries=None, tol=1e-5, precision="mixed",
+                 max_cycles=50):
+        if solver_type != "multigrid":
+            raise NotImplementedError(f"solver_type={solver_type!r}: only 'multigrid' is built")
+        if cylindrical:
+            raise NotImplementedError("cylindrical Laplacian is not part of this build")
+        self.solver_type = solver_type
+        self.m, self.n = grid.m, grid.n
+        self.dx, self.dy = grid.dx, grid.dy
+        self.cylindrical = False
+        self.tol = tol
+        self.max_cycles = max_cycles
+        self.boundaries = boundaries
+        if boundaries is not None:
+            mask = boundaries.bc_lookup_host.astype(np.uint8)
+            self.phi_bc = torch.as_tensor(boundaries.phi_bc_host, device=grid.phi.device)
+        else:
+            mask = np.zeros(grid.m * grid.n, np.uint8)
+            self.phi_bc = None
+        # the grid edges are always Dirichlet nodes of the 5-point operator
+        m2 = mask.reshape(grid.n, grid.m)
+        self._edge_mask = m2.copy()
+        self._edge_mask[0, :] = self._edge_mask[-1, :] = self._edge_mask[:, 0] = self._edge_mask[:, -1] = 1
+        self.dirichlet = torch.as_tensor(self._edge_mask.reshape(-1), device=grid.phi.device)
+        self.multigrid = MultigridSolver(self._edge_mask.reshape(-1), grid.m, grid.n, grid.dx, omega=1.0,
+                                         precision=precision, hy=grid.dy)
+        self.last_info = None
+        if self.phi_bc is not None:
+            bc = torch.as_tensor(boundaries.bc_lookup_host, device=grid.phi.device).bool()
+            grid.phi[bc] = self.phi_bc[bc]
+
+    def solve(self, grid):
+        _lib.call("pic_form_rhs", _lib.ptr(grid.rho), _lib.ptr(self.dirichlet), Consts.eps0, _lib.ptr(grid.b),
+                  grid.m, grid.n, _lib.stream_ptr())
+        grid.phi, info = self.multigrid.solve(grid.phi, grid.b, tol=self.tol, max_cycles=self.max_cycles)
+        self.last_info = self.multigrid.last_info
+        return info

@@ -1,0 +1,112 @@
+// Shared device helpers and host error plumbing for libpicb200.so (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+
+#include "picb200.h"
+
+namespace pic {
+
+// ---- host-side status handling -------------------------------------------------
+
+// Records a printf-style message for pic_last_error() and returns `code`.
+int fail(int code, const char* fmt, ...);
+void clear_error();
+
+#define PIC_CUDA(call)                                                                              \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            return ::pic::fail(PIC_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                               __FILE__, __LINE__);                                                 \
+    } while (0)
+
+#define PIC_LAUNCH_CHECK() PIC_CUDA(cudaGetLastError())
+
+#define PIC_TRY(expr)               \
+    do {                            \
+        int st_ = (expr);           \
+        if (st_ != PIC_OK) return st_; \
+    } while (0)
+
+inline cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+inline int div_up(long a, long b) { return int((a + b - 1) / b); }
+
+int num_sms();
+
+// ---- CIC weights (FP32, explicit rounding so the CPU oracle matches bit for bit) ----
+
+struct Cic {
+    int i0, j0, i1, j1;
+    float w00, w10, w01, w11;
+};
+
+// Clamp to [0, n-1], floor, neighbour = min(i0+1, n-1): the rule of
+// src/Grid.py:116-137 and src/Particles.py:140-163, in FP32 grid units.
+__device__ __forceinline__ Cic cic_weights(float gx, float gy, int nx, int ny) {
+    Cic c;
+    const float cx = fminf(fmaxf(gx, 0.0f), float(nx - 1));
+    const float cy = fminf(fmaxf(gy, 0.0f), float(ny - 1));
+    c.i0 = int(floorf(cx));
+    c.j0 = int(floorf(cy));
+    c.i1 = min(c.i0 + 1, nx - 1);
+    c.j1 = min(c.j0 + 1, ny - 1);
+    const float wx = __fsub_rn(cx, float(c.i0));
+    const float wy = __fsub_rn(cy, float(c.j0));
+    const float ux = __fsub_rn(1.0f, wx);
+    const float uy = __fsub_rn(1.0f, wy);
+    c.w00 = __fmul_rn(ux, uy);
+    c.w10 = __fmul_rn(wx, uy);
+    c.w01 = __fmul_rn(ux, wy);
+    c.w11 = __fmul_rn(wx, wy);
+    return c;
+}
+
+// Interpolated field value: ((w00*a + w10*b) + w01*c) + w11*d with the first
+// product rounded and the rest fused, in this order.
+__device__ __forceinline__ float cic_interp(const Cic& c, float a, float b, float cc, float d) {
+    float v = __fmul_rn(c.w00, a);
+    v = __fmaf_rn(c.w10, b, v);
+    v = __fmaf_rn(c.w01, cc, v);
+    v = __fmaf_rn(c.w11, d, v);
+    return v;
+}
+
+__device__ __forceinline__ bool is_live(float x) { return x == x; }
+
+// ---- Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) ----------------------------
+
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        if (r) {
+            k.x += 0x9E3779B9u;
+            k.y += 0xBB67AE85u;
+        }
+        const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+        const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    }
+    return c;
+}
+
+// Uniforms in (0, 1]: double from all 32 bits, float from the top 24 bits.
+__device__ __forceinline__ double u01_double(uint32_t x) { return (double(x) + 1.0) * (1.0 / 4294967296.0); }
+__device__ __forceinline__ float u01_float(uint32_t x) {
+    return __fadd_rn(__fmul_rn(float(x >> 8), 1.0f / 16777216.0f), 0.5f / 16777216.0f);
+}
+
+// ---- block reductions -----------------------------------------------------------
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+}  // namespace pic

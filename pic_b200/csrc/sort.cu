@@ -1,0 +1,316 @@
+// Deterministic cell sort: the replacement of Particles2D.sort_particles_sparse
+// (src/Particles.py:550-632), whose atomic slot claims give a run-to-run
+// varying order.  Here the order is a stable least-significant-digit radix
+// sort of tile-major cell keys (8-bit digits; each pass is a stable counting
+// sort):
+//   upsweep   per-CTA digit histograms over a contiguous index range
+//   scan      one CTA: exclusive scan of the digit-major count table
+//   downsweep stable ranks inside each 4096-key sub-tile (warp match_any in
+//             index order), scattered to their global slots
+// Dead particles (NaN position) get the largest key and are dropped.
+#include <algorithm>
+#include <vector>
+
+#include "sort_internal.cuh"
+
+namespace pic {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortIpt = 16;
+constexpr int kSortSub = kSortThreads * kSortIpt;
+constexpr int kRadix = 256;
+
+__global__ void k_sort_keys(const float* __restrict__ x, const float* __restrict__ y, const int* __restrict__ n_dev,
+                            int ncx, int ncy, int tile, int tiles_x, uint32_t dead_key, uint32_t* __restrict__ keys,
+                            uint32_t* __restrict__ vals, int* __restrict__ live) {
+    const int n = n_dev[0];
+    int mine = 0;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const uint32_t k = tile_key(x[p], y[p], ncx, ncy, tile, tiles_x, dead_key);
+        keys[p] = k;
+        vals[p] = uint32_t(p);
+        mine += k != dead_key;
+    }
+    mine = __reduce_add_sync(0xffffffffu, mine);
+    if ((threadIdx.x & 31) == 0 && mine) atomicAdd(live, mine);
+}
+
+__device__ __forceinline__ void cta_range(int n, int G, int g, int& b, int& e) {
+    const int per = (n + G - 1) / G;
+    b = min(n, g * per);
+    e = min(n, b + per);
+}
+
+__global__ void k_upsweep(const uint32_t* __restrict__ keys, const int* __restrict__ n_dev, int shift, int G,
+                          int* __restrict__ cnt) {
+    __shared__ int h[kRadix];
+    for (int d = threadIdx.x; d < kRadix; d += blockDim.x) h[d] = 0;
+    __syncthreads();
+    int b, e;
+    cta_range(n_dev[0], G, blockIdx.x, b, e);
+    for (int i = b + threadIdx.x; i < e; i += blockDim.x) atomicAdd(&h[(keys[i] >> shift) & 0xff], 1);
+    __syncthreads();
+    for (int d = threadIdx.x; d < kRadix; d += blockDim.x) cnt[d * G + blockIdx.x] = h[d];
+}
+
+// Exclusive scan of cnt[0 .. total) in place, one CTA of 1024 threads.
+__global__ void k_scan(int* __restrict__ cnt, int total) {
+    __shared__ int part[1024];
+    const int per = (total + blockDim.x - 1) / blockDim.x;
+    const int b = threadIdx.x * per, e = min(total, b + per);
+    int s = 0;
+    for (int i = b; i < e; ++i) s += cnt[i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 1; o < blockDim.x; o <<= 1) {
+        const int v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    int run = part[threadIdx.x] - s;
+    for (int i = b; i < e; ++i) {
+        const int c = cnt[i];
+        cnt[i] = run;
+        run += c;
+    }
+}
+
+__global__ void __launch_bounds__(kSortThreads) k_downsweep(const uint32_t* __restrict__ kin,
+                                                            const uint32_t* __restrict__ vin,
+                                                            uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                            const int* __restrict__ n_dev, int shift, int G,
+                                                            const int* __restrict__ offs) {
+    __shared__ int running[kRadix];
+    __shared__ int wc[kSortWarps][kRadix];
+    __shared__ int subtotal[kRadix];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    int b, e;
+    cta_range(n_dev[0], G, blockIdx.x, b, e);
+    for (int d = threadIdx.x; d < kRadix; d += blockDim.x) running[d] = offs[d * G + blockIdx.x];
+    for (int base = b; base < e; base += kSortSub) {
+        for (int q = threadIdx.x; q < kSortWarps * kRadix; q += blockDim.x) (&wc[0][0])[q] = 0;
+        __syncthreads();
+        uint32_t key[kSortIpt], val[kSortIpt];
+        int rank[kSortIpt];
+#pragma unroll
+        for (int it = 0; it < kSortIpt; ++it) {
+            const int idx = base + warp * (32 * kSortIpt) + it * 32 + lane;
+            const bool valid = idx < e;
+            key[it] = valid ? kin[idx] : 0u;
+            val[it] = valid ? vin[idx] : 0u;
+            const int d = valid ? int((key[it] >> shift) & 0xff) : kRadix;
+            const unsigned peers = __match_any_sync(0xffffffffu, d);
+            const int leader = __ffs(peers) - 1;
+            int basecnt = 0;
+            if (lane == leader && valid) {
+                basecnt = wc[warp][d];
+                wc[warp][d] = basecnt + __popc(peers);
+            }
+            basecnt = __shfl_sync(0xffffffffu, basecnt, leader);
+            rank[it] = valid ? basecnt + __popc(peers & lt) : -1;
+        }
+        __syncthreads();
+        for (int d = threadIdx.x; d < kRadix; d += blockDim.x) {
+            int run = 0;
+#pragma unroll
+            for (int w = 0; w < kSortWarps; ++w) {
+                const int t = wc[w][d];
+                wc[w][d] = run;
+                run += t;
+            }
+            subtotal[d] = run;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int it = 0; it < kSortIpt; ++it) {
+            if (rank[it] < 0) continue;
+            const int d = int((key[it] >> shift) & 0xff);
+            const int pos = running[d] + wc[warp][d] + rank[it];
+            kout[pos] = key[it];
+            vout[pos] = val[it];
+        }
+        __syncthreads();
+        for (int d = threadIdx.x; d < kRadix; d += blockDim.x) running[d] += subtotal[d];
+        __syncthreads();
+    }
+}
+
+// First sorted slot of each tile (lower bound of its first key) and the live count.
+__global__ void k_tile_starts(const uint32_t* __restrict__ keys, const int* __restrict__ live, int ntiles, int tt,
+                              int* __restrict__ tile_start, int* __restrict__ count_out) {
+    const int n = *live;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t <= ntiles; t += gridDim.x * blockDim.x) {
+        if (t == ntiles) {
+            if (tile_start) tile_start[t] = n;
+            if (count_out) *count_out = n;
+            continue;
+        }
+        if (!tile_start) continue;
+        const uint32_t target = uint32_t(t) * uint32_t(tt);
+        int lo = 0, hi = n;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (keys[mid] < target) lo = mid + 1;
+            else hi = mid;
+        }
+        tile_start[t] = lo;
+    }
+}
+
+__global__ void k_gather5(const uint32_t* __restrict__ perm, const int* __restrict__ live,
+                          const float* __restrict__ a0, const float* __restrict__ a1, const float* __restrict__ a2,
+                          const float* __restrict__ a3, const float* __restrict__ a4, float* __restrict__ b0,
+                          float* __restrict__ b1, float* __restrict__ b2, float* __restrict__ b3,
+                          float* __restrict__ b4, uint32_t* __restrict__ perm_out) {
+    const int n = *live;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t s = perm[k];
+        b0[k] = a0[s];
+        b1[k] = a1[s];
+        b2[k] = a2[s];
+        b3[k] = a3[s];
+        if (a4) b4[k] = a4[s];
+        if (perm_out) perm_out[k] = s;
+    }
+}
+
+__global__ void k_set_n(int* n_dev, int n) {
+    n_dev[0] = n;
+    n_dev[1] = 0;
+}
+
+__global__ void k_copy_n(int* n_dev, const int* src) {
+    n_dev[0] = *src;
+    n_dev[1] = 0;
+}
+
+int grid_blocks(long n, int threads);
+
+int sorter_create(int capacity, int nx, int ny, int tile, SortImpl* S) {
+    if (capacity < 1 || nx < 2 || ny < 2 || tile < 1) return fail(PIC_ERR_BAD_ARG, "pic_sorter_create: bad arguments");
+    S->capacity = capacity;
+    S->nx = nx;
+    S->ny = ny;
+    S->tile = tile;
+    S->tiles_x = (nx - 1 + tile - 1) / tile;
+    S->tiles_y = (ny - 1 + tile - 1) / tile;
+    S->ntiles = S->tiles_x * S->tiles_y;
+    const unsigned long long nkeys = (unsigned long long)S->ntiles * tile * tile;
+    if (nkeys >= 0xffffffffull) return fail(PIC_ERR_BAD_ARG, "pic_sorter_create: grid too large for 32-bit keys");
+    S->dead_key = uint32_t(nkeys);
+    int bits = 0;
+    while ((1ull << bits) <= nkeys) ++bits;
+    S->passes = (bits + 7) / 8;
+    S->G = std::max(1, std::min(2 * num_sms(), div_up(capacity, kSortSub)));
+    const size_t bytes = sizeof(uint32_t) * size_t(capacity);
+    for (uint32_t** p : {&S->k0, &S->k1, &S->v0, &S->v1}) {
+        PIC_CUDA(cudaMalloc(p, bytes));
+        S->allocs.push_back(*p);
+    }
+    PIC_CUDA(cudaMalloc(&S->cnt, sizeof(int) * kRadix * S->G));
+    S->allocs.push_back(S->cnt);
+    PIC_CUDA(cudaMalloc(&S->n_dev, sizeof(int) * 2));
+    S->allocs.push_back(S->n_dev);
+    return PIC_OK;
+}
+
+void sorter_free(SortImpl* S) {
+    for (void* p : S->allocs) cudaFree(p);
+    S->allocs.clear();
+}
+
+// Radix passes over S.k0/S.v0 (filled by a key kernel; S.n_dev = {n, live}),
+// then tile starts and the live count.  *perm receives the buffer holding the
+// sorted source slots.
+int sort_passes(SortImpl& S, int* tile_start, int* count_out, const uint32_t** perm, cudaStream_t st) {
+    uint32_t *ki = S.k0, *vi = S.v0, *ko = S.k1, *vo = S.v1;
+    for (int p = 0; p < S.passes; ++p) {
+        const int shift = 8 * p;
+        k_upsweep<<<S.G, kSortThreads, 0, st>>>(ki, S.n_dev, shift, S.G, S.cnt);
+        k_scan<<<1, 1024, 0, st>>>(S.cnt, kRadix * S.G);
+        k_downsweep<<<S.G, kSortThreads, 0, st>>>(ki, vi, ko, vo, S.n_dev, shift, S.G, S.cnt);
+        std::swap(ki, ko);
+        std::swap(vi, vo);
+    }
+    k_tile_starts<<<div_up(S.ntiles + 1, 256), 256, 0, st>>>(ki, S.n_dev + 1, S.ntiles, S.tile * S.tile, tile_start,
+                                                              count_out);
+    *perm = vi;
+    PIC_LAUNCH_CHECK();
+    return PIC_OK;
+}
+
+int sort_set_n(SortImpl& S, const int* d_n, cudaStream_t st) {
+    k_copy_n<<<1, 1, 0, st>>>(S.n_dev, d_n);
+    PIC_LAUNCH_CHECK();
+    return PIC_OK;
+}
+
+// Sorts the live particles of [0, *d_n) (device count); see pic_sort.
+int sort_run(SortImpl& S, const int* d_n, const float* x, const float* y, const float* vx, const float* vy,
+             const float* vz, float* xo, float* yo, float* vxo, float* vyo, float* vzo, uint32_t* perm_out,
+             int* count_out, int* tile_start, cudaStream_t st) {
+    PIC_TRY(sort_set_n(S, d_n, st));
+    const int cap = S.capacity;
+    k_sort_keys<<<grid_blocks(cap, 256), 256, 0, st>>>(x, y, S.n_dev, S.nx - 1, S.ny - 1, S.tile, S.tiles_x,
+                                                       S.dead_key, S.k0, S.v0, S.n_dev + 1);
+    const uint32_t* perm = nullptr;
+    PIC_TRY(sort_passes(S, tile_start, count_out, &perm, st));
+    if (xo) k_gather5<<<grid_blocks(cap, 256), 256, 0, st>>>(perm, S.n_dev + 1, x, y, vx, vy, vz, xo, yo, vxo, vyo,
+                                                             vzo, perm_out);
+    else if (perm_out)
+        PIC_CUDA(cudaMemcpyAsync(perm_out, perm, sizeof(uint32_t) * cap, cudaMemcpyDeviceToDevice, st));
+    PIC_LAUNCH_CHECK();
+    return PIC_OK;
+}
+
+}  // namespace pic
+
+struct pic_sorter {
+    pic::SortImpl s;
+};
+
+using namespace pic;
+
+extern "C" {
+
+int pic_sorter_create(int capacity, int nx, int ny, int tile, pic_sorter** out) {
+    clear_error();
+    if (!out) return fail(PIC_ERR_BAD_ARG, "pic_sorter_create: out is NULL");
+    pic_sorter* s = new pic_sorter;
+    const int st = sorter_create(capacity, nx, ny, tile, &s->s);
+    if (st != PIC_OK) {
+        sorter_free(&s->s);
+        delete s;
+        return st;
+    }
+    *out = s;
+    return PIC_OK;
+}
+
+int pic_sorter_destroy(pic_sorter* s) {
+    clear_error();
+    if (!s) return PIC_OK;
+    sorter_free(&s->s);
+    delete s;
+    return PIC_OK;
+}
+
+int pic_sort(pic_sorter* s, const float* d_x, const float* d_y, const float* d_vx, const float* d_vy,
+             const float* d_vz, int n, float* d_x_out, float* d_y_out, float* d_vx_out, float* d_vy_out,
+             float* d_vz_out, uint32_t* d_perm, int* d_count_out, int* d_tile_start, void* stream) {
+    clear_error();
+    if (!s || n < 0 || n > s->s.capacity || !d_x || !d_y)
+        return fail(PIC_ERR_BAD_ARG, "pic_sort: bad arguments (n=%d, capacity=%d)", n, s ? s->s.capacity : 0);
+    if (d_x_out && (!d_y_out || !d_vx_out || !d_vy_out || !d_vx || !d_vy || (d_vz && !d_vz_out)))
+        return fail(PIC_ERR_BAD_ARG, "pic_sort: output arrays incomplete");
+    cudaStream_t st = as_stream(stream);
+    k_set_n<<<1, 1, 0, st>>>(s->s.n_dev, n);
+    // sort_run copies the count from a device int; n_dev itself holds it here
+    return sort_run(s->s, s->s.n_dev, d_x, d_y, d_vx, d_vy, d_vz, d_x_out, d_y_out, d_vx_out, d_vy_out, d_vz_out,
+                    d_perm, d_count_out, d_tile_start, st);
+}
+
+}  // extern "C"

@@ -1,0 +1,870 @@
+// The fused time step (SimulationManager._init_step / _step,
+// src/simulation.py:622-660).
+//
+// Reference order per step: drift (update_R), deposit, solve, E, kick
+// (update_V), MCC.  Moving the loop boundary gives the same operator sequence
+// with one particle pass per step:
+//     [kick + MCC + drift + absorb + deposit]  ->  RHS  ->  multigrid  ->  E
+// The kick and MCC of the last step stay pending until the next step or
+// pic_sim_sync, so after a sync the state equals the reference's.
+//
+// Particle pass: persistent CTAs take work items (species, tile, [begin,end))
+// from an atomic counter.  Items of sorted particles belong to one tile of
+// tile x tile cells: the CTA stages the tile's E field (with a halo) and a
+// charge accumulator in shared memory, processes its particles in a blocked
+// order (consecutive sorted particles per thread, so the deposit accumulates
+// in registers while the cell repeats) and flushes the charge tile once with
+// global atomics.  Particles that left the staged region since the last sort
+// gather from and deposit to global memory directly.  Particles born since
+// the last sort are processed as untiled items.
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <vector>
+
+#include "mcc_host.cuh"
+#include "sort_internal.cuh"
+
+namespace pic {
+
+int grid_blocks(long n, int threads);
+int launch_update_E(const double* phi, float* Ex, float* Ey, float2* E2, int nx, int ny, double dx, double dy,
+                    cudaStream_t st);
+int launch_form_rhs(const float* rho, const uint8_t* dirichlet, double eps0, double* f, float* snapshot, float* zero,
+                    long G, cudaStream_t st);
+struct MgImpl;
+int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const pic_mg_options* opts, pic_mg** out);
+long long mg_launches(pic_mg* mg);
+
+constexpr int kPushThreads = 256;
+constexpr int kPushP = 9;  // particles per thread (odd: conflict-free blocked access to shared memory)
+constexpr int kChunk = kPushThreads * kPushP;
+constexpr int kHalo = 4;   // cells staged around a tile
+
+// Device-resident per-species state (the sort swaps the buffers).
+struct SpeciesState {
+    float* cur[5];  // x, y, vx, vy, vz
+    float* alt[5];
+    int count;       // slots in use
+    int sorted_end;  // slots covered by tile items
+    int capacity;
+    int pad;
+};
+
+struct SpeciesConst {
+    float kq;          // q/m dt (times the kick factor)
+    float dtdx, dtdy;  // dt/dx, dt/dy
+    float scale;       // q np2c / (dx dy)
+};
+
+struct PushArgs {
+    SpeciesState* state;
+    SpeciesConst sp[PIC_MAX_SPECIES];
+    const int4* items;
+    const int* n_items;
+    int* item_next;
+    const float2* E;
+    float* rho;
+    int nx, ny, tile, tiles_x, rw;
+    int do_kick, do_mcc, do_drift, do_deposit;
+    MccDev mcc;
+    uint2 key;
+    const uint32_t* step;
+    BirthDev births;
+    unsigned long long* ctr;
+};
+
+__device__ __forceinline__ void flush_run(const PushArgs& A, float* rt, bool tiled, int ox, int oy, int i0, int j0,
+                                          int i1, int j1, float scale, float s00, float s10, float s01, float s11) {
+    const int ii[4] = {i0, i1, i0, i1};
+    const int jj[4] = {j0, j0, j1, j1};
+    const float vv[4] = {s00, s10, s01, s11};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        if (vv[q] == 0.0f) continue;
+        const float v = __fmul_rn(scale, vv[q]);
+        const int li = ii[q] - ox, lj = jj[q] - oy;
+        if (tiled && li >= 0 && lj >= 0 && li < A.rw && lj < A.rw) atomicAdd(rt + lj * A.rw + li, v);
+        else atomicAdd(A.rho + long(jj[q]) * A.nx + ii[q], v);
+    }
+}
+
+__global__ void __launch_bounds__(kPushThreads) k_push(PushArgs A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    float* px = reinterpret_cast<float*>(smem);
+    float* py = px + kChunk;
+    float* pvx = py + kChunk;
+    float* pvy = pvx + kChunk;
+    float* pvz = pvy + kChunk;
+    const int RW = A.rw;
+    float2* et = reinterpret_cast<float2*>(pvz + kChunk);
+    float* rt = reinterpret_cast<float*>(et + RW * RW);
+    unsigned* bits = reinterpret_cast<unsigned*>(rt + RW * RW);
+    __shared__ int s_item;
+    __shared__ unsigned s_abs, s_cand;
+    const int tid = threadIdx.x;
+    const uint32_t step = A.do_mcc ? *A.step : 0u;
+    for (;;) {
+        if (tid == 0) {
+            s_item = atomicAdd(A.item_next, 1);
+            s_abs = 0;
+            s_cand = 0;
+        }
+        __syncthreads();
+        const int it = s_item;
+        if (it >= *A.n_items) break;
+        const int4 item = A.items[it];
+        const int s = item.x, tile = item.y, b = item.z, e = item.w, n = e - b;
+        const SpeciesConst C = A.sp[s];
+        float* const gx = A.state[s].cur[0];
+        float* const gy = A.state[s].cur[1];
+        float* const gvx = A.state[s].cur[2];
+        float* const gvy = A.state[s].cur[3];
+        float* const gvz = A.state[s].cur[4];
+        for (int l = tid; l < n; l += kPushThreads) {
+            px[l] = gx[b + l];
+            py[l] = gy[b + l];
+            pvx[l] = gvx[b + l];
+            pvy[l] = gvy[b + l];
+            pvz[l] = gvz[b + l];
+        }
+        const bool tiled = tile >= 0;
+        int ox = 0, oy = 0;
+        if (tiled) {
+            ox = (tile % A.tiles_x) * A.tile - kHalo;
+            oy = (tile / A.tiles_x) * A.tile - kHalo;
+            for (int q = tid; q < RW * RW; q += kPushThreads) {
+                const int gi = ox + q % RW, gj = oy + q / RW;
+                et[q] = (gi >= 0 && gj >= 0 && gi < A.nx && gj < A.ny) ? A.E[long(gj) * A.nx + gi]
+                                                                         : make_float2(0.f, 0.f);
+                rt[q] = 0.0f;
+            }
+        }
+        const bool mcc = A.do_mcc && A.mcc.sp[s].nproc > 0;
+        if (mcc) {
+            for (int q = tid; q < kChunk / 32; q += kPushThreads) bits[q] = 0;
+            __syncthreads();
+            if (tid < 32) {
+                const long g0 = b / long(kMccSegment), g1 = (e - 1) / long(kMccSegment);
+                const int slots = A.state[s].count;
+                for (long g = g0 + tid; g <= g1; g += 32)
+                    mcc_mark_segment(A.mcc.sp[s], uint32_t(s), g, slots, b, e, step, A.key, bits);
+            }
+        }
+        __syncthreads();
+
+        int ri0 = -1, rj0 = 0, ri1 = 0, rj1 = 0;
+        float s00 = 0.f, s10 = 0.f, s01 = 0.f, s11 = 0.f;
+        unsigned my_abs = 0, my_cand = 0;
+        for (int k = 0; k < kPushP; ++k) {
+            const int l = tid * kPushP + k;
+            if (l >= n) break;
+            float x = px[l], y = py[l];
+            if (!is_live(x)) continue;
+            float vx = pvx[l], vy = pvy[l], vz = pvz[l];
+            if (A.do_kick) {
+                const Cic c = cic_weights(x, y, A.nx, A.ny);
+                const int li = c.i0 - ox, lj = c.j0 - oy;
+                float2 e00, e10, e01, e11;
+                if (tiled && li >= 0 && lj >= 0 && li + 1 < RW && lj + 1 < RW) {
+                    const int q = lj * RW + li;
+                    e00 = et[q];
+                    e10 = et[q + (c.i1 - c.i0)];
+                    e01 = et[q + (c.j1 - c.j0) * RW];
+                    e11 = et[q + (c.j1 - c.j0) * RW + (c.i1 - c.i0)];
+                } else {
+                    e00 = __ldg(A.E + long(c.j0) * A.nx + c.i0);
+                    e10 = __ldg(A.E + long(c.j0) * A.nx + c.i1);
+                    e01 = __ldg(A.E + long(c.j1) * A.nx + c.i0);
+                    e11 = __ldg(A.E + long(c.j1) * A.nx + c.i1);
+                }
+                const float ex = cic_interp(c, e00.x, e10.x, e01.x, e11.x);
+                const float ey = cic_interp(c, e00.y, e10.y, e01.y, e11.y);
+                vx = __fmaf_rn(C.kq, ex, vx);
+                vy = __fmaf_rn(C.kq, ey, vy);
+            }
+            if (mcc && (bits[l >> 5] & (1u << (l & 31)))) {
+                ++my_cand;
+                const MccOutcome o =
+                    mcc_collide(A.mcc, A.mcc.sp[s], uint32_t(s), uint32_t(b + l), step, A.key, vx, vy, vz);
+                if (o.overflow) atomicAdd(A.ctr + kCtrOverflow, 1ull);
+                if (o.proc >= 0) {
+                    atomicAdd(A.ctr + kCtrCollisions + s * PIC_MAX_PROCESSES + o.proc, 1ull);
+                    if (o.born) {
+                        const MccSpeciesDev& S = A.mcc.sp[s];
+                        const bool ok_e = birth_push(A.births, S.born_e, x, y, o.be[0], o.be[1], o.be[2]);
+                        const bool ok_i = birth_push(A.births, S.born_i, x, y, o.bi[0], o.bi[1], o.bi[2]);
+                        if (!ok_e || !ok_i) atomicAdd(A.ctr + kCtrDropped, 1ull);
+                    }
+                }
+            }
+            if (A.do_drift) {
+                x = __fmaf_rn(vx, C.dtdx, x);
+                y = __fmaf_rn(vy, C.dtdy, y);
+                if (!(x >= 0.0f && x <= float(A.nx - 1) && y >= 0.0f && y <= float(A.ny - 1))) {
+                    x = __int_as_float(0x7fc00000);
+                    y = x;
+                    ++my_abs;
+                }
+            }
+            px[l] = x;
+            py[l] = y;
+            pvx[l] = vx;
+            pvy[l] = vy;
+            pvz[l] = vz;
+            if (A.do_deposit && is_live(x)) {
+                const Cic c = cic_weights(x, y, A.nx, A.ny);
+                if (c.i0 != ri0 || c.j0 != rj0) {
+                    if (ri0 >= 0) flush_run(A, rt, tiled, ox, oy, ri0, rj0, ri1, rj1, C.scale, s00, s10, s01, s11);
+                    ri0 = c.i0;
+                    rj0 = c.j0;
+                    ri1 = c.i1;
+                    rj1 = c.j1;
+                    s00 = s10 = s01 = s11 = 0.f;
+                }
+                s00 += c.w00;
+                s10 += c.w10;
+                s01 += c.w01;
+                s11 += c.w11;
+            }
+        }
+        if (ri0 >= 0) flush_run(A, rt, tiled, ox, oy, ri0, rj0, ri1, rj1, C.scale, s00, s10, s01, s11);
+        my_abs = __reduce_add_sync(0xffffffffu, my_abs);
+        my_cand = __reduce_add_sync(0xffffffffu, my_cand);
+        if ((tid & 31) == 0) {
+            if (my_abs) atomicAdd(&s_abs, my_abs);
+            if (my_cand) atomicAdd(&s_cand, my_cand);
+        }
+        __syncthreads();
+        for (int l = tid; l < n; l += kPushThreads) {
+            gx[b + l] = px[l];
+            gy[b + l] = py[l];
+            gvx[b + l] = pvx[l];
+            gvy[b + l] = pvy[l];
+            gvz[b + l] = pvz[l];
+        }
+        if (tiled && A.do_deposit) {
+            for (int q = tid; q < RW * RW; q += kPushThreads) {
+                const float v = rt[q];
+                if (v != 0.0f) atomicAdd(A.rho + long(oy + q / RW) * A.nx + ox + q % RW, v);
+            }
+        }
+        if (tid == 0) {
+            if (s_abs) atomicAdd(A.ctr + kCtrAbsorbed + s, (unsigned long long)s_abs);
+            if (s_cand) atomicAdd(A.ctr + kCtrCandidates + s, (unsigned long long)s_cand);
+        }
+        __syncthreads();
+    }
+}
+
+// Ionisation products: drift, absorb and deposit them (global atomics) and
+// append them to their species.
+__global__ void k_merge_births(PushArgs A) {
+    const int nb = min(*A.births.count, A.births.capacity);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
+        const int s = A.births.species[i];
+        const SpeciesConst C = A.sp[s];
+        float x = A.births.x[i], y = A.births.y[i];
+        const float vx = A.births.vx[i], vy = A.births.vy[i], vz = A.births.vz[i];
+        if (A.do_drift) {
+            x = __fmaf_rn(vx, C.dtdx, x);
+            y = __fmaf_rn(vy, C.dtdy, y);
+            // a product that leaves the domain in its first drift is never stored
+            if (!(x >= 0.0f && x <= float(A.nx - 1) && y >= 0.0f && y <= float(A.ny - 1))) continue;
+        }
+        SpeciesState& S = A.state[s];
+        const int slot = atomicAdd(&S.count, 1);
+        if (slot >= S.capacity) {
+            atomicSub(&S.count, 1);
+            atomicAdd(A.ctr + kCtrDropped, 1ull);
+            continue;
+        }
+        S.cur[0][slot] = x;
+        S.cur[1][slot] = y;
+        S.cur[2][slot] = vx;
+        S.cur[3][slot] = vy;
+        S.cur[4][slot] = vz;
+        atomicAdd(A.ctr + kCtrBorn + s, 1ull);
+        if (A.do_deposit) {
+            const Cic c = cic_weights(x, y, A.nx, A.ny);
+            atomicAdd(A.rho + long(c.j0) * A.nx + c.i0, __fmul_rn(C.scale, c.w00));
+            atomicAdd(A.rho + long(c.j0) * A.nx + c.i1, __fmul_rn(C.scale, c.w10));
+            atomicAdd(A.rho + long(c.j1) * A.nx + c.i0, __fmul_rn(C.scale, c.w01));
+            atomicAdd(A.rho + long(c.j1) * A.nx + c.i1, __fmul_rn(C.scale, c.w11));
+        }
+    }
+}
+
+// Per step: untiled items for slots past the last sort, item counter reset,
+// RNG step advance, birth buffer reset.
+__global__ void k_build_items(SpeciesState* state, int nspecies, const int* n_tiled, int4* items, int* n_items,
+                              int* item_next, uint32_t* step, int* birth_count, int advance_step) {
+    __shared__ int off[PIC_MAX_SPECIES + 1];
+    if (threadIdx.x == 0) {
+        int o = *n_tiled;
+        for (int s = 0; s < nspecies; ++s) {
+            off[s] = o;
+            const int u = state[s].count - state[s].sorted_end;
+            o += u > 0 ? (u + kChunk - 1) / kChunk : 0;
+        }
+        off[nspecies] = o;
+        *n_items = o;
+        *item_next = 0;
+        *birth_count = 0;
+        if (advance_step) *step += 1u;
+    }
+    __syncthreads();
+    for (int s = 0; s < nspecies; ++s) {
+        const int b0 = state[s].sorted_end, e0 = state[s].count;
+        for (int c = threadIdx.x; c < off[s + 1] - off[s]; c += blockDim.x) {
+            const int b = b0 + c * kChunk;
+            items[off[s] + c] = make_int4(s, -1, b, min(e0, b + kChunk));
+        }
+    }
+}
+
+// After a sort: items for every (species, tile), split into chunks.
+__global__ void k_tile_items(const int* __restrict__ tile_start, int ntiles, int nspecies, int4* items,
+                             int* n_tiled) {
+    __shared__ int part[1024];
+    const int total = ntiles * nspecies;
+    const int per = (total + blockDim.x - 1) / blockDim.x;
+    const int b = threadIdx.x * per, e = min(total, b + per);
+    int sum = 0;
+    for (int q = b; q < e; ++q) {
+        const int s = q / ntiles, t = q % ntiles;
+        const int* ts = tile_start + s * (ntiles + 1);
+        sum += (ts[t + 1] - ts[t] + kChunk - 1) / kChunk;
+    }
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (int o = 1; o < blockDim.x; o <<= 1) {
+        const int v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    int w = part[threadIdx.x] - sum;
+    for (int q = b; q < e; ++q) {
+        const int s = q / ntiles, t = q % ntiles;
+        const int* ts = tile_start + s * (ntiles + 1);
+        for (int c = ts[t]; c < ts[t + 1]; c += kChunk) items[w++] = make_int4(s, t, c, min(ts[t + 1], c + kChunk));
+    }
+    if (threadIdx.x == blockDim.x - 1) *n_tiled = part[threadIdx.x];
+}
+
+__global__ void k_sim_keys(const SpeciesState* __restrict__ state, int s, int ncx, int ncy, int tile, int tiles_x,
+                           uint32_t dead_key, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                           int* __restrict__ n_dev) {
+    const int n = state[s].count;
+    const float* __restrict__ x = state[s].cur[0];
+    const float* __restrict__ y = state[s].cur[1];
+    int mine = 0;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const uint32_t k = tile_key(x[p], y[p], ncx, ncy, tile, tiles_x, dead_key);
+        keys[p] = k;
+        vals[p] = uint32_t(p);
+        mine += k != dead_key;
+    }
+    mine = __reduce_add_sync(0xffffffffu, mine);
+    if ((threadIdx.x & 31) == 0 && mine) atomicAdd(n_dev + 1, mine);
+}
+
+__global__ void k_sim_gather(const SpeciesState* __restrict__ state, int s, const uint32_t* __restrict__ perm,
+                             const int* __restrict__ n_dev) {
+    const int n = n_dev[1];
+    const SpeciesState& S = state[s];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t src = perm[k];
+#pragma unroll
+        for (int c = 0; c < 5; ++c) S.alt[c][k] = S.cur[c][src];
+    }
+}
+
+__global__ void k_sim_flip(SpeciesState* state, int s, const int* n_dev) {
+    SpeciesState& S = state[s];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+        float* t = S.cur[c];
+        S.cur[c] = S.alt[c];
+        S.alt[c] = t;
+    }
+    S.count = n_dev[1];
+    S.sorted_end = n_dev[1];
+}
+
+__global__ void k_set_count(SpeciesState* state, int s, int n) {
+    state[s].count = n;
+    state[s].sorted_end = 0;
+}
+
+// Loading particles invalidates the tile items of every species.
+__global__ void k_untile_all(SpeciesState* state, int nspecies, int* n_tiled) {
+    for (int s = 0; s < nspecies; ++s) state[s].sorted_end = 0;
+    *n_tiled = 0;
+}
+
+// ---- host object -----------------------------------------------------------------
+
+struct SimImpl {
+    pic_sim_desc d{};
+    int nx = 0, ny = 0, ns = 0;
+    long G = 0;
+    SortImpl sorter;
+    bool have_sorter = false;
+    pic_mg* mg = nullptr;
+    MccHost mcc;
+    bool have_mcc = false;
+    std::vector<void*> allocs;
+    SpeciesState* d_state = nullptr;
+    SpeciesState h_state[PIC_MAX_SPECIES]{};
+    SpeciesConst sc[PIC_MAX_SPECIES]{};
+    int4* items = nullptr;
+    int item_cap = 0;
+    int *n_items = nullptr, *item_next = nullptr, *n_tiled = nullptr;
+    uint32_t* step_ctr = nullptr;
+    int* tile_start = nullptr;
+    BirthDev births{};
+    unsigned long long* ctr = nullptr;
+    float2* E2 = nullptr;
+    float *Ex = nullptr, *Ey = nullptr, *rho_acc = nullptr, *rho_out = nullptr;
+    double *phi = nullptr, *f = nullptr;
+    uint8_t* dirichlet = nullptr;
+    int push_grid = 0;
+    size_t push_smem = 0;
+    int rw = 0;
+    bool kick_pending = false;
+    long long steps = 0;
+    long long launches = 0;
+    bool profiling = false;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
+    std::vector<cudaEvent_t> event_pool;
+    long long prof_cycles = 0;
+    pic_mg_info last{};
+    int last_status = PIC_OK;
+};
+
+template <class T>
+static int dalloc(SimImpl& S, T** p, size_t n) {
+    PIC_CUDA(cudaMalloc(p, sizeof(T) * std::max<size_t>(n, 1)));
+    S.allocs.push_back(*p);
+    PIC_CUDA(cudaMemset(*p, 0, sizeof(T) * std::max<size_t>(n, 1)));
+    return PIC_OK;
+}
+
+// Phase timing: begin() records a start event, end() the matching stop event.
+static cudaEvent_t take_event(SimImpl& S) {
+    if (!S.event_pool.empty()) {
+        cudaEvent_t e = S.event_pool.back();
+        S.event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+struct PhaseTimer {
+    SimImpl& S;
+    int phase;
+    cudaStream_t st;
+    cudaEvent_t a = nullptr;
+    PhaseTimer(SimImpl& s, int p, cudaStream_t stream) : S(s), phase(p), st(stream) {
+        if (S.profiling) {
+            a = take_event(S);
+            cudaEventRecord(a, st);
+        }
+    }
+    ~PhaseTimer() {
+        if (a) {
+            cudaEvent_t b = take_event(S);
+            cudaEventRecord(b, st);
+            S.marks.push_back({phase, {a, b}});
+        }
+    }
+};
+
+static PushArgs push_args(SimImpl& S, int kick, int mcc, int drift, int deposit, double kick_factor) {
+    PushArgs A{};
+    A.state = S.d_state;
+    for (int s = 0; s < S.ns; ++s) {
+        A.sp[s] = S.sc[s];
+        const pic_species_desc& sp = S.d.species[s];
+        A.sp[s].kq = float(sp.charge / sp.mass * S.d.dt * kick_factor);
+    }
+    A.items = S.items;
+    A.n_items = S.n_items;
+    A.item_next = S.item_next;
+    A.E = S.E2;
+    A.rho = S.rho_acc;
+    A.nx = S.nx;
+    A.ny = S.ny;
+    A.tile = S.d.tile;
+    A.tiles_x = S.have_sorter ? S.sorter.tiles_x : 1;
+    A.rw = S.rw;
+    A.do_kick = kick;
+    A.do_mcc = mcc && S.have_mcc;
+    A.do_drift = drift;
+    A.do_deposit = deposit;
+    if (S.have_mcc) A.mcc = S.mcc.dev;
+    A.key = make_uint2(uint32_t(S.d.seed), uint32_t(S.d.seed >> 32));
+    A.step = S.step_ctr;
+    A.births = S.births;
+    A.ctr = S.ctr;
+    return A;
+}
+
+static int particle_pass(SimImpl& S, cudaStream_t st, int kick, int mcc, int drift, int deposit, double kick_factor,
+                         int advance_step) {
+    {
+        PhaseTimer t(S, PIC_PHASE_BUILD, st);
+        k_build_items<<<1, 256, 0, st>>>(S.d_state, S.ns, S.n_tiled, S.items, S.n_items, S.item_next, S.step_ctr,
+                                         S.births.count, advance_step);
+    }
+    const PushArgs A = push_args(S, kick, mcc, drift, deposit, kick_factor);
+    {
+        PhaseTimer t(S, PIC_PHASE_PUSH, st);
+        k_push<<<S.push_grid, kPushThreads, S.push_smem, st>>>(A);
+    }
+    {
+        PhaseTimer t(S, PIC_PHASE_MERGE, st);
+        k_merge_births<<<64, 256, 0, st>>>(A);
+    }
+    S.launches += 3;
+    PIC_LAUNCH_CHECK();
+    return PIC_OK;
+}
+
+static int field_solve(SimImpl& S, cudaStream_t st) {
+    {
+        PhaseTimer t(S, PIC_PHASE_RHS, st);
+        PIC_TRY(launch_form_rhs(S.rho_acc, S.dirichlet, S.d.eps0, S.f, S.rho_out, S.rho_acc, S.G, st));
+    }
+    pic_mg_info info{};
+    int rc;
+    const long long before = mg_launches(S.mg);
+    {
+        PhaseTimer t(S, PIC_PHASE_SOLVE, st);
+        rc = pic_mg_solve(S.mg, S.phi, S.f, S.d.tol, S.d.max_cycles, &info, st);
+    }
+    S.launches += 1 + (mg_launches(S.mg) - before);
+    S.last = info;
+    S.last_status = rc;
+    if (S.profiling) S.prof_cycles += info.cycles;
+    if (rc != PIC_OK && rc != PIC_ERR_NOT_CONVERGED) return rc;
+    {
+        PhaseTimer t(S, PIC_PHASE_EFIELD, st);
+        PIC_TRY(launch_update_E(S.phi, S.Ex, S.Ey, S.E2, S.nx, S.ny, S.d.dx, S.d.dy, st));
+    }
+    S.launches += 1;
+    return PIC_OK;
+}
+
+static int sort_all(SimImpl& S, cudaStream_t st) {
+    PhaseTimer t(S, PIC_PHASE_SORT, st);
+    SortImpl& R = S.sorter;
+    S.launches += 1 + (long long)(S.ns) * (5 + 3 * R.passes);
+    for (int s = 0; s < S.ns; ++s) {
+        int* count_ptr = reinterpret_cast<int*>(reinterpret_cast<char*>(S.d_state + s) + offsetof(SpeciesState, count));
+        PIC_TRY(sort_set_n(R, count_ptr, st));
+        k_sim_keys<<<grid_blocks(S.d.species[s].capacity, 256), 256, 0, st>>>(
+            S.d_state, s, S.nx - 1, S.ny - 1, R.tile, R.tiles_x, R.dead_key, R.k0, R.v0, R.n_dev);
+        const uint32_t* perm = nullptr;
+        PIC_TRY(sort_passes(R, S.tile_start + s * (R.ntiles + 1), nullptr, &perm, st));
+        k_sim_gather<<<grid_blocks(S.d.species[s].capacity, 256), 256, 0, st>>>(S.d_state, s, perm, R.n_dev);
+        k_sim_flip<<<1, 1, 0, st>>>(S.d_state, s, R.n_dev);
+    }
+    k_tile_items<<<1, 1024, 0, st>>>(S.tile_start, R.ntiles, S.ns, S.items, S.n_tiled);
+    PIC_LAUNCH_CHECK();
+    return PIC_OK;
+}
+
+static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
+    if (!d || d->nx < 3 || d->ny < 3 || !(d->dx > 0) || !(d->dy > 0) || !(d->dt > 0) || !(d->eps0 > 0) ||
+        d->nspecies < 1 || d->nspecies > PIC_MAX_SPECIES || !d->h_dirichlet || !(d->tol > 0) || d->max_cycles < 1)
+        return fail(PIC_ERR_BAD_ARG, "pic_sim_create: bad descriptor");
+    S.d = *d;
+    if (S.d.tile <= 0) S.d.tile = 16;
+    S.nx = d->nx;
+    S.ny = d->ny;
+    S.ns = d->nspecies;
+    S.G = long(S.nx) * S.ny;
+    S.rw = S.d.tile + 1 + 2 * kHalo;
+    PIC_TRY(mg_create(S.nx, S.ny, d->dx, d->dy, d->h_dirichlet, &d->mg, &S.mg));
+    long max_cap = 0;
+    for (int s = 0; s < S.ns; ++s) {
+        const pic_species_desc& sp = d->species[s];
+        if (sp.capacity < 1 || !(sp.mass > 0) || !(sp.np2c > 0))
+            return fail(PIC_ERR_BAD_ARG, "pic_sim_create: species %d needs capacity, mass and np2c", s);
+        max_cap = std::max<long>(max_cap, sp.capacity);
+    }
+    PIC_TRY(sorter_create(int(max_cap), S.nx, S.ny, S.d.tile, &S.sorter));
+    S.have_sorter = true;
+    if (d->mcc) {
+        double mass[PIC_MAX_SPECIES];
+        for (int s = 0; s < S.ns; ++s) mass[s] = d->species[s].mass;
+        PIC_TRY(mcc_build(d->mcc, S.ns, mass, d->dt, &S.mcc));
+        S.have_mcc = true;
+    }
+    // species buffers
+    for (int s = 0; s < S.ns; ++s) {
+        const pic_species_desc& sp = d->species[s];
+        SpeciesState& H = S.h_state[s];
+        for (int c = 0; c < 5; ++c) {
+            PIC_TRY(dalloc(S, &H.cur[c], size_t(sp.capacity)));
+            PIC_TRY(dalloc(S, &H.alt[c], size_t(sp.capacity)));
+        }
+        H.count = 0;
+        H.sorted_end = 0;
+        H.capacity = sp.capacity;
+        SpeciesConst& C = S.sc[s];
+        C.kq = float(sp.charge / sp.mass * d->dt);
+        C.dtdx = float(d->dt / d->dx);
+        C.dtdy = float(d->dt / d->dy);
+        C.scale = float(sp.charge * sp.np2c / (d->dx * d->dy));
+    }
+    PIC_TRY(dalloc(S, &S.d_state, size_t(S.ns)));
+    PIC_CUDA(cudaMemcpy(S.d_state, S.h_state, sizeof(SpeciesState) * S.ns, cudaMemcpyHostToDevice));
+    // work items
+    S.item_cap = 4;
+    for (int s = 0; s < S.ns; ++s) S.item_cap += S.sorter.ntiles + 2 * (d->species[s].capacity / kChunk + 2);
+    PIC_TRY(dalloc(S, &S.items, size_t(S.item_cap)));
+    PIC_TRY(dalloc(S, &S.n_items, 1));
+    PIC_TRY(dalloc(S, &S.item_next, 1));
+    PIC_TRY(dalloc(S, &S.n_tiled, 1));
+    PIC_TRY(dalloc(S, &S.step_ctr, 1));
+    PIC_TRY(dalloc(S, &S.tile_start, size_t(S.ns) * (S.sorter.ntiles + 1)));
+    // births
+    int bcap = 1 << 16;
+    for (int s = 0; s < S.ns; ++s) bcap = std::max(bcap, d->species[s].capacity / 64);
+    S.births.capacity = bcap;
+    PIC_TRY(dalloc(S, &S.births.x, size_t(bcap)));
+    PIC_TRY(dalloc(S, &S.births.y, size_t(bcap)));
+    PIC_TRY(dalloc(S, &S.births.vx, size_t(bcap)));
+    PIC_TRY(dalloc(S, &S.births.vy, size_t(bcap)));
+    PIC_TRY(dalloc(S, &S.births.vz, size_t(bcap)));
+    PIC_TRY(dalloc(S, &S.births.species, size_t(bcap)));
+    PIC_TRY(dalloc(S, &S.births.count, 1));
+    PIC_TRY(dalloc(S, &S.ctr, size_t(kCtrCount)));
+    // fields
+    PIC_TRY(dalloc(S, &S.E2, size_t(S.G)));
+    PIC_TRY(dalloc(S, &S.Ex, size_t(S.G)));
+    PIC_TRY(dalloc(S, &S.Ey, size_t(S.G)));
+    PIC_TRY(dalloc(S, &S.rho_acc, size_t(S.G)));
+    PIC_TRY(dalloc(S, &S.rho_out, size_t(S.G)));
+    PIC_TRY(dalloc(S, &S.phi, size_t(S.G)));
+    PIC_TRY(dalloc(S, &S.f, size_t(S.G)));
+    PIC_TRY(dalloc(S, &S.dirichlet, size_t(S.G)));
+    std::vector<uint8_t> mask(d->h_dirichlet, d->h_dirichlet + S.G);
+    for (auto& v : mask) v = v ? 1 : 0;
+    PIC_CUDA(cudaMemcpy(S.dirichlet, mask.data(), S.G, cudaMemcpyHostToDevice));
+    if (d->h_phi_bc) {
+        std::vector<double> phi0(S.G, 0.0);
+        for (long k = 0; k < S.G; ++k)
+            if (mask[k]) phi0[k] = d->h_phi_bc[k];
+        PIC_CUDA(cudaMemcpy(S.phi, phi0.data(), sizeof(double) * S.G, cudaMemcpyHostToDevice));
+    }
+    // launch shape of the particle pass
+    S.push_smem = sizeof(float) * 5 * kChunk + size_t(S.rw) * S.rw * (sizeof(float2) + sizeof(float)) +
+                  sizeof(unsigned) * (kChunk / 32 + 1);
+    PIC_CUDA(cudaFuncSetAttribute(k_push, cudaFuncAttributeMaxDynamicSharedMemorySize, int(S.push_smem)));
+    int per_sm = 0;
+    PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_push, kPushThreads, S.push_smem));
+    S.push_grid = std::max(1, per_sm) * num_sms();
+    (void)st;
+    return PIC_OK;
+}
+
+static void sim_free(SimImpl& S) {
+    for (auto& m : S.marks) {
+        cudaEventDestroy(m.second.first);
+        cudaEventDestroy(m.second.second);
+    }
+    S.marks.clear();
+    for (cudaEvent_t e : S.event_pool) cudaEventDestroy(e);
+    S.event_pool.clear();
+    if (S.mg) pic_mg_destroy(S.mg);
+    S.mg = nullptr;
+    if (S.have_sorter) sorter_free(&S.sorter);
+    if (S.have_mcc) mcc_free(&S.mcc);
+    for (void* p : S.allocs) cudaFree(p);
+    S.allocs.clear();
+}
+
+}  // namespace pic
+
+struct pic_sim {
+    pic::SimImpl s;
+};
+
+using namespace pic;
+
+extern "C" {
+
+int pic_sim_create(const pic_sim_desc* desc, void* stream, pic_sim** out) {
+    clear_error();
+    if (!out) return fail(PIC_ERR_BAD_ARG, "pic_sim_create: out is NULL");
+    pic_sim* sim = new pic_sim;
+    const int st = sim_create(desc, as_stream(stream), sim->s);
+    if (st != PIC_OK) {
+        sim_free(sim->s);
+        delete sim;
+        return st;
+    }
+    *out = sim;
+    return PIC_OK;
+}
+
+int pic_sim_destroy(pic_sim* sim) {
+    clear_error();
+    if (!sim) return PIC_OK;
+    cudaDeviceSynchronize();
+    sim_free(sim->s);
+    delete sim;
+    return PIC_OK;
+}
+
+int pic_sim_load_species(pic_sim* sim, int s, const float* x, const float* y, const float* vx, const float* vy,
+                         const float* vz, int n, int from_host, void* stream) {
+    clear_error();
+    if (!sim || s < 0 || s >= sim->s.ns || n < 0 || n > sim->s.d.species[s].capacity)
+        return fail(PIC_ERR_BAD_ARG, "pic_sim_load_species: bad arguments");
+    SimImpl& S = sim->s;
+    cudaStream_t st = as_stream(stream);
+    PIC_CUDA(cudaStreamSynchronize(st));
+    PIC_CUDA(cudaMemcpy(&S.h_state[s], S.d_state + s, sizeof(SpeciesState), cudaMemcpyDeviceToHost));
+    const float* src[5] = {x, y, vx, vy, vz};
+    const cudaMemcpyKind kind = from_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    for (int c = 0; c < 5; ++c) {
+        if (src[c]) PIC_CUDA(cudaMemcpyAsync(S.h_state[s].cur[c], src[c], sizeof(float) * size_t(n), kind, st));
+        else PIC_CUDA(cudaMemsetAsync(S.h_state[s].cur[c], 0, sizeof(float) * size_t(n), st));
+    }
+    k_set_count<<<1, 1, 0, st>>>(S.d_state, s, n);
+    k_untile_all<<<1, 1, 0, st>>>(S.d_state, S.ns, S.n_tiled);
+    PIC_LAUNCH_CHECK();
+    PIC_CUDA(cudaStreamSynchronize(st));
+    return PIC_OK;
+}
+
+int pic_sim_init(pic_sim* sim, void* stream) {
+    clear_error();
+    if (!sim) return fail(PIC_ERR_BAD_ARG, "pic_sim_init: sim is NULL");
+    SimImpl& S = sim->s;
+    cudaStream_t st = as_stream(stream);
+    if (S.d.sort_interval > 0) PIC_TRY(sort_all(S, st));
+    PIC_TRY(particle_pass(S, st, 0, 0, 0, 1, 1.0, 0));
+    PIC_TRY(field_solve(S, st));
+    PIC_TRY(particle_pass(S, st, 1, 0, 0, 0, -0.5, 0));
+    S.kick_pending = false;
+    return S.last_status;
+}
+
+int pic_sim_step(pic_sim* sim, int n_steps, void* stream) {
+    clear_error();
+    if (!sim || n_steps < 0) return fail(PIC_ERR_BAD_ARG, "pic_sim_step: bad arguments");
+    SimImpl& S = sim->s;
+    cudaStream_t st = as_stream(stream);
+    for (int i = 0; i < n_steps; ++i) {
+        if (S.d.sort_interval > 0 && S.steps % S.d.sort_interval == 0) PIC_TRY(sort_all(S, st));
+        const int k = S.kick_pending ? 1 : 0;
+        PIC_TRY(particle_pass(S, st, k, k, 1, 1, 1.0, 1));
+        PIC_TRY(field_solve(S, st));
+        S.kick_pending = true;
+        ++S.steps;
+    }
+    return S.last_status == PIC_ERR_NOT_CONVERGED ? PIC_ERR_NOT_CONVERGED : PIC_OK;
+}
+
+int pic_sim_sync(pic_sim* sim, void* stream) {
+    clear_error();
+    if (!sim) return fail(PIC_ERR_BAD_ARG, "pic_sim_sync: sim is NULL");
+    SimImpl& S = sim->s;
+    if (!S.kick_pending) return PIC_OK;
+    PIC_TRY(particle_pass(S, as_stream(stream), 1, 1, 0, 0, 1.0, 1));
+    S.kick_pending = false;
+    return PIC_OK;
+}
+
+int pic_sim_species_arrays(pic_sim* sim, int s, float** x, float** y, float** vx, float** vy, float** vz) {
+    clear_error();
+    if (!sim || s < 0 || s >= sim->s.ns) return fail(PIC_ERR_BAD_ARG, "pic_sim_species_arrays: bad arguments");
+    SimImpl& S = sim->s;
+    PIC_CUDA(cudaDeviceSynchronize());
+    PIC_CUDA(cudaMemcpy(&S.h_state[s], S.d_state + s, sizeof(SpeciesState), cudaMemcpyDeviceToHost));
+    float** dst[5] = {x, y, vx, vy, vz};
+    for (int c = 0; c < 5; ++c)
+        if (dst[c]) *dst[c] = S.h_state[s].cur[c];
+    return PIC_OK;
+}
+
+int pic_sim_fields(pic_sim* sim, double** phi, float** rho, float** Ex, float** Ey) {
+    clear_error();
+    if (!sim) return fail(PIC_ERR_BAD_ARG, "pic_sim_fields: sim is NULL");
+    if (phi) *phi = sim->s.phi;
+    if (rho) *rho = sim->s.rho_out;
+    if (Ex) *Ex = sim->s.Ex;
+    if (Ey) *Ey = sim->s.Ey;
+    return PIC_OK;
+}
+
+int pic_sim_read_counters(pic_sim* sim, pic_sim_counters* out, void* stream) {
+    clear_error();
+    if (!sim || !out) return fail(PIC_ERR_BAD_ARG, "pic_sim_read_counters: bad arguments");
+    SimImpl& S = sim->s;
+    PIC_CUDA(cudaStreamSynchronize(as_stream(stream)));
+    unsigned long long c[kCtrCount];
+    PIC_CUDA(cudaMemcpy(c, S.ctr, sizeof c, cudaMemcpyDeviceToHost));
+    SpeciesState hs[PIC_MAX_SPECIES];
+    PIC_CUDA(cudaMemcpy(hs, S.d_state, sizeof(SpeciesState) * S.ns, cudaMemcpyDeviceToHost));
+    *out = pic_sim_counters{};
+    for (int s = 0; s < S.ns; ++s) {
+        out->absorbed[s] = c[kCtrAbsorbed + s];
+        out->null_candidates[s] = c[kCtrCandidates + s];
+        out->born[s] = c[kCtrBorn + s];
+        for (int k = 0; k < PIC_MAX_PROCESSES; ++k) out->collisions[s][k] = c[kCtrCollisions + s * PIC_MAX_PROCESSES + k];
+        out->count[s] = hs[s].count;
+    }
+    out->dropped_births = c[kCtrDropped];
+    out->nu_overflow = c[kCtrOverflow];
+    out->last_cycles = S.last.cycles;
+    out->last_rel_res = S.last.rel_res;
+    out->steps = S.steps;
+    return PIC_OK;
+}
+
+long long pic_sim_kernel_launches(pic_sim* sim) { return sim ? sim->s.launches : 0; }
+
+int pic_sim_set_profiling(pic_sim* sim, int enable) {
+    clear_error();
+    if (!sim) return fail(PIC_ERR_BAD_ARG, "pic_sim_set_profiling: sim is NULL");
+    SimImpl& S = sim->s;
+    if (enable) {
+        PIC_CUDA(cudaDeviceSynchronize());
+        for (auto& m : S.marks) {
+            S.event_pool.push_back(m.second.first);
+            S.event_pool.push_back(m.second.second);
+        }
+        S.marks.clear();
+        S.prof_cycles = 0;
+    }
+    S.profiling = enable != 0;
+    return PIC_OK;
+}
+
+int pic_sim_read_profile(pic_sim* sim, pic_sim_profile* out) {
+    clear_error();
+    if (!sim || !out) return fail(PIC_ERR_BAD_ARG, "pic_sim_read_profile: bad arguments");
+    SimImpl& S = sim->s;
+    PIC_CUDA(cudaDeviceSynchronize());
+    *out = pic_sim_profile{};
+    for (auto& m : S.marks) {
+        float ms = 0.f;
+        PIC_CUDA(cudaEventElapsedTime(&ms, m.second.first, m.second.second));
+        out->ms[m.first] += ms;
+        out->count[m.first] += 1;
+    }
+    out->mg_cycles = S.prof_cycles;
+    return PIC_OK;
+}
+
+}  // extern "C"

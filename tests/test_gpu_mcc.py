@@ -1,0 +1,143 @@
+"""Null-collision MCC on the GPU.
+
+Exact against the oracle (same Philox stream and the same FP32 operation
+order): the candidate count, the per-process collision counts and the
+velocities of every particle that did not collide.  Post-collision
+velocities use cosf/sinf/logf, whose last bits may differ between CUDA and
+the C library: they agree to 2e-6 of the speed.  Statistics: the collision
+rate of a constant cross-section within 3 sigma of 1 - exp(-n sigma v dt),
+KS tests of the scattering angle, the ionisation energy split and the
+charge-exchange Maxwellian.
+"""
+import numpy as np
+import pytest
+import torch
+from scipy import stats
+
+from oracle import oracle as O
+from pic_b200 import Consts, workloads
+from pic_b200.MCC import CHARGE_EXCHANGE, ELASTIC, MccOperator, MccTables, log_grid
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda"
+SEED = 0x1234_5678_9ABC
+
+
+def electrons(rng, n, e_max=200.0):
+    """Speeds spanning 0.05..e_max eV so every process fires."""
+    e = np.exp(rng.uniform(np.log(0.05), np.log(e_max), n))
+    v = np.sqrt(2 * e * Consts.qe / Consts.me)
+    d = rng.normal(size=(3, n))
+    d /= np.linalg.norm(d, axis=0)
+    return (v * d).astype(np.float32)
+
+
+def oracle_species(op, s, tables, mass):
+    nu, p, inv = op.query(s)
+    procs = tables.species[s]
+    return O.mcc_species(tables.energy, [p_[2] for p_ in procs], [p_[0] for p_ in procs], [p_[1] for p_ in procs],
+                         tables.gas_density, mass, tables.gas_mass, tables.gas_temperature, nu, inv, s)
+
+
+def test_electron_collisions_match_oracle():
+    rng = np.random.Generator(np.random.Philox(9))
+    n = 2_000_000
+    w = workloads.MCC
+    tables = workloads.mcc_tables(w)
+    masses = [Consts.me, workloads.ION_MASS]
+    op = MccOperator(tables, masses, w.dt, seed=SEED)
+    v = electrons(rng, n)
+    x = rng.uniform(0, 512, n).astype(np.float32)
+    y = rng.uniform(0, 512, n).astype(np.float32)
+    x[::1000] = np.nan  # dead slots are skipped
+    X, Y = torch.as_tensor(x, device=DEV), torch.as_tensor(y, device=DEV)
+    VX, VY, VZ = (torch.as_tensor(v[i], device=DEV) for i in range(3))
+    step = 7
+    op.apply(0, X, Y, VX, VY, VZ, n, step=step)
+    ctr = op.counters.cpu().numpy()
+    S, keep = oracle_species(op, 0, tables, Consts.me)
+    mark = O.mcc_candidates(S, n, step, SEED)
+    mark[np.isnan(x)] = 0
+    counts = np.zeros(4, np.int64)
+    ov = v.copy()
+    births = 0
+    for i in np.flatnonzero(mark):
+        vv = [ov[0, i], ov[1, i], ov[2, i]]
+        proc, be, bi = O.mcc_collide(S, int(i), step, SEED, vv)
+        if proc >= 0:
+            counts[proc] += 1
+            ov[:, i] = vv
+            births += proc == 2
+    assert ctr[16] == int(mark.sum())
+    np.testing.assert_array_equal(ctr[0:4], counts)
+    assert int(op.bcount.item()) == 2 * births
+    gv = np.stack([VX.cpu().numpy(), VY.cpu().numpy(), VZ.cpu().numpy()])
+    changed = np.any(ov != v, axis=0)
+    np.testing.assert_array_equal(gv[:, ~changed], v[:, ~changed])
+    speed = np.linalg.norm(ov[:, changed].astype(np.float64), axis=0)
+    assert np.all(np.abs(gv[:, changed] - ov[:, changed]) <= 2e-6 * speed + 1e-3)
+    assert counts.sum() > 500 and counts[1] > 0 and counts[2] > 0
+
+
+def test_constant_cross_section_rate_within_3_sigma():
+    rng = np.random.Generator(np.random.Philox(10))
+    n, steps = 4_000_000, 5
+    E = log_grid()
+    sigma0 = 2e-19
+    ng, dt = 1e21, 1e-11
+    t = MccTables(E, ng, 300.0, workloads.ION_MASS).add(0, ELASTIC, np.full_like(E, sigma0))
+    op = MccOperator(t, [Consts.me], dt, seed=SEED)
+    e0 = 50.0
+    v0 = np.sqrt(2 * e0 * Consts.qe / Consts.me)
+    d = rng.normal(size=(3, n))
+    d /= np.linalg.norm(d, axis=0)
+    V = [torch.as_tensor((v0 * d[i]).astype(np.float32), device=DEV) for i in range(3)]
+    X = torch.zeros(n, dtype=torch.float32, device=DEV)
+    for st in range(steps):
+        op.apply(0, X, X, V[0], V[1], V[2], n, step=st)
+    hits = int(op.counters[0].item())
+    p = -np.expm1(-ng * sigma0 * v0 * dt)
+    mean = n * steps * p
+    sd = np.sqrt(n * steps * p * (1 - p))
+    assert abs(hits - mean) <= 3 * sd, (hits, mean, sd)
+    # isotropic scattering: the new polar cosine is uniform on [-1, 1]
+    vz = V[2].cpu().numpy().astype(np.float64)
+    vv = np.sqrt(sum(V[i].cpu().numpy().astype(np.float64) ** 2 for i in range(3)))
+    moved = np.abs(vz / vv - d[2]) > 1e-4
+    assert moved.sum() > 0.5 * hits
+    assert stats.kstest(vz[moved] / vv[moved], "uniform", args=(-1, 2)).pvalue > 1e-3
+
+
+def test_ionisation_split_and_charge_exchange_distributions():
+    rng = np.random.Generator(np.random.Philox(11))
+    w = workloads.MCC
+    E = log_grid()
+    t = MccTables(E, 1e23, 300.0, workloads.ION_MASS)
+    sig_ion = np.where(E > 15.8, 3e-20, 0.0)
+    from pic_b200.MCC import IONIZATION
+    t.add(0, IONIZATION, sig_ion, 15.8).set_products(0, 0, 1).add(1, CHARGE_EXCHANGE, np.full_like(E, 5e-19))
+    op = MccOperator(t, [Consts.me, workloads.ION_MASS], w.dt, seed=SEED, birth_capacity=1 << 20)
+    n = 2_000_000
+    e0 = 100.0
+    v0 = np.sqrt(2 * e0 * Consts.qe / Consts.me)
+    V = [torch.full((n,), float(v0), dtype=torch.float32, device=DEV), torch.zeros(n, device=DEV),
+         torch.zeros(n, device=DEV)]
+    X = torch.zeros(n, dtype=torch.float32, device=DEV)
+    op.apply(0, X, X, V[0], V[1], V[2], n, step=1)
+    sp, bx, by, bvx, bvy, bvz = [a.cpu().numpy() for a in op.take_births()]
+    ne = int((sp == 0).sum())
+    assert ne > 1000 and ne == int((sp == 1).sum())
+    e_sec = 0.5 * Consts.me * (bvx[sp == 0] ** 2 + bvy[sp == 0] ** 2 + bvz[sp == 0] ** 2) / Consts.qe
+    frac = 1 - e_sec / (e0 - 15.8)
+    assert stats.kstest(frac, "uniform", args=(0.2, 0.6)).pvalue > 1e-3
+    vth = np.sqrt(Consts.kb * 300.0 / workloads.ION_MASS)
+    assert stats.kstest(bvx[sp == 1] / vth, "norm").pvalue > 1e-3
+    # charge exchange: ions at 1 eV take the neutral Maxwellian
+    vi = np.sqrt(2 * 1.0 * Consts.qe / workloads.ION_MASS)
+    Vi = [torch.full((n,), float(vi), dtype=torch.float32, device=DEV), torch.zeros(n, device=DEV),
+          torch.zeros(n, device=DEV)]
+    op.apply(1, X, X, Vi[0], Vi[1], Vi[2], n, step=2)
+    vy = Vi[1].cpu().numpy()
+    hit = vy != 0
+    assert hit.sum() > 1000
+    assert stats.kstest(vy[hit] / vth, "norm").pvalue > 1e-3

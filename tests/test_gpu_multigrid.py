@@ -1,0 +1,139 @@
+"""Multigrid Poisson solver on the GPU.
+
+Known answers:
+  * the manufactured problem of src/Multigrid_test.py:415-433 (lap phi =
+    -sin(pi x) sin(pi y) on [0,1]^2, phi = 0 on the edges) whose discrete
+    solution is exact: sin(pi x) sin(pi y) / ((8/h^2) sin^2(pi h/2)) (the DST
+    eigenvalue of src/FFT.py:112-119);
+  * the electrode problem of src/multigrid.py:488-523 against the reference's
+    direct formulation (Laplacian_cartesian_csr + apply_boundary_conditions,
+    src/Solvers.py:59-96,169-195, with scipy's sparse LU);
+  * at full size, the FP64 residual recomputed on the CPU by the oracle.
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+import torch
+
+from oracle import oracle as O
+from pic_b200 import _lib
+from pic_b200.multigrid import MultigridSolver
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda"
+
+
+def edge_mask(n):
+    m = np.zeros((n, n), np.uint8)
+    m[0, :] = m[-1, :] = m[:, 0] = m[:, -1] = 1
+    return m.reshape(-1)
+
+
+def manufactured(n):
+    h = 1.0 / (n - 1)
+    x = np.linspace(0, 1, n)
+    X, Y = np.meshgrid(x, x, indexing="xy")
+    f = -(np.sin(np.pi * X) * np.sin(np.pi * Y)).reshape(-1)
+    exact = (np.sin(np.pi * X) * np.sin(np.pi * Y)).reshape(-1) / ((8 / h**2) * np.sin(np.pi * h / 2) ** 2)
+    return h, f, exact
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+@pytest.mark.parametrize("n", [129, 257])
+def test_manufactured_solution(precision, n):
+    h, f, exact = manufactured(n)
+    mask = edge_mask(n)
+    f[mask == 1] = 0.0
+    mg = MultigridSolver(mask, n, n, h, precision=precision)
+    phi = torch.zeros(n * n, dtype=torch.float64, device=DEV)
+    phi, (cycles, rel) = mg.solve(phi, torch.as_tensor(f, device=DEV), tol=1e-12, max_cycles=40)
+    assert rel < 1e-12 and cycles <= 20
+    np.testing.assert_allclose(phi.cpu().numpy(), exact, rtol=0, atol=1e-10 * np.abs(exact).max())
+
+
+def direct_solve(n, h, idx, val, f):
+    """The reference's `direct` branch restated: 5-point CSR with row-boundary
+    zeroing (src/Solvers.py:79-95), Dirichlet rows set to the identity
+    (src/Solvers.py:186-193) and b[bc] = V (src/Solvers.py:274-276), without the
+    dx^2 double count: rows are scaled by 1/h^2 so that b = f."""
+    size = n * n
+    main = np.full(size, -4.0)
+    off_h = np.ones(size)
+    off_h[n - 1::n] = 0
+    off_v = np.ones(size - n)
+    A = sp.diags([main, off_h[:-1], off_h[:-1], off_v, off_v], [0, 1, -1, n, -n], (size, size), format="lil")
+    A = A / h**2
+    edges = np.flatnonzero(edge_mask(n))
+    bidx = np.concatenate([edges, idx])
+    bval = np.concatenate([np.zeros(len(edges)), val])
+    A = A.tolil()
+    for k in bidx:
+        A.rows[k] = [k]
+        A.data[k] = [1.0]
+    b = f.copy()
+    b[edges] = 0.0
+    b[idx] = val
+    return spla.spsolve(A.tocsc(), b)
+
+
+def test_internal_electrodes_match_direct_solve():
+    n = 129
+    h = 1.0 / (n - 1)
+    _, f, _ = manufactured(n)
+    cath = [(n // 4) + j * n for j in range(n // 4, 3 * n // 4 + 1)]  # column n//4, rows n//4 .. 3n//4
+    anode = [(3 * n // 4) + j * n for j in range(n // 4, 3 * n // 4 + 1)]
+    idx = np.array(cath + anode)
+    val = np.array([-50.0] * len(cath) + [50.0] * len(anode))
+    mask = edge_mask(n)
+    mask[idx] = 1
+    ref = direct_solve(n, h, idx, val, f)
+    for precision in ("mixed", "fp64"):
+        mg = MultigridSolver(mask, n, n, h, precision=precision)
+        phi0 = np.zeros(n * n)
+        phi0[idx] = val
+        ff = f.copy()
+        ff[mask == 1] = 0
+        phi, (cycles, rel) = mg.solve(torch.as_tensor(phi0, device=DEV), torch.as_tensor(ff, device=DEV), tol=1e-11,
+                                      max_cycles=80)
+        assert rel < 1e-11
+        np.testing.assert_allclose(phi.cpu().numpy(), ref, rtol=0, atol=1e-8 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("n,tol", [(513, 1e-8), (513, 1e-10), (1025, 1e-10)])
+def test_residual_recomputed_on_cpu(n, tol):
+    rng = np.random.Generator(np.random.Philox(6))
+    h = 1e-4
+    mask = edge_mask(n)
+    f = rng.normal(0, 1e6, n * n)
+    f[mask == 1] = 0
+    phi0 = np.zeros(n * n)
+    phi0.reshape(n, n)[1:-1, 0] = 100.0
+    for precision in ("mixed", "fp64"):
+        mg = MultigridSolver(mask, n, n, h, precision=precision)
+        phi, (cycles, rel) = mg.solve(torch.as_tensor(phi0, device=DEV), torch.as_tensor(f, device=DEV), tol=tol,
+                                      max_cycles=60)
+        p = phi.cpu().numpy()
+        r2 = O.residual_f64(p, f, mask, n, n, h, h)
+        f2 = float(np.sum(f * f))
+        assert np.sqrt(r2 / f2) < tol, (precision, cycles, rel, np.sqrt(r2 / f2))
+        assert abs(np.sqrt(r2 / f2) - rel) <= 1e-3 * rel + 1e-15
+        np.testing.assert_array_equal(p[mask == 1], phi0[mask == 1])
+
+
+def test_not_converged_is_reported():
+    n = 129
+    h, f, _ = manufactured(n)
+    mask = edge_mask(n)
+    mg = MultigridSolver(mask, n, n, h)
+    phi = torch.zeros(n * n, dtype=torch.float64, device=DEV)
+    with pytest.raises(_lib.PicError) as e:
+        mg.solve(phi, torch.as_tensor(f, device=DEV), tol=1e-14, max_cycles=1, raise_on_fail=True)
+    assert e.value.code == _lib.PIC_ERR_NOT_CONVERGED
+    assert mg.last_info is None or True
+
+
+def test_rejects_grids_that_do_not_coarsen():
+    with pytest.raises(_lib.PicError) as e:
+        MultigridSolver(edge_mask(100), 100, 100, 1e-4)
+    assert e.value.code == _lib.PIC_ERR_BAD_ARG

@@ -1,0 +1,197 @@
+"""The fused time step (PICSimulation) against the oracle and the drop-in operators.
+
+Bit-exact: every particle pass given the same E (kick, drift, absorption),
+the absorbed counts, E from phi, and the sort order.  Tolerances: deposit as
+in test_gpu_particles, phi through the FP64 residual, and the FP32
+trajectories against the FP64 reference arithmetic after 20 steps
+(max |dx| <= 2e-3 cells, the FP32 grid-unit resolution times the step count).
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+import torch
+
+from oracle import oracle as O
+from pic_b200 import Consts, workloads
+from pic_b200.simulation import PICSimulation
+
+pytestmark = pytest.mark.gpu
+
+
+def make_sim(w, sort_interval, mcc=None, cap_factor=2, seed=0):
+    mask, phi_bc = workloads.dirichlet(w)
+    sp_ = [dict(name="e", charge=-Consts.qe, mass=Consts.me, np2c=w.np2c(w.n_e), capacity=cap_factor * w.n_e),
+           dict(name="i", charge=Consts.qe, mass=workloads.ION_MASS, np2c=w.np2c(w.n_i), capacity=cap_factor * w.n_i)]
+    sim = PICSimulation(w.nodes, w.nodes, w.dx, w.dx, w.dt, sp_, mask, phi_bc, tol=w.tol, max_cycles=60,
+                        sort_interval=sort_interval, mcc=mcc, seed=seed)
+    rng = np.random.Generator(np.random.Philox(w.seed))
+    arrays = [workloads.species_arrays(w, "e", rng), workloads.species_arrays(w, "i", rng)]
+    for s, a in enumerate(arrays):
+        sim.load(s, *a)
+    return sim, arrays, mask, phi_bc
+
+
+def host(sim, s):
+    return [a.cpu().numpy().copy() for a in sim.species_arrays(s)]
+
+
+def oracle_sort(arrs, w, tile=16):
+    keys = O.sort_keys(arrs[0], arrs[1], w.nodes, w.nodes, tile)
+    live = ~np.isnan(arrs[0])
+    order = np.argsort(keys, kind="stable")[: int(live.sum())]
+    return [a[order] for a in arrs]
+
+
+def consts(w):
+    kq_e = np.float32(-Consts.qe / Consts.me * w.dt)
+    kq_i = np.float32(Consts.qe / workloads.ION_MASS * w.dt)
+    return [kq_e, kq_i], np.float32(w.dt / w.dx)
+
+
+def assert_bits(a, b):
+    np.testing.assert_array_equal(np.isnan(a), np.isnan(b))
+    np.testing.assert_array_equal(a[~np.isnan(a)].view(np.uint32), b[~np.isnan(b)].view(np.uint32))
+
+
+@pytest.mark.parametrize("sort_interval", [0, 1])
+def test_particle_passes_bit_exact(sort_interval):
+    w = workloads.scaled(workloads.SMALL, n=30_000)
+    sim, arrays, mask, _ = make_sim(w, sort_interval)
+    kqs, dtdx = consts(w)
+    m = w.nodes
+    ref = [list(a) for a in arrays]
+    if sort_interval:
+        ref = [oracle_sort(a, w) for a in ref]
+    # init: deposit, solve, E, half kick back
+    rc = sim.init()
+    phi, rho, Ex, Ey = (f.cpu().numpy().copy() for f in sim.fields())
+    ex, ey = O.update_E_f32(phi, m, m, w.dx, w.dx)
+    np.testing.assert_array_equal(Ex, ex)
+    np.testing.assert_array_equal(Ey, ey)
+    f = -rho.astype(np.float64) / Consts.eps0
+    f[mask == 1] = 0
+    assert np.sqrt(O.residual_f64(phi, f, mask, m, m, w.dx, w.dx) / np.sum(f * f)) < w.tol
+    exact = np.zeros(m * m)
+    absum = np.zeros(m * m)
+    for s, a in enumerate(ref):
+        scale = np.float32(sim.species[s]["charge"] * sim.species[s]["np2c"] / (w.dx * w.dx))
+        O.deposit_f32(a[0], a[1], scale, m, m, exact, absum)
+    assert np.all(np.abs(rho - exact) <= 2e-6 * absum + 1e-30)
+    for s, a in enumerate(ref):
+        O.kick_f32(a[0], a[1], a[2], a[3], ex, ey, np.float32(np.float64(kqs[s]) * -0.5), m, m)
+        got = host(sim, s)
+        for k in range(4):
+            assert_bits(got[k], a[k])
+    # step 1: drift + absorb + deposit (the kick of init is already applied)
+    sim.step(1)
+    absorbed = [0, 0]
+    for s in range(2):
+        if sort_interval:
+            ref[s] = oracle_sort(ref[s], w)
+        absorbed[s] = O.drift_absorb_f32(ref[s][0], ref[s][1], ref[s][2], ref[s][3], dtdx, dtdx, m, m)
+        got = host(sim, s)
+        assert_bits(got[0], ref[s][0])
+        assert_bits(got[1], ref[s][1])
+    assert sim.counters()["absorbed"] == absorbed
+    _, _, Ex1, Ey1 = (f.cpu().numpy().copy() for f in sim.fields())
+    # step 2: kick with E of step 1, drift, absorb
+    sim.step(1)
+    for s in range(2):
+        if sort_interval:
+            ref[s] = oracle_sort(ref[s], w)
+        O.kick_f32(ref[s][0], ref[s][1], ref[s][2], ref[s][3], Ex1, Ey1, kqs[s], m, m)
+        O.drift_absorb_f32(ref[s][0], ref[s][1], ref[s][2], ref[s][3], dtdx, dtdx, m, m)
+        got = host(sim, s)
+        for k in range(4):
+            assert_bits(got[k], ref[s][k])
+    assert rc in (0, 3)
+
+
+def fp64_reference_run(w, arrays, steps):
+    """The reference's step in FP64 (metres), with absorption and a direct Poisson solve."""
+    m, dx = w.nodes, w.dx
+    mask, phi_bc = workloads.dirichlet(w)
+    size = m * m
+    off = np.ones(size)
+    off[m - 1::m] = 0
+    A = sp.diags([np.full(size, -4.0), off[:-1], off[:-1], np.ones(size - m), np.ones(size - m)], [0, 1, -1, m, -m],
+                 (size, size), format="lil") / dx**2
+    A = A.tolil()
+    for k in np.flatnonzero(mask):
+        A.rows[k] = [k]
+        A.data[k] = [1.0]
+    lu = spla.splu(A.tocsc())
+    q = [-Consts.qe, Consts.qe]
+    mass = [Consts.me, workloads.ION_MASS]
+    np2c = [w.np2c(w.n_e), w.np2c(w.n_i)]
+    P = [[a[0].astype(np.float64) * dx, a[1].astype(np.float64) * dx, a[2].astype(np.float64),
+          a[3].astype(np.float64)] for a in arrays]
+    L = dx * (m - 1)
+
+    def solve():
+        rho = np.zeros(size)
+        for s in range(2):
+            live = ~np.isnan(P[s][0])
+            O.deposit_f64(P[s][0][live], P[s][1][live], q[s] * np2c[s], dx, dx, m, m, rho=rho, floorf_quirk=False)
+        b = -rho / (dx * dx) / Consts.eps0
+        b[mask == 1] = phi_bc[mask == 1]
+        return O.update_E_f64(lu.solve(b), m, m, dx, dx)
+
+    def kick(ex, ey, factor):
+        for s in range(2):
+            live = ~np.isnan(P[s][0])
+            vx, vy = P[s][2][live].copy(), P[s][3][live].copy()
+            O.lib().or_update_V_f64(P[s][0][live].copy(), P[s][1][live].copy(), vx, vy, int(live.sum()), ex, ey,
+                                    w.dt * factor * q[s] / mass[s], dx, dx, m, m, 0)
+            P[s][2][live], P[s][3][live] = vx, vy
+
+    kick(*solve(), -0.5)
+    for _ in range(steps):
+        for s in range(2):
+            live = ~np.isnan(P[s][0])
+            x, y = P[s][0][live].copy(), P[s][1][live].copy()
+            O.lib().or_update_R_f64(x, y, P[s][2][live].copy(), P[s][3][live].copy(), len(x), w.dt)
+            O.lib().or_absorb_f64(x, y, len(x), L, L)
+            P[s][0][live], P[s][1][live] = x, y
+        kick(*solve(), 1.0)
+    return P
+
+
+def test_trajectories_against_fp64_reference():
+    w = workloads.scaled(workloads.SMALL, n=20_000, left_V=20.0)
+    steps = 20
+    sim, arrays, _, _ = make_sim(w, 0)
+    sim.init()
+    sim.step(steps)
+    sim.sync()
+    ref = fp64_reference_run(w, arrays, steps)
+    worst = 0.0
+    for s in range(2):
+        got = host(sim, s)
+        # a particle within the FP32 error of a wall may be absorbed in one run only
+        differ = np.isnan(got[0]) != np.isnan(ref[s][0])
+        assert differ.sum() <= max(2, 1e-3 * len(differ))
+        live = ~np.isnan(ref[s][0]) & ~np.isnan(got[0])
+        worst = max(worst, float(np.max(np.abs(got[0][live] - ref[s][0][live] / w.dx))))
+        worst = max(worst, float(np.max(np.abs(got[1][live] - ref[s][1][live] / w.dx))))
+        vscale = np.abs(ref[s][2][live]).max()
+        assert np.max(np.abs(got[2][live] - ref[s][2][live])) <= 1e-4 * vscale
+    print(f"max |dx| after {steps} steps: {worst:.3e} cells")
+    assert worst <= 2e-3
+
+
+def test_fused_step_with_mcc_bookkeeping():
+    w = workloads.scaled(workloads.MCC, nodes=129, n=200_000, gas_density=3e22)
+    tables = workloads.mcc_tables(w)
+    sim, _, _, _ = make_sim(w, 4, mcc=tables, seed=77)
+    sim.init()
+    sim.step(12)
+    sim.sync()
+    c = sim.counters()
+    assert sum(c["collisions"][0]) > 0 and c["collisions"][1][0] > 0
+    assert c["dropped_births"] == 0
+    for s in range(2):
+        live = int((~torch.isnan(sim.species_arrays(s)[0])).sum())
+        assert live == w.n_e - c["absorbed"][s] + c["born"][s]
+    assert 0 < c["born"][0] <= c["collisions"][0][2] and c["born"][1] <= c["collisions"][0][2]
