@@ -1,16 +1,31 @@
 // Geometric multigrid Poisson solver (replaces src/multigrid.py:277-455).
 //
 // Outer loop: FP64 iterative refinement on the fine grid
-//     r = f - A phi   (FP64, 5-point operator, free nodes only)
+//     r = f - A phi   (FP64, 5-point operator on free nodes)
 //     solve A e = r approximately with one V-cycle from e = 0
 //     phi += e        (FP64)
-// until ||r|| / ||f|| < tol.  The V-cycle runs in FP32 (PIC_MG_MIXED) or FP64
-// (PIC_MG_FP64); it is a correction scheme with red-black Gauss-Seidel
-// smoothing, full-weighting restriction, bilinear prolongation and a dense
-// FP64 direct solve on the coarsest level.  Dirichlet nodes (mask = 1, and
-// the grid edges) carry a zero correction on every level; a coarse node is
-// Dirichlet when its injected fine node is.
+// until ||r|| / ||f|| < tol or max_cycles.  The V-cycle runs in FP32
+// (PIC_MG_MIXED) or FP64 (PIC_MG_FP64): red-black Gauss-Seidel smoothing,
+// full-weighting restriction, bilinear prolongation, a dense FP64 solve on
+// the coarsest level.  Dirichlet nodes (mask = 1, and the grid edges) carry a
+// zero correction; a coarse node is Dirichlet when its injected fine node is.
+//
+// Kernels per V-cycle (8 launches for a 513^2 grid):
+//   down(l)   l < Lc: 2*pre red/black half-sweeps on a 32x32 tile held in
+//             shared memory with a halo of 2*pre+2 nodes (the valid region
+//             shrinks by one node per half-sweep), then the residual and its
+//             full-weighting restriction to level l+1
+//   coarse    one CTA: the whole V-cycle of the levels that fit in shared
+//             memory (<= 65^2 nodes), down to the direct solve and back up
+//   up(l)     prolongation-add of level l+1 and 2*post half-sweeps on a tile
+//             with a halo of 2*post; on level 0 it adds e to phi instead of
+//             storing e
+//   r0        the FP64 residual, a deterministic norm (last-block reduction)
+//             and the loop decision
+// The loop is a CUDA-graph conditional WHILE node whose condition r0 sets,
+// so a solve issues no host synchronisation.
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "common.cuh"
@@ -19,218 +34,390 @@ namespace pic {
 
 int grid_blocks(long n, int threads);
 
+constexpr int kMgTile = 32;
+constexpr int kMgThreads = 256;
+constexpr int kMgMaxCoarseLevels = 8;
+constexpr int kCoarseThreads = 1024;
+constexpr long kCoarseMaxNodes = 65L * 65L;  // levels at or below this size run in the single-CTA kernel
+
 template <class T>
-struct MgLevel {
+struct LevelDev {
     int nx, ny;
-    T cx, cy;        // 1/dx^2, 1/dy^2 at this level
-    uint8_t* mask;   // 1 = Dirichlet
-    T* e;            // correction
-    T* g;            // right-hand side of the correction equation
+    T cx, cy, inv_diag;
+    const uint8_t* mask;  // 1 = Dirichlet
+    T* e;
+    T* g;
 };
 
-// ---- kernels ---------------------------------------------------------------------
-
 template <class T>
-__global__ void k_smooth(T* __restrict__ e, const T* __restrict__ g, const uint8_t* __restrict__ mask, int nx, int ny,
-                         T cx, T cy, T omega, int color, const int* __restrict__ skip) {
-    if (skip && *skip) return;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((color + j) & 1);
-    if (j >= ny - 1 || i < 1 || i >= nx - 1) return;
-    const long k = long(j) * nx + i;
-    if (mask[k]) return;
-    const T inv_diag = T(1) / (T(2) * (cx + cy));
-    const T s = cx * (e[k - 1] + e[k + 1]) + cy * (e[k - nx] + e[k + nx]);
-    const T upd = (s - g[k]) * inv_diag;
-    const T old = e[k];
-    e[k] = old + omega * (upd - old);
-}
+struct CoarseDesc {
+    int nlev;
+    LevelDev<T> lv[kMgMaxCoarseLevels];
+    int off_e[kMgMaxCoarseLevels], off_g[kMgMaxCoarseLevels], off_m[kMgMaxCoarseLevels];  // bytes into smem
+    const double* ainv;
+    const int* cidx;
+    int nf;
+    T omega;
+    int pre, post;
+    double* phi0;  // set when the coarse kernel owns level 0: phi += e
+};
 
-template <class T>
-__device__ __forceinline__ T fine_residual(const T* __restrict__ e, const T* __restrict__ g,
-                                           const uint8_t* __restrict__ mask, long k, int nx, T cx, T cy) {
-    if (mask[k]) return T(0);
-    const T c = e[k];
-    const T lap = cx * (e[k - 1] + e[k + 1] - T(2) * c) + cy * (e[k - nx] + e[k + nx] - T(2) * c);
-    return g[k] - lap;
-}
+// ---- shared-memory tile smoothing -------------------------------------------------
 
+// One red or black half-sweep over the nodes 1..W-2 of a W x W shared tile;
+// `par` selects the nodes whose local (li + lj) parity equals it.
 template <class T>
-__global__ void k_resid_restrict(const T* __restrict__ e, const T* __restrict__ g, const uint8_t* __restrict__ mask,
-                                 int nxf, T cx, T cy, T* __restrict__ gc, T* __restrict__ ec,
-                                 const uint8_t* __restrict__ maskc, int nxc, int nyc, const int* __restrict__ skip) {
-    if (skip && *skip) return;
-    const int I = blockIdx.x * blockDim.x + threadIdx.x;
-    const int J = blockIdx.y * blockDim.y + threadIdx.y;
-    if (I >= nxc || J >= nyc) return;
-    const long K = long(J) * nxc + I;
-    ec[K] = T(0);
-    if (I == 0 || J == 0 || I == nxc - 1 || J == nyc - 1 || maskc[K]) {
-        gc[K] = T(0);
-        return;
+__device__ __forceinline__ void tile_half_sweep(T* __restrict__ se, const T* __restrict__ sg,
+                                                const uint8_t* __restrict__ sm, int W, int par, T cx, T cy, T inv_diag,
+                                                T omega, int nthreads, int tid) {
+    const int half = W / 2;
+    for (int q = tid; q < half * W; q += nthreads) {
+        const int lj = q / half;
+        const int li = 2 * (q - lj * half) + ((par + lj) & 1);
+        if (lj < 1 || lj > W - 2 || li < 1 || li > W - 2) continue;
+        const int p = lj * W + li;
+        if (sm[p]) continue;
+        const T s = cx * (se[p - 1] + se[p + 1]) + cy * (se[p - W] + se[p + W]);
+        const T upd = (s - sg[p]) * inv_diag;
+        const T old = se[p];
+        se[p] = old + omega * (upd - old);
     }
-    const long kc = long(2 * J) * nxf + 2 * I;
-    T s = T(0.25) * fine_residual(e, g, mask, kc, nxf, cx, cy);
-    s += T(0.125) * (fine_residual(e, g, mask, kc - 1, nxf, cx, cy) + fine_residual(e, g, mask, kc + 1, nxf, cx, cy) +
-                     fine_residual(e, g, mask, kc - nxf, nxf, cx, cy) + fine_residual(e, g, mask, kc + nxf, nxf, cx, cy));
-    s += T(0.0625) *
-         (fine_residual(e, g, mask, kc - nxf - 1, nxf, cx, cy) + fine_residual(e, g, mask, kc - nxf + 1, nxf, cx, cy) +
-          fine_residual(e, g, mask, kc + nxf - 1, nxf, cx, cy) + fine_residual(e, g, mask, kc + nxf + 1, nxf, cx, cy));
-    gc[K] = s;
+}
+
+// Loads level L over the W x W region at (ox, oy): mask (edges and outside
+// the grid count as Dirichlet), g, and e (zero or the stored correction).
+template <class T>
+__device__ __forceinline__ void tile_load(const LevelDev<T>& L, int ox, int oy, int W, T* se, T* sg, uint8_t* sm,
+                                          bool load_e, int nthreads, int tid) {
+    for (int q = tid; q < W * W; q += nthreads) {
+        const int li = q % W, lj = q / W;
+        const int i = ox + li, j = oy + lj;
+        const bool inside = i >= 0 && j >= 0 && i < L.nx && j < L.ny;
+        const long k = long(j) * L.nx + i;
+        const bool fr = inside && i > 0 && j > 0 && i < L.nx - 1 && j < L.ny - 1 && !L.mask[k];
+        sm[q] = fr ? 0 : 1;
+        sg[q] = inside ? L.g[k] : T(0);
+        se[q] = (fr && load_e) ? L.e[k] : T(0);
+    }
 }
 
 template <class T>
-__global__ void k_prolong_add(T* __restrict__ ef, const uint8_t* __restrict__ maskf, int nxf, int nyf,
-                              const T* __restrict__ ec, int nxc, const int* __restrict__ skip) {
-    if (skip && *skip) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i < 1 || j < 1 || i >= nxf - 1 || j >= nyf - 1) return;
-    const long k = long(j) * nxf + i;
-    if (maskf[k]) return;
-    const int I = i >> 1, J = j >> 1;
-    const long K = long(J) * nxc + I;
-    T v;
-    if (!(i & 1) && !(j & 1)) v = ec[K];
-    else if ((i & 1) && !(j & 1)) v = T(0.5) * (ec[K] + ec[K + 1]);
-    else if (!(i & 1) && (j & 1)) v = T(0.5) * (ec[K] + ec[K + nxc]);
-    else v = T(0.25) * (ec[K] + ec[K + 1] + ec[K + nxc] + ec[K + nxc + 1]);
-    ef[k] += v;
-}
-
-template <class T>
-__global__ void k_coarse_solve(T* __restrict__ e, const T* __restrict__ g, const double* __restrict__ ainv,
-                               const int* __restrict__ idx, int nf, const int* __restrict__ skip) {
-    if (skip && *skip) return;
-    extern __shared__ double gs[];
-    for (int b = threadIdx.x; b < nf; b += blockDim.x) gs[b] = double(g[idx[b]]);
+__global__ void __launch_bounds__(kMgThreads) k_mg_down(LevelDev<T> F, LevelDev<T> Cc, T omega, int pre) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int H = 2 * pre + 2, W = kMgTile + 2 * H;
+    T* se = reinterpret_cast<T*>(smem);
+    T* sg = se + W * W;
+    uint8_t* sm = reinterpret_cast<uint8_t*>(sg + W * W);
+    const int x0 = blockIdx.x * kMgTile, y0 = blockIdx.y * kMgTile;
+    const int ox = x0 - H, oy = y0 - H;
+    const int tid = threadIdx.x;
+    tile_load(F, ox, oy, W, se, sg, sm, false, kMgThreads, tid);
     __syncthreads();
-    for (int a = threadIdx.x; a < nf; a += blockDim.x) {
-        const double* row = ainv + long(a) * nf;
-        double s = 0.0;
-        for (int b = 0; b < nf; ++b) s += row[b] * gs[b];
-        e[idx[a]] = T(s);
+    // global red nodes have (i + j) even; locally (li + lj + ox + oy) even
+    const int par0 = (ox + oy) & 1;
+    for (int s = 0; s < pre; ++s)
+        for (int color = 0; color < 2; ++color) {
+            tile_half_sweep(se, sg, sm, W, color ^ par0, F.cx, F.cy, F.inv_diag, omega, kMgThreads, tid);
+            __syncthreads();
+        }
+    for (int q = tid; q < kMgTile * kMgTile; q += kMgThreads) {
+        const int i = x0 + q % kMgTile, j = y0 + q / kMgTile;
+        if (i < F.nx && j < F.ny) F.e[long(j) * F.nx + i] = se[(H + q / kMgTile) * W + H + q % kMgTile];
+    }
+    // residual in place of g (each node reads only its own g)
+    for (int q = tid; q < W * W; q += kMgThreads) {
+        const int li = q % W, lj = q / W;
+        if (li < 1 || lj < 1 || li > W - 2 || lj > W - 2 || sm[q]) continue;
+        const T c = se[q];
+        const T lap = F.cx * (se[q - 1] + se[q + 1] - T(2) * c) + F.cy * (se[q - W] + se[q + W] - T(2) * c);
+        sg[q] = sg[q] - lap;
+    }
+    __syncthreads();
+    // full weighting onto the coarse nodes injected from this tile
+    const int hx = kMgTile / 2;
+    for (int q = tid; q < hx * hx; q += kMgThreads) {
+        const int I = x0 / 2 + q % hx, J = y0 / 2 + q / hx;
+        if (I >= Cc.nx || J >= Cc.ny) continue;
+        const long K = long(J) * Cc.nx + I;
+        if (I == 0 || J == 0 || I == Cc.nx - 1 || J == Cc.ny - 1 || Cc.mask[K]) {
+            Cc.g[K] = T(0);
+            continue;
+        }
+        const int p = (2 * J - oy) * W + (2 * I - ox);
+        auto r = [&](int o) { return sm[p + o] ? T(0) : sg[p + o]; };
+        T v = T(0.25) * r(0);
+        v += T(0.125) * (r(-1) + r(1) + r(-W) + r(W));
+        v += T(0.0625) * (r(-W - 1) + r(-W + 1) + r(W - 1) + r(W + 1));
+        Cc.g[K] = v;
     }
 }
 
-// Fine-grid FP64 residual; writes the correction equation's right-hand side
-// g0 = r (in T), zeroes e0 and leaves one partial sum of r^2 per block.
 template <class T>
-__global__ void k_residual0(const double* __restrict__ phi, const double* __restrict__ f,
-                            const uint8_t* __restrict__ mask, int nx, int ny, double cx, double cy, T* __restrict__ g0,
-                            T* __restrict__ e0, double* __restrict__ partial, const int* __restrict__ skip) {
-    if (skip && *skip) return;
+__global__ void __launch_bounds__(kMgThreads) k_mg_up(LevelDev<T> F, LevelDev<T> Cc, T omega, int post,
+                                                      double* __restrict__ phi) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int H = 2 * post, W = kMgTile + 2 * H;
+    T* se = reinterpret_cast<T*>(smem);
+    T* sg = se + W * W;
+    uint8_t* sm = reinterpret_cast<uint8_t*>(sg + W * W);
+    const int x0 = blockIdx.x * kMgTile, y0 = blockIdx.y * kMgTile;
+    const int ox = x0 - H, oy = y0 - H;
+    const int tid = threadIdx.x;
+    tile_load(F, ox, oy, W, se, sg, sm, true, kMgThreads, tid);
+    __syncthreads();
+    // bilinear prolongation of the coarse correction, added on free nodes
+    for (int q = tid; q < W * W; q += kMgThreads) {
+        if (sm[q]) continue;
+        const int i = ox + q % W, j = oy + q / W;
+        const int I = i >> 1, J = j >> 1;
+        const long K = long(J) * Cc.nx + I;
+        const T* ec = Cc.e;
+        T v;
+        if (!(i & 1) && !(j & 1)) v = ec[K];
+        else if ((i & 1) && !(j & 1)) v = T(0.5) * (ec[K] + ec[K + 1]);
+        else if (!(i & 1) && (j & 1)) v = T(0.5) * (ec[K] + ec[K + Cc.nx]);
+        else v = T(0.25) * (ec[K] + ec[K + 1] + ec[K + Cc.nx] + ec[K + Cc.nx + 1]);
+        se[q] += v;
+    }
+    __syncthreads();
+    const int par0 = (ox + oy) & 1;
+    for (int s = 0; s < post; ++s)
+        for (int color = 0; color < 2; ++color) {
+            tile_half_sweep(se, sg, sm, W, color ^ par0, F.cx, F.cy, F.inv_diag, omega, kMgThreads, tid);
+            __syncthreads();
+        }
+    for (int q = tid; q < kMgTile * kMgTile; q += kMgThreads) {
+        const int i = x0 + q % kMgTile, j = y0 + q / kMgTile;
+        if (i >= F.nx || j >= F.ny) continue;
+        const long k = long(j) * F.nx + i;
+        const T v = se[(H + q / kMgTile) * W + H + q % kMgTile];
+        if (phi) phi[k] += double(v);
+        else F.e[k] = v;
+    }
+}
+
+// ---- single-CTA V-cycle of the coarse levels --------------------------------------
+
+template <class T>
+__device__ void level_sweeps(T* se, const T* sg, const uint8_t* sm, const LevelDev<T>& L, T omega, int sweeps) {
+    const int nx = L.nx, ny = L.ny;
+    const int hx = (nx + 1) / 2;
+    for (int s = 0; s < sweeps; ++s)
+        for (int color = 0; color < 2; ++color) {
+            for (int q = threadIdx.x; q < hx * ny; q += blockDim.x) {
+                const int j = q / hx;
+                const int i = 2 * (q - j * hx) + ((color + j) & 1);
+                if (i >= nx) continue;
+                const int p = j * nx + i;
+                if (sm[p]) continue;
+                const T sum = L.cx * (se[p - 1] + se[p + 1]) + L.cy * (se[p - nx] + se[p + nx]);
+                const T upd = (sum - sg[p]) * L.inv_diag;
+                const T old = se[p];
+                se[p] = old + omega * (upd - old);
+            }
+            __syncthreads();
+        }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kCoarseThreads) k_mg_coarse(CoarseDesc<T> D) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    T* E[kMgMaxCoarseLevels];
+    T* Gs[kMgMaxCoarseLevels];
+    uint8_t* M[kMgMaxCoarseLevels];
+    for (int l = 0; l < D.nlev; ++l) {
+        E[l] = reinterpret_cast<T*>(smem + D.off_e[l]);
+        Gs[l] = reinterpret_cast<T*>(smem + D.off_g[l]);
+        M[l] = smem + D.off_m[l];
+        const LevelDev<T>& L = D.lv[l];
+        for (int q = threadIdx.x; q < L.nx * L.ny; q += blockDim.x) {
+            const int i = q % L.nx, j = q / L.nx;
+            M[l][q] = (i == 0 || j == 0 || i == L.nx - 1 || j == L.ny - 1 || L.mask[q]) ? 1 : 0;
+            E[l][q] = T(0);
+            if (l == 0) Gs[0][q] = L.g[q];
+        }
+    }
+    __syncthreads();
+    const int last = D.nlev - 1;
+    for (int l = 0; l < last; ++l) {
+        const LevelDev<T>& L = D.lv[l];
+        const LevelDev<T>& C = D.lv[l + 1];
+        level_sweeps(E[l], Gs[l], M[l], L, D.omega, D.pre);
+        T* r = Gs[l];
+        const int nx = L.nx;
+        for (int q = threadIdx.x; q < L.nx * L.ny; q += blockDim.x) {
+            if (M[l][q]) continue;
+            const T c = E[l][q];
+            r[q] = r[q] - (L.cx * (E[l][q - 1] + E[l][q + 1] - T(2) * c) + L.cy * (E[l][q - nx] + E[l][q + nx] - T(2) * c));
+        }
+        __syncthreads();
+        for (int Q = threadIdx.x; Q < C.nx * C.ny; Q += blockDim.x) {
+            if (M[l + 1][Q]) {
+                Gs[l + 1][Q] = T(0);
+                continue;
+            }
+            const int I = Q % C.nx, J = Q / C.nx;
+            const int p = 2 * J * nx + 2 * I;
+            auto rr = [&](int o) { return M[l][p + o] ? T(0) : r[p + o]; };
+            T v = T(0.25) * rr(0);
+            v += T(0.125) * (rr(-1) + rr(1) + rr(-nx) + rr(nx));
+            v += T(0.0625) * (rr(-nx - 1) + rr(-nx + 1) + rr(nx - 1) + rr(nx + 1));
+            Gs[l + 1][Q] = v;
+        }
+        __syncthreads();
+    }
+    // dense direct solve on the coarsest level
+    for (int a = threadIdx.x; a < D.nf; a += blockDim.x) {
+        const double* row = D.ainv + long(a) * D.nf;
+        double s = 0.0;
+        for (int b = 0; b < D.nf; ++b) s += row[b] * double(Gs[last][D.cidx[b]]);
+        E[last][D.cidx[a]] = T(s);
+    }
+    __syncthreads();
+    for (int l = last - 1; l >= 0; --l) {
+        const LevelDev<T>& L = D.lv[l];
+        const LevelDev<T>& C = D.lv[l + 1];
+        for (int q = threadIdx.x; q < L.nx * L.ny; q += blockDim.x) {
+            if (M[l][q]) continue;
+            const int i = q % L.nx, j = q / L.nx;
+            const int K = (j >> 1) * C.nx + (i >> 1);
+            const T* ec = E[l + 1];
+            T v;
+            if (!(i & 1) && !(j & 1)) v = ec[K];
+            else if ((i & 1) && !(j & 1)) v = T(0.5) * (ec[K] + ec[K + 1]);
+            else if (!(i & 1) && (j & 1)) v = T(0.5) * (ec[K] + ec[K + C.nx]);
+            else v = T(0.25) * (ec[K] + ec[K + 1] + ec[K + C.nx] + ec[K + C.nx + 1]);
+            E[l][q] += v;
+        }
+        __syncthreads();
+        level_sweeps(E[l], Gs[l], M[l], L, D.omega, D.post);
+    }
+    const LevelDev<T>& L0 = D.lv[0];
+    for (int q = threadIdx.x; q < L0.nx * L0.ny; q += blockDim.x) {
+        if (D.phi0) D.phi0[q] += double(E[0][q]);
+        else L0.e[q] = E[0][q];
+    }
+}
+
+// ---- FP64 residual, norms and the loop decision -----------------------------------
+
+struct NormState {
+    double* partial;   // [nblocks] r^2, then [nblocks] f^2
+    unsigned* done;    // blocks finished
+    double* norms;     // [||f||^2, ||r||^2]
+    int* converged;
+    int* cycles;       // V-cycles of the current solve
+    long long* total;  // V-cycles since creation
+};
+
+template <class T>
+__global__ void __launch_bounds__(256) k_mg_r0(const double* __restrict__ phi, const double* __restrict__ f,
+                                               const uint8_t* __restrict__ mask, int nx, int ny, double cx, double cy,
+                                               T* __restrict__ g0, NormState N, double tol2, int max_cycles,
+                                               int initial, cudaGraphConditionalHandle cond, int use_cond) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    double r = 0.0;
+    double r = 0.0, fv = 0.0;
     if (i < nx && j < ny) {
         const long k = long(j) * nx + i;
         if (i > 0 && j > 0 && i < nx - 1 && j < ny - 1 && !mask[k]) {
             const double c = phi[k];
-            const double lap = cx * ((phi[k - 1] - c) + (phi[k + 1] - c)) + cy * ((phi[k - nx] - c) + (phi[k + nx] - c));
-            r = f[k] - lap;
+            const double lap =
+                cx * ((phi[k - 1] - c) + (phi[k + 1] - c)) + cy * ((phi[k - nx] - c) + (phi[k + nx] - c));
+            fv = f[k];
+            r = fv - lap;
         }
         g0[k] = T(r);
-        e0[k] = T(0);
     }
-    __shared__ double ws[32];
-    double s = warp_sum(r * r);
+    __shared__ double ws[2][8];
+    __shared__ bool last;
     const int t = threadIdx.y * blockDim.x + threadIdx.x;
-    if ((t & 31) == 0) ws[t >> 5] = s;
-    __syncthreads();
-    if (t < 32) {
-        const int nw = (blockDim.x * blockDim.y) >> 5;
-        s = t < nw ? ws[t] : 0.0;
-        s = warp_sum(s);
-        if (t == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = s;
+    double a = warp_sum(r * r), b = warp_sum(fv * fv);
+    if ((t & 31) == 0) {
+        ws[0][t >> 5] = a;
+        ws[1][t >> 5] = b;
     }
-}
-
-template <class T>
-__global__ void k_correct0(double* __restrict__ phi, const T* __restrict__ e0, long G, const int* __restrict__ skip) {
-    if (skip && *skip) return;
-    for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < G; k += long(gridDim.x) * blockDim.x)
-        phi[k] += double(e0[k]);
-}
-
-__global__ void k_sumsq_free(const double* __restrict__ v, const uint8_t* __restrict__ mask, int nx, int ny,
-                             double* __restrict__ partial) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    double x = 0.0;
-    if (i > 0 && j > 0 && i < nx - 1 && j < ny - 1) {
-        const long k = long(j) * nx + i;
-        if (!mask[k]) x = v[k];
-    }
-    __shared__ double ws[32];
-    double s = warp_sum(x * x);
-    const int t = threadIdx.y * blockDim.x + threadIdx.x;
-    if ((t & 31) == 0) ws[t >> 5] = s;
     __syncthreads();
-    if (t < 32) {
-        const int nw = (blockDim.x * blockDim.y) >> 5;
-        s = t < nw ? ws[t] : 0.0;
-        s = warp_sum(s);
-        if (t == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = s;
-    }
-}
-
-// Deterministic sum of the block partials.  mode 0: store ||f||^2 in norms[0];
-// mode 1: store ||r||^2 in norms[1], count the cycle and raise *flag once
-// ||r|| < tol ||f|| (||f|| = 0 falls back to the absolute residual).
-__global__ void k_finalize(const double* __restrict__ partial, int np, double* __restrict__ norms, int mode,
-                           double tol2, int* __restrict__ flag, int* __restrict__ cycles) {
-    if (mode == 1 && flag && *flag) return;
-    __shared__ double ws[32];
-    double s = 0.0;
-    for (int b = threadIdx.x; b < np; b += blockDim.x) s += partial[b];
-    s = warp_sum(s);
-    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        s = threadIdx.x < (blockDim.x >> 5) ? ws[threadIdx.x] : 0.0;
-        s = warp_sum(s);
-        if (threadIdx.x == 0) {
-            if (mode == 0) {
-                norms[0] = s;
-            } else {
-                norms[1] = s;
-                const double f2 = norms[0] > 0.0 ? norms[0] : 1.0;
-                if (s < tol2 * f2) {
-                    if (flag) *flag = 1;
-                } else if (cycles) {
-                    *cycles += 1;
-                }
-            }
+    const int nb = gridDim.x * gridDim.y, bid = blockIdx.y * gridDim.x + blockIdx.x;
+    if (t == 0) {
+        double sa = 0.0, sb = 0.0;
+        for (int w = 0; w < 8; ++w) {
+            sa += ws[0][w];
+            sb += ws[1][w];
         }
+        N.partial[bid] = sa;
+        N.partial[nb + bid] = sb;
+        __threadfence();
+        last = atomicAdd(N.done, 1u) == unsigned(nb - 1);
     }
-}
-
-__global__ void k_reset(int* flag, int* cycles) {
-    *flag = 0;
-    *cycles = 0;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // deterministic sum of the block partials: fixed stride per thread, fixed tree
+    const volatile double* P = N.partial;
+    double sa = 0.0, sb = 0.0;
+    for (int q = t; q < nb; q += 256) {
+        sa += P[q];
+        sb += P[nb + q];
+    }
+    sa = warp_sum(sa);
+    sb = warp_sum(sb);
+    __syncthreads();
+    if ((t & 31) == 0) {
+        ws[0][t >> 5] = sa;
+        ws[1][t >> 5] = sb;
+    }
+    __syncthreads();
+    if (t == 0) {
+        double r2 = 0.0, f2 = 0.0;
+        for (int w = 0; w < 8; ++w) {
+            r2 += ws[0][w];
+            f2 += ws[1][w];
+        }
+        if (initial) {
+            N.norms[0] = f2;
+            *N.cycles = 0;
+        } else {
+            *N.cycles += 1;
+            *N.total += 1;
+        }
+        N.norms[1] = r2;
+        const double ref = N.norms[0] > 0.0 ? N.norms[0] : 1.0;
+        const int conv = r2 < tol2 * ref;
+        *N.converged = conv;
+        const int cont = !conv && *N.cycles < max_cycles;
+        if (use_cond) cudaGraphSetConditional(cond, cont ? 1u : 0u);
+        *N.done = 0u;
+    }
 }
 
 // ---- host object ---------------------------------------------------------------
 
 struct MgImpl {
     int precision = PIC_MG_MIXED;
-    int nx = 0, ny = 0, L = 0;
+    int nx = 0, ny = 0, L = 0, Lc = 0;
     double dx = 0, dy = 0;
     pic_mg_options o{};
-    std::vector<MgLevel<float>> lf;
-    std::vector<MgLevel<double>> ld;
+    std::vector<LevelDev<float>> lf;
+    std::vector<LevelDev<double>> ld;
     std::vector<void*> allocs;
     double* ainv = nullptr;
     int* cidx = nullptr;
     int nfree_c = 0;
-    double* partial = nullptr;
-    int npartial = 0;
-    double* norms = nullptr;  // [||f||^2, ||r||^2]
-    int* flag = nullptr;      // converged
-    int* cycles = nullptr;    // V-cycles run (device count)
+    NormState N{};
     dim3 blk0{32, 8}, grd0;
-    long long launches = 0;  // kernel launches issued (all calls)
+    size_t coarse_smem = 0;
+    int coarse_off_e[kMgMaxCoarseLevels]{}, coarse_off_g[kMgMaxCoarseLevels]{}, coarse_off_m[kMgMaxCoarseLevels]{};
+    long long launches = 0;  // kernels executed by solves
+    int body_launches = 0;   // kernels per V-cycle
+    cudaStream_t side = nullptr;
+    cudaStream_t cap = nullptr;
+    // cached solve graph
+    cudaGraphExec_t exec = nullptr;
+    double* g_phi = nullptr;
+    const double* g_f = nullptr;
+    double g_tol = 0;
+    int g_max = -1;
 };
 
 }  // namespace pic
@@ -242,19 +429,23 @@ struct pic_mg {
 namespace pic {
 
 template <class T>
-static int alloc_levels(MgImpl& M, std::vector<MgLevel<T>>& lv, const std::vector<std::vector<uint8_t>>& masks,
+static int alloc_levels(MgImpl& M, std::vector<LevelDev<T>>& lv, const std::vector<std::vector<uint8_t>>& masks,
                         const std::vector<int>& nxs, const std::vector<int>& nys) {
     for (int l = 0; l < M.L; ++l) {
-        MgLevel<T> v;
+        LevelDev<T> v{};
         v.nx = nxs[l];
         v.ny = nys[l];
         const double hx = M.dx * double(1 << l), hy = M.dy * double(1 << l);
-        v.cx = T(1.0 / (hx * hx));
-        v.cy = T(1.0 / (hy * hy));
+        const double cx = 1.0 / (hx * hx), cy = 1.0 / (hy * hy);
+        v.cx = T(cx);
+        v.cy = T(cy);
+        v.inv_diag = T(1.0 / (2.0 * (cx + cy)));
         const size_t G = size_t(v.nx) * v.ny;
-        PIC_CUDA(cudaMalloc(&v.mask, G));
-        M.allocs.push_back(v.mask);
-        PIC_CUDA(cudaMemcpy(v.mask, masks[l].data(), G, cudaMemcpyHostToDevice));
+        uint8_t* mk = nullptr;
+        PIC_CUDA(cudaMalloc(&mk, G));
+        M.allocs.push_back(mk);
+        PIC_CUDA(cudaMemcpy(mk, masks[l].data(), G, cudaMemcpyHostToDevice));
+        v.mask = mk;
         PIC_CUDA(cudaMalloc(&v.e, G * sizeof(T)));
         M.allocs.push_back(v.e);
         PIC_CUDA(cudaMalloc(&v.g, G * sizeof(T)));
@@ -299,6 +490,34 @@ static bool invert(std::vector<double>& a, int n) {
     return true;
 }
 
+template <class T>
+static size_t tile_smem(int halo) {
+    const int W = kMgTile + 2 * halo;
+    return size_t(W) * W * (2 * sizeof(T) + 1);
+}
+
+template <class T>
+static int configure_kernels(MgImpl& M) {
+    const size_t down = tile_smem<T>(2 * M.o.pre_sweeps + 2), up = tile_smem<T>(2 * M.o.post_sweeps);
+    if (down > 227 * 1024 || up > 227 * 1024 || M.coarse_smem > 227 * 1024)
+        return fail(PIC_ERR_BAD_ARG, "multigrid: shared memory too large (sweeps %d/%d)", M.o.pre_sweeps,
+                    M.o.post_sweeps);
+    PIC_CUDA(cudaFuncSetAttribute(k_mg_down<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(down)));
+    PIC_CUDA(cudaFuncSetAttribute(k_mg_up<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(up)));
+    PIC_CUDA(cudaFuncSetAttribute(k_mg_coarse<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(M.coarse_smem)));
+    return PIC_OK;
+}
+
+static void mg_release(pic_mg* mg) {
+    if (!mg) return;
+    MgImpl& M = mg->m;
+    if (M.exec) cudaGraphExecDestroy(M.exec);
+    if (M.side) cudaStreamDestroy(M.side);
+    if (M.cap) cudaStreamDestroy(M.cap);
+    for (void* p : M.allocs) cudaFree(p);
+    delete mg;
+}
+
 int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const pic_mg_options* opts,
               pic_mg** out) {
     if (!out || !h_mask || nx < 3 || ny < 3 || !(dx > 0) || !(dy > 0))
@@ -317,10 +536,14 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
         if (opts->omega > 0) M.o.omega = opts->omega;
         if (opts->coarsest_max >= 3) M.o.coarsest_max = opts->coarsest_max;
     }
-    if (M.o.precision != PIC_MG_MIXED && M.o.precision != PIC_MG_FP64) {
-        delete mg;
-        return fail(PIC_ERR_BAD_ARG, "pic_mg_create: unknown precision %d", M.o.precision);
-    }
+    auto bail = [&](int code) {
+        mg_release(mg);
+        return code;
+    };
+    if (M.o.precision != PIC_MG_MIXED && M.o.precision != PIC_MG_FP64)
+        return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: unknown precision %d", M.o.precision));
+    if (M.o.pre_sweeps > 8 || M.o.post_sweeps > 8)
+        return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: at most 8 pre/post sweeps"));
     M.precision = M.o.precision;
     M.nx = nx;
     M.ny = ny;
@@ -341,8 +564,14 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
         masks.push_back(std::move(mc));
     }
     M.L = int(nxs.size());
+    M.Lc = 0;
+    while (M.Lc < M.L && long(nxs[M.Lc]) * nys[M.Lc] > kCoarseMaxNodes) ++M.Lc;
+    if (M.L - M.Lc > kMgMaxCoarseLevels) M.Lc = M.L - kMgMaxCoarseLevels;
+    if (M.Lc >= M.L)
+        return bail(fail(PIC_ERR_BAD_ARG,
+                         "pic_mg_create: grid %dx%d does not coarsen below %ld nodes; node counts must be 2^k*c+1", nx,
+                         ny, kCoarseMaxNodes));
     const int ncx = nxs.back(), ncy = nys.back();
-    // coarsest dense system over free interior nodes
     std::vector<int> idx;
     std::vector<int> where(size_t(ncx) * ncy, -1);
     for (int j = 1; j < ncy - 1; ++j)
@@ -352,12 +581,8 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
                 idx.push_back(j * ncx + i);
             }
     M.nfree_c = int(idx.size());
-    if (M.nfree_c > 4096) {
-        delete mg;
-        return fail(PIC_ERR_BAD_ARG,
-                    "pic_mg_create: coarsest level %dx%d has %d unknowns; node counts must be 2^k*c+1 with a small c",
-                    ncx, ncy, M.nfree_c);
-    }
+    if (M.nfree_c > 4096)
+        return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: coarsest level %dx%d has %d unknowns", ncx, ncy, M.nfree_c));
     if (M.nfree_c > 0) {
         const double hx = dx * double(1 << (M.L - 1)), hy = dy * double(1 << (M.L - 1));
         const double ccx = 1.0 / (hx * hx), ccy = 1.0 / (hy * hy);
@@ -373,159 +598,197 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
                 if (b >= 0) A[size_t(a) * n + b] += w[q];
             }
         }
-        if (!invert(A, n)) {
-            delete mg;
-            return fail(PIC_ERR_NUMERIC, "pic_mg_create: singular coarsest system");
-        }
-        PIC_CUDA(cudaMalloc(&M.ainv, A.size() * sizeof(double)));
+        if (!invert(A, n)) return bail(fail(PIC_ERR_NUMERIC, "pic_mg_create: singular coarsest system"));
+        if (cudaMalloc(&M.ainv, A.size() * sizeof(double)) != cudaSuccess)
+            return bail(fail(PIC_ERR_CUDA, "pic_mg_create: out of device memory"));
         M.allocs.push_back(M.ainv);
-        PIC_CUDA(cudaMemcpy(M.ainv, A.data(), A.size() * sizeof(double), cudaMemcpyHostToDevice));
-        PIC_CUDA(cudaMalloc(&M.cidx, idx.size() * sizeof(int)));
+        cudaMemcpy(M.ainv, A.data(), A.size() * sizeof(double), cudaMemcpyHostToDevice);
+        if (cudaMalloc(&M.cidx, idx.size() * sizeof(int)) != cudaSuccess)
+            return bail(fail(PIC_ERR_CUDA, "pic_mg_create: out of device memory"));
         M.allocs.push_back(M.cidx);
-        PIC_CUDA(cudaMemcpy(M.cidx, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice));
+        cudaMemcpy(M.cidx, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice);
     }
+    const size_t esz = M.precision == PIC_MG_MIXED ? sizeof(float) : sizeof(double);
+    size_t off = 0;
+    for (int l = M.Lc; l < M.L; ++l) {
+        const size_t G = size_t(nxs[l]) * nys[l];
+        const int c = l - M.Lc;
+        M.coarse_off_e[c] = int(off);
+        off += ((G * esz + 15) / 16) * 16;
+        M.coarse_off_g[c] = int(off);
+        off += ((G * esz + 15) / 16) * 16;
+        M.coarse_off_m[c] = int(off);
+        off += ((G + 15) / 16) * 16;
+    }
+    M.coarse_smem = off;
     int st = M.precision == PIC_MG_MIXED ? alloc_levels(M, M.lf, masks, nxs, nys)
                                          : alloc_levels(M, M.ld, masks, nxs, nys);
-    if (st != PIC_OK) {
-        delete mg;
-        return st;
-    }
+    if (st == PIC_OK) st = M.precision == PIC_MG_MIXED ? configure_kernels<float>(M) : configure_kernels<double>(M);
+    if (st != PIC_OK) return bail(st);
     M.grd0 = dim3(div_up(nx, M.blk0.x), div_up(ny, M.blk0.y));
-    M.npartial = int(M.grd0.x * M.grd0.y);
-    PIC_CUDA(cudaMalloc(&M.partial, sizeof(double) * M.npartial));
-    M.allocs.push_back(M.partial);
-    PIC_CUDA(cudaMalloc(&M.norms, sizeof(double) * 2));
-    M.allocs.push_back(M.norms);
-    PIC_CUDA(cudaMalloc(&M.flag, sizeof(int) * 2));
-    M.allocs.push_back(M.flag);
-    M.cycles = M.flag + 1;
-    PIC_CUDA(cudaMemset(M.flag, 0, sizeof(int) * 2));
-    PIC_CUDA(cudaMemset(M.norms, 0, sizeof(double) * 2));
+    const int nb = int(M.grd0.x * M.grd0.y);
+    if (cudaMalloc(&M.N.partial, sizeof(double) * 2 * nb) != cudaSuccess)
+        return bail(fail(PIC_ERR_CUDA, "pic_mg_create: out of device memory"));
+    M.allocs.push_back(M.N.partial);
+    char* small = nullptr;
+    if (cudaMalloc(&small, 256) != cudaSuccess) return bail(fail(PIC_ERR_CUDA, "pic_mg_create: out of device memory"));
+    M.allocs.push_back(small);
+    cudaMemset(small, 0, 256);
+    M.N.norms = reinterpret_cast<double*>(small);
+    M.N.total = reinterpret_cast<long long*>(small + 16);
+    M.N.done = reinterpret_cast<unsigned*>(small + 24);
+    M.N.converged = reinterpret_cast<int*>(small + 28);
+    M.N.cycles = reinterpret_cast<int*>(small + 32);
+    if (cudaStreamCreateWithFlags(&M.side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&M.cap, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(PIC_ERR_CUDA, "pic_mg_create: stream creation failed"));
     *out = mg;
     return PIC_OK;
 }
 
+// One V-cycle followed by the residual check, launched on stream st.
 template <class T>
-static int vcycle(MgImpl& M, std::vector<MgLevel<T>>& lv, cudaStream_t st, const int* skip) {
-    const dim3 b2(32, 8);
-    M.launches += (long long)(M.L - 1) * (2 * M.o.pre_sweeps + 2 + 2 * M.o.post_sweeps) + (M.nfree_c > 0 ? 1 : 0);
+static int launch_cycle(MgImpl& M, std::vector<LevelDev<T>>& lv, double* phi, const double* f, double tol,
+                        int max_cycles, cudaGraphConditionalHandle cond, cudaStream_t st, int& count) {
     const T omega = T(M.o.omega);
-    for (int l = 0; l < M.L - 1; ++l) {
-        MgLevel<T>& f = lv[l];
-        MgLevel<T>& c = lv[l + 1];
-        const dim3 gs(div_up((f.nx + 1) / 2, b2.x), div_up(f.ny - 2, b2.y));
-        for (int s = 0; s < M.o.pre_sweeps; ++s)
-            for (int color = 0; color < 2; ++color)
-                k_smooth<T><<<gs, b2, 0, st>>>(f.e, f.g, f.mask, f.nx, f.ny, f.cx, f.cy, omega, color, skip);
-        const dim3 gc(div_up(c.nx, b2.x), div_up(c.ny, b2.y));
-        k_resid_restrict<T><<<gc, b2, 0, st>>>(f.e, f.g, f.mask, f.nx, f.cx, f.cy, c.g, c.e, c.mask, c.nx, c.ny, skip);
+    const size_t down = tile_smem<T>(2 * M.o.pre_sweeps + 2), up = tile_smem<T>(2 * M.o.post_sweeps);
+    count = 0;
+    for (int l = 0; l < M.Lc; ++l) {
+        const dim3 g(div_up(lv[l].nx, kMgTile), div_up(lv[l].ny, kMgTile));
+        k_mg_down<T><<<g, kMgThreads, down, st>>>(lv[l], lv[l + 1], omega, M.o.pre_sweeps);
+        ++count;
     }
-    MgLevel<T>& cl = lv[M.L - 1];
-    if (M.nfree_c > 0) {
-        const int thr = M.nfree_c < 1024 ? ((M.nfree_c + 31) / 32) * 32 : 1024;
-        k_coarse_solve<T><<<1, thr, sizeof(double) * M.nfree_c, st>>>(cl.e, cl.g, M.ainv, M.cidx, M.nfree_c, skip);
+    CoarseDesc<T> D{};
+    D.nlev = M.L - M.Lc;
+    for (int c = 0; c < D.nlev; ++c) {
+        D.lv[c] = lv[M.Lc + c];
+        D.off_e[c] = M.coarse_off_e[c];
+        D.off_g[c] = M.coarse_off_g[c];
+        D.off_m[c] = M.coarse_off_m[c];
     }
-    for (int l = M.L - 2; l >= 0; --l) {
-        MgLevel<T>& f = lv[l];
-        MgLevel<T>& c = lv[l + 1];
-        const dim3 gp(div_up(f.nx, b2.x), div_up(f.ny, b2.y));
-        k_prolong_add<T><<<gp, b2, 0, st>>>(f.e, f.mask, f.nx, f.ny, c.e, c.nx, skip);
-        const dim3 gs(div_up((f.nx + 1) / 2, b2.x), div_up(f.ny - 2, b2.y));
-        for (int s = 0; s < M.o.post_sweeps; ++s)
-            for (int color = 0; color < 2; ++color)
-                k_smooth<T><<<gs, b2, 0, st>>>(f.e, f.g, f.mask, f.nx, f.ny, f.cx, f.cy, omega, color, skip);
+    D.ainv = M.ainv;
+    D.cidx = M.cidx;
+    D.nf = M.nfree_c;
+    D.omega = omega;
+    D.pre = M.o.pre_sweeps;
+    D.post = M.o.post_sweeps;
+    D.phi0 = M.Lc == 0 ? phi : nullptr;
+    k_mg_coarse<T><<<1, kCoarseThreads, M.coarse_smem, st>>>(D);
+    ++count;
+    for (int l = M.Lc - 1; l >= 0; --l) {
+        const dim3 g(div_up(lv[l].nx, kMgTile), div_up(lv[l].ny, kMgTile));
+        k_mg_up<T><<<g, kMgThreads, up, st>>>(lv[l], lv[l + 1], omega, M.o.post_sweeps, l == 0 ? phi : nullptr);
+        ++count;
     }
+    k_mg_r0<T><<<M.grd0, M.blk0, 0, st>>>(phi, f, lv[0].mask, M.nx, M.ny, 1.0 / (M.dx * M.dx), 1.0 / (M.dy * M.dy),
+                                          lv[0].g, M.N, tol * tol, max_cycles, 0, cond, 1);
+    ++count;
     PIC_LAUNCH_CHECK();
     return PIC_OK;
 }
 
 template <class T>
-static int residual0(MgImpl& M, std::vector<MgLevel<T>>& lv, const double* phi, const double* f, cudaStream_t st,
-                     const int* skip, double tol, bool count) {
-    MgLevel<T>& l0 = lv[0];
-    k_residual0<T><<<M.grd0, M.blk0, 0, st>>>(phi, f, l0.mask, M.nx, M.ny, 1.0 / (M.dx * M.dx),
-                                              1.0 / (M.dy * M.dy), l0.g, l0.e, M.partial, skip);
-    k_finalize<<<1, 1024, 0, st>>>(M.partial, M.npartial, M.norms, 1, tol * tol, M.flag, count ? M.cycles : nullptr);
-    M.launches += 2;
+static int capture_solve(MgImpl& M, std::vector<LevelDev<T>>& lv, double* phi, const double* f, double tol,
+                         int max_cycles, cudaStream_t st) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    PIC_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
+    if (cs != cudaStreamCaptureStatusActive) return fail(PIC_ERR_BAD_ARG, "multigrid: stream is not capturing");
+    cudaGraphConditionalHandle h;
+    PIC_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+    k_mg_r0<T><<<M.grd0, M.blk0, 0, st>>>(phi, f, lv[0].mask, M.nx, M.ny, 1.0 / (M.dx * M.dx), 1.0 / (M.dy * M.dy),
+                                          lv[0].g, M.N, tol * tol, max_cycles, 1, h, 1);
     PIC_LAUNCH_CHECK();
+    PIC_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
+    cudaGraphNodeParams p{};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t cn;
+    PIC_CUDA(cudaGraphAddNode(&cn, g, deps, nd, &p));
+    cudaGraph_t body = p.conditional.phGraph_out[0];
+    PIC_CUDA(cudaStreamUpdateCaptureDependencies(st, &cn, 1, cudaStreamSetCaptureDependencies));
+    PIC_CUDA(cudaStreamBeginCaptureToGraph(M.side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    int count = 0;
+    const int rc = launch_cycle(M, lv, phi, f, tol, max_cycles, h, M.side, count);
+    cudaGraph_t body_out = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(M.side, &body_out);
+    if (rc != PIC_OK) return rc;
+    if (ec != cudaSuccess) return fail(PIC_ERR_CUDA, "multigrid body capture: %s", cudaGetErrorString(ec));
+    M.body_launches = count;
     return PIC_OK;
 }
 
-template <class T>
-static int correct0(MgImpl& M, std::vector<MgLevel<T>>& lv, double* phi, cudaStream_t st, const int* skip) {
-    const long G = long(M.nx) * M.ny;
-    k_correct0<T><<<grid_blocks(G, 256), 256, 0, st>>>(phi, lv[0].e, G, skip);
-    M.launches += 1;
-    PIC_LAUNCH_CHECK();
-    return PIC_OK;
+// Appends the whole solve (the residual, then a WHILE node over V-cycles) to
+// a capture in progress on `st`.
+int mg_capture(MgImpl& M, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
+    return M.precision == PIC_MG_MIXED ? capture_solve(M, M.lf, phi, f, tol, max_cycles, st)
+                                       : capture_solve(M, M.ld, phi, f, tol, max_cycles, st);
 }
 
-static int rhs_norm(MgImpl& M, const double* f, cudaStream_t st) {
-    const uint8_t* mask0 = M.precision == PIC_MG_MIXED ? M.lf[0].mask : M.ld[0].mask;
-    k_sumsq_free<<<M.grd0, M.blk0, 0, st>>>(f, mask0, M.nx, M.ny, M.partial);
-    k_finalize<<<1, 1024, 0, st>>>(M.partial, M.npartial, M.norms, 0, 0.0, nullptr, nullptr);
-    M.launches += 2;
-    PIC_LAUNCH_CHECK();
-    return PIC_OK;
-}
-
-int mg_residual_step(MgImpl& M, const double* phi, const double* f, cudaStream_t st, const int* skip, double tol,
-                     bool count) {
-    return M.precision == PIC_MG_MIXED ? residual0(M, M.lf, phi, f, st, skip, tol, count)
-                                       : residual0(M, M.ld, phi, f, st, skip, tol, count);
-}
-
-int mg_cycle_and_correct(MgImpl& M, double* phi, cudaStream_t st, const int* skip) {
-    if (M.precision == PIC_MG_MIXED) {
-        PIC_TRY(vcycle(M, M.lf, st, skip));
-        return correct0(M, M.lf, phi, st, skip);
+static int ensure_graph(MgImpl& M, double* phi, const double* f, double tol, int max_cycles) {
+    if (M.exec && M.g_phi == phi && M.g_f == f && M.g_tol == tol && M.g_max == max_cycles) return PIC_OK;
+    if (M.exec) {
+        cudaGraphExecDestroy(M.exec);
+        M.exec = nullptr;
     }
-    PIC_TRY(vcycle(M, M.ld, st, skip));
-    return correct0(M, M.ld, phi, st, skip);
-}
-
-int mg_solve_async(MgImpl& M, double* phi, const double* f, double tol, int cycles, cudaStream_t st) {
-    k_reset<<<1, 1, 0, st>>>(M.flag, M.cycles);
-    M.launches += 1;
-    PIC_TRY(rhs_norm(M, f, st));
-    for (int c = 0; c < cycles; ++c) {
-        PIC_TRY(mg_residual_step(M, phi, f, st, M.flag, tol, true));
-        PIC_TRY(mg_cycle_and_correct(M, phi, st, M.flag));
+    PIC_CUDA(cudaStreamBeginCapture(M.cap, cudaStreamCaptureModeThreadLocal));
+    const int rc = mg_capture(M, phi, f, tol, max_cycles, M.cap);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(M.cap, &g);
+    if (rc != PIC_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
     }
-    // final residual of the last correction
-    PIC_TRY(mg_residual_step(M, phi, f, st, M.flag, tol, false));
+    if (ec != cudaSuccess) return fail(PIC_ERR_CUDA, "multigrid capture: %s", cudaGetErrorString(ec));
+    const cudaError_t ei = cudaGraphInstantiate(&M.exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) return fail(PIC_ERR_CUDA, "multigrid graph instantiate: %s", cudaGetErrorString(ei));
+    M.g_phi = phi;
+    M.g_f = f;
+    M.g_tol = tol;
+    M.g_max = max_cycles;
     return PIC_OK;
 }
 
-int mg_read_info(MgImpl& M, double tol, pic_mg_info* info) {
+int mg_read_info(MgImpl& M, pic_mg_info* info) {
+    unsigned char small[40];
+    PIC_CUDA(cudaMemcpy(small, M.N.norms, sizeof small, cudaMemcpyDeviceToHost));
     double norms[2];
-    int fc[2];
-    PIC_CUDA(cudaMemcpy(norms, M.norms, sizeof norms, cudaMemcpyDeviceToHost));
-    PIC_CUDA(cudaMemcpy(fc, M.flag, sizeof fc, cudaMemcpyDeviceToHost));
+    int conv, cycles;
+    memcpy(norms, small, 16);
+    memcpy(&conv, small + 28, 4);
+    memcpy(&cycles, small + 32, 4);
     info->rhs_norm = std::sqrt(norms[0]);
-    const double f = norms[0] > 0 ? std::sqrt(norms[0]) : 1.0;
-    info->rel_res = std::sqrt(norms[1]) / f;
-    info->cycles = fc[1];
-    info->converged = fc[0] ? 1 : (info->rel_res < tol ? 1 : 0);
+    const double fn = norms[0] > 0 ? std::sqrt(norms[0]) : 1.0;
+    info->rel_res = std::sqrt(norms[1]) / fn;
+    info->cycles = cycles;
+    info->converged = conv ? 1 : 0;
+    return PIC_OK;
+}
+
+long long mg_total_cycles(pic_mg* mg) {
+    long long t = 0;
+    if (mg) cudaMemcpy(&t, mg->m.N.total, sizeof t, cudaMemcpyDeviceToHost);
+    return t;
+}
+
+int mg_launch(MgImpl& M, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
+    PIC_TRY(ensure_graph(M, phi, f, tol, max_cycles));
+    PIC_CUDA(cudaGraphLaunch(M.exec, st));
     return PIC_OK;
 }
 
 int mg_solve(MgImpl& M, double* phi, const double* f, double tol, int max_cycles, pic_mg_info* info,
              cudaStream_t st) {
-    k_reset<<<1, 1, 0, st>>>(M.flag, M.cycles);
-    M.launches += 1;
-    PIC_TRY(rhs_norm(M, f, st));
+    PIC_TRY(mg_launch(M, phi, f, tol, max_cycles, st));
+    PIC_CUDA(cudaStreamSynchronize(st));
     pic_mg_info loc{};
-    int c = 0;
-    for (;;) {
-        PIC_TRY(mg_residual_step(M, phi, f, st, nullptr, tol, false));
-        PIC_CUDA(cudaStreamSynchronize(st));
-        PIC_TRY(mg_read_info(M, tol, &loc));
-        loc.cycles = c;
-        if (loc.converged || c >= max_cycles) break;
-        PIC_TRY(mg_cycle_and_correct(M, phi, st, nullptr));
-        ++c;
-    }
+    PIC_TRY(mg_read_info(M, &loc));
+    M.launches += 1 + (long long)(loc.cycles) * M.body_launches;
     if (info) *info = loc;
     if (!loc.converged)
         return fail(PIC_ERR_NOT_CONVERGED, "multigrid: relative residual %.3e after %d cycles (tol %.1e)", loc.rel_res,
@@ -534,6 +797,14 @@ int mg_solve(MgImpl& M, double* phi, const double* f, double tol, int max_cycles
 }
 
 long long mg_launches(pic_mg* mg) { return mg ? mg->m.launches : 0; }
+int mg_body_launches(pic_mg* mg) { return mg ? mg->m.body_launches : 0; }
+int mg_capture_into(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
+    return mg_capture(mg->m, phi, f, tol, max_cycles, st);
+}
+int mg_launch_graph(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
+    return mg_launch(mg->m, phi, f, tol, max_cycles, st);
+}
+int mg_info(pic_mg* mg, pic_mg_info* info) { return mg_read_info(mg->m, info); }
 
 }  // namespace pic
 
@@ -550,8 +821,8 @@ int pic_mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_dirichl
 int pic_mg_destroy(pic_mg* mg) {
     clear_error();
     if (!mg) return PIC_OK;
-    for (void* p : mg->m.allocs) cudaFree(p);
-    delete mg;
+    cudaDeviceSynchronize();
+    mg_release(mg);
     return PIC_OK;
 }
 
@@ -566,13 +837,15 @@ int pic_mg_solve_async(pic_mg* mg, double* d_phi, const double* d_f, double tol,
     clear_error();
     if (!mg || !d_phi || !d_f || !(tol > 0) || cycles < 0)
         return fail(PIC_ERR_BAD_ARG, "pic_mg_solve_async: bad arguments");
-    return mg_solve_async(mg->m, d_phi, d_f, tol, cycles, as_stream(stream));
+    return mg_launch(mg->m, d_phi, d_f, tol, cycles, as_stream(stream));
 }
 
 int pic_mg_read_info(pic_mg* mg, double tol, pic_mg_info* info) {
     clear_error();
+    (void)tol;
     if (!mg || !info) return fail(PIC_ERR_BAD_ARG, "pic_mg_read_info: bad arguments");
-    return mg_read_info(mg->m, tol, info);
+    PIC_CUDA(cudaDeviceSynchronize());
+    return mg_read_info(mg->m, info);
 }
 
 }  // extern "C"

@@ -32,14 +32,20 @@ int launch_update_E(const double* phi, float* Ex, float* Ey, float2* E2, int nx,
                     cudaStream_t st);
 int launch_form_rhs(const float* rho, const uint8_t* dirichlet, double eps0, double* f, float* snapshot, float* zero,
                     long G, cudaStream_t st);
-struct MgImpl;
 int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const pic_mg_options* opts, pic_mg** out);
-long long mg_launches(pic_mg* mg);
+int mg_body_launches(pic_mg* mg);
+long long mg_total_cycles(pic_mg* mg);
+int mg_capture_into(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st);
+int mg_launch_graph(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st);
+int mg_info(pic_mg* mg, pic_mg_info* info);
 
 constexpr int kPushThreads = 256;
-constexpr int kPushP = 9;  // particles per thread (odd: conflict-free blocked access to shared memory)
+constexpr int kPushP = 7;  // particles per thread (odd: conflict-free blocked access to shared memory)
 constexpr int kChunk = kPushThreads * kPushP;
-constexpr int kHalo = 4;   // cells staged around a tile
+constexpr int kBufStride = kChunk + 8;  // floats per array per buffer: room for the 16-byte alignment window
+constexpr int kHalo = 4;                // cells staged around a tile
+constexpr int kArraySlack = 16;         // floats allocated past each species' capacity (bulk-copy window)
+constexpr unsigned long long kWaitLimit = 1ull << 24;  // bounded mbarrier wait
 
 // Device-resident per-species state (the sort swaps the buffers).
 struct SpeciesState {
@@ -67,11 +73,12 @@ struct PushArgs {
     float* rho;
     int nx, ny, tile, tiles_x, rw;
     int do_kick, do_mcc, do_drift, do_deposit;
-    MccDev mcc;
+    const MccDev* mcc;  // device copy of the tables' descriptor
     uint2 key;
     const uint32_t* step;
     BirthDev births;
     unsigned long long* ctr;
+    int* error;  // set when a bounded wait gives up
 };
 
 __device__ __forceinline__ void flush_run(const PushArgs& A, float* rt, bool tiled, int ox, int oy, int i0, int j0,
@@ -89,45 +96,127 @@ __device__ __forceinline__ void flush_run(const PushArgs& A, float* rt, bool til
     }
 }
 
-__global__ void __launch_bounds__(kPushThreads) k_push(PushArgs A) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    float* px = reinterpret_cast<float*>(smem);
-    float* py = px + kChunk;
-    float* pvx = py + kChunk;
-    float* pvy = pvx + kChunk;
-    float* pvz = pvy + kChunk;
+// ---- TMA bulk copies and mbarriers (inline PTX, no multicast) -------------------
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return unsigned(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* m, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(m)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* m, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(m)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* m) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(m))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* m, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(m)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Waits for the phase with the given parity; false after kWaitLimit polls.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* m, unsigned parity) {
+    for (unsigned long long k = 0; k < kWaitLimit; ++k)
+        if (mbar_try_wait(m, parity)) return true;
+    return false;
+}
+
+// Issues the bulk copies of item `it` into buffer `buf` (one thread).
+__device__ __forceinline__ void issue_item(const PushArgs& A, int it, float* buf, unsigned long long* bar) {
+    const int4 item = A.items[it];
+    const int a0 = item.z & ~3, a1 = (item.w + 3) & ~3;
+    const unsigned bytes = unsigned(a1 - a0) * 4u;
+    if (bytes == 0) {
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+        return;
+    }
+    mbar_expect_tx(bar, 5u * bytes);
+    const SpeciesState& S = A.state[item.x];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) bulk_g2s(buf + c * kBufStride, S.cur[c] + a0, bytes, bar);
+}
+
+// The rarely taken collision branch, kept out of line to spare registers.
+__device__ __noinline__ void push_collide(const MccDev* __restrict__ M, BirthDev B, unsigned long long* ctr, uint2 key,
+                                          int s, int slot, uint32_t step, float x, float y, float* v) {
+    float vx = v[0], vy = v[1], vz = v[2];
+    const MccOutcome o = mcc_collide(*M, M->sp[s], uint32_t(s), uint32_t(slot), step, key, vx, vy, vz);
+    if (o.overflow) atomicAdd(ctr + kCtrOverflow, 1ull);
+    if (o.proc >= 0) {
+        atomicAdd(ctr + kCtrCollisions + s * PIC_MAX_PROCESSES + o.proc, 1ull);
+        if (o.born) {
+            const MccSpeciesDev& S = M->sp[s];
+            const bool ok_e = birth_push(B, S.born_e, x, y, o.be[0], o.be[1], o.be[2]);
+            const bool ok_i = birth_push(B, S.born_i, x, y, o.bi[0], o.bi[1], o.bi[2]);
+            if (!ok_e || !ok_i) atomicAdd(ctr + kCtrDropped, 1ull);
+        }
+    }
+    v[0] = vx;
+    v[1] = vy;
+    v[2] = vz;
+}
+
+__global__ void __launch_bounds__(kPushThreads, 2) k_push(PushArgs A) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    float* bufs = reinterpret_cast<float*>(smem);  // [2][5][kBufStride]
     const int RW = A.rw;
-    float2* et = reinterpret_cast<float2*>(pvz + kChunk);
+    float2* et = reinterpret_cast<float2*>(bufs + 2 * 5 * kBufStride);
     float* rt = reinterpret_cast<float*>(et + RW * RW);
     unsigned* bits = reinterpret_cast<unsigned*>(rt + RW * RW);
-    __shared__ int s_item;
+    __shared__ __align__(8) unsigned long long bar[2];
+    __shared__ int s_item[2];
     __shared__ unsigned s_abs, s_cand;
     const int tid = threadIdx.x;
     const uint32_t step = A.do_mcc ? *A.step : 0u;
+    const int n_items = *A.n_items;
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+        const int it0 = atomicAdd(A.item_next, 1);
+        s_item[0] = it0;
+        if (it0 < n_items) issue_item(A, it0, bufs, &bar[0]);
+    }
+    __syncthreads();
+    unsigned phase[2] = {0u, 0u};
+    int cur = 0;
     for (;;) {
+        const int it = s_item[cur];
+        if (it >= n_items) break;
         if (tid == 0) {
-            s_item = atomicAdd(A.item_next, 1);
             s_abs = 0;
             s_cand = 0;
+            const int nx_it = atomicAdd(A.item_next, 1);
+            s_item[cur ^ 1] = nx_it;
+            if (nx_it < n_items) {
+                fence_proxy_async();
+                issue_item(A, nx_it, bufs + (cur ^ 1) * 5 * kBufStride, &bar[cur ^ 1]);
+            }
         }
-        __syncthreads();
-        const int it = s_item;
-        if (it >= *A.n_items) break;
         const int4 item = A.items[it];
         const int s = item.x, tile = item.y, b = item.z, e = item.w, n = e - b;
+        const int off = b - (b & ~3);
+        float* const px = bufs + cur * 5 * kBufStride + off;
+        float* const py = px + kBufStride;
+        float* const pvx = py + kBufStride;
+        float* const pvy = pvx + kBufStride;
+        float* const pvz = pvy + kBufStride;
         const SpeciesConst C = A.sp[s];
-        float* const gx = A.state[s].cur[0];
-        float* const gy = A.state[s].cur[1];
-        float* const gvx = A.state[s].cur[2];
-        float* const gvy = A.state[s].cur[3];
-        float* const gvz = A.state[s].cur[4];
-        for (int l = tid; l < n; l += kPushThreads) {
-            px[l] = gx[b + l];
-            py[l] = gy[b + l];
-            pvx[l] = gvx[b + l];
-            pvy[l] = gvy[b + l];
-            pvz[l] = gvz[b + l];
-        }
         const bool tiled = tile >= 0;
         int ox = 0, oy = 0;
         if (tiled) {
@@ -135,23 +224,33 @@ __global__ void __launch_bounds__(kPushThreads) k_push(PushArgs A) {
             oy = (tile / A.tiles_x) * A.tile - kHalo;
             for (int q = tid; q < RW * RW; q += kPushThreads) {
                 const int gi = ox + q % RW, gj = oy + q / RW;
-                et[q] = (gi >= 0 && gj >= 0 && gi < A.nx && gj < A.ny) ? A.E[long(gj) * A.nx + gi]
+                et[q] = (gi >= 0 && gj >= 0 && gi < A.nx && gj < A.ny) ? __ldg(A.E + long(gj) * A.nx + gi)
                                                                          : make_float2(0.f, 0.f);
                 rt[q] = 0.0f;
             }
         }
-        const bool mcc = A.do_mcc && A.mcc.sp[s].nproc > 0;
+        const bool mcc = A.do_mcc && A.mcc->sp[s].nproc > 0;
         if (mcc) {
-            for (int q = tid; q < kChunk / 32; q += kPushThreads) bits[q] = 0;
+            for (int q = tid; q < kChunk / 32 + 1; q += kPushThreads) bits[q] = 0;
             __syncthreads();
             if (tid < 32) {
                 const long g0 = b / long(kMccSegment), g1 = (e - 1) / long(kMccSegment);
                 const int slots = A.state[s].count;
                 for (long g = g0 + tid; g <= g1; g += 32)
-                    mcc_mark_segment(A.mcc.sp[s], uint32_t(s), g, slots, b, e, step, A.key, bits);
+                    mcc_mark_segment(A.mcc->sp[s], uint32_t(s), g, slots, b, e, step, A.key, bits);
             }
         }
-        __syncthreads();
+        const bool ok = mbar_wait(&bar[cur], phase[cur]);
+        phase[cur] ^= 1u;
+        if (__syncthreads_or(!ok)) {
+            // give up on this launch: flag it, then wait (bounded) for the copies still in flight
+            if (tid == 0) {
+                atomicExch(A.error, 1);
+                mbar_wait(&bar[cur ^ 1], phase[cur ^ 1]);
+            }
+            __syncthreads();
+            break;
+        }
 
         int ri0 = -1, rj0 = 0, ri1 = 0, rj1 = 0;
         float s00 = 0.f, s10 = 0.f, s01 = 0.f, s11 = 0.f;
@@ -161,17 +260,18 @@ __global__ void __launch_bounds__(kPushThreads) k_push(PushArgs A) {
             if (l >= n) break;
             float x = px[l], y = py[l];
             if (!is_live(x)) continue;
-            float vx = pvx[l], vy = pvy[l], vz = pvz[l];
+            float v[3] = {pvx[l], pvy[l], pvz[l]};
             if (A.do_kick) {
                 const Cic c = cic_weights(x, y, A.nx, A.ny);
                 const int li = c.i0 - ox, lj = c.j0 - oy;
                 float2 e00, e10, e01, e11;
                 if (tiled && li >= 0 && lj >= 0 && li + 1 < RW && lj + 1 < RW) {
                     const int q = lj * RW + li;
+                    const int dq = c.i1 - c.i0, dr = (c.j1 - c.j0) * RW;
                     e00 = et[q];
-                    e10 = et[q + (c.i1 - c.i0)];
-                    e01 = et[q + (c.j1 - c.j0) * RW];
-                    e11 = et[q + (c.j1 - c.j0) * RW + (c.i1 - c.i0)];
+                    e10 = et[q + dq];
+                    e01 = et[q + dr];
+                    e11 = et[q + dr + dq];
                 } else {
                     e00 = __ldg(A.E + long(c.j0) * A.nx + c.i0);
                     e10 = __ldg(A.E + long(c.j0) * A.nx + c.i1);
@@ -180,27 +280,16 @@ __global__ void __launch_bounds__(kPushThreads) k_push(PushArgs A) {
                 }
                 const float ex = cic_interp(c, e00.x, e10.x, e01.x, e11.x);
                 const float ey = cic_interp(c, e00.y, e10.y, e01.y, e11.y);
-                vx = __fmaf_rn(C.kq, ex, vx);
-                vy = __fmaf_rn(C.kq, ey, vy);
+                v[0] = __fmaf_rn(C.kq, ex, v[0]);
+                v[1] = __fmaf_rn(C.kq, ey, v[1]);
             }
             if (mcc && (bits[l >> 5] & (1u << (l & 31)))) {
                 ++my_cand;
-                const MccOutcome o =
-                    mcc_collide(A.mcc, A.mcc.sp[s], uint32_t(s), uint32_t(b + l), step, A.key, vx, vy, vz);
-                if (o.overflow) atomicAdd(A.ctr + kCtrOverflow, 1ull);
-                if (o.proc >= 0) {
-                    atomicAdd(A.ctr + kCtrCollisions + s * PIC_MAX_PROCESSES + o.proc, 1ull);
-                    if (o.born) {
-                        const MccSpeciesDev& S = A.mcc.sp[s];
-                        const bool ok_e = birth_push(A.births, S.born_e, x, y, o.be[0], o.be[1], o.be[2]);
-                        const bool ok_i = birth_push(A.births, S.born_i, x, y, o.bi[0], o.bi[1], o.bi[2]);
-                        if (!ok_e || !ok_i) atomicAdd(A.ctr + kCtrDropped, 1ull);
-                    }
-                }
+                push_collide(A.mcc, A.births, A.ctr, A.key, s, b + l, step, x, y, v);
             }
             if (A.do_drift) {
-                x = __fmaf_rn(vx, C.dtdx, x);
-                y = __fmaf_rn(vy, C.dtdy, y);
+                x = __fmaf_rn(v[0], C.dtdx, x);
+                y = __fmaf_rn(v[1], C.dtdy, y);
                 if (!(x >= 0.0f && x <= float(A.nx - 1) && y >= 0.0f && y <= float(A.ny - 1))) {
                     x = __int_as_float(0x7fc00000);
                     y = x;
@@ -209,9 +298,9 @@ __global__ void __launch_bounds__(kPushThreads) k_push(PushArgs A) {
             }
             px[l] = x;
             py[l] = y;
-            pvx[l] = vx;
-            pvy[l] = vy;
-            pvz[l] = vz;
+            pvx[l] = v[0];
+            pvy[l] = v[1];
+            pvz[l] = v[2];
             if (A.do_deposit && is_live(x)) {
                 const Cic c = cic_weights(x, y, A.nx, A.ny);
                 if (c.i0 != ri0 || c.j0 != rj0) {
@@ -236,17 +325,22 @@ __global__ void __launch_bounds__(kPushThreads) k_push(PushArgs A) {
             if (my_cand) atomicAdd(&s_cand, my_cand);
         }
         __syncthreads();
+        float* const gx = A.state[s].cur[0] + b;
+        float* const gy = A.state[s].cur[1] + b;
+        float* const gvx = A.state[s].cur[2] + b;
+        float* const gvy = A.state[s].cur[3] + b;
+        float* const gvz = A.state[s].cur[4] + b;
         for (int l = tid; l < n; l += kPushThreads) {
-            gx[b + l] = px[l];
-            gy[b + l] = py[l];
-            gvx[b + l] = pvx[l];
-            gvy[b + l] = pvy[l];
-            gvz[b + l] = pvz[l];
+            gx[l] = px[l];
+            gy[l] = py[l];
+            gvx[l] = pvx[l];
+            gvy[l] = pvy[l];
+            gvz[l] = pvz[l];
         }
         if (tiled && A.do_deposit) {
             for (int q = tid; q < RW * RW; q += kPushThreads) {
-                const float v = rt[q];
-                if (v != 0.0f) atomicAdd(A.rho + long(oy + q / RW) * A.nx + ox + q % RW, v);
+                const float val = rt[q];
+                if (val != 0.0f) atomicAdd(A.rho + long(oy + q / RW) * A.nx + ox + q % RW, val);
             }
         }
         if (tid == 0) {
@@ -254,6 +348,7 @@ __global__ void __launch_bounds__(kPushThreads) k_push(PushArgs A) {
             if (s_cand) atomicAdd(A.ctr + kCtrCandidates + s, (unsigned long long)s_cand);
         }
         __syncthreads();
+        cur ^= 1;
     }
 }
 
@@ -415,6 +510,7 @@ struct SimImpl {
     pic_mg* mg = nullptr;
     MccHost mcc;
     bool have_mcc = false;
+    MccDev* mcc_dev = nullptr;  // device copy of mcc.dev
     std::vector<void*> allocs;
     SpeciesState* d_state = nullptr;
     SpeciesState h_state[PIC_MAX_SPECIES]{};
@@ -426,6 +522,7 @@ struct SimImpl {
     int* tile_start = nullptr;
     BirthDev births{};
     unsigned long long* ctr = nullptr;
+    int* error = nullptr;
     float2* E2 = nullptr;
     float *Ex = nullptr, *Ey = nullptr, *rho_acc = nullptr, *rho_out = nullptr;
     double *phi = nullptr, *f = nullptr;
@@ -435,8 +532,11 @@ struct SimImpl {
     int rw = 0;
     bool kick_pending = false;
     long long steps = 0;
-    long long launches = 0;
+    long long launches = 0;  // launches outside the multigrid loop
+    long long solves = 0;    // multigrid solves issued (each runs 1 + cycles * body kernels)
     bool profiling = false;
+    cudaStream_t cap = nullptr;
+    cudaGraphExec_t g_step = nullptr, g_sort_step = nullptr;
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
     std::vector<cudaEvent_t> event_pool;
     long long prof_cycles = 0;
@@ -506,11 +606,12 @@ static PushArgs push_args(SimImpl& S, int kick, int mcc, int drift, int deposit,
     A.do_mcc = mcc && S.have_mcc;
     A.do_drift = drift;
     A.do_deposit = deposit;
-    if (S.have_mcc) A.mcc = S.mcc.dev;
+    A.mcc = S.mcc_dev;
     A.key = make_uint2(uint32_t(S.d.seed), uint32_t(S.d.seed >> 32));
     A.step = S.step_ctr;
     A.births = S.births;
     A.ctr = S.ctr;
+    A.error = S.error;
     return A;
 }
 
@@ -535,28 +636,22 @@ static int particle_pass(SimImpl& S, cudaStream_t st, int kick, int mcc, int dri
     return PIC_OK;
 }
 
-static int field_solve(SimImpl& S, cudaStream_t st) {
+static int field_solve(SimImpl& S, cudaStream_t st, bool capturing) {
     {
         PhaseTimer t(S, PIC_PHASE_RHS, st);
         PIC_TRY(launch_form_rhs(S.rho_acc, S.dirichlet, S.d.eps0, S.f, S.rho_out, S.rho_acc, S.G, st));
     }
-    pic_mg_info info{};
-    int rc;
-    const long long before = mg_launches(S.mg);
     {
         PhaseTimer t(S, PIC_PHASE_SOLVE, st);
-        rc = pic_mg_solve(S.mg, S.phi, S.f, S.d.tol, S.d.max_cycles, &info, st);
+        if (capturing) PIC_TRY(mg_capture_into(S.mg, S.phi, S.f, S.d.tol, S.d.max_cycles, st));
+        else PIC_TRY(mg_launch_graph(S.mg, S.phi, S.f, S.d.tol, S.d.max_cycles, st));
     }
-    S.launches += 1 + (mg_launches(S.mg) - before);
-    S.last = info;
-    S.last_status = rc;
-    if (S.profiling) S.prof_cycles += info.cycles;
-    if (rc != PIC_OK && rc != PIC_ERR_NOT_CONVERGED) return rc;
     {
         PhaseTimer t(S, PIC_PHASE_EFIELD, st);
         PIC_TRY(launch_update_E(S.phi, S.Ex, S.Ey, S.E2, S.nx, S.ny, S.d.dx, S.d.dy, st));
     }
-    S.launches += 1;
+    S.launches += 2;
+    S.solves += 1;
     return PIC_OK;
 }
 
@@ -576,6 +671,33 @@ static int sort_all(SimImpl& S, cudaStream_t st) {
     }
     k_tile_items<<<1, 1024, 0, st>>>(S.tile_start, R.ntiles, S.ns, S.items, S.n_tiled);
     PIC_LAUNCH_CHECK();
+    return PIC_OK;
+}
+
+// The steady-state step (kick + MCC + drift + deposit, solve, E), optionally
+// preceded by the cell sort, captured once into a CUDA graph.
+static int capture_step(SimImpl& S, bool with_sort, cudaGraphExec_t* out) {
+    const bool prof = S.profiling;
+    S.profiling = false;
+    const long long l0 = S.launches, s0 = S.solves;
+    PIC_CUDA(cudaStreamBeginCapture(S.cap, cudaStreamCaptureModeThreadLocal));
+    int rc = PIC_OK;
+    if (with_sort) rc = sort_all(S, S.cap);
+    if (rc == PIC_OK) rc = particle_pass(S, S.cap, 1, 1, 1, 1, 1.0, 1);
+    if (rc == PIC_OK) rc = field_solve(S, S.cap, true);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(S.cap, &g);
+    S.profiling = prof;
+    S.launches = l0;  // counted when the graph is launched
+    S.solves = s0;
+    if (rc != PIC_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (ec != cudaSuccess) return fail(PIC_ERR_CUDA, "step capture: %s", cudaGetErrorString(ec));
+    const cudaError_t ei = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) return fail(PIC_ERR_CUDA, "step graph instantiate: %s", cudaGetErrorString(ei));
     return PIC_OK;
 }
 
@@ -606,13 +728,15 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
         PIC_TRY(mcc_build(d->mcc, S.ns, mass, d->dt, &S.mcc));
         S.have_mcc = true;
     }
+    PIC_TRY(dalloc(S, &S.mcc_dev, 1));
+    if (S.have_mcc) PIC_CUDA(cudaMemcpy(S.mcc_dev, &S.mcc.dev, sizeof(MccDev), cudaMemcpyHostToDevice));
     // species buffers
     for (int s = 0; s < S.ns; ++s) {
         const pic_species_desc& sp = d->species[s];
         SpeciesState& H = S.h_state[s];
         for (int c = 0; c < 5; ++c) {
-            PIC_TRY(dalloc(S, &H.cur[c], size_t(sp.capacity)));
-            PIC_TRY(dalloc(S, &H.alt[c], size_t(sp.capacity)));
+            PIC_TRY(dalloc(S, &H.cur[c], size_t(sp.capacity) + kArraySlack));
+            PIC_TRY(dalloc(S, &H.alt[c], size_t(sp.capacity) + kArraySlack));
         }
         H.count = 0;
         H.sorted_end = 0;
@@ -646,6 +770,7 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
     PIC_TRY(dalloc(S, &S.births.species, size_t(bcap)));
     PIC_TRY(dalloc(S, &S.births.count, 1));
     PIC_TRY(dalloc(S, &S.ctr, size_t(kCtrCount)));
+    PIC_TRY(dalloc(S, &S.error, 1));
     // fields
     PIC_TRY(dalloc(S, &S.E2, size_t(S.G)));
     PIC_TRY(dalloc(S, &S.Ex, size_t(S.G)));
@@ -665,17 +790,23 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
         PIC_CUDA(cudaMemcpy(S.phi, phi0.data(), sizeof(double) * S.G, cudaMemcpyHostToDevice));
     }
     // launch shape of the particle pass
-    S.push_smem = sizeof(float) * 5 * kChunk + size_t(S.rw) * S.rw * (sizeof(float2) + sizeof(float)) +
-                  sizeof(unsigned) * (kChunk / 32 + 1);
+    S.push_smem = sizeof(float) * 2 * 5 * kBufStride + size_t(S.rw) * S.rw * (sizeof(float2) + sizeof(float)) +
+                  sizeof(unsigned) * (kChunk / 32 + 2);
     PIC_CUDA(cudaFuncSetAttribute(k_push, cudaFuncAttributeMaxDynamicSharedMemorySize, int(S.push_smem)));
     int per_sm = 0;
     PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_push, kPushThreads, S.push_smem));
     S.push_grid = std::max(1, per_sm) * num_sms();
+    PIC_CUDA(cudaStreamCreateWithFlags(&S.cap, cudaStreamNonBlocking));
     (void)st;
     return PIC_OK;
 }
 
 static void sim_free(SimImpl& S) {
+    if (S.g_step) cudaGraphExecDestroy(S.g_step);
+    if (S.g_sort_step) cudaGraphExecDestroy(S.g_sort_step);
+    S.g_step = S.g_sort_step = nullptr;
+    if (S.cap) cudaStreamDestroy(S.cap);
+    S.cap = nullptr;
     for (auto& m : S.marks) {
         cudaEventDestroy(m.second.first);
         cudaEventDestroy(m.second.second);
@@ -753,10 +884,12 @@ int pic_sim_init(pic_sim* sim, void* stream) {
     cudaStream_t st = as_stream(stream);
     if (S.d.sort_interval > 0) PIC_TRY(sort_all(S, st));
     PIC_TRY(particle_pass(S, st, 0, 0, 0, 1, 1.0, 0));
-    PIC_TRY(field_solve(S, st));
+    PIC_TRY(field_solve(S, st, false));
     PIC_TRY(particle_pass(S, st, 1, 0, 0, 0, -0.5, 0));
     S.kick_pending = false;
-    return S.last_status;
+    PIC_CUDA(cudaStreamSynchronize(st));
+    PIC_TRY(mg_info(S.mg, &S.last));
+    return S.last.converged ? PIC_OK : PIC_ERR_NOT_CONVERGED;
 }
 
 int pic_sim_step(pic_sim* sim, int n_steps, void* stream) {
@@ -765,14 +898,23 @@ int pic_sim_step(pic_sim* sim, int n_steps, void* stream) {
     SimImpl& S = sim->s;
     cudaStream_t st = as_stream(stream);
     for (int i = 0; i < n_steps; ++i) {
-        if (S.d.sort_interval > 0 && S.steps % S.d.sort_interval == 0) PIC_TRY(sort_all(S, st));
-        const int k = S.kick_pending ? 1 : 0;
-        PIC_TRY(particle_pass(S, st, k, k, 1, 1, 1.0, 1));
-        PIC_TRY(field_solve(S, st));
+        const bool sort = S.d.sort_interval > 0 && S.steps % S.d.sort_interval == 0;
+        if (S.d.use_graph && S.kick_pending && !S.profiling) {
+            cudaGraphExec_t& g = sort ? S.g_sort_step : S.g_step;
+            if (!g) PIC_TRY(capture_step(S, sort, &g));
+            PIC_CUDA(cudaGraphLaunch(g, st));
+            S.launches += 3 + 2 + (sort ? 1 + (long long)S.ns * (5 + 3 * S.sorter.passes) : 0);
+            S.solves += 1;
+        } else {
+            if (sort) PIC_TRY(sort_all(S, st));
+            const int k = S.kick_pending ? 1 : 0;
+            PIC_TRY(particle_pass(S, st, k, k, 1, 1, 1.0, 1));
+            PIC_TRY(field_solve(S, st, false));
+        }
         S.kick_pending = true;
         ++S.steps;
     }
-    return S.last_status == PIC_ERR_NOT_CONVERGED ? PIC_ERR_NOT_CONVERGED : PIC_OK;
+    return PIC_OK;
 }
 
 int pic_sim_sync(pic_sim* sim, void* stream) {
@@ -826,13 +968,20 @@ int pic_sim_read_counters(pic_sim* sim, pic_sim_counters* out, void* stream) {
     }
     out->dropped_births = c[kCtrDropped];
     out->nu_overflow = c[kCtrOverflow];
+    PIC_TRY(mg_info(S.mg, &S.last));
     out->last_cycles = S.last.cycles;
     out->last_rel_res = S.last.rel_res;
     out->steps = S.steps;
     return PIC_OK;
 }
 
-long long pic_sim_kernel_launches(pic_sim* sim) { return sim ? sim->s.launches : 0; }
+long long pic_sim_kernel_launches(pic_sim* sim) {
+    if (!sim) return 0;
+    SimImpl& S = sim->s;
+    cudaDeviceSynchronize();
+    // each solve runs its residual kernel plus `body` kernels per V-cycle
+    return S.launches + S.solves + mg_total_cycles(S.mg) * mg_body_launches(S.mg);
+}
 
 int pic_sim_set_profiling(pic_sim* sim, int enable) {
     clear_error();
@@ -845,7 +994,7 @@ int pic_sim_set_profiling(pic_sim* sim, int enable) {
             S.event_pool.push_back(m.second.second);
         }
         S.marks.clear();
-        S.prof_cycles = 0;
+        S.prof_cycles = mg_total_cycles(S.mg);
     }
     S.profiling = enable != 0;
     return PIC_OK;
@@ -863,7 +1012,7 @@ int pic_sim_read_profile(pic_sim* sim, pic_sim_profile* out) {
         out->ms[m.first] += ms;
         out->count[m.first] += 1;
     }
-    out->mg_cycles = S.prof_cycles;
+    out->mg_cycles = mg_total_cycles(S.mg) - S.prof_cycles;
     return PIC_OK;
 }
 

@@ -81,10 +81,12 @@ def test_electron_collisions_match_oracle():
 
 def test_constant_cross_section_rate_within_3_sigma():
     rng = np.random.Generator(np.random.Philox(10))
-    n, steps = 4_000_000, 5
+    n, steps = 4_000_000, 10
     E = log_grid()
+    # nu' dt = 3.7e-3: the null-collision probability (1 - exp(-nu' dt)) nu / nu' then differs from
+    # 1 - exp(-nu dt) by (nu' - nu) dt / 2 = 0.15 %, a fifth of one standard deviation here
     sigma0 = 2e-19
-    ng, dt = 1e21, 1e-11
+    ng, dt = 1e20, 1e-11
     t = MccTables(E, ng, 300.0, workloads.ION_MASS).add(0, ELASTIC, np.full_like(E, sigma0))
     op = MccOperator(t, [Consts.me], dt, seed=SEED)
     e0 = 50.0
@@ -100,6 +102,10 @@ def test_constant_cross_section_rate_within_3_sigma():
     mean = n * steps * p
     sd = np.sqrt(n * steps * p * (1 - p))
     assert abs(hits - mean) <= 3 * sd, (hits, mean, sd)
+    # and the method's own per-step probability
+    nu_max, p_null, _ = op.query(0)
+    p_method = p_null * (ng * sigma0 * v0) / nu_max
+    assert abs(hits - n * steps * p_method) <= 3 * np.sqrt(n * steps * p_method)
     # isotropic scattering: the new polar cosine is uniform on [-1, 1]
     vz = V[2].cpu().numpy().astype(np.float64)
     vv = np.sqrt(sum(V[i].cpu().numpy().astype(np.float64) ** 2 for i in range(3)))

@@ -66,7 +66,8 @@ def test_update_E_bit_exact():
     phi = rng.normal(0, 30, m * nn)
     Ex = torch.zeros(m * nn, dtype=torch.float32, device=DEV)
     Ey = torch.zeros_like(Ex)
-    _lib.call("pic_update_E", _lib.ptr(t(phi)), _lib.ptr(Ex), _lib.ptr(Ey), m, nn, dx, dy, s())
+    PHI = t(phi)
+    _lib.call("pic_update_E", _lib.ptr(PHI), _lib.ptr(Ex), _lib.ptr(Ey), m, nn, dx, dy, s())
     ox, oy = O.update_E_f32(phi, m, nn, dx, dy)
     np.testing.assert_array_equal(Ex.cpu().numpy(), ox)
     np.testing.assert_array_equal(Ey.cpu().numpy(), oy)
@@ -83,9 +84,9 @@ def test_gather_kick_bit_exact(m, nn, n):
     vx = rng.normal(0, 1e5, n).astype(np.float32)
     vy = rng.normal(0, 1e5, n).astype(np.float32)
     kq = np.float32(-1.6e-19 / 9.10938356e-31 * 1e-11)
-    VX, VY = t(vx), t(vy)
-    _lib.call("pic_update_V", _lib.ptr(t(x)), _lib.ptr(t(y)), _lib.ptr(VX), _lib.ptr(VY), n, _lib.ptr(t(ex)),
-              _lib.ptr(t(ey)), m, nn, float(kq), s())
+    X, Y, VX, VY, EX, EY = t(x), t(y), t(vx), t(vy), t(ex), t(ey)  # keep every buffer alive during the call
+    _lib.call("pic_update_V", _lib.ptr(X), _lib.ptr(Y), _lib.ptr(VX), _lib.ptr(VY), n, _lib.ptr(EX), _lib.ptr(EY), m,
+              nn, float(kq), s())
     ovx, ovy = vx.copy(), vy.copy()
     O.kick_f32(x, y, ovx, ovy, ex, ey, kq, m, nn)
     np.testing.assert_array_equal(VX.cpu().numpy().view(np.uint32), ovx.view(np.uint32))
@@ -98,7 +99,8 @@ def test_deposit_against_oracle(m, nn, n):
     x, y = rand_particles(rng, n, m, nn)
     scale = np.float32(-1.6e-19 * 6.55e4 / 1e-8)
     rho = torch.zeros(m * nn, dtype=torch.float32, device=DEV)
-    _lib.call("pic_deposit", _lib.ptr(t(x)), _lib.ptr(t(y)), n, float(scale), _lib.ptr(rho), m, nn, s())
+    X, Y = t(x), t(y)
+    _lib.call("pic_deposit", _lib.ptr(X), _lib.ptr(Y), n, float(scale), _lib.ptr(rho), m, nn, s())
     exact, abs_sum = O.deposit_f32(x, y, scale, m, nn)
     got = rho.cpu().numpy().astype(np.float64)
     assert np.all(np.abs(got - exact) <= 2e-6 * abs_sum + 1e-30)
@@ -114,7 +116,8 @@ def test_deposit_fp32_error_against_fp64_reference_arithmetic():
     q, np2c = -1.6e-19, 1.638e5
     scale = np.float32(q * np2c / (dx * dy))
     rho = torch.zeros(m * nn, dtype=torch.float32, device=DEV)
-    _lib.call("pic_deposit", _lib.ptr(t(x)), _lib.ptr(t(y)), n, float(scale), _lib.ptr(rho), m, nn, s())
+    X, Y = t(x), t(y)
+    _lib.call("pic_deposit", _lib.ptr(X), _lib.ptr(Y), n, float(scale), _lib.ptr(rho), m, nn, s())
     ref = O.deposit_f64(x.astype(np.float64) * dx, y.astype(np.float64) * dy, q * np2c, dx, dy, m, nn,
                         floorf_quirk=False) / (dx * dy)
     _, abs_sum = O.deposit_f32(x, y, scale, m, nn)
