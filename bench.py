@@ -46,13 +46,15 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--sort-interval", type=int, default=20)
+    ap.add_argument("--sort-interval", type=int, default=40)
     ap.add_argument("--particles", type=int, default=4_000_000, help="per species")
     ap.add_argument("--no-poisson", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-collisionless", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-graph", action="store_true", help="launch every kernel from the host (profilers)")
+    ap.add_argument("--mg-no-graph", action="store_true", help="host-driven multigrid cycles (profilers)")
     return ap.parse_args()
 
 
@@ -138,6 +140,9 @@ def ncu_traffic():
     return None
 
 
+GRAPH_OPTS = {"use_graph": True, "mg_graph": True}
+
+
 def make_sim(w, rank, sort_interval, mcc=True):
     from pic_b200 import Consts, workloads
     from pic_b200.simulation import PICSimulation
@@ -148,7 +153,7 @@ def make_sim(w, rank, sort_interval, mcc=True):
                     capacity=int(w.n_i * 1.25))]
     tables = workloads.mcc_tables(w) if mcc else None
     return PICSimulation(w.nodes, w.nodes, w.dx, w.dx, w.dt, species, mask, phi_bc, tol=w.tol, max_cycles=50,
-                         sort_interval=sort_interval, mcc=tables, seed=1000 + rank, use_graph=True)
+                         sort_interval=sort_interval, mcc=tables, seed=1000 + rank, **GRAPH_OPTS)
 
 
 def gen_arrays(w, rank):
@@ -447,6 +452,8 @@ def run_reference(args, world, rank):
 
 def main():
     args = parse()
+    GRAPH_OPTS["use_graph"] = not args.no_graph
+    GRAPH_OPTS["mg_graph"] = not args.mg_no_graph
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, world, rank)

@@ -109,6 +109,8 @@ typedef struct pic_mg_options {
     int post_sweeps;  /* sweeps after prolongation (default 2) */
     double omega;     /* over-relaxation of the smoother (default 1.0) */
     int coarsest_max; /* coarsen while both node counts exceed this (default 9) */
+    int no_graph;     /* 1: launch each cycle from the host and test convergence there
+                         (for profilers that do not follow graph conditional nodes) */
 } pic_mg_options;
 
 typedef struct pic_mg_info {

@@ -325,7 +325,7 @@ def interp_ref(e, xs_e, xs_s, mask):
 
 
 def mcc_species(tables_energy, sigmas, types, thresholds, gas_density, mass, gas_mass, gas_temperature, nu_max,
-                inv_log1m_p, species, seg=4096):
+                inv_log1m_p, species, seg=256):
     """An or_mcc_species for or_mcc_candidates / or_mcc_collide; returns (struct, keep-alive list)."""
     from math import log, sqrt
 

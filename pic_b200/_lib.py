@@ -50,7 +50,7 @@ class PicError(RuntimeError):
 
 class MgOptions(C.Structure):
     _fields_ = [("precision", C.c_int), ("pre_sweeps", C.c_int), ("post_sweeps", C.c_int), ("omega", C.c_double),
-                ("coarsest_max", C.c_int)]
+                ("coarsest_max", C.c_int), ("no_graph", C.c_int)]
 
 
 class MgInfo(C.Structure):

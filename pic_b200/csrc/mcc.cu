@@ -96,19 +96,24 @@ void mcc_free(MccHost* H) {
     H->allocs.clear();
 }
 
-// One block per candidate segment of 4096 slots.
+// One block per 4096 slots (16 candidate segments, one lane each).
+constexpr int kMccBlockSlots = 4096;
+
 __global__ void __launch_bounds__(256) k_mcc_apply(MccDev M, int s, const float* __restrict__ x,
                                                    const float* __restrict__ y, float* __restrict__ vx,
                                                    float* __restrict__ vy, float* __restrict__ vz, int n,
                                                    uint32_t step, uint2 key, BirthDev B,
                                                    unsigned long long* __restrict__ ctr) {
-    __shared__ unsigned bits[kMccSegment / 32];
+    __shared__ unsigned bits[kMccBlockSlots / 32];
     const MccSpeciesDev& S = M.sp[s];
-    const long g = blockIdx.x;
-    const int b = int(g * kMccSegment), e = min(n, b + int(kMccSegment));
-    for (int q = threadIdx.x; q < int(kMccSegment / 32); q += blockDim.x) bits[q] = 0;
+    const int b = blockIdx.x * kMccBlockSlots, e = min(n, b + kMccBlockSlots);
+    for (int q = threadIdx.x; q < kMccBlockSlots / 32; q += blockDim.x) bits[q] = 0;
     __syncthreads();
-    if (threadIdx.x == 0) mcc_mark_segment(S, uint32_t(s), g, n, b, e, step, key, bits);
+    constexpr int segs = kMccBlockSlots / int(kMccSegment);
+    if (threadIdx.x < segs) {
+        const long g = long(b) / kMccSegment + threadIdx.x;
+        if (g * long(kMccSegment) < e) mcc_mark_segment(S, uint32_t(s), g, n, b, e, step, key, bits);
+    }
     __syncthreads();
     for (int l = threadIdx.x; l < e - b; l += blockDim.x) {
         if (!(bits[l >> 5] & (1u << (l & 31)))) continue;
@@ -186,7 +191,7 @@ int pic_mcc_apply(pic_mcc* m, int s, const float* d_x, const float* d_y, float* 
     BirthDev B{births->x, births->y, births->vx, births->vy, births->vz, births->species, births->count,
                births->capacity};
     const uint2 key = make_uint2(uint32_t(seed), uint32_t(seed >> 32));
-    const int blocks = div_up(n, kMccSegment);
+    const int blocks = div_up(n, kMccBlockSlots);
     k_mcc_apply<<<blocks, 256, 0, as_stream(stream)>>>(m->h.dev, s, d_x, d_y, d_vx, d_vy, d_vz, n, step, key, B,
                                                        d_counters);
     PIC_LAUNCH_CHECK();

@@ -5,8 +5,9 @@
 // Method (Vahedi & Surendra, Comput. Phys. Commun. 87 (1995) 179):
 //   nu' = n_g * max_E sigma_T(E) v(E) over the table, P_null = 1 - exp(-nu' dt).
 //   Candidates: independent Bernoulli(P_null) trials per particle, drawn as
-//   geometric gaps (floor(log u / log(1 - P_null))) over fixed segments of the
-//   slot index, so that only ~P_null*N particles touch the random stream.
+//   geometric gaps (floor(log u / log(1 - P_null))) over fixed 256-slot
+//   segments of the slot index, so that only ~P_null*N particles touch the
+//   random stream and every segment is drawn by its own lane.
 //   A candidate picks process k when u*nu' falls in the k-th slice of the
 //   cumulative n_g*sigma_k(E)*v; past the last slice it is a null collision.
 // Random numbers: Philox4x32-10 keyed by the run seed; counters
@@ -20,7 +21,7 @@
 
 namespace pic {
 
-constexpr uint32_t kMccSegment = 4096;
+constexpr uint32_t kMccSegment = 256;  // slots per candidate segment (one lane draws one segment)
 
 struct MccSpeciesDev {
     int nproc;

@@ -38,7 +38,8 @@ constexpr int kMgTile = 32;
 constexpr int kMgThreads = 256;
 constexpr int kMgMaxCoarseLevels = 8;
 constexpr int kCoarseThreads = 1024;
-constexpr long kCoarseMaxNodes = 65L * 65L;  // levels at or below this size run in the single-CTA kernel
+constexpr long kCoarseMaxNodes32 = 65L * 65L;    // FP32 levels at or below this size run in the single-CTA kernel
+constexpr long kCoarseMaxNodes64 = 65L * 65L;    // FP64 levels (twice the shared memory per node)
 
 template <class T>
 struct LevelDev {
@@ -243,14 +244,12 @@ __global__ void __launch_bounds__(kCoarseThreads) k_mg_coarse(CoarseDesc<T> D) {
         const LevelDev<T>& L = D.lv[l];
         const LevelDev<T>& C = D.lv[l + 1];
         level_sweeps(E[l], Gs[l], M[l], L, D.omega, D.pre);
-        T* r = Gs[l];
+        // restriction of the residual, evaluated on the fly: g of this level
+        // must survive for the post-smoothing on the way back up
+        const T* e = E[l];
+        const T* g = Gs[l];
+        const uint8_t* mk = M[l];
         const int nx = L.nx;
-        for (int q = threadIdx.x; q < L.nx * L.ny; q += blockDim.x) {
-            if (M[l][q]) continue;
-            const T c = E[l][q];
-            r[q] = r[q] - (L.cx * (E[l][q - 1] + E[l][q + 1] - T(2) * c) + L.cy * (E[l][q - nx] + E[l][q + nx] - T(2) * c));
-        }
-        __syncthreads();
         for (int Q = threadIdx.x; Q < C.nx * C.ny; Q += blockDim.x) {
             if (M[l + 1][Q]) {
                 Gs[l + 1][Q] = T(0);
@@ -258,7 +257,12 @@ __global__ void __launch_bounds__(kCoarseThreads) k_mg_coarse(CoarseDesc<T> D) {
             }
             const int I = Q % C.nx, J = Q / C.nx;
             const int p = 2 * J * nx + 2 * I;
-            auto rr = [&](int o) { return M[l][p + o] ? T(0) : r[p + o]; };
+            auto rr = [&](int o) {
+                const int q = p + o;
+                if (mk[q]) return T(0);
+                const T c = e[q];
+                return g[q] - (L.cx * (e[q - 1] + e[q + 1] - T(2) * c) + L.cy * (e[q - nx] + e[q + nx] - T(2) * c));
+            };
             T v = T(0.25) * rr(0);
             v += T(0.125) * (rr(-1) + rr(1) + rr(-nx) + rr(nx));
             v += T(0.0625) * (rr(-nx - 1) + rr(-nx + 1) + rr(nx - 1) + rr(nx + 1));
@@ -266,12 +270,17 @@ __global__ void __launch_bounds__(kCoarseThreads) k_mg_coarse(CoarseDesc<T> D) {
         }
         __syncthreads();
     }
-    // dense direct solve on the coarsest level
-    for (int a = threadIdx.x; a < D.nf; a += blockDim.x) {
-        const double* row = D.ainv + long(a) * D.nf;
-        double s = 0.0;
-        for (int b = 0; b < D.nf; ++b) s += row[b] * double(Gs[last][D.cidx[b]]);
-        E[last][D.cidx[a]] = T(s);
+    // dense direct solve on the coarsest level: one warp per row, lanes
+    // striding over the (coalesced) row of the inverse
+    {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        for (int a = warp; a < D.nf; a += nw) {
+            const double* row = D.ainv + long(a) * D.nf;
+            double s = 0.0;
+            for (int b = lane; b < D.nf; b += 32) s += row[b] * double(Gs[last][D.cidx[b]]);
+            s = warp_sum(s);
+            if (lane == 0) E[last][D.cidx[a]] = T(s);
+        }
     }
     __syncthreads();
     for (int l = last - 1; l >= 0; --l) {
@@ -535,6 +544,7 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
         if (opts->post_sweeps > 0) M.o.post_sweeps = opts->post_sweeps;
         if (opts->omega > 0) M.o.omega = opts->omega;
         if (opts->coarsest_max >= 3) M.o.coarsest_max = opts->coarsest_max;
+        M.o.no_graph = opts->no_graph;
     }
     auto bail = [&](int code) {
         mg_release(mg);
@@ -564,13 +574,14 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
         masks.push_back(std::move(mc));
     }
     M.L = int(nxs.size());
+    const long coarse_max = M.precision == PIC_MG_MIXED ? kCoarseMaxNodes32 : kCoarseMaxNodes64;
     M.Lc = 0;
-    while (M.Lc < M.L && long(nxs[M.Lc]) * nys[M.Lc] > kCoarseMaxNodes) ++M.Lc;
+    while (M.Lc < M.L && long(nxs[M.Lc]) * nys[M.Lc] > coarse_max) ++M.Lc;
     if (M.L - M.Lc > kMgMaxCoarseLevels) M.Lc = M.L - kMgMaxCoarseLevels;
     if (M.Lc >= M.L)
         return bail(fail(PIC_ERR_BAD_ARG,
                          "pic_mg_create: grid %dx%d does not coarsen below %ld nodes; node counts must be 2^k*c+1", nx,
-                         ny, kCoarseMaxNodes));
+                         ny, coarse_max));
     const int ncx = nxs.back(), ncy = nys.back();
     std::vector<int> idx;
     std::vector<int> where(size_t(ncx) * ncy, -1);
@@ -649,7 +660,7 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
 // One V-cycle followed by the residual check, launched on stream st.
 template <class T>
 static int launch_cycle(MgImpl& M, std::vector<LevelDev<T>>& lv, double* phi, const double* f, double tol,
-                        int max_cycles, cudaGraphConditionalHandle cond, cudaStream_t st, int& count) {
+                        int max_cycles, cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st, int& count) {
     const T omega = T(M.o.omega);
     const size_t down = tile_smem<T>(2 * M.o.pre_sweeps + 2), up = tile_smem<T>(2 * M.o.post_sweeps);
     count = 0;
@@ -681,7 +692,7 @@ static int launch_cycle(MgImpl& M, std::vector<LevelDev<T>>& lv, double* phi, co
         ++count;
     }
     k_mg_r0<T><<<M.grd0, M.blk0, 0, st>>>(phi, f, lv[0].mask, M.nx, M.ny, 1.0 / (M.dx * M.dx), 1.0 / (M.dy * M.dy),
-                                          lv[0].g, M.N, tol * tol, max_cycles, 0, cond, 1);
+                                          lv[0].g, M.N, tol * tol, max_cycles, 0, cond, use_cond);
     ++count;
     PIC_LAUNCH_CHECK();
     return PIC_OK;
@@ -713,7 +724,7 @@ static int capture_solve(MgImpl& M, std::vector<LevelDev<T>>& lv, double* phi, c
     PIC_CUDA(cudaStreamUpdateCaptureDependencies(st, &cn, 1, cudaStreamSetCaptureDependencies));
     PIC_CUDA(cudaStreamBeginCaptureToGraph(M.side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
     int count = 0;
-    const int rc = launch_cycle(M, lv, phi, f, tol, max_cycles, h, M.side, count);
+    const int rc = launch_cycle(M, lv, phi, f, tol, max_cycles, h, 1, M.side, count);
     cudaGraph_t body_out = nullptr;
     const cudaError_t ec = cudaStreamEndCapture(M.side, &body_out);
     if (rc != PIC_OK) return rc;
@@ -776,7 +787,31 @@ long long mg_total_cycles(pic_mg* mg) {
     return t;
 }
 
+int mg_read_info(MgImpl& M, pic_mg_info* info);
+
+// Host-driven solve: one launch per kernel and a synchronisation per cycle.
+template <class T>
+static int solve_eager(MgImpl& M, std::vector<LevelDev<T>>& lv, double* phi, const double* f, double tol,
+                       int max_cycles, cudaStream_t st) {
+    k_mg_r0<T><<<M.grd0, M.blk0, 0, st>>>(phi, f, lv[0].mask, M.nx, M.ny, 1.0 / (M.dx * M.dx), 1.0 / (M.dy * M.dy),
+                                          lv[0].g, M.N, tol * tol, max_cycles, 1, cudaGraphConditionalHandle{}, 0);
+    PIC_LAUNCH_CHECK();
+    pic_mg_info info{};
+    for (;;) {
+        PIC_CUDA(cudaStreamSynchronize(st));
+        PIC_TRY(mg_read_info(M, &info));
+        if (info.converged || info.cycles >= max_cycles) break;
+        int count = 0;
+        PIC_TRY(launch_cycle(M, lv, phi, f, tol, max_cycles, cudaGraphConditionalHandle{}, 0, st, count));
+        M.body_launches = count;
+    }
+    return PIC_OK;
+}
+
 int mg_launch(MgImpl& M, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
+    if (M.o.no_graph)
+        return M.precision == PIC_MG_MIXED ? solve_eager(M, M.lf, phi, f, tol, max_cycles, st)
+                                           : solve_eager(M, M.ld, phi, f, tol, max_cycles, st);
     PIC_TRY(ensure_graph(M, phi, f, tol, max_cycles));
     PIC_CUDA(cudaGraphLaunch(M.exec, st));
     return PIC_OK;
@@ -801,6 +836,7 @@ int mg_body_launches(pic_mg* mg) { return mg ? mg->m.body_launches : 0; }
 int mg_capture_into(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
     return mg_capture(mg->m, phi, f, tol, max_cycles, st);
 }
+bool mg_uses_graph(pic_mg* mg) { return !mg->m.o.no_graph; }
 int mg_launch_graph(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
     return mg_launch(mg->m, phi, f, tol, max_cycles, st);
 }

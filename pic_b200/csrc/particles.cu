@@ -124,14 +124,23 @@ __global__ void k_update_E(const double* __restrict__ phi, float* __restrict__ E
     if (E2) E2[k] = make_float2(fx, fy);
 }
 
+// rho -> f = -rho/eps0 on free nodes.  With phi_prev given, also replaces the
+// initial guess by its linear extrapolation in time, phi <- 2 phi - phi_prev,
+// on free nodes and keeps the old phi in phi_prev.
 __global__ void k_form_rhs(const float* __restrict__ rho, const uint8_t* __restrict__ dirichlet, double neg_inv_eps0,
                            double* __restrict__ f, float* __restrict__ rho_snapshot, float* __restrict__ rho_zero,
-                           long G) {
+                           double* __restrict__ phi, double* __restrict__ phi_prev, long G) {
     for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < G; k += long(gridDim.x) * blockDim.x) {
         const float r = rho[k];
-        f[k] = dirichlet[k] ? 0.0 : double(r) * neg_inv_eps0;
+        const bool dir = dirichlet[k] != 0;
+        f[k] = dir ? 0.0 : double(r) * neg_inv_eps0;
         if (rho_snapshot) rho_snapshot[k] = r;
         if (rho_zero) rho_zero[k] = 0.0f;
+        if (phi_prev && !dir) {
+            const double p = phi[k];
+            phi[k] = 2.0 * p - phi_prev[k];
+            phi_prev[k] = p;
+        }
     }
 }
 
@@ -152,8 +161,8 @@ int launch_update_E(const double* phi, float* Ex, float* Ey, float2* E2, int nx,
 }
 
 int launch_form_rhs(const float* rho, const uint8_t* dirichlet, double eps0, double* f, float* snapshot,
-                    float* zero, long G, cudaStream_t st) {
-    k_form_rhs<<<grid_blocks(G, 256), 256, 0, st>>>(rho, dirichlet, -1.0 / eps0, f, snapshot, zero, G);
+                    float* zero, double* phi, double* phi_prev, long G, cudaStream_t st) {
+    k_form_rhs<<<grid_blocks(G, 256), 256, 0, st>>>(rho, dirichlet, -1.0 / eps0, f, snapshot, zero, phi, phi_prev, G);
     PIC_LAUNCH_CHECK();
     return PIC_OK;
 }
@@ -223,7 +232,8 @@ int pic_form_rhs(const float* d_rho, const uint8_t* d_dirichlet, double eps0, do
     clear_error();
     if (!d_rho || !d_dirichlet || !d_f || nx < 2 || ny < 2 || !(eps0 > 0))
         return fail(PIC_ERR_BAD_ARG, "pic_form_rhs: bad arguments");
-    return launch_form_rhs(d_rho, d_dirichlet, eps0, d_f, nullptr, nullptr, long(nx) * ny, as_stream(stream));
+    return launch_form_rhs(d_rho, d_dirichlet, eps0, d_f, nullptr, nullptr, nullptr, nullptr, long(nx) * ny,
+                           as_stream(stream));
 }
 
 }  // extern "C"

@@ -49,31 +49,66 @@ __global__ void k_upsweep(const uint32_t* __restrict__ keys, const int* __restri
     __syncthreads();
     int b, e;
     cta_range(n_dev[0], G, blockIdx.x, b, e);
-    for (int i = b + threadIdx.x; i < e; i += blockDim.x) atomicAdd(&h[(keys[i] >> shift) & 0xff], 1);
+    const int lane = threadIdx.x & 31;
+    // keys are nearly sorted, so a warp's 32 digits are mostly equal: one
+    // shared-memory increment per distinct digit and warp
+    for (int base = b; base < e; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const int d = i < e ? int((keys[i] >> shift) & 0xff) : kRadix;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        if (d < kRadix && lane == __ffs(peers) - 1) atomicAdd(&h[d], __popc(peers));
+    }
     __syncthreads();
     for (int d = threadIdx.x; d < kRadix; d += blockDim.x) cnt[d * G + blockIdx.x] = h[d];
 }
 
-// Exclusive scan of cnt[0 .. total) in place, one CTA of 1024 threads.
-__global__ void k_scan(int* __restrict__ cnt, int total) {
-    __shared__ int part[1024];
-    const int per = (total + blockDim.x - 1) / blockDim.x;
-    const int b = threadIdx.x * per, e = min(total, b + per);
-    int s = 0;
-    for (int i = b; i < e; ++i) s += cnt[i];
-    part[threadIdx.x] = s;
+// Exclusive scan of cnt[0 .. total) in place, one CTA of 1024 threads: the
+// table is walked in coalesced tiles of 4096 counts (4 per thread), each
+// scanned by warp shuffles and carried into the next.
+__global__ void __launch_bounds__(1024) k_scan(int* __restrict__ cnt, int total) {
+    __shared__ int warp_tot[32];
+    __shared__ int carry;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    for (int o = 1; o < blockDim.x; o <<= 1) {
-        const int v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+    for (int base = 0; base < total; base += 4096) {
+        int v[4];
+        int sum = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int i = base + threadIdx.x * 4 + k;
+            v[k] = i < total ? cnt[i] : 0;
+            sum += v[k];
+        }
+        int incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) warp_tot[warp] = incl;
         __syncthreads();
-        part[threadIdx.x] += v;
+        if (warp == 0) {
+            int w = warp_tot[lane];
+            int wi = w;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, wi, o);
+                if (lane >= o) wi += t;
+            }
+            warp_tot[lane] = wi - w;  // exclusive prefix of the warp totals
+        }
         __syncthreads();
-    }
-    int run = part[threadIdx.x] - s;
-    for (int i = b; i < e; ++i) {
-        const int c = cnt[i];
-        cnt[i] = run;
-        run += c;
+        int run = carry + warp_tot[warp] + incl - sum;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int i = base + threadIdx.x * 4 + k;
+            if (i < total) cnt[i] = run;
+            run += v[k];
+        }
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = run;
+        __syncthreads();
     }
 }
 
@@ -204,7 +239,7 @@ int sorter_create(int capacity, int nx, int ny, int tile, SortImpl* S) {
     int bits = 0;
     while ((1ull << bits) <= nkeys) ++bits;
     S->passes = (bits + 7) / 8;
-    S->G = std::max(1, std::min(2 * num_sms(), div_up(capacity, kSortSub)));
+    S->G = std::max(1, std::min(num_sms(), div_up(capacity, kSortSub)));
     const size_t bytes = sizeof(uint32_t) * size_t(capacity);
     for (uint32_t** p : {&S->k0, &S->k1, &S->v0, &S->v1}) {
         PIC_CUDA(cudaMalloc(p, bytes));

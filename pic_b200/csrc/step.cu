@@ -31,18 +31,21 @@ int grid_blocks(long n, int threads);
 int launch_update_E(const double* phi, float* Ex, float* Ey, float2* E2, int nx, int ny, double dx, double dy,
                     cudaStream_t st);
 int launch_form_rhs(const float* rho, const uint8_t* dirichlet, double eps0, double* f, float* snapshot, float* zero,
-                    long G, cudaStream_t st);
+                    double* phi, double* phi_prev, long G, cudaStream_t st);
 int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const pic_mg_options* opts, pic_mg** out);
 int mg_body_launches(pic_mg* mg);
 long long mg_total_cycles(pic_mg* mg);
 int mg_capture_into(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st);
 int mg_launch_graph(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st);
 int mg_info(pic_mg* mg, pic_mg_info* info);
+bool mg_uses_graph(pic_mg* mg);
 
 constexpr int kPushThreads = 256;
-constexpr int kPushP = 7;  // particles per thread (odd: conflict-free blocked access to shared memory)
+constexpr int kPushP = 5;  // particles per thread per chunk (odd: conflict-free blocked access to shared memory)
 constexpr int kChunk = kPushThreads * kPushP;
 constexpr int kBufStride = kChunk + 8;  // floats per array per buffer: room for the 16-byte alignment window
+constexpr int kUnitMax = 8192;          // particles per work unit (one E tile staging, one charge flush)
+constexpr int kBitWords = kChunk / 32 + 2;
 constexpr int kHalo = 4;                // cells staged around a tile
 constexpr int kArraySlack = 16;         // floats allocated past each species' capacity (bulk-copy window)
 constexpr unsigned long long kWaitLimit = 1ull << 24;  // bounded mbarrier wait
@@ -136,19 +139,47 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* m, unsigned parity
     return false;
 }
 
-// Issues the bulk copies of item `it` into buffer `buf` (one thread).
-__device__ __forceinline__ void issue_item(const PushArgs& A, int it, float* buf, unsigned long long* bar) {
-    const int4 item = A.items[it];
-    const int a0 = item.z & ~3, a1 = (item.w + 3) & ~3;
+// One chunk of a work unit, as the producer thread hands it to the CTA.
+struct ChunkDesc {
+    int valid;
+    int s, tile, b, e;  // species, tile (-1: untiled), slot range of the chunk
+    int unit_e;         // end of the unit's slot range
+    int first;          // first chunk of its unit
+};
+
+// Issues the bulk copies of slots [b, e) of species s into `buf` (one thread).
+__device__ __forceinline__ void issue_chunk(const PushArgs& A, const ChunkDesc& c, float* buf,
+                                            unsigned long long* bar) {
+    const int a0 = c.b & ~3, a1 = (c.e + 3) & ~3;
     const unsigned bytes = unsigned(a1 - a0) * 4u;
-    if (bytes == 0) {
-        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-        return;
-    }
     mbar_expect_tx(bar, 5u * bytes);
-    const SpeciesState& S = A.state[item.x];
+    const SpeciesState& S = A.state[c.s];
 #pragma unroll
-    for (int c = 0; c < 5; ++c) bulk_g2s(buf + c * kBufStride, S.cur[c] + a0, bytes, bar);
+    for (int k = 0; k < 5; ++k) bulk_g2s(buf + k * kBufStride, S.cur[k] + a0, bytes, bar);
+}
+
+// The chunk after `c`: the rest of its unit, else the first chunk of a newly
+// claimed unit (one thread).
+__device__ __forceinline__ ChunkDesc next_chunk(const PushArgs& A, const ChunkDesc& c, int n_items) {
+    ChunkDesc d;
+    if (c.valid && c.e < c.unit_e) {
+        d = c;
+        d.b = c.e;
+        d.e = min(c.unit_e, c.e + kChunk);
+        d.first = 0;
+        return d;
+    }
+    const int it = atomicAdd(A.item_next, 1);
+    d.valid = it < n_items;
+    if (!d.valid) return d;
+    const int4 u = A.items[it];
+    d.s = u.x;
+    d.tile = u.y;
+    d.b = u.z;
+    d.unit_e = u.w;
+    d.e = min(u.w, u.z + kChunk);
+    d.first = 1;
+    return d;
 }
 
 // The rarely taken collision branch, kept out of line to spare registers.
@@ -171,75 +202,75 @@ __device__ __noinline__ void push_collide(const MccDev* __restrict__ M, BirthDev
     v[2] = vz;
 }
 
-__global__ void __launch_bounds__(kPushThreads, 2) k_push(PushArgs A) {
+// Candidate bits of chunk c (warp 0: zero the words, then one lane per segment).
+__device__ __forceinline__ void mark_chunk(const PushArgs& A, const ChunkDesc& c, uint32_t step, unsigned* bits,
+                                           int lane) {
+    for (int q = lane; q < kBitWords; q += 32) bits[q] = 0;
+    __syncwarp();
+    if (!c.valid || !A.do_mcc || A.mcc->sp[c.s].nproc == 0) return;
+    const long g0 = c.b / long(kMccSegment), g1 = (c.e - 1) / long(kMccSegment);
+    const int slots = A.state[c.s].count;
+    for (long g = g0 + lane; g <= g1; g += 32)
+        mcc_mark_segment(A.mcc->sp[c.s], uint32_t(c.s), g, slots, c.b, c.e, step, A.key, bits);
+    __syncwarp();
+}
+
+// Stages the E tile of a unit's tile and zeroes its charge tile.
+__device__ __forceinline__ void stage_tile(const PushArgs& A, int tile, float2* et, float* rt, int& ox, int& oy) {
+    const int RW = A.rw;
+    ox = (tile % A.tiles_x) * A.tile - kHalo;
+    oy = (tile / A.tiles_x) * A.tile - kHalo;
+    for (int q = threadIdx.x; q < RW * RW; q += kPushThreads) {
+        const int gi = ox + q % RW, gj = oy + q / RW;
+        et[q] = (gi >= 0 && gj >= 0 && gi < A.nx && gj < A.ny) ? __ldg(A.E + long(gj) * A.nx + gi)
+                                                                 : make_float2(0.f, 0.f);
+        rt[q] = 0.0f;
+    }
+}
+
+// Work units (species, tile, slot range) are claimed from an atomic counter
+// and streamed through the CTA in chunks of kChunk particles: the bulk copy
+// of chunk k+1 runs while chunk k is processed, with one CTA barrier per
+// chunk (two more at the end of each unit, around the charge-tile flush).
+// The chunk after a non-final chunk is computed by every thread; only the
+// first chunk of a new unit is published through shared memory, across the
+// unit-end barrier.
+__global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
     extern __shared__ __align__(128) unsigned char smem[];
     float* bufs = reinterpret_cast<float*>(smem);  // [2][5][kBufStride]
     const int RW = A.rw;
     float2* et = reinterpret_cast<float2*>(bufs + 2 * 5 * kBufStride);
     float* rt = reinterpret_cast<float*>(et + RW * RW);
-    unsigned* bits = reinterpret_cast<unsigned*>(rt + RW * RW);
+    unsigned* bits = reinterpret_cast<unsigned*>(rt + RW * RW);  // [2][kBitWords]
     __shared__ __align__(8) unsigned long long bar[2];
-    __shared__ int s_item[2];
+    __shared__ ChunkDesc s_ch[2];
     __shared__ unsigned s_abs, s_cand;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31;
     const uint32_t step = A.do_mcc ? *A.step : 0u;
     const int n_items = *A.n_items;
-    if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
-        fence_mbar_init();
-        const int it0 = atomicAdd(A.item_next, 1);
-        s_item[0] = it0;
-        if (it0 < n_items) issue_item(A, it0, bufs, &bar[0]);
-    }
-    __syncthreads();
-    unsigned phase[2] = {0u, 0u};
-    int cur = 0;
-    for (;;) {
-        const int it = s_item[cur];
-        if (it >= n_items) break;
+    if (tid < 32) {
         if (tid == 0) {
+            mbar_init(&bar[0], 1);
+            mbar_init(&bar[1], 1);
+            fence_mbar_init();
             s_abs = 0;
             s_cand = 0;
-            const int nx_it = atomicAdd(A.item_next, 1);
-            s_item[cur ^ 1] = nx_it;
-            if (nx_it < n_items) {
-                fence_proxy_async();
-                issue_item(A, nx_it, bufs + (cur ^ 1) * 5 * kBufStride, &bar[cur ^ 1]);
-            }
+            ChunkDesc none;
+            none.valid = 0;
+            const ChunkDesc c = next_chunk(A, none, n_items);
+            s_ch[0] = c;
+            if (c.valid) issue_chunk(A, c, bufs, &bar[0]);
         }
-        const int4 item = A.items[it];
-        const int s = item.x, tile = item.y, b = item.z, e = item.w, n = e - b;
-        const int off = b - (b & ~3);
-        float* const px = bufs + cur * 5 * kBufStride + off;
-        float* const py = px + kBufStride;
-        float* const pvx = py + kBufStride;
-        float* const pvy = pvx + kBufStride;
-        float* const pvz = pvy + kBufStride;
-        const SpeciesConst C = A.sp[s];
-        const bool tiled = tile >= 0;
-        int ox = 0, oy = 0;
-        if (tiled) {
-            ox = (tile % A.tiles_x) * A.tile - kHalo;
-            oy = (tile / A.tiles_x) * A.tile - kHalo;
-            for (int q = tid; q < RW * RW; q += kPushThreads) {
-                const int gi = ox + q % RW, gj = oy + q / RW;
-                et[q] = (gi >= 0 && gj >= 0 && gi < A.nx && gj < A.ny) ? __ldg(A.E + long(gj) * A.nx + gi)
-                                                                         : make_float2(0.f, 0.f);
-                rt[q] = 0.0f;
-            }
-        }
-        const bool mcc = A.do_mcc && A.mcc->sp[s].nproc > 0;
-        if (mcc) {
-            for (int q = tid; q < kChunk / 32 + 1; q += kPushThreads) bits[q] = 0;
-            __syncthreads();
-            if (tid < 32) {
-                const long g0 = b / long(kMccSegment), g1 = (e - 1) / long(kMccSegment);
-                const int slots = A.state[s].count;
-                for (long g = g0 + tid; g <= g1; g += 32)
-                    mcc_mark_segment(A.mcc->sp[s], uint32_t(s), g, slots, b, e, step, A.key, bits);
-            }
-        }
+        __syncwarp();
+        mark_chunk(A, s_ch[0], step, bits, lane);
+    }
+    __syncthreads();
+    ChunkDesc ch = s_ch[0];
+    unsigned phase[2] = {0u, 0u};
+    int cur = 0, ox = 0, oy = 0;
+    if (ch.valid && ch.tile >= 0) stage_tile(A, ch.tile, et, rt, ox, oy);
+    while (ch.valid) {
+        const bool tiled = ch.tile >= 0;
         const bool ok = mbar_wait(&bar[cur], phase[cur]);
         phase[cur] ^= 1u;
         if (__syncthreads_or(!ok)) {
@@ -251,10 +282,38 @@ __global__ void __launch_bounds__(kPushThreads, 2) k_push(PushArgs A) {
             __syncthreads();
             break;
         }
-
+        // the other buffer is free: hand out and prefetch the next chunk
+        if (tid < 32) {
+            if (tid == 0) {
+                const ChunkDesc nc = next_chunk(A, ch, n_items);
+                s_ch[cur ^ 1] = nc;
+                if (nc.valid) {
+                    fence_proxy_async();
+                    issue_chunk(A, nc, bufs + (cur ^ 1) * 5 * kBufStride, &bar[cur ^ 1]);
+                }
+            }
+            __syncwarp();
+            mark_chunk(A, s_ch[cur ^ 1], step, bits + (cur ^ 1) * kBitWords, lane);
+        }
+        const int s = ch.s, b = ch.b, n = ch.e - ch.b;
+        const int off = b & 3;
+        const float* const px = bufs + cur * 5 * kBufStride + off;
+        const float* const py = px + kBufStride;
+        const float* const pvx = py + kBufStride;
+        const float* const pvy = pvx + kBufStride;
+        const float* const pvz = pvy + kBufStride;
+        const unsigned* const cb = bits + cur * kBitWords;
+        const SpeciesConst C = A.sp[s];
+        float* const gx = A.state[s].cur[0] + b;
+        float* const gy = A.state[s].cur[1] + b;
+        float* const gvx = A.state[s].cur[2] + b;
+        float* const gvy = A.state[s].cur[3] + b;
+        float* const gvz = A.state[s].cur[4] + b;
+        const bool mcc = A.do_mcc && A.mcc->sp[s].nproc > 0;
         int ri0 = -1, rj0 = 0, ri1 = 0, rj1 = 0;
         float s00 = 0.f, s10 = 0.f, s01 = 0.f, s11 = 0.f;
         unsigned my_abs = 0, my_cand = 0;
+#pragma unroll 1
         for (int k = 0; k < kPushP; ++k) {
             const int l = tid * kPushP + k;
             if (l >= n) break;
@@ -278,12 +337,10 @@ __global__ void __launch_bounds__(kPushThreads, 2) k_push(PushArgs A) {
                     e01 = __ldg(A.E + long(c.j1) * A.nx + c.i0);
                     e11 = __ldg(A.E + long(c.j1) * A.nx + c.i1);
                 }
-                const float ex = cic_interp(c, e00.x, e10.x, e01.x, e11.x);
-                const float ey = cic_interp(c, e00.y, e10.y, e01.y, e11.y);
-                v[0] = __fmaf_rn(C.kq, ex, v[0]);
-                v[1] = __fmaf_rn(C.kq, ey, v[1]);
+                v[0] = __fmaf_rn(C.kq, cic_interp(c, e00.x, e10.x, e01.x, e11.x), v[0]);
+                v[1] = __fmaf_rn(C.kq, cic_interp(c, e00.y, e10.y, e01.y, e11.y), v[1]);
             }
-            if (mcc && (bits[l >> 5] & (1u << (l & 31)))) {
+            if (mcc && (cb[l >> 5] & (1u << (l & 31)))) {
                 ++my_cand;
                 push_collide(A.mcc, A.births, A.ctr, A.key, s, b + l, step, x, y, v);
             }
@@ -296,11 +353,11 @@ __global__ void __launch_bounds__(kPushThreads, 2) k_push(PushArgs A) {
                     ++my_abs;
                 }
             }
-            px[l] = x;
-            py[l] = y;
-            pvx[l] = v[0];
-            pvy[l] = v[1];
-            pvz[l] = v[2];
+            gx[l] = x;
+            gy[l] = y;
+            gvx[l] = v[0];
+            gvy[l] = v[1];
+            gvz[l] = v[2];
             if (A.do_deposit && is_live(x)) {
                 const Cic c = cic_weights(x, y, A.nx, A.ny);
                 if (c.i0 != ri0 || c.j0 != rj0) {
@@ -320,34 +377,34 @@ __global__ void __launch_bounds__(kPushThreads, 2) k_push(PushArgs A) {
         if (ri0 >= 0) flush_run(A, rt, tiled, ox, oy, ri0, rj0, ri1, rj1, C.scale, s00, s10, s01, s11);
         my_abs = __reduce_add_sync(0xffffffffu, my_abs);
         my_cand = __reduce_add_sync(0xffffffffu, my_cand);
-        if ((tid & 31) == 0) {
+        if (lane == 0) {
             if (my_abs) atomicAdd(&s_abs, my_abs);
             if (my_cand) atomicAdd(&s_cand, my_cand);
         }
-        __syncthreads();
-        float* const gx = A.state[s].cur[0] + b;
-        float* const gy = A.state[s].cur[1] + b;
-        float* const gvx = A.state[s].cur[2] + b;
-        float* const gvy = A.state[s].cur[3] + b;
-        float* const gvz = A.state[s].cur[4] + b;
-        for (int l = tid; l < n; l += kPushThreads) {
-            gx[l] = px[l];
-            gy[l] = py[l];
-            gvx[l] = pvx[l];
-            gvy[l] = pvy[l];
-            gvz[l] = pvz[l];
-        }
-        if (tiled && A.do_deposit) {
-            for (int q = tid; q < RW * RW; q += kPushThreads) {
-                const float val = rt[q];
-                if (val != 0.0f) atomicAdd(A.rho + long(oy + q / RW) * A.nx + ox + q % RW, val);
+        if (ch.e < ch.unit_e) {
+            // the unit continues: every thread derives the next chunk itself
+            ch.b = ch.e;
+            ch.e = min(ch.unit_e, ch.e + kChunk);
+            ch.first = 0;
+        } else {
+            // end of the unit: flush the charge tile and the counters
+            __syncthreads();
+            if (tiled && A.do_deposit) {
+                for (int q = tid; q < RW * RW; q += kPushThreads) {
+                    const float val = rt[q];
+                    if (val != 0.0f) atomicAdd(A.rho + long(oy + q / RW) * A.nx + ox + q % RW, val);
+                }
             }
+            if (tid == 0) {
+                if (s_abs) atomicAdd(A.ctr + kCtrAbsorbed + s, (unsigned long long)s_abs);
+                if (s_cand) atomicAdd(A.ctr + kCtrCandidates + s, (unsigned long long)s_cand);
+                s_abs = 0;
+                s_cand = 0;
+            }
+            __syncthreads();
+            ch = s_ch[cur ^ 1];
+            if (ch.valid && ch.tile >= 0) stage_tile(A, ch.tile, et, rt, ox, oy);
         }
-        if (tid == 0) {
-            if (s_abs) atomicAdd(A.ctr + kCtrAbsorbed + s, (unsigned long long)s_abs);
-            if (s_cand) atomicAdd(A.ctr + kCtrCandidates + s, (unsigned long long)s_cand);
-        }
-        __syncthreads();
         cur ^= 1;
     }
 }
@@ -400,7 +457,7 @@ __global__ void k_build_items(SpeciesState* state, int nspecies, const int* n_ti
         for (int s = 0; s < nspecies; ++s) {
             off[s] = o;
             const int u = state[s].count - state[s].sorted_end;
-            o += u > 0 ? (u + kChunk - 1) / kChunk : 0;
+            o += u > 0 ? (u + kUnitMax - 1) / kUnitMax : 0;
         }
         off[nspecies] = o;
         *n_items = o;
@@ -412,8 +469,8 @@ __global__ void k_build_items(SpeciesState* state, int nspecies, const int* n_ti
     for (int s = 0; s < nspecies; ++s) {
         const int b0 = state[s].sorted_end, e0 = state[s].count;
         for (int c = threadIdx.x; c < off[s + 1] - off[s]; c += blockDim.x) {
-            const int b = b0 + c * kChunk;
-            items[off[s] + c] = make_int4(s, -1, b, min(e0, b + kChunk));
+            const int b = b0 + c * kUnitMax;
+            items[off[s] + c] = make_int4(s, -1, b, min(e0, b + kUnitMax));
         }
     }
 }
@@ -429,7 +486,7 @@ __global__ void k_tile_items(const int* __restrict__ tile_start, int ntiles, int
     for (int q = b; q < e; ++q) {
         const int s = q / ntiles, t = q % ntiles;
         const int* ts = tile_start + s * (ntiles + 1);
-        sum += (ts[t + 1] - ts[t] + kChunk - 1) / kChunk;
+        sum += (ts[t + 1] - ts[t] + kUnitMax - 1) / kUnitMax;
     }
     part[threadIdx.x] = sum;
     __syncthreads();
@@ -443,7 +500,7 @@ __global__ void k_tile_items(const int* __restrict__ tile_start, int ntiles, int
     for (int q = b; q < e; ++q) {
         const int s = q / ntiles, t = q % ntiles;
         const int* ts = tile_start + s * (ntiles + 1);
-        for (int c = ts[t]; c < ts[t + 1]; c += kChunk) items[w++] = make_int4(s, t, c, min(ts[t + 1], c + kChunk));
+        for (int c = ts[t]; c < ts[t + 1]; c += kUnitMax) items[w++] = make_int4(s, t, c, min(ts[t + 1], c + kUnitMax));
     }
     if (threadIdx.x == blockDim.x - 1) *n_tiled = part[threadIdx.x];
 }
@@ -525,7 +582,8 @@ struct SimImpl {
     int* error = nullptr;
     float2* E2 = nullptr;
     float *Ex = nullptr, *Ey = nullptr, *rho_acc = nullptr, *rho_out = nullptr;
-    double *phi = nullptr, *f = nullptr;
+    double *phi = nullptr, *f = nullptr, *phi_prev = nullptr;
+    bool have_prev = false;  // phi_prev holds the potential of the previous solve
     uint8_t* dirichlet = nullptr;
     int push_grid = 0;
     size_t push_smem = 0;
@@ -639,12 +697,18 @@ static int particle_pass(SimImpl& S, cudaStream_t st, int kick, int mcc, int dri
 static int field_solve(SimImpl& S, cudaStream_t st, bool capturing) {
     {
         PhaseTimer t(S, PIC_PHASE_RHS, st);
-        PIC_TRY(launch_form_rhs(S.rho_acc, S.dirichlet, S.d.eps0, S.f, S.rho_out, S.rho_acc, S.G, st));
+        // from the second solve on, the guess is extrapolated from the last two potentials
+        PIC_TRY(launch_form_rhs(S.rho_acc, S.dirichlet, S.d.eps0, S.f, S.rho_out, S.rho_acc, S.phi,
+                                S.have_prev ? S.phi_prev : nullptr, S.G, st));
     }
     {
         PhaseTimer t(S, PIC_PHASE_SOLVE, st);
         if (capturing) PIC_TRY(mg_capture_into(S.mg, S.phi, S.f, S.d.tol, S.d.max_cycles, st));
         else PIC_TRY(mg_launch_graph(S.mg, S.phi, S.f, S.d.tol, S.d.max_cycles, st));
+    }
+    if (!S.have_prev) {
+        PIC_CUDA(cudaMemcpyAsync(S.phi_prev, S.phi, sizeof(double) * S.G, cudaMemcpyDeviceToDevice, st));
+        S.have_prev = true;
     }
     {
         PhaseTimer t(S, PIC_PHASE_EFIELD, st);
@@ -751,7 +815,7 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
     PIC_CUDA(cudaMemcpy(S.d_state, S.h_state, sizeof(SpeciesState) * S.ns, cudaMemcpyHostToDevice));
     // work items
     S.item_cap = 4;
-    for (int s = 0; s < S.ns; ++s) S.item_cap += S.sorter.ntiles + 2 * (d->species[s].capacity / kChunk + 2);
+    for (int s = 0; s < S.ns; ++s) S.item_cap += S.sorter.ntiles + 2 * (d->species[s].capacity / kUnitMax + 2);
     PIC_TRY(dalloc(S, &S.items, size_t(S.item_cap)));
     PIC_TRY(dalloc(S, &S.n_items, 1));
     PIC_TRY(dalloc(S, &S.item_next, 1));
@@ -778,6 +842,7 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
     PIC_TRY(dalloc(S, &S.rho_acc, size_t(S.G)));
     PIC_TRY(dalloc(S, &S.rho_out, size_t(S.G)));
     PIC_TRY(dalloc(S, &S.phi, size_t(S.G)));
+    PIC_TRY(dalloc(S, &S.phi_prev, size_t(S.G)));
     PIC_TRY(dalloc(S, &S.f, size_t(S.G)));
     PIC_TRY(dalloc(S, &S.dirichlet, size_t(S.G)));
     std::vector<uint8_t> mask(d->h_dirichlet, d->h_dirichlet + S.G);
@@ -791,7 +856,7 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
     }
     // launch shape of the particle pass
     S.push_smem = sizeof(float) * 2 * 5 * kBufStride + size_t(S.rw) * S.rw * (sizeof(float2) + sizeof(float)) +
-                  sizeof(unsigned) * (kChunk / 32 + 2);
+                  sizeof(unsigned) * 2 * kBitWords;
     PIC_CUDA(cudaFuncSetAttribute(k_push, cudaFuncAttributeMaxDynamicSharedMemorySize, int(S.push_smem)));
     int per_sm = 0;
     PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_push, kPushThreads, S.push_smem));
@@ -899,7 +964,7 @@ int pic_sim_step(pic_sim* sim, int n_steps, void* stream) {
     cudaStream_t st = as_stream(stream);
     for (int i = 0; i < n_steps; ++i) {
         const bool sort = S.d.sort_interval > 0 && S.steps % S.d.sort_interval == 0;
-        if (S.d.use_graph && S.kick_pending && !S.profiling) {
+        if (S.d.use_graph && S.kick_pending && !S.profiling && mg_uses_graph(S.mg)) {
             cudaGraphExec_t& g = sort ? S.g_sort_step : S.g_step;
             if (!g) PIC_TRY(capture_step(S, sort, &g));
             PIC_CUDA(cudaGraphLaunch(g, st));

@@ -40,15 +40,17 @@ def manufactured(n):
 
 
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
-@pytest.mark.parametrize("n", [129, 257])
+@pytest.mark.parametrize("n", [17, 33, 65, 129, 257])
 def test_manufactured_solution(precision, n):
+    """17..65 nodes run entirely in the single-CTA coarse kernel; 129 and 257 use the tiled kernels too."""
     h, f, exact = manufactured(n)
     mask = edge_mask(n)
     f[mask == 1] = 0.0
     mg = MultigridSolver(mask, n, n, h, precision=precision)
     phi = torch.zeros(n * n, dtype=torch.float64, device=DEV)
     phi, (cycles, rel) = mg.solve(phi, torch.as_tensor(f, device=DEV), tol=1e-12, max_cycles=40)
-    assert rel < 1e-12 and cycles <= 20
+    # a V(2,2) cycle reduces the residual ~10x; from phi = 0 to 1e-12 takes about 12 cycles
+    assert rel < 1e-12 and cycles <= 14, (cycles, rel)
     np.testing.assert_allclose(phi.cpu().numpy(), exact, rtol=0, atol=1e-10 * np.abs(exact).max())
 
 
