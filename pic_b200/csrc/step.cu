@@ -57,7 +57,7 @@ struct SpeciesState {
     int count;       // slots in use
     int sorted_end;  // slots covered by tile items
     int capacity;
-    int pad;
+    int stride;      // cur[k] = cur[0] + k * stride (the five arrays share one allocation)
 };
 
 struct SpeciesConst {
@@ -80,6 +80,9 @@ struct PushArgs {
     uint2 key;
     const uint32_t* step;
     BirthDev births;
+    int2* cand;       // collision candidates (species, slot), processed by k_collide after the pass
+    int* cand_count;
+    int cand_cap;
     unsigned long long* ctr;
     int* error;  // set when a bounded wait gives up
 };
@@ -152,10 +155,11 @@ __device__ __forceinline__ void issue_chunk(const PushArgs& A, const ChunkDesc& 
                                             unsigned long long* bar) {
     const int a0 = c.b & ~3, a1 = (c.e + 3) & ~3;
     const unsigned bytes = unsigned(a1 - a0) * 4u;
-    mbar_expect_tx(bar, 5u * bytes);
+    // x, y, vx, vy: vz is touched only by collision candidates (k_collide)
+    mbar_expect_tx(bar, 4u * bytes);
     const SpeciesState& S = A.state[c.s];
 #pragma unroll
-    for (int k = 0; k < 5; ++k) bulk_g2s(buf + k * kBufStride, S.cur[k] + a0, bytes, bar);
+    for (int k = 0; k < 4; ++k) bulk_g2s(buf + k * kBufStride, S.cur[k] + a0, bytes, bar);
 }
 
 // The chunk after `c`: the rest of its unit, else the first chunk of a newly
@@ -182,37 +186,20 @@ __device__ __forceinline__ ChunkDesc next_chunk(const PushArgs& A, const ChunkDe
     return d;
 }
 
-// The rarely taken collision branch, kept out of line to spare registers.
-__device__ __noinline__ void push_collide(const MccDev* __restrict__ M, BirthDev B, unsigned long long* ctr, uint2 key,
-                                          int s, int slot, uint32_t step, float x, float y, float* v) {
-    float vx = v[0], vy = v[1], vz = v[2];
-    const MccOutcome o = mcc_collide(*M, M->sp[s], uint32_t(s), uint32_t(slot), step, key, vx, vy, vz);
-    if (o.overflow) atomicAdd(ctr + kCtrOverflow, 1ull);
-    if (o.proc >= 0) {
-        atomicAdd(ctr + kCtrCollisions + s * PIC_MAX_PROCESSES + o.proc, 1ull);
-        if (o.born) {
-            const MccSpeciesDev& S = M->sp[s];
-            const bool ok_e = birth_push(B, S.born_e, x, y, o.be[0], o.be[1], o.be[2]);
-            const bool ok_i = birth_push(B, S.born_i, x, y, o.bi[0], o.bi[1], o.bi[2]);
-            if (!ok_e || !ok_i) atomicAdd(ctr + kCtrDropped, 1ull);
-        }
-    }
-    v[0] = vx;
-    v[1] = vy;
-    v[2] = vz;
+// Candidate bits of chunk c: segment g0 + t goes to the calling thread t
+// (t < nthreads).  The bit words start out zero: every candidate bit is
+// cleared again by the thread that consumes it.
+__device__ __noinline__ void mark_segments(const MccDev* __restrict__ M, const SpeciesState* __restrict__ state, int s,
+                                           int b, int e, uint32_t step, uint2 key, unsigned* bits, int t, int nthreads) {
+    const long g0 = b / long(kMccSegment), g1 = (e - 1) / long(kMccSegment);
+    const int slots = state[s].count;
+    for (long g = g0 + t; g <= g1; g += nthreads) mcc_mark_segment(M->sp[s], uint32_t(s), g, slots, b, e, step, key, bits);
 }
 
-// Candidate bits of chunk c (warp 0: zero the words, then one lane per segment).
-__device__ __forceinline__ void mark_chunk(const PushArgs& A, const ChunkDesc& c, uint32_t step, unsigned* bits,
-                                           int lane) {
-    for (int q = lane; q < kBitWords; q += 32) bits[q] = 0;
-    __syncwarp();
+__device__ __forceinline__ void mark_chunk(const PushArgs& A, const ChunkDesc& c, uint32_t step, unsigned* bits, int t,
+                                           int nthreads) {
     if (!c.valid || !A.do_mcc || A.mcc->sp[c.s].nproc == 0) return;
-    const long g0 = c.b / long(kMccSegment), g1 = (c.e - 1) / long(kMccSegment);
-    const int slots = A.state[c.s].count;
-    for (long g = g0 + lane; g <= g1; g += 32)
-        mcc_mark_segment(A.mcc->sp[c.s], uint32_t(c.s), g, slots, c.b, c.e, step, A.key, bits);
-    __syncwarp();
+    mark_segments(A.mcc, A.state, c.s, c.b, c.e, step, A.key, bits, t, nthreads);
 }
 
 // Stages the E tile of a unit's tile and zeroes its charge tile.
@@ -237,9 +224,9 @@ __device__ __forceinline__ void stage_tile(const PushArgs& A, int tile, float2* 
 // unit-end barrier.
 __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
     extern __shared__ __align__(128) unsigned char smem[];
-    float* bufs = reinterpret_cast<float*>(smem);  // [2][5][kBufStride]
+    float* bufs = reinterpret_cast<float*>(smem);  // [2][4][kBufStride]
     const int RW = A.rw;
-    float2* et = reinterpret_cast<float2*>(bufs + 2 * 5 * kBufStride);
+    float2* et = reinterpret_cast<float2*>(bufs + 2 * 4 * kBufStride);
     float* rt = reinterpret_cast<float*>(et + RW * RW);
     unsigned* bits = reinterpret_cast<unsigned*>(rt + RW * RW);  // [2][kBitWords]
     __shared__ __align__(8) unsigned long long bar[2];
@@ -248,6 +235,8 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
     const int tid = threadIdx.x, lane = tid & 31;
     const uint32_t step = A.do_mcc ? *A.step : 0u;
     const int n_items = *A.n_items;
+    for (int q = tid; q < 2 * kBitWords; q += kPushThreads) bits[q] = 0;
+    __syncthreads();
     if (tid < 32) {
         if (tid == 0) {
             mbar_init(&bar[0], 1);
@@ -262,7 +251,7 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
             if (c.valid) issue_chunk(A, c, bufs, &bar[0]);
         }
         __syncwarp();
-        mark_chunk(A, s_ch[0], step, bits, lane);
+        mark_chunk(A, s_ch[0], step, bits, lane, 32);
     }
     __syncthreads();
     ChunkDesc ch = s_ch[0];
@@ -282,44 +271,57 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
             __syncthreads();
             break;
         }
-        // the other buffer is free: hand out and prefetch the next chunk
-        if (tid < 32) {
-            if (tid == 0) {
-                const ChunkDesc nc = next_chunk(A, ch, n_items);
-                s_ch[cur ^ 1] = nc;
-                if (nc.valid) {
-                    fence_proxy_async();
-                    issue_chunk(A, nc, bufs + (cur ^ 1) * 5 * kBufStride, &bar[cur ^ 1]);
-                }
+        // the other buffer is free: hand out and prefetch the next chunk, and
+        // mark its collision candidates (spread over the warps when the chunk
+        // continues this unit, by warp 0 when it opens a new one)
+        const bool continues = ch.e < ch.unit_e;
+        if (tid == 0) {
+            const ChunkDesc nc = next_chunk(A, ch, n_items);
+            s_ch[cur ^ 1] = nc;
+            if (nc.valid) {
+                fence_proxy_async();
+                issue_chunk(A, nc, bufs + (cur ^ 1) * 4 * kBufStride, &bar[cur ^ 1]);
             }
+        }
+        if (continues) {
+            if (lane == 0) {
+                ChunkDesc nc = ch;
+                nc.b = ch.e;
+                nc.e = min(ch.unit_e, ch.e + kChunk);
+                mark_chunk(A, nc, step, bits + (cur ^ 1) * kBitWords, tid >> 5, kPushThreads / 32);
+            }
+        } else if (tid < 32) {
             __syncwarp();
-            mark_chunk(A, s_ch[cur ^ 1], step, bits + (cur ^ 1) * kBitWords, lane);
+            mark_chunk(A, s_ch[cur ^ 1], step, bits + (cur ^ 1) * kBitWords, lane, 32);
         }
         const int s = ch.s, b = ch.b, n = ch.e - ch.b;
         const int off = b & 3;
-        const float* const px = bufs + cur * 5 * kBufStride + off;
+        const float* const px = bufs + cur * 4 * kBufStride + off;
         const float* const py = px + kBufStride;
         const float* const pvx = py + kBufStride;
         const float* const pvy = pvx + kBufStride;
-        const float* const pvz = pvy + kBufStride;
-        const unsigned* const cb = bits + cur * kBitWords;
+        const unsigned* const cb = bits + cur * kBitWords;  // read-only view of this chunk's candidate bits
         const SpeciesConst C = A.sp[s];
-        float* const gx = A.state[s].cur[0] + b;
-        float* const gy = A.state[s].cur[1] + b;
-        float* const gvx = A.state[s].cur[2] + b;
-        float* const gvy = A.state[s].cur[3] + b;
-        float* const gvz = A.state[s].cur[4] + b;
+        float* const g = A.state[s].cur[0] + b;
+        const int gs = A.state[s].stride;
         const bool mcc = A.do_mcc && A.mcc->sp[s].nproc > 0;
-        int ri0 = -1, rj0 = 0, ri1 = 0, rj1 = 0;
-        float s00 = 0.f, s10 = 0.f, s01 = 0.f, s11 = 0.f;
+        unsigned* const cbw = bits + cur * kBitWords;
         unsigned my_abs = 0, my_cand = 0;
 #pragma unroll 1
         for (int k = 0; k < kPushP; ++k) {
             const int l = tid * kPushP + k;
             if (l >= n) break;
+            bool candidate = false;
+            if (mcc) {
+                const unsigned bit = 1u << (l & 31);
+                if (cb[l >> 5] & bit) {
+                    candidate = true;
+                    atomicAnd(cbw + (l >> 5), ~bit);  // leave the word zero for the next chunk
+                }
+            }
             float x = px[l], y = py[l];
             if (!is_live(x)) continue;
-            float v[3] = {pvx[l], pvy[l], pvz[l]};
+            float vx = pvx[l], vy = pvy[l];
             if (A.do_kick) {
                 const Cic c = cic_weights(x, y, A.nx, A.ny);
                 const int li = c.i0 - ox, lj = c.j0 - oy;
@@ -337,44 +339,54 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
                     e01 = __ldg(A.E + long(c.j1) * A.nx + c.i0);
                     e11 = __ldg(A.E + long(c.j1) * A.nx + c.i1);
                 }
-                v[0] = __fmaf_rn(C.kq, cic_interp(c, e00.x, e10.x, e01.x, e11.x), v[0]);
-                v[1] = __fmaf_rn(C.kq, cic_interp(c, e00.y, e10.y, e01.y, e11.y), v[1]);
+                vx = __fmaf_rn(C.kq, cic_interp(c, e00.x, e10.x, e01.x, e11.x), vx);
+                vy = __fmaf_rn(C.kq, cic_interp(c, e00.y, e10.y, e01.y, e11.y), vy);
             }
-            if (mcc && (cb[l >> 5] & (1u << (l & 31)))) {
+            if (candidate) {
+                // kicked but not moved: k_collide finishes it after this pass
                 ++my_cand;
-                push_collide(A.mcc, A.births, A.ctr, A.key, s, b + l, step, x, y, v);
+                const int slot = atomicAdd(A.cand_count, 1);
+                if (slot < A.cand_cap) {
+                    A.cand[slot] = make_int2(s, b + l);
+                    g[2 * gs + l] = vx;
+                    g[3 * gs + l] = vy;
+                    continue;
+                }
+                atomicAdd(A.ctr + kCtrCandOverflow, 1ull);
             }
             if (A.do_drift) {
-                x = __fmaf_rn(v[0], C.dtdx, x);
-                y = __fmaf_rn(v[1], C.dtdy, y);
+                x = __fmaf_rn(vx, C.dtdx, x);
+                y = __fmaf_rn(vy, C.dtdy, y);
                 if (!(x >= 0.0f && x <= float(A.nx - 1) && y >= 0.0f && y <= float(A.ny - 1))) {
                     x = __int_as_float(0x7fc00000);
                     y = x;
                     ++my_abs;
                 }
             }
-            gx[l] = x;
-            gy[l] = y;
-            gvx[l] = v[0];
-            gvy[l] = v[1];
-            gvz[l] = v[2];
+            g[l] = x;
+            g[gs + l] = y;
+            g[2 * gs + l] = vx;
+            g[3 * gs + l] = vy;
             if (A.do_deposit && is_live(x)) {
                 const Cic c = cic_weights(x, y, A.nx, A.ny);
-                if (c.i0 != ri0 || c.j0 != rj0) {
-                    if (ri0 >= 0) flush_run(A, rt, tiled, ox, oy, ri0, rj0, ri1, rj1, C.scale, s00, s10, s01, s11);
-                    ri0 = c.i0;
-                    rj0 = c.j0;
-                    ri1 = c.i1;
-                    rj1 = c.j1;
-                    s00 = s10 = s01 = s11 = 0.f;
+                const int li = c.i0 - ox, lj = c.j0 - oy;
+                const float w00 = __fmul_rn(C.scale, c.w00), w10 = __fmul_rn(C.scale, c.w10);
+                const float w01 = __fmul_rn(C.scale, c.w01), w11 = __fmul_rn(C.scale, c.w11);
+                if (tiled && li >= 0 && lj >= 0 && li + 1 < RW && lj + 1 < RW) {
+                    const int q = lj * RW + li;
+                    const int dq = c.i1 - c.i0, dr = (c.j1 - c.j0) * RW;
+                    atomicAdd(rt + q, w00);
+                    atomicAdd(rt + q + dq, w10);
+                    atomicAdd(rt + q + dr, w01);
+                    atomicAdd(rt + q + dr + dq, w11);
+                } else {
+                    atomicAdd(A.rho + long(c.j0) * A.nx + c.i0, w00);
+                    atomicAdd(A.rho + long(c.j0) * A.nx + c.i1, w10);
+                    atomicAdd(A.rho + long(c.j1) * A.nx + c.i0, w01);
+                    atomicAdd(A.rho + long(c.j1) * A.nx + c.i1, w11);
                 }
-                s00 += c.w00;
-                s10 += c.w10;
-                s01 += c.w01;
-                s11 += c.w11;
             }
         }
-        if (ri0 >= 0) flush_run(A, rt, tiled, ox, oy, ri0, rj0, ri1, rj1, C.scale, s00, s10, s01, s11);
         my_abs = __reduce_add_sync(0xffffffffu, my_abs);
         my_cand = __reduce_add_sync(0xffffffffu, my_cand);
         if (lane == 0) {
@@ -406,6 +418,53 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
             if (ch.valid && ch.tile >= 0) stage_tile(A, ch.tile, et, rt, ox, oy);
         }
         cur ^= 1;
+    }
+}
+
+// The collision candidates of the pass: MCC, then the drift, absorption and
+// deposit the pass skipped for them (global atomics; a few per thousand).
+__global__ void __launch_bounds__(128) k_collide(PushArgs A) {
+    const int nc = min(*A.cand_count, A.cand_cap);
+    const uint32_t step = *A.step;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nc; i += gridDim.x * blockDim.x) {
+        const int2 c = A.cand[i];
+        const int s = c.x, p = c.y;
+        const SpeciesState& S = A.state[s];
+        const SpeciesConst C = A.sp[s];
+        float x = S.cur[0][p], y = S.cur[1][p];
+        float vx = S.cur[2][p], vy = S.cur[3][p], vz = S.cur[4][p];
+        const MccOutcome o = mcc_collide(*A.mcc, A.mcc->sp[s], uint32_t(s), uint32_t(p), step, A.key, vx, vy, vz);
+        if (o.overflow) atomicAdd(A.ctr + kCtrOverflow, 1ull);
+        if (o.proc >= 0) {
+            atomicAdd(A.ctr + kCtrCollisions + s * PIC_MAX_PROCESSES + o.proc, 1ull);
+            if (o.born) {
+                const MccSpeciesDev& M = A.mcc->sp[s];
+                const bool ok_e = birth_push(A.births, M.born_e, x, y, o.be[0], o.be[1], o.be[2]);
+                const bool ok_i = birth_push(A.births, M.born_i, x, y, o.bi[0], o.bi[1], o.bi[2]);
+                if (!ok_e || !ok_i) atomicAdd(A.ctr + kCtrDropped, 1ull);
+            }
+        }
+        if (A.do_drift) {
+            x = __fmaf_rn(vx, C.dtdx, x);
+            y = __fmaf_rn(vy, C.dtdy, y);
+            if (!(x >= 0.0f && x <= float(A.nx - 1) && y >= 0.0f && y <= float(A.ny - 1))) {
+                x = __int_as_float(0x7fc00000);
+                y = x;
+                atomicAdd(A.ctr + kCtrAbsorbed + s, 1ull);
+            }
+        }
+        S.cur[0][p] = x;
+        S.cur[1][p] = y;
+        S.cur[2][p] = vx;
+        S.cur[3][p] = vy;
+        S.cur[4][p] = vz;
+        if (A.do_deposit && is_live(x)) {
+            const Cic w = cic_weights(x, y, A.nx, A.ny);
+            atomicAdd(A.rho + long(w.j0) * A.nx + w.i0, __fmul_rn(C.scale, w.w00));
+            atomicAdd(A.rho + long(w.j0) * A.nx + w.i1, __fmul_rn(C.scale, w.w10));
+            atomicAdd(A.rho + long(w.j1) * A.nx + w.i0, __fmul_rn(C.scale, w.w01));
+            atomicAdd(A.rho + long(w.j1) * A.nx + w.i1, __fmul_rn(C.scale, w.w11));
+        }
     }
 }
 
@@ -450,7 +509,7 @@ __global__ void k_merge_births(PushArgs A) {
 // Per step: untiled items for slots past the last sort, item counter reset,
 // RNG step advance, birth buffer reset.
 __global__ void k_build_items(SpeciesState* state, int nspecies, const int* n_tiled, int4* items, int* n_items,
-                              int* item_next, uint32_t* step, int* birth_count, int advance_step) {
+                              int* item_next, uint32_t* step, int* birth_count, int* cand_count, int advance_step) {
     __shared__ int off[PIC_MAX_SPECIES + 1];
     if (threadIdx.x == 0) {
         int o = *n_tiled;
@@ -463,6 +522,7 @@ __global__ void k_build_items(SpeciesState* state, int nspecies, const int* n_ti
         *n_items = o;
         *item_next = 0;
         *birth_count = 0;
+        *cand_count = 0;
         if (advance_step) *step += 1u;
     }
     __syncthreads();
@@ -568,6 +628,9 @@ struct SimImpl {
     MccHost mcc;
     bool have_mcc = false;
     MccDev* mcc_dev = nullptr;  // device copy of mcc.dev
+    int2* cand = nullptr;       // collision candidates of one pass
+    int* cand_count = nullptr;
+    int cand_cap = 0;
     std::vector<void*> allocs;
     SpeciesState* d_state = nullptr;
     SpeciesState h_state[PIC_MAX_SPECIES]{};
@@ -668,6 +731,9 @@ static PushArgs push_args(SimImpl& S, int kick, int mcc, int drift, int deposit,
     A.key = make_uint2(uint32_t(S.d.seed), uint32_t(S.d.seed >> 32));
     A.step = S.step_ctr;
     A.births = S.births;
+    A.cand = S.cand;
+    A.cand_count = S.cand_count;
+    A.cand_cap = S.cand_cap;
     A.ctr = S.ctr;
     A.error = S.error;
     return A;
@@ -678,7 +744,7 @@ static int particle_pass(SimImpl& S, cudaStream_t st, int kick, int mcc, int dri
     {
         PhaseTimer t(S, PIC_PHASE_BUILD, st);
         k_build_items<<<1, 256, 0, st>>>(S.d_state, S.ns, S.n_tiled, S.items, S.n_items, S.item_next, S.step_ctr,
-                                         S.births.count, advance_step);
+                                         S.births.count, S.cand_count, advance_step);
     }
     const PushArgs A = push_args(S, kick, mcc, drift, deposit, kick_factor);
     {
@@ -687,6 +753,10 @@ static int particle_pass(SimImpl& S, cudaStream_t st, int kick, int mcc, int dri
     }
     {
         PhaseTimer t(S, PIC_PHASE_MERGE, st);
+        if (A.do_mcc) {
+            k_collide<<<64, 128, 0, st>>>(A);
+            S.launches += 1;
+        }
         k_merge_births<<<64, 256, 0, st>>>(A);
     }
     S.launches += 3;
@@ -798,10 +868,17 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
     for (int s = 0; s < S.ns; ++s) {
         const pic_species_desc& sp = d->species[s];
         SpeciesState& H = S.h_state[s];
+        // one allocation per buffer set; each array padded to a multiple of 4
+        // floats so that every array starts 16-byte aligned
+        const int stride = ((sp.capacity + kArraySlack + 3) / 4) * 4;
+        float *cur = nullptr, *alt = nullptr;
+        PIC_TRY(dalloc(S, &cur, size_t(stride) * 5));
+        PIC_TRY(dalloc(S, &alt, size_t(stride) * 5));
         for (int c = 0; c < 5; ++c) {
-            PIC_TRY(dalloc(S, &H.cur[c], size_t(sp.capacity) + kArraySlack));
-            PIC_TRY(dalloc(S, &H.alt[c], size_t(sp.capacity) + kArraySlack));
+            H.cur[c] = cur + size_t(c) * stride;
+            H.alt[c] = alt + size_t(c) * stride;
         }
+        H.stride = stride;
         H.count = 0;
         H.sorted_end = 0;
         H.capacity = sp.capacity;
@@ -833,6 +910,13 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
     PIC_TRY(dalloc(S, &S.births.vz, size_t(bcap)));
     PIC_TRY(dalloc(S, &S.births.species, size_t(bcap)));
     PIC_TRY(dalloc(S, &S.births.count, 1));
+    // candidates per pass: P_null N on average (binomial); eight times the mean plus a margin
+    double expect = 0.0;
+    if (S.have_mcc)
+        for (int s = 0; s < S.ns; ++s) expect += S.mcc.p_null[s] * d->species[s].capacity;
+    S.cand_cap = int(std::min(2.0e9, 8.0 * expect + 65536.0));
+    PIC_TRY(dalloc(S, &S.cand, size_t(S.cand_cap)));
+    PIC_TRY(dalloc(S, &S.cand_count, 1));
     PIC_TRY(dalloc(S, &S.ctr, size_t(kCtrCount)));
     PIC_TRY(dalloc(S, &S.error, 1));
     // fields
@@ -855,7 +939,7 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
         PIC_CUDA(cudaMemcpy(S.phi, phi0.data(), sizeof(double) * S.G, cudaMemcpyHostToDevice));
     }
     // launch shape of the particle pass
-    S.push_smem = sizeof(float) * 2 * 5 * kBufStride + size_t(S.rw) * S.rw * (sizeof(float2) + sizeof(float)) +
+    S.push_smem = sizeof(float) * 2 * 4 * kBufStride + size_t(S.rw) * S.rw * (sizeof(float2) + sizeof(float)) +
                   sizeof(unsigned) * 2 * kBitWords;
     PIC_CUDA(cudaFuncSetAttribute(k_push, cudaFuncAttributeMaxDynamicSharedMemorySize, int(S.push_smem)));
     int per_sm = 0;
@@ -968,7 +1052,7 @@ int pic_sim_step(pic_sim* sim, int n_steps, void* stream) {
             cudaGraphExec_t& g = sort ? S.g_sort_step : S.g_step;
             if (!g) PIC_TRY(capture_step(S, sort, &g));
             PIC_CUDA(cudaGraphLaunch(g, st));
-            S.launches += 3 + 2 + (sort ? 1 + (long long)S.ns * (5 + 3 * S.sorter.passes) : 0);
+            S.launches += 3 + (S.have_mcc ? 1 : 0) + 2 + (sort ? 1 + (long long)S.ns * (5 + 3 * S.sorter.passes) : 0);
             S.solves += 1;
         } else {
             if (sort) PIC_TRY(sort_all(S, st));
