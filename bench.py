@@ -38,6 +38,8 @@ sys.path.insert(0, ROOT)
 METRIC = "particle-steps/s/GPU at 512², 8M ptcl; mixed vs FP64 multigrid at 1e-10 residual"
 UNIT = "particle-steps/s"
 FALLBACK_HBM_GBS = 6650.0
+BYTES_PER_PARTICLE = 32.0  # x, y, vx, vy float32, read and written by the fused pass
+BYTES_PER_NODE = 12.0      # E (float2) read, charge (float) written
 
 
 def parse():
@@ -225,14 +227,14 @@ def run_ours(args, world, rank, local):
     value = float(work.item()) / (ms_max / 1e3)
     counters = sim.counters()
 
-    # roofline of the fused particle kernel: 16 B read + 16 B written per
-    # particle (x, y, vx, vy), + 8 B (vz read and written) for species with
-    # collisions -- here both -- plus the E tile read (8 B/node) and the
-    # charge flush (4 B/node) per step.
+    # roofline of the fused particle kernel: x, y, vx, vy read and written
+    # (32 B per particle; vz is touched only by the collision candidates,
+    # a few per thousand, in their own pass) plus the E field read
+    # (8 B per node) and the charge written (4 B per node) once per step.
     G = w.nodes * w.nodes
     push = prof["push"]
     push_ms = push["ms"] / max(1, push["count"])
-    bytes_per_launch = 0.5 * (n0 + n1) * 40.0 + G * 12.0
+    bytes_per_launch = 0.5 * (n0 + n1) * BYTES_PER_PARTICLE + G * BYTES_PER_NODE
     achieved = bytes_per_launch / (push_ms / 1e3) / 1e9
     peak, peak_kind = peak_hbm()
     traffic = ncu_traffic()
@@ -277,8 +279,8 @@ def run_ours(args, world, rank, local):
         out["collisionless"] = {"value": world * 0.5 * (m0 + m1) * args.steps / (float(t2.item()) / 1e3),
                                 "ms_per_step": float(t2.item()) / args.steps,
                                 "push_ms": round(p2, 5),
-                                "push_frac_of_peak": round((0.5 * (m0 + m1) * 40.0 + G * 12.0) / (p2 / 1e3) / 1e9
-                                                           / peak, 4),
+                                "push_frac_of_peak": round((0.5 * (m0 + m1) * BYTES_PER_PARTICLE + G * BYTES_PER_NODE)
+                                                           / (p2 / 1e3) / 1e9 / peak, 4),
                                 "mg_cycles_per_step": prof2["mg_cycles"] / args.steps}
         sim.close()
         del sim

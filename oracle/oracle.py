@@ -150,6 +150,23 @@ def deposit_f32(gx, gy, scale, m, n, rho=None, abs_sum=None):
     return rho, abs_sum
 
 
+def deposit_counts(gx, gy, m, n):
+    """Number of particles contributing to each node (CIC: the four nodes around each live particle)."""
+    gx = np.asarray(gx, np.float32)
+    gy = np.asarray(gy, np.float32)
+    live = ~np.isnan(gx)
+    cx = np.minimum(np.maximum(gx[live], 0), np.float32(m - 1))
+    cy = np.minimum(np.maximum(gy[live], 0), np.float32(n - 1))
+    i0 = np.floor(cx).astype(np.int64)
+    j0 = np.floor(cy).astype(np.int64)
+    i1 = np.minimum(i0 + 1, m - 1)
+    j1 = np.minimum(j0 + 1, n - 1)
+    cnt = np.zeros(m * n, np.int64)
+    for a, b in ((i0, j0), (i1, j0), (i0, j1), (i1, j1)):
+        np.add.at(cnt, b * m + a, 1)
+    return cnt
+
+
 def kick_f32(gx, gy, vx, vy, ex, ey, kq, m, n):
     lib().or_kick_f32(gx, gy, vx, vy, len(gx), ex, ey, np.float32(kq), m, n)
 

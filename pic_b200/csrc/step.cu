@@ -45,6 +45,11 @@ constexpr int kPushP = 5;  // particles per thread per chunk (odd: conflict-free
 constexpr int kChunk = kPushThreads * kPushP;
 constexpr int kBufStride = kChunk + 8;  // floats per array per buffer: room for the 16-byte alignment window
 constexpr int kUnitMax = 8192;          // particles per work unit (one E tile staging, one charge flush)
+// The charge tile accumulates CIC weights as unsigned fixed point, 2^-19 per
+// unit: integer shared-memory atomics are native (float ones retry), the sum
+// is independent of the order, and 8192 weights <= 1 cannot overflow 2^32.
+constexpr float kFixScale = 524288.0f;  // 2^19
+constexpr float kFixInv = 1.0f / 524288.0f;
 constexpr int kBitWords = kChunk / 32 + 2;
 constexpr int kHalo = 4;                // cells staged around a tile
 constexpr int kArraySlack = 16;         // floats allocated past each species' capacity (bulk-copy window)
@@ -86,21 +91,6 @@ struct PushArgs {
     unsigned long long* ctr;
     int* error;  // set when a bounded wait gives up
 };
-
-__device__ __forceinline__ void flush_run(const PushArgs& A, float* rt, bool tiled, int ox, int oy, int i0, int j0,
-                                          int i1, int j1, float scale, float s00, float s10, float s01, float s11) {
-    const int ii[4] = {i0, i1, i0, i1};
-    const int jj[4] = {j0, j0, j1, j1};
-    const float vv[4] = {s00, s10, s01, s11};
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        if (vv[q] == 0.0f) continue;
-        const float v = __fmul_rn(scale, vv[q]);
-        const int li = ii[q] - ox, lj = jj[q] - oy;
-        if (tiled && li >= 0 && lj >= 0 && li < A.rw && lj < A.rw) atomicAdd(rt + lj * A.rw + li, v);
-        else atomicAdd(A.rho + long(jj[q]) * A.nx + ii[q], v);
-    }
-}
 
 // ---- TMA bulk copies and mbarriers (inline PTX, no multicast) -------------------
 
@@ -203,7 +193,7 @@ __device__ __forceinline__ void mark_chunk(const PushArgs& A, const ChunkDesc& c
 }
 
 // Stages the E tile of a unit's tile and zeroes its charge tile.
-__device__ __forceinline__ void stage_tile(const PushArgs& A, int tile, float2* et, float* rt, int& ox, int& oy) {
+__device__ __forceinline__ void stage_tile(const PushArgs& A, int tile, float2* et, unsigned* rt, int& ox, int& oy) {
     const int RW = A.rw;
     ox = (tile % A.tiles_x) * A.tile - kHalo;
     oy = (tile / A.tiles_x) * A.tile - kHalo;
@@ -211,7 +201,7 @@ __device__ __forceinline__ void stage_tile(const PushArgs& A, int tile, float2* 
         const int gi = ox + q % RW, gj = oy + q / RW;
         et[q] = (gi >= 0 && gj >= 0 && gi < A.nx && gj < A.ny) ? __ldg(A.E + long(gj) * A.nx + gi)
                                                                  : make_float2(0.f, 0.f);
-        rt[q] = 0.0f;
+        rt[q] = 0u;
     }
 }
 
@@ -227,7 +217,7 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
     float* bufs = reinterpret_cast<float*>(smem);  // [2][4][kBufStride]
     const int RW = A.rw;
     float2* et = reinterpret_cast<float2*>(bufs + 2 * 4 * kBufStride);
-    float* rt = reinterpret_cast<float*>(et + RW * RW);
+    unsigned* rt = reinterpret_cast<unsigned*>(et + RW * RW);
     unsigned* bits = reinterpret_cast<unsigned*>(rt + RW * RW);  // [2][kBitWords]
     __shared__ __align__(8) unsigned long long bar[2];
     __shared__ ChunkDesc s_ch[2];
@@ -370,20 +360,18 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
             if (A.do_deposit && is_live(x)) {
                 const Cic c = cic_weights(x, y, A.nx, A.ny);
                 const int li = c.i0 - ox, lj = c.j0 - oy;
-                const float w00 = __fmul_rn(C.scale, c.w00), w10 = __fmul_rn(C.scale, c.w10);
-                const float w01 = __fmul_rn(C.scale, c.w01), w11 = __fmul_rn(C.scale, c.w11);
                 if (tiled && li >= 0 && lj >= 0 && li + 1 < RW && lj + 1 < RW) {
                     const int q = lj * RW + li;
                     const int dq = c.i1 - c.i0, dr = (c.j1 - c.j0) * RW;
-                    atomicAdd(rt + q, w00);
-                    atomicAdd(rt + q + dq, w10);
-                    atomicAdd(rt + q + dr, w01);
-                    atomicAdd(rt + q + dr + dq, w11);
+                    atomicAdd(rt + q, __float2uint_rn(__fmul_rn(c.w00, kFixScale)));
+                    atomicAdd(rt + q + dq, __float2uint_rn(__fmul_rn(c.w10, kFixScale)));
+                    atomicAdd(rt + q + dr, __float2uint_rn(__fmul_rn(c.w01, kFixScale)));
+                    atomicAdd(rt + q + dr + dq, __float2uint_rn(__fmul_rn(c.w11, kFixScale)));
                 } else {
-                    atomicAdd(A.rho + long(c.j0) * A.nx + c.i0, w00);
-                    atomicAdd(A.rho + long(c.j0) * A.nx + c.i1, w10);
-                    atomicAdd(A.rho + long(c.j1) * A.nx + c.i0, w01);
-                    atomicAdd(A.rho + long(c.j1) * A.nx + c.i1, w11);
+                    atomicAdd(A.rho + long(c.j0) * A.nx + c.i0, __fmul_rn(C.scale, c.w00));
+                    atomicAdd(A.rho + long(c.j0) * A.nx + c.i1, __fmul_rn(C.scale, c.w10));
+                    atomicAdd(A.rho + long(c.j1) * A.nx + c.i0, __fmul_rn(C.scale, c.w01));
+                    atomicAdd(A.rho + long(c.j1) * A.nx + c.i1, __fmul_rn(C.scale, c.w11));
                 }
             }
         }
@@ -403,8 +391,10 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
             __syncthreads();
             if (tiled && A.do_deposit) {
                 for (int q = tid; q < RW * RW; q += kPushThreads) {
-                    const float val = rt[q];
-                    if (val != 0.0f) atomicAdd(A.rho + long(oy + q / RW) * A.nx + ox + q % RW, val);
+                    const unsigned sum = rt[q];
+                    if (sum)
+                        atomicAdd(A.rho + long(oy + q / RW) * A.nx + ox + q % RW,
+                                  __fmul_rn(C.scale, __fmul_rn(float(sum), kFixInv)));
                 }
             }
             if (tid == 0) {
@@ -939,7 +929,7 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
         PIC_CUDA(cudaMemcpy(S.phi, phi0.data(), sizeof(double) * S.G, cudaMemcpyHostToDevice));
     }
     // launch shape of the particle pass
-    S.push_smem = sizeof(float) * 2 * 4 * kBufStride + size_t(S.rw) * S.rw * (sizeof(float2) + sizeof(float)) +
+    S.push_smem = sizeof(float) * 2 * 4 * kBufStride + size_t(S.rw) * S.rw * (sizeof(float2) + sizeof(unsigned)) +
                   sizeof(unsigned) * 2 * kBitWords;
     PIC_CUDA(cudaFuncSetAttribute(k_push, cudaFuncAttributeMaxDynamicSharedMemorySize, int(S.push_smem)));
     int per_sm = 0;
