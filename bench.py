@@ -56,7 +56,8 @@ def parse():
     ap.add_argument("--no-collisionless", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-graph", action="store_true", help="launch every kernel from the host (profilers)")
-    ap.add_argument("--mg-no-graph", action="store_true", help="host-driven multigrid cycles (profilers)")
+    ap.add_argument("--mg-launch", default="persistent", choices=["persistent", "host", "graph"],
+                    help="multigrid launch mode (host: one launch per kernel, for profilers)")
     return ap.parse_args()
 
 
@@ -142,7 +143,7 @@ def ncu_traffic():
     return None
 
 
-GRAPH_OPTS = {"use_graph": True, "mg_graph": True}
+GRAPH_OPTS = {"use_graph": True, "mg_launch": "persistent"}
 
 
 def make_sim(w, rank, sort_interval, mcc=True):
@@ -455,7 +456,7 @@ def run_reference(args, world, rank):
 def main():
     args = parse()
     GRAPH_OPTS["use_graph"] = not args.no_graph
-    GRAPH_OPTS["mg_graph"] = not args.mg_no_graph
+    GRAPH_OPTS["mg_launch"] = args.mg_launch
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, world, rank)

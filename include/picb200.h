@@ -103,14 +103,19 @@ typedef enum pic_mg_precision {
     PIC_MG_FP64 = 1   /* the same V-cycle in FP64 throughout                    */
 } pic_mg_precision;
 
+typedef enum pic_mg_launch_mode {
+    PIC_MG_PERSISTENT = 0, /* one cooperative kernel per solve; phases separated by grid barriers */
+    PIC_MG_HOST_LOOP = 1,  /* one launch per kernel, convergence tested on the host each cycle */
+    PIC_MG_GRAPH_LOOP = 2  /* one launch per kernel inside a CUDA-graph conditional WHILE node */
+} pic_mg_launch_mode;
+
 typedef struct pic_mg_options {
     int precision;    /* pic_mg_precision */
     int pre_sweeps;   /* red-black Gauss-Seidel sweeps before restriction (default 2) */
     int post_sweeps;  /* sweeps after prolongation (default 2) */
     double omega;     /* over-relaxation of the smoother (default 1.0) */
     int coarsest_max; /* coarsen while both node counts exceed this (default 9) */
-    int no_graph;     /* 1: launch each cycle from the host and test convergence there
-                         (for profilers that do not follow graph conditional nodes) */
+    int launch_mode;  /* pic_mg_launch_mode */
 } pic_mg_options;
 
 typedef struct pic_mg_info {

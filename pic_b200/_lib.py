@@ -36,6 +36,11 @@ STATUS_NAMES = {
 PIC_MG_MIXED = 0
 PIC_MG_FP64 = 1
 
+PIC_MG_PERSISTENT = 0
+PIC_MG_HOST_LOOP = 1
+PIC_MG_GRAPH_LOOP = 2
+MG_LAUNCH_MODES = {"persistent": PIC_MG_PERSISTENT, "host": PIC_MG_HOST_LOOP, "graph": PIC_MG_GRAPH_LOOP}
+
 PIC_ELASTIC = 0
 PIC_EXCITATION = 1
 PIC_IONIZATION = 2
@@ -50,7 +55,7 @@ class PicError(RuntimeError):
 
 class MgOptions(C.Structure):
     _fields_ = [("precision", C.c_int), ("pre_sweeps", C.c_int), ("post_sweeps", C.c_int), ("omega", C.c_double),
-                ("coarsest_max", C.c_int), ("no_graph", C.c_int)]
+                ("coarsest_max", C.c_int), ("launch_mode", C.c_int)]
 
 
 class MgInfo(C.Structure):

@@ -24,6 +24,8 @@
 //             and the loop decision
 // The loop is a CUDA-graph conditional WHILE node whose condition r0 sets,
 // so a solve issues no host synchronisation.
+#include <cuda/atomic>
+
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -40,6 +42,9 @@ constexpr int kMgMaxCoarseLevels = 8;
 constexpr int kCoarseThreads = 1024;
 constexpr long kCoarseMaxNodes32 = 65L * 65L;    // FP32 levels at or below this size run in the single-CTA kernel
 constexpr long kCoarseMaxNodes64 = 65L * 65L;    // FP64 levels (twice the shared memory per node)
+constexpr int kMgMaxLevels = 16;
+constexpr long kPersistCoarseMax = 33L * 33L;    // levels the persistent kernel's single block solves
+constexpr unsigned long long kBarrierPolls = 1ull << 26;  // a grid barrier gives up (error flag) after this
 
 template <class T>
 struct LevelDev {
@@ -103,13 +108,13 @@ __device__ __forceinline__ void tile_load(const LevelDev<T>& L, int ox, int oy, 
 }
 
 template <class T>
-__global__ void __launch_bounds__(kMgThreads) k_mg_down(LevelDev<T> F, LevelDev<T> Cc, T omega, int pre) {
-    extern __shared__ __align__(16) unsigned char smem[];
+__device__ void down_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, int pre, int tx, int ty,
+                          unsigned char* smem) {
     const int H = 2 * pre + 2, W = kMgTile + 2 * H;
     T* se = reinterpret_cast<T*>(smem);
     T* sg = se + W * W;
     uint8_t* sm = reinterpret_cast<uint8_t*>(sg + W * W);
-    const int x0 = blockIdx.x * kMgTile, y0 = blockIdx.y * kMgTile;
+    const int x0 = tx * kMgTile, y0 = ty * kMgTile;
     const int ox = x0 - H, oy = y0 - H;
     const int tid = threadIdx.x;
     tile_load(F, ox, oy, W, se, sg, sm, false, kMgThreads, tid);
@@ -151,17 +156,23 @@ __global__ void __launch_bounds__(kMgThreads) k_mg_down(LevelDev<T> F, LevelDev<
         v += T(0.0625) * (r(-W - 1) + r(-W + 1) + r(W - 1) + r(W + 1));
         Cc.g[K] = v;
     }
+    __syncthreads();  // the caller may reuse the shared tile
 }
 
 template <class T>
-__global__ void __launch_bounds__(kMgThreads) k_mg_up(LevelDev<T> F, LevelDev<T> Cc, T omega, int post,
-                                                      double* __restrict__ phi) {
+__global__ void __launch_bounds__(kMgThreads) k_mg_down(LevelDev<T> F, LevelDev<T> Cc, T omega, int pre) {
     extern __shared__ __align__(16) unsigned char smem[];
+    down_tile(F, Cc, omega, pre, blockIdx.x, blockIdx.y, smem);
+}
+
+template <class T>
+__device__ void up_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, int post, double* __restrict__ phi,
+                        int tx, int ty, unsigned char* smem) {
     const int H = 2 * post, W = kMgTile + 2 * H;
     T* se = reinterpret_cast<T*>(smem);
     T* sg = se + W * W;
     uint8_t* sm = reinterpret_cast<uint8_t*>(sg + W * W);
-    const int x0 = blockIdx.x * kMgTile, y0 = blockIdx.y * kMgTile;
+    const int x0 = tx * kMgTile, y0 = ty * kMgTile;
     const int ox = x0 - H, oy = y0 - H;
     const int tid = threadIdx.x;
     tile_load(F, ox, oy, W, se, sg, sm, true, kMgThreads, tid);
@@ -195,6 +206,14 @@ __global__ void __launch_bounds__(kMgThreads) k_mg_up(LevelDev<T> F, LevelDev<T>
         if (phi) phi[k] += double(v);
         else F.e[k] = v;
     }
+    __syncthreads();  // the caller may reuse the shared tile
+}
+
+template <class T>
+__global__ void __launch_bounds__(kMgThreads) k_mg_up(LevelDev<T> F, LevelDev<T> Cc, T omega, int post,
+                                                      double* __restrict__ phi) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    up_tile(F, Cc, omega, post, phi, blockIdx.x, blockIdx.y, smem);
 }
 
 // ---- single-CTA V-cycle of the coarse levels --------------------------------------
@@ -221,8 +240,7 @@ __device__ void level_sweeps(T* se, const T* sg, const uint8_t* sm, const LevelD
 }
 
 template <class T>
-__global__ void __launch_bounds__(kCoarseThreads) k_mg_coarse(CoarseDesc<T> D) {
-    extern __shared__ __align__(16) unsigned char smem[];
+__device__ void coarse_vcycle(const CoarseDesc<T>& D, unsigned char* smem) {
     T* E[kMgMaxCoarseLevels];
     T* Gs[kMgMaxCoarseLevels];
     uint8_t* M[kMgMaxCoarseLevels];
@@ -306,6 +324,13 @@ __global__ void __launch_bounds__(kCoarseThreads) k_mg_coarse(CoarseDesc<T> D) {
         if (D.phi0) D.phi0[q] += double(E[0][q]);
         else L0.e[q] = E[0][q];
     }
+    __syncthreads();
+}
+
+template <class T>
+__global__ void __launch_bounds__(kCoarseThreads) k_mg_coarse(CoarseDesc<T> D) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    coarse_vcycle(D, smem);
 }
 
 // ---- FP64 residual, norms and the loop decision -----------------------------------
@@ -400,6 +425,174 @@ __global__ void __launch_bounds__(256) k_mg_r0(const double* __restrict__ phi, c
     }
 }
 
+// ---- persistent cooperative solve -------------------------------------------------
+
+struct GridBar {
+    unsigned count;
+    unsigned gen;
+};
+
+// Grid-wide barrier of a cooperative launch; false (and *error set) if it
+// did not complete within kBarrierPolls polls.
+__device__ __forceinline__ bool grid_barrier(GridBar* b, int* error) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(b->gen), cnt(b->count);
+        const unsigned g = gen.load(cuda::memory_order_acquire);
+        const unsigned nb = gridDim.x * gridDim.y;
+        int ok = 1;
+        __threadfence();
+        if (cnt.fetch_add(1u, cuda::memory_order_acq_rel) == nb - 1u) {
+            cnt.store(0u, cuda::memory_order_relaxed);
+            gen.fetch_add(1u, cuda::memory_order_release);
+        } else {
+            unsigned long long k = 0;
+            while (gen.load(cuda::memory_order_acquire) == g) {
+                if (++k > kBarrierPolls) {
+                    ok = 0;
+                    atomicExch(error, 1);
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+template <class T>
+struct SolveDesc {
+    int L, Lp;  // levels; first level handled by the single-block coarse phase
+    LevelDev<T> lv[kMgMaxLevels];
+    CoarseDesc<T> coarse;  // levels Lp..L-1
+    const double* f;
+    double* phi;
+    int nx, ny;
+    double cx, cy;
+    NormState N;
+    double tol2;
+    int max_cycles;
+    T omega;
+    int pre, post;
+    GridBar* bar;
+    int* error;
+};
+
+// FP64 residual of phi on level 0 (written to g0 as the next V-cycle's
+// right-hand side) and its norm, identical in every block: the block partials
+// are summed after a grid barrier in a fixed order.
+template <class T>
+__device__ bool r0_phase(const SolveDesc<T>& S, double& r2, double& f2) {
+    const int tnx = (S.nx + kMgTile - 1) / kMgTile, tny = (S.ny + kMgTile - 1) / kMgTile;
+    const double* __restrict__ phi = S.phi;
+    const uint8_t* __restrict__ mask = S.lv[0].mask;
+    const int nx = S.nx, ny = S.ny;
+    double a = 0.0, b = 0.0;
+    for (int t = blockIdx.x; t < tnx * tny; t += gridDim.x) {
+        const int x0 = (t % tnx) * kMgTile, y0 = (t / tnx) * kMgTile;
+        for (int q = threadIdx.x; q < kMgTile * kMgTile; q += blockDim.x) {
+            const int i = x0 + q % kMgTile, j = y0 + q / kMgTile;
+            if (i >= nx || j >= ny) continue;
+            const long k = long(j) * nx + i;
+            double r = 0.0;
+            if (i > 0 && j > 0 && i < nx - 1 && j < ny - 1 && !mask[k]) {
+                const double c = phi[k];
+                const double lap = S.cx * ((phi[k - 1] - c) + (phi[k + 1] - c)) +
+                                   S.cy * ((phi[k - nx] - c) + (phi[k + nx] - c));
+                const double fv = S.f[k];
+                r = fv - lap;
+                b += fv * fv;
+            }
+            S.lv[0].g[k] = T(r);
+            a += r * r;
+        }
+    }
+    __shared__ double ws[2][kMgThreads / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    if (lane == 0) {
+        ws[0][w] = a;
+        ws[1][w] = b;
+    }
+    __syncthreads();
+    const int nb = gridDim.x;
+    if (threadIdx.x == 0) {
+        double sa = 0.0, sb = 0.0;
+        for (int q = 0; q < nw; ++q) {
+            sa += ws[0][q];
+            sb += ws[1][q];
+        }
+        S.N.partial[blockIdx.x] = sa;
+        S.N.partial[nb + blockIdx.x] = sb;
+    }
+    if (!grid_barrier(S.bar, S.error)) return false;
+    const volatile double* P = S.N.partial;
+    double sa = 0.0, sb = 0.0;
+    for (int q = threadIdx.x; q < nb; q += blockDim.x) {
+        sa += P[q];
+        sb += P[nb + q];
+    }
+    sa = warp_sum(sa);
+    sb = warp_sum(sb);
+    __syncthreads();
+    if (lane == 0) {
+        ws[0][w] = sa;
+        ws[1][w] = sb;
+    }
+    __syncthreads();
+    r2 = 0.0;
+    f2 = 0.0;
+    for (int q = 0; q < nw; ++q) {
+        r2 += ws[0][q];
+        f2 += ws[1][q];
+    }
+    __syncthreads();
+    return true;
+}
+
+// The whole solve in one cooperative launch: residual, then V-cycles until
+// converged or max_cycles, each phase separated by a grid barrier.
+template <class T>
+__global__ void __launch_bounds__(kMgThreads) k_mg_solve(SolveDesc<T> S) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    double r2 = 0.0, f2 = 0.0, dummy = 0.0;
+    if (!r0_phase(S, r2, f2)) return;
+    const double ref = f2 > 0.0 ? f2 : 1.0;
+    int cycles = 0;
+    bool conv = r2 < S.tol2 * ref;
+    while (!conv && cycles < S.max_cycles) {
+        for (int l = 0; l < S.Lp; ++l) {
+            const int tnx = (S.lv[l].nx + kMgTile - 1) / kMgTile, tny = (S.lv[l].ny + kMgTile - 1) / kMgTile;
+            for (int t = blockIdx.x; t < tnx * tny; t += gridDim.x)
+                down_tile(S.lv[l], S.lv[l + 1], S.omega, S.pre, t % tnx, t / tnx, smem);
+            if (!grid_barrier(S.bar, S.error)) return;
+        }
+        if (blockIdx.x == 0) coarse_vcycle(S.coarse, smem);
+        if (!grid_barrier(S.bar, S.error)) return;
+        for (int l = S.Lp - 1; l >= 0; --l) {
+            const int tnx = (S.lv[l].nx + kMgTile - 1) / kMgTile, tny = (S.lv[l].ny + kMgTile - 1) / kMgTile;
+            for (int t = blockIdx.x; t < tnx * tny; t += gridDim.x)
+                up_tile(S.lv[l], S.lv[l + 1], S.omega, S.post, l == 0 ? S.phi : nullptr, t % tnx, t / tnx, smem);
+            if (!grid_barrier(S.bar, S.error)) return;
+        }
+        if (!r0_phase(S, r2, dummy)) return;
+        ++cycles;
+        conv = r2 < S.tol2 * ref;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        S.N.norms[0] = f2;
+        S.N.norms[1] = r2;
+        *S.N.cycles = cycles;
+        *S.N.converged = conv ? 1 : 0;
+        *S.N.total += cycles;
+    }
+}
+
 // ---- host object ---------------------------------------------------------------
 
 struct MgImpl {
@@ -418,7 +611,14 @@ struct MgImpl {
     size_t coarse_smem = 0;
     int coarse_off_e[kMgMaxCoarseLevels]{}, coarse_off_g[kMgMaxCoarseLevels]{}, coarse_off_m[kMgMaxCoarseLevels]{};
     long long launches = 0;  // kernels executed by solves
-    int body_launches = 0;   // kernels per V-cycle
+    int body_launches = 0;   // kernels per V-cycle (graph and host loops)
+    // persistent cooperative solve
+    int Lp = 0;
+    size_t solve_smem = 0, coarse2_smem = 0;
+    int coarse2_off_e[kMgMaxCoarseLevels]{}, coarse2_off_g[kMgMaxCoarseLevels]{}, coarse2_off_m[kMgMaxCoarseLevels]{};
+    int solve_grid = 0;
+    GridBar* bar = nullptr;
+    int* error = nullptr;
     cudaStream_t side = nullptr;
     cudaStream_t cap = nullptr;
     // cached solve graph
@@ -514,6 +714,12 @@ static int configure_kernels(MgImpl& M) {
     PIC_CUDA(cudaFuncSetAttribute(k_mg_down<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(down)));
     PIC_CUDA(cudaFuncSetAttribute(k_mg_up<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(up)));
     PIC_CUDA(cudaFuncSetAttribute(k_mg_coarse<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(M.coarse_smem)));
+    M.solve_smem = std::max(std::max(down, up), M.coarse2_smem);
+    PIC_CUDA(cudaFuncSetAttribute(k_mg_solve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(M.solve_smem)));
+    int per_sm = 0;
+    PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mg_solve<T>, kMgThreads, M.solve_smem));
+    if (per_sm < 1) return fail(PIC_ERR_CUDA, "multigrid: the persistent kernel does not fit on an SM");
+    M.solve_grid = std::min(per_sm, 2) * num_sms();
     return PIC_OK;
 }
 
@@ -544,7 +750,7 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
         if (opts->post_sweeps > 0) M.o.post_sweeps = opts->post_sweeps;
         if (opts->omega > 0) M.o.omega = opts->omega;
         if (opts->coarsest_max >= 3) M.o.coarsest_max = opts->coarsest_max;
-        M.o.no_graph = opts->no_graph;
+        M.o.launch_mode = opts->launch_mode;
     }
     auto bail = [&](int code) {
         mg_release(mg);
@@ -554,6 +760,8 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
         return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: unknown precision %d", M.o.precision));
     if (M.o.pre_sweeps > 8 || M.o.post_sweeps > 8)
         return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: at most 8 pre/post sweeps"));
+    if (M.o.launch_mode < PIC_MG_PERSISTENT || M.o.launch_mode > PIC_MG_GRAPH_LOOP)
+        return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: unknown launch mode %d", M.o.launch_mode));
     M.precision = M.o.precision;
     M.nx = nx;
     M.ny = ny;
@@ -574,6 +782,7 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
         masks.push_back(std::move(mc));
     }
     M.L = int(nxs.size());
+    if (M.L > kMgMaxLevels) return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: more than %d levels", kMgMaxLevels));
     const long coarse_max = M.precision == PIC_MG_MIXED ? kCoarseMaxNodes32 : kCoarseMaxNodes64;
     M.Lc = 0;
     while (M.Lc < M.L && long(nxs[M.Lc]) * nys[M.Lc] > coarse_max) ++M.Lc;
@@ -632,6 +841,21 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
         off += ((G + 15) / 16) * 16;
     }
     M.coarse_smem = off;
+    M.Lp = 0;
+    while (M.Lp < M.L && long(nxs[M.Lp]) * nys[M.Lp] > kPersistCoarseMax) ++M.Lp;
+    if (M.L - M.Lp > kMgMaxCoarseLevels) M.Lp = M.L - kMgMaxCoarseLevels;
+    off = 0;
+    for (int l = M.Lp; l < M.L; ++l) {
+        const size_t G = size_t(nxs[l]) * nys[l];
+        const int c = l - M.Lp;
+        M.coarse2_off_e[c] = int(off);
+        off += ((G * esz + 15) / 16) * 16;
+        M.coarse2_off_g[c] = int(off);
+        off += ((G * esz + 15) / 16) * 16;
+        M.coarse2_off_m[c] = int(off);
+        off += ((G + 15) / 16) * 16;
+    }
+    M.coarse2_smem = off;
     int st = M.precision == PIC_MG_MIXED ? alloc_levels(M, M.lf, masks, nxs, nys)
                                          : alloc_levels(M, M.ld, masks, nxs, nys);
     if (st == PIC_OK) st = M.precision == PIC_MG_MIXED ? configure_kernels<float>(M) : configure_kernels<double>(M);
@@ -650,6 +874,8 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
     M.N.done = reinterpret_cast<unsigned*>(small + 24);
     M.N.converged = reinterpret_cast<int*>(small + 28);
     M.N.cycles = reinterpret_cast<int*>(small + 32);
+    M.bar = reinterpret_cast<GridBar*>(small + 40);
+    M.error = reinterpret_cast<int*>(small + 48);
     if (cudaStreamCreateWithFlags(&M.side, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&M.cap, cudaStreamNonBlocking) != cudaSuccess)
         return bail(fail(PIC_ERR_CUDA, "pic_mg_create: stream creation failed"));
@@ -733,9 +959,64 @@ static int capture_solve(MgImpl& M, std::vector<LevelDev<T>>& lv, double* phi, c
     return PIC_OK;
 }
 
-// Appends the whole solve (the residual, then a WHILE node over V-cycles) to
-// a capture in progress on `st`.
+template <class T>
+static int launch_persistent(MgImpl& M, std::vector<LevelDev<T>>& lv, double* phi, const double* f, double tol,
+                             int max_cycles, cudaStream_t st) {
+    SolveDesc<T> S{};
+    S.L = M.L;
+    S.Lp = M.Lp;
+    for (int l = 0; l < M.L; ++l) S.lv[l] = lv[l];
+    CoarseDesc<T>& D = S.coarse;
+    D.nlev = M.L - M.Lp;
+    for (int c = 0; c < D.nlev; ++c) {
+        D.lv[c] = lv[M.Lp + c];
+        D.off_e[c] = M.coarse2_off_e[c];
+        D.off_g[c] = M.coarse2_off_g[c];
+        D.off_m[c] = M.coarse2_off_m[c];
+    }
+    D.ainv = M.ainv;
+    D.cidx = M.cidx;
+    D.nf = M.nfree_c;
+    D.omega = T(M.o.omega);
+    D.pre = M.o.pre_sweeps;
+    D.post = M.o.post_sweeps;
+    D.phi0 = M.Lp == 0 ? phi : nullptr;
+    S.f = f;
+    S.phi = phi;
+    S.nx = M.nx;
+    S.ny = M.ny;
+    S.cx = 1.0 / (M.dx * M.dx);
+    S.cy = 1.0 / (M.dy * M.dy);
+    S.N = M.N;
+    S.tol2 = tol * tol;
+    S.max_cycles = max_cycles;
+    S.omega = T(M.o.omega);
+    S.pre = M.o.pre_sweeps;
+    S.post = M.o.post_sweeps;
+    S.bar = M.bar;
+    S.error = M.error;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(M.solve_grid);
+    cfg.blockDim = dim3(kMgThreads);
+    cfg.dynamicSmemBytes = M.solve_smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    PIC_CUDA(cudaLaunchKernelEx(&cfg, k_mg_solve<T>, S));
+    return PIC_OK;
+}
+
+// Appends the whole solve to a capture in progress on `st`: the persistent
+// kernel, or the residual and a WHILE node over V-cycles.
 int mg_capture(MgImpl& M, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
+    if (M.o.launch_mode == PIC_MG_PERSISTENT)
+        return M.precision == PIC_MG_MIXED ? launch_persistent(M, M.lf, phi, f, tol, max_cycles, st)
+                                           : launch_persistent(M, M.ld, phi, f, tol, max_cycles, st);
+    if (M.o.launch_mode == PIC_MG_HOST_LOOP)
+        return fail(PIC_ERR_BAD_ARG, "multigrid: the host-driven loop cannot be captured in a graph");
     return M.precision == PIC_MG_MIXED ? capture_solve(M, M.lf, phi, f, tol, max_cycles, st)
                                        : capture_solve(M, M.ld, phi, f, tol, max_cycles, st);
 }
@@ -766,8 +1047,11 @@ static int ensure_graph(MgImpl& M, double* phi, const double* f, double tol, int
 }
 
 int mg_read_info(MgImpl& M, pic_mg_info* info) {
-    unsigned char small[40];
+    unsigned char small[52];
     PIC_CUDA(cudaMemcpy(small, M.N.norms, sizeof small, cudaMemcpyDeviceToHost));
+    int err = 0;
+    memcpy(&err, small + 48, 4);
+    if (err) return fail(PIC_ERR_TIMEOUT, "multigrid: a grid barrier of the persistent solve timed out");
     double norms[2];
     int conv, cycles;
     memcpy(norms, small, 16);
@@ -809,7 +1093,10 @@ static int solve_eager(MgImpl& M, std::vector<LevelDev<T>>& lv, double* phi, con
 }
 
 int mg_launch(MgImpl& M, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
-    if (M.o.no_graph)
+    if (M.o.launch_mode == PIC_MG_PERSISTENT)
+        return M.precision == PIC_MG_MIXED ? launch_persistent(M, M.lf, phi, f, tol, max_cycles, st)
+                                           : launch_persistent(M, M.ld, phi, f, tol, max_cycles, st);
+    if (M.o.launch_mode == PIC_MG_HOST_LOOP)
         return M.precision == PIC_MG_MIXED ? solve_eager(M, M.lf, phi, f, tol, max_cycles, st)
                                            : solve_eager(M, M.ld, phi, f, tol, max_cycles, st);
     PIC_TRY(ensure_graph(M, phi, f, tol, max_cycles));
@@ -823,7 +1110,7 @@ int mg_solve(MgImpl& M, double* phi, const double* f, double tol, int max_cycles
     PIC_CUDA(cudaStreamSynchronize(st));
     pic_mg_info loc{};
     PIC_TRY(mg_read_info(M, &loc));
-    M.launches += 1 + (long long)(loc.cycles) * M.body_launches;
+    M.launches += 1 + (M.o.launch_mode == PIC_MG_PERSISTENT ? 0 : (long long)(loc.cycles) * M.body_launches);
     if (info) *info = loc;
     if (!loc.converged)
         return fail(PIC_ERR_NOT_CONVERGED, "multigrid: relative residual %.3e after %d cycles (tol %.1e)", loc.rel_res,
@@ -832,11 +1119,13 @@ int mg_solve(MgImpl& M, double* phi, const double* f, double tol, int max_cycles
 }
 
 long long mg_launches(pic_mg* mg) { return mg ? mg->m.launches : 0; }
-int mg_body_launches(pic_mg* mg) { return mg ? mg->m.body_launches : 0; }
+int mg_body_launches(pic_mg* mg) {
+    return (mg && mg->m.o.launch_mode != PIC_MG_PERSISTENT) ? mg->m.body_launches : 0;
+}
 int mg_capture_into(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
     return mg_capture(mg->m, phi, f, tol, max_cycles, st);
 }
-bool mg_uses_graph(pic_mg* mg) { return !mg->m.o.no_graph; }
+bool mg_uses_graph(pic_mg* mg) { return mg->m.o.launch_mode != PIC_MG_HOST_LOOP; }
 int mg_launch_graph(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
     return mg_launch(mg->m, phi, f, tol, max_cycles, st);
 }

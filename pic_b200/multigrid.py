@@ -24,7 +24,7 @@ from . import _lib
 
 class MultigridSolver:
     def __init__(self, bc_mask, nx, ny, h, levels=4, omega=1.0, precision="mixed", pre_sweeps=2, post_sweeps=2,
-                 hy=None, graph=True):
+                 hy=None, launch="persistent"):
         self.nx, self.ny = int(nx), int(ny)
         self.h = float(h)
         self.hy = float(h if hy is None else hy)
@@ -35,7 +35,7 @@ class MultigridSolver:
             raise ValueError("bc_mask must have nx*ny entries")
         self.precision = precision
         opts = _lib.MgOptions(_lib.PIC_MG_MIXED if precision == "mixed" else _lib.PIC_MG_FP64, pre_sweeps,
-                              post_sweeps, self.omega, 9, 0 if graph else 1)
+                              post_sweeps, self.omega, 9, _lib.MG_LAUNCH_MODES[launch])
         self._h = C.c_void_p()
         _lib.call("pic_mg_create", self.nx, self.ny, self.h, self.hy, mask.ctypes.data, C.byref(opts),
                   C.byref(self._h))

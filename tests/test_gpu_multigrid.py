@@ -39,14 +39,16 @@ def manufactured(n):
     return h, f, exact
 
 
+@pytest.mark.parametrize("launch", ["persistent", "graph", "host"])
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
 @pytest.mark.parametrize("n", [17, 33, 65, 129, 257])
-def test_manufactured_solution(precision, n):
-    """17..65 nodes run entirely in the single-CTA coarse kernel; 129 and 257 use the tiled kernels too."""
+def test_manufactured_solution(launch, precision, n):
+    """Small grids run entirely in the single-block coarse V-cycle; larger ones use the tiled phases too.
+    The three launch modes run the same arithmetic."""
     h, f, exact = manufactured(n)
     mask = edge_mask(n)
     f[mask == 1] = 0.0
-    mg = MultigridSolver(mask, n, n, h, precision=precision)
+    mg = MultigridSolver(mask, n, n, h, precision=precision, launch=launch)
     phi = torch.zeros(n * n, dtype=torch.float64, device=DEV)
     phi, (cycles, rel) = mg.solve(phi, torch.as_tensor(f, device=DEV), tol=1e-12, max_cycles=40)
     # a V(2,2) cycle reduces the residual ~10x; from phi = 0 to 1e-12 takes about 12 cycles
@@ -103,7 +105,7 @@ def test_internal_electrodes_match_direct_solve():
         np.testing.assert_allclose(phi.cpu().numpy(), ref, rtol=0, atol=1e-8 * np.abs(ref).max())
 
 
-@pytest.mark.parametrize("n,tol", [(513, 1e-8), (513, 1e-10), (1025, 1e-10)])
+@pytest.mark.parametrize("n,tol", [(513, 1e-8), (513, 1e-10), (1025, 1e-10), (2049, 1e-10)])
 def test_residual_recomputed_on_cpu(n, tol):
     rng = np.random.Generator(np.random.Philox(6))
     h = 1e-4
