@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--no-collisionless", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-graph", action="store_true", help="launch every kernel from the host (profilers)")
-    ap.add_argument("--mg-launch", default="persistent", choices=["persistent", "host", "graph"],
+    ap.add_argument("--mg-launch", default="graph", choices=["persistent", "host", "graph"],
                     help="multigrid launch mode (host: one launch per kernel, for profilers)")
     return ap.parse_args()
 
@@ -143,7 +143,7 @@ def ncu_traffic():
     return None
 
 
-GRAPH_OPTS = {"use_graph": True, "mg_launch": "persistent"}
+GRAPH_OPTS = {"use_graph": True, "mg_launch": "graph"}
 
 
 def make_sim(w, rank, sort_interval, mcc=True):

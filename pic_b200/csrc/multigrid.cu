@@ -44,7 +44,7 @@ constexpr long kCoarseMaxNodes32 = 65L * 65L;    // FP32 levels at or below this
 constexpr long kCoarseMaxNodes64 = 65L * 65L;    // FP64 levels (twice the shared memory per node)
 constexpr int kMgMaxLevels = 16;
 constexpr long kPersistCoarseMax = 33L * 33L;    // levels the persistent kernel's single block solves
-constexpr unsigned long long kBarrierPolls = 1ull << 26;  // a grid barrier gives up (error flag) after this
+constexpr unsigned long long kBarrierPolls = 1ull << 24;  // a grid barrier gives up (error flag) after this
 
 template <class T>
 struct LevelDev {
@@ -433,8 +433,10 @@ struct GridBar {
 };
 
 // Grid-wide barrier of a cooperative launch; false (and *error set) if it
-// did not complete within kBarrierPolls polls.
-__device__ __forceinline__ bool grid_barrier(GridBar* b, int* error) {
+// did not complete within kBarrierPolls polls.  On a timeout the block also
+// records, in error[1..5], the barrier's sequence number, its block index and
+// the counter state it saw.
+__device__ __forceinline__ bool grid_barrier(GridBar* b, int* error, int seq) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -451,10 +453,15 @@ __device__ __forceinline__ bool grid_barrier(GridBar* b, int* error) {
             while (gen.load(cuda::memory_order_acquire) == g) {
                 if (++k > kBarrierPolls) {
                     ok = 0;
-                    atomicExch(error, 1);
+                    if (atomicExch(error, 1) == 0) {
+                        error[1] = seq;
+                        error[2] = int(blockIdx.x);
+                        error[3] = int(cnt.load(cuda::memory_order_relaxed));
+                        error[4] = int(gen.load(cuda::memory_order_relaxed));
+                        error[5] = int(g);
+                    }
                     break;
                 }
-                __nanosleep(32);
             }
         }
         __threadfence();
@@ -486,7 +493,7 @@ struct SolveDesc {
 // right-hand side) and its norm, identical in every block: the block partials
 // are summed after a grid barrier in a fixed order.
 template <class T>
-__device__ bool r0_phase(const SolveDesc<T>& S, double& r2, double& f2) {
+__device__ bool r0_phase(const SolveDesc<T>& S, double& r2, double& f2, int& seq) {
     const int tnx = (S.nx + kMgTile - 1) / kMgTile, tny = (S.ny + kMgTile - 1) / kMgTile;
     const double* __restrict__ phi = S.phi;
     const uint8_t* __restrict__ mask = S.lv[0].mask;
@@ -530,7 +537,7 @@ __device__ bool r0_phase(const SolveDesc<T>& S, double& r2, double& f2) {
         S.N.partial[blockIdx.x] = sa;
         S.N.partial[nb + blockIdx.x] = sb;
     }
-    if (!grid_barrier(S.bar, S.error)) return false;
+    if (!grid_barrier(S.bar, S.error, seq++)) return false;
     const volatile double* P = S.N.partial;
     double sa = 0.0, sb = 0.0;
     for (int q = threadIdx.x; q < nb; q += blockDim.x) {
@@ -561,7 +568,8 @@ template <class T>
 __global__ void __launch_bounds__(kMgThreads) k_mg_solve(SolveDesc<T> S) {
     extern __shared__ __align__(16) unsigned char smem[];
     double r2 = 0.0, f2 = 0.0, dummy = 0.0;
-    if (!r0_phase(S, r2, f2)) return;
+    int seq = 0;
+    if (!r0_phase(S, r2, f2, seq)) return;
     const double ref = f2 > 0.0 ? f2 : 1.0;
     int cycles = 0;
     bool conv = r2 < S.tol2 * ref;
@@ -570,17 +578,17 @@ __global__ void __launch_bounds__(kMgThreads) k_mg_solve(SolveDesc<T> S) {
             const int tnx = (S.lv[l].nx + kMgTile - 1) / kMgTile, tny = (S.lv[l].ny + kMgTile - 1) / kMgTile;
             for (int t = blockIdx.x; t < tnx * tny; t += gridDim.x)
                 down_tile(S.lv[l], S.lv[l + 1], S.omega, S.pre, t % tnx, t / tnx, smem);
-            if (!grid_barrier(S.bar, S.error)) return;
+            if (!grid_barrier(S.bar, S.error, seq++)) return;
         }
         if (blockIdx.x == 0) coarse_vcycle(S.coarse, smem);
-        if (!grid_barrier(S.bar, S.error)) return;
+        if (!grid_barrier(S.bar, S.error, seq++)) return;
         for (int l = S.Lp - 1; l >= 0; --l) {
             const int tnx = (S.lv[l].nx + kMgTile - 1) / kMgTile, tny = (S.lv[l].ny + kMgTile - 1) / kMgTile;
             for (int t = blockIdx.x; t < tnx * tny; t += gridDim.x)
                 up_tile(S.lv[l], S.lv[l + 1], S.omega, S.post, l == 0 ? S.phi : nullptr, t % tnx, t / tnx, smem);
-            if (!grid_barrier(S.bar, S.error)) return;
+            if (!grid_barrier(S.bar, S.error, seq++)) return;
         }
-        if (!r0_phase(S, r2, dummy)) return;
+        if (!r0_phase(S, r2, dummy, seq)) return;
         ++cycles;
         conv = r2 < S.tol2 * ref;
     }
@@ -861,7 +869,9 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
     if (st == PIC_OK) st = M.precision == PIC_MG_MIXED ? configure_kernels<float>(M) : configure_kernels<double>(M);
     if (st != PIC_OK) return bail(st);
     M.grd0 = dim3(div_up(nx, M.blk0.x), div_up(ny, M.blk0.y));
-    const int nb = int(M.grd0.x * M.grd0.y);
+    // block partials of the residual norm: one pair per block of the level-0
+    // tiling (k_mg_r0) or of the persistent grid (k_mg_solve), whichever is larger
+    const int nb = std::max(int(M.grd0.x * M.grd0.y), M.solve_grid);
     if (cudaMalloc(&M.N.partial, sizeof(double) * 2 * nb) != cudaSuccess)
         return bail(fail(PIC_ERR_CUDA, "pic_mg_create: out of device memory"));
     M.allocs.push_back(M.N.partial);
@@ -1047,11 +1057,15 @@ static int ensure_graph(MgImpl& M, double* phi, const double* f, double tol, int
 }
 
 int mg_read_info(MgImpl& M, pic_mg_info* info) {
-    unsigned char small[52];
+    unsigned char small[72];
     PIC_CUDA(cudaMemcpy(small, M.N.norms, sizeof small, cudaMemcpyDeviceToHost));
-    int err = 0;
-    memcpy(&err, small + 48, 4);
-    if (err) return fail(PIC_ERR_TIMEOUT, "multigrid: a grid barrier of the persistent solve timed out");
+    int err[6];
+    memcpy(err, small + 48, sizeof err);
+    if (err[0])
+        return fail(PIC_ERR_TIMEOUT,
+                    "multigrid: grid barrier %d of the persistent solve timed out (block %d saw count %d, "
+                    "generation %d, waited on %d)",
+                    err[1], err[2], err[3], err[4], err[5]);
     double norms[2];
     int conv, cycles;
     memcpy(norms, small, 16);

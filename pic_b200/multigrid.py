@@ -24,7 +24,7 @@ from . import _lib
 
 class MultigridSolver:
     def __init__(self, bc_mask, nx, ny, h, levels=4, omega=1.0, precision="mixed", pre_sweeps=2, post_sweeps=2,
-                 hy=None, launch="persistent"):
+                 hy=None, launch="graph"):
         self.nx, self.ny = int(nx), int(ny)
         self.h = float(h)
         self.hy = float(h if hy is None else hy)
