@@ -171,6 +171,22 @@ int pic_sort(pic_sorter* s, const float* d_x, const float* d_y, const float* d_v
              const float* d_vz, int n, float* d_x_out, float* d_y_out, float* d_vx_out, float* d_vy_out,
              float* d_vz_out, uint32_t* d_perm, int* d_count_out, int* d_tile_start, void* stream);
 
+/* The cell sort of pic_sort without allocation.  No counterpart in the
+ * reference: it serves callers that must not allocate device memory.  Its
+ * scratch is a fixed device array sized for PIC_SORT_STATIC_MAX particles
+ * (about 16 MiB, held by every GPU that loads the library until the process
+ * exits); n above that is rejected with PIC_ERR_BAD_ARG.  nx, ny and tile
+ * are the arguments of pic_sorter_create; the rest, and the results, are
+ * those of pic_sort.  Every call shares the array, which keeps the last
+ * call's contents, so calls that overlap on the GPU race.  The first call on
+ * a device (with that device current) looks up the array's address; make it
+ * before any stream capture. */
+#define PIC_SORT_STATIC_MAX (1 << 20)
+int pic_sort_static(const float* d_x, const float* d_y, const float* d_vx, const float* d_vy, const float* d_vz,
+                    int n, int nx, int ny, int tile, float* d_x_out, float* d_y_out, float* d_vx_out,
+                    float* d_vy_out, float* d_vz_out, uint32_t* d_perm, int* d_count_out, int* d_tile_start,
+                    void* stream);
+
 /* ------------------------------------------------------------------ */
 /* Null-collision Monte-Carlo collisions (src/MCC.py:308-415)          */
 /* ------------------------------------------------------------------ */

@@ -122,6 +122,7 @@ SIGNATURES = {
     "pic_sorter_create": [_i, _i, _i, _i, C.POINTER(_vp)],
     "pic_sorter_destroy": [_vp],
     "pic_sort": [_vp, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "pic_sort_static": [_vp, _vp, _vp, _vp, _vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "pic_mcc_create": [C.POINTER(MccDesc), _i, C.POINTER(_d), _d, C.POINTER(_vp)],
     "pic_mcc_destroy": [_vp],
     "pic_mcc_query": [_vp, _i, C.POINTER(_d), C.POINTER(_d), C.POINTER(_d)],

@@ -9,6 +9,7 @@
 //             index order), scattered to their global slots
 // Dead particles (NaN position) get the largest key and are dropped.
 #include <algorithm>
+#include <atomic>
 #include <vector>
 
 #include "sort_internal.cuh"
@@ -301,6 +302,42 @@ int sort_run(SortImpl& S, const int* d_n, const float* x, const float* y, const 
     return PIC_OK;
 }
 
+// ---- sort without allocation: scratch in a fixed device array -----------------------
+//
+// pic_sort_static keeps its scratch (key and slot ping-pong buffers, the
+// digit-count table and the count pair) in one file-scope device array of
+// kStaticSortBytes, which every GPU that loads the library holds until the
+// process exits.  Every call shares it: calls that overlap on the GPU race.
+// The first call on a device, with that device current, looks up the array's
+// address (cudaGetSymbolAddress) and caches it; that first call should come
+// before any stream capture.
+constexpr int kStaticSortCtas = 256;  // upper bound of the radix passes' CTA count
+constexpr size_t kStaticSortKeyBytes = sizeof(uint32_t) * size_t(PIC_SORT_STATIC_MAX);
+constexpr size_t kStaticSortCntBytes = sizeof(int) * size_t(kRadix) * kStaticSortCtas;
+constexpr size_t kStaticSortBytes = 4 * kStaticSortKeyBytes + kStaticSortCntBytes + 256;
+
+static __device__ __align__(256) unsigned char g_sort_scratch[kStaticSortBytes];
+
+constexpr int kStaticMaxDevices = 64;
+static std::atomic<unsigned char*> g_sort_scratch_ptr[kStaticMaxDevices];
+
+// Address of this device's scratch array (looked up once per device).
+static int static_scratch(unsigned char** out) {
+    int dev = 0;
+    PIC_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kStaticMaxDevices)
+        return fail(PIC_ERR_BAD_ARG, "pic_sort_static: device %d beyond the supported %d", dev, kStaticMaxDevices);
+    unsigned char* p = g_sort_scratch_ptr[dev].load(std::memory_order_acquire);
+    if (!p) {
+        void* addr = nullptr;
+        PIC_CUDA(cudaGetSymbolAddress(&addr, g_sort_scratch));
+        p = static_cast<unsigned char*>(addr);
+        g_sort_scratch_ptr[dev].store(p, std::memory_order_release);
+    }
+    *out = p;
+    return PIC_OK;
+}
+
 }  // namespace pic
 
 struct pic_sorter {
@@ -346,6 +383,49 @@ int pic_sort(pic_sorter* s, const float* d_x, const float* d_y, const float* d_v
     // sort_run copies the count from a device int; n_dev itself holds it here
     return sort_run(s->s, s->s.n_dev, d_x, d_y, d_vx, d_vy, d_vz, d_x_out, d_y_out, d_vx_out, d_vy_out, d_vz_out,
                     d_perm, d_count_out, d_tile_start, st);
+}
+
+int pic_sort_static(const float* d_x, const float* d_y, const float* d_vx, const float* d_vy, const float* d_vz,
+                    int n, int nx, int ny, int tile, float* d_x_out, float* d_y_out, float* d_vx_out,
+                    float* d_vy_out, float* d_vz_out, uint32_t* d_perm, int* d_count_out, int* d_tile_start,
+                    void* stream) {
+    clear_error();
+    if (n < 0 || n > PIC_SORT_STATIC_MAX)
+        return fail(PIC_ERR_BAD_ARG, "pic_sort_static: n=%d outside [0, %d] (the fixed scratch holds %d slots)", n,
+                    PIC_SORT_STATIC_MAX, PIC_SORT_STATIC_MAX);
+    if (!d_x || !d_y || nx < 2 || ny < 2 || tile < 1)
+        return fail(PIC_ERR_BAD_ARG, "pic_sort_static: bad arguments");
+    if (d_x_out && (!d_y_out || !d_vx_out || !d_vy_out || !d_vx || !d_vy || (d_vz && !d_vz_out)))
+        return fail(PIC_ERR_BAD_ARG, "pic_sort_static: output arrays incomplete");
+    // the same geometry and pass count as sorter_create, without its allocations
+    SortImpl S;
+    S.capacity = std::max(n, 1);
+    S.nx = nx;
+    S.ny = ny;
+    S.tile = tile;
+    S.tiles_x = (nx - 1 + tile - 1) / tile;
+    S.tiles_y = (ny - 1 + tile - 1) / tile;
+    S.ntiles = S.tiles_x * S.tiles_y;
+    const unsigned long long nkeys = (unsigned long long)S.ntiles * tile * tile;
+    if (nkeys >= 0xffffffffull) return fail(PIC_ERR_BAD_ARG, "pic_sort_static: grid too large for 32-bit keys");
+    S.dead_key = uint32_t(nkeys);
+    int bits = 0;
+    while ((1ull << bits) <= nkeys) ++bits;
+    S.passes = (bits + 7) / 8;
+    S.G = std::max(1, std::min(std::min(num_sms(), kStaticSortCtas), div_up(S.capacity, kSortSub)));
+    unsigned char* base = nullptr;
+    PIC_TRY(static_scratch(&base));
+    S.k0 = reinterpret_cast<uint32_t*>(base);
+    S.k1 = reinterpret_cast<uint32_t*>(base + kStaticSortKeyBytes);
+    S.v0 = reinterpret_cast<uint32_t*>(base + 2 * kStaticSortKeyBytes);
+    S.v1 = reinterpret_cast<uint32_t*>(base + 3 * kStaticSortKeyBytes);
+    S.cnt = reinterpret_cast<int*>(base + 4 * kStaticSortKeyBytes);
+    S.n_dev = reinterpret_cast<int*>(base + 4 * kStaticSortKeyBytes + kStaticSortCntBytes);
+    cudaStream_t st = as_stream(stream);
+    // n_dev = {n, 0}: the live count starts at zero whatever the last call left
+    k_set_n<<<1, 1, 0, st>>>(S.n_dev, n);
+    return sort_run(S, S.n_dev, d_x, d_y, d_vx, d_vy, d_vz, d_x_out, d_y_out, d_vx_out, d_vy_out, d_vz_out, d_perm,
+                    d_count_out, d_tile_start, st);
 }
 
 }  // extern "C"
