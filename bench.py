@@ -133,7 +133,7 @@ def peak_hbm():
 
 def ncu_traffic():
     """DRAM bytes per k_push launch from the committed ncu summary (profiles/), or None."""
-    p = os.path.join(ROOT, "profiles", "k_push_traffic.txt")
+    p = os.path.join(ROOT, "profiles", "k_push_mcc_513x513_8M.md")
     try:
         for line in open(p):
             if line.startswith("bytes_per_launch:"):
