@@ -170,6 +170,22 @@ def live_count(sim):
     return sum(sim.counters()["count"])
 
 
+def reduce_replicas(ms, work, world, device):
+    """Whole-job throughput of independent replicas: the work (particle-steps)
+    summed over ranks divided by the slowest rank's time.  Returns
+    (units per second, max ms)."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    w = torch.tensor([work], device=device, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(w)
+    ms_max = float(t.item())
+    return float(w.item()) / (ms_max / 1e3), ms_max
+
+
 def time_steps(sim, K, world):
     """K steps timed with CUDA events on the launching stream (the captured-graph path),
     then K more steps with per-phase event timing (the same kernels launched one by one)."""
@@ -218,14 +234,7 @@ def run_ours(args, world, rank, local):
     with ClockSampler(local) as clk:
         ms, prof, launches, n0, n1 = time_steps(sim, args.steps, world)
     clocks = clk.summary()
-    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    work = torch.tensor([0.5 * (n0 + n1) * args.steps], device="cuda", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(work)
-    value = float(work.item()) / (ms_max / 1e3)
+    value, ms_max = reduce_replicas(ms, 0.5 * (n0 + n1) * args.steps, world, "cuda")
     counters = sim.counters()
 
     # roofline of the fused particle kernel: x, y, vx, vy read and written

@@ -37,7 +37,8 @@ namespace pic {
 int grid_blocks(long n, int threads);
 
 constexpr int kMgTile = 32;
-constexpr int kMgThreads = 256;
+constexpr int kMgThreads = 512;
+constexpr int kMgMaxSweeps = 8;
 constexpr int kMgMaxCoarseLevels = 8;
 constexpr int kCoarseThreads = 1024;
 constexpr long kCoarseMaxNodes32 = 65L * 65L;    // FP32 levels at or below this size run in the single-CTA kernel
@@ -69,15 +70,32 @@ struct CoarseDesc {
 };
 
 // ---- shared-memory tile smoothing -------------------------------------------------
+//
+// Tile kernels are instantiated per sweep count S (1..kMgMaxSweeps), so the
+// tile width W is a compile-time constant: index arithmetic becomes
+// multiply-shift, and every global load of a phase is issued before the first
+// one is used.
+
+template <int S>
+struct DownGeom {
+    static constexpr int H = 2 * S + 2, W = kMgTile + 2 * H;
+};
+template <int S>
+struct UpGeom {
+    static constexpr int H = 2 * S, W = kMgTile + 2 * H, CW = W / 2 + 2;
+};
 
 // One red or black half-sweep over the nodes 1..W-2 of a W x W shared tile;
 // `par` selects the nodes whose local (li + lj) parity equals it.
-template <class T>
+template <class T, int W>
 __device__ __forceinline__ void tile_half_sweep(T* __restrict__ se, const T* __restrict__ sg,
-                                                const uint8_t* __restrict__ sm, int W, int par, T cx, T cy, T inv_diag,
-                                                T omega, int nthreads, int tid) {
-    const int half = W / 2;
-    for (int q = tid; q < half * W; q += nthreads) {
+                                                const uint8_t* __restrict__ sm, int par, T cx, T cy, T inv_diag,
+                                                T omega) {
+    constexpr int half = W / 2, N = half * W, IT = (N + kMgThreads - 1) / kMgThreads;
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int q = it * kMgThreads + int(threadIdx.x);
+        if (q >= N) break;
         const int lj = q / half;
         const int li = 2 * (q - lj * half) + ((par + lj) & 1);
         if (lj < 1 || lj > W - 2 || li < 1 || li > W - 2) continue;
@@ -91,47 +109,74 @@ __device__ __forceinline__ void tile_half_sweep(T* __restrict__ se, const T* __r
 }
 
 // Loads level L over the W x W region at (ox, oy): mask (edges and outside
-// the grid count as Dirichlet), g, and e (zero or the stored correction).
-template <class T>
-__device__ __forceinline__ void tile_load(const LevelDev<T>& L, int ox, int oy, int W, T* se, T* sg, uint8_t* sm,
-                                          bool load_e, int nthreads, int tid) {
-    for (int q = tid; q < W * W; q += nthreads) {
-        const int li = q % W, lj = q / W;
-        const int i = ox + li, j = oy + lj;
-        const bool inside = i >= 0 && j >= 0 && i < L.nx && j < L.ny;
+// the grid count as Dirichlet), g, and e (zero, or the stored correction on
+// free nodes).
+template <class T, int W, bool LOAD_E>
+__device__ __forceinline__ void tile_load(const LevelDev<T>& L, int ox, int oy, T* __restrict__ se,
+                                          T* __restrict__ sg, uint8_t* __restrict__ sm) {
+    constexpr int N = W * W, IT = (N + kMgThreads - 1) / kMgThreads;
+    uint8_t mk[IT];
+    T gv[IT], ev[IT];
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int q = it * kMgThreads + int(threadIdx.x);
+        const int i = ox + q % W, j = oy + q / W;
+        const bool in = q < N && i >= 0 && j >= 0 && i < L.nx && j < L.ny;
         const long k = long(j) * L.nx + i;
-        const bool fr = inside && i > 0 && j > 0 && i < L.nx - 1 && j < L.ny - 1 && !L.mask[k];
+        mk[it] = in ? L.mask[k] : uint8_t(1);
+        gv[it] = in ? L.g[k] : T(0);
+        ev[it] = (LOAD_E && in) ? L.e[k] : T(0);
+    }
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int q = it * kMgThreads + int(threadIdx.x);
+        if (q >= N) break;
+        const int i = ox + q % W, j = oy + q / W;
+        const bool fr = i > 0 && j > 0 && i < L.nx - 1 && j < L.ny - 1 && !mk[it];
         sm[q] = fr ? 0 : 1;
-        sg[q] = inside ? L.g[k] : T(0);
-        se[q] = (fr && load_e) ? L.e[k] : T(0);
+        sg[q] = gv[it];
+        se[q] = fr ? ev[it] : T(0);
     }
 }
 
-template <class T>
-__device__ void down_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, int pre, int tx, int ty,
+template <class T, int S>
+__device__ void down_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, int tx, int ty,
                           unsigned char* smem) {
-    const int H = 2 * pre + 2, W = kMgTile + 2 * H;
+    constexpr int H = DownGeom<S>::H, W = DownGeom<S>::W, hx = kMgTile / 2;
+    static_assert(hx * hx <= kMgThreads, "one coarse node per thread");
     T* se = reinterpret_cast<T*>(smem);
     T* sg = se + W * W;
     uint8_t* sm = reinterpret_cast<uint8_t*>(sg + W * W);
     const int x0 = tx * kMgTile, y0 = ty * kMgTile;
     const int ox = x0 - H, oy = y0 - H;
     const int tid = threadIdx.x;
-    tile_load(F, ox, oy, W, se, sg, sm, false, kMgThreads, tid);
+    // the coarse node this thread restricts to, and its mask (loaded early)
+    const int I = x0 / 2 + tid % hx, J = y0 / 2 + tid / hx;
+    const bool own = tid < hx * hx && I < Cc.nx && J < Cc.ny;
+    const long K = long(J) * Cc.nx + I;
+    const bool cdir = own && (I == 0 || J == 0 || I == Cc.nx - 1 || J == Cc.ny - 1 || Cc.mask[K]);
+    tile_load<T, W, false>(F, ox, oy, se, sg, sm);
     __syncthreads();
     // global red nodes have (i + j) even; locally (li + lj + ox + oy) even
     const int par0 = (ox + oy) & 1;
-    for (int s = 0; s < pre; ++s)
+#pragma unroll 1
+    for (int s = 0; s < S; ++s)
+#pragma unroll
         for (int color = 0; color < 2; ++color) {
-            tile_half_sweep(se, sg, sm, W, color ^ par0, F.cx, F.cy, F.inv_diag, omega, kMgThreads, tid);
+            tile_half_sweep<T, W>(se, sg, sm, color ^ par0, F.cx, F.cy, F.inv_diag, omega);
             __syncthreads();
         }
+#pragma unroll
     for (int q = tid; q < kMgTile * kMgTile; q += kMgThreads) {
         const int i = x0 + q % kMgTile, j = y0 + q / kMgTile;
         if (i < F.nx && j < F.ny) F.e[long(j) * F.nx + i] = se[(H + q / kMgTile) * W + H + q % kMgTile];
     }
     // residual in place of g (each node reads only its own g)
-    for (int q = tid; q < W * W; q += kMgThreads) {
+    constexpr int IT = (W * W + kMgThreads - 1) / kMgThreads;
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int q = it * kMgThreads + tid;
+        if (q >= W * W) break;
         const int li = q % W, lj = q / W;
         if (li < 1 || lj < 1 || li > W - 2 || lj > W - 2 || sm[q]) continue;
         const T c = se[q];
@@ -140,92 +185,189 @@ __device__ void down_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, 
     }
     __syncthreads();
     // full weighting onto the coarse nodes injected from this tile
-    const int hx = kMgTile / 2;
-    for (int q = tid; q < hx * hx; q += kMgThreads) {
-        const int I = x0 / 2 + q % hx, J = y0 / 2 + q / hx;
-        if (I >= Cc.nx || J >= Cc.ny) continue;
-        const long K = long(J) * Cc.nx + I;
-        if (I == 0 || J == 0 || I == Cc.nx - 1 || J == Cc.ny - 1 || Cc.mask[K]) {
+    if (own) {
+        if (cdir) {
             Cc.g[K] = T(0);
-            continue;
+        } else {
+            const int p = (2 * J - oy) * W + (2 * I - ox);
+            auto r = [&](int o) { return sm[p + o] ? T(0) : sg[p + o]; };
+            T v = T(0.25) * r(0);
+            v += T(0.125) * (r(-1) + r(1) + r(-W) + r(W));
+            v += T(0.0625) * (r(-W - 1) + r(-W + 1) + r(W - 1) + r(W + 1));
+            Cc.g[K] = v;
         }
-        const int p = (2 * J - oy) * W + (2 * I - ox);
-        auto r = [&](int o) { return sm[p + o] ? T(0) : sg[p + o]; };
-        T v = T(0.25) * r(0);
-        v += T(0.125) * (r(-1) + r(1) + r(-W) + r(W));
-        v += T(0.0625) * (r(-W - 1) + r(-W + 1) + r(W - 1) + r(W + 1));
-        Cc.g[K] = v;
     }
     __syncthreads();  // the caller may reuse the shared tile
 }
 
-template <class T>
-__global__ void __launch_bounds__(kMgThreads) k_mg_down(LevelDev<T> F, LevelDev<T> Cc, T omega, int pre) {
+template <class T, int S>
+__global__ void __launch_bounds__(kMgThreads) k_mg_down(LevelDev<T> F, LevelDev<T> Cc, T omega) {
     extern __shared__ __align__(16) unsigned char smem[];
-    down_tile(F, Cc, omega, pre, blockIdx.x, blockIdx.y, smem);
+    down_tile<T, S>(F, Cc, omega, blockIdx.x, blockIdx.y, smem);
 }
 
-template <class T>
-__device__ void up_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, int post, double* __restrict__ phi,
-                        int tx, int ty, unsigned char* smem) {
-    const int H = 2 * post, W = kMgTile + 2 * H;
+template <class T, int S>
+__device__ void up_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, double* __restrict__ phi, int tx,
+                        int ty, unsigned char* smem) {
+    constexpr int H = UpGeom<S>::H, W = UpGeom<S>::W, CW = UpGeom<S>::CW;
+    constexpr int CIT = (CW * CW + kMgThreads - 1) / kMgThreads;
+    constexpr int OIT = (kMgTile * kMgTile + kMgThreads - 1) / kMgThreads;
     T* se = reinterpret_cast<T*>(smem);
     T* sg = se + W * W;
-    uint8_t* sm = reinterpret_cast<uint8_t*>(sg + W * W);
+    T* sc = sg + W * W;
+    uint8_t* sm = reinterpret_cast<uint8_t*>(sc + CW * CW);
     const int x0 = tx * kMgTile, y0 = ty * kMgTile;
     const int ox = x0 - H, oy = y0 - H;
+    const int cox = ox >> 1, coy = oy >> 1;  // floor for negative origins
     const int tid = threadIdx.x;
-    tile_load(F, ox, oy, W, se, sg, sm, true, kMgThreads, tid);
+    // every global load of this tile is issued up front: the coarse
+    // correction, phi of the core (level 0), then the fine tile
+    T cv[CIT];
+#pragma unroll
+    for (int it = 0; it < CIT; ++it) {
+        const int q = it * kMgThreads + tid;
+        const int I = cox + q % CW, J = coy + q / CW;
+        const bool in = q < CW * CW && I >= 0 && J >= 0 && I < Cc.nx && J < Cc.ny;
+        cv[it] = in ? Cc.e[long(J) * Cc.nx + I] : T(0);
+    }
+    double pv[OIT];
+#pragma unroll
+    for (int it = 0; it < OIT; ++it) {
+        const int q = it * kMgThreads + tid;
+        const int i = x0 + q % kMgTile, j = y0 + q / kMgTile;
+        pv[it] = (phi && i < F.nx && j < F.ny) ? phi[long(j) * F.nx + i] : 0.0;
+    }
+    tile_load<T, W, true>(F, ox, oy, se, sg, sm);
+#pragma unroll
+    for (int it = 0; it < CIT; ++it) {
+        const int q = it * kMgThreads + tid;
+        if (q < CW * CW) sc[q] = cv[it];
+    }
     __syncthreads();
     // bilinear prolongation of the coarse correction, added on free nodes
-    for (int q = tid; q < W * W; q += kMgThreads) {
+    constexpr int IT = (W * W + kMgThreads - 1) / kMgThreads;
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int q = it * kMgThreads + tid;
+        if (q >= W * W) break;
         if (sm[q]) continue;
         const int i = ox + q % W, j = oy + q / W;
-        const int I = i >> 1, J = j >> 1;
-        const long K = long(J) * Cc.nx + I;
-        const T* ec = Cc.e;
+        const int c = ((j >> 1) - coy) * CW + ((i >> 1) - cox);
         T v;
-        if (!(i & 1) && !(j & 1)) v = ec[K];
-        else if ((i & 1) && !(j & 1)) v = T(0.5) * (ec[K] + ec[K + 1]);
-        else if (!(i & 1) && (j & 1)) v = T(0.5) * (ec[K] + ec[K + Cc.nx]);
-        else v = T(0.25) * (ec[K] + ec[K + 1] + ec[K + Cc.nx] + ec[K + Cc.nx + 1]);
+        if (!(i & 1) && !(j & 1)) v = sc[c];
+        else if ((i & 1) && !(j & 1)) v = T(0.5) * (sc[c] + sc[c + 1]);
+        else if (!(i & 1) && (j & 1)) v = T(0.5) * (sc[c] + sc[c + CW]);
+        else v = T(0.25) * (sc[c] + sc[c + 1] + sc[c + CW] + sc[c + CW + 1]);
         se[q] += v;
     }
     __syncthreads();
     const int par0 = (ox + oy) & 1;
-    for (int s = 0; s < post; ++s)
+#pragma unroll 1
+    for (int s = 0; s < S; ++s)
+#pragma unroll
         for (int color = 0; color < 2; ++color) {
-            tile_half_sweep(se, sg, sm, W, color ^ par0, F.cx, F.cy, F.inv_diag, omega, kMgThreads, tid);
+            tile_half_sweep<T, W>(se, sg, sm, color ^ par0, F.cx, F.cy, F.inv_diag, omega);
             __syncthreads();
         }
-    for (int q = tid; q < kMgTile * kMgTile; q += kMgThreads) {
+#pragma unroll
+    for (int it = 0; it < OIT; ++it) {
+        const int q = it * kMgThreads + tid;
         const int i = x0 + q % kMgTile, j = y0 + q / kMgTile;
-        if (i >= F.nx || j >= F.ny) continue;
+        if (q >= kMgTile * kMgTile || i >= F.nx || j >= F.ny) continue;
         const long k = long(j) * F.nx + i;
         const T v = se[(H + q / kMgTile) * W + H + q % kMgTile];
-        if (phi) phi[k] += double(v);
+        if (phi) phi[k] = pv[it] + double(v);
         else F.e[k] = v;
     }
     __syncthreads();  // the caller may reuse the shared tile
 }
 
-template <class T>
-__global__ void __launch_bounds__(kMgThreads) k_mg_up(LevelDev<T> F, LevelDev<T> Cc, T omega, int post,
+template <class T, int S>
+__global__ void __launch_bounds__(kMgThreads) k_mg_up(LevelDev<T> F, LevelDev<T> Cc, T omega,
                                                       double* __restrict__ phi) {
     extern __shared__ __align__(16) unsigned char smem[];
-    up_tile(F, Cc, omega, post, phi, blockIdx.x, blockIdx.y, smem);
+    up_tile<T, S>(F, Cc, omega, phi, blockIdx.x, blockIdx.y, smem);
+}
+
+// Runtime sweep counts (the persistent kernel) dispatched to the instances.
+template <class T>
+__device__ void down_tile_n(int pre, const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, int tx, int ty,
+                            unsigned char* smem) {
+    switch (pre) {
+        case 1: down_tile<T, 1>(F, Cc, omega, tx, ty, smem); break;
+        case 2: down_tile<T, 2>(F, Cc, omega, tx, ty, smem); break;
+        case 3: down_tile<T, 3>(F, Cc, omega, tx, ty, smem); break;
+        case 4: down_tile<T, 4>(F, Cc, omega, tx, ty, smem); break;
+        case 5: down_tile<T, 5>(F, Cc, omega, tx, ty, smem); break;
+        case 6: down_tile<T, 6>(F, Cc, omega, tx, ty, smem); break;
+        case 7: down_tile<T, 7>(F, Cc, omega, tx, ty, smem); break;
+        default: down_tile<T, 8>(F, Cc, omega, tx, ty, smem); break;
+    }
+}
+
+template <class T>
+__device__ void up_tile_n(int post, const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, double* phi, int tx,
+                          int ty, unsigned char* smem) {
+    switch (post) {
+        case 1: up_tile<T, 1>(F, Cc, omega, phi, tx, ty, smem); break;
+        case 2: up_tile<T, 2>(F, Cc, omega, phi, tx, ty, smem); break;
+        case 3: up_tile<T, 3>(F, Cc, omega, phi, tx, ty, smem); break;
+        case 4: up_tile<T, 4>(F, Cc, omega, phi, tx, ty, smem); break;
+        case 5: up_tile<T, 5>(F, Cc, omega, phi, tx, ty, smem); break;
+        case 6: up_tile<T, 6>(F, Cc, omega, phi, tx, ty, smem); break;
+        case 7: up_tile<T, 7>(F, Cc, omega, phi, tx, ty, smem); break;
+        default: up_tile<T, 8>(F, Cc, omega, phi, tx, ty, smem); break;
+    }
+}
+
+template <class T>
+using DownKernel = void (*)(LevelDev<T>, LevelDev<T>, T);
+template <class T>
+using UpKernel = void (*)(LevelDev<T>, LevelDev<T>, T, double*);
+
+template <class T>
+static DownKernel<T> down_kernel(int s) {
+    static const DownKernel<T> k[kMgMaxSweeps + 1] = {nullptr,         k_mg_down<T, 1>, k_mg_down<T, 2>,
+                                                      k_mg_down<T, 3>, k_mg_down<T, 4>, k_mg_down<T, 5>,
+                                                      k_mg_down<T, 6>, k_mg_down<T, 7>, k_mg_down<T, 8>};
+    return k[s];
+}
+
+template <class T>
+static UpKernel<T> up_kernel(int s) {
+    static const UpKernel<T> k[kMgMaxSweeps + 1] = {nullptr,       k_mg_up<T, 1>, k_mg_up<T, 2>, k_mg_up<T, 3>,
+                                                    k_mg_up<T, 4>, k_mg_up<T, 5>, k_mg_up<T, 6>, k_mg_up<T, 7>,
+                                                    k_mg_up<T, 8>};
+    return k[s];
+}
+
+template <class T>
+static size_t down_smem(int s) {
+    const size_t W = kMgTile + 2 * (2 * s + 2);
+    return W * W * (2 * sizeof(T) + 1);
+}
+
+template <class T>
+static size_t up_smem(int s) {
+    const size_t W = kMgTile + 2 * (2 * s), CW = W / 2 + 2;
+    return W * W * (2 * sizeof(T) + 1) + CW * CW * sizeof(T);
 }
 
 // ---- single-CTA V-cycle of the coarse levels --------------------------------------
+
+// q / d for 0 <= q < 2^22 from a float reciprocal of d: (q + 1/2) / d lies at
+// least 1/(2d) from an integer and the two float roundings move it by less.
+__device__ __forceinline__ int div_small(int q, float inv_d) { return int((float(q) + 0.5f) * inv_d); }
 
 template <class T>
 __device__ void level_sweeps(T* se, const T* sg, const uint8_t* sm, const LevelDev<T>& L, T omega, int sweeps) {
     const int nx = L.nx, ny = L.ny;
     const int hx = (nx + 1) / 2;
+    const float inv_hx = 1.0f / float(hx);
     for (int s = 0; s < sweeps; ++s)
         for (int color = 0; color < 2; ++color) {
             for (int q = threadIdx.x; q < hx * ny; q += blockDim.x) {
-                const int j = q / hx;
+                const int j = div_small(q, inv_hx);
                 const int i = 2 * (q - j * hx) + ((color + j) & 1);
                 if (i >= nx) continue;
                 const int p = j * nx + i;
@@ -249,8 +391,9 @@ __device__ void coarse_vcycle(const CoarseDesc<T>& D, unsigned char* smem) {
         Gs[l] = reinterpret_cast<T*>(smem + D.off_g[l]);
         M[l] = smem + D.off_m[l];
         const LevelDev<T>& L = D.lv[l];
+        const float inv_nx = 1.0f / float(L.nx);
         for (int q = threadIdx.x; q < L.nx * L.ny; q += blockDim.x) {
-            const int i = q % L.nx, j = q / L.nx;
+            const int j = div_small(q, inv_nx), i = q - j * L.nx;
             M[l][q] = (i == 0 || j == 0 || i == L.nx - 1 || j == L.ny - 1 || L.mask[q]) ? 1 : 0;
             E[l][q] = T(0);
             if (l == 0) Gs[0][q] = L.g[q];
@@ -268,12 +411,13 @@ __device__ void coarse_vcycle(const CoarseDesc<T>& D, unsigned char* smem) {
         const T* g = Gs[l];
         const uint8_t* mk = M[l];
         const int nx = L.nx;
+        const float inv_cnx = 1.0f / float(C.nx);
         for (int Q = threadIdx.x; Q < C.nx * C.ny; Q += blockDim.x) {
             if (M[l + 1][Q]) {
                 Gs[l + 1][Q] = T(0);
                 continue;
             }
-            const int I = Q % C.nx, J = Q / C.nx;
+            const int J = div_small(Q, inv_cnx), I = Q - J * C.nx;
             const int p = 2 * J * nx + 2 * I;
             auto rr = [&](int o) {
                 const int q = p + o;
@@ -304,9 +448,10 @@ __device__ void coarse_vcycle(const CoarseDesc<T>& D, unsigned char* smem) {
     for (int l = last - 1; l >= 0; --l) {
         const LevelDev<T>& L = D.lv[l];
         const LevelDev<T>& C = D.lv[l + 1];
+        const float inv_nx = 1.0f / float(L.nx);
         for (int q = threadIdx.x; q < L.nx * L.ny; q += blockDim.x) {
             if (M[l][q]) continue;
-            const int i = q % L.nx, j = q / L.nx;
+            const int j = div_small(q, inv_nx), i = q - j * L.nx;
             const int K = (j >> 1) * C.nx + (i >> 1);
             const T* ec = E[l + 1];
             T v;
@@ -577,7 +722,7 @@ __global__ void __launch_bounds__(kMgThreads) k_mg_solve(SolveDesc<T> S) {
         for (int l = 0; l < S.Lp; ++l) {
             const int tnx = (S.lv[l].nx + kMgTile - 1) / kMgTile, tny = (S.lv[l].ny + kMgTile - 1) / kMgTile;
             for (int t = blockIdx.x; t < tnx * tny; t += gridDim.x)
-                down_tile(S.lv[l], S.lv[l + 1], S.omega, S.pre, t % tnx, t / tnx, smem);
+                down_tile_n(S.pre, S.lv[l], S.lv[l + 1], S.omega, t % tnx, t / tnx, smem);
             if (!grid_barrier(S.bar, S.error, seq++)) return;
         }
         if (blockIdx.x == 0) coarse_vcycle(S.coarse, smem);
@@ -585,7 +730,7 @@ __global__ void __launch_bounds__(kMgThreads) k_mg_solve(SolveDesc<T> S) {
         for (int l = S.Lp - 1; l >= 0; --l) {
             const int tnx = (S.lv[l].nx + kMgTile - 1) / kMgTile, tny = (S.lv[l].ny + kMgTile - 1) / kMgTile;
             for (int t = blockIdx.x; t < tnx * tny; t += gridDim.x)
-                up_tile(S.lv[l], S.lv[l + 1], S.omega, S.post, l == 0 ? S.phi : nullptr, t % tnx, t / tnx, smem);
+                up_tile_n(S.post, S.lv[l], S.lv[l + 1], S.omega, l == 0 ? S.phi : nullptr, t % tnx, t / tnx, smem);
             if (!grid_barrier(S.bar, S.error, seq++)) return;
         }
         if (!r0_phase(S, r2, dummy, seq)) return;
@@ -708,19 +853,15 @@ static bool invert(std::vector<double>& a, int n) {
 }
 
 template <class T>
-static size_t tile_smem(int halo) {
-    const int W = kMgTile + 2 * halo;
-    return size_t(W) * W * (2 * sizeof(T) + 1);
-}
-
-template <class T>
 static int configure_kernels(MgImpl& M) {
-    const size_t down = tile_smem<T>(2 * M.o.pre_sweeps + 2), up = tile_smem<T>(2 * M.o.post_sweeps);
+    const size_t down = down_smem<T>(M.o.pre_sweeps), up = up_smem<T>(M.o.post_sweeps);
     if (down > 227 * 1024 || up > 227 * 1024 || M.coarse_smem > 227 * 1024)
         return fail(PIC_ERR_BAD_ARG, "multigrid: shared memory too large (sweeps %d/%d)", M.o.pre_sweeps,
                     M.o.post_sweeps);
-    PIC_CUDA(cudaFuncSetAttribute(k_mg_down<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(down)));
-    PIC_CUDA(cudaFuncSetAttribute(k_mg_up<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(up)));
+    PIC_CUDA(cudaFuncSetAttribute(down_kernel<T>(M.o.pre_sweeps), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(down)));
+    PIC_CUDA(cudaFuncSetAttribute(up_kernel<T>(M.o.post_sweeps), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(up)));
     PIC_CUDA(cudaFuncSetAttribute(k_mg_coarse<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(M.coarse_smem)));
     M.solve_smem = std::max(std::max(down, up), M.coarse2_smem);
     PIC_CUDA(cudaFuncSetAttribute(k_mg_solve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(M.solve_smem)));
@@ -766,7 +907,7 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
     };
     if (M.o.precision != PIC_MG_MIXED && M.o.precision != PIC_MG_FP64)
         return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: unknown precision %d", M.o.precision));
-    if (M.o.pre_sweeps > 8 || M.o.post_sweeps > 8)
+    if (M.o.pre_sweeps > kMgMaxSweeps || M.o.post_sweeps > kMgMaxSweeps)
         return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: at most 8 pre/post sweeps"));
     if (M.o.launch_mode < PIC_MG_PERSISTENT || M.o.launch_mode > PIC_MG_GRAPH_LOOP)
         return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: unknown launch mode %d", M.o.launch_mode));
@@ -898,11 +1039,13 @@ template <class T>
 static int launch_cycle(MgImpl& M, std::vector<LevelDev<T>>& lv, double* phi, const double* f, double tol,
                         int max_cycles, cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st, int& count) {
     const T omega = T(M.o.omega);
-    const size_t down = tile_smem<T>(2 * M.o.pre_sweeps + 2), up = tile_smem<T>(2 * M.o.post_sweeps);
+    const size_t down = down_smem<T>(M.o.pre_sweeps), up = up_smem<T>(M.o.post_sweeps);
+    const DownKernel<T> kdown = down_kernel<T>(M.o.pre_sweeps);
+    const UpKernel<T> kup = up_kernel<T>(M.o.post_sweeps);
     count = 0;
     for (int l = 0; l < M.Lc; ++l) {
         const dim3 g(div_up(lv[l].nx, kMgTile), div_up(lv[l].ny, kMgTile));
-        k_mg_down<T><<<g, kMgThreads, down, st>>>(lv[l], lv[l + 1], omega, M.o.pre_sweeps);
+        kdown<<<g, kMgThreads, down, st>>>(lv[l], lv[l + 1], omega);
         ++count;
     }
     CoarseDesc<T> D{};
@@ -924,7 +1067,7 @@ static int launch_cycle(MgImpl& M, std::vector<LevelDev<T>>& lv, double* phi, co
     ++count;
     for (int l = M.Lc - 1; l >= 0; --l) {
         const dim3 g(div_up(lv[l].nx, kMgTile), div_up(lv[l].ny, kMgTile));
-        k_mg_up<T><<<g, kMgThreads, up, st>>>(lv[l], lv[l + 1], omega, M.o.post_sweeps, l == 0 ? phi : nullptr);
+        kup<<<g, kMgThreads, up, st>>>(lv[l], lv[l + 1], omega, l == 0 ? phi : nullptr);
         ++count;
     }
     k_mg_r0<T><<<M.grd0, M.blk0, 0, st>>>(phi, f, lv[0].mask, M.nx, M.ny, 1.0 / (M.dx * M.dx), 1.0 / (M.dy * M.dy),
