@@ -339,6 +339,31 @@ int pic_sim_set_profiling(pic_sim* sim, int enable);
 /* Synchronises the device and sums the recorded intervals. */
 int pic_sim_read_profile(pic_sim* sim, pic_sim_profile* out);
 
+/* ------------------------------------------------------------------ */
+/* Ensembles of independent simulations                                */
+/* ------------------------------------------------------------------ */
+
+/* Many independent simulations stepped together: one CUDA graph holds a step
+ * of every member as independent branches, and a conditional WHILE node
+ * repeats it, so that n steps of the whole ensemble are one graph launch.
+ * Each member's cell sort sits under a conditional IF node that fires when
+ * the member's own step count is a multiple of its sort interval; each
+ * member's multigrid loop is a nested conditional WHILE node.  Members may
+ * differ in grid size, particle counts, tile, sort interval and multigrid
+ * options, keep their own state, and must have been created with use_graph
+ * and a graph multigrid launch mode, then loaded and initialised.  The
+ * reference runs one simulation per process (src/simulation.py:562-567);
+ * this has no single counterpart there.  Members stay owned by the caller
+ * and must outlive the ensemble. */
+typedef struct pic_ens pic_ens;
+int pic_ens_create(pic_sim* const* sims, int n, pic_ens** out);
+int pic_ens_destroy(pic_ens* e);
+/* n steps of every member, asynchronous on `stream`: one graph launch.  A
+ * member fresh from pic_sim_init takes its first step without the kick,
+ * which the graph does not hold, so while any member is fresh every member
+ * takes its first of the n steps eagerly. */
+int pic_ens_step(pic_ens* e, int n_steps, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -139,6 +139,9 @@ SIGNATURES = {
     "pic_sim_kernel_launches": [_vp],
     "pic_sim_set_profiling": [_vp, _i],
     "pic_sim_read_profile": [_vp, C.c_void_p],
+    "pic_ens_create": [C.POINTER(_vp), _i, C.POINTER(_vp)],
+    "pic_ens_destroy": [_vp],
+    "pic_ens_step": [_vp, _i, _vp],
 }
 _RESTYPE = {"pic_last_error": C.c_char_p, "pic_sim_kernel_launches": C.c_longlong}
 

@@ -39,6 +39,11 @@ inline int div_up(long a, long b) { return int((a + b - 1) / b); }
 
 int num_sms();
 
+// Raises a kernel's dynamic shared-memory limit to at least `bytes`.  The
+// limit is one process-wide attribute of the kernel, so objects that need
+// different sizes only ever raise it.
+int raise_smem_limit(const void* kernel, size_t bytes);
+
 // ---- CIC weights (FP32, explicit rounding so the CPU oracle matches bit for bit) ----
 
 struct Cic {

@@ -858,13 +858,11 @@ static int configure_kernels(MgImpl& M) {
     if (down > 227 * 1024 || up > 227 * 1024 || M.coarse_smem > 227 * 1024)
         return fail(PIC_ERR_BAD_ARG, "multigrid: shared memory too large (sweeps %d/%d)", M.o.pre_sweeps,
                     M.o.post_sweeps);
-    PIC_CUDA(cudaFuncSetAttribute(down_kernel<T>(M.o.pre_sweeps), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  int(down)));
-    PIC_CUDA(cudaFuncSetAttribute(up_kernel<T>(M.o.post_sweeps), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  int(up)));
-    PIC_CUDA(cudaFuncSetAttribute(k_mg_coarse<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(M.coarse_smem)));
+    PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(down_kernel<T>(M.o.pre_sweeps)), down));
+    PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(up_kernel<T>(M.o.post_sweeps)), up));
+    PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(k_mg_coarse<T>), M.coarse_smem));
     M.solve_smem = std::max(std::max(down, up), M.coarse2_smem);
-    PIC_CUDA(cudaFuncSetAttribute(k_mg_solve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(M.solve_smem)));
+    PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(k_mg_solve<T>), M.solve_smem));
     int per_sm = 0;
     PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mg_solve<T>, kMgThreads, M.solve_smem));
     if (per_sm < 1) return fail(PIC_ERR_CUDA, "multigrid: the persistent kernel does not fit on an SM");

@@ -33,6 +33,14 @@ int num_sms() {
     return sms;
 }
 
+int raise_smem_limit(const void* kernel, size_t bytes) {
+    cudaFuncAttributes a{};
+    PIC_CUDA(cudaFuncGetAttributes(&a, kernel));
+    if (size_t(a.maxDynamicSharedSizeBytes) < bytes)
+        PIC_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+    return PIC_OK;
+}
+
 // ---- kernels -------------------------------------------------------------------
 
 __global__ void k_update_R(float* __restrict__ x, float* __restrict__ y, const float* __restrict__ vx,

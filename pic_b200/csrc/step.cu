@@ -931,7 +931,7 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
     // launch shape of the particle pass
     S.push_smem = sizeof(float) * 2 * 4 * kBufStride + size_t(S.rw) * S.rw * (sizeof(float2) + sizeof(unsigned)) +
                   sizeof(unsigned) * 2 * kBitWords;
-    PIC_CUDA(cudaFuncSetAttribute(k_push, cudaFuncAttributeMaxDynamicSharedMemorySize, int(S.push_smem)));
+    PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(k_push), S.push_smem));
     int per_sm = 0;
     PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_push, kPushThreads, S.push_smem));
     S.push_grid = std::max(1, per_sm) * num_sms();
@@ -961,10 +961,190 @@ static void sim_free(SimImpl& S) {
     S.allocs.clear();
 }
 
+// ---- ensembles: many independent simulations in one graph --------------------------
+//
+// One CUDA graph holds a step of every member as independent branches and a
+// conditional WHILE node repeats it, so n steps of the whole ensemble are one
+// graph launch.  A member's branch:
+//     k_ens_sort_cond -> IF { cell sort } -> particle pass -> field solve
+//     (its multigrid loop is a nested WHILE node) -> k_ens_advance
+// The IF condition is the member's own step counter (on the device) modulo
+// its sort interval, so members with different intervals share one graph.
+
+struct EnsControl {
+    long long remaining;  // ensemble steps left in this launch
+};
+
+__global__ void k_ens_sort_cond(const long long* __restrict__ steps, int interval, cudaGraphConditionalHandle h) {
+    cudaGraphSetConditional(h, (interval > 0 && *steps % interval == 0) ? 1u : 0u);
+}
+
+__global__ void k_ens_advance(long long* steps) { *steps += 1; }
+
+__global__ void k_ens_loop(EnsControl* c, cudaGraphConditionalHandle h) {
+    c->remaining -= 1;
+    cudaGraphSetConditional(h, c->remaining > 0 ? 1u : 0u);
+}
+
+struct EnsImpl {
+    std::vector<SimImpl*> m;
+    std::vector<cudaStream_t> branch, side;
+    std::vector<cudaEvent_t> ev;
+    cudaStream_t cap = nullptr;
+    long long* d_steps = nullptr;
+    EnsControl* d_ctl = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<long long> per_step_launches;  // per member, without the sort
+    std::vector<long long> sort_launches;
+};
+
+// Adds, to the graph that st is capturing into, a conditional IF node whose
+// body is the member's cell sort, and moves st past it.
+static int capture_sort_if(SimImpl& S, long long* d_step, cudaStream_t st, cudaStream_t side) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    PIC_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
+    if (cs != cudaStreamCaptureStatusActive) return fail(PIC_ERR_BAD_ARG, "ensemble: stream is not capturing");
+    cudaGraphConditionalHandle h;
+    PIC_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+    k_ens_sort_cond<<<1, 1, 0, st>>>(d_step, S.d.sort_interval, h);
+    PIC_LAUNCH_CHECK();
+    PIC_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
+    cudaGraphNodeParams p{};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeIf;
+    p.conditional.size = 1;
+    cudaGraphNode_t cn;
+    PIC_CUDA(cudaGraphAddNode(&cn, g, deps, nd, &p));
+    cudaGraph_t body = p.conditional.phGraph_out[0];
+    PIC_CUDA(cudaStreamUpdateCaptureDependencies(st, &cn, 1, cudaStreamSetCaptureDependencies));
+    PIC_CUDA(cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    const int rc = sort_all(S, side);
+    cudaGraph_t out = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(side, &out);
+    if (rc != PIC_OK) return rc;
+    if (ec != cudaSuccess) return fail(PIC_ERR_CUDA, "ensemble sort capture: %s", cudaGetErrorString(ec));
+    return PIC_OK;
+}
+
+static int ens_capture_body(EnsImpl& E);
+
+static int ens_capture(EnsImpl& E) {
+    // launches are counted when the graph runs; phase timing stays out of graphs
+    std::vector<long long> l0, s0;
+    std::vector<bool> prof;
+    for (SimImpl* S : E.m) {
+        l0.push_back(S->launches);
+        s0.push_back(S->solves);
+        prof.push_back(S->profiling);
+        S->profiling = false;
+    }
+    const int rc = ens_capture_body(E);
+    for (size_t i = 0; i < E.m.size(); ++i) {
+        E.m[i]->launches = l0[i];
+        E.m[i]->solves = s0[i];
+        E.m[i]->profiling = prof[i];
+    }
+    return rc;
+}
+
+static int ens_capture_body(EnsImpl& E) {
+    const int n = int(E.m.size());
+    PIC_CUDA(cudaStreamBeginCapture(E.cap, cudaStreamCaptureModeThreadLocal));
+    int rc = PIC_OK;
+    cudaGraph_t g = nullptr;
+    do {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t top = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        if (cudaStreamGetCaptureInfo(E.cap, &cs, nullptr, &top, &deps, &nd) != cudaSuccess) {
+            rc = fail(PIC_ERR_CUDA, "ensemble: capture info");
+            break;
+        }
+        cudaGraphConditionalHandle h;
+        if (cudaGraphConditionalHandleCreate(&h, top, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
+            rc = fail(PIC_ERR_CUDA, "ensemble: conditional handle");
+            break;
+        }
+        cudaGraphNodeParams p{};
+        p.type = cudaGraphNodeTypeConditional;
+        p.conditional.handle = h;
+        p.conditional.type = cudaGraphCondTypeWhile;
+        p.conditional.size = 1;
+        cudaGraphNode_t cn;
+        if (cudaGraphAddNode(&cn, top, deps, nd, &p) != cudaSuccess ||
+            cudaStreamUpdateCaptureDependencies(E.cap, &cn, 1, cudaStreamSetCaptureDependencies) != cudaSuccess) {
+            rc = fail(PIC_ERR_CUDA, "ensemble: loop node");
+            break;
+        }
+        cudaGraph_t body = p.conditional.phGraph_out[0];
+        // the loop body is captured on branch 0's stream as the root, forked to every member
+        cudaStream_t root = E.side.back();
+        if (cudaStreamBeginCaptureToGraph(root, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) !=
+            cudaSuccess) {
+            rc = fail(PIC_ERR_CUDA, "ensemble: body capture");
+            break;
+        }
+        if (cudaEventRecord(E.ev[n], root) != cudaSuccess) rc = fail(PIC_ERR_CUDA, "ensemble: fork event");
+        for (int i = 0; i < n && rc == PIC_OK; ++i) {
+            SimImpl& S = *E.m[i];
+            cudaStream_t st = E.branch[i];
+            if (cudaStreamWaitEvent(st, E.ev[n], 0) != cudaSuccess) rc = fail(PIC_ERR_CUDA, "ensemble: fork wait");
+            if (rc == PIC_OK && S.d.sort_interval > 0) rc = capture_sort_if(S, E.d_steps + i, st, E.side[i]);
+            if (rc == PIC_OK) rc = particle_pass(S, st, 1, 1, 1, 1, 1.0, 1);
+            if (rc == PIC_OK) rc = field_solve(S, st, true);
+            if (rc == PIC_OK) {
+                k_ens_advance<<<1, 1, 0, st>>>(E.d_steps + i);
+                if (cudaEventRecord(E.ev[i], st) != cudaSuccess || cudaStreamWaitEvent(root, E.ev[i], 0) != cudaSuccess)
+                    rc = fail(PIC_ERR_CUDA, "ensemble: join of member %d", i);
+            }
+        }
+        if (rc == PIC_OK) k_ens_loop<<<1, 1, 0, root>>>(E.d_ctl, h);
+        cudaGraph_t body_out = nullptr;
+        const cudaError_t eb = cudaStreamEndCapture(root, &body_out);
+        if (rc == PIC_OK && eb != cudaSuccess) rc = fail(PIC_ERR_CUDA, "ensemble body: %s", cudaGetErrorString(eb));
+    } while (false);
+    const cudaError_t ec = cudaStreamEndCapture(E.cap, &g);
+    if (rc != PIC_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (ec != cudaSuccess) return fail(PIC_ERR_CUDA, "ensemble capture: %s", cudaGetErrorString(ec));
+    const cudaError_t ei = cudaGraphInstantiate(&E.exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) return fail(PIC_ERR_CUDA, "ensemble graph instantiate: %s", cudaGetErrorString(ei));
+    return PIC_OK;
+}
+
+static void ens_free(EnsImpl& E) {
+    if (E.exec) cudaGraphExecDestroy(E.exec);
+    E.exec = nullptr;
+    for (cudaStream_t s : E.branch) cudaStreamDestroy(s);
+    for (cudaStream_t s : E.side) cudaStreamDestroy(s);
+    for (cudaEvent_t e : E.ev) cudaEventDestroy(e);
+    E.branch.clear();
+    E.side.clear();
+    E.ev.clear();
+    if (E.cap) cudaStreamDestroy(E.cap);
+    E.cap = nullptr;
+    if (E.d_steps) cudaFree(E.d_steps);
+    if (E.d_ctl) cudaFree(E.d_ctl);
+    E.d_steps = nullptr;
+    E.d_ctl = nullptr;
+}
+
 }  // namespace pic
 
 struct pic_sim {
     pic::SimImpl s;
+};
+
+struct pic_ens {
+    pic::EnsImpl e;
 };
 
 using namespace pic;
@@ -1152,6 +1332,97 @@ int pic_sim_read_profile(pic_sim* sim, pic_sim_profile* out) {
         out->count[m.first] += 1;
     }
     out->mg_cycles = mg_total_cycles(S.mg) - S.prof_cycles;
+    return PIC_OK;
+}
+
+
+int pic_ens_create(pic_sim* const* sims, int n, pic_ens** out) {
+    clear_error();
+    if (!out || !sims || n < 1) return fail(PIC_ERR_BAD_ARG, "pic_ens_create: bad arguments");
+    for (int i = 0; i < n; ++i) {
+        if (!sims[i]) return fail(PIC_ERR_BAD_ARG, "pic_ens_create: member %d is NULL", i);
+        if (!sims[i]->s.d.use_graph || !mg_uses_graph(sims[i]->s.mg))
+            return fail(PIC_ERR_BAD_ARG, "pic_ens_create: member %d must use graphs (use_graph and a graph multigrid)", i);
+        for (int j = 0; j < i; ++j)
+            if (sims[j] == sims[i]) return fail(PIC_ERR_BAD_ARG, "pic_ens_create: member %d appears twice", i);
+    }
+    pic_ens* e = new pic_ens;
+    EnsImpl& E = e->e;
+    auto bail = [&](int code) {
+        ens_free(E);
+        delete e;
+        return code;
+    };
+    for (int i = 0; i < n; ++i) E.m.push_back(&sims[i]->s);
+    E.branch.resize(n);
+    E.side.resize(n + 1);
+    E.ev.resize(n + 1);
+    for (int i = 0; i < n; ++i)
+        if (cudaStreamCreateWithFlags(&E.branch[i], cudaStreamNonBlocking) != cudaSuccess)
+            return bail(fail(PIC_ERR_CUDA, "pic_ens_create: stream creation failed"));
+    for (int i = 0; i <= n; ++i)
+        if (cudaStreamCreateWithFlags(&E.side[i], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&E.ev[i], cudaEventDisableTiming) != cudaSuccess)
+            return bail(fail(PIC_ERR_CUDA, "pic_ens_create: stream creation failed"));
+    if (cudaStreamCreateWithFlags(&E.cap, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&E.d_steps, sizeof(long long) * n) != cudaSuccess ||
+        cudaMalloc(&E.d_ctl, sizeof(EnsControl)) != cudaSuccess)
+        return bail(fail(PIC_ERR_CUDA, "pic_ens_create: out of device memory"));
+    *out = e;
+    return PIC_OK;
+}
+
+int pic_ens_destroy(pic_ens* e) {
+    clear_error();
+    if (!e) return PIC_OK;
+    cudaDeviceSynchronize();
+    ens_free(e->e);
+    delete e;
+    return PIC_OK;
+}
+
+int pic_ens_step(pic_ens* e, int n_steps, void* stream) {
+    clear_error();
+    if (!e || n_steps < 0) return fail(PIC_ERR_BAD_ARG, "pic_ens_step: bad arguments");
+    EnsImpl& E = e->e;
+    if (n_steps == 0) return PIC_OK;
+    cudaStream_t st = as_stream(stream);
+    // A member fresh from pic_sim_init takes its first step without the kick,
+    // which the graph does not hold: if any member is fresh, every member
+    // takes one step eagerly and the graph runs the other n - 1.
+    bool fresh = false;
+    for (SimImpl* S : E.m) fresh = fresh || !S->kick_pending;
+    if (fresh) {
+        for (SimImpl* S : E.m) {
+            const int k = S->kick_pending ? 1 : 0;
+            if (S->d.sort_interval > 0 && S->steps % S->d.sort_interval == 0) PIC_TRY(sort_all(*S, st));
+            PIC_TRY(particle_pass(*S, st, k, k, 1, 1, 1.0, 1));
+            PIC_TRY(field_solve(*S, st, false));
+            S->kick_pending = true;
+            ++S->steps;
+        }
+        if (--n_steps == 0) return PIC_OK;
+    }
+    if (!E.exec) PIC_TRY(ens_capture(E));
+    const int n = int(E.m.size());
+    std::vector<long long> steps(n);
+    for (int i = 0; i < n; ++i) steps[i] = E.m[i]->steps;
+    const EnsControl ctl{n_steps};
+    PIC_CUDA(cudaMemcpyAsync(E.d_steps, steps.data(), sizeof(long long) * n, cudaMemcpyHostToDevice, st));
+    PIC_CUDA(cudaMemcpyAsync(E.d_ctl, &ctl, sizeof ctl, cudaMemcpyHostToDevice, st));
+    PIC_CUDA(cudaStreamSynchronize(st));  // the host copies above read stack memory
+    PIC_CUDA(cudaGraphLaunch(E.exec, st));
+    for (SimImpl* S : E.m) {
+        long long sorts = 0;
+        if (S->d.sort_interval > 0)
+            for (long long k = S->steps; k < S->steps + n_steps; ++k) sorts += (k % S->d.sort_interval == 0);
+        // the step counter, the particle pass (3, plus the collisions), the RHS and E
+        S->launches += n_steps * (1LL + 3 + (S->have_mcc ? 1 : 0) + 2) +
+                       sorts * (1 + (long long)S->ns * (5 + 3 * S->sorter.passes));
+        if (S->d.sort_interval > 0) S->launches += n_steps;  // the sort condition
+        S->solves += n_steps;
+        S->steps += n_steps;
+    }
     return PIC_OK;
 }
 

@@ -59,7 +59,8 @@ class PICSimulation:
 
     def __init__(self, nx, ny, dx, dy, dt, species, dirichlet, phi_bc=None, tol=1e-8, max_cycles=50,
                  precision="mixed", pre_sweeps=2, post_sweeps=2, omega=1.0, sort_interval=20, tile=16,
-                 mcc: MccTables | None = None, seed=0, use_graph=False, eps0=Consts.eps0, mg_launch="graph"):
+                 mcc: MccTables | None = None, seed=0, use_graph=False, eps0=Consts.eps0, mg_launch="graph",
+                 coarsest_max=9):
         self.nx, self.ny, self.dx, self.dy, self.dt = int(nx), int(ny), float(dx), float(dy), float(dt)
         self.species = list(species)
         d = _lib.SimDesc()
@@ -76,7 +77,7 @@ class PICSimulation:
         d.tol = float(tol)
         d.max_cycles = int(max_cycles)
         d.mg = _lib.MgOptions(_lib.PIC_MG_MIXED if precision == "mixed" else _lib.PIC_MG_FP64, pre_sweeps,
-                              post_sweeps, omega, 9, _lib.MG_LAUNCH_MODES[mg_launch])
+                              post_sweeps, omega, int(coarsest_max), _lib.MG_LAUNCH_MODES[mg_launch])
         d.sort_interval = int(sort_interval)
         d.tile = int(tile)
         self._mcc_desc = mcc.desc() if mcc is not None else None

@@ -1,0 +1,94 @@
+"""Ensembles: members stepped together in one graph (pic_ens_step) against
+twins stepped alone (pic_sim_step) from the same inputs.
+
+The members differ in grid side, particle counts, tile, sort interval and
+multigrid depth.  The deposit's global flush uses float atomics, so the two
+runs differ in the last bits of rho; the comparison allows for that:
+particle counts equal, phi within 1e-4 of its largest value (both solves
+stop at a 1e-8 relative residual, possibly after different cycle counts),
+and slot-by-slot positions
+within 1e-3 cells on at least 99 % of the slots (this also requires every
+member's cell sorts to have run at the same steps in both runs, since a sort
+reorders the slots)."""
+import numpy as np
+import pytest
+import torch
+
+from pic_b200 import ensemble, workloads
+
+pytestmark = pytest.mark.gpu
+
+MEMBERS = [  # (side, n_e, n_i, tile, sort_interval, coarsest_max)
+    (129, 30_000, 20_000, 16, 5, 9),
+    (257, 60_000, 45_000, 8, 7, 17),
+    (129, 12_000, 16_000, 8, 3, 9),
+    (257, 25_000, 35_000, 16, 10, 9),
+    (513, 50_000, 50_000, 16, 4, 33),
+]
+
+
+def _workloads():
+    out = []
+    rng = np.random.Generator(np.random.Philox(99))
+    for i, (side, ne, ni, *_ ) in enumerate(MEMBERS):
+        out.append(workloads.Workload(f"m{i}", side, ne, ni, Te=float(rng.uniform(1, 5)),
+                                      left_V=float(rng.uniform(0, 200)), seed=500 + i))
+    return out
+
+
+def _make(w, cfg):
+    _, _, _, tile, K, cmax = cfg
+    sim = ensemble.member_simulation(w, tile=tile, sort_interval=K, coarsest_max=cmax)
+    for s, a in enumerate(ensemble.member_arrays(w)):
+        sim.load(s, *a)
+    sim.init()
+    return sim
+
+
+def _state(sim):
+    sim.sync()
+    torch.cuda.synchronize()
+    c = sim.counters()
+    xs = [sim.species_arrays(s)[0][: c["count"][s]].cpu().numpy().copy() for s in range(2)]
+    phi = sim.fields()[0].cpu().numpy().copy()
+    return c, xs, phi
+
+
+@pytest.mark.parametrize("steps", [23])
+def test_ensemble_matches_members_stepped_alone(steps):
+    ws = _workloads()
+    together = [_make(w, cfg) for w, cfg in zip(ws, MEMBERS)]
+    alone = [_make(w, cfg) for w, cfg in zip(ws, MEMBERS)]
+    ens = ensemble.Ensemble(together)
+    ens.step(steps - 3)
+    ens.step(3)  # a second launch of the same graph
+    for sim in alone:
+        sim.step(steps)
+    torch.cuda.synchronize()
+    for i, (a, b) in enumerate(zip(together, alone)):
+        ca, xa, pa = _state(a)
+        cb, xb, pb = _state(b)
+        assert ca["steps"] == cb["steps"] == steps, i
+        assert ca["count"] == cb["count"], (i, ca["count"], cb["count"])
+        scale = max(1.0, float(np.abs(pb).max()))
+        assert np.abs(pa - pb).max() <= 1e-4 * scale, i
+        for s in range(2):
+            close = np.abs(xa[s] - xb[s]) <= 1e-3
+            assert close.mean() >= 0.99, (i, s, close.mean())
+    ens.close()
+    for sim in together + alone:
+        sim.close()
+
+
+def test_ensemble_rejects_eager_members_and_duplicates():
+    w = _workloads()[0]
+    sim = ensemble.member_simulation(w, use_graph=False)
+    from pic_b200 import _lib
+
+    with pytest.raises(_lib.PicError):
+        ensemble.Ensemble([sim])
+    g = ensemble.member_simulation(w)
+    with pytest.raises(_lib.PicError):
+        ensemble.Ensemble([g, g])
+    sim.close()
+    g.close()
