@@ -58,6 +58,11 @@ def parse():
     ap.add_argument("--no-graph", action="store_true", help="launch every kernel from the host (profilers)")
     ap.add_argument("--mg-launch", default="graph", choices=["persistent", "host", "graph"],
                     help="multigrid launch mode (host: one launch per kernel, for profilers)")
+    ap.add_argument("--ensemble", type=int, default=0,
+                    help="also time an ensemble of this many independent collisionless members (0: off)")
+    ap.add_argument("--ensemble-steps", type=int, default=100)
+    ap.add_argument("--tune-cache", default=os.path.join(ROOT, "pic_b200", "tuned_b200.json"),
+                    help="autotuner results (read if present, written after tuning)")
     return ap.parse_args()
 
 
@@ -300,6 +305,8 @@ def run_ours(args, world, rank, local):
         out["e2e"] = run_e2e(w, arrays, args, world, rank)
     if not args.no_poisson and rank == 0:
         out["poisson"] = run_poisson()
+    if args.ensemble > 0 and rank == 0:
+        out["ensemble"] = run_ensemble(args)
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         out["cpu_baseline"] = run_cpu_baseline(w, arrays, args.cpu_steps)
     if rank == 0:
@@ -309,6 +316,52 @@ def run_ours(args, world, rank, local):
         dist.destroy_process_group()
 
 
+def run_ensemble(args):
+    """Ensemble workload: members with grid sides from {129, 257, 513}, 1e5-2e6
+    particles per species, Te 1-5 eV, left wall 0-200 V, collisionless; each
+    member shape tuned by the autotuner; all members stepped by one graph
+    launch per call (pic_ens_step)."""
+    import torch
+
+    from pic_b200 import autotune, ensemble
+
+    ws = ensemble.ensemble_workloads(args.ensemble)
+    tuner = autotune.Autotuner(cache_path=args.tune_cache)
+    t0 = time.time()
+    choices = tuner.tune_ensemble(ws)
+    tune_s = time.time() - t0
+    sims = []
+    for w, ch in zip(ws, choices):
+        sim = ensemble.member_simulation(w, **ch.config())
+        for s, a in enumerate(ensemble.member_arrays(w)):
+            sim.load(s, *a)
+        sim.init()
+        sims.append(sim)
+    ens = ensemble.Ensemble(sims)
+    ens.step(3)
+    torch.cuda.synchronize()
+    n0 = ens.particle_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    ens.step(args.ensemble_steps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    n1 = ens.particle_count()
+    ens.close()
+    for sim in sims:
+        sim.close()
+    picked = {}
+    for ch in choices:
+        k = f"tile {ch.tile}, sort every {ch.sort_interval}, coarsest {ch.coarsest_max}"
+        picked[k] = picked.get(k, 0) + 1
+    sides = [w.nodes for w in ws]
+    return {"members": len(ws), "particles": n0, "steps": args.ensemble_steps, "ms_per_step": ms / args.ensemble_steps,
+            "value": 0.5 * (n0 + n1) * args.ensemble_steps / (ms / 1e3), "unit": UNIT,
+            "sides": {str(k): sides.count(k) for k in ensemble.SIDES}, "tuned": picked,
+            "tune_s": round(tune_s, 1), "tune_measurements": tuner.measurements}
+
+
 def run_e2e(w, arrays, args, world, rank):
     """Public API from pinned host arrays: load, init, K steps, read back particles and phi."""
     import torch
@@ -316,23 +369,34 @@ def run_e2e(w, arrays, args, world, rank):
 
     pinned = [[torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in sp] for sp in arrays]
     sim = make_sim(w, rank, args.sort_interval, mcc=True)
+    # read-back buffers (pinned, allocated before the timed region like the inputs)
+    cap = [int(len(sp[0]) * 1.25) for sp in arrays]
+    host_out = [[torch.empty(c, dtype=torch.float32).pin_memory() for _ in range(5)] for c in cap]
+    host_phi = torch.empty(w.nodes * w.nodes, dtype=torch.float64).pin_memory()
     stream = torch.cuda.current_stream()
     outs = None
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    ev[0].record(stream)
     for s, a in enumerate(pinned):
-        sim.load(s, *[t.numpy() for t in a])
+        sim.load(s, *a)
+    ev[1].record(stream)
     sim.init()
+    ev[2].record(stream)
     sim.step(args.steps)
     sim.sync()
-    outs = [[t.to("cpu", non_blocking=False) for t in sim.species_arrays(s)] for s in range(2)]
-    phi = sim.fields()[0].to("cpu")
-    e1.record(stream)
+    ev[3].record(stream)
+    outs = []
+    for s in range(2):
+        views = sim.species_arrays(s)
+        outs.append([h[: v.numel()].copy_(v, non_blocking=True) for h, v in zip(host_out[s], views)])
+    phi = host_phi.copy_(sim.fields()[0], non_blocking=True)
+    ev[4].record(stream)
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
+    ms = ev[0].elapsed_time(ev[4])
+    phases = {k: round(ev[i].elapsed_time(ev[i + 1]), 3) for i, k in enumerate(("load", "init", "steps", "read"))}
     t = torch.tensor([ms], device="cuda", dtype=torch.float64)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -341,9 +405,9 @@ def run_e2e(w, arrays, args, world, rank):
     d2h = sum(a.numel() * 4 for sp in outs for a in sp) + phi.numel() * 8
     sim.close()
     return {"value": world * n * args.steps / (float(t.item()) / 1e3), "unit": UNIT,
-            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps, "phase_ms": phases,
             "ms_total": float(t.item()), "includes": "H2D of all particles from pinned host memory, init, "
-                                                     f"{args.steps} steps, D2H of particles and phi"}
+                                                     f"{args.steps} steps, D2H of particles and phi into pinned host memory"}
 
 
 def run_poisson():

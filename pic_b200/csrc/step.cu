@@ -44,10 +44,11 @@ constexpr int kPushThreads = 256;
 constexpr int kPushP = 5;  // particles per thread per chunk (odd: conflict-free blocked access to shared memory)
 constexpr int kChunk = kPushThreads * kPushP;
 constexpr int kBufStride = kChunk + 8;  // floats per array per buffer: room for the 16-byte alignment window
-constexpr int kUnitMax = 8192;          // particles per work unit (one E tile staging, one charge flush)
+constexpr int kUnitMax = 8160;          // particles per work unit (one E tile staging, one charge flush)
 // The charge tile accumulates CIC weights as unsigned fixed point, 2^-19 per
 // unit: integer shared-memory atomics are native (float ones retry), the sum
-// is independent of the order, and 8192 weights <= 1 cannot overflow 2^32.
+// is independent of the order, and 8160 weights <= 1 stay below 2^32
+// (8160 * 2^19 = 2^32 - 2^24).
 constexpr float kFixScale = 524288.0f;  // 2^19
 constexpr float kFixInv = 1.0f / 524288.0f;
 constexpr int kBitWords = kChunk / 32 + 2;

@@ -102,12 +102,19 @@ class PICSimulation:
 
     # ---- state ----
     def load(self, s, x, y, vx, vy, vz=None):
-        """Load species s: positions in grid units, velocities in m/s (numpy or torch)."""
+        """Load species s: positions in grid units, velocities in m/s (numpy arrays,
+        host torch tensors or device tensors)."""
         arrs = [x, y, vx, vy, vz]
         if all(a is None or isinstance(a, np.ndarray) for a in arrs):
             host = [None if a is None else np.ascontiguousarray(a, dtype=np.float32) for a in arrs]
             n = len(host[0])
             _lib.call("pic_sim_load_species", self._h, s, *[None if a is None else a.ctypes.data for a in host], n, 1,
+                      _lib.stream_ptr())
+        elif all(a is None or (isinstance(a, torch.Tensor) and a.device.type == "cpu") for a in arrs):
+            # host tensors (pinned ones copy by DMA without staging)
+            host = [None if a is None else a.to(torch.float32).contiguous() for a in arrs]
+            n = host[0].numel()
+            _lib.call("pic_sim_load_species", self._h, s, *[None if a is None else a.data_ptr() for a in host], n, 1,
                       _lib.stream_ptr())
         else:
             dev = [None if a is None else torch.as_tensor(a, dtype=torch.float32, device="cuda").contiguous()
