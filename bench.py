@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--ensemble", type=int, default=0,
                     help="also time an ensemble of this many independent collisionless members (0: off)")
     ap.add_argument("--ensemble-steps", type=int, default=100)
+    ap.add_argument("--adjoint", action="store_true",
+                    help="also time the differentiable workload (forward, adjoint, finite-difference check)")
     ap.add_argument("--tune-cache", default=os.path.join(ROOT, "pic_b200", "tuned_b200.json"),
                     help="autotuner results (read if present, written after tuning)")
     return ap.parse_args()
@@ -307,6 +309,8 @@ def run_ours(args, world, rank, local):
         out["poisson"] = run_poisson()
     if args.ensemble > 0 and rank == 0:
         out["ensemble"] = run_ensemble(args)
+    if args.adjoint and rank == 0:
+        out["adjoint"] = run_adjoint()
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         out["cpu_baseline"] = run_cpu_baseline(w, arrays, args.cpu_steps)
     if rank == 0:
@@ -360,6 +364,62 @@ def run_ensemble(args):
             "value": 0.5 * (n0 + n1) * args.ensemble_steps / (ms / 1e3), "unit": UNIT,
             "sides": {str(k): sides.count(k) for k in ensemble.SIDES}, "tuned": picked,
             "tune_s": round(tune_s, 1), "tune_measurements": tuner.measurements}
+
+
+def run_adjoint():
+    """Differentiable workload: 257^2 nodes, 1e6 + 1e6 particles, 200 FP64
+    collisionless steps, checkpoints every 20; gradients of the final
+    electron-density loss with respect to four wall potentials and a velocity
+    perturbation amplitude, against central finite differences."""
+    from pic_b200 import adjoint
+
+    w = adjoint.AdjWorkload()
+    prob, V0, A0, _ = adjoint.build(w)
+    prob.forward(V0, A0)
+    prob.backward()  # graphs captured
+    t0 = time.perf_counter()
+    loss = prob.forward(V0, A0)
+    t1 = time.perf_counter()
+    dV, dA = prob.backward()
+    t2 = time.perf_counter()
+    fd = {}
+    # absorption as computed (wall crossings flip between runs), then frozen at
+    # the base run's steps (the fixed mask the adjoint differentiates with)
+    for frozen, h, hA in ((False, 1e-3, 1.0), (True, 1e-3, 1.0), (True, 1e-5, 0.1)):
+        prob.forward(V0, A0)
+        prob.freeze_absorption(frozen)
+        g = []
+        for q in range(4):
+            e = np.zeros(4)
+            e[q] = h
+            g.append((prob.forward(V0 + e, A0) - prob.forward(V0 - e, A0)) / (2 * h))
+        gA = (prob.forward(V0, A0 + hA) - prob.forward(V0, A0 - hA)) / (2 * hA)
+        prob.freeze_absorption(False)
+        err = max(abs(a - b) for a, b in zip(dV, g)) / max(abs(b) for b in g)
+        fd[f"h={h:g} V{', absorption frozen' if frozen else ''}"] = {
+            "dV_fd": g, "dA_fd": gA, "max_rel_err_dV": err, "rel_err_dA": abs(dA - gA) / abs(gA)}
+    prob.close()
+    # every solve a fixed 10 V-cycles: the solve map is smooth in V, so small
+    # steps isolate the adjoint's agreement from the solver's stopping point
+    fixed = adjoint.AdjWorkload(tol=0.0, max_cycles=10)
+    prob, V0, A0, _ = adjoint.build(fixed)
+    prob.forward(V0, A0)
+    fdV, fdA = prob.backward()
+    prob.freeze_absorption(True)
+    for h, hA in ((1e-4, 0.1), (1e-6, 0.01)):
+        g = []
+        for q in range(4):
+            e = np.zeros(4)
+            e[q] = h
+            g.append((prob.forward(V0 + e, A0) - prob.forward(V0 - e, A0)) / (2 * h))
+        gA = (prob.forward(V0, A0 + hA) - prob.forward(V0, A0 - hA)) / (2 * hA)
+        err = max(abs(a - b) for a, b in zip(fdV, g)) / max(abs(b) for b in g)
+        fd[f"h={h:g} V, absorption frozen, 10 V-cycles per solve"] = {
+            "dV_adjoint": list(fdV), "dV_fd": g, "dA_fd": gA, "max_rel_err_dV": err, "rel_err_dA": abs(fdA - gA) / abs(gA)}
+    prob.close()
+    return {"workload": "257x257 nodes, 1e6 e- + 1e6 ions, 200 FP64 steps, checkpoints every 20, 4 wall electrodes",
+            "loss": loss, "dV": list(dV), "dA": dA, "forward_ms": 1e3 * (t1 - t0), "backward_ms": 1e3 * (t2 - t1),
+            "backward_over_forward": (t2 - t1) / (t1 - t0), "finite_differences": fd}
 
 
 def run_e2e(w, arrays, args, world, rank):

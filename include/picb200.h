@@ -364,6 +364,76 @@ int pic_ens_destroy(pic_ens* e);
  * takes its first of the n steps eagerly. */
 int pic_ens_step(pic_ens* e, int n_steps, void* stream);
 
+/* ------------------------------------------------------------------ */
+/* Hand-written adjoint of the collisionless step                      */
+/* ------------------------------------------------------------------ */
+
+/* Gradients of L = mean over nodes of (n_s - n_target)^2, the final number
+ * density of one species after N collisionless steps, with respect to the
+ * potentials of electrode segments (Dirichlet node groups) and to the
+ * amplitude A of an initial-velocity perturbation v_0 + A dv.  The forward
+ * model is the reference's step order (src/simulation.py:622-660: drift,
+ * deposit, Poisson solve, E, kick; init: deposit, solve, E, backward half
+ * kick) in FP64, with absorption on the grid edges treated as a fixed mask
+ * in the adjoint.  The adjoint is hand-written: the CIC deposit's transpose
+ * is a gather of the weight gradients, the Poisson solve is self-adjoint (one
+ * extra multigrid solve per step with zero boundary values), the leapfrog runs
+ * in reverse.  The forward pass stores a checkpoint every checkpoint_every
+ * steps; the backward pass recomputes each segment from its checkpoint.
+ * The reference has no differentiable path; this extends its step. */
+#define PIC_ADJ_MAX_SEGMENTS 16
+
+typedef struct pic_adj pic_adj;
+
+typedef struct pic_adj_species {
+    int n;          /* particles */
+    double charge;  /* C */
+    double mass;    /* kg */
+    double np2c;    /* physical particles per macro-particle (per unit depth) */
+} pic_adj_species;
+
+typedef struct pic_adj_desc {
+    int nx, ny;                 /* nodes */
+    double dx, dy, dt, eps0;
+    int nspecies;
+    pic_adj_species species[PIC_MAX_SPECIES];
+    const uint8_t* h_dirichlet; /* nx*ny, 1 = Dirichlet (the grid edges always are) */
+    const int* h_segment;       /* nx*ny: electrode segment of a Dirichlet node, or -1 */
+    const double* h_phi_fixed;  /* nx*ny potentials of Dirichlet nodes without a segment (NULL: 0) */
+    int nseg;                   /* electrode segments (<= PIC_ADJ_MAX_SEGMENTS) */
+    int steps;                  /* N */
+    int checkpoint_every;       /* C */
+    int loss_species;           /* s of the loss */
+    double tol;                 /* relative residual of every Poisson solve (FP64 multigrid); 0: every
+                                   solve runs exactly max_cycles V-cycles (a fixed linear map of its
+                                   warm start and right-hand side, smooth in the parameters) */
+    int max_cycles;
+} pic_adj_desc;
+
+int pic_adj_create(const pic_adj_desc* desc, pic_adj** out);
+int pic_adj_destroy(pic_adj* a);
+/* Initial state of species s (device FP64 arrays of desc.species[s].n):
+ * positions in grid units, velocities and the perturbation direction dv in
+ * m/s (dv NULL = 0). */
+int pic_adj_set_particles(pic_adj* a, int s, const double* d_x, const double* d_y, const double* d_vx,
+                          const double* d_vy, const double* d_dvx, const double* d_dvy, void* stream);
+/* Target number density, device FP64 nx*ny (m^-3). */
+int pic_adj_set_target(pic_adj* a, const double* d_target, void* stream);
+/* N steps from the initial state with segment potentials h_V[nseg] (host)
+ * and amplitude A; writes the loss (synchronises). */
+int pic_adj_forward(pic_adj* a, const double* h_V, double A, double* loss, void* stream);
+/* dL/dV[nseg] and dL/dA at the last forward's parameters (synchronises). */
+int pic_adj_backward(pic_adj* a, double* h_dV, double* h_dA, void* stream);
+/* With on = 1, later forward passes reuse the absorption steps of the last
+ * forward pass instead of computing them: the loss is then smooth in the
+ * parameters (absorption is the fixed mask the adjoint differentiates with),
+ * which is what a finite-difference check of the adjoint needs.  on = 0
+ * restores absorption at the walls. */
+int pic_adj_freeze_absorption(pic_adj* a, int on);
+/* Device arrays of the state after the last forward pass (death: first state
+ * at which a particle is outside the grid). */
+int pic_adj_state(pic_adj* a, double** x, double** y, double** ux, double** uy, int** death, double** phi);
+
 #ifdef __cplusplus
 }
 #endif

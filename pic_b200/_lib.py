@@ -91,6 +91,21 @@ class SimDesc(C.Structure):
                 ("seed", C.c_ulonglong), ("use_graph", C.c_int)]
 
 
+PIC_ADJ_MAX_SEGMENTS = 16
+
+
+class AdjSpecies(C.Structure):
+    _fields_ = [("n", C.c_int), ("charge", C.c_double), ("mass", C.c_double), ("np2c", C.c_double)]
+
+
+class AdjDesc(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("dx", C.c_double), ("dy", C.c_double), ("dt", C.c_double),
+                ("eps0", C.c_double), ("nspecies", C.c_int), ("species", AdjSpecies * PIC_MAX_SPECIES),
+                ("h_dirichlet", C.c_void_p), ("h_segment", C.c_void_p), ("h_phi_fixed", C.c_void_p),
+                ("nseg", C.c_int), ("steps", C.c_int), ("checkpoint_every", C.c_int), ("loss_species", C.c_int),
+                ("tol", C.c_double), ("max_cycles", C.c_int)]
+
+
 class SimCounters(C.Structure):
     _fields_ = [("absorbed", C.c_ulonglong * PIC_MAX_SPECIES),
                 ("collisions", (C.c_ulonglong * PIC_MAX_PROCESSES) * PIC_MAX_SPECIES),
@@ -142,6 +157,15 @@ SIGNATURES = {
     "pic_ens_create": [C.POINTER(_vp), _i, C.POINTER(_vp)],
     "pic_ens_destroy": [_vp],
     "pic_ens_step": [_vp, _i, _vp],
+    "pic_adj_create": [_vp, C.POINTER(_vp)],
+    "pic_adj_destroy": [_vp],
+    "pic_adj_set_particles": [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "pic_adj_set_target": [_vp, _vp, _vp],
+    "pic_adj_forward": [_vp, _vp, C.c_double, C.POINTER(C.c_double), _vp],
+    "pic_adj_backward": [_vp, _vp, C.POINTER(C.c_double), _vp],
+    "pic_adj_freeze_absorption": [_vp, _i],
+    "pic_adj_state": [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp),
+                      C.POINTER(_vp)],
 }
 _RESTYPE = {"pic_last_error": C.c_char_p, "pic_sim_kernel_launches": C.c_longlong}
 

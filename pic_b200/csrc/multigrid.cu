@@ -1285,6 +1285,7 @@ int mg_launch_graph(pic_mg* mg, double* phi, const double* f, double tol, int ma
     return mg_launch(mg->m, phi, f, tol, max_cycles, st);
 }
 int mg_info(pic_mg* mg, pic_mg_info* info) { return mg_read_info(mg->m, info); }
+const int* mg_device_converged(pic_mg* mg) { return mg->m.N.converged; }
 
 }  // namespace pic
 
