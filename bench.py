@@ -48,7 +48,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--sort-interval", type=int, default=40)
+    ap.add_argument("--sort-interval", type=int, default=80,
+                    help="steps between cell sorts (80: the autotuner's choice for 513^2 shapes)")
     ap.add_argument("--particles", type=int, default=4_000_000, help="per species")
     ap.add_argument("--no-poisson", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -357,7 +358,8 @@ def run_ensemble(args):
         sim.close()
     picked = {}
     for ch in choices:
-        k = f"tile {ch.tile}, sort every {ch.sort_interval}, coarsest {ch.coarsest_max}"
+        k = (f"tile {ch.tile}, sort every {ch.sort_interval}, coarsest {ch.coarsest_max}, omega {ch.omega}, "
+             f"{ch.mg_launch} multigrid")
         picked[k] = picked.get(k, 0) + 1
     sides = [w.nodes for w in ws]
     return {"members": len(ws), "particles": n0, "steps": args.ensemble_steps, "ms_per_step": ms / args.ensemble_steps,

@@ -106,14 +106,16 @@ typedef enum pic_mg_precision {
 typedef enum pic_mg_launch_mode {
     PIC_MG_PERSISTENT = 0, /* one cooperative kernel per solve; phases separated by grid barriers */
     PIC_MG_HOST_LOOP = 1,  /* one launch per kernel, convergence tested on the host each cycle */
-    PIC_MG_GRAPH_LOOP = 2  /* one launch per kernel inside a CUDA-graph conditional WHILE node */
+    PIC_MG_GRAPH_LOOP = 2, /* one launch per kernel inside a CUDA-graph conditional WHILE node */
+    PIC_MG_CLUSTER = 3     /* one launch of a single thread-block cluster per solve (FP32 levels whose
+                              row bands fit in shared memory; otherwise the graph loop) */
 } pic_mg_launch_mode;
 
 typedef struct pic_mg_options {
     int precision;    /* pic_mg_precision */
     int pre_sweeps;   /* red-black Gauss-Seidel sweeps before restriction (default 2) */
     int post_sweeps;  /* sweeps after prolongation (default 2) */
-    double omega;     /* over-relaxation of the smoother (default 1.0) */
+    double omega;     /* over-relaxation of the red-black smoother (default, when <= 0: 1.15) */
     int coarsest_max; /* coarsen while both node counts exceed this (default 9) */
     int launch_mode;  /* pic_mg_launch_mode */
 } pic_mg_options;
@@ -149,6 +151,9 @@ int pic_mg_solve(pic_mg* mg, double* d_phi, const double* d_f, double tol, int m
  * pic_mg_read_info after synchronising the stream. */
 int pic_mg_solve_async(pic_mg* mg, double* d_phi, const double* d_f, double tol, int cycles, void* stream);
 int pic_mg_read_info(pic_mg* mg, double tol, pic_mg_info* info);
+/* The launch mode solves actually use (PIC_MG_CLUSTER falls back to
+ * PIC_MG_GRAPH_LOOP where the cluster solve does not apply). */
+int pic_mg_effective_launch_mode(pic_mg* mg, int* mode);
 
 /* ------------------------------------------------------------------ */
 /* Cell sort (replaces Particles2D.sort_particles_sparse, src/Particles.py:550-632) */

@@ -40,7 +40,7 @@ class Solver:
         self._edge_mask = m2.copy()
         self._edge_mask[0, :] = self._edge_mask[-1, :] = self._edge_mask[:, 0] = self._edge_mask[:, -1] = 1
         self.dirichlet = torch.as_tensor(self._edge_mask.reshape(-1), device=grid.phi.device)
-        self.multigrid = MultigridSolver(self._edge_mask.reshape(-1), grid.m, grid.n, grid.dx, omega=1.0,
+        self.multigrid = MultigridSolver(self._edge_mask.reshape(-1), grid.m, grid.n, grid.dx, omega=1.15,
                                          precision=precision, hy=grid.dy)
         self.last_info = None
         if self.phi_bc is not None:

@@ -39,7 +39,9 @@ PIC_MG_FP64 = 1
 PIC_MG_PERSISTENT = 0
 PIC_MG_HOST_LOOP = 1
 PIC_MG_GRAPH_LOOP = 2
-MG_LAUNCH_MODES = {"persistent": PIC_MG_PERSISTENT, "host": PIC_MG_HOST_LOOP, "graph": PIC_MG_GRAPH_LOOP}
+PIC_MG_CLUSTER = 3
+MG_LAUNCH_MODES = {"persistent": PIC_MG_PERSISTENT, "host": PIC_MG_HOST_LOOP, "graph": PIC_MG_GRAPH_LOOP,
+                   "cluster": PIC_MG_CLUSTER}
 
 PIC_ELASTIC = 0
 PIC_EXCITATION = 1
@@ -134,6 +136,7 @@ SIGNATURES = {
     "pic_mg_solve": [_vp, _vp, _vp, _d, _i, C.POINTER(MgInfo), _vp],
     "pic_mg_solve_async": [_vp, _vp, _vp, _d, _i, _vp],
     "pic_mg_read_info": [_vp, _d, C.POINTER(MgInfo)],
+    "pic_mg_effective_launch_mode": [_vp, C.POINTER(_i)],
     "pic_sorter_create": [_i, _i, _i, _i, C.POINTER(_vp)],
     "pic_sorter_destroy": [_vp],
     "pic_sort": [_vp, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],

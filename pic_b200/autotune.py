@@ -8,6 +8,9 @@ calls).  The choices here trade against each other on the GPU:
                  passes, while the particles drift out of their tiles between
                  sorts (untiled particles gather and deposit in global memory)
   coarsest_max   largest side of the coarsest multigrid level (V-cycle depth)
+  omega          over-relaxation of the red-black smoother (cycles per solve)
+  mg_launch      multigrid launch mode: the graph loop of tiled kernels, or
+                 one thread-block cluster per solve (faster on small grids)
 
 Candidates are timed on the GPU (CUDA events over graph-launched steps) by a
 coordinate descent from a default, one parameter at a time; results are kept
@@ -22,9 +25,10 @@ import os
 from dataclasses import asdict, dataclass
 from typing import Callable
 
-SPACE = {"tile": (8, 16, 32), "sort_interval": (10, 20, 40, 80), "coarsest_max": (5, 9, 17)}
-DEFAULT = {"tile": 16, "sort_interval": 20, "coarsest_max": 9}
-ORDER = ("tile", "sort_interval", "coarsest_max")
+SPACE = {"tile": (8, 16, 32), "sort_interval": (10, 20, 40, 80), "coarsest_max": (5, 9, 17),
+         "omega": (1.0, 1.15, 1.3), "mg_launch": ("graph", "cluster")}
+DEFAULT = {"tile": 16, "sort_interval": 20, "coarsest_max": 9, "omega": 1.15, "mg_launch": "graph"}
+ORDER = ("tile", "sort_interval", "coarsest_max", "omega", "mg_launch")
 
 
 @dataclass
@@ -33,9 +37,12 @@ class Choice:
     sort_interval: int
     coarsest_max: int
     ns_per_particle_step: float  # measured cost of the chosen configuration
+    omega: float = DEFAULT["omega"]
+    mg_launch: str = DEFAULT["mg_launch"]
 
     def config(self) -> dict:
-        return {"tile": self.tile, "sort_interval": self.sort_interval, "coarsest_max": self.coarsest_max}
+        return {"tile": self.tile, "sort_interval": self.sort_interval, "coarsest_max": self.coarsest_max,
+                "omega": self.omega, "mg_launch": self.mg_launch}
 
 
 def shape_key(nodes: int, particles: int) -> str:
@@ -48,6 +55,7 @@ def coordinate_descent(measure: Callable[[dict], float], space=SPACE, start=DEFA
     in `order`, the others held at their best values so far), starting from
     `start` (or a parameter's first candidate where `start` is not one).  Returns
     (best config, its cost, every measured (config, cost))."""
+    order = [k for k in order if k in space]
     best = {k: (start[k] if start[k] in space[k] else space[k][0]) for k in order}
     seen = {}
 
@@ -111,7 +119,8 @@ class Autotuner:
         if key in self.cache:
             return self.cache[key]
         best, cost, _ = coordinate_descent(lambda cfg: self.measure(make_sim, cfg), self.space)
-        ch = Choice(best["tile"], best["sort_interval"], best["coarsest_max"], cost)
+        ch = Choice(best["tile"], best["sort_interval"], best["coarsest_max"], cost,
+                    best.get("omega", DEFAULT["omega"]), best.get("mg_launch", DEFAULT["mg_launch"]))
         self.cache[key] = ch
         self.save()
         return ch

@@ -24,6 +24,7 @@
 //             and the loop decision
 // The loop is a CUDA-graph conditional WHILE node whose condition r0 sets,
 // so a solve issues no host synchronisation.
+#include <cooperative_groups.h>
 #include <cuda/atomic>
 
 #include <cmath>
@@ -383,20 +384,19 @@ __device__ void level_sweeps(T* se, const T* sg, const uint8_t* sm, const LevelD
 
 template <class T>
 __device__ void coarse_vcycle(const CoarseDesc<T>& D, unsigned char* smem) {
-    T* E[kMgMaxCoarseLevels];
-    T* Gs[kMgMaxCoarseLevels];
-    uint8_t* M[kMgMaxCoarseLevels];
+    // level pointers into shared memory, from the descriptor's offsets (no
+    // per-thread pointer arrays: they would live in local memory)
+    auto E = [&](int l) { return reinterpret_cast<T*>(smem + D.off_e[l]); };
+    auto Gs = [&](int l) { return reinterpret_cast<T*>(smem + D.off_g[l]); };
+    auto M = [&](int l) { return smem + D.off_m[l]; };
     for (int l = 0; l < D.nlev; ++l) {
-        E[l] = reinterpret_cast<T*>(smem + D.off_e[l]);
-        Gs[l] = reinterpret_cast<T*>(smem + D.off_g[l]);
-        M[l] = smem + D.off_m[l];
         const LevelDev<T>& L = D.lv[l];
         const float inv_nx = 1.0f / float(L.nx);
         for (int q = threadIdx.x; q < L.nx * L.ny; q += blockDim.x) {
             const int j = div_small(q, inv_nx), i = q - j * L.nx;
-            M[l][q] = (i == 0 || j == 0 || i == L.nx - 1 || j == L.ny - 1 || L.mask[q]) ? 1 : 0;
-            E[l][q] = T(0);
-            if (l == 0) Gs[0][q] = L.g[q];
+            M(l)[q] = (i == 0 || j == 0 || i == L.nx - 1 || j == L.ny - 1 || L.mask[q]) ? 1 : 0;
+            E(l)[q] = T(0);
+            if (l == 0) Gs(0)[q] = L.g[q];
         }
     }
     __syncthreads();
@@ -404,17 +404,17 @@ __device__ void coarse_vcycle(const CoarseDesc<T>& D, unsigned char* smem) {
     for (int l = 0; l < last; ++l) {
         const LevelDev<T>& L = D.lv[l];
         const LevelDev<T>& C = D.lv[l + 1];
-        level_sweeps(E[l], Gs[l], M[l], L, D.omega, D.pre);
+        level_sweeps(E(l), Gs(l), M(l), L, D.omega, D.pre);
         // restriction of the residual, evaluated on the fly: g of this level
         // must survive for the post-smoothing on the way back up
-        const T* e = E[l];
-        const T* g = Gs[l];
-        const uint8_t* mk = M[l];
+        const T* e = E(l);
+        const T* g = Gs(l);
+        const uint8_t* mk = M(l);
         const int nx = L.nx;
         const float inv_cnx = 1.0f / float(C.nx);
         for (int Q = threadIdx.x; Q < C.nx * C.ny; Q += blockDim.x) {
-            if (M[l + 1][Q]) {
-                Gs[l + 1][Q] = T(0);
+            if (M(l + 1)[Q]) {
+                Gs(l + 1)[Q] = T(0);
                 continue;
             }
             const int J = div_small(Q, inv_cnx), I = Q - J * C.nx;
@@ -428,7 +428,7 @@ __device__ void coarse_vcycle(const CoarseDesc<T>& D, unsigned char* smem) {
             T v = T(0.25) * rr(0);
             v += T(0.125) * (rr(-1) + rr(1) + rr(-nx) + rr(nx));
             v += T(0.0625) * (rr(-nx - 1) + rr(-nx + 1) + rr(nx - 1) + rr(nx + 1));
-            Gs[l + 1][Q] = v;
+            Gs(l + 1)[Q] = v;
         }
         __syncthreads();
     }
@@ -439,9 +439,9 @@ __device__ void coarse_vcycle(const CoarseDesc<T>& D, unsigned char* smem) {
         for (int a = warp; a < D.nf; a += nw) {
             const double* row = D.ainv + long(a) * D.nf;
             double s = 0.0;
-            for (int b = lane; b < D.nf; b += 32) s += row[b] * double(Gs[last][D.cidx[b]]);
+            for (int b = lane; b < D.nf; b += 32) s += row[b] * double(Gs(last)[D.cidx[b]]);
             s = warp_sum(s);
-            if (lane == 0) E[last][D.cidx[a]] = T(s);
+            if (lane == 0) E(last)[D.cidx[a]] = T(s);
         }
     }
     __syncthreads();
@@ -450,24 +450,24 @@ __device__ void coarse_vcycle(const CoarseDesc<T>& D, unsigned char* smem) {
         const LevelDev<T>& C = D.lv[l + 1];
         const float inv_nx = 1.0f / float(L.nx);
         for (int q = threadIdx.x; q < L.nx * L.ny; q += blockDim.x) {
-            if (M[l][q]) continue;
+            if (M(l)[q]) continue;
             const int j = div_small(q, inv_nx), i = q - j * L.nx;
             const int K = (j >> 1) * C.nx + (i >> 1);
-            const T* ec = E[l + 1];
+            const T* ec = E(l + 1);
             T v;
             if (!(i & 1) && !(j & 1)) v = ec[K];
             else if ((i & 1) && !(j & 1)) v = T(0.5) * (ec[K] + ec[K + 1]);
             else if (!(i & 1) && (j & 1)) v = T(0.5) * (ec[K] + ec[K + C.nx]);
             else v = T(0.25) * (ec[K] + ec[K + 1] + ec[K + C.nx] + ec[K + C.nx + 1]);
-            E[l][q] += v;
+            E(l)[q] += v;
         }
         __syncthreads();
-        level_sweeps(E[l], Gs[l], M[l], L, D.omega, D.post);
+        level_sweeps(E(l), Gs(l), M(l), L, D.omega, D.post);
     }
     const LevelDev<T>& L0 = D.lv[0];
     for (int q = threadIdx.x; q < L0.nx * L0.ny; q += blockDim.x) {
-        if (D.phi0) D.phi0[q] += double(E[0][q]);
-        else L0.e[q] = E[0][q];
+        if (D.phi0) D.phi0[q] += double(E(0)[q]);
+        else L0.e[q] = E(0)[q];
     }
     __syncthreads();
 }
@@ -746,6 +746,323 @@ __global__ void __launch_bounds__(kMgThreads) k_mg_solve(SolveDesc<T> S) {
     }
 }
 
+// ---- cluster-resident solve ---------------------------------------------------------
+//
+// The whole solve in one launch of a single thread-block cluster (16 CTAs of
+// 1024 threads where the device allows, else 8): every level of more than
+// 33^2 nodes is cut into row bands, one per CTA; a phase loads the CTA's band
+// with its halo rows into shared memory, works there and writes the band
+// back; the cluster barrier (a hardware barrier, no polling) separates the
+// phases.  CTA 0 alone runs the levels of at most 33^2 nodes.  The FP64
+// residual norm is summed over the CTAs through distributed shared memory,
+// in rank order, so every CTA takes the same loop decision.
+
+constexpr int kClusterThreads = 1024;
+constexpr int kBandBatch = 4;  // global loads a thread issues before the first is used
+
+struct ClusterDesc {
+    int L, Lb;  // levels; [0, Lb) in bands over the cluster, [Lb, L) in CTA 0
+    LevelDev<float> lv[kMgMaxLevels];
+    CoarseDesc<float> coarse;
+    const double* f;
+    double* phi;
+    int nx, ny;
+    double cx, cy;
+    NormState N;
+    double tol2;
+    int max_cycles;
+    float omega;
+    int pre, post;
+};
+
+// Rows [a, b) of an n-row level that CTA r of `parts` owns.
+__device__ __host__ __forceinline__ void band_rows(int n, int parts, int r, int& a, int& b) {
+    const int per = (n + parts - 1) / parts;
+    a = n < r * per ? n : r * per;
+    b = n < a + per ? n : a + per;
+}
+
+// Loads rows [j0, j0 + R) of level L (full width) into the shared band:
+// mask (edges, electrodes and rows outside the grid are Dirichlet), g, and e
+// (zero, or the stored correction on free nodes).
+__device__ void band_load(const LevelDev<float>& L, int j0, int R, float* __restrict__ se, float* __restrict__ sg,
+                          uint8_t* __restrict__ sm, bool load_e) {
+    const int nx = L.nx, N = R * nx, T = blockDim.x;
+    const float inv = 1.0f / float(nx);
+    for (int base = 0; base < N; base += kBandBatch * T) {
+        uint8_t m[kBandBatch];
+        float g[kBandBatch], e[kBandBatch];
+#pragma unroll
+        for (int u = 0; u < kBandBatch; ++u) {
+            const int q = base + u * T + int(threadIdx.x);
+            const int lr = div_small(q, inv), i = q - lr * nx, j = j0 + lr;
+            const bool in = q < N && j >= 0 && j < L.ny;
+            const long k = long(j) * nx + i;
+            m[u] = in ? L.mask[k] : uint8_t(1);
+            g[u] = in ? L.g[k] : 0.0f;
+            e[u] = (load_e && in) ? L.e[k] : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < kBandBatch; ++u) {
+            const int q = base + u * T + int(threadIdx.x);
+            if (q >= N) break;
+            const int lr = div_small(q, inv), i = q - lr * nx, j = j0 + lr;
+            const bool fr = i > 0 && j > 0 && i < nx - 1 && j < L.ny - 1 && !m[u];
+            sm[q] = fr ? 0 : 1;
+            sg[q] = g[u];
+            se[q] = fr ? e[u] : 0.0f;
+        }
+    }
+}
+
+// One red (color 0: (i + j) even) or black half-sweep over the band's rows
+// 1 .. R-2 (j0: global row of band row 0).
+__device__ void band_half_sweep(float* __restrict__ se, const float* __restrict__ sg, const uint8_t* __restrict__ sm,
+                                const LevelDev<float>& L, int j0, int R, int color, float omega) {
+    const int nx = L.nx, hx = (nx + 1) / 2, T = blockDim.x;
+    const float inv = 1.0f / float(hx);
+    for (int q = threadIdx.x; q < R * hx; q += T) {
+        const int lr = div_small(q, inv);
+        const int i = 2 * (q - lr * hx) + ((color + j0 + lr) & 1);
+        if (lr < 1 || lr > R - 2 || i >= nx) continue;
+        const int p = lr * nx + i;
+        if (sm[p]) continue;
+        const float s = L.cx * (se[p - 1] + se[p + 1]) + L.cy * (se[p - nx] + se[p + nx]);
+        const float upd = (s - sg[p]) * L.inv_diag;
+        const float old = se[p];
+        se[p] = old + omega * (upd - old);
+    }
+}
+
+__device__ void band_sweeps(float* se, const float* sg, const uint8_t* sm, const LevelDev<float>& L, int j0, int R,
+                            int sweeps, float omega) {
+    for (int s = 0; s < sweeps; ++s)
+        for (int color = 0; color < 2; ++color) {
+            band_half_sweep(se, sg, sm, L, j0, R, color, omega);
+            __syncthreads();
+        }
+}
+
+// Pre-smoothing of level F on this CTA's band, the residual, and its
+// full-weighting restriction onto the coarse rows J with 2J in the band.
+__device__ void band_down(const LevelDev<float>& F, const LevelDev<float>& Cc, float omega, int pre, int rank,
+                          int parts, unsigned char* smem) {
+    int fa, fb;
+    band_rows(F.ny, parts, rank, fa, fb);
+    const int H = 2 * pre + 2, j0 = fa - H, R = (fb - fa) + 2 * H, nx = F.nx, T = blockDim.x;
+    float* se = reinterpret_cast<float*>(smem);
+    float* sg = se + R * nx;
+    uint8_t* sm = reinterpret_cast<uint8_t*>(sg + R * nx);
+    if (fa < fb) {
+        band_load(F, j0, R, se, sg, sm, false);
+        __syncthreads();
+        band_sweeps(se, sg, sm, F, j0, R, pre, omega);
+        // the smoothed correction of the band's own rows
+        for (int q = threadIdx.x; q < (fb - fa) * nx; q += T) F.e[long(fa) * nx + q] = se[H * nx + q];
+        // residual in place of g (each node reads only its own g)
+        const float inv = 1.0f / float(nx);
+        for (int q = threadIdx.x; q < R * nx; q += T) {
+            const int lr = div_small(q, inv);
+            if (lr < 1 || lr > R - 2 || sm[q]) continue;
+            const float c = se[q];
+            const float lap = F.cx * (se[q - 1] + se[q + 1] - 2.0f * c) + F.cy * (se[q - nx] + se[q + nx] - 2.0f * c);
+            sg[q] = sg[q] - lap;
+        }
+        __syncthreads();
+        const int Ja = (fa + 1) / 2, Jb = min(Cc.ny, (fb + 1) / 2);
+        const int cnx = Cc.nx;
+        const float cinv = 1.0f / float(cnx);
+        for (int q = threadIdx.x; q < (Jb - Ja) * cnx; q += T) {
+            const int dJ = div_small(q, cinv), I = q - dJ * cnx, J = Ja + dJ;
+            const long K = long(J) * cnx + I;
+            if (I == 0 || J == 0 || I == cnx - 1 || J == Cc.ny - 1 || Cc.mask[K]) {
+                Cc.g[K] = 0.0f;
+                continue;
+            }
+            const int p = (2 * J - j0) * nx + 2 * I;
+            auto r = [&](int o) { return sm[p + o] ? 0.0f : sg[p + o]; };
+            float v = 0.25f * r(0);
+            v += 0.125f * (r(-1) + r(1) + r(-nx) + r(nx));
+            v += 0.0625f * (r(-nx - 1) + r(-nx + 1) + r(nx - 1) + r(nx + 1));
+            Cc.g[K] = v;
+        }
+    }
+    __syncthreads();
+}
+
+// Prolongation-add of the coarse correction and post-smoothing on this CTA's
+// band of level F; on level 0 (phi given) phi += e instead of storing e.
+__device__ void band_up(const LevelDev<float>& F, const LevelDev<float>& Cc, float omega, int post, double* phi,
+                        int rank, int parts, unsigned char* smem) {
+    int fa, fb;
+    band_rows(F.ny, parts, rank, fa, fb);
+    const int H = 2 * post, j0 = fa - H, R = (fb - fa) + 2 * H, nx = F.nx, T = blockDim.x;
+    const int cj0 = j0 >> 1, CR = ((j0 + R - 1) >> 1) + 2 - cj0, cnx = Cc.nx;
+    float* se = reinterpret_cast<float*>(smem);
+    float* sg = se + R * nx;
+    float* sc = sg + R * nx;
+    uint8_t* sm = reinterpret_cast<uint8_t*>(sc + CR * cnx);
+    if (fa < fb) {
+        // the coarse rows the band's prolongation reads
+        const float cinv = 1.0f / float(cnx);
+        for (int base = 0; base < CR * cnx; base += kBandBatch * T) {
+            float v[kBandBatch];
+#pragma unroll
+            for (int u = 0; u < kBandBatch; ++u) {
+                const int q = base + u * T + int(threadIdx.x);
+                const int dJ = div_small(q, cinv), I = q - dJ * cnx, J = cj0 + dJ;
+                const bool in = q < CR * cnx && J >= 0 && J < Cc.ny;
+                v[u] = in ? Cc.e[long(J) * cnx + I] : 0.0f;
+            }
+#pragma unroll
+            for (int u = 0; u < kBandBatch; ++u) {
+                const int q = base + u * T + int(threadIdx.x);
+                if (q < CR * cnx) sc[q] = v[u];
+            }
+        }
+        band_load(F, j0, R, se, sg, sm, true);
+        __syncthreads();
+        const float inv = 1.0f / float(nx);
+        for (int q = threadIdx.x; q < R * nx; q += T) {
+            if (sm[q]) continue;
+            const int lr = div_small(q, inv), i = q - lr * nx, j = j0 + lr;
+            const int c = ((j >> 1) - cj0) * cnx + (i >> 1);
+            float v;
+            if (!(i & 1) && !(j & 1)) v = sc[c];
+            else if ((i & 1) && !(j & 1)) v = 0.5f * (sc[c] + sc[c + 1]);
+            else if (!(i & 1) && (j & 1)) v = 0.5f * (sc[c] + sc[c + cnx]);
+            else v = 0.25f * (sc[c] + sc[c + 1] + sc[c + cnx] + sc[c + cnx + 1]);
+            se[q] += v;
+        }
+        __syncthreads();
+        band_sweeps(se, sg, sm, F, j0, R, post, omega);
+        const int N = (fb - fa) * nx;
+        if (phi) {
+            for (int base = 0; base < N; base += kBandBatch * T) {
+                double pv[kBandBatch];
+#pragma unroll
+                for (int u = 0; u < kBandBatch; ++u) {
+                    const int q = base + u * T + int(threadIdx.x);
+                    pv[u] = q < N ? phi[long(fa) * nx + q] : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < kBandBatch; ++u) {
+                    const int q = base + u * T + int(threadIdx.x);
+                    if (q < N) phi[long(fa) * nx + q] = pv[u] + double(se[H * nx + q]);
+                }
+            }
+        } else {
+            for (int q = threadIdx.x; q < N; q += T) F.e[long(fa) * nx + q] = se[H * nx + q];
+        }
+    }
+    __syncthreads();
+}
+
+// FP64 residual of phi on this CTA's rows of level 0 (written to g0 as the
+// next V-cycle's right-hand side) and the norms summed over the cluster in
+// rank order.
+__device__ void cluster_r0(const ClusterDesc& S, int rank, int parts, double* s_part, double& r2, double& f2) {
+    namespace cg = cooperative_groups;
+    int fa, fb;
+    band_rows(S.ny, parts, rank, fa, fb);
+    const int nx = S.nx, ny = S.ny, T = blockDim.x;
+    const double* __restrict__ phi = S.phi;
+    const uint8_t* __restrict__ mask = S.lv[0].mask;
+    double a = 0.0, b = 0.0;
+    const int N = (fb - fa) * nx;
+    const float inv = 1.0f / float(nx);
+    for (int base = 0; base < N; base += 4 * T) {
+        double rv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int q = base + u * T + int(threadIdx.x);
+            rv[u] = 0.0;
+            if (q >= N) continue;
+            const long k = long(fa) * nx + q;
+            const int lr = div_small(q, inv), i = q - lr * nx, j = fa + lr;
+            if (i > 0 && j > 0 && i < nx - 1 && j < ny - 1 && !mask[k]) {
+                const double c = phi[k];
+                const double lap =
+                    S.cx * ((phi[k - 1] - c) + (phi[k + 1] - c)) + S.cy * ((phi[k - nx] - c) + (phi[k + nx] - c));
+                const double fv = S.f[k];
+                rv[u] = fv - lap;
+                b += fv * fv;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int q = base + u * T + int(threadIdx.x);
+            if (q < N) S.lv[0].g[long(fa) * nx + q] = float(rv[u]);
+            a += rv[u] * rv[u];
+        }
+    }
+    __shared__ double ws[2][kClusterThreads / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    if (lane == 0) {
+        ws[0][w] = a;
+        ws[1][w] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sa = 0.0, sb = 0.0;
+        for (int q = 0; q < nw; ++q) {
+            sa += ws[0][q];
+            sb += ws[1][q];
+        }
+        s_part[0] = sa;
+        s_part[1] = sb;
+    }
+    cg::cluster_group cl = cg::this_cluster();
+    cl.sync();
+    double sa = 0.0, sb = 0.0;
+    for (int r = 0; r < parts; ++r) {
+        const double* p = cl.map_shared_rank(s_part, r);
+        sa += p[0];
+        sb += p[1];
+    }
+    r2 = sa;
+    f2 = sb;
+}
+
+__global__ void __launch_bounds__(kClusterThreads, 1) k_mg_cluster(ClusterDesc S) {
+    namespace cg = cooperative_groups;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ double s_part[2];
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = int(cl.block_rank()), parts = int(cl.num_blocks());
+    double r2 = 0.0, f2 = 0.0, dummy = 0.0;
+    cluster_r0(S, rank, parts, s_part, r2, f2);
+    const double ref = f2 > 0.0 ? f2 : 1.0;
+    int cycles = 0;
+    bool conv = r2 < S.tol2 * ref;
+    while (!conv && cycles < S.max_cycles) {
+        for (int l = 0; l < S.Lb; ++l) {
+            band_down(S.lv[l], S.lv[l + 1], S.omega, S.pre, rank, parts, smem);
+            cl.sync();
+        }
+        if (rank == 0) coarse_vcycle(S.coarse, smem);
+        cl.sync();
+        for (int l = S.Lb - 1; l >= 0; --l) {
+            band_up(S.lv[l], S.lv[l + 1], S.omega, S.post, l == 0 ? S.phi : nullptr, rank, parts, smem);
+            cl.sync();
+        }
+        cluster_r0(S, rank, parts, s_part, r2, dummy);
+        ++cycles;
+        conv = r2 < S.tol2 * ref;
+    }
+    if (rank == 0 && threadIdx.x == 0) {
+        S.N.norms[0] = f2;
+        S.N.norms[1] = r2;
+        *S.N.cycles = cycles;
+        *S.N.converged = conv ? 1 : 0;
+        *S.N.total += cycles;
+    }
+    // no CTA may exit while another can still read its shared memory
+    cl.sync();
+}
+
 // ---- host object ---------------------------------------------------------------
 
 struct MgImpl {
@@ -770,6 +1087,10 @@ struct MgImpl {
     size_t solve_smem = 0, coarse2_smem = 0;
     int coarse2_off_e[kMgMaxCoarseLevels]{}, coarse2_off_g[kMgMaxCoarseLevels]{}, coarse2_off_m[kMgMaxCoarseLevels]{};
     int solve_grid = 0;
+    // cluster-resident solve
+    bool cluster_ok = false;
+    int cluster_size = 0;
+    size_t cluster_smem = 0;
     GridBar* bar = nullptr;
     int* error = nullptr;
     cudaStream_t side = nullptr;
@@ -870,6 +1191,56 @@ static int configure_kernels(MgImpl& M) {
     return PIC_OK;
 }
 
+// Picks the cluster size (16 CTAs where the device allows, else 8) whose
+// band phases fit in shared memory; leaves cluster_ok false (the graph loop
+// is used instead) for FP64 levels or bands that do not fit.
+static int configure_cluster(MgImpl& M, const std::vector<int>& nxs, const std::vector<int>& nys) {
+    M.cluster_ok = false;
+    if (M.precision != PIC_MG_MIXED) return PIC_OK;
+    const int pre = M.o.pre_sweeps, post = M.o.post_sweeps;
+    for (int cs : {16, 8}) {
+        size_t need = M.coarse2_smem;
+        for (int l = 0; l < M.Lp; ++l) {
+            const size_t per = size_t((nys[l] + cs - 1) / cs);
+            const size_t Rd = per + 2 * size_t(2 * pre + 2), Ru = per + 4 * size_t(post);
+            const size_t down = Rd * nxs[l] * (2 * sizeof(float) + 1);
+            const size_t CR = Ru / 2 + 3;
+            const size_t up = Ru * nxs[l] * (2 * sizeof(float) + 1) + CR * nxs[l + 1] * sizeof(float);
+            need = std::max(need, std::max(down, up));
+        }
+        if (need > 227 * 1024) continue;
+        if (cs > 8 &&
+            cudaFuncSetAttribute(k_mg_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(k_mg_cluster), need));
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(cs);
+        cfg.blockDim = dim3(kClusterThreads);
+        cfg.dynamicSmemBytes = need;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = cs;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, k_mg_cluster, &cfg) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        if (n >= 1) {
+            M.cluster_ok = true;
+            M.cluster_size = cs;
+            M.cluster_smem = need;
+            return PIC_OK;
+        }
+    }
+    return PIC_OK;
+}
+
 static void mg_release(pic_mg* mg) {
     if (!mg) return;
     MgImpl& M = mg->m;
@@ -889,7 +1260,7 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
     M.o.precision = PIC_MG_MIXED;
     M.o.pre_sweeps = 2;
     M.o.post_sweeps = 2;
-    M.o.omega = 1.0;
+    M.o.omega = 1.15;
     M.o.coarsest_max = 9;
     if (opts) {
         M.o.precision = opts->precision;
@@ -907,7 +1278,7 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
         return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: unknown precision %d", M.o.precision));
     if (M.o.pre_sweeps > kMgMaxSweeps || M.o.post_sweeps > kMgMaxSweeps)
         return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: at most 8 pre/post sweeps"));
-    if (M.o.launch_mode < PIC_MG_PERSISTENT || M.o.launch_mode > PIC_MG_GRAPH_LOOP)
+    if (M.o.launch_mode < PIC_MG_PERSISTENT || M.o.launch_mode > PIC_MG_CLUSTER)
         return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: unknown launch mode %d", M.o.launch_mode));
     M.precision = M.o.precision;
     M.nx = nx;
@@ -1006,6 +1377,7 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
     int st = M.precision == PIC_MG_MIXED ? alloc_levels(M, M.lf, masks, nxs, nys)
                                          : alloc_levels(M, M.ld, masks, nxs, nys);
     if (st == PIC_OK) st = M.precision == PIC_MG_MIXED ? configure_kernels<float>(M) : configure_kernels<double>(M);
+    if (st == PIC_OK && M.o.launch_mode == PIC_MG_CLUSTER) st = configure_cluster(M, nxs, nys);
     if (st != PIC_OK) return bail(st);
     M.grd0 = dim3(div_up(nx, M.blk0.x), div_up(ny, M.blk0.y));
     // block partials of the residual norm: one pair per block of the level-0
@@ -1160,9 +1532,58 @@ static int launch_persistent(MgImpl& M, std::vector<LevelDev<T>>& lv, double* ph
     return PIC_OK;
 }
 
-// Appends the whole solve to a capture in progress on `st`: the persistent
-// kernel, or the residual and a WHILE node over V-cycles.
+static int launch_cluster(MgImpl& M, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
+    ClusterDesc S{};
+    S.L = M.L;
+    S.Lb = M.Lp;
+    for (int l = 0; l < M.L; ++l) S.lv[l] = M.lf[l];
+    CoarseDesc<float>& D = S.coarse;
+    D.nlev = M.L - M.Lp;
+    for (int c = 0; c < D.nlev; ++c) {
+        D.lv[c] = M.lf[M.Lp + c];
+        D.off_e[c] = M.coarse2_off_e[c];
+        D.off_g[c] = M.coarse2_off_g[c];
+        D.off_m[c] = M.coarse2_off_m[c];
+    }
+    D.ainv = M.ainv;
+    D.cidx = M.cidx;
+    D.nf = M.nfree_c;
+    D.omega = float(M.o.omega);
+    D.pre = M.o.pre_sweeps;
+    D.post = M.o.post_sweeps;
+    D.phi0 = M.Lp == 0 ? phi : nullptr;
+    S.f = f;
+    S.phi = phi;
+    S.nx = M.nx;
+    S.ny = M.ny;
+    S.cx = 1.0 / (M.dx * M.dx);
+    S.cy = 1.0 / (M.dy * M.dy);
+    S.N = M.N;
+    S.tol2 = tol * tol;
+    S.max_cycles = max_cycles;
+    S.omega = float(M.o.omega);
+    S.pre = M.o.pre_sweeps;
+    S.post = M.o.post_sweeps;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(M.cluster_size);
+    cfg.blockDim = dim3(kClusterThreads);
+    cfg.dynamicSmemBytes = M.cluster_smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = M.cluster_size;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    PIC_CUDA(cudaLaunchKernelEx(&cfg, k_mg_cluster, S));
+    return PIC_OK;
+}
+
+// Appends the whole solve to a capture in progress on `st`: the persistent or
+// cluster kernel, or the residual and a WHILE node over V-cycles.
 int mg_capture(MgImpl& M, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
+    if (M.o.launch_mode == PIC_MG_CLUSTER && M.cluster_ok) return launch_cluster(M, phi, f, tol, max_cycles, st);
     if (M.o.launch_mode == PIC_MG_PERSISTENT)
         return M.precision == PIC_MG_MIXED ? launch_persistent(M, M.lf, phi, f, tol, max_cycles, st)
                                            : launch_persistent(M, M.ld, phi, f, tol, max_cycles, st);
@@ -1248,6 +1669,7 @@ static int solve_eager(MgImpl& M, std::vector<LevelDev<T>>& lv, double* phi, con
 }
 
 int mg_launch(MgImpl& M, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
+    if (M.o.launch_mode == PIC_MG_CLUSTER && M.cluster_ok) return launch_cluster(M, phi, f, tol, max_cycles, st);
     if (M.o.launch_mode == PIC_MG_PERSISTENT)
         return M.precision == PIC_MG_MIXED ? launch_persistent(M, M.lf, phi, f, tol, max_cycles, st)
                                            : launch_persistent(M, M.ld, phi, f, tol, max_cycles, st);
@@ -1265,7 +1687,8 @@ int mg_solve(MgImpl& M, double* phi, const double* f, double tol, int max_cycles
     PIC_CUDA(cudaStreamSynchronize(st));
     pic_mg_info loc{};
     PIC_TRY(mg_read_info(M, &loc));
-    M.launches += 1 + (M.o.launch_mode == PIC_MG_PERSISTENT ? 0 : (long long)(loc.cycles) * M.body_launches);
+    const bool one_kernel = M.o.launch_mode == PIC_MG_PERSISTENT || (M.o.launch_mode == PIC_MG_CLUSTER && M.cluster_ok);
+    M.launches += 1 + (one_kernel ? 0 : (long long)(loc.cycles) * M.body_launches);
     if (info) *info = loc;
     if (!loc.converged)
         return fail(PIC_ERR_NOT_CONVERGED, "multigrid: relative residual %.3e after %d cycles (tol %.1e)", loc.rel_res,
@@ -1275,7 +1698,10 @@ int mg_solve(MgImpl& M, double* phi, const double* f, double tol, int max_cycles
 
 long long mg_launches(pic_mg* mg) { return mg ? mg->m.launches : 0; }
 int mg_body_launches(pic_mg* mg) {
-    return (mg && mg->m.o.launch_mode != PIC_MG_PERSISTENT) ? mg->m.body_launches : 0;
+    if (!mg) return 0;
+    const MgImpl& M = mg->m;
+    const bool one_kernel = M.o.launch_mode == PIC_MG_PERSISTENT || (M.o.launch_mode == PIC_MG_CLUSTER && M.cluster_ok);
+    return one_kernel ? 0 : M.body_launches;
 }
 int mg_capture_into(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
     return mg_capture(mg->m, phi, f, tol, max_cycles, st);
@@ -1297,6 +1723,14 @@ int pic_mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_dirichl
                   pic_mg** out) {
     clear_error();
     return mg_create(nx, ny, dx, dy, h_dirichlet, opts, out);
+}
+
+int pic_mg_effective_launch_mode(pic_mg* mg, int* mode) {
+    clear_error();
+    if (!mg || !mode) return fail(PIC_ERR_BAD_ARG, "pic_mg_effective_launch_mode: bad arguments");
+    const MgImpl& M = mg->m;
+    *mode = (M.o.launch_mode == PIC_MG_CLUSTER && !M.cluster_ok) ? int(PIC_MG_GRAPH_LOOP) : M.o.launch_mode;
+    return PIC_OK;
 }
 
 int pic_mg_destroy(pic_mg* mg) {

@@ -34,15 +34,15 @@ def ensemble_workloads(count=64, seed=2026, n_range=(100_000, 2_000_000), sides=
     return out
 
 
-def member_simulation(w: workloads.Workload, tile=16, sort_interval=20, coarsest_max=9, use_graph=True,
-                      seed=None) -> PICSimulation:
+def member_simulation(w: workloads.Workload, tile=16, sort_interval=20, coarsest_max=9, omega=1.15,
+                      mg_launch="graph", use_graph=True, seed=None) -> PICSimulation:
     """A collisionless simulation of workload w (graph-captured steps)."""
     mask, phi_bc = workloads.dirichlet(w)
     species = [dict(name="e", charge=-Consts.qe, mass=Consts.me, np2c=w.np2c(w.n_e), capacity=w.n_e + 64),
                dict(name="i", charge=Consts.qe, mass=workloads.ION_MASS, np2c=w.np2c(w.n_i), capacity=w.n_i + 64)]
     return PICSimulation(w.nodes, w.nodes, w.dx, w.dx, w.dt, species, mask, phi_bc, tol=w.tol, max_cycles=50,
                          sort_interval=sort_interval, tile=tile, mcc=None, seed=w.seed if seed is None else seed,
-                         use_graph=use_graph, mg_launch="graph", coarsest_max=coarsest_max)
+                         use_graph=use_graph, mg_launch=mg_launch, coarsest_max=coarsest_max, omega=omega)
 
 
 def member_arrays(w: workloads.Workload):

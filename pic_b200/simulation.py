@@ -58,7 +58,7 @@ class PICSimulation:
     """
 
     def __init__(self, nx, ny, dx, dy, dt, species, dirichlet, phi_bc=None, tol=1e-8, max_cycles=50,
-                 precision="mixed", pre_sweeps=2, post_sweeps=2, omega=1.0, sort_interval=20, tile=16,
+                 precision="mixed", pre_sweeps=2, post_sweeps=2, omega=1.15, sort_interval=20, tile=16,
                  mcc: MccTables | None = None, seed=0, use_graph=False, eps0=Consts.eps0, mg_launch="graph",
                  coarsest_max=9):
         self.nx, self.ny, self.dx, self.dy, self.dt = int(nx), int(ny), float(dx), float(dy), float(dt)

@@ -8,8 +8,8 @@ from pic_b200 import autotune
 
 
 def test_coordinate_descent_finds_the_separable_minimum():
-    # cost is separable with its minimum at tile 32, K 40, coarsest 5
-    want = {"tile": 32, "sort_interval": 40, "coarsest_max": 5}
+    # cost is separable with its minimum at tile 32, K 40, coarsest 5, omega 1.3, cluster solves
+    want = {"tile": 32, "sort_interval": 40, "coarsest_max": 5, "omega": 1.3, "mg_launch": "cluster"}
     calls = []
 
     def cost(cfg):
@@ -55,7 +55,7 @@ def test_tuning_a_small_member_on_the_gpu():
     from pic_b200 import workloads
 
     w = workloads.Workload("tune", 129, 40_000, 40_000, seed=3)
-    space = {"tile": (8, 16), "sort_interval": (10, 40), "coarsest_max": (9,)}
+    space = {"tile": (8, 16), "sort_interval": (10, 40), "coarsest_max": (9,), "omega": (1.15,), "mg_launch": ("graph",)}
     t = autotune.Autotuner(space=space, steps=20, warmup=2)
     ch = t.tune_workload(w)
     assert ch.tile in space["tile"] and ch.sort_interval in space["sort_interval"] and ch.coarsest_max == 9
