@@ -18,6 +18,7 @@
 // gather from and deposit to global memory directly.  Particles born since
 // the last sort are processed as untiled items.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstddef>
 #include <vector>
@@ -51,7 +52,6 @@ constexpr int kUnitMax = 8160;          // particles per work unit (one E tile s
 // (8160 * 2^19 = 2^32 - 2^24).
 constexpr float kFixScale = 524288.0f;  // 2^19
 constexpr float kFixInv = 1.0f / 524288.0f;
-constexpr int kBitWords = kChunk / 32 + 2;
 constexpr int kHalo = 4;                // cells staged around a tile
 constexpr int kArraySlack = 16;         // floats allocated past each species' capacity (bulk-copy window)
 constexpr unsigned long long kWaitLimit = 1ull << 24;  // bounded mbarrier wait
@@ -86,6 +86,7 @@ struct PushArgs {
     uint2 key;
     const uint32_t* step;
     BirthDev births;
+    const unsigned* cbits[PIC_MAX_SPECIES];  // null-collision candidate bit per slot (k_mcc_bits), or null
     int2* cand;       // collision candidates (species, slot), processed by k_collide after the pass
     int* cand_count;
     int cand_cap;
@@ -177,20 +178,30 @@ __device__ __forceinline__ ChunkDesc next_chunk(const PushArgs& A, const ChunkDe
     return d;
 }
 
-// Candidate bits of chunk c: segment g0 + t goes to the calling thread t
-// (t < nthreads).  The bit words start out zero: every candidate bit is
-// cleared again by the thread that consumes it.
-__device__ __noinline__ void mark_segments(const MccDev* __restrict__ M, const SpeciesState* __restrict__ state, int s,
-                                           int b, int e, uint32_t step, uint2 key, unsigned* bits, int t, int nthreads) {
-    const long g0 = b / long(kMccSegment), g1 = (e - 1) / long(kMccSegment);
-    const int slots = state[s].count;
-    for (long g = g0 + t; g <= g1; g += nthreads) mcc_mark_segment(M->sp[s], uint32_t(s), g, slots, b, e, step, key, bits);
-}
-
-__device__ __forceinline__ void mark_chunk(const PushArgs& A, const ChunkDesc& c, uint32_t step, unsigned* bits, int t,
-                                           int nthreads) {
-    if (!c.valid || !A.do_mcc || A.mcc->sp[c.s].nproc == 0) return;
-    mark_segments(A.mcc, A.state, c.s, c.b, c.e, step, A.key, bits, t, nthreads);
+// Null-collision candidates of a step, one bit per slot: one thread per
+// 256-slot segment draws the segment's geometric gaps (mcc_mark_segment) into
+// its eight words.  The draws depend only on (segment, step, species), not on
+// the particles, so the mask is ready before the particle pass reads it.
+__global__ void __launch_bounds__(256) k_mcc_bits(const MccDev* __restrict__ M, int nspecies,
+                                                  const uint32_t* __restrict__ step_ptr, uint2 key,
+                                                  unsigned* const* __restrict__ bits, const int* __restrict__ nseg) {
+    __shared__ unsigned w[256 * (kMccSegment / 32)];
+    constexpr int kW = kMccSegment / 32;
+    const uint32_t step = *step_ptr;
+    int g = blockIdx.x * blockDim.x + threadIdx.x, s = 0;
+    while (s < nspecies && g >= nseg[s]) g -= nseg[s++];
+    unsigned* mine = w + threadIdx.x * kW;
+#pragma unroll
+    for (int q = 0; q < kW; ++q) mine[q] = 0u;
+    if (s < nspecies && M->sp[s].nproc > 0) {
+        const int b = g * int(kMccSegment);
+        mcc_mark_segment(M->sp[s], uint32_t(s), long(g), INT_MAX, b, b + int(kMccSegment), step, key, mine);
+    }
+    if (s < nspecies) {
+        unsigned* out = bits[s] + long(g) * kW;
+#pragma unroll
+        for (int q = 0; q < kW; ++q) out[q] = mine[q];
+    }
 }
 
 // Stages the E tile of a unit's tile and zeroes its charge tile.
@@ -206,110 +217,129 @@ __device__ __forceinline__ void stage_tile(const PushArgs& A, int tile, float2* 
     }
 }
 
+// Bulk copies from shared memory back to global memory (one bulk group per
+// commit; wait_group.read N returns once at most N groups still read shared
+// memory).
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, unsigned bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+// Writes chunk c back from its buffer: the 16-byte-aligned middle of each
+// array by bulk copies (one thread).  The slots outside it (fewer than 4 at
+// each end) belong to neighbouring units on other CTAs' copies and go by
+// plain stores (store_chunk_edges).
+__device__ __forceinline__ void store_chunk_bulk(const PushArgs& A, const ChunkDesc& c, const float* buf) {
+    const int a0 = c.b & ~3, b4 = (c.b + 3) & ~3, e4 = c.e & ~3;
+    if (e4 <= b4) return;
+    const unsigned bytes = unsigned(e4 - b4) * 4u;
+    const SpeciesState& S = A.state[c.s];
+    fence_proxy_async();  // the threads' shared-memory writes, visible to the bulk copy
+#pragma unroll
+    for (int k = 0; k < 4; ++k) bulk_s2g(S.cur[k] + b4, buf + k * kBufStride + (b4 - a0), bytes);
+}
+
+__device__ __forceinline__ void store_chunk_edges(const PushArgs& A, const ChunkDesc& c, const float* buf, int tid) {
+    if (tid >= 24) return;
+    const int a0 = c.b & ~3, b4 = (c.b + 3) & ~3, e4 = c.e & ~3;
+    const int k = tid / 6, j = tid % 6;
+    const int slot = j < 3 ? c.b + j : max(e4, b4) + (j - 3);
+    const int lim = j < 3 ? min(b4, c.e) : c.e;
+    if (slot >= lim) return;
+    A.state[c.s].cur[k][slot] = buf[k * kBufStride + (slot - a0)];
+}
+
+constexpr int kStages = 3;  // chunk buffers: one loading, one in work, one draining to global memory
+
 // Work units (species, tile, slot range) are claimed from an atomic counter
-// and streamed through the CTA in chunks of kChunk particles: the bulk copy
-// of chunk k+1 runs while chunk k is processed, with one CTA barrier per
-// chunk (two more at the end of each unit, around the charge-tile flush).
-// The chunk after a non-final chunk is computed by every thread; only the
-// first chunk of a new unit is published through shared memory, across the
-// unit-end barrier.
+// and streamed through the CTA in chunks of kChunk particles over a ring of
+// three shared-memory buffers: the bulk load of chunk k+1, the work on chunk
+// k (results written back in place) and the bulk store of chunk k-1 overlap,
+// with one CTA barrier per chunk (two more at the end of each unit, around
+// the charge-tile flush).  The chunk after a non-final chunk is computed by
+// every thread; only the first chunk of a new unit is published through
+// shared memory, across the unit-end barrier.
 __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
     extern __shared__ __align__(128) unsigned char smem[];
-    float* bufs = reinterpret_cast<float*>(smem);  // [2][4][kBufStride]
+    float* bufs = reinterpret_cast<float*>(smem);  // [kStages][4][kBufStride]
     const int RW = A.rw;
-    float2* et = reinterpret_cast<float2*>(bufs + 2 * 4 * kBufStride);
+    float2* et = reinterpret_cast<float2*>(bufs + kStages * 4 * kBufStride);
     unsigned* rt = reinterpret_cast<unsigned*>(et + RW * RW);
-    unsigned* bits = reinterpret_cast<unsigned*>(rt + RW * RW);  // [2][kBitWords]
-    __shared__ __align__(8) unsigned long long bar[2];
-    __shared__ ChunkDesc s_ch[2];
+    __shared__ __align__(8) unsigned long long bar[kStages];
+    __shared__ ChunkDesc s_ch[kStages];
     __shared__ unsigned s_abs, s_cand;
-    const int tid = threadIdx.x, lane = tid & 31;
-    const uint32_t step = A.do_mcc ? *A.step : 0u;
+    const int tid = threadIdx.x;
     const int n_items = *A.n_items;
-    for (int q = tid; q < 2 * kBitWords; q += kPushThreads) bits[q] = 0;
-    __syncthreads();
-    if (tid < 32) {
-        if (tid == 0) {
-            mbar_init(&bar[0], 1);
-            mbar_init(&bar[1], 1);
-            fence_mbar_init();
-            s_abs = 0;
-            s_cand = 0;
-            ChunkDesc none;
-            none.valid = 0;
-            const ChunkDesc c = next_chunk(A, none, n_items);
-            s_ch[0] = c;
-            if (c.valid) issue_chunk(A, c, bufs, &bar[0]);
-        }
-        __syncwarp();
-        mark_chunk(A, s_ch[0], step, bits, lane, 32);
+    if (tid == 0) {
+        for (int k = 0; k < kStages; ++k) mbar_init(&bar[k], 1);
+        fence_mbar_init();
+        s_abs = 0;
+        s_cand = 0;
+        ChunkDesc none;
+        none.valid = 0;
+        const ChunkDesc c = next_chunk(A, none, n_items);
+        s_ch[0] = c;
+        if (c.valid) issue_chunk(A, c, bufs, &bar[0]);
     }
     __syncthreads();
     ChunkDesc ch = s_ch[0];
-    unsigned phase[2] = {0u, 0u};
+    ChunkDesc prev;  // the chunk processed before `ch`, still to be written back
+    prev.valid = 0;
+    unsigned phases = 0u;  // expected parity of each stage's mbarrier
     int cur = 0, ox = 0, oy = 0;
     if (ch.valid && ch.tile >= 0) stage_tile(A, ch.tile, et, rt, ox, oy);
     while (ch.valid) {
         const bool tiled = ch.tile >= 0;
-        const bool ok = mbar_wait(&bar[cur], phase[cur]);
-        phase[cur] ^= 1u;
+        const int prv = cur == 0 ? kStages - 1 : cur - 1;
+        const int nxt = cur == kStages - 1 ? 0 : cur + 1;
+        const unsigned par = (phases >> cur) & 1u;
+        const bool ok = mbar_wait(&bar[cur], par);
+        phases ^= 1u << cur;
         if (__syncthreads_or(!ok)) {
-            // give up on this launch: flag it, then wait (bounded) for the copies still in flight
+            // give up on this launch: flag it, then wait (bounded) for the one
+            // load in flight (the next chunk's load is issued only after a wait succeeds)
             if (tid == 0) {
                 atomicExch(A.error, 1);
-                mbar_wait(&bar[cur ^ 1], phase[cur ^ 1]);
+                mbar_wait(&bar[cur], par);
             }
             __syncthreads();
             break;
         }
-        // the other buffer is free: hand out and prefetch the next chunk, and
-        // mark its collision candidates (spread over the warps when the chunk
-        // continues this unit, by warp 0 when it opens a new one)
-        const bool continues = ch.e < ch.unit_e;
         if (tid == 0) {
+            // write back the previous chunk, then reuse the buffer of the one
+            // before it (its store has been read) for the next chunk's load
+            if (prev.valid) {
+                store_chunk_bulk(A, prev, bufs + prv * 4 * kBufStride);
+                bulk_commit();
+            }
+            bulk_wait_read1();
             const ChunkDesc nc = next_chunk(A, ch, n_items);
-            s_ch[cur ^ 1] = nc;
+            s_ch[nxt] = nc;
             if (nc.valid) {
                 fence_proxy_async();
-                issue_chunk(A, nc, bufs + (cur ^ 1) * 4 * kBufStride, &bar[cur ^ 1]);
+                issue_chunk(A, nc, bufs + nxt * 4 * kBufStride, &bar[nxt]);
             }
         }
-        if (continues) {
-            if (lane == 0) {
-                ChunkDesc nc = ch;
-                nc.b = ch.e;
-                nc.e = min(ch.unit_e, ch.e + kChunk);
-                mark_chunk(A, nc, step, bits + (cur ^ 1) * kBitWords, tid >> 5, kPushThreads / 32);
-            }
-        } else if (tid < 32) {
-            __syncwarp();
-            mark_chunk(A, s_ch[cur ^ 1], step, bits + (cur ^ 1) * kBitWords, lane, 32);
-        }
+        if (prev.valid) store_chunk_edges(A, prev, bufs + prv * 4 * kBufStride, tid);
         const int s = ch.s, b = ch.b, n = ch.e - ch.b;
         const int off = b & 3;
-        const float* const px = bufs + cur * 4 * kBufStride + off;
-        const float* const py = px + kBufStride;
-        const float* const pvx = py + kBufStride;
-        const float* const pvy = pvx + kBufStride;
-        const unsigned* const cb = bits + cur * kBitWords;  // read-only view of this chunk's candidate bits
+        float* const px = bufs + cur * 4 * kBufStride + off;
+        float* const py = px + kBufStride;
+        float* const pvx = py + kBufStride;
+        float* const pvy = pvx + kBufStride;
         const SpeciesConst C = A.sp[s];
-        float* const g = A.state[s].cur[0] + b;
-        const int gs = A.state[s].stride;
-        const bool mcc = A.do_mcc && A.mcc->sp[s].nproc > 0;
-        unsigned* const cbw = bits + cur * kBitWords;
+        const unsigned* const cbits = (A.do_mcc && A.mcc->sp[s].nproc > 0) ? A.cbits[s] : nullptr;
         unsigned my_abs = 0, my_cand = 0;
-#pragma unroll 1
+#pragma unroll
         for (int k = 0; k < kPushP; ++k) {
             const int l = tid * kPushP + k;
             if (l >= n) break;
-            bool candidate = false;
-            if (mcc) {
-                const unsigned bit = 1u << (l & 31);
-                if (cb[l >> 5] & bit) {
-                    candidate = true;
-                    atomicAnd(cbw + (l >> 5), ~bit);  // leave the word zero for the next chunk
-                }
-            }
+            const int slot = b + l;
+            const bool candidate = cbits && ((__ldg(cbits + (slot >> 5)) >> (slot & 31)) & 1u);
             float x = px[l], y = py[l];
             if (!is_live(x)) continue;
             float vx = pvx[l], vy = pvy[l];
@@ -339,8 +369,8 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
                 const int slot = atomicAdd(A.cand_count, 1);
                 if (slot < A.cand_cap) {
                     A.cand[slot] = make_int2(s, b + l);
-                    g[2 * gs + l] = vx;
-                    g[3 * gs + l] = vy;
+                    pvx[l] = vx;
+                    pvy[l] = vy;
                     continue;
                 }
                 atomicAdd(A.ctr + kCtrCandOverflow, 1ull);
@@ -354,10 +384,10 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
                     ++my_abs;
                 }
             }
-            g[l] = x;
-            g[gs + l] = y;
-            g[2 * gs + l] = vx;
-            g[3 * gs + l] = vy;
+            px[l] = x;
+            py[l] = y;
+            pvx[l] = vx;
+            pvy[l] = vy;
             if (A.do_deposit && is_live(x)) {
                 const Cic c = cic_weights(x, y, A.nx, A.ny);
                 const int li = c.i0 - ox, lj = c.j0 - oy;
@@ -378,10 +408,11 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
         }
         my_abs = __reduce_add_sync(0xffffffffu, my_abs);
         my_cand = __reduce_add_sync(0xffffffffu, my_cand);
-        if (lane == 0) {
+        if ((tid & 31) == 0) {
             if (my_abs) atomicAdd(&s_abs, my_abs);
             if (my_cand) atomicAdd(&s_cand, my_cand);
         }
+        prev = ch;
         if (ch.e < ch.unit_e) {
             // the unit continues: every thread derives the next chunk itself
             ch.b = ch.e;
@@ -405,11 +436,22 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
                 s_cand = 0;
             }
             __syncthreads();
-            ch = s_ch[cur ^ 1];
+            ch = s_ch[nxt];
             if (ch.valid && ch.tile >= 0) stage_tile(A, ch.tile, et, rt, ox, oy);
         }
-        cur ^= 1;
+        cur = nxt;
     }
+    // write back the last chunk processed, then wait for every bulk store
+    __syncthreads();
+    if (prev.valid) {
+        const int prv = cur == 0 ? kStages - 1 : cur - 1;
+        if (tid == 0) {
+            store_chunk_bulk(A, prev, bufs + prv * 4 * kBufStride);
+            bulk_commit();
+        }
+        store_chunk_edges(A, prev, bufs + prv * 4 * kBufStride, tid);
+    }
+    if (tid == 0) bulk_wait_all();
 }
 
 // The collision candidates of the pass: MCC, then the drift, absorption and
@@ -619,6 +661,10 @@ struct SimImpl {
     MccHost mcc;
     bool have_mcc = false;
     MccDev* mcc_dev = nullptr;  // device copy of mcc.dev
+    unsigned* cbits[PIC_MAX_SPECIES]{};  // candidate bit per slot of each colliding species
+    unsigned** d_cbits = nullptr;         // device copy of cbits
+    int* d_nseg = nullptr;                // 256-slot segments per species (0: no collisions)
+    int cbits_segments = 0;               // sum of d_nseg
     int2* cand = nullptr;       // collision candidates of one pass
     int* cand_count = nullptr;
     int cand_cap = 0;
@@ -722,6 +768,7 @@ static PushArgs push_args(SimImpl& S, int kick, int mcc, int drift, int deposit,
     A.key = make_uint2(uint32_t(S.d.seed), uint32_t(S.d.seed >> 32));
     A.step = S.step_ctr;
     A.births = S.births;
+    for (int s = 0; s < S.ns; ++s) A.cbits[s] = S.cbits[s];
     A.cand = S.cand;
     A.cand_count = S.cand_count;
     A.cand_cap = S.cand_cap;
@@ -740,12 +787,19 @@ static int particle_pass(SimImpl& S, cudaStream_t st, int kick, int mcc, int dri
     const PushArgs A = push_args(S, kick, mcc, drift, deposit, kick_factor);
     {
         PhaseTimer t(S, PIC_PHASE_PUSH, st);
+        if (A.do_mcc) {
+            k_mcc_bits<<<div_up(S.cbits_segments, 256), 256, 0, st>>>(S.mcc_dev, S.ns, S.step_ctr, A.key, S.d_cbits,
+                                                                     S.d_nseg);
+            S.launches += 1;
+        }
         k_push<<<S.push_grid, kPushThreads, S.push_smem, st>>>(A);
     }
     {
         PhaseTimer t(S, PIC_PHASE_MERGE, st);
         if (A.do_mcc) {
-            k_collide<<<64, 128, 0, st>>>(A);
+            // one thread per candidate: each is a long chain of dependent
+            // table lookups and Philox rounds
+            k_collide<<<4 * num_sms(), 128, 0, st>>>(A);
             S.launches += 1;
         }
         k_merge_births<<<64, 256, 0, st>>>(A);
@@ -907,6 +961,21 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
         for (int s = 0; s < S.ns; ++s) expect += S.mcc.p_null[s] * d->species[s].capacity;
     S.cand_cap = int(std::min(2.0e9, 8.0 * expect + 65536.0));
     PIC_TRY(dalloc(S, &S.cand, size_t(S.cand_cap)));
+    // candidate bit masks, one bit per slot of every colliding species
+    {
+        int nseg[PIC_MAX_SPECIES] = {};
+        S.cbits_segments = 0;
+        for (int s = 0; s < S.ns; ++s) {
+            if (!S.have_mcc || S.mcc.dev.sp[s].nproc == 0) continue;
+            nseg[s] = div_up(d->species[s].capacity + kArraySlack, kMccSegment);
+            PIC_TRY(dalloc(S, &S.cbits[s], size_t(nseg[s]) * (kMccSegment / 32)));
+            S.cbits_segments += nseg[s];
+        }
+        PIC_TRY(dalloc(S, &S.d_cbits, size_t(PIC_MAX_SPECIES)));
+        PIC_CUDA(cudaMemcpy(S.d_cbits, S.cbits, sizeof(unsigned*) * PIC_MAX_SPECIES, cudaMemcpyHostToDevice));
+        PIC_TRY(dalloc(S, &S.d_nseg, size_t(PIC_MAX_SPECIES)));
+        PIC_CUDA(cudaMemcpy(S.d_nseg, nseg, sizeof(int) * PIC_MAX_SPECIES, cudaMemcpyHostToDevice));
+    }
     PIC_TRY(dalloc(S, &S.cand_count, 1));
     PIC_TRY(dalloc(S, &S.ctr, size_t(kCtrCount)));
     PIC_TRY(dalloc(S, &S.error, 1));
@@ -930,8 +999,8 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
         PIC_CUDA(cudaMemcpy(S.phi, phi0.data(), sizeof(double) * S.G, cudaMemcpyHostToDevice));
     }
     // launch shape of the particle pass
-    S.push_smem = sizeof(float) * 2 * 4 * kBufStride + size_t(S.rw) * S.rw * (sizeof(float2) + sizeof(unsigned)) +
-                  sizeof(unsigned) * 2 * kBitWords;
+    S.push_smem =
+        sizeof(float) * kStages * 4 * kBufStride + size_t(S.rw) * S.rw * (sizeof(float2) + sizeof(unsigned));
     PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(k_push), S.push_smem));
     int per_sm = 0;
     PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_push, kPushThreads, S.push_smem));
@@ -1223,7 +1292,7 @@ int pic_sim_step(pic_sim* sim, int n_steps, void* stream) {
             cudaGraphExec_t& g = sort ? S.g_sort_step : S.g_step;
             if (!g) PIC_TRY(capture_step(S, sort, &g));
             PIC_CUDA(cudaGraphLaunch(g, st));
-            S.launches += 3 + (S.have_mcc ? 1 : 0) + 2 + (sort ? 1 + (long long)S.ns * (5 + 3 * S.sorter.passes) : 0);
+            S.launches += 3 + (S.have_mcc ? 2 : 0) + 2 + (sort ? 1 + (long long)S.ns * (5 + 3 * S.sorter.passes) : 0);
             S.solves += 1;
         } else {
             if (sort) PIC_TRY(sort_all(S, st));
@@ -1418,7 +1487,7 @@ int pic_ens_step(pic_ens* e, int n_steps, void* stream) {
         if (S->d.sort_interval > 0)
             for (long long k = S->steps; k < S->steps + n_steps; ++k) sorts += (k % S->d.sort_interval == 0);
         // the step counter, the particle pass (3, plus the collisions), the RHS and E
-        S->launches += n_steps * (1LL + 3 + (S->have_mcc ? 1 : 0) + 2) +
+        S->launches += n_steps * (1LL + 3 + (S->have_mcc ? 2 : 0) + 2) +
                        sorts * (1 + (long long)S->ns * (5 + 3 * S->sorter.passes));
         if (S->d.sort_interval > 0) S->launches += n_steps;  // the sort condition
         S->solves += n_steps;
