@@ -61,7 +61,19 @@ template <class T>
 struct CoarseDesc {
     int nlev;
     LevelDev<T> lv[kMgMaxCoarseLevels];
-    int off_e[kMgMaxCoarseLevels], off_g[kMgMaxCoarseLevels], off_m[kMgMaxCoarseLevels];  // bytes into smem
+    // shared memory, in bytes: the e arrays [0, e_bytes), then the g arrays, the
+    // masks [m_off, ...) and, when they fit, the dense inverse (a_off) and its
+    // node table (c_off); a_off < 0 reads those two from global memory
+    int off_e[kMgMaxCoarseLevels], off_g[kMgMaxCoarseLevels], off_m[kMgMaxCoarseLevels];
+    int e_bytes, m_off, a_off, c_off;
+    // 16-byte sources of the one batch of loads that fills shared memory: the
+    // mask image (edges and electrodes of every level), the finest level's g,
+    // the inverse and the table; *_vec = 16-byte words of each
+    const uint4* mimg;
+    const uint4* g16;
+    const uint4* ainv16;
+    const uint4* cidx16;
+    int m_vec, g_vec, a_vec, c_vec;
     const double* ainv;
     const int* cidx;
     int nf;
@@ -389,14 +401,38 @@ __device__ void coarse_vcycle(const CoarseDesc<T>& D, unsigned char* smem) {
     auto E = [&](int l) { return reinterpret_cast<T*>(smem + D.off_e[l]); };
     auto Gs = [&](int l) { return reinterpret_cast<T*>(smem + D.off_g[l]); };
     auto M = [&](int l) { return smem + D.off_m[l]; };
-    for (int l = 0; l < D.nlev; ++l) {
-        const LevelDev<T>& L = D.lv[l];
-        const float inv_nx = 1.0f / float(L.nx);
-        for (int q = threadIdx.x; q < L.nx * L.ny; q += blockDim.x) {
-            const int j = div_small(q, inv_nx), i = q - j * L.nx;
-            M(l)[q] = (i == 0 || j == 0 || i == L.nx - 1 || j == L.ny - 1 || L.mask[q]) ? 1 : 0;
-            E(l)[q] = T(0);
-            if (l == 0) Gs(0)[q] = L.g[q];
+    {
+        uint4* s4 = reinterpret_cast<uint4*>(smem);
+        const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+        for (int q = threadIdx.x; q < D.e_bytes / 16; q += blockDim.x) s4[q] = z;
+        // every global read of the set in one batch: each thread issues its
+        // loads before storing any of them
+        const int n1 = D.m_vec, n2 = n1 + D.g_vec, n3 = n2 + D.a_vec, n4 = n3 + D.c_vec;
+        for (int base = 0; base < n4; base += 4 * int(blockDim.x)) {
+            uint4 v[4];
+            int dst[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int q = base + u * int(blockDim.x) + int(threadIdx.x);
+                dst[u] = -1;
+                v[u] = z;
+                if (q < n1) {
+                    v[u] = __ldg(D.mimg + q);
+                    dst[u] = D.m_off / 16 + q;
+                } else if (q < n2) {
+                    v[u] = D.g16[q - n1];
+                    dst[u] = D.off_g[0] / 16 + (q - n1);
+                } else if (q < n3) {
+                    v[u] = __ldg(D.ainv16 + (q - n2));
+                    dst[u] = D.a_off / 16 + (q - n2);
+                } else if (q < n4) {
+                    v[u] = __ldg(D.cidx16 + (q - n3));
+                    dst[u] = D.c_off / 16 + (q - n3);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (dst[u] >= 0) s4[dst[u]] = v[u];
         }
     }
     __syncthreads();
@@ -433,15 +469,17 @@ __device__ void coarse_vcycle(const CoarseDesc<T>& D, unsigned char* smem) {
         __syncthreads();
     }
     // dense direct solve on the coarsest level: one warp per row, lanes
-    // striding over the (coalesced) row of the inverse
+    // striding over the row of the inverse (in shared memory when it fits)
     {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        const double* ainv = D.a_off >= 0 ? reinterpret_cast<const double*>(smem + D.a_off) : D.ainv;
+        const int* cidx = D.a_off >= 0 ? reinterpret_cast<const int*>(smem + D.c_off) : D.cidx;
         for (int a = warp; a < D.nf; a += nw) {
-            const double* row = D.ainv + long(a) * D.nf;
+            const double* row = ainv + long(a) * D.nf;
             double s = 0.0;
-            for (int b = lane; b < D.nf; b += 32) s += row[b] * double(Gs(last)[D.cidx[b]]);
+            for (int b = lane; b < D.nf; b += 32) s += row[b] * double(Gs(last)[cidx[b]]);
             s = warp_sum(s);
-            if (lane == 0) E(last)[D.cidx[a]] = T(s);
+            if (lane == 0) E(last)[cidx[a]] = T(s);
         }
     }
     __syncthreads();
@@ -1065,6 +1103,16 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_mg_cluster(ClusterDesc S
 
 // ---- host object ---------------------------------------------------------------
 
+// Shared-memory layout of a set of coarse levels (see CoarseDesc).
+struct CoarseLayout {
+    int first = 0;
+    int off_e[kMgMaxCoarseLevels]{}, off_g[kMgMaxCoarseLevels]{}, off_m[kMgMaxCoarseLevels]{};
+    int e_bytes = 0, m_off = 0, a_off = -1, c_off = -1;
+    int m_vec = 0, g_vec = 0, a_vec = 0, c_vec = 0;
+    size_t smem = 0;
+    uint4* mimg = nullptr;
+};
+
 struct MgImpl {
     int precision = PIC_MG_MIXED;
     int nx = 0, ny = 0, L = 0, Lc = 0;
@@ -1078,14 +1126,12 @@ struct MgImpl {
     int nfree_c = 0;
     NormState N{};
     dim3 blk0{32, 8}, grd0;
-    size_t coarse_smem = 0;
-    int coarse_off_e[kMgMaxCoarseLevels]{}, coarse_off_g[kMgMaxCoarseLevels]{}, coarse_off_m[kMgMaxCoarseLevels]{};
+    CoarseLayout cl[2];  // the coarse kernel's levels (from Lc) and the persistent/cluster ones (from Lp)
     long long launches = 0;  // kernels executed by solves
     int body_launches = 0;   // kernels per V-cycle (graph and host loops)
     // persistent cooperative solve
     int Lp = 0;
-    size_t solve_smem = 0, coarse2_smem = 0;
-    int coarse2_off_e[kMgMaxCoarseLevels]{}, coarse2_off_g[kMgMaxCoarseLevels]{}, coarse2_off_m[kMgMaxCoarseLevels]{};
+    size_t solve_smem = 0;
     int solve_grid = 0;
     // cluster-resident solve
     bool cluster_ok = false;
@@ -1129,12 +1175,14 @@ static int alloc_levels(MgImpl& M, std::vector<LevelDev<T>>& lv, const std::vect
         M.allocs.push_back(mk);
         PIC_CUDA(cudaMemcpy(mk, masks[l].data(), G, cudaMemcpyHostToDevice));
         v.mask = mk;
-        PIC_CUDA(cudaMalloc(&v.e, G * sizeof(T)));
+        // padded to 16 bytes: the coarse kernel reads g in 16-byte words
+        const size_t bytes = (G * sizeof(T) + 15) / 16 * 16;
+        PIC_CUDA(cudaMalloc(&v.e, bytes));
         M.allocs.push_back(v.e);
-        PIC_CUDA(cudaMalloc(&v.g, G * sizeof(T)));
+        PIC_CUDA(cudaMalloc(&v.g, bytes));
         M.allocs.push_back(v.g);
-        PIC_CUDA(cudaMemset(v.e, 0, G * sizeof(T)));
-        PIC_CUDA(cudaMemset(v.g, 0, G * sizeof(T)));
+        PIC_CUDA(cudaMemset(v.e, 0, bytes));
+        PIC_CUDA(cudaMemset(v.g, 0, bytes));
         lv.push_back(v);
     }
     return PIC_OK;
@@ -1176,19 +1224,101 @@ static bool invert(std::vector<double>& a, int n) {
 template <class T>
 static int configure_kernels(MgImpl& M) {
     const size_t down = down_smem<T>(M.o.pre_sweeps), up = up_smem<T>(M.o.post_sweeps);
-    if (down > 227 * 1024 || up > 227 * 1024 || M.coarse_smem > 227 * 1024)
+    if (down > 227 * 1024 || up > 227 * 1024 || M.cl[0].smem > 227 * 1024 || M.cl[1].smem > 227 * 1024)
         return fail(PIC_ERR_BAD_ARG, "multigrid: shared memory too large (sweeps %d/%d)", M.o.pre_sweeps,
                     M.o.post_sweeps);
     PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(down_kernel<T>(M.o.pre_sweeps)), down));
     PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(up_kernel<T>(M.o.post_sweeps)), up));
-    PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(k_mg_coarse<T>), M.coarse_smem));
-    M.solve_smem = std::max(std::max(down, up), M.coarse2_smem);
+    PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(k_mg_coarse<T>), M.cl[0].smem));
+    M.solve_smem = std::max(std::max(down, up), M.cl[1].smem);
     PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(k_mg_solve<T>), M.solve_smem));
     int per_sm = 0;
     PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mg_solve<T>, kMgThreads, M.solve_smem));
     if (per_sm < 1) return fail(PIC_ERR_CUDA, "multigrid: the persistent kernel does not fit on an SM");
     M.solve_grid = std::min(per_sm, 2) * num_sms();
     return PIC_OK;
+}
+
+static size_t pad16(size_t n) { return (n + 15) / 16 * 16; }
+
+// Shared-memory layout of levels [first, L) for the single-block coarse
+// V-cycle, and the device image of their masks (grid edges included).
+static int build_layout(MgImpl& M, int first, const std::vector<int>& nxs, const std::vector<int>& nys,
+                        const std::vector<std::vector<uint8_t>>& masks, size_t esz, CoarseLayout& C) {
+    C.first = first;
+    size_t off = 0;
+    for (int l = first; l < M.L; ++l) {
+        C.off_e[l - first] = int(off);
+        off += pad16(size_t(nxs[l]) * nys[l] * esz);
+    }
+    C.e_bytes = int(off);
+    for (int l = first; l < M.L; ++l) {
+        C.off_g[l - first] = int(off);
+        off += pad16(size_t(nxs[l]) * nys[l] * esz);
+    }
+    C.m_off = int(off);
+    std::vector<uint8_t> img;
+    for (int l = first; l < M.L; ++l) {
+        C.off_m[l - first] = int(off);
+        const int nx = nxs[l], ny = nys[l];
+        const size_t G = size_t(nx) * ny;
+        std::vector<uint8_t> m(pad16(G), 1);
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i)
+                m[size_t(j) * nx + i] = (i == 0 || j == 0 || i == nx - 1 || j == ny - 1 || masks[l][size_t(j) * nx + i]);
+        img.insert(img.end(), m.begin(), m.end());
+        off += m.size();
+    }
+    C.m_vec = int(img.size() / 16);
+    if (cudaMalloc(&C.mimg, img.size()) != cudaSuccess) return PIC_ERR_CUDA;
+    M.allocs.push_back(C.mimg);
+    if (cudaMemcpy(C.mimg, img.data(), img.size(), cudaMemcpyHostToDevice) != cudaSuccess) return PIC_ERR_CUDA;
+    C.g_vec = int(pad16(size_t(nxs[first]) * nys[first] * esz) / 16);
+    const size_t nf = size_t(M.nfree_c), ab = pad16(nf * nf * sizeof(double)), cb = pad16(nf * sizeof(int));
+    if (nf > 0 && off + ab + cb <= 200 * 1024) {
+        C.a_off = int(off);
+        off += ab;
+        C.c_off = int(off);
+        off += cb;
+        C.a_vec = int(ab / 16);
+        C.c_vec = int(cb / 16);
+    } else {
+        C.a_off = C.c_off = -1;
+        C.a_vec = C.c_vec = 0;
+    }
+    C.smem = off;
+    return PIC_OK;
+}
+
+template <class T>
+static void fill_coarse(const MgImpl& M, const CoarseLayout& C, const std::vector<LevelDev<T>>& lv, double* phi,
+                        CoarseDesc<T>& D) {
+    D.nlev = M.L - C.first;
+    for (int c = 0; c < D.nlev; ++c) {
+        D.lv[c] = lv[C.first + c];
+        D.off_e[c] = C.off_e[c];
+        D.off_g[c] = C.off_g[c];
+        D.off_m[c] = C.off_m[c];
+    }
+    D.e_bytes = C.e_bytes;
+    D.m_off = C.m_off;
+    D.a_off = C.a_off;
+    D.c_off = C.c_off;
+    D.mimg = C.mimg;
+    D.g16 = reinterpret_cast<const uint4*>(lv[C.first].g);
+    D.ainv16 = reinterpret_cast<const uint4*>(M.ainv);
+    D.cidx16 = reinterpret_cast<const uint4*>(M.cidx);
+    D.m_vec = C.m_vec;
+    D.g_vec = C.g_vec;
+    D.a_vec = C.a_vec;
+    D.c_vec = C.c_vec;
+    D.ainv = M.ainv;
+    D.cidx = M.cidx;
+    D.nf = M.nfree_c;
+    D.omega = T(M.o.omega);
+    D.pre = M.o.pre_sweeps;
+    D.post = M.o.post_sweeps;
+    D.phi0 = C.first == 0 ? phi : nullptr;
 }
 
 // Picks the cluster size (16 CTAs where the device allows, else 8) whose
@@ -1199,7 +1329,7 @@ static int configure_cluster(MgImpl& M, const std::vector<int>& nxs, const std::
     if (M.precision != PIC_MG_MIXED) return PIC_OK;
     const int pre = M.o.pre_sweeps, post = M.o.post_sweeps;
     for (int cs : {16, 8}) {
-        size_t need = M.coarse2_smem;
+        size_t need = M.cl[1].smem;
         for (int l = 0; l < M.Lp; ++l) {
             const size_t per = size_t((nys[l] + cs - 1) / cs);
             const size_t Rd = per + 2 * size_t(2 * pre + 2), Ru = per + 4 * size_t(post);
@@ -1337,43 +1467,26 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
             }
         }
         if (!invert(A, n)) return bail(fail(PIC_ERR_NUMERIC, "pic_mg_create: singular coarsest system"));
-        if (cudaMalloc(&M.ainv, A.size() * sizeof(double)) != cudaSuccess)
+        // padded to 16 bytes: the coarse kernel reads both in 16-byte words
+        const size_t ab = (A.size() * sizeof(double) + 15) / 16 * 16, cb = (idx.size() * sizeof(int) + 15) / 16 * 16;
+        if (cudaMalloc(&M.ainv, ab) != cudaSuccess)
             return bail(fail(PIC_ERR_CUDA, "pic_mg_create: out of device memory"));
         M.allocs.push_back(M.ainv);
+        cudaMemset(M.ainv, 0, ab);
         cudaMemcpy(M.ainv, A.data(), A.size() * sizeof(double), cudaMemcpyHostToDevice);
-        if (cudaMalloc(&M.cidx, idx.size() * sizeof(int)) != cudaSuccess)
+        if (cudaMalloc(&M.cidx, cb) != cudaSuccess)
             return bail(fail(PIC_ERR_CUDA, "pic_mg_create: out of device memory"));
         M.allocs.push_back(M.cidx);
+        cudaMemset(M.cidx, 0, cb);
         cudaMemcpy(M.cidx, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice);
     }
     const size_t esz = M.precision == PIC_MG_MIXED ? sizeof(float) : sizeof(double);
-    size_t off = 0;
-    for (int l = M.Lc; l < M.L; ++l) {
-        const size_t G = size_t(nxs[l]) * nys[l];
-        const int c = l - M.Lc;
-        M.coarse_off_e[c] = int(off);
-        off += ((G * esz + 15) / 16) * 16;
-        M.coarse_off_g[c] = int(off);
-        off += ((G * esz + 15) / 16) * 16;
-        M.coarse_off_m[c] = int(off);
-        off += ((G + 15) / 16) * 16;
-    }
-    M.coarse_smem = off;
     M.Lp = 0;
     while (M.Lp < M.L && long(nxs[M.Lp]) * nys[M.Lp] > kPersistCoarseMax) ++M.Lp;
     if (M.L - M.Lp > kMgMaxCoarseLevels) M.Lp = M.L - kMgMaxCoarseLevels;
-    off = 0;
-    for (int l = M.Lp; l < M.L; ++l) {
-        const size_t G = size_t(nxs[l]) * nys[l];
-        const int c = l - M.Lp;
-        M.coarse2_off_e[c] = int(off);
-        off += ((G * esz + 15) / 16) * 16;
-        M.coarse2_off_g[c] = int(off);
-        off += ((G * esz + 15) / 16) * 16;
-        M.coarse2_off_m[c] = int(off);
-        off += ((G + 15) / 16) * 16;
-    }
-    M.coarse2_smem = off;
+    if (build_layout(M, M.Lc, nxs, nys, masks, esz, M.cl[0]) != PIC_OK ||
+        build_layout(M, M.Lp, nxs, nys, masks, esz, M.cl[1]) != PIC_OK)
+        return bail(fail(PIC_ERR_CUDA, "pic_mg_create: out of device memory"));
     int st = M.precision == PIC_MG_MIXED ? alloc_levels(M, M.lf, masks, nxs, nys)
                                          : alloc_levels(M, M.ld, masks, nxs, nys);
     if (st == PIC_OK) st = M.precision == PIC_MG_MIXED ? configure_kernels<float>(M) : configure_kernels<double>(M);
@@ -1419,21 +1532,8 @@ static int launch_cycle(MgImpl& M, std::vector<LevelDev<T>>& lv, double* phi, co
         ++count;
     }
     CoarseDesc<T> D{};
-    D.nlev = M.L - M.Lc;
-    for (int c = 0; c < D.nlev; ++c) {
-        D.lv[c] = lv[M.Lc + c];
-        D.off_e[c] = M.coarse_off_e[c];
-        D.off_g[c] = M.coarse_off_g[c];
-        D.off_m[c] = M.coarse_off_m[c];
-    }
-    D.ainv = M.ainv;
-    D.cidx = M.cidx;
-    D.nf = M.nfree_c;
-    D.omega = omega;
-    D.pre = M.o.pre_sweeps;
-    D.post = M.o.post_sweeps;
-    D.phi0 = M.Lc == 0 ? phi : nullptr;
-    k_mg_coarse<T><<<1, kCoarseThreads, M.coarse_smem, st>>>(D);
+    fill_coarse(M, M.cl[0], lv, phi, D);
+    k_mg_coarse<T><<<1, kCoarseThreads, M.cl[0].smem, st>>>(D);
     ++count;
     for (int l = M.Lc - 1; l >= 0; --l) {
         const dim3 g(div_up(lv[l].nx, kMgTile), div_up(lv[l].ny, kMgTile));
@@ -1489,21 +1589,7 @@ static int launch_persistent(MgImpl& M, std::vector<LevelDev<T>>& lv, double* ph
     S.L = M.L;
     S.Lp = M.Lp;
     for (int l = 0; l < M.L; ++l) S.lv[l] = lv[l];
-    CoarseDesc<T>& D = S.coarse;
-    D.nlev = M.L - M.Lp;
-    for (int c = 0; c < D.nlev; ++c) {
-        D.lv[c] = lv[M.Lp + c];
-        D.off_e[c] = M.coarse2_off_e[c];
-        D.off_g[c] = M.coarse2_off_g[c];
-        D.off_m[c] = M.coarse2_off_m[c];
-    }
-    D.ainv = M.ainv;
-    D.cidx = M.cidx;
-    D.nf = M.nfree_c;
-    D.omega = T(M.o.omega);
-    D.pre = M.o.pre_sweeps;
-    D.post = M.o.post_sweeps;
-    D.phi0 = M.Lp == 0 ? phi : nullptr;
+    fill_coarse(M, M.cl[1], lv, phi, S.coarse);
     S.f = f;
     S.phi = phi;
     S.nx = M.nx;
@@ -1537,21 +1623,7 @@ static int launch_cluster(MgImpl& M, double* phi, const double* f, double tol, i
     S.L = M.L;
     S.Lb = M.Lp;
     for (int l = 0; l < M.L; ++l) S.lv[l] = M.lf[l];
-    CoarseDesc<float>& D = S.coarse;
-    D.nlev = M.L - M.Lp;
-    for (int c = 0; c < D.nlev; ++c) {
-        D.lv[c] = M.lf[M.Lp + c];
-        D.off_e[c] = M.coarse2_off_e[c];
-        D.off_g[c] = M.coarse2_off_g[c];
-        D.off_m[c] = M.coarse2_off_m[c];
-    }
-    D.ainv = M.ainv;
-    D.cidx = M.cidx;
-    D.nf = M.nfree_c;
-    D.omega = float(M.o.omega);
-    D.pre = M.o.pre_sweeps;
-    D.post = M.o.post_sweeps;
-    D.phi0 = M.Lp == 0 ? phi : nullptr;
+    fill_coarse(M, M.cl[1], M.lf, phi, S.coarse);
     S.f = f;
     S.phi = phi;
     S.nx = M.nx;
