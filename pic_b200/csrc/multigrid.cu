@@ -48,14 +48,31 @@ constexpr int kMgMaxLevels = 16;
 constexpr long kPersistCoarseMax = 33L * 33L;    // levels the persistent kernel's single block solves
 constexpr unsigned long long kBarrierPolls = 1ull << 24;  // a grid barrier gives up (error flag) after this
 
+// One level of the hierarchy.  The correction has two arrays: the down
+// phase writes e, and the up phase reads e (with its halo) and writes its
+// result to eu, so that no kernel reads a neighbour tile's e while another
+// CTA overwrites it.  ec is the correction the next finer level prolongs:
+// eu on levels the up kernels smooth, e on the first level of a single-block
+// coarse V-cycle (which writes e); the launch code sets it per launch mode.
 template <class T>
 struct LevelDev {
     int nx, ny;
     T cx, cy, inv_diag;
     const uint8_t* mask;  // 1 = Dirichlet
     T* e;
+    T* eu;
+    T* ec;
     T* g;
 };
+
+// The levels as a launch mode uses them: up phases on the levels below
+// `first_coarse` (their final correction is eu), the coarse V-cycle from it.
+template <class T>
+static std::vector<LevelDev<T>> with_corrections(const std::vector<LevelDev<T>>& lv, int first_coarse) {
+    std::vector<LevelDev<T>> out = lv;
+    for (size_t l = 0; l < out.size(); ++l) out[l].ec = int(l) < first_coarse ? out[l].eu : out[l].e;
+    return out;
+}
 
 template <class T>
 struct CoarseDesc {
@@ -241,7 +258,7 @@ __device__ void up_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, do
         const int q = it * kMgThreads + tid;
         const int I = cox + q % CW, J = coy + q / CW;
         const bool in = q < CW * CW && I >= 0 && J >= 0 && I < Cc.nx && J < Cc.ny;
-        cv[it] = in ? Cc.e[long(J) * Cc.nx + I] : T(0);
+        cv[it] = in ? Cc.ec[long(J) * Cc.nx + I] : T(0);
     }
     double pv[OIT];
 #pragma unroll
@@ -290,7 +307,7 @@ __device__ void up_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, do
         const long k = long(j) * F.nx + i;
         const T v = se[(H + q / kMgTile) * W + H + q % kMgTile];
         if (phi) phi[k] = pv[it] + double(v);
-        else F.e[k] = v;
+        else F.ec[k] = v;
     }
     __syncthreads();  // the caller may reuse the shared tile
 }
@@ -950,7 +967,7 @@ __device__ void band_up(const LevelDev<float>& F, const LevelDev<float>& Cc, flo
                 const int q = base + u * T + int(threadIdx.x);
                 const int dJ = div_small(q, cinv), I = q - dJ * cnx, J = cj0 + dJ;
                 const bool in = q < CR * cnx && J >= 0 && J < Cc.ny;
-                v[u] = in ? Cc.e[long(J) * cnx + I] : 0.0f;
+                v[u] = in ? Cc.ec[long(J) * cnx + I] : 0.0f;
             }
 #pragma unroll
             for (int u = 0; u < kBandBatch; ++u) {
@@ -990,7 +1007,7 @@ __device__ void band_up(const LevelDev<float>& F, const LevelDev<float>& Cc, flo
                 }
             }
         } else {
-            for (int q = threadIdx.x; q < N; q += T) F.e[long(fa) * nx + q] = se[H * nx + q];
+            for (int q = threadIdx.x; q < N; q += T) F.ec[long(fa) * nx + q] = se[H * nx + q];
         }
     }
     __syncthreads();
@@ -1179,10 +1196,14 @@ static int alloc_levels(MgImpl& M, std::vector<LevelDev<T>>& lv, const std::vect
         const size_t bytes = (G * sizeof(T) + 15) / 16 * 16;
         PIC_CUDA(cudaMalloc(&v.e, bytes));
         M.allocs.push_back(v.e);
+        PIC_CUDA(cudaMalloc(&v.eu, bytes));
+        M.allocs.push_back(v.eu);
         PIC_CUDA(cudaMalloc(&v.g, bytes));
         M.allocs.push_back(v.g);
         PIC_CUDA(cudaMemset(v.e, 0, bytes));
+        PIC_CUDA(cudaMemset(v.eu, 0, bytes));
         PIC_CUDA(cudaMemset(v.g, 0, bytes));
+        v.ec = v.e;
         lv.push_back(v);
     }
     return PIC_OK;
@@ -1519,8 +1540,9 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
 
 // One V-cycle followed by the residual check, launched on stream st.
 template <class T>
-static int launch_cycle(MgImpl& M, std::vector<LevelDev<T>>& lv, double* phi, const double* f, double tol,
+static int launch_cycle(MgImpl& M, std::vector<LevelDev<T>>& lv_in, double* phi, const double* f, double tol,
                         int max_cycles, cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st, int& count) {
+    const std::vector<LevelDev<T>> lv = with_corrections(lv_in, M.Lc);
     const T omega = T(M.o.omega);
     const size_t down = down_smem<T>(M.o.pre_sweeps), up = up_smem<T>(M.o.post_sweeps);
     const DownKernel<T> kdown = down_kernel<T>(M.o.pre_sweeps);
@@ -1583,8 +1605,9 @@ static int capture_solve(MgImpl& M, std::vector<LevelDev<T>>& lv, double* phi, c
 }
 
 template <class T>
-static int launch_persistent(MgImpl& M, std::vector<LevelDev<T>>& lv, double* phi, const double* f, double tol,
+static int launch_persistent(MgImpl& M, std::vector<LevelDev<T>>& lv_in, double* phi, const double* f, double tol,
                              int max_cycles, cudaStream_t st) {
+    const std::vector<LevelDev<T>> lv = with_corrections(lv_in, M.Lp);
     SolveDesc<T> S{};
     S.L = M.L;
     S.Lp = M.Lp;
@@ -1622,8 +1645,9 @@ static int launch_cluster(MgImpl& M, double* phi, const double* f, double tol, i
     ClusterDesc S{};
     S.L = M.L;
     S.Lb = M.Lp;
-    for (int l = 0; l < M.L; ++l) S.lv[l] = M.lf[l];
-    fill_coarse(M, M.cl[1], M.lf, phi, S.coarse);
+    const std::vector<LevelDev<float>> lv = with_corrections(M.lf, M.Lp);
+    for (int l = 0; l < M.L; ++l) S.lv[l] = lv[l];
+    fill_coarse(M, M.cl[1], lv, phi, S.coarse);
     S.f = f;
     S.phi = phi;
     S.nx = M.nx;
