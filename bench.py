@@ -57,7 +57,10 @@ def parse():
     ap.add_argument("--no-collisionless", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-graph", action="store_true", help="launch every kernel from the host (profilers)")
-    ap.add_argument("--mg-launch", default="graph", choices=["persistent", "host", "graph"],
+    ap.add_argument("--mg-sweeps", type=int, nargs=2, default=(2, 2), metavar=("PRE", "POST"),
+                    help="red-black sweeps before and after each coarse-grid correction")
+    ap.add_argument("--omega", type=float, default=1.15, help="smoother over-relaxation")
+    ap.add_argument("--mg-launch", default="graph", choices=["persistent", "host", "graph", "cluster"],
                     help="multigrid launch mode (host: one launch per kernel, for profilers)")
     ap.add_argument("--ensemble", type=int, default=0,
                     help="also time an ensemble of this many independent collisionless members (0: off)")
@@ -592,6 +595,8 @@ def main():
     args = parse()
     GRAPH_OPTS["use_graph"] = not args.no_graph
     GRAPH_OPTS["mg_launch"] = args.mg_launch
+    GRAPH_OPTS["pre_sweeps"], GRAPH_OPTS["post_sweeps"] = args.mg_sweeps
+    GRAPH_OPTS["omega"] = args.omega
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, world, rank)

@@ -16,7 +16,7 @@
 //             shrinks by one node per half-sweep), then the residual and its
 //             full-weighting restriction to level l+1
 //   coarse    one CTA: the whole V-cycle of the levels that fit in shared
-//             memory (<= 65^2 nodes), down to the direct solve and back up
+//             memory (<= 33^2 nodes), down to the direct solve and back up
 //   up(l)     prolongation-add of level l+1 and 2*post half-sweeps on a tile
 //             with a halo of 2*post; on level 0 it adds e to phi instead of
 //             storing e
@@ -42,8 +42,8 @@ constexpr int kMgThreads = 512;
 constexpr int kMgMaxSweeps = 8;
 constexpr int kMgMaxCoarseLevels = 8;
 constexpr int kCoarseThreads = 1024;
-constexpr long kCoarseMaxNodes32 = 65L * 65L;    // FP32 levels at or below this size run in the single-CTA kernel
-constexpr long kCoarseMaxNodes64 = 65L * 65L;    // FP64 levels (twice the shared memory per node)
+constexpr long kCoarseMaxNodes32 = 33L * 33L;    // FP32 levels at or below this size run in the single-CTA kernel
+constexpr long kCoarseMaxNodes64 = 33L * 33L;    // FP64 levels
 constexpr int kMgMaxLevels = 16;
 constexpr long kPersistCoarseMax = 33L * 33L;    // levels the persistent kernel's single block solves
 constexpr unsigned long long kBarrierPolls = 1ull << 24;  // a grid barrier gives up (error flag) after this
