@@ -544,29 +544,50 @@ struct NormState {
     long long* total;  // V-cycles since creation
 };
 
+constexpr int kR0Rows = 4;  // rows per thread of the residual kernel
+
 template <class T>
 __global__ void __launch_bounds__(256) k_mg_r0(const double* __restrict__ phi, const double* __restrict__ f,
                                                const uint8_t* __restrict__ mask, int nx, int ny, double cx, double cy,
                                                T* __restrict__ g0, NormState N, double tol2, int max_cycles,
                                                int initial, cudaGraphConditionalHandle cond, int use_cond) {
+    // a 32 x 8 block covers 32 x 32 nodes, four rows per thread, every load
+    // of a thread issued before the first is used
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
     double r = 0.0, fv = 0.0;
-    if (i < nx && j < ny) {
+    double pc[kR0Rows], pw[kR0Rows], pe[kR0Rows], ps[kR0Rows], pn[kR0Rows], pf[kR0Rows];
+    bool use[kR0Rows];
+#pragma unroll
+    for (int u = 0; u < kR0Rows; ++u) {
+        const int j = blockIdx.y * (blockDim.y * kR0Rows) + threadIdx.y + u * blockDim.y;
         const long k = long(j) * nx + i;
-        if (i > 0 && j > 0 && i < nx - 1 && j < ny - 1 && !mask[k]) {
-            const double c = phi[k];
-            const double lap =
-                cx * ((phi[k - 1] - c) + (phi[k + 1] - c)) + cy * ((phi[k - nx] - c) + (phi[k + nx] - c));
-            fv = f[k];
-            r = fv - lap;
+        const bool inner = i > 0 && j > 0 && i < nx - 1 && j < ny - 1;
+        use[u] = inner && !mask[k];
+        pc[u] = inner ? phi[k] : 0.0;
+        pw[u] = inner ? phi[k - 1] : 0.0;
+        pe[u] = inner ? phi[k + 1] : 0.0;
+        ps[u] = inner ? phi[k - nx] : 0.0;
+        pn[u] = inner ? phi[k + nx] : 0.0;
+        pf[u] = inner ? f[k] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kR0Rows; ++u) {
+        const int j = blockIdx.y * (blockDim.y * kR0Rows) + threadIdx.y + u * blockDim.y;
+        if (i >= nx || j >= ny) continue;
+        double ru = 0.0;
+        if (use[u]) {
+            const double c = pc[u];
+            const double lap = cx * ((pw[u] - c) + (pe[u] - c)) + cy * ((ps[u] - c) + (pn[u] - c));
+            ru = pf[u] - lap;
+            fv += pf[u] * pf[u];
         }
-        g0[k] = T(r);
+        r += ru * ru;
+        g0[long(j) * nx + i] = T(ru);
     }
     __shared__ double ws[2][8];
     __shared__ bool last;
     const int t = threadIdx.y * blockDim.x + threadIdx.x;
-    double a = warp_sum(r * r), b = warp_sum(fv * fv);
+    double a = warp_sum(r), b = warp_sum(fv);
     if ((t & 31) == 0) {
         ws[0][t >> 5] = a;
         ws[1][t >> 5] = b;
@@ -1513,7 +1534,7 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
     if (st == PIC_OK) st = M.precision == PIC_MG_MIXED ? configure_kernels<float>(M) : configure_kernels<double>(M);
     if (st == PIC_OK && M.o.launch_mode == PIC_MG_CLUSTER) st = configure_cluster(M, nxs, nys);
     if (st != PIC_OK) return bail(st);
-    M.grd0 = dim3(div_up(nx, M.blk0.x), div_up(ny, M.blk0.y));
+    M.grd0 = dim3(div_up(nx, M.blk0.x), div_up(ny, M.blk0.y * kR0Rows));
     // block partials of the residual norm: one pair per block of the level-0
     // tiling (k_mg_r0) or of the persistent grid (k_mg_solve), whichever is larger
     const int nb = std::max(int(M.grd0.x * M.grd0.y), M.solve_grid);
