@@ -296,6 +296,10 @@ typedef struct pic_sim_counters {
     int last_cycles;              /* V-cycles of the last solve */
     double last_rel_res;
     long long steps;
+    /* particles collected by internal electrodes (grid-line segments of
+     * internal Dirichlet nodes, src/collisions.py:73-175 in the reference,
+     * where the tracing exists but is unused) */
+    unsigned long long electrode_absorbed[PIC_MAX_SPECIES];
 } pic_sim_counters;
 
 int pic_sim_create(const pic_sim_desc* desc, void* stream, pic_sim** out);

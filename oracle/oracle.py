@@ -62,6 +62,11 @@ def lib():
         L.or_kick_f32.argtypes = [_fp, _fp, _fp, _fp, C.c_long, _fp, _fp, C.c_float, C.c_int, C.c_int]
         L.or_drift_absorb_f32.argtypes = [_fp, _fp, _fp, _fp, C.c_long, C.c_float, C.c_float, C.c_int, C.c_int]
         L.or_drift_absorb_f32.restype = C.c_long
+        L.or_hits_electrode.argtypes = [C.c_float, C.c_float, C.c_float, C.c_float, C.c_int, C.c_int, _up, _up]
+        L.or_hits_electrode.restype = C.c_int
+        L.or_drift_absorb_electrodes_f32.argtypes = [_fp, _fp, _fp, _fp, C.c_long, C.c_float, C.c_float, C.c_int,
+                                                     C.c_int, _up, _up, C.POINTER(C.c_long)]
+        L.or_drift_absorb_electrodes_f32.restype = C.c_long
         L.or_sort_keys.argtypes = [_fp, _fp, C.c_long, C.c_int, C.c_int, C.c_int, _up]
         L.or_counting_sort.argtypes = [_up, C.c_long, C.c_uint32, _up]
         L.or_philox4x32_10.argtypes = [_up, _up, _up]
@@ -173,6 +178,47 @@ def kick_f32(gx, gy, vx, vy, ex, ey, kq, m, n):
 
 def drift_absorb_f32(gx, gy, vx, vy, dtdx, dtdy, m, n) -> int:
     return int(lib().or_drift_absorb_f32(gx, gy, vx, vy, len(gx), np.float32(dtdx), np.float32(dtdy), m, n))
+
+
+def electrode_bits(mask, m, n):
+    """Edge bit arrays (vertical, horizontal) of the internal electrodes of a
+    node mask: grid-line segments between two Dirichlet nodes, at least one of
+    them internal (an electrode that reaches the domain boundary keeps its end
+    segment); segments on the boundary lines themselves are not included."""
+    mk = np.asarray(mask).reshape(n, m).astype(bool)
+    inner = np.zeros_like(mk)
+    inner[1:-1, 1:-1] = mk[1:-1, 1:-1]
+    vb = np.zeros((m * (n - 1) + 31) // 32, np.uint32)
+    hb = np.zeros(((m - 1) * n + 31) // 32, np.uint32)
+
+    def end(j, i, boundary_ok):
+        return inner[j, i] or (boundary_ok and mk[j, i])
+
+    for X in range(1, m - 1):
+        for j in range(n - 1):
+            a, b = end(j, X, j == 0), end(j + 1, X, j + 1 == n - 1)
+            if a and b and (inner[j, X] or inner[j + 1, X]):
+                k = X * (n - 1) + j
+                vb[k >> 5] |= np.uint32(1 << (k & 31))
+    for Y in range(1, n - 1):
+        for i in range(m - 1):
+            a, b = end(Y, i, i == 0), end(Y, i + 1, i + 1 == m - 1)
+            if a and b and (inner[Y, i] or inner[Y, i + 1]):
+                k = Y * (m - 1) + i
+                hb[k >> 5] |= np.uint32(1 << (k & 31))
+    return vb, hb
+
+
+def hits_electrode(x0, y0, x1, y1, m, n, vb, hb) -> bool:
+    return bool(lib().or_hits_electrode(np.float32(x0), np.float32(y0), np.float32(x1), np.float32(y1), m, n, vb, hb))
+
+
+def drift_absorb_electrodes_f32(gx, gy, vx, vy, dtdx, dtdy, m, n, vb, hb):
+    """(wall-absorbed, electrode-collected) counts; gx, gy updated in place."""
+    c = C.c_long()
+    a = lib().or_drift_absorb_electrodes_f32(gx, gy, vx, vy, len(gx), np.float32(dtdx), np.float32(dtdy), m, n, vb,
+                                             hb, C.byref(c))
+    return int(a), int(c.value)
 
 
 def residual_f64(phi, f, dirichlet, m, n, dx, dy, want_r=False):

@@ -249,6 +249,71 @@ long or_drift_absorb_f32(float* gx, float* gy, const float* vx, const float* vy,
     return a;
 }
 
+/* Internal electrodes (the build's collection of particles by internal
+ * equipotentials; the reference's tracing in src/collisions.py:73-175 is
+ * unused).  Vertical edge (X, j): x = X, j < y < j + 1, bit X*(ny-1)+j of vb;
+ * horizontal edge (i, Y): y = Y, i < x < i + 1, bit Y*(nx-1)+i of hb.  A line
+ * is crossed when the drift ends on it or passes it, not when it starts on
+ * it; each crossing is intersected in FP32 (x - x0) / dx, fmaf(t, dy, y0). */
+static int edge_bit(const uint32_t* b, long k) { return (int)((b[k >> 5] >> (k & 31)) & 1u); }
+
+int or_hits_electrode(float x0, float y0, float x1, float y1, int nx, int ny, const uint32_t* vb,
+                      const uint32_t* hb) {
+    const float ddx = x1 - x0, ddy = y1 - y0;
+    if (ddx != 0.0f) {
+        int a = ddx > 0.0f ? (int)floorf(x0) + 1 : (int)ceilf(x1);
+        int b = ddx > 0.0f ? (int)floorf(x1) : (int)ceilf(x0) - 1;
+        if (a < 1) a = 1;
+        if (b > nx - 2) b = nx - 2;
+        for (int X = a; X <= b; ++X) {
+            const float t = ((float)X - x0) / ddx;
+            const int j = (int)floorf(fmaf(t, ddy, y0));
+            if (j >= 0 && j < ny - 1 && edge_bit(vb, (long)X * (ny - 1) + j)) return 1;
+        }
+    }
+    if (ddy != 0.0f) {
+        int a = ddy > 0.0f ? (int)floorf(y0) + 1 : (int)ceilf(y1);
+        int b = ddy > 0.0f ? (int)floorf(y1) : (int)ceilf(y0) - 1;
+        if (a < 1) a = 1;
+        if (b > ny - 2) b = ny - 2;
+        for (int Y = a; Y <= b; ++Y) {
+            const float t = ((float)Y - y0) / ddy;
+            const int i = (int)floorf(fmaf(t, ddx, x0));
+            if (i >= 0 && i < nx - 1 && edge_bit(hb, (long)Y * (nx - 1) + i)) return 1;
+        }
+    }
+    return 0;
+}
+
+/* or_drift_absorb_f32 plus collection by internal electrodes; *collected
+ * receives the particles the electrodes took, the return value the wall count. */
+long or_drift_absorb_electrodes_f32(float* gx, float* gy, const float* vx, const float* vy, long n, float dtdx,
+                                    float dtdy, int m, int nn, const uint32_t* vb, const uint32_t* hb,
+                                    long* collected) {
+    long a = 0, c = 0;
+    const float X = (float)(m - 1), Y = (float)(nn - 1);
+    for (long p = 0; p < n; ++p) {
+        if (gx[p] != gx[p]) continue;
+        const float x0 = gx[p], y0 = gy[p];
+        float x = fmaf(vx[p], dtdx, x0);
+        float y = fmaf(vy[p], dtdy, y0);
+        if (!(x >= 0.0f && x <= X && y >= 0.0f && y <= Y)) {
+            gx[p] = NAN;
+            gy[p] = NAN;
+            ++a;
+        } else if (or_hits_electrode(x0, y0, x, y, m, nn, vb, hb)) {
+            gx[p] = NAN;
+            gy[p] = NAN;
+            ++c;
+        } else {
+            gx[p] = x;
+            gy[p] = y;
+        }
+    }
+    *collected = c;
+    return a;
+}
+
 /* ------------------------------------------------------------------ */
 /* Cell sort (the deterministic replacement of src/Particles.py:550-632) */
 /* ------------------------------------------------------------------ */

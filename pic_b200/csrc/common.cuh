@@ -44,6 +44,48 @@ int num_sms();
 // different sizes only ever raise it.
 int raise_smem_limit(const void* kernel, size_t bytes);
 
+// ---- internal electrodes --------------------------------------------------------
+//
+// Electrode edges are grid-line segments whose two end nodes are internal
+// Dirichlet nodes: the vertical edge (X, j) is x = X, j < y < j + 1 (bit
+// X * (ny - 1) + j of vb); the horizontal edge (i, Y) is y = Y, i < x < i + 1
+// (bit Y * (nx - 1) + i of hb).  A particle whose straight drift (x0, y0) ->
+// (x1, y1) (grid units, both inside the grid) crosses one is collected by the
+// electrode.  A line is crossed when the drift ends on it or passes it, not
+// when it starts on it; every crossing is intersected in FP32 with explicit
+// rounding (the CPU oracle restates it operation for operation).
+__device__ __forceinline__ bool edge_bit(const unsigned* b, long k) {
+    return (__ldg(b + (k >> 5)) >> (k & 31)) & 1u;
+}
+
+__device__ inline bool hits_electrode(float x0, float y0, float x1, float y1, int nx, int ny,
+                                      const unsigned* __restrict__ vb, const unsigned* __restrict__ hb) {
+    const float ddx = __fsub_rn(x1, x0), ddy = __fsub_rn(y1, y0);
+    if (ddx != 0.0f) {
+        int a = ddx > 0.0f ? int(floorf(x0)) + 1 : int(ceilf(x1));
+        int b = ddx > 0.0f ? int(floorf(x1)) : int(ceilf(x0)) - 1;
+        a = max(a, 1);
+        b = min(b, nx - 2);
+        for (int X = a; X <= b; ++X) {
+            const float t = __fdiv_rn(__fsub_rn(float(X), x0), ddx);
+            const int j = int(floorf(__fmaf_rn(t, ddy, y0)));
+            if (j >= 0 && j < ny - 1 && edge_bit(vb, long(X) * (ny - 1) + j)) return true;
+        }
+    }
+    if (ddy != 0.0f) {
+        int a = ddy > 0.0f ? int(floorf(y0)) + 1 : int(ceilf(y1));
+        int b = ddy > 0.0f ? int(floorf(y1)) : int(ceilf(y0)) - 1;
+        a = max(a, 1);
+        b = min(b, ny - 2);
+        for (int Y = a; Y <= b; ++Y) {
+            const float t = __fdiv_rn(__fsub_rn(float(Y), y0), ddy);
+            const int i = int(floorf(__fmaf_rn(t, ddx, x0)));
+            if (i >= 0 && i < nx - 1 && edge_bit(hb, long(Y) * (nx - 1) + i)) return true;
+        }
+    }
+    return false;
+}
+
 // ---- CIC weights (FP32, explicit rounding so the CPU oracle matches bit for bit) ----
 
 struct Cic {

@@ -201,8 +201,9 @@ __device__ __forceinline__ bool birth_push(const BirthDev& B, int species, float
 
 // Counter layout (uint64): collisions[s][k] at s*4+k, candidates[s] at 16+s,
 // dropped births at 20, nu overflow at 21, absorbed[s] at 22+s, born[s] at 26+s,
-// candidates that did not fit the fused step's candidate list at 30.
+// candidates that did not fit the fused step's candidate list at 30, particles
+// collected by internal electrodes[s] at 31+s.
 constexpr int kCtrCollisions = 0, kCtrCandidates = 16, kCtrDropped = 20, kCtrOverflow = 21, kCtrAbsorbed = 22,
-              kCtrBorn = 26, kCtrCandOverflow = 30, kCtrCount = 31;
+              kCtrBorn = 26, kCtrCandOverflow = 30, kCtrElectrode = 31, kCtrCount = 35;
 
 }  // namespace pic

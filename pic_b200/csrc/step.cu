@@ -87,6 +87,8 @@ struct PushArgs {
     const uint32_t* step;
     BirthDev births;
     const unsigned* cbits[PIC_MAX_SPECIES];  // null-collision candidate bit per slot (k_mcc_bits), or null
+    const unsigned *vbits, *hbits;           // internal electrode edges (hits_electrode), when `electrodes`
+    int electrodes;
     int2* cand;       // collision candidates (species, slot), processed by k_collide after the pass
     int* cand_count;
     int cand_cap;
@@ -271,7 +273,7 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
     unsigned* rt = reinterpret_cast<unsigned*>(et + RW * RW);
     __shared__ __align__(8) unsigned long long bar[kStages];
     __shared__ ChunkDesc s_ch[kStages];
-    __shared__ unsigned s_abs, s_cand;
+    __shared__ unsigned s_abs, s_cand, s_elec;
     const int tid = threadIdx.x;
     const int n_items = *A.n_items;
     if (tid == 0) {
@@ -279,6 +281,7 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
         fence_mbar_init();
         s_abs = 0;
         s_cand = 0;
+        s_elec = 0;
         ChunkDesc none;
         none.valid = 0;
         const ChunkDesc c = next_chunk(A, none, n_items);
@@ -333,7 +336,7 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
         float* const pvy = pvx + kBufStride;
         const SpeciesConst C = A.sp[s];
         const unsigned* const cbits = (A.do_mcc && A.mcc->sp[s].nproc > 0) ? A.cbits[s] : nullptr;
-        unsigned my_abs = 0, my_cand = 0;
+        unsigned my_abs = 0, my_cand = 0, my_elec = 0;
 #pragma unroll
         for (int k = 0; k < kPushP; ++k) {
             const int l = tid * kPushP + k;
@@ -376,12 +379,17 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
                 atomicAdd(A.ctr + kCtrCandOverflow, 1ull);
             }
             if (A.do_drift) {
+                const float x0 = x, y0 = y;
                 x = __fmaf_rn(vx, C.dtdx, x);
                 y = __fmaf_rn(vy, C.dtdy, y);
                 if (!(x >= 0.0f && x <= float(A.nx - 1) && y >= 0.0f && y <= float(A.ny - 1))) {
                     x = __int_as_float(0x7fc00000);
                     y = x;
                     ++my_abs;
+                } else if (A.electrodes && hits_electrode(x0, y0, x, y, A.nx, A.ny, A.vbits, A.hbits)) {
+                    x = __int_as_float(0x7fc00000);
+                    y = x;
+                    ++my_elec;
                 }
             }
             px[l] = x;
@@ -408,9 +416,11 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
         }
         my_abs = __reduce_add_sync(0xffffffffu, my_abs);
         my_cand = __reduce_add_sync(0xffffffffu, my_cand);
+        my_elec = __reduce_add_sync(0xffffffffu, my_elec);
         if ((tid & 31) == 0) {
             if (my_abs) atomicAdd(&s_abs, my_abs);
             if (my_cand) atomicAdd(&s_cand, my_cand);
+            if (my_elec) atomicAdd(&s_elec, my_elec);
         }
         prev = ch;
         if (ch.e < ch.unit_e) {
@@ -432,8 +442,10 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
             if (tid == 0) {
                 if (s_abs) atomicAdd(A.ctr + kCtrAbsorbed + s, (unsigned long long)s_abs);
                 if (s_cand) atomicAdd(A.ctr + kCtrCandidates + s, (unsigned long long)s_cand);
+                if (s_elec) atomicAdd(A.ctr + kCtrElectrode + s, (unsigned long long)s_elec);
                 s_abs = 0;
                 s_cand = 0;
+                s_elec = 0;
             }
             __syncthreads();
             ch = s_ch[nxt];
@@ -478,12 +490,17 @@ __global__ void __launch_bounds__(128) k_collide(PushArgs A) {
             }
         }
         if (A.do_drift) {
+            const float x0 = x, y0 = y;
             x = __fmaf_rn(vx, C.dtdx, x);
             y = __fmaf_rn(vy, C.dtdy, y);
             if (!(x >= 0.0f && x <= float(A.nx - 1) && y >= 0.0f && y <= float(A.ny - 1))) {
                 x = __int_as_float(0x7fc00000);
                 y = x;
                 atomicAdd(A.ctr + kCtrAbsorbed + s, 1ull);
+            } else if (A.electrodes && hits_electrode(x0, y0, x, y, A.nx, A.ny, A.vbits, A.hbits)) {
+                x = __int_as_float(0x7fc00000);
+                y = x;
+                atomicAdd(A.ctr + kCtrElectrode + s, 1ull);
             }
         }
         S.cur[0][p] = x;
@@ -511,10 +528,13 @@ __global__ void k_merge_births(PushArgs A) {
         float x = A.births.x[i], y = A.births.y[i];
         const float vx = A.births.vx[i], vy = A.births.vy[i], vz = A.births.vz[i];
         if (A.do_drift) {
+            const float x0 = x, y0 = y;
             x = __fmaf_rn(vx, C.dtdx, x);
             y = __fmaf_rn(vy, C.dtdy, y);
-            // a product that leaves the domain in its first drift is never stored
+            // a product that leaves the domain or reaches an electrode in its
+            // first drift is never stored
             if (!(x >= 0.0f && x <= float(A.nx - 1) && y >= 0.0f && y <= float(A.ny - 1))) continue;
+            if (A.electrodes && hits_electrode(x0, y0, x, y, A.nx, A.ny, A.vbits, A.hbits)) continue;
         }
         SpeciesState& S = A.state[s];
         const int slot = atomicAdd(&S.count, 1);
@@ -662,6 +682,8 @@ struct SimImpl {
     bool have_mcc = false;
     MccDev* mcc_dev = nullptr;  // device copy of mcc.dev
     unsigned* cbits[PIC_MAX_SPECIES]{};  // candidate bit per slot of each colliding species
+    unsigned *vbits = nullptr, *hbits = nullptr;  // internal electrode edges
+    bool electrodes = false;
     unsigned** d_cbits = nullptr;         // device copy of cbits
     int* d_nseg = nullptr;                // 256-slot segments per species (0: no collisions)
     int cbits_segments = 0;               // sum of d_nseg
@@ -769,6 +791,9 @@ static PushArgs push_args(SimImpl& S, int kick, int mcc, int drift, int deposit,
     A.step = S.step_ctr;
     A.births = S.births;
     for (int s = 0; s < S.ns; ++s) A.cbits[s] = S.cbits[s];
+    A.vbits = S.vbits;
+    A.hbits = S.hbits;
+    A.electrodes = S.electrodes ? 1 : 0;
     A.cand = S.cand;
     A.cand_count = S.cand_count;
     A.cand_cap = S.cand_cap;
@@ -992,6 +1017,40 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
     std::vector<uint8_t> mask(d->h_dirichlet, d->h_dirichlet + S.G);
     for (auto& v : mask) v = v ? 1 : 0;
     PIC_CUDA(cudaMemcpy(S.dirichlet, mask.data(), S.G, cudaMemcpyHostToDevice));
+    // internal electrode edges: grid-line segments between two internal Dirichlet nodes
+    {
+        const int nx = S.nx, ny = S.ny;
+        auto inner_dir = [&](int i, int j) {
+            return i > 0 && j > 0 && i < nx - 1 && j < ny - 1 && mask[size_t(j) * nx + i];
+        };
+        const long nv = long(nx) * (ny - 1), nh = long(nx - 1) * ny;
+        std::vector<unsigned> vb((nv + 31) / 32, 0u), hb((nh + 31) / 32, 0u);
+        for (int X = 1; X < nx - 1; ++X)
+            for (int j = 0; j + 1 < ny; ++j) {
+                // an edge with one end on the domain boundary still belongs to the electrode
+                const bool a = inner_dir(X, j) || (j == 0 && mask[size_t(j) * nx + X]);
+                const bool b = inner_dir(X, j + 1) || (j + 1 == ny - 1 && mask[size_t(j + 1) * nx + X]);
+                if (a && b && (inner_dir(X, j) || inner_dir(X, j + 1))) {
+                    const long k = long(X) * (ny - 1) + j;
+                    vb[k >> 5] |= 1u << (k & 31);
+                    S.electrodes = true;
+                }
+            }
+        for (int Y = 1; Y < ny - 1; ++Y)
+            for (int i = 0; i + 1 < nx; ++i) {
+                const bool a = inner_dir(i, Y) || (i == 0 && mask[size_t(Y) * nx + i]);
+                const bool b = inner_dir(i + 1, Y) || (i + 1 == nx - 1 && mask[size_t(Y) * nx + i + 1]);
+                if (a && b && (inner_dir(i, Y) || inner_dir(i + 1, Y))) {
+                    const long k = long(Y) * (nx - 1) + i;
+                    hb[k >> 5] |= 1u << (k & 31);
+                    S.electrodes = true;
+                }
+            }
+        PIC_TRY(dalloc(S, &S.vbits, vb.size()));
+        PIC_TRY(dalloc(S, &S.hbits, hb.size()));
+        PIC_CUDA(cudaMemcpy(S.vbits, vb.data(), sizeof(unsigned) * vb.size(), cudaMemcpyHostToDevice));
+        PIC_CUDA(cudaMemcpy(S.hbits, hb.data(), sizeof(unsigned) * hb.size(), cudaMemcpyHostToDevice));
+    }
     if (d->h_phi_bc) {
         std::vector<double> phi0(S.G, 0.0);
         for (long k = 0; k < S.G; ++k)
@@ -1355,6 +1414,7 @@ int pic_sim_read_counters(pic_sim* sim, pic_sim_counters* out, void* stream) {
         for (int k = 0; k < PIC_MAX_PROCESSES; ++k) out->collisions[s][k] = c[kCtrCollisions + s * PIC_MAX_PROCESSES + k];
         out->count[s] = hs[s].count;
     }
+    for (int s = 0; s < S.ns; ++s) out->electrode_absorbed[s] = c[kCtrElectrode + s];
     out->dropped_births = c[kCtrDropped];
     out->nu_overflow = c[kCtrOverflow];
     PIC_TRY(mg_info(S.mg, &S.last));

@@ -152,6 +152,7 @@ class PICSimulation:
             "last_cycles": c.last_cycles,
             "last_rel_res": c.last_rel_res,
             "steps": c.steps,
+            "electrode_absorbed": [c.electrode_absorbed[s] for s in range(ns)],
         }
 
     def species_arrays(self, s):

@@ -199,3 +199,55 @@ def test_fused_step_with_mcc_bookkeeping():
         live = int((~torch.isnan(sim.species_arrays(s)[0])).sum())
         assert live == w.n_e - c["absorbed"][s] + c["born"][s]
     assert 0 < c["born"][0] <= c["collisions"][0][2] and c["born"][1] <= c["collisions"][0][2]
+
+
+def test_internal_electrodes_collect_bit_exact():
+    """Cathode and anode lines inside the domain (the equipotentials of the
+    reference's test.inp, at x = L/4 and 3L/4 from the bottom wall to half
+    height): drifts that cross them are collected, bit-exact against the
+    oracle's FP32 crossing test, and counted apart from the wall absorption."""
+    w = workloads.scaled(workloads.SMALL, n=60_000, Te=20.0)
+    m = w.nodes
+    mask2 = np.zeros((m, m), np.uint8)
+    mask2[0, :] = mask2[-1, :] = mask2[:, 0] = mask2[:, -1] = 1
+    phi2 = np.zeros((m, m))
+    xa, xb, top = (m - 1) // 4, 3 * (m - 1) // 4, (m - 1) // 2
+    mask2[0:top + 1, xa] = 1
+    mask2[0:top + 1, xb] = 1
+    phi2[1:top + 1, xa] = -5.0
+    phi2[1:top + 1, xb] = 5.0
+    mask, phi_bc = mask2.reshape(-1), phi2.reshape(-1)
+    sp_ = [dict(name="e", charge=-Consts.qe, mass=Consts.me, np2c=w.np2c(w.n_e), capacity=2 * w.n_e),
+           dict(name="i", charge=Consts.qe, mass=workloads.ION_MASS, np2c=w.np2c(w.n_i), capacity=2 * w.n_i)]
+    # dt 1e-10 s: 20 eV electrons move ~0.3 cells a step, many cross the lines
+    dt = 1e-10
+    sim = PICSimulation(m, m, w.dx, w.dx, dt, sp_, mask, phi_bc, tol=w.tol, max_cycles=60, sort_interval=0)
+    rng = np.random.Generator(np.random.Philox(w.seed))
+    ref = [list(workloads.species_arrays(w, "e", rng)), list(workloads.species_arrays(w, "i", rng))]
+    for s, a in enumerate(ref):
+        sim.load(s, *a)
+    vb, hb = O.electrode_bits(mask, m, m)
+    kqs = [np.float32(-Consts.qe / Consts.me * dt), np.float32(Consts.qe / workloads.ION_MASS * dt)]
+    dtdx = np.float32(dt / w.dx)
+    sim.init()
+    _, _, ex, ey = (f.cpu().numpy().copy() for f in sim.fields())
+    for s, a in enumerate(ref):
+        O.kick_f32(a[0], a[1], a[2], a[3], ex, ey, np.float32(np.float64(kqs[s]) * -0.5), m, m)
+    walls, collected = [0, 0], [0, 0]
+    for step in range(2):
+        sim.step(1)
+        for s in range(2):
+            if step:
+                O.kick_f32(ref[s][0], ref[s][1], ref[s][2], ref[s][3], ex, ey, kqs[s], m, m)
+            a, c = O.drift_absorb_electrodes_f32(ref[s][0], ref[s][1], ref[s][2], ref[s][3], dtdx, dtdx, m, m, vb,
+                                                  hb)
+            walls[s] += a
+            collected[s] += c
+            got = host(sim, s)
+            for k in range(4):
+                assert_bits(got[k], ref[s][k])
+        _, _, ex, ey = (f.cpu().numpy().copy() for f in sim.fields())
+    cnt = sim.counters()
+    assert cnt["absorbed"] == walls
+    assert cnt["electrode_absorbed"] == collected
+    assert collected[0] > 100  # the electrons do reach the electrodes
