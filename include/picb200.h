@@ -324,6 +324,20 @@ int pic_sim_species_arrays(pic_sim* sim, int s, float** x, float** y, float** vx
 int pic_sim_fields(pic_sim* sim, double** phi, float** rho, float** Ex, float** Ey);
 /* Synchronises `stream` and reads counters. */
 int pic_sim_read_counters(pic_sim* sim, pic_sim_counters* out, void* stream);
+
+/* Diagnostics of the current state (the reference's Diagnostics,
+ * src/simulation.py:116-345, computed on the device in FP64 with a fixed
+ * reduction order).  Per unit depth; rho and E of the last field solve. */
+typedef struct pic_sim_diag {
+    long long live[PIC_MAX_SPECIES];        /* live particles */
+    double kinetic[PIC_MAX_SPECIES];        /* J: sum of 1/2 m np2c |v|^2 (vx, vy, vz) */
+    double momentum[PIC_MAX_SPECIES][3];    /* kg m/s: sum of m np2c v */
+    double field_energy;                    /* J: 1/2 sum rho phi dx dy */
+    double gauss_flux;                      /* V: outward node sum of E along the domain boundary */
+    double gauss_charge;                    /* V: sum rho dx dy / eps0 */
+    double div_error_l2;                    /* V/m^2: || div E - rho/eps0 || over the nodes */
+} pic_sim_diag;
+int pic_sim_diagnostics(pic_sim* sim, pic_sim_diag* out, void* stream);
 /* Kernel launches issued by this object since creation (all phases). */
 long long pic_sim_kernel_launches(pic_sim* sim);
 

@@ -108,6 +108,12 @@ class AdjDesc(C.Structure):
                 ("tol", C.c_double), ("max_cycles", C.c_int)]
 
 
+class SimDiag(C.Structure):
+    _fields_ = [("live", C.c_longlong * PIC_MAX_SPECIES), ("kinetic", C.c_double * PIC_MAX_SPECIES),
+                ("momentum", (C.c_double * 3) * PIC_MAX_SPECIES), ("field_energy", C.c_double),
+                ("gauss_flux", C.c_double), ("gauss_charge", C.c_double), ("div_error_l2", C.c_double)]
+
+
 class SimCounters(C.Structure):
     _fields_ = [("absorbed", C.c_ulonglong * PIC_MAX_SPECIES),
                 ("collisions", (C.c_ulonglong * PIC_MAX_PROCESSES) * PIC_MAX_SPECIES),
@@ -154,6 +160,7 @@ SIGNATURES = {
     "pic_sim_species_arrays": [_vp, _i, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)],
     "pic_sim_fields": [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)],
     "pic_sim_read_counters": [_vp, C.POINTER(SimCounters), _vp],
+    "pic_sim_diagnostics": [_vp, C.c_void_p, _vp],
     "pic_sim_kernel_launches": [_vp],
     "pic_sim_set_profiling": [_vp, _i],
     "pic_sim_read_profile": [_vp, C.c_void_p],

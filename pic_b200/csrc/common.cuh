@@ -44,6 +44,12 @@ int num_sms();
 // different sizes only ever raise it.
 int raise_smem_limit(const void* kernel, size_t bytes);
 
+// Velocity and position arrays of one species for the diagnostics kernels.
+struct DiagSpecies {
+    const float *vx, *vy, *vz, *x;
+    int n;
+};
+
 // ---- internal electrodes --------------------------------------------------------
 //
 // Electrode edges are grid-line segments whose two end nodes are internal

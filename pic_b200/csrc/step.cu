@@ -39,6 +39,10 @@ long long mg_total_cycles(pic_mg* mg);
 int mg_capture_into(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st);
 int mg_launch_graph(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st);
 int mg_info(pic_mg* mg, pic_mg_info* info);
+int diagnostics(const DiagSpecies* sp, const double* mass, const double* np2c, int ns, const double* phi,
+                const float* rho, const float* Ex, const float* Ey, int nx, int ny, double dx, double dy, double eps0,
+                double* scratch, pic_sim_diag* out, cudaStream_t st);
+size_t diagnostics_scratch_doubles();
 bool mg_uses_graph(pic_mg* mg);
 
 constexpr int kPushThreads = 256;
@@ -683,6 +687,7 @@ struct SimImpl {
     MccDev* mcc_dev = nullptr;  // device copy of mcc.dev
     unsigned* cbits[PIC_MAX_SPECIES]{};  // candidate bit per slot of each colliding species
     unsigned *vbits = nullptr, *hbits = nullptr;  // internal electrode edges
+    double* diag = nullptr;                        // diagnostics scratch
     bool electrodes = false;
     unsigned** d_cbits = nullptr;         // device copy of cbits
     int* d_nseg = nullptr;                // 256-slot segments per species (0: no collisions)
@@ -1395,6 +1400,26 @@ int pic_sim_fields(pic_sim* sim, double** phi, float** rho, float** Ex, float** 
     if (Ex) *Ex = sim->s.Ex;
     if (Ey) *Ey = sim->s.Ey;
     return PIC_OK;
+}
+
+int pic_sim_diagnostics(pic_sim* sim, pic_sim_diag* out, void* stream) {
+    clear_error();
+    if (!sim || !out) return fail(PIC_ERR_BAD_ARG, "pic_sim_diagnostics: bad arguments");
+    SimImpl& S = sim->s;
+    cudaStream_t st = as_stream(stream);
+    if (!S.diag) PIC_TRY(dalloc(S, &S.diag, diagnostics_scratch_doubles()));
+    PIC_CUDA(cudaStreamSynchronize(st));
+    PIC_CUDA(cudaMemcpy(S.h_state, S.d_state, sizeof(SpeciesState) * S.ns, cudaMemcpyDeviceToHost));
+    DiagSpecies sp[PIC_MAX_SPECIES];
+    double mass[PIC_MAX_SPECIES], np2c[PIC_MAX_SPECIES];
+    for (int s = 0; s < S.ns; ++s) {
+        const SpeciesState& H = S.h_state[s];
+        sp[s] = DiagSpecies{H.cur[2], H.cur[3], H.cur[4], H.cur[0], H.count};
+        mass[s] = S.d.species[s].mass;
+        np2c[s] = S.d.species[s].np2c;
+    }
+    return diagnostics(sp, mass, np2c, S.ns, S.phi, S.rho_out, S.Ex, S.Ey, S.nx, S.ny, S.d.dx, S.d.dy, S.d.eps0,
+                       S.diag, out, st);
 }
 
 int pic_sim_read_counters(pic_sim* sim, pic_sim_counters* out, void* stream) {

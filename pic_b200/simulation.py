@@ -155,6 +155,17 @@ class PICSimulation:
             "electrode_absorbed": [c.electrode_absorbed[s] for s in range(ns)],
         }
 
+    def diagnostics(self) -> dict:
+        """Kinetic energy and momentum per species, field energy and Gauss's law
+        terms of the current state (pic_sim_diagnostics)."""
+        d = _lib.SimDiag()
+        _lib.call("pic_sim_diagnostics", self._h, C.byref(d), _lib.stream_ptr())
+        ns = len(self.species)
+        return {"live": [d.live[s] for s in range(ns)], "kinetic": [d.kinetic[s] for s in range(ns)],
+                "momentum": [[d.momentum[s][c] for c in range(3)] for s in range(ns)],
+                "field_energy": d.field_energy, "gauss_flux": d.gauss_flux, "gauss_charge": d.gauss_charge,
+                "div_error_l2": d.div_error_l2}
+
     def species_arrays(self, s):
         """Zero-copy torch views (x, y, vx, vy, vz) of the first `count` slots of species s."""
         ptrs = [C.c_void_p() for _ in range(5)]

@@ -251,3 +251,40 @@ def test_internal_electrodes_collect_bit_exact():
     assert cnt["absorbed"] == walls
     assert cnt["electrode_absorbed"] == collected
     assert collected[0] > 100  # the electrons do reach the electrodes
+
+
+def test_diagnostics_match_numpy():
+    """pic_sim_diagnostics against numpy FP64 sums over the same arrays and fields."""
+    w = workloads.scaled(workloads.SMALL, n=40_000)
+    sim, arrays, mask, _ = make_sim(w, 20)
+    sim.init()
+    sim.step(5)
+    sim.sync()
+    d = sim.diagnostics()
+    m = w.nodes
+    for s in range(2):
+        x, y, vx, vy, vz = (a.astype(np.float64) for a in host(sim, s))
+        live = ~np.isnan(x)
+        sp = sim.species[s]
+        assert d["live"][s] == int(live.sum())
+        v2 = vx[live] ** 2 + vy[live] ** 2 + vz[live] ** 2
+        assert d["kinetic"][s] == pytest.approx(0.5 * sp["mass"] * sp["np2c"] * v2.sum(), rel=1e-12)
+        mom = [sp["mass"] * sp["np2c"] * c[live].sum() for c in (vx, vy, vz)]
+        np.testing.assert_allclose(d["momentum"][s], mom, rtol=1e-9, atol=1e-40)
+    phi, rho, ex, ey = (f.cpu().numpy().astype(np.float64) for f in sim.fields())
+    dx = dy = w.dx
+    assert d["field_energy"] == pytest.approx(0.5 * np.sum(rho * phi) * dx * dy, rel=1e-12)
+    E = [ex.reshape(m, m), ey.reshape(m, m)]
+    flux = (E[0][:, -1].sum() - E[0][:, 0].sum()) * dy + (E[1][-1, :].sum() - E[1][0, :].sum()) * dx
+    assert d["gauss_flux"] == pytest.approx(flux, rel=1e-10, abs=1e-12 * np.abs(E[0]).max() * m * dx)
+    assert d["gauss_charge"] == pytest.approx(rho.sum() * dx * dy / Consts.eps0, rel=1e-12)
+    dex = np.empty((m, m))
+    dey = np.empty((m, m))
+    dex[:, 1:-1] = (E[0][:, 2:] - E[0][:, :-2]) / (2 * dx)
+    dex[:, 0] = (E[0][:, 1] - E[0][:, 0]) / dx
+    dex[:, -1] = (E[0][:, -1] - E[0][:, -2]) / dx
+    dey[1:-1, :] = (E[1][2:, :] - E[1][:-2, :]) / (2 * dy)
+    dey[0, :] = (E[1][1, :] - E[1][0, :]) / dy
+    dey[-1, :] = (E[1][-1, :] - E[1][-2, :]) / dy
+    err = np.sqrt(np.sum((dex + dey - rho.reshape(m, m) / Consts.eps0) ** 2))
+    assert d["div_error_l2"] == pytest.approx(err, rel=1e-9)
