@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define PIC_ABI_VERSION 1
+#define PIC_ABI_VERSION 2
 #define PIC_MAX_SPECIES 4
 #define PIC_MAX_PROCESSES 4
 
@@ -92,6 +92,27 @@ int pic_update_E(const double* d_phi, float* d_Ex, float* d_Ey, int nx, int ny, 
 int pic_form_rhs(const float* d_rho, const uint8_t* d_dirichlet, double eps0, double* d_f, int nx, int ny,
                  void* stream);
 
+/* r-z (axisymmetric) variants of the operators above, for Grid2D /
+ * Particles2D with cylindrical=True (the reference's cylindrical kernels,
+ * src/Grid.py:5-93 and src/Particles.py:183-248, with the corrections listed
+ * in the design notes).  Coordinates: x axial, y radial (grid units), row 0
+ * the axis.
+ *
+ * pic_update_E_rz: pic_update_E with E_r = 0 on the axis row (symmetry).
+ * pic_rz_density: turns a charge deposited by pic_deposit (per dx*dy) into
+ *   the charge density, rho_j *= dx*dy / V_j, with V_j the node volumes of
+ *   the linear weighting (2 pi r_j dr dz inside; pi dr^2 dz / 3 on the axis;
+ *   pi dr dz (r_top - dr/3) on the outer row), so a uniform load gives a
+ *   uniform density.
+ * pic_update_R_rz: the drift in 3D with the radial and azimuthal velocities
+ *   (d_vy, d_vz) turned into the new local frame (Birdsall and Langdon,
+ *   sec. 14-12), for live slots [0, n). */
+int pic_update_E_rz(const double* d_phi, float* d_Ex, float* d_Ey, int nx, int ny, double dx, double dy,
+                    void* stream);
+int pic_rz_density(float* d_rho, int nx, int ny, double dy, void* stream);
+int pic_update_R_rz(float* d_x, float* d_y, const float* d_vx, float* d_vy, float* d_vz, int n, float dtdx,
+                    float dtdy, void* stream);
+
 /* ------------------------------------------------------------------ */
 /* Multigrid Poisson solver (src/multigrid.py:277-455, src/Solvers.py:258-299) */
 /* ------------------------------------------------------------------ */
@@ -111,13 +132,27 @@ typedef enum pic_mg_launch_mode {
                               row bands fit in shared memory; otherwise the graph loop) */
 } pic_mg_launch_mode;
 
+/* Geometry of the grid.  PIC_GEOM_RZ is axisymmetric r-z (the reference's
+ * Grid.Cylindrical = 1, src/Grid.py:5-93, src/Solvers.py:100-166): x is the
+ * axial coordinate z (nodes i, spacing dx), y the radius r (rows j, r = j*dy),
+ * row 0 is the axis.  The axis row is not a boundary: its nodes are free
+ * unless the mask marks them, and the operator there is the symmetric limit
+ * 2 d2phi/dr2.  In a simulation, vx is the axial, vy the radial and vz the
+ * azimuthal velocity, and particle counts (np2c) are real particles, not
+ * particles per unit depth. */
+typedef enum pic_geometry {
+    PIC_GEOM_CARTESIAN = 0,
+    PIC_GEOM_RZ = 1
+} pic_geometry;
+
 typedef struct pic_mg_options {
     int precision;    /* pic_mg_precision */
     int pre_sweeps;   /* red-black Gauss-Seidel sweeps before restriction (default 2) */
     int post_sweeps;  /* sweeps after prolongation (default 2) */
     double omega;     /* over-relaxation of the red-black smoother (default, when <= 0: 1.15) */
     int coarsest_max; /* coarsen while both node counts exceed this (default 9) */
-    int launch_mode;  /* pic_mg_launch_mode */
+    int launch_mode;  /* pic_mg_launch_mode (r-z solves use the graph or host loop) */
+    int geometry;     /* pic_geometry (default 0: Cartesian) */
 } pic_mg_options;
 
 typedef struct pic_mg_info {
@@ -327,7 +362,12 @@ int pic_sim_read_counters(pic_sim* sim, pic_sim_counters* out, void* stream);
 
 /* Diagnostics of the current state (the reference's Diagnostics,
  * src/simulation.py:116-345, computed on the device in FP64 with a fixed
- * reduction order).  Per unit depth; rho and E of the last field solve. */
+ * reduction order).  Per unit depth; rho and E of the last field solve.
+ * In r-z geometry the node volumes V_j (pic_rz_density) replace dx*dy (the
+ * sums are then totals, not per unit depth), the flux is through the two end
+ * disks and the outer cylinder (2 pi R dx per node), the divergence is
+ * (1/r) d(r E_r)/dr + dE_z/dz (2 dE_r/dr on the axis), and the momentum
+ * components are sums of the axial, radial and azimuthal velocities. */
 typedef struct pic_sim_diag {
     long long live[PIC_MAX_SPECIES];        /* live particles */
     double kinetic[PIC_MAX_SPECIES];        /* J: sum of 1/2 m np2c |v|^2 (vx, vy, vz) */

@@ -1,4 +1,4 @@
-"""Particles2D: drop-in for src/Particles.py:283-690 (Cartesian).
+"""Particles2D: drop-in for src/Particles.py:283-690, Cartesian or r-z.
 
 Storage is one SoA group per species (x, y, vx, vy, vz float32 on the GPU),
 positions in grid units (x/dx, y/dy) and velocities in m/s, instead of the
@@ -6,6 +6,14 @@ reference's AoS FP64 R (N,2) / V (N,3) with a part_type column.  The
 reference's attributes are provided as computed views: ``R`` and ``V`` (FP64,
 metres and m/s, live particles of all species in species order) and
 ``part_type``.  Slots of absorbed particles hold NaN until ``compact()``.
+
+cylindrical=True (r-z): x is the axial and y the radial position, vx, vy,
+vz the axial, radial and azimuthal velocities.  update_V is the reference's
+cylindrical kick (src/Particles.py:183-248, the same gather as Cartesian);
+update_R drifts in 3D and turns (vy, vz) into the new local frame
+(pic_update_R_rz), where the reference drifts in the plane and reflects at
+the axis (src/Particles.py:267-280).  The loaders then draw radii uniform in
+volume (density proportional to r).
 """
 from __future__ import annotations
 
@@ -39,9 +47,7 @@ class Particles2D:
     """Particles2D(N) -- N slots per species (src/Particles.py:284)."""
 
     def __init__(self, N, cylindrical=False):
-        if cylindrical:
-            raise NotImplementedError("cylindrical (r-z) particles are not part of this build")
-        self.cylindrical = False
+        self.cylindrical = bool(cylindrical)
         self.N = int(N)
         self.species: list[Species] = []
         self.part_name = ["reserved"]
@@ -138,8 +144,14 @@ class Particles2D:
         n = int(n)
         u = torch.rand((2, n), generator=self._gen, dtype=torch.float64)
         vx0 = float(torch.rand(1, generator=self._gen, dtype=torch.float64) * 0.2 - 0.1)
-        self.load_species_arrays(species, x1 + (x2 - x1) * u[0], y1 + (y2 - y1) * u[1], torch.full((n,), vx0),
+        self.load_species_arrays(species, x1 + (x2 - x1) * u[0], self._radial(y1, y2, u[1]), torch.full((n,), vx0),
                                  torch.zeros(n), None, grid)
+
+    def _radial(self, y1, y2, u):
+        """y1 + (y2 - y1) u; in r-z, radii with density proportional to r (uniform in volume)."""
+        if not self.cylindrical:
+            return y1 + (y2 - y1) * u
+        return (y1 * y1 + (y2 * y2 - y1 * y1) * u) ** 0.5
 
     def maxwellian_species_load(self, x1, y1, x2, y2, n, species, T_eV, seed=0, grid=None):
         """Uniform positions and Maxwellian velocities N(0, sqrt(kT/m)) per component."""
@@ -148,8 +160,10 @@ class Particles2D:
         s = self.get_species(species)
         rng = np.random.Generator(np.random.Philox(seed))
         vth = np.sqrt(T_eV * qe / s.mass)
-        self.load_species_arrays(species, rng.uniform(x1, x2, n), rng.uniform(y1, y2, n), rng.normal(0, vth, n),
-                                 rng.normal(0, vth, n), rng.normal(0, vth, n), grid)
+        x = rng.uniform(x1, x2, n)
+        y = self._radial(y1, y2, rng.uniform(0.0, 1.0, n)) if self.cylindrical else rng.uniform(y1, y2, n)
+        self.load_species_arrays(species, x, y, rng.normal(0, vth, n), rng.normal(0, vth, n), rng.normal(0, vth, n),
+                                 grid)
 
     # ---- reference views ----
     @property
@@ -170,10 +184,15 @@ class Particles2D:
 
     # ---- push (src/Particles.py:359-410) ----
     def update_R(self, dt):
-        """x += v dt (src/Particles.py:359-367)."""
+        """x += v dt (src/Particles.py:359-367); r-z: the drift of pic_update_R_rz."""
         g = self._require_grid()
         for s in self.species:
-            if s.n:
+            if not s.n:
+                continue
+            if self.cylindrical:
+                _lib.call("pic_update_R_rz", _lib.ptr(s.x), _lib.ptr(s.y), _lib.ptr(s.vx), _lib.ptr(s.vy),
+                          _lib.ptr(s.vz), s.n, float(dt / g.dx), float(dt / g.dy), _lib.stream_ptr())
+            else:
                 _lib.call("pic_update_R", _lib.ptr(s.x), _lib.ptr(s.y), _lib.ptr(s.vx), _lib.ptr(s.vy), s.n,
                           float(dt / g.dx), float(dt / g.dy), None, None, _lib.stream_ptr())
 

@@ -1,10 +1,16 @@
-"""Solver: drop-in for src/Solvers.py:198-299, multigrid branch.
+"""Solver: drop-in for src/Solvers.py:198-299, multigrid branch, Cartesian or r-z.
 
 ``solve(grid)`` forms b = -rho/eps0 on free nodes (without the reference's
 extra dx^2, src/Solvers.py:271, which its multigrid then applies a second
 time), keeps the Dirichlet values in phi, and runs the GPU multigrid.
 The direct/cg/gmres/inverse branches use cupyx library solvers in the
 reference and are not part of this build.
+
+cylindrical=True solves the axisymmetric equation (the operator the
+reference builds in Laplacian_cylindrical_csr, src/Solvers.py:100-166, and
+hands only to its cupyx solvers; its multigrid stays Cartesian): row 0 is the
+axis, a free row, and the r-weights are (1 +- 1/2j) / dr^2, with 4 / dr^2 on
+the axis.
 """
 from __future__ import annotations
 
@@ -20,12 +26,10 @@ class Solver:
                  max_cycles=50):
         if solver_type != "multigrid":
             raise NotImplementedError(f"solver_type={solver_type!r}: only 'multigrid' is built")
-        if cylindrical:
-            raise NotImplementedError("cylindrical Laplacian is not part of this build")
         self.solver_type = solver_type
         self.m, self.n = grid.m, grid.n
         self.dx, self.dy = grid.dx, grid.dy
-        self.cylindrical = False
+        self.cylindrical = bool(cylindrical)
         self.tol = tol
         self.max_cycles = max_cycles
         self.boundaries = boundaries
@@ -36,12 +40,16 @@ class Solver:
             mask = np.zeros(grid.m * grid.n, np.uint8)
             self.phi_bc = None
         # the grid edges are always Dirichlet nodes of the 5-point operator
+        # (in r-z all but the axis row)
         m2 = mask.reshape(grid.n, grid.m)
         self._edge_mask = m2.copy()
-        self._edge_mask[0, :] = self._edge_mask[-1, :] = self._edge_mask[:, 0] = self._edge_mask[:, -1] = 1
+        self._edge_mask[-1, :] = self._edge_mask[:, 0] = self._edge_mask[:, -1] = 1
+        if not self.cylindrical:
+            self._edge_mask[0, :] = 1
         self.dirichlet = torch.as_tensor(self._edge_mask.reshape(-1), device=grid.phi.device)
         self.multigrid = MultigridSolver(self._edge_mask.reshape(-1), grid.m, grid.n, grid.dx, omega=1.15,
-                                         precision=precision, hy=grid.dy)
+                                         precision=precision, hy=grid.dy,
+                                         geometry="rz" if self.cylindrical else "cartesian")
         self.last_info = None
         if self.phi_bc is not None:
             bc = torch.as_tensor(boundaries.bc_lookup_host, device=grid.phi.device).bool()

@@ -57,7 +57,10 @@ class PicError(RuntimeError):
 
 class MgOptions(C.Structure):
     _fields_ = [("precision", C.c_int), ("pre_sweeps", C.c_int), ("post_sweeps", C.c_int), ("omega", C.c_double),
-                ("coarsest_max", C.c_int), ("launch_mode", C.c_int)]
+                ("coarsest_max", C.c_int), ("launch_mode", C.c_int), ("geometry", C.c_int)]
+
+
+GEOMETRIES = {"cartesian": 0, "rz": 1}
 
 
 class MgInfo(C.Structure):
@@ -137,6 +140,9 @@ SIGNATURES = {
     "pic_deposit": [_vp, _vp, _i, _f, _vp, _i, _i, _vp],
     "pic_update_E": [_vp, _vp, _vp, _i, _i, _d, _d, _vp],
     "pic_form_rhs": [_vp, _vp, _d, _vp, _i, _i, _vp],
+    "pic_update_E_rz": [_vp, _vp, _vp, _i, _i, _d, _d, _vp],
+    "pic_rz_density": [_vp, _i, _i, _d, _vp],
+    "pic_update_R_rz": [_vp, _vp, _vp, _vp, _vp, _i, _f, _f, _vp],
     "pic_mg_create": [_i, _i, _d, _d, _vp, C.POINTER(MgOptions), C.POINTER(_vp)],
     "pic_mg_destroy": [_vp],
     "pic_mg_solve": [_vp, _vp, _vp, _d, _i, C.POINTER(MgInfo), _vp],

@@ -92,6 +92,45 @@ __device__ inline bool hits_electrode(float x0, float y0, float x1, float y1, in
     return false;
 }
 
+// ---- r-z node volumes -------------------------------------------------------------
+//
+// Volume of node row j of an r-z grid divided by dx*dy (so, in metres): the
+// integral of 2 pi r times the row's linear weighting function over r.  With
+// these volumes a uniformly loaded plasma deposits a uniform density:
+// 2 pi r_j inside, pi dy / 3 on the axis, pi (r_top - dy/3) on the outer row.
+__host__ __device__ inline double rz_row_volume(int j, int ny, double dy) {
+    const double pi = 3.14159265358979323846;
+    if (j == 0) return pi * dy / 3.0;
+    if (j == ny - 1) return pi * (double(j) * dy - dy / 3.0);
+    return 2.0 * pi * double(j) * dy;
+}
+
+// ---- r-z drift ---------------------------------------------------------------------
+//
+// One drift of an axisymmetric particle (x axial and y radial, grid units; vx
+// axial, vy radial, vz azimuthal, m/s).  The particle moves on a straight line
+// in 3D: in the plane normal to the axis it goes from (y, 0) to (y', t) =
+// (y + vy dt/dy, vz dt/dy), its new radius is |(y', t)|, and (vy, vz) are
+// turned by the angle of (y', t) into the new radial and azimuthal directions
+// (Birdsall and Langdon, Plasma Physics via Computer Simulation, sec. 14-12).
+// A path through the axis comes out on the other side with r >= 0.  Every
+// operation is correctly rounded (IEEE square root and division), so the
+// FP32 oracle reproduces it bit for bit.
+__device__ __forceinline__ void drift_rz(float& x, float& y, float vx, float& vy, float& vz, float dtdx, float dtdy) {
+    x = __fmaf_rn(vx, dtdx, x);
+    const float yr = __fmaf_rn(vy, dtdy, y);
+    const float yt = __fmul_rn(vz, dtdy);
+    const float r = __fsqrt_rn(__fmaf_rn(yr, yr, __fmul_rn(yt, yt)));
+    if (r > 0.0f) {
+        const float c = __fdiv_rn(yr, r), s = __fdiv_rn(yt, r);
+        const float vr = __fmaf_rn(c, vy, __fmul_rn(s, vz));
+        const float vt = __fmaf_rn(c, vz, -__fmul_rn(s, vy));
+        vy = vr;
+        vz = vt;
+    }
+    y = r;
+}
+
 // ---- CIC weights (FP32, explicit rounding so the CPU oracle matches bit for bit) ----
 
 struct Cic {

@@ -48,30 +48,42 @@ __global__ void __launch_bounds__(kDiagThreads) k_diag_particles(DiagSpecies sp,
     }
 }
 
-// Field energy, Gauss's law terms; partial[k * gridDim.x + block].
+// Field energy, Gauss's law terms; partial[k * gridDim.x + block].  rowv
+// (r-z geometry): per row V_j / (dx*dy), the node volume in units of dx*dy;
+// null in Cartesian geometry (volume dx*dy per unit depth).
 __global__ void __launch_bounds__(kDiagThreads) k_diag_grid(const double* __restrict__ phi, const float* __restrict__ rho,
                                                            const float* __restrict__ Ex, const float* __restrict__ Ey,
                                                            int nx, int ny, double dx, double dy, double inv_eps0,
+                                                           const double* __restrict__ rowv,
                                                            double* __restrict__ partial) {
     __shared__ double ws[kDiagThreads / 32];
     double a[kDiagGridSums] = {0, 0, 0, 0};
     const long G = long(nx) * ny;
+    const double two_pi = 6.283185307179586476925;
     for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < G; k += long(gridDim.x) * blockDim.x) {
         const int i = int(k % nx), j = int(k / nx);
         const double r = rho[k];
-        a[0] += r * phi[k];
-        a[2] += r;
-        // outward flux through the domain boundary (node sums, as the reference)
-        if (i == nx - 1) a[1] += double(Ex[k]) * dy;
-        if (i == 0) a[1] -= double(Ex[k]) * dy;
-        if (j == ny - 1) a[1] += double(Ey[k]) * dx;
-        if (j == 0) a[1] -= double(Ey[k]) * dx;
-        // divergence of E with the stencil of the gradient (central inside, one-sided on the edges)
+        const double w = rowv ? rowv[j] : 1.0;
+        a[0] += r * phi[k] * w;
+        a[2] += r * w;
+        // outward flux through the domain boundary (node sums, as the reference);
+        // r-z: the end disks (areas V_j / dx per node) and the outer cylinder
+        if (i == nx - 1) a[1] += double(Ex[k]) * dy * w;
+        if (i == 0) a[1] -= double(Ex[k]) * dy * w;
+        if (j == ny - 1) a[1] += double(Ey[k]) * dx * (rowv ? two_pi * double(j) * dy : 1.0);
+        if (j == 0 && !rowv) a[1] -= double(Ey[k]) * dx;
+        // divergence of E with the stencil of the gradient (central inside, one-sided on the edges);
+        // r-z: (1/r) d(r E_r)/dr, and 2 dE_r/dr on the axis
         double dex, dey;
         if (i > 0 && i < nx - 1) dex = (double(Ex[k + 1]) - double(Ex[k - 1])) / (2.0 * dx);
         else if (i == 0) dex = (double(Ex[k + 1]) - double(Ex[k])) / dx;
         else dex = (double(Ex[k]) - double(Ex[k - 1])) / dx;
-        if (j > 0 && j < ny - 1) dey = (double(Ey[k + nx]) - double(Ey[k - nx])) / (2.0 * dy);
+        if (rowv) {
+            if (j > 0 && j < ny - 1)
+                dey = (double(j + 1) * double(Ey[k + nx]) - double(j - 1) * double(Ey[k - nx])) / (2.0 * double(j) * dy);
+            else if (j == 0) dey = 2.0 * (double(Ey[k + nx]) - double(Ey[k])) / dy;
+            else dey = (double(j) * double(Ey[k]) - double(j - 1) * double(Ey[k - nx])) / (double(j) * dy);
+        } else if (j > 0 && j < ny - 1) dey = (double(Ey[k + nx]) - double(Ey[k - nx])) / (2.0 * dy);
         else if (j == 0) dey = (double(Ey[k + nx]) - double(Ey[k])) / dy;
         else dey = (double(Ey[k]) - double(Ey[k - nx])) / dy;
         const double e = dex + dey - r * inv_eps0;
@@ -95,14 +107,15 @@ __global__ void k_diag_final(const double* __restrict__ partial, int ncols, int 
 // The diagnostics of `ns` species and the fields; writes `out` (host).
 int diagnostics(const DiagSpecies* sp, const double* mass, const double* np2c, int ns, const double* phi,
                 const float* rho, const float* Ex, const float* Ey, int nx, int ny, double dx, double dy, double eps0,
-                double* scratch, pic_sim_diag* out, cudaStream_t st) {
+                const double* rowv, double* scratch, pic_sim_diag* out, cudaStream_t st) {
     const int nb = kDiagBlocks;
     const int pcols = PIC_MAX_SPECIES * kDiagParticleSums;
     double* part = scratch;                        // [(pcols + kDiagGridSums) * nb]
     double* sums = scratch + size_t(pcols + kDiagGridSums) * nb;  // [pcols + kDiagGridSums]
     PIC_CUDA(cudaMemsetAsync(part, 0, sizeof(double) * size_t(pcols + kDiagGridSums) * nb, st));
     for (int s = 0; s < ns; ++s) k_diag_particles<<<nb, kDiagThreads, 0, st>>>(sp[s], s, part);
-    k_diag_grid<<<nb, kDiagThreads, 0, st>>>(phi, rho, Ex, Ey, nx, ny, dx, dy, 1.0 / eps0, part + size_t(pcols) * nb);
+    k_diag_grid<<<nb, kDiagThreads, 0, st>>>(phi, rho, Ex, Ey, nx, ny, dx, dy, 1.0 / eps0, rowv,
+                                             part + size_t(pcols) * nb);
     k_diag_final<<<1, 64, 0, st>>>(part, pcols + kDiagGridSums, nb, sums);
     PIC_LAUNCH_CHECK();
     double h[PIC_MAX_SPECIES * kDiagParticleSums + kDiagGridSums];

@@ -63,6 +63,11 @@ struct LevelDev {
     T* eu;
     T* ec;
     T* g;
+    // r-z geometry (row j = radius j*hy, row 0 the axis): per row
+    // {wN, wS, 1/diag, D}, the weights of rows j+1 and j-1, the inverse
+    // diagonal and the row's volume weight (j, 1/8 on the axis); null in
+    // Cartesian geometry
+    const T* rz;
 };
 
 // The levels as a launch mode uses them: up phases on the levels below
@@ -117,10 +122,10 @@ struct UpGeom {
 
 // One red or black half-sweep over the nodes 1..W-2 of a W x W shared tile;
 // `par` selects the nodes whose local (li + lj) parity equals it.
-template <class T, int W>
+template <class T, int W, bool CYL>
 __device__ __forceinline__ void tile_half_sweep(T* __restrict__ se, const T* __restrict__ sg,
                                                 const uint8_t* __restrict__ sm, int par, T cx, T cy, T inv_diag,
-                                                T omega) {
+                                                T omega, const T* __restrict__ srz) {
     constexpr int half = W / 2, N = half * W, IT = (N + kMgThreads - 1) / kMgThreads;
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
@@ -131,19 +136,27 @@ __device__ __forceinline__ void tile_half_sweep(T* __restrict__ se, const T* __r
         if (lj < 1 || lj > W - 2 || li < 1 || li > W - 2) continue;
         const int p = lj * W + li;
         if (sm[p]) continue;
-        const T s = cx * (se[p - 1] + se[p + 1]) + cy * (se[p - W] + se[p + W]);
-        const T upd = (s - sg[p]) * inv_diag;
+        T upd;
+        if constexpr (CYL) {
+            const T* rc = srz + 4 * lj;
+            const T s = cx * (se[p - 1] + se[p + 1]) + rc[0] * se[p + W] + rc[1] * se[p - W];
+            upd = (s - sg[p]) * rc[2];
+        } else {
+            const T s = cx * (se[p - 1] + se[p + 1]) + cy * (se[p - W] + se[p + W]);
+            upd = (s - sg[p]) * inv_diag;
+        }
         const T old = se[p];
         se[p] = old + omega * (upd - old);
     }
 }
 
 // Loads level L over the W x W region at (ox, oy): mask (edges and outside
-// the grid count as Dirichlet), g, and e (zero, or the stored correction on
-// free nodes).
-template <class T, int W, bool LOAD_E>
+// the grid count as Dirichlet; in r-z geometry the axis row is free), g, e
+// (zero, or the stored correction on free nodes) and, in r-z geometry, the
+// row coefficients of the W rows (zero outside the grid).
+template <class T, int W, bool LOAD_E, bool CYL>
 __device__ __forceinline__ void tile_load(const LevelDev<T>& L, int ox, int oy, T* __restrict__ se,
-                                          T* __restrict__ sg, uint8_t* __restrict__ sm) {
+                                          T* __restrict__ sg, uint8_t* __restrict__ sm, T* __restrict__ srz) {
     constexpr int N = W * W, IT = (N + kMgThreads - 1) / kMgThreads;
     uint8_t mk[IT];
     T gv[IT], ev[IT];
@@ -157,26 +170,33 @@ __device__ __forceinline__ void tile_load(const LevelDev<T>& L, int ox, int oy, 
         gv[it] = in ? L.g[k] : T(0);
         ev[it] = (LOAD_E && in) ? L.e[k] : T(0);
     }
+    if constexpr (CYL) {
+        for (int q = threadIdx.x; q < 4 * W; q += kMgThreads) {
+            const int j = oy + q / 4;
+            srz[q] = (j >= 0 && j < L.ny) ? L.rz[4 * j + q % 4] : T(0);
+        }
+    }
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
         const int q = it * kMgThreads + int(threadIdx.x);
         if (q >= N) break;
         const int i = ox + q % W, j = oy + q / W;
-        const bool fr = i > 0 && j > 0 && i < L.nx - 1 && j < L.ny - 1 && !mk[it];
+        const bool fr = i > 0 && (CYL ? j >= 0 : j > 0) && i < L.nx - 1 && j < L.ny - 1 && !mk[it];
         sm[q] = fr ? 0 : 1;
         sg[q] = gv[it];
         se[q] = fr ? ev[it] : T(0);
     }
 }
 
-template <class T, int S>
+template <class T, int S, bool CYL = false>
 __device__ void down_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, int tx, int ty,
                           unsigned char* smem) {
     constexpr int H = DownGeom<S>::H, W = DownGeom<S>::W, hx = kMgTile / 2;
     static_assert(hx * hx <= kMgThreads, "one coarse node per thread");
     T* se = reinterpret_cast<T*>(smem);
     T* sg = se + W * W;
-    uint8_t* sm = reinterpret_cast<uint8_t*>(sg + W * W);
+    T* srz = sg + W * W;  // r-z row coefficients (4 W values), only with CYL
+    uint8_t* sm = reinterpret_cast<uint8_t*>(srz + (CYL ? 4 * W : 0));
     const int x0 = tx * kMgTile, y0 = ty * kMgTile;
     const int ox = x0 - H, oy = y0 - H;
     const int tid = threadIdx.x;
@@ -184,8 +204,8 @@ __device__ void down_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, 
     const int I = x0 / 2 + tid % hx, J = y0 / 2 + tid / hx;
     const bool own = tid < hx * hx && I < Cc.nx && J < Cc.ny;
     const long K = long(J) * Cc.nx + I;
-    const bool cdir = own && (I == 0 || J == 0 || I == Cc.nx - 1 || J == Cc.ny - 1 || Cc.mask[K]);
-    tile_load<T, W, false>(F, ox, oy, se, sg, sm);
+    const bool cdir = own && (I == 0 || (!CYL && J == 0) || I == Cc.nx - 1 || J == Cc.ny - 1 || Cc.mask[K]);
+    tile_load<T, W, false, CYL>(F, ox, oy, se, sg, sm, srz);
     __syncthreads();
     // global red nodes have (i + j) even; locally (li + lj + ox + oy) even
     const int par0 = (ox + oy) & 1;
@@ -193,7 +213,7 @@ __device__ void down_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, 
     for (int s = 0; s < S; ++s)
 #pragma unroll
         for (int color = 0; color < 2; ++color) {
-            tile_half_sweep<T, W>(se, sg, sm, color ^ par0, F.cx, F.cy, F.inv_diag, omega);
+            tile_half_sweep<T, W, CYL>(se, sg, sm, color ^ par0, F.cx, F.cy, F.inv_diag, omega, srz);
             __syncthreads();
         }
 #pragma unroll
@@ -210,8 +230,15 @@ __device__ void down_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, 
         const int li = q % W, lj = q / W;
         if (li < 1 || lj < 1 || li > W - 2 || lj > W - 2 || sm[q]) continue;
         const T c = se[q];
-        const T lap = F.cx * (se[q - 1] + se[q + 1] - T(2) * c) + F.cy * (se[q - W] + se[q + W] - T(2) * c);
-        sg[q] = sg[q] - lap;
+        if constexpr (CYL) {
+            // the residual weighted by the row's volume, for the volume-weighted restriction
+            const T* rc = srz + 4 * lj;
+            const T lap = F.cx * (se[q - 1] + se[q + 1] - T(2) * c) + rc[0] * (se[q + W] - c) + rc[1] * (se[q - W] - c);
+            sg[q] = rc[3] * (sg[q] - lap);
+        } else {
+            const T lap = F.cx * (se[q - 1] + se[q + 1] - T(2) * c) + F.cy * (se[q - W] + se[q + W] - T(2) * c);
+            sg[q] = sg[q] - lap;
+        }
     }
     __syncthreads();
     // full weighting onto the coarse nodes injected from this tile
@@ -224,19 +251,22 @@ __device__ void down_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, 
             T v = T(0.25) * r(0);
             v += T(0.125) * (r(-1) + r(1) + r(-W) + r(W));
             v += T(0.0625) * (r(-W - 1) + r(-W + 1) + r(W - 1) + r(W + 1));
+            // r-z: divided by the stencil's weighted volume (2J; 5/16 on the
+            // axis, where the row below the axis is absent)
+            if constexpr (CYL) v *= J == 0 ? T(3.2) : T(0.5) / T(J);
             Cc.g[K] = v;
         }
     }
     __syncthreads();  // the caller may reuse the shared tile
 }
 
-template <class T, int S>
+template <class T, int S, bool CYL>
 __global__ void __launch_bounds__(kMgThreads) k_mg_down(LevelDev<T> F, LevelDev<T> Cc, T omega) {
     extern __shared__ __align__(16) unsigned char smem[];
-    down_tile<T, S>(F, Cc, omega, blockIdx.x, blockIdx.y, smem);
+    down_tile<T, S, CYL>(F, Cc, omega, blockIdx.x, blockIdx.y, smem);
 }
 
-template <class T, int S>
+template <class T, int S, bool CYL = false>
 __device__ void up_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, double* __restrict__ phi, int tx,
                         int ty, unsigned char* smem) {
     constexpr int H = UpGeom<S>::H, W = UpGeom<S>::W, CW = UpGeom<S>::CW;
@@ -245,7 +275,8 @@ __device__ void up_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, do
     T* se = reinterpret_cast<T*>(smem);
     T* sg = se + W * W;
     T* sc = sg + W * W;
-    uint8_t* sm = reinterpret_cast<uint8_t*>(sc + CW * CW);
+    T* srz = sc + CW * CW;  // r-z row coefficients (4 W values), only with CYL
+    uint8_t* sm = reinterpret_cast<uint8_t*>(srz + (CYL ? 4 * W : 0));
     const int x0 = tx * kMgTile, y0 = ty * kMgTile;
     const int ox = x0 - H, oy = y0 - H;
     const int cox = ox >> 1, coy = oy >> 1;  // floor for negative origins
@@ -267,7 +298,7 @@ __device__ void up_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, do
         const int i = x0 + q % kMgTile, j = y0 + q / kMgTile;
         pv[it] = (phi && i < F.nx && j < F.ny) ? phi[long(j) * F.nx + i] : 0.0;
     }
-    tile_load<T, W, true>(F, ox, oy, se, sg, sm);
+    tile_load<T, W, true, CYL>(F, ox, oy, se, sg, sm, srz);
 #pragma unroll
     for (int it = 0; it < CIT; ++it) {
         const int q = it * kMgThreads + tid;
@@ -296,7 +327,7 @@ __device__ void up_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, do
     for (int s = 0; s < S; ++s)
 #pragma unroll
         for (int color = 0; color < 2; ++color) {
-            tile_half_sweep<T, W>(se, sg, sm, color ^ par0, F.cx, F.cy, F.inv_diag, omega);
+            tile_half_sweep<T, W, CYL>(se, sg, sm, color ^ par0, F.cx, F.cy, F.inv_diag, omega, srz);
             __syncthreads();
         }
 #pragma unroll
@@ -312,11 +343,11 @@ __device__ void up_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, do
     __syncthreads();  // the caller may reuse the shared tile
 }
 
-template <class T, int S>
+template <class T, int S, bool CYL>
 __global__ void __launch_bounds__(kMgThreads) k_mg_up(LevelDev<T> F, LevelDev<T> Cc, T omega,
                                                       double* __restrict__ phi) {
     extern __shared__ __align__(16) unsigned char smem[];
-    up_tile<T, S>(F, Cc, omega, phi, blockIdx.x, blockIdx.y, smem);
+    up_tile<T, S, CYL>(F, Cc, omega, phi, blockIdx.x, blockIdx.y, smem);
 }
 
 // Runtime sweep counts (the persistent kernel) dispatched to the instances.
@@ -355,32 +386,33 @@ using DownKernel = void (*)(LevelDev<T>, LevelDev<T>, T);
 template <class T>
 using UpKernel = void (*)(LevelDev<T>, LevelDev<T>, T, double*);
 
-template <class T>
+template <class T, bool CYL>
 static DownKernel<T> down_kernel(int s) {
-    static const DownKernel<T> k[kMgMaxSweeps + 1] = {nullptr,         k_mg_down<T, 1>, k_mg_down<T, 2>,
-                                                      k_mg_down<T, 3>, k_mg_down<T, 4>, k_mg_down<T, 5>,
-                                                      k_mg_down<T, 6>, k_mg_down<T, 7>, k_mg_down<T, 8>};
+    static const DownKernel<T> k[kMgMaxSweeps + 1] = {
+        nullptr,                 k_mg_down<T, 1, CYL>, k_mg_down<T, 2, CYL>, k_mg_down<T, 3, CYL>,
+        k_mg_down<T, 4, CYL>,    k_mg_down<T, 5, CYL>, k_mg_down<T, 6, CYL>, k_mg_down<T, 7, CYL>,
+        k_mg_down<T, 8, CYL>};
     return k[s];
 }
 
-template <class T>
+template <class T, bool CYL>
 static UpKernel<T> up_kernel(int s) {
-    static const UpKernel<T> k[kMgMaxSweeps + 1] = {nullptr,       k_mg_up<T, 1>, k_mg_up<T, 2>, k_mg_up<T, 3>,
-                                                    k_mg_up<T, 4>, k_mg_up<T, 5>, k_mg_up<T, 6>, k_mg_up<T, 7>,
-                                                    k_mg_up<T, 8>};
+    static const UpKernel<T> k[kMgMaxSweeps + 1] = {
+        nullptr,              k_mg_up<T, 1, CYL>, k_mg_up<T, 2, CYL>, k_mg_up<T, 3, CYL>, k_mg_up<T, 4, CYL>,
+        k_mg_up<T, 5, CYL>,   k_mg_up<T, 6, CYL>, k_mg_up<T, 7, CYL>, k_mg_up<T, 8, CYL>};
     return k[s];
 }
 
 template <class T>
-static size_t down_smem(int s) {
+static size_t down_smem(int s, bool cyl = false) {
     const size_t W = kMgTile + 2 * (2 * s + 2);
-    return W * W * (2 * sizeof(T) + 1);
+    return W * W * (2 * sizeof(T) + 1) + (cyl ? 4 * W * sizeof(T) : 0);
 }
 
 template <class T>
-static size_t up_smem(int s) {
+static size_t up_smem(int s, bool cyl = false) {
     const size_t W = kMgTile + 2 * (2 * s), CW = W / 2 + 2;
-    return W * W * (2 * sizeof(T) + 1) + CW * CW * sizeof(T);
+    return W * W * (2 * sizeof(T) + 1) + CW * CW * sizeof(T) + (cyl ? 4 * W * sizeof(T) : 0);
 }
 
 // ---- single-CTA V-cycle of the coarse levels --------------------------------------
@@ -389,7 +421,7 @@ static size_t up_smem(int s) {
 // least 1/(2d) from an integer and the two float roundings move it by less.
 __device__ __forceinline__ int div_small(int q, float inv_d) { return int((float(q) + 0.5f) * inv_d); }
 
-template <class T>
+template <class T, bool CYL>
 __device__ void level_sweeps(T* se, const T* sg, const uint8_t* sm, const LevelDev<T>& L, T omega, int sweeps) {
     const int nx = L.nx, ny = L.ny;
     const int hx = (nx + 1) / 2;
@@ -402,8 +434,17 @@ __device__ void level_sweeps(T* se, const T* sg, const uint8_t* sm, const LevelD
                 if (i >= nx) continue;
                 const int p = j * nx + i;
                 if (sm[p]) continue;
-                const T sum = L.cx * (se[p - 1] + se[p + 1]) + L.cy * (se[p - nx] + se[p + nx]);
-                const T upd = (sum - sg[p]) * L.inv_diag;
+                T upd;
+                if constexpr (CYL) {
+                    // no row below the axis (its weight is zero)
+                    const T s = j > 0 ? se[p - nx] : T(0);
+                    const T* rc = L.rz + 4 * j;
+                    upd = (L.cx * (se[p - 1] + se[p + 1]) + __ldg(rc) * se[p + nx] + __ldg(rc + 1) * s - sg[p]) *
+                          __ldg(rc + 2);
+                } else {
+                    const T sum = L.cx * (se[p - 1] + se[p + 1]) + L.cy * (se[p - nx] + se[p + nx]);
+                    upd = (sum - sg[p]) * L.inv_diag;
+                }
                 const T old = se[p];
                 se[p] = old + omega * (upd - old);
             }
@@ -411,7 +452,7 @@ __device__ void level_sweeps(T* se, const T* sg, const uint8_t* sm, const LevelD
         }
 }
 
-template <class T>
+template <class T, bool CYL = false>
 __device__ void coarse_vcycle(const CoarseDesc<T>& D, unsigned char* smem) {
     // level pointers into shared memory, from the descriptor's offsets (no
     // per-thread pointer arrays: they would live in local memory)
@@ -457,7 +498,7 @@ __device__ void coarse_vcycle(const CoarseDesc<T>& D, unsigned char* smem) {
     for (int l = 0; l < last; ++l) {
         const LevelDev<T>& L = D.lv[l];
         const LevelDev<T>& C = D.lv[l + 1];
-        level_sweeps(E(l), Gs(l), M(l), L, D.omega, D.pre);
+        level_sweeps<T, CYL>(E(l), Gs(l), M(l), L, D.omega, D.pre);
         // restriction of the residual, evaluated on the fly: g of this level
         // must survive for the post-smoothing on the way back up
         const T* e = E(l);
@@ -472,16 +513,35 @@ __device__ void coarse_vcycle(const CoarseDesc<T>& D, unsigned char* smem) {
             }
             const int J = div_small(Q, inv_cnx), I = Q - J * C.nx;
             const int p = 2 * J * nx + 2 * I;
-            auto rr = [&](int o) {
-                const int q = p + o;
-                if (mk[q]) return T(0);
-                const T c = e[q];
-                return g[q] - (L.cx * (e[q - 1] + e[q + 1] - T(2) * c) + L.cy * (e[q - nx] + e[q + nx] - T(2) * c));
-            };
-            T v = T(0.25) * rr(0);
-            v += T(0.125) * (rr(-1) + rr(1) + rr(-nx) + rr(nx));
-            v += T(0.0625) * (rr(-nx - 1) + rr(-nx + 1) + rr(nx - 1) + rr(nx + 1));
-            Gs(l + 1)[Q] = v;
+            if constexpr (CYL) {
+                // volume-weighted full weighting; the axis row has no row below
+                auto rrow = [&](int jf, int q) {
+                    if (mk[q]) return T(0);
+                    const T c = e[q];
+                    const T* rc = L.rz + 4 * jf;
+                    const T s = jf > 0 ? e[q - nx] : T(0);
+                    const T lap = L.cx * (e[q - 1] + e[q + 1] - T(2) * c) + __ldg(rc) * (e[q + nx] - c) +
+                                  __ldg(rc + 1) * (s - c);
+                    return __ldg(rc + 3) * (g[q] - lap);
+                };
+                auto line = [&](int jf, int q) {
+                    return T(0.5) * rrow(jf, q) + T(0.25) * (rrow(jf, q - 1) + rrow(jf, q + 1));
+                };
+                T v = T(0.5) * line(2 * J, p) + T(0.25) * line(2 * J + 1, p + nx);
+                if (J > 0) v += T(0.25) * line(2 * J - 1, p - nx);
+                Gs(l + 1)[Q] = v * (J == 0 ? T(3.2) : T(0.5) / T(J));
+            } else {
+                auto rr = [&](int o) {
+                    const int q = p + o;
+                    if (mk[q]) return T(0);
+                    const T c = e[q];
+                    return g[q] - (L.cx * (e[q - 1] + e[q + 1] - T(2) * c) + L.cy * (e[q - nx] + e[q + nx] - T(2) * c));
+                };
+                T v = T(0.25) * rr(0);
+                v += T(0.125) * (rr(-1) + rr(1) + rr(-nx) + rr(nx));
+                v += T(0.0625) * (rr(-nx - 1) + rr(-nx + 1) + rr(nx - 1) + rr(nx + 1));
+                Gs(l + 1)[Q] = v;
+            }
         }
         __syncthreads();
     }
@@ -517,7 +577,7 @@ __device__ void coarse_vcycle(const CoarseDesc<T>& D, unsigned char* smem) {
             E(l)[q] += v;
         }
         __syncthreads();
-        level_sweeps(E(l), Gs(l), M(l), L, D.omega, D.post);
+        level_sweeps<T, CYL>(E(l), Gs(l), M(l), L, D.omega, D.post);
     }
     const LevelDev<T>& L0 = D.lv[0];
     for (int q = threadIdx.x; q < L0.nx * L0.ny; q += blockDim.x) {
@@ -527,10 +587,10 @@ __device__ void coarse_vcycle(const CoarseDesc<T>& D, unsigned char* smem) {
     __syncthreads();
 }
 
-template <class T>
+template <class T, bool CYL>
 __global__ void __launch_bounds__(kCoarseThreads) k_mg_coarse(CoarseDesc<T> D) {
     extern __shared__ __align__(16) unsigned char smem[];
-    coarse_vcycle(D, smem);
+    coarse_vcycle<T, CYL>(D, smem);
 }
 
 // ---- FP64 residual, norms and the loop decision -----------------------------------
@@ -546,11 +606,14 @@ struct NormState {
 
 constexpr int kR0Rows = 4;  // rows per thread of the residual kernel
 
-template <class T>
+// rz0: in r-z geometry the level-0 row coefficients in FP64 ({wN, wS, 1/diag,
+// D} per row, as LevelDev::rz), else null.
+template <class T, bool CYL>
 __global__ void __launch_bounds__(256) k_mg_r0(const double* __restrict__ phi, const double* __restrict__ f,
                                                const uint8_t* __restrict__ mask, int nx, int ny, double cx, double cy,
                                                T* __restrict__ g0, NormState N, double tol2, int max_cycles,
-                                               int initial, cudaGraphConditionalHandle cond, int use_cond) {
+                                               int initial, cudaGraphConditionalHandle cond, int use_cond,
+                                               const double* __restrict__ rz0) {
     // a 32 x 8 block covers 32 x 32 nodes, four rows per thread, every load
     // of a thread issued before the first is used
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -561,12 +624,12 @@ __global__ void __launch_bounds__(256) k_mg_r0(const double* __restrict__ phi, c
     for (int u = 0; u < kR0Rows; ++u) {
         const int j = blockIdx.y * (blockDim.y * kR0Rows) + threadIdx.y + u * blockDim.y;
         const long k = long(j) * nx + i;
-        const bool inner = i > 0 && j > 0 && i < nx - 1 && j < ny - 1;
+        const bool inner = i > 0 && (CYL ? j >= 0 : j > 0) && i < nx - 1 && j < ny - 1;
         use[u] = inner && !mask[k];
         pc[u] = inner ? phi[k] : 0.0;
         pw[u] = inner ? phi[k - 1] : 0.0;
         pe[u] = inner ? phi[k + 1] : 0.0;
-        ps[u] = inner ? phi[k - nx] : 0.0;
+        ps[u] = (inner && j > 0) ? phi[k - nx] : 0.0;
         pn[u] = inner ? phi[k + nx] : 0.0;
         pf[u] = inner ? f[k] : 0.0;
     }
@@ -577,7 +640,11 @@ __global__ void __launch_bounds__(256) k_mg_r0(const double* __restrict__ phi, c
         double ru = 0.0;
         if (use[u]) {
             const double c = pc[u];
-            const double lap = cx * ((pw[u] - c) + (pe[u] - c)) + cy * ((ps[u] - c) + (pn[u] - c));
+            double lap;
+            if constexpr (CYL)
+                lap = cx * ((pw[u] - c) + (pe[u] - c)) + rz0[4 * j] * (pn[u] - c) + rz0[4 * j + 1] * (ps[u] - c);
+            else
+                lap = cx * ((pw[u] - c) + (pe[u] - c)) + cy * ((ps[u] - c) + (pn[u] - c));
             ru = pf[u] - lap;
             fv += pf[u] * pf[u];
         }
@@ -1155,6 +1222,8 @@ struct MgImpl {
     int precision = PIC_MG_MIXED;
     int nx = 0, ny = 0, L = 0, Lc = 0;
     double dx = 0, dy = 0;
+    bool rz = false;          // r-z geometry (PIC_GEOM_RZ)
+    double* rz0 = nullptr;    // level-0 row coefficients in FP64 (r-z)
     pic_mg_options o{};
     std::vector<LevelDev<float>> lf;
     std::vector<LevelDev<double>> ld;
@@ -1195,6 +1264,26 @@ struct pic_mg {
 
 namespace pic {
 
+// Row coefficients of the r-z operator on a level with spacings hx (axial)
+// and hy (radial), row j at radius j*hy:
+//   (1/r) d/dr (r dphi/dr) ~ [(1 + 1/2j) phi_{j+1} + (1 - 1/2j) phi_{j-1} - 2 phi_j] / hy^2,
+// and on the axis, by symmetry, 2 d2phi/dr2 ~ 4 (phi_1 - phi_0) / hy^2.
+// Per row {wN, wS, 1/diag, D}; D is the row's volume weight (2 pi r dr per
+// 2 pi hy^2: j, and 1/8 for the axis control volume of radius hy/2).
+static std::vector<double> rz_rows(int ny, double hx, double hy) {
+    const double cx = 1.0 / (hx * hx), cy = 1.0 / (hy * hy);
+    std::vector<double> r(size_t(4) * ny);
+    for (int j = 0; j < ny; ++j) {
+        const double wn = j == 0 ? 4.0 * cy : cy * (1.0 + 0.5 / j);
+        const double ws = j == 0 ? 0.0 : cy * (1.0 - 0.5 / j);
+        r[4 * j] = wn;
+        r[4 * j + 1] = ws;
+        r[4 * j + 2] = 1.0 / (2.0 * cx + wn + ws);
+        r[4 * j + 3] = j == 0 ? 0.125 : double(j);
+    }
+    return r;
+}
+
 template <class T>
 static int alloc_levels(MgImpl& M, std::vector<LevelDev<T>>& lv, const std::vector<std::vector<uint8_t>>& masks,
                         const std::vector<int>& nxs, const std::vector<int>& nys) {
@@ -1225,6 +1314,21 @@ static int alloc_levels(MgImpl& M, std::vector<LevelDev<T>>& lv, const std::vect
         PIC_CUDA(cudaMemset(v.eu, 0, bytes));
         PIC_CUDA(cudaMemset(v.g, 0, bytes));
         v.ec = v.e;
+        v.rz = nullptr;
+        if (M.rz) {
+            const std::vector<double> rd = rz_rows(v.ny, hx, hy);
+            std::vector<T> rt(rd.begin(), rd.end());
+            T* d = nullptr;
+            PIC_CUDA(cudaMalloc(&d, rt.size() * sizeof(T)));
+            M.allocs.push_back(d);
+            PIC_CUDA(cudaMemcpy(d, rt.data(), rt.size() * sizeof(T), cudaMemcpyHostToDevice));
+            v.rz = d;
+            if (l == 0) {
+                PIC_CUDA(cudaMalloc(&M.rz0, rd.size() * sizeof(double)));
+                M.allocs.push_back(M.rz0);
+                PIC_CUDA(cudaMemcpy(M.rz0, rd.data(), rd.size() * sizeof(double), cudaMemcpyHostToDevice));
+            }
+        }
         lv.push_back(v);
     }
     return PIC_OK;
@@ -1265,13 +1369,19 @@ static bool invert(std::vector<double>& a, int n) {
 
 template <class T>
 static int configure_kernels(MgImpl& M) {
-    const size_t down = down_smem<T>(M.o.pre_sweeps), up = up_smem<T>(M.o.post_sweeps);
+    const size_t down = down_smem<T>(M.o.pre_sweeps, M.rz), up = up_smem<T>(M.o.post_sweeps, M.rz);
     if (down > 227 * 1024 || up > 227 * 1024 || M.cl[0].smem > 227 * 1024 || M.cl[1].smem > 227 * 1024)
         return fail(PIC_ERR_BAD_ARG, "multigrid: shared memory too large (sweeps %d/%d)", M.o.pre_sweeps,
                     M.o.post_sweeps);
-    PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(down_kernel<T>(M.o.pre_sweeps)), down));
-    PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(up_kernel<T>(M.o.post_sweeps)), up));
-    PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(k_mg_coarse<T>), M.cl[0].smem));
+    if (M.rz) {
+        PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(down_kernel<T, true>(M.o.pre_sweeps)), down));
+        PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(up_kernel<T, true>(M.o.post_sweeps)), up));
+        PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(k_mg_coarse<T, true>), M.cl[0].smem));
+        return PIC_OK;  // r-z solves use the graph and host loops only
+    }
+    PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(down_kernel<T, false>(M.o.pre_sweeps)), down));
+    PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(up_kernel<T, false>(M.o.post_sweeps)), up));
+    PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(k_mg_coarse<T, false>), M.cl[0].smem));
     M.solve_smem = std::max(std::max(down, up), M.cl[1].smem);
     PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(k_mg_solve<T>), M.solve_smem));
     int per_sm = 0;
@@ -1307,7 +1417,8 @@ static int build_layout(MgImpl& M, int first, const std::vector<int>& nxs, const
         std::vector<uint8_t> m(pad16(G), 1);
         for (int j = 0; j < ny; ++j)
             for (int i = 0; i < nx; ++i)
-                m[size_t(j) * nx + i] = (i == 0 || j == 0 || i == nx - 1 || j == ny - 1 || masks[l][size_t(j) * nx + i]);
+                m[size_t(j) * nx + i] = (i == 0 || (j == 0 && !M.rz) || i == nx - 1 || j == ny - 1 ||
+                                         masks[l][size_t(j) * nx + i]);
         img.insert(img.end(), m.begin(), m.end());
         off += m.size();
     }
@@ -1441,6 +1552,7 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
         if (opts->omega > 0) M.o.omega = opts->omega;
         if (opts->coarsest_max >= 3) M.o.coarsest_max = opts->coarsest_max;
         M.o.launch_mode = opts->launch_mode;
+        M.o.geometry = opts->geometry;
     }
     auto bail = [&](int code) {
         mg_release(mg);
@@ -1452,6 +1564,13 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
         return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: at most 8 pre/post sweeps"));
     if (M.o.launch_mode < PIC_MG_PERSISTENT || M.o.launch_mode > PIC_MG_CLUSTER)
         return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: unknown launch mode %d", M.o.launch_mode));
+    if (M.o.geometry != PIC_GEOM_CARTESIAN && M.o.geometry != PIC_GEOM_RZ)
+        return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: unknown geometry %d", M.o.geometry));
+    M.rz = M.o.geometry == PIC_GEOM_RZ;
+    // r-z solves run in the graph or host loop (the persistent and cluster
+    // kernels are Cartesian)
+    if (M.rz && (M.o.launch_mode == PIC_MG_PERSISTENT || M.o.launch_mode == PIC_MG_CLUSTER))
+        M.o.launch_mode = PIC_MG_GRAPH_LOOP;
     M.precision = M.o.precision;
     M.nx = nx;
     M.ny = ny;
@@ -1484,7 +1603,7 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
     const int ncx = nxs.back(), ncy = nys.back();
     std::vector<int> idx;
     std::vector<int> where(size_t(ncx) * ncy, -1);
-    for (int j = 1; j < ncy - 1; ++j)
+    for (int j = M.rz ? 0 : 1; j < ncy - 1; ++j)
         for (int i = 1; i < ncx - 1; ++i)
             if (!masks.back()[size_t(j) * ncx + i]) {
                 where[size_t(j) * ncx + i] = int(idx.size());
@@ -1496,15 +1615,17 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
     if (M.nfree_c > 0) {
         const double hx = dx * double(1 << (M.L - 1)), hy = dy * double(1 << (M.L - 1));
         const double ccx = 1.0 / (hx * hx), ccy = 1.0 / (hy * hy);
+        const std::vector<double> rows = M.rz ? rz_rows(ncy, hx, hy) : std::vector<double>();
         const int n = M.nfree_c;
         std::vector<double> A(size_t(n) * n, 0.0);
         for (int a = 0; a < n; ++a) {
-            const int k = idx[a];
-            A[size_t(a) * n + a] = -2.0 * (ccx + ccy);
-            const int nb[4] = {k - 1, k + 1, k - ncx, k + ncx};
-            const double w[4] = {ccx, ccx, ccy, ccy};
+            const int k = idx[a], j = k / ncx;
+            const double wn = M.rz ? rows[4 * j] : ccy, ws = M.rz ? rows[4 * j + 1] : ccy;
+            A[size_t(a) * n + a] = -(2.0 * ccx + wn + ws);
+            const int nb[4] = {k - 1, k + 1, j > 0 ? k - ncx : -1, k + ncx};
+            const double w[4] = {ccx, ccx, ws, wn};
             for (int q = 0; q < 4; ++q) {
-                const int b = where[nb[q]];
+                const int b = nb[q] >= 0 ? where[nb[q]] : -1;
                 if (b >= 0) A[size_t(a) * n + b] += w[q];
             }
         }
@@ -1559,15 +1680,28 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
     return PIC_OK;
 }
 
+// The FP64 residual and the loop decision (k_mg_r0) of either geometry.
+template <class T>
+static void launch_r0(MgImpl& M, const std::vector<LevelDev<T>>& lv, double* phi, const double* f, double tol,
+                      int max_cycles, int initial, cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st) {
+    const double cx = 1.0 / (M.dx * M.dx), cy = 1.0 / (M.dy * M.dy);
+    if (M.rz)
+        k_mg_r0<T, true><<<M.grd0, M.blk0, 0, st>>>(phi, f, lv[0].mask, M.nx, M.ny, cx, cy, lv[0].g, M.N, tol * tol,
+                                                    max_cycles, initial, cond, use_cond, M.rz0);
+    else
+        k_mg_r0<T, false><<<M.grd0, M.blk0, 0, st>>>(phi, f, lv[0].mask, M.nx, M.ny, cx, cy, lv[0].g, M.N, tol * tol,
+                                                     max_cycles, initial, cond, use_cond, nullptr);
+}
+
 // One V-cycle followed by the residual check, launched on stream st.
 template <class T>
 static int launch_cycle(MgImpl& M, std::vector<LevelDev<T>>& lv_in, double* phi, const double* f, double tol,
                         int max_cycles, cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st, int& count) {
     const std::vector<LevelDev<T>> lv = with_corrections(lv_in, M.Lc);
     const T omega = T(M.o.omega);
-    const size_t down = down_smem<T>(M.o.pre_sweeps), up = up_smem<T>(M.o.post_sweeps);
-    const DownKernel<T> kdown = down_kernel<T>(M.o.pre_sweeps);
-    const UpKernel<T> kup = up_kernel<T>(M.o.post_sweeps);
+    const size_t down = down_smem<T>(M.o.pre_sweeps, M.rz), up = up_smem<T>(M.o.post_sweeps, M.rz);
+    const DownKernel<T> kdown = M.rz ? down_kernel<T, true>(M.o.pre_sweeps) : down_kernel<T, false>(M.o.pre_sweeps);
+    const UpKernel<T> kup = M.rz ? up_kernel<T, true>(M.o.post_sweeps) : up_kernel<T, false>(M.o.post_sweeps);
     count = 0;
     for (int l = 0; l < M.Lc; ++l) {
         const dim3 g(div_up(lv[l].nx, kMgTile), div_up(lv[l].ny, kMgTile));
@@ -1576,15 +1710,15 @@ static int launch_cycle(MgImpl& M, std::vector<LevelDev<T>>& lv_in, double* phi,
     }
     CoarseDesc<T> D{};
     fill_coarse(M, M.cl[0], lv, phi, D);
-    k_mg_coarse<T><<<1, kCoarseThreads, M.cl[0].smem, st>>>(D);
+    if (M.rz) k_mg_coarse<T, true><<<1, kCoarseThreads, M.cl[0].smem, st>>>(D);
+    else k_mg_coarse<T, false><<<1, kCoarseThreads, M.cl[0].smem, st>>>(D);
     ++count;
     for (int l = M.Lc - 1; l >= 0; --l) {
         const dim3 g(div_up(lv[l].nx, kMgTile), div_up(lv[l].ny, kMgTile));
         kup<<<g, kMgThreads, up, st>>>(lv[l], lv[l + 1], omega, l == 0 ? phi : nullptr);
         ++count;
     }
-    k_mg_r0<T><<<M.grd0, M.blk0, 0, st>>>(phi, f, lv[0].mask, M.nx, M.ny, 1.0 / (M.dx * M.dx), 1.0 / (M.dy * M.dy),
-                                          lv[0].g, M.N, tol * tol, max_cycles, 0, cond, use_cond);
+    launch_r0(M, lv, phi, f, tol, max_cycles, 0, cond, use_cond, st);
     ++count;
     PIC_LAUNCH_CHECK();
     return PIC_OK;
@@ -1601,8 +1735,7 @@ static int capture_solve(MgImpl& M, std::vector<LevelDev<T>>& lv, double* phi, c
     if (cs != cudaStreamCaptureStatusActive) return fail(PIC_ERR_BAD_ARG, "multigrid: stream is not capturing");
     cudaGraphConditionalHandle h;
     PIC_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
-    k_mg_r0<T><<<M.grd0, M.blk0, 0, st>>>(phi, f, lv[0].mask, M.nx, M.ny, 1.0 / (M.dx * M.dx), 1.0 / (M.dy * M.dy),
-                                          lv[0].g, M.N, tol * tol, max_cycles, 1, h, 1);
+    launch_r0(M, lv, phi, f, tol, max_cycles, 1, h, 1, st);
     PIC_LAUNCH_CHECK();
     PIC_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
     cudaGraphNodeParams p{};
@@ -1770,8 +1903,7 @@ int mg_read_info(MgImpl& M, pic_mg_info* info);
 template <class T>
 static int solve_eager(MgImpl& M, std::vector<LevelDev<T>>& lv, double* phi, const double* f, double tol,
                        int max_cycles, cudaStream_t st) {
-    k_mg_r0<T><<<M.grd0, M.blk0, 0, st>>>(phi, f, lv[0].mask, M.nx, M.ny, 1.0 / (M.dx * M.dx), 1.0 / (M.dy * M.dy),
-                                          lv[0].g, M.N, tol * tol, max_cycles, 1, cudaGraphConditionalHandle{}, 0);
+    launch_r0(M, lv, phi, f, tol, max_cycles, 1, cudaGraphConditionalHandle{}, 0, st);
     PIC_LAUNCH_CHECK();
     pic_mg_info info{};
     for (;;) {

@@ -106,25 +106,26 @@ __global__ void k_deposit(const float* __restrict__ x, const float* __restrict__
 }
 
 // E = -grad(phi) (src/Grid.py:167-194), FP64 arithmetic, rounded once to float.
+// axis: r-z geometry, where row 0 is the axis and E_r vanishes there by symmetry.
 __device__ __forceinline__ double2 grad_node(const double* __restrict__ phi, int i, int j, int nx, int ny,
-                                             double dx, double dy) {
+                                             double dx, double dy, bool axis) {
     const long k = long(j) * nx + i;
     double ex, ey;
     if (i > 0 && i < nx - 1) ex = -(phi[k + 1] - phi[k - 1]) / (2.0 * dx);
     else if (i == 0) ex = -(phi[k + 1] - phi[k]) / dx;
     else ex = -(phi[k] - phi[k - 1]) / dx;
     if (j > 0 && j < ny - 1) ey = -(phi[k + nx] - phi[k - nx]) / (2.0 * dy);
-    else if (j == 0) ey = -(phi[k + nx] - phi[k]) / dy;
+    else if (j == 0) ey = axis ? 0.0 : -(phi[k + nx] - phi[k]) / dy;
     else ey = -(phi[k] - phi[k - nx]) / dy;
     return make_double2(ex, ey);
 }
 
 __global__ void k_update_E(const double* __restrict__ phi, float* __restrict__ Ex, float* __restrict__ Ey,
-                           float2* __restrict__ E2, int nx, int ny, double dx, double dy) {
+                           float2* __restrict__ E2, int nx, int ny, double dx, double dy, int axis) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
     if (i >= nx) return;
-    const double2 e = grad_node(phi, i, j, nx, ny, dx, dy);
+    const double2 e = grad_node(phi, i, j, nx, ny, dx, dy, axis != 0);
     const long k = long(j) * nx + i;
     const float fx = float(e.x), fy = float(e.y);
     if (Ex) Ex[k] = fx;
@@ -134,14 +135,22 @@ __global__ void k_update_E(const double* __restrict__ phi, float* __restrict__ E
 
 // rho -> f = -rho/eps0 on free nodes.  With phi_prev given, also replaces the
 // initial guess by its linear extrapolation in time, phi <- 2 phi - phi_prev,
-// on free nodes and keeps the old phi in phi_prev.
+// on free nodes and keeps the old phi in phi_prev.  With rowf (r-z geometry),
+// the deposited charge of row j (per dx*dy) becomes a charge density first:
+// rho *= rowf[j] = dx*dy / V_j; the snapshot holds the density.
 __global__ void k_form_rhs(const float* __restrict__ rho, const uint8_t* __restrict__ dirichlet, double neg_inv_eps0,
                            double* __restrict__ f, float* __restrict__ rho_snapshot, float* __restrict__ rho_zero,
-                           double* __restrict__ phi, double* __restrict__ phi_prev, long G) {
+                           double* __restrict__ phi, double* __restrict__ phi_prev, long G,
+                           const double* __restrict__ rowf, int nx) {
     for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < G; k += long(gridDim.x) * blockDim.x) {
-        const float r = rho[k];
+        float r = rho[k];
+        double rd = double(r);
+        if (rowf) {
+            rd *= rowf[int(k) / nx];
+            r = float(rd);
+        }
         const bool dir = dirichlet[k] != 0;
-        f[k] = dir ? 0.0 : double(r) * neg_inv_eps0;
+        f[k] = dir ? 0.0 : rd * neg_inv_eps0;
         if (rho_snapshot) rho_snapshot[k] = r;
         if (rho_zero) rho_zero[k] = 0.0f;
         if (phi_prev && !dir) {
@@ -149,6 +158,27 @@ __global__ void k_form_rhs(const float* __restrict__ rho, const uint8_t* __restr
             phi[k] = 2.0 * p - phi_prev[k];
             phi_prev[k] = p;
         }
+    }
+}
+
+// Deposited charge (per dx*dy) -> r-z charge density, rho_j *= dx*dy / V_j.
+__global__ void k_rz_density(float* __restrict__ rho, int nx, int ny, double dy, long G) {
+    for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < G; k += long(gridDim.x) * blockDim.x)
+        rho[k] = float(double(rho[k]) * (1.0 / rz_row_volume(int(k / nx), ny, dy)));
+}
+
+// The r-z drift of every live particle (drift_rz); dead slots are skipped.
+__global__ void k_update_R_rz(float* __restrict__ x, float* __restrict__ y, const float* __restrict__ vx,
+                              float* __restrict__ vy, float* __restrict__ vz, int n, float dtdx, float dtdy) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        float px = x[p], py = y[p];
+        if (!is_live(px)) continue;
+        float v1 = vy[p], v2 = vz[p];
+        drift_rz(px, py, vx[p], v1, v2, dtdx, dtdy);
+        x[p] = px;
+        y[p] = py;
+        vy[p] = v1;
+        vz[p] = v2;
     }
 }
 
@@ -161,16 +191,17 @@ int grid_blocks(long n, int threads) {
 }
 
 int launch_update_E(const double* phi, float* Ex, float* Ey, float2* E2, int nx, int ny, double dx, double dy,
-                    cudaStream_t st) {
+                    cudaStream_t st, bool axis) {
     dim3 grid(div_up(nx, 128), ny);
-    k_update_E<<<grid, 128, 0, st>>>(phi, Ex, Ey, E2, nx, ny, dx, dy);
+    k_update_E<<<grid, 128, 0, st>>>(phi, Ex, Ey, E2, nx, ny, dx, dy, axis ? 1 : 0);
     PIC_LAUNCH_CHECK();
     return PIC_OK;
 }
 
 int launch_form_rhs(const float* rho, const uint8_t* dirichlet, double eps0, double* f, float* snapshot,
-                    float* zero, double* phi, double* phi_prev, long G, cudaStream_t st) {
-    k_form_rhs<<<grid_blocks(G, 256), 256, 0, st>>>(rho, dirichlet, -1.0 / eps0, f, snapshot, zero, phi, phi_prev, G);
+                    float* zero, double* phi, double* phi_prev, long G, cudaStream_t st, const double* rowf, int nx) {
+    k_form_rhs<<<grid_blocks(G, 256), 256, 0, st>>>(rho, dirichlet, -1.0 / eps0, f, snapshot, zero, phi, phi_prev, G,
+                                                    rowf, nx);
     PIC_LAUNCH_CHECK();
     return PIC_OK;
 }
@@ -232,7 +263,35 @@ int pic_update_E(const double* d_phi, float* d_Ex, float* d_Ey, int nx, int ny, 
     clear_error();
     if (!d_phi || !d_Ex || !d_Ey || nx < 2 || ny < 2 || !(dx > 0) || !(dy > 0))
         return fail(PIC_ERR_BAD_ARG, "pic_update_E: bad arguments");
-    return launch_update_E(d_phi, d_Ex, d_Ey, nullptr, nx, ny, dx, dy, as_stream(stream));
+    return launch_update_E(d_phi, d_Ex, d_Ey, nullptr, nx, ny, dx, dy, as_stream(stream), false);
+}
+
+int pic_update_E_rz(const double* d_phi, float* d_Ex, float* d_Ey, int nx, int ny, double dx, double dy,
+                    void* stream) {
+    clear_error();
+    if (!d_phi || !d_Ex || !d_Ey || nx < 2 || ny < 2 || !(dx > 0) || !(dy > 0))
+        return fail(PIC_ERR_BAD_ARG, "pic_update_E_rz: bad arguments");
+    return launch_update_E(d_phi, d_Ex, d_Ey, nullptr, nx, ny, dx, dy, as_stream(stream), true);
+}
+
+int pic_rz_density(float* d_rho, int nx, int ny, double dy, void* stream) {
+    clear_error();
+    if (!d_rho || nx < 2 || ny < 2 || !(dy > 0)) return fail(PIC_ERR_BAD_ARG, "pic_rz_density: bad arguments");
+    const long G = long(nx) * ny;
+    k_rz_density<<<grid_blocks(G, 256), 256, 0, as_stream(stream)>>>(d_rho, nx, ny, dy, G);
+    PIC_LAUNCH_CHECK();
+    return PIC_OK;
+}
+
+int pic_update_R_rz(float* d_x, float* d_y, const float* d_vx, float* d_vy, float* d_vz, int n, float dtdx,
+                    float dtdy, void* stream) {
+    clear_error();
+    if (n < 0 || (n > 0 && (!d_x || !d_y || !d_vx || !d_vy || !d_vz)))
+        return fail(PIC_ERR_BAD_ARG, "pic_update_R_rz: bad arguments");
+    if (n == 0) return PIC_OK;
+    k_update_R_rz<<<grid_blocks(n, 256), 256, 0, as_stream(stream)>>>(d_x, d_y, d_vx, d_vy, d_vz, n, dtdx, dtdy);
+    PIC_LAUNCH_CHECK();
+    return PIC_OK;
 }
 
 int pic_form_rhs(const float* d_rho, const uint8_t* d_dirichlet, double eps0, double* d_f, int nx, int ny,
@@ -241,7 +300,7 @@ int pic_form_rhs(const float* d_rho, const uint8_t* d_dirichlet, double eps0, do
     if (!d_rho || !d_dirichlet || !d_f || nx < 2 || ny < 2 || !(eps0 > 0))
         return fail(PIC_ERR_BAD_ARG, "pic_form_rhs: bad arguments");
     return launch_form_rhs(d_rho, d_dirichlet, eps0, d_f, nullptr, nullptr, nullptr, nullptr, long(nx) * ny,
-                           as_stream(stream));
+                           as_stream(stream), nullptr, 0);
 }
 
 }  // extern "C"

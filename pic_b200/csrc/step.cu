@@ -30,9 +30,9 @@ namespace pic {
 
 int grid_blocks(long n, int threads);
 int launch_update_E(const double* phi, float* Ex, float* Ey, float2* E2, int nx, int ny, double dx, double dy,
-                    cudaStream_t st);
+                    cudaStream_t st, bool axis);
 int launch_form_rhs(const float* rho, const uint8_t* dirichlet, double eps0, double* f, float* snapshot, float* zero,
-                    double* phi, double* phi_prev, long G, cudaStream_t st);
+                    double* phi, double* phi_prev, long G, cudaStream_t st, const double* rowf, int nx);
 int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const pic_mg_options* opts, pic_mg** out);
 int mg_body_launches(pic_mg* mg);
 long long mg_total_cycles(pic_mg* mg);
@@ -41,7 +41,7 @@ int mg_launch_graph(pic_mg* mg, double* phi, const double* f, double tol, int ma
 int mg_info(pic_mg* mg, pic_mg_info* info);
 int diagnostics(const DiagSpecies* sp, const double* mass, const double* np2c, int ns, const double* phi,
                 const float* rho, const float* Ex, const float* Ey, int nx, int ny, double dx, double dy, double eps0,
-                double* scratch, pic_sim_diag* out, cudaStream_t st);
+                const double* rowv, double* scratch, pic_sim_diag* out, cudaStream_t st);
 size_t diagnostics_scratch_doubles();
 bool mg_uses_graph(pic_mg* mg);
 
@@ -93,6 +93,7 @@ struct PushArgs {
     const unsigned* cbits[PIC_MAX_SPECIES];  // null-collision candidate bit per slot (k_mcc_bits), or null
     const unsigned *vbits, *hbits;           // internal electrode edges (hits_electrode), when `electrodes`
     int electrodes;
+    int rz;           // r-z geometry: drift_rz (y radial, vz azimuthal)
     int2* cand;       // collision candidates (species, slot), processed by k_collide after the pass
     int* cand_count;
     int cand_cap;
@@ -340,6 +341,8 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
         float* const pvy = pvx + kBufStride;
         const SpeciesConst C = A.sp[s];
         const unsigned* const cbits = (A.do_mcc && A.mcc->sp[s].nproc > 0) ? A.cbits[s] : nullptr;
+        // r-z: the azimuthal velocity is not staged; it is read and written in place
+        float* const gvz = A.rz ? A.state[s].cur[4] + b : nullptr;
         unsigned my_abs = 0, my_cand = 0, my_elec = 0;
 #pragma unroll
         for (int k = 0; k < kPushP; ++k) {
@@ -384,8 +387,14 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
             }
             if (A.do_drift) {
                 const float x0 = x, y0 = y;
-                x = __fmaf_rn(vx, C.dtdx, x);
-                y = __fmaf_rn(vy, C.dtdy, y);
+                if (gvz) {
+                    float vz = gvz[l];
+                    drift_rz(x, y, vx, vy, vz, C.dtdx, C.dtdy);
+                    gvz[l] = vz;
+                } else {
+                    x = __fmaf_rn(vx, C.dtdx, x);
+                    y = __fmaf_rn(vy, C.dtdy, y);
+                }
                 if (!(x >= 0.0f && x <= float(A.nx - 1) && y >= 0.0f && y <= float(A.ny - 1))) {
                     x = __int_as_float(0x7fc00000);
                     y = x;
@@ -495,8 +504,12 @@ __global__ void __launch_bounds__(128) k_collide(PushArgs A) {
         }
         if (A.do_drift) {
             const float x0 = x, y0 = y;
-            x = __fmaf_rn(vx, C.dtdx, x);
-            y = __fmaf_rn(vy, C.dtdy, y);
+            if (A.rz) {
+                drift_rz(x, y, vx, vy, vz, C.dtdx, C.dtdy);
+            } else {
+                x = __fmaf_rn(vx, C.dtdx, x);
+                y = __fmaf_rn(vy, C.dtdy, y);
+            }
             if (!(x >= 0.0f && x <= float(A.nx - 1) && y >= 0.0f && y <= float(A.ny - 1))) {
                 x = __int_as_float(0x7fc00000);
                 y = x;
@@ -530,11 +543,15 @@ __global__ void k_merge_births(PushArgs A) {
         const int s = A.births.species[i];
         const SpeciesConst C = A.sp[s];
         float x = A.births.x[i], y = A.births.y[i];
-        const float vx = A.births.vx[i], vy = A.births.vy[i], vz = A.births.vz[i];
+        float vx = A.births.vx[i], vy = A.births.vy[i], vz = A.births.vz[i];
         if (A.do_drift) {
             const float x0 = x, y0 = y;
-            x = __fmaf_rn(vx, C.dtdx, x);
-            y = __fmaf_rn(vy, C.dtdy, y);
+            if (A.rz) {
+                drift_rz(x, y, vx, vy, vz, C.dtdx, C.dtdy);
+            } else {
+                x = __fmaf_rn(vx, C.dtdx, x);
+                y = __fmaf_rn(vy, C.dtdy, y);
+            }
             // a product that leaves the domain or reaches an electrode in its
             // first drift is never stored
             if (!(x >= 0.0f && x <= float(A.nx - 1) && y >= 0.0f && y <= float(A.ny - 1))) continue;
@@ -689,6 +706,9 @@ struct SimImpl {
     unsigned *vbits = nullptr, *hbits = nullptr;  // internal electrode edges
     double* diag = nullptr;                        // diagnostics scratch
     bool electrodes = false;
+    bool rz = false;                               // r-z geometry (desc.mg.geometry)
+    double* rowf = nullptr;  // r-z: per row dx*dy / V_j, deposit -> charge density (null: Cartesian)
+    double* rowv = nullptr;  // r-z: per row V_j / (dx*dy)
     unsigned** d_cbits = nullptr;         // device copy of cbits
     int* d_nseg = nullptr;                // 256-slot segments per species (0: no collisions)
     int cbits_segments = 0;               // sum of d_nseg
@@ -799,6 +819,7 @@ static PushArgs push_args(SimImpl& S, int kick, int mcc, int drift, int deposit,
     A.vbits = S.vbits;
     A.hbits = S.hbits;
     A.electrodes = S.electrodes ? 1 : 0;
+    A.rz = S.rz ? 1 : 0;
     A.cand = S.cand;
     A.cand_count = S.cand_count;
     A.cand_cap = S.cand_cap;
@@ -844,7 +865,7 @@ static int field_solve(SimImpl& S, cudaStream_t st, bool capturing) {
         PhaseTimer t(S, PIC_PHASE_RHS, st);
         // from the second solve on, the guess is extrapolated from the last two potentials
         PIC_TRY(launch_form_rhs(S.rho_acc, S.dirichlet, S.d.eps0, S.f, S.rho_out, S.rho_acc, S.phi,
-                                S.have_prev ? S.phi_prev : nullptr, S.G, st));
+                                S.have_prev ? S.phi_prev : nullptr, S.G, st, S.rowf, S.nx));
     }
     {
         PhaseTimer t(S, PIC_PHASE_SOLVE, st);
@@ -857,7 +878,7 @@ static int field_solve(SimImpl& S, cudaStream_t st, bool capturing) {
     }
     {
         PhaseTimer t(S, PIC_PHASE_EFIELD, st);
-        PIC_TRY(launch_update_E(S.phi, S.Ex, S.Ey, S.E2, S.nx, S.ny, S.d.dx, S.d.dy, st));
+        PIC_TRY(launch_update_E(S.phi, S.Ex, S.Ey, S.E2, S.nx, S.ny, S.d.dx, S.d.dy, st, S.rz));
     }
     S.launches += 2;
     S.solves += 1;
@@ -922,6 +943,19 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
     S.G = long(S.nx) * S.ny;
     S.rw = S.d.tile + 1 + 2 * kHalo;
     PIC_TRY(mg_create(S.nx, S.ny, d->dx, d->dy, d->h_dirichlet, &d->mg, &S.mg));
+    if (d->mg.geometry == PIC_GEOM_RZ) {
+        // r-z: deposits become densities with the node volumes of each row
+        S.rz = true;
+        std::vector<double> f(size_t(S.ny)), v(size_t(S.ny));
+        for (int j = 0; j < S.ny; ++j) {
+            v[j] = rz_row_volume(j, S.ny, d->dy);
+            f[j] = 1.0 / v[j];
+        }
+        PIC_TRY(dalloc(S, &S.rowf, size_t(S.ny)));
+        PIC_TRY(dalloc(S, &S.rowv, size_t(S.ny)));
+        PIC_CUDA(cudaMemcpy(S.rowf, f.data(), sizeof(double) * S.ny, cudaMemcpyHostToDevice));
+        PIC_CUDA(cudaMemcpy(S.rowv, v.data(), sizeof(double) * S.ny, cudaMemcpyHostToDevice));
+    }
     long max_cap = 0;
     for (int s = 0; s < S.ns; ++s) {
         const pic_species_desc& sp = d->species[s];
@@ -1419,7 +1453,7 @@ int pic_sim_diagnostics(pic_sim* sim, pic_sim_diag* out, void* stream) {
         np2c[s] = S.d.species[s].np2c;
     }
     return diagnostics(sp, mass, np2c, S.ns, S.phi, S.rho_out, S.Ex, S.Ey, S.nx, S.ny, S.d.dx, S.d.dy, S.d.eps0,
-                       S.diag, out, st);
+                       S.rowv, S.diag, out, st);
 }
 
 int pic_sim_read_counters(pic_sim* sim, pic_sim_counters* out, void* stream) {

@@ -12,6 +12,11 @@ the solver to converge (the reference's own wiring cannot run):
   * `omega` is the smoother's over-relaxation; the reference's 1.9 is
     accepted, but a red-black smoother inside a V-cycle converges fastest
     near 1.15 (measured on 513^2: 5 V(2,2) cycles to 1e-8 instead of 6 at 1.0).
+
+geometry="rz" solves the axisymmetric Poisson equation (the reference's
+cylindrical Laplacian, src/Solvers.py:100-166, which its multigrid never
+used): x is the axis, y the radius with row 0 on the axis; the axis row is
+free (symmetry) rather than a boundary.
 """
 from __future__ import annotations
 
@@ -25,7 +30,7 @@ from . import _lib
 
 class MultigridSolver:
     def __init__(self, bc_mask, nx, ny, h, levels=4, omega=1.15, precision="mixed", pre_sweeps=2, post_sweeps=2,
-                 hy=None, launch="graph"):
+                 hy=None, launch="graph", geometry="cartesian"):
         self.nx, self.ny = int(nx), int(ny)
         self.h = float(h)
         self.hy = float(h if hy is None else hy)
@@ -35,8 +40,9 @@ class MultigridSolver:
         if mask.size != self.nx * self.ny:
             raise ValueError("bc_mask must have nx*ny entries")
         self.precision = precision
+        self.geometry = geometry
         opts = _lib.MgOptions(_lib.PIC_MG_MIXED if precision == "mixed" else _lib.PIC_MG_FP64, pre_sweeps,
-                              post_sweeps, self.omega, 9, _lib.MG_LAUNCH_MODES[launch])
+                              post_sweeps, self.omega, 9, _lib.MG_LAUNCH_MODES[launch], _lib.GEOMETRIES[geometry])
         self._h = C.c_void_p()
         _lib.call("pic_mg_create", self.nx, self.ny, self.h, self.hy, mask.ctypes.data, C.byref(opts),
                   C.byref(self._h))

@@ -55,14 +55,20 @@ class PICSimulation:
 
     species: list of dicts with keys name, charge (C), mass (kg), np2c, capacity.
     dirichlet / phi_bc: node mask (1 = Dirichlet) and potentials, nx*ny.
+    geometry: "cartesian", or "rz" for the axisymmetric r-z step (the
+    reference's Grid.Cylindrical = 1): x axial, y radial (row 0 the axis, a
+    free row), vx axial, vy radial, vz azimuthal; np2c counts real particles;
+    rho is the charge density of the node volumes; the drift turns (vy, vz)
+    into the particle's new local frame.
     """
 
     def __init__(self, nx, ny, dx, dy, dt, species, dirichlet, phi_bc=None, tol=1e-8, max_cycles=50,
                  precision="mixed", pre_sweeps=2, post_sweeps=2, omega=1.15, sort_interval=20, tile=16,
                  mcc: MccTables | None = None, seed=0, use_graph=False, eps0=Consts.eps0, mg_launch="graph",
-                 coarsest_max=9):
+                 coarsest_max=9, geometry="cartesian"):
         self.nx, self.ny, self.dx, self.dy, self.dt = int(nx), int(ny), float(dx), float(dy), float(dt)
         self.species = list(species)
+        self.geometry = geometry
         d = _lib.SimDesc()
         d.nx, d.ny, d.dx, d.dy, d.dt, d.eps0 = self.nx, self.ny, self.dx, self.dy, self.dt, eps0
         d.nspecies = len(self.species)
@@ -77,7 +83,8 @@ class PICSimulation:
         d.tol = float(tol)
         d.max_cycles = int(max_cycles)
         d.mg = _lib.MgOptions(_lib.PIC_MG_MIXED if precision == "mixed" else _lib.PIC_MG_FP64, pre_sweeps,
-                              post_sweeps, omega, int(coarsest_max), _lib.MG_LAUNCH_MODES[mg_launch])
+                              post_sweeps, omega, int(coarsest_max), _lib.MG_LAUNCH_MODES[mg_launch],
+                              _lib.GEOMETRIES[geometry])
         d.sort_interval = int(sort_interval)
         d.tile = int(tile)
         self._mcc_desc = mcc.desc() if mcc is not None else None
