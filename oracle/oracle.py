@@ -67,6 +67,9 @@ def lib():
         L.or_drift_absorb_electrodes_f32.argtypes = [_fp, _fp, _fp, _fp, C.c_long, C.c_float, C.c_float, C.c_int,
                                                      C.c_int, _up, _up, C.POINTER(C.c_long)]
         L.or_drift_absorb_electrodes_f32.restype = C.c_long
+        L.or_drift_rz_absorb_f32.argtypes = [_fp, _fp, _fp, _fp, _fp, C.c_long, C.c_float, C.c_float, C.c_int,
+                                             C.c_int, C.c_void_p, C.c_void_p, C.POINTER(C.c_long)]
+        L.or_drift_rz_absorb_f32.restype = C.c_long
         L.or_sort_keys.argtypes = [_fp, _fp, C.c_long, C.c_int, C.c_int, C.c_int, _up]
         L.or_counting_sort.argtypes = [_up, C.c_long, C.c_uint32, _up]
         L.or_philox4x32_10.argtypes = [_up, _up, _up]
@@ -219,6 +222,122 @@ def drift_absorb_electrodes_f32(gx, gy, vx, vy, dtdx, dtdy, m, n, vb, hb):
     a = lib().or_drift_absorb_electrodes_f32(gx, gy, vx, vy, len(gx), np.float32(dtdx), np.float32(dtdy), m, n, vb,
                                              hb, C.byref(c))
     return int(a), int(c.value)
+
+
+def drift_rz_absorb_f32(gx, gy, vx, vy, vz, dtdx, dtdy, m, n, vb=None, hb=None):
+    """r-z drift (pic_oracle.c or_drift_rz_absorb_f32) in place; (wall, electrode) counts."""
+    c = C.c_long()
+    a = lib().or_drift_rz_absorb_f32(gx, gy, vx, vy, vz, len(gx), np.float32(dtdx), np.float32(dtdy), m, n,
+                                     None if vb is None else vb.ctypes.data, None if hb is None else hb.ctypes.data,
+                                     C.byref(c))
+    return int(a), int(c.value)
+
+
+# ---- r-z operator (FP64, numpy / scipy) --------------------------------------------
+
+def rz_row_volume(j, n, dy):
+    """Node volume of row j of an r-z grid per dx*dy (m): the integral of 2 pi r
+    times the row's linear weighting function (2 pi r_j inside, pi dy/3 on the
+    axis, pi (r_top - dy/3) on the outer row)."""
+    j = np.asarray(j)
+    r = 2.0 * np.pi * j * dy
+    r = np.where(j == 0, np.pi * dy / 3.0, r)
+    return np.where(j == n - 1, np.pi * (j * dy - dy / 3.0), r)
+
+
+def rz_rows(n, dx, dy):
+    """(wN, wS, diag) per row of the build's r-z operator: conservative
+    differences of (1/r) d/dr (r dphi/dr) + d2phi/dz2, with the axis limit
+    2 d2phi/dr2 -> 4 (phi_1 - phi_0)/dy^2 on row 0."""
+    cx, cy = 1.0 / dx ** 2, 1.0 / dy ** 2
+    j = np.arange(n, dtype=np.float64)
+    with np.errstate(divide="ignore"):
+        wn = np.where(j == 0, 4.0 * cy, cy * (1.0 + 0.5 / j))
+        ws = np.where(j == 0, 0.0, cy * (1.0 - 0.5 / j))
+    return wn, ws, -(2.0 * cx + wn + ws)
+
+
+def rz_free(mask, m, n):
+    """Free nodes of an r-z grid: not masked, not on the x edges or the outer row (the axis row is free)."""
+    mk = np.asarray(mask).reshape(n, m).astype(bool).copy()
+    mk[:, 0] = mk[:, -1] = mk[-1, :] = True
+    return ~mk
+
+
+def rz_apply(phi, m, n, dx, dy):
+    """The r-z operator applied at every node with an in-grid stencil (rows
+    0..n-2, columns 1..m-2); zero elsewhere."""
+    p = np.asarray(phi, np.float64).reshape(n, m)
+    wn, ws, dg = rz_rows(n, dx, dy)
+    out = np.zeros_like(p)
+    c = p[:-1, 1:-1]
+    south = np.vstack([np.zeros((1, m - 2)), p[:-2, 1:-1]])
+    out[:-1, 1:-1] = ((p[:-1, :-2] + p[:-1, 2:]) / dx ** 2 + wn[:-1, None] * p[1:, 1:-1] + ws[:-1, None] * south
+                      + dg[:-1, None] * c)
+    return out.reshape(-1)
+
+
+def rz_residual(phi, f, mask, m, n, dx, dy):
+    """||f - L phi|| / ||f|| over the free nodes (the build's convergence measure)."""
+    free = rz_free(mask, m, n).reshape(-1)
+    r = (np.asarray(f, np.float64) - rz_apply(phi, m, n, dx, dy))[free]
+    fn = np.linalg.norm(np.asarray(f, np.float64)[free])
+    return float(np.linalg.norm(r) / (fn if fn > 0 else 1.0))
+
+
+def rz_solve(f, phi_bc, mask, m, n, dx, dy):
+    """Direct sparse solve of L phi = f on the free nodes of an r-z grid,
+    phi = phi_bc elsewhere."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spl
+
+    free = rz_free(mask, m, n).reshape(-1)
+    wn, ws, dg = rz_rows(n, dx, dy)
+    idx = np.full(m * n, -1)
+    fi = np.flatnonzero(free)
+    idx[fi] = np.arange(fi.size)
+    phi = np.asarray(phi_bc, np.float64).reshape(-1).copy()
+    rows, cols, vals = [], [], []
+    rhs = np.asarray(f, np.float64).reshape(-1)[fi].copy()
+    for a, k in enumerate(fi):
+        j, i = divmod(int(k), m)
+        rows.append(a); cols.append(a); vals.append(dg[j])
+        nb = [(k - 1, 1.0 / dx ** 2), (k + 1, 1.0 / dx ** 2), (k + m, wn[j])]
+        if j > 0:
+            nb.append((k - m, ws[j]))
+        for q, w in nb:
+            if idx[q] >= 0:
+                rows.append(a); cols.append(int(idx[q])); vals.append(w)
+            else:
+                rhs[a] -= w * phi[q]
+    A = sp.csr_matrix((vals, (rows, cols)), shape=(fi.size, fi.size))
+    phi[fi] = spl.spsolve(A, rhs)
+    return phi
+
+
+def ref_cylindrical_laplacian(m, n, dz, dr):
+    """Dense restatement of the reference's Laplacian_cylindrical_csr
+    (src/Solvers.py:100-166) as its source reads: m nodes in z (fast index), n
+    in r; main diagonal -4; z neighbours 1 except across rows; lower r
+    neighbour of row r 1 - 1/(2 r/dr); upper r neighbour of row r set from the
+    next row's index, 1 + 1/(2 (r+1)/dr), and left 0 for row n-2; axis rows
+    -4 with z neighbours and 2 towards row 1."""
+    size = m * n
+    A = np.zeros((size, size))
+    for k in range(size):
+        A[k, k] = -4.0
+        if (k + 1) % m != 0 and k + 1 < size:
+            A[k, k + 1] = 1.0
+            A[k + 1, k] = 1.0
+    for i, r in enumerate(range(1, n)):
+        lo = i * m
+        for k in range(lo, lo + m):
+            if i + 1 < n - 1:
+                A[k, k + m] = 1.0 + 1.0 / (2 * r / dr)
+            A[k + m, k] = 1.0 - 1.0 / (2 * r / dr)
+    for k in range(m):
+        A[k, k + m] = 2.0
+    return A
 
 
 def residual_f64(phi, f, dirichlet, m, n, dx, dy, want_r=False):

@@ -314,6 +314,61 @@ long or_drift_absorb_electrodes_f32(float* gx, float* gy, const float* vx, const
     return a;
 }
 
+/* r-z (axisymmetric) drift, the build's replacement of the planar drift and
+ * axis reflection the reference uses in cylindrical mode too
+ * (src/Particles.py:359-376, kernels K6/K7 at :251-280).  x axial, y radial
+ * (grid units), vx axial, vy radial, vz azimuthal.  The particle moves on a
+ * straight line in 3D; in the plane normal to the axis it goes from (y, 0)
+ * to (y + vy dtdy, vz dtdy), its new radius is the length of that vector and
+ * (vy, vz) are turned by its angle (Birdsall and Langdon sec. 14-12).  The
+ * operation order is the CUDA build's (drift_rz); sqrtf and / are correctly
+ * rounded, as there. */
+static void drift_rz1(float* x, float* y, float vx, float* vy, float* vz, float dtdx, float dtdy) {
+    *x = fmaf(vx, dtdx, *x);
+    const float yr = fmaf(*vy, dtdy, *y);
+    const float yt = *vz * dtdy;
+    const float r = sqrtf(fmaf(yr, yr, yt * yt));
+    if (r > 0.0f) {
+        const float c = yr / r, s = yt / r;
+        const float vr = fmaf(c, *vy, s * *vz);
+        const float vt = fmaf(c, *vz, -(s * *vy));
+        *vy = vr;
+        *vz = vt;
+    }
+    *y = r;
+}
+
+/* r-z drift of every live particle with wall absorption (x outside [0, m-1]
+ * or r > n-1) and, with vb/hb not NULL, collection by internal electrodes;
+ * returns the wall count, *collected the electrode count. */
+long or_drift_rz_absorb_f32(float* gx, float* gy, const float* vx, float* vy, float* vz, long n, float dtdx,
+                            float dtdy, int m, int nn, const uint32_t* vb, const uint32_t* hb, long* collected) {
+    long a = 0, c = 0;
+    const float X = (float)(m - 1), Y = (float)(nn - 1);
+    for (long p = 0; p < n; ++p) {
+        if (gx[p] != gx[p]) continue;
+        const float x0 = gx[p], y0 = gy[p];
+        float x = x0, y = y0, v1 = vy[p], v2 = vz[p];
+        drift_rz1(&x, &y, vx[p], &v1, &v2, dtdx, dtdy);
+        vy[p] = v1;
+        vz[p] = v2;
+        if (!(x >= 0.0f && x <= X && y >= 0.0f && y <= Y)) {
+            gx[p] = NAN;
+            gy[p] = NAN;
+            ++a;
+        } else if (vb && hb && or_hits_electrode(x0, y0, x, y, m, nn, vb, hb)) {
+            gx[p] = NAN;
+            gy[p] = NAN;
+            ++c;
+        } else {
+            gx[p] = x;
+            gy[p] = y;
+        }
+    }
+    if (collected) *collected = c;
+    return a;
+}
+
 /* ------------------------------------------------------------------ */
 /* Cell sort (the deterministic replacement of src/Particles.py:550-632) */
 /* ------------------------------------------------------------------ */

@@ -13,11 +13,13 @@ substrings and calls eval (so that a variable `X` would also rewrite `Jmax`),
 expressions are parsed and only numbers, names, + - * / // % **, unary
 signs and abs/int/float/pow/min/max/sqrt calls are evaluated.
 
-`build_simulation` turns a configuration into a PICSimulation (Cartesian):
-Grid J x K nodes over [x1s, x1f] x [x2s, x2f], the Equipotential segments as
-Dirichlet nodes (src/Boundaries.py:36-52; the grid edges are always
-Dirichlet), the Species, uniform Load boxes with Maxwellian velocities, and
-Control.dt.
+`build_simulation` turns a configuration into a PICSimulation: Grid J x K
+nodes over [x1s, x1f] x [x2s, x2f], the Equipotential segments as Dirichlet
+nodes (src/Boundaries.py:36-52; the grid edges are always Dirichlet, except
+the axis row x2 = x2s of a cylindrical grid), the Species, uniform Load boxes
+with Maxwellian velocities, and Control.dt.  Grid.Cylindrical = 1 builds the
+axisymmetric r-z simulation (x1 axial, x2 radial), with Load radii uniform
+in volume.
 """
 from __future__ import annotations
 
@@ -169,17 +171,14 @@ def build_simulation(cfg, seed=0, temperature_eV=None, np2c=None, tol=1e-8, sort
                      cartesian=False, **kw):
     """A PICSimulation of the configuration with its Load blocks loaded.
 
-    Cylindrical grids (Grid.Cylindrical = 1) are not built: pass
-    cartesian=True to run such a file in Cartesian geometry.  Load velocities
-    are Maxwellian at Load.temperature (eV), else at `temperature_eV`, else
-    zero; np2c per Load block (Load.np2c), else `np2c`, else the reference's
-    1 (src/Particles.py:326)."""
+    Grid.Cylindrical = 1 gives the r-z simulation unless cartesian=True.
+    Load velocities are Maxwellian at Load.temperature (eV), else at
+    `temperature_eV`, else zero; np2c per Load block (Load.np2c), else
+    `np2c`, else the reference's 1 (src/Particles.py:326)."""
     from .simulation import PICSimulation
 
     grid = cfg["grid"]
-    if int(grid.get("Cylindrical", 0)) and not cartesian:
-        raise NotImplementedError("cylindrical (r-z) grids are not built; pass cartesian=True to run the file in "
-                                  "Cartesian geometry")
+    rz = bool(int(grid.get("Cylindrical", 0))) and not cartesian
     m, n = int(grid["J"]), int(grid["K"])
     for name, v in (("J", m), ("K", n)):
         if not multigrid_compatible(v):
@@ -196,7 +195,9 @@ def build_simulation(cfg, seed=0, temperature_eV=None, np2c=None, tol=1e-8, sort
     mask[idx] = 1
     phi_bc[idx] = val
     edge = np.zeros((n, m), bool)
-    edge[0, :] = edge[-1, :] = edge[:, 0] = edge[:, -1] = True
+    edge[-1, :] = edge[:, 0] = edge[:, -1] = True
+    if not rz:
+        edge[0, :] = True
     mask[edge.reshape(-1)] = 1
 
     names = [str(s["name"]) for s in cfg["species"]]
@@ -212,7 +213,7 @@ def build_simulation(cfg, seed=0, temperature_eV=None, np2c=None, tol=1e-8, sort
                    1.0 if np2c is None else float(np2c))
         species.append(dict(name=nm, charge=float(s["q"]), mass=float(s["m"]), np2c=p2c, capacity=cap))
     sim = PICSimulation(m, n, dx, dy, dt, species, mask, phi_bc, tol=tol, sort_interval=sort_interval, seed=seed,
-                        use_graph=use_graph, **kw)
+                        use_graph=use_graph, geometry="rz" if rz else "cartesian", **kw)
     rng = np.random.Generator(np.random.Philox(seed))
     per = {nm: [] for nm in names}
     for load in cfg["loads"]:
@@ -220,7 +221,12 @@ def build_simulation(cfg, seed=0, temperature_eV=None, np2c=None, tol=1e-8, sort
         s = species[names.index(nm)]
         k = int(load["n"])
         x = (rng.uniform(float(load["x1MinMKS"]), float(load["x1MaxMKS"]), k) - x0) / dx
-        y = (rng.uniform(float(load["x2MinMKS"]), float(load["x2MaxMKS"]), k) - y0) / dy
+        if rz:
+            # radii uniform in volume: r^2 uniform between the bounds (measured from the axis x2s)
+            r1, r2 = float(load["x2MinMKS"]) - y0, float(load["x2MaxMKS"]) - y0
+            y = np.sqrt(rng.uniform(r1 * r1, r2 * r2, k)) / dy
+        else:
+            y = (rng.uniform(float(load["x2MinMKS"]), float(load["x2MaxMKS"]), k) - y0) / dy
         T = load.get("temperature", temperature_eV)
         vth = math.sqrt(float(T) * Consts.qe / s["mass"]) if T is not None else 0.0
         v = rng.normal(0.0, vth, (3, k)) if vth > 0 else np.zeros((3, k))

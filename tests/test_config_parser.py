@@ -134,13 +134,11 @@ def test_grid_node_counts():
     assert not CP.multigrid_compatible(128) and not CP.multigrid_compatible(1000)
 
 
-def test_cylindrical_files_need_the_cartesian_override():
-    cfg = CP.ConfigParser().parse_text(TEXT.replace("Cylindrical = 0", "Cylindrical = 1"))
-    with pytest.raises(NotImplementedError):
-        CP.build_simulation(cfg)
-    cfg = CP.ConfigParser().parse_text(TEXT.replace("Jmax = 129", "Jmax = 128"))
-    with pytest.raises(ValueError):
-        CP.build_simulation(cfg)
+def test_node_counts_must_coarsen():
+    for text in (TEXT, TEXT.replace("Cylindrical = 0", "Cylindrical = 1")):
+        cfg = CP.ConfigParser().parse_text(text.replace("Jmax = 129", "Jmax = 128"))
+        with pytest.raises(ValueError):
+            CP.build_simulation(cfg)
 
 
 @pytest.mark.gpu
@@ -163,4 +161,31 @@ def test_build_run_and_dump(tmp_path):
     data = np.loadtxt(path)
     assert data.shape == (129 * 129, 6)
     np.testing.assert_allclose(data[:, 3], phi.reshape(-1), rtol=6e-3, atol=1e-30)
+    sim.close()
+
+
+@pytest.mark.gpu
+def test_cylindrical_file_runs_in_rz():
+    """Cylindrical = 1 (the reference's shipped input is cylindrical): the two
+    electrodes are disks on the axis; the axis row is free, particles stay at
+    r >= 0 and charge is conserved between the live particles, the walls and
+    the electrodes."""
+    cfg = CP.ConfigParser().parse_text(TEXT.replace("Cylindrical = 0", "Cylindrical = 1"))
+    sim = CP.build_simulation(cfg, seed=4)
+    assert sim.geometry == "rz"
+    sim.init()
+    sim.step(10)
+    sim.sync()
+    c = sim.counters()
+    live = sum(sim.diagnostics()["live"])
+    assert live + sum(c["absorbed"]) + sum(c["electrode_absorbed"]) == 100_000
+    assert sum(c["electrode_absorbed"]) > 0
+    for s in range(2):
+        x, y = (a.cpu().numpy() for a in sim.species_arrays(s)[:2])
+        yl = y[np.isfinite(x)]
+        assert yl.size and yl.min() >= 0.0 and yl.max() <= 128.0
+    phi = sim.fields()[0].cpu().numpy().reshape(129, 129)
+    # electrode nodes keep their potentials, the axis nodes between them are free
+    assert phi[0, 32] == -20.0 and phi[0, 96] == 20.0
+    assert -20.0 < phi[0, 64] < 20.0
     sim.close()
