@@ -1583,9 +1583,26 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
            ((nys.back() - 1) % 2 == 0)) {
         const int fx = nxs.back(), fy = nys.back();
         const int cx = (fx - 1) / 2 + 1, cy = (fy - 1) / 2 + 1;
+        const std::vector<uint8_t>& mf = masks.back();
+        // A coarse node is Dirichlet if the fine node it injects from is, or if
+        // an internal Dirichlet node (an electrode; not the grid edges, which
+        // are Dirichlet on every level) lies in its 3 x 3 fine neighbourhood:
+        // an electrode on an odd line would otherwise vanish from the coarse
+        // grid, whose correction then spans it, and the cycle can diverge.
+        auto inner = [&](int i, int j) {
+            return i > 0 && i < fx - 1 && j < fy - 1 && (j > 0 || M.rz) && mf[size_t(j) * fx + i] != 0;
+        };
         std::vector<uint8_t> mc(size_t(cx) * cy);
         for (int J = 0; J < cy; ++J)
-            for (int I = 0; I < cx; ++I) mc[size_t(J) * cx + I] = masks.back()[size_t(2 * J) * fx + 2 * I];
+            for (int I = 0; I < cx; ++I) {
+                uint8_t v = mf[size_t(2 * J) * fx + 2 * I];
+                for (int dj = -1; dj <= 1 && !v; ++dj)
+                    for (int di = -1; di <= 1 && !v; ++di) {
+                        const int i = 2 * I + di, j = 2 * J + dj;
+                        if (i >= 0 && j >= 0 && i < fx && j < fy && inner(i, j)) v = 1;
+                    }
+                mc[size_t(J) * cx + I] = v;
+            }
         nxs.push_back(cx);
         nys.push_back(cy);
         masks.push_back(std::move(mc));

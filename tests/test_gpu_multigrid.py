@@ -106,6 +106,36 @@ def test_internal_electrodes_match_direct_solve():
         np.testing.assert_allclose(phi.cpu().numpy(), ref, rtol=0, atol=1e-8 * np.abs(ref).max())
 
 
+@pytest.mark.parametrize("launch", ["graph", "persistent", "cluster"])
+def test_electrodes_on_odd_lines(launch):
+    """Electrodes on lines that do not survive injection to the coarse grids
+    (column 43 and row 77, both odd; column 85): the coarse grids keep them as
+    two-line bands, and the cycle converges to the direct solution (about 55
+    V-cycles to 1e-9; with the electrodes left out of the coarse grids it
+    diverged)."""
+    n = 129
+    h = 1.0 / (n - 1)
+    _, f, _ = manufactured(n)
+    cath = [43 + j * n for j in range(30, 91)]
+    anode = [85 + j * n for j in range(20, 70)]
+    bar = [i + 77 * n for i in range(50, 80)]
+    idx = np.array(sorted(set(cath + anode + bar)))
+    val = np.where(np.isin(idx, cath), -50.0, 50.0)
+    mask = edge_mask(n)
+    mask[idx] = 1
+    ref = direct_solve(n, h, idx, val, f)
+    for precision in ("mixed", "fp64"):
+        mg = MultigridSolver(mask, n, n, h, precision=precision, launch=launch)
+        phi0 = np.zeros(n * n)
+        phi0[idx] = val
+        ff = f.copy()
+        ff[mask == 1] = 0
+        phi, (cycles, rel) = mg.solve(torch.as_tensor(phi0, device=DEV), torch.as_tensor(ff, device=DEV), tol=1e-9,
+                                      max_cycles=100)
+        assert rel < 1e-9 and cycles <= 70, (precision, cycles, rel)
+        np.testing.assert_allclose(phi.cpu().numpy(), ref, rtol=0, atol=1e-8 * np.abs(ref).max())
+
+
 @pytest.mark.parametrize("n,tol", [(513, 1e-8), (513, 1e-10), (1025, 1e-10), (2049, 1e-10)])
 def test_residual_recomputed_on_cpu(n, tol):
     rng = np.random.Generator(np.random.Philox(6))

@@ -54,17 +54,18 @@ def test_exact_quadratic(launch, precision, shape):
     assert mg.effective_launch() in ("graph", "host")
     phi0 = np.where(mask == 1, exact, 0.0)
     phi = torch.as_tensor(phi0, device=DEV)
-    phi, (cycles, rel) = mg.solve(phi, torch.as_tensor(f, device=DEV), tol=1e-12, max_cycles=40)
-    assert rel < 1e-12 and cycles <= 20, (cycles, rel)
-    np.testing.assert_allclose(phi.cpu().numpy(), exact, rtol=0, atol=1e-9 * exact.max())
+    # phi ~ 0.1 against 1/h^2 = 1e6: the FP64 residual of this problem bottoms out near 2e-12
+    phi, (cycles, rel) = mg.solve(phi, torch.as_tensor(f, device=DEV), tol=1e-10, max_cycles=40)
+    assert rel < 1e-10 and cycles <= 16, (cycles, rel)
+    np.testing.assert_allclose(phi.cpu().numpy(), exact, rtol=0, atol=1e-8 * exact.max())
 
 
-def electrode_problem(m, n, h):
+def electrode_problem(m, n, h, cols=None):
     """Two disk electrodes on the axis at -10 V and +10 V, a Gaussian charge cloud."""
     j, i = np.divmod(np.arange(m * n), m)
     mask = rz_mask(m, n)
     phi_bc = np.zeros(m * n)
-    for col, v in ((m // 4, -10.0), (3 * m // 4, 10.0)):
+    for col, v in zip(cols or (m // 4, 3 * m // 4), (-10.0, 10.0)):
         sel = (i == col) & (j <= n // 2)
         mask[sel] = 1
         phi_bc[sel] = v
@@ -75,20 +76,24 @@ def electrode_problem(m, n, h):
     return mask, phi_bc, f
 
 
+@pytest.mark.parametrize("cols", [(32, 96), (43, 85)])
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
-def test_electrodes_against_direct_solve(precision):
+def test_electrodes_against_direct_solve(precision, cols):
+    """Electrodes on lines that coarsen exactly (32, 96) and on odd lines (43,
+    85), which the coarse grids keep as two-line bands (slower: about 35
+    cycles to 1e-10 instead of under 20)."""
     m, n, h = 129, 65, 2e-4
-    mask, phi_bc, f = electrode_problem(m, n, h)
+    mask, phi_bc, f = electrode_problem(m, n, h, cols)
     direct = O.rz_solve(f, phi_bc, mask, m, n, h, h)
     mg = MultigridSolver(mask, m, n, h, precision=precision, hy=h, geometry="rz")
     phi = torch.as_tensor(phi_bc.copy(), device=DEV)
-    phi, (cycles, rel) = mg.solve(phi, torch.as_tensor(f, device=DEV), tol=1e-11, max_cycles=40)
+    phi, (cycles, rel) = mg.solve(phi, torch.as_tensor(f, device=DEV), tol=1e-10, max_cycles=60)
     got = phi.cpu().numpy()
-    assert rel < 1e-11 and cycles <= 20, (cycles, rel)
+    assert rel < 1e-10 and cycles <= (20 if cols[0] % 2 == 0 else 45), (cycles, rel)
     np.testing.assert_allclose(got, direct, rtol=0, atol=1e-8 * np.abs(direct).max())
-    # the reported residual is the oracle's FP64 residual
+    # the reported residual is the oracle's FP64 residual (to 2 %, above the FP64 floor)
     cpu = O.rz_residual(got, f, mask, m, n, h, h)
-    assert abs(rel - cpu) <= 2e-2 * cpu + 1e-13, (rel, cpu)
+    assert abs(rel - cpu) <= 2e-2 * cpu + 1e-12, (rel, cpu)
     # the axis nodes between the electrodes are unknowns, not boundary values
     assert -10.0 < got[m // 2] < 10.0 and got[m // 2] != 0.0
 
