@@ -270,6 +270,9 @@ constexpr int kStages = 3;  // chunk buffers: one loading, one in work, one drai
 // the charge-tile flush).  The chunk after a non-final chunk is computed by
 // every thread; only the first chunk of a new unit is published through
 // shared memory, across the unit-end barrier.
+// RZ: r-z geometry (drift_rz); a separate instance, so that the Cartesian
+// pass carries none of it.
+template <bool RZ>
 __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
     extern __shared__ __align__(128) unsigned char smem[];
     float* bufs = reinterpret_cast<float*>(smem);  // [kStages][4][kBufStride]
@@ -342,7 +345,7 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
         const SpeciesConst C = A.sp[s];
         const unsigned* const cbits = (A.do_mcc && A.mcc->sp[s].nproc > 0) ? A.cbits[s] : nullptr;
         // r-z: the azimuthal velocity is not staged; it is read and written in place
-        float* const gvz = A.rz ? A.state[s].cur[4] + b : nullptr;
+        float* const gvz = RZ ? A.state[s].cur[4] + b : nullptr;
         unsigned my_abs = 0, my_cand = 0, my_elec = 0;
 #pragma unroll
         for (int k = 0; k < kPushP; ++k) {
@@ -387,7 +390,7 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
             }
             if (A.do_drift) {
                 const float x0 = x, y0 = y;
-                if (gvz) {
+                if constexpr (RZ) {
                     float vz = gvz[l];
                     drift_rz(x, y, vx, vy, vz, C.dtdx, C.dtdy);
                     gvz[l] = vz;
@@ -843,7 +846,8 @@ static int particle_pass(SimImpl& S, cudaStream_t st, int kick, int mcc, int dri
                                                                      S.d_nseg);
             S.launches += 1;
         }
-        k_push<<<S.push_grid, kPushThreads, S.push_smem, st>>>(A);
+        if (S.rz) k_push<true><<<S.push_grid, kPushThreads, S.push_smem, st>>>(A);
+        else k_push<false><<<S.push_grid, kPushThreads, S.push_smem, st>>>(A);
     }
     {
         PhaseTimer t(S, PIC_PHASE_MERGE, st);
@@ -1099,9 +1103,10 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
     // launch shape of the particle pass
     S.push_smem =
         sizeof(float) * kStages * 4 * kBufStride + size_t(S.rw) * S.rw * (sizeof(float2) + sizeof(unsigned));
-    PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(k_push), S.push_smem));
+    const void* push_fn = S.rz ? reinterpret_cast<const void*>(k_push<true>) : reinterpret_cast<const void*>(k_push<false>);
+    PIC_TRY(raise_smem_limit(push_fn, S.push_smem));
     int per_sm = 0;
-    PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_push, kPushThreads, S.push_smem));
+    PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_fn, kPushThreads, S.push_smem));
     S.push_grid = std::max(1, per_sm) * num_sms();
     PIC_CUDA(cudaStreamCreateWithFlags(&S.cap, cudaStreamNonBlocking));
     (void)st;
