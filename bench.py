@@ -55,13 +55,15 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-collisionless", action="store_true")
+    ap.add_argument("--no-dst", action="store_true", help="skip the step timed with the sine-transform solve")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-graph", action="store_true", help="launch every kernel from the host (profilers)")
     ap.add_argument("--mg-sweeps", type=int, nargs=2, default=(2, 2), metavar=("PRE", "POST"),
                     help="red-black sweeps before and after each coarse-grid correction")
     ap.add_argument("--omega", type=float, default=1.15, help="smoother over-relaxation")
-    ap.add_argument("--mg-launch", default="graph", choices=["persistent", "host", "graph", "cluster"],
-                    help="multigrid launch mode (host: one launch per kernel, for profilers)")
+    ap.add_argument("--mg-launch", default="graph", choices=["persistent", "host", "graph", "cluster", "dst"],
+                    help="multigrid launch mode (host: one launch per kernel, for profilers; dst: the "
+                         "sine-transform solve in place of the V-cycles)")
     ap.add_argument("--ensemble", type=int, default=0,
                     help="also time an ensemble of this many independent collisionless members (0: off)")
     ap.add_argument("--ensemble-steps", type=int, default=100)
@@ -157,7 +159,7 @@ def ncu_traffic():
 GRAPH_OPTS = {"use_graph": True, "mg_launch": "graph"}
 
 
-def make_sim(w, rank, sort_interval, mcc=True):
+def make_sim(w, rank, sort_interval, mcc=True, **over):
     from pic_b200 import Consts, workloads
     from pic_b200.simulation import PICSimulation
 
@@ -166,8 +168,9 @@ def make_sim(w, rank, sort_interval, mcc=True):
                dict(name="i", charge=Consts.qe, mass=workloads.ION_MASS, np2c=w.np2c(w.n_i),
                     capacity=int(w.n_i * 1.25))]
     tables = workloads.mcc_tables(w) if mcc else None
+    opts = dict(GRAPH_OPTS, **over)
     return PICSimulation(w.nodes, w.nodes, w.dx, w.dx, w.dt, species, mask, phi_bc, tol=w.tol, max_cycles=50,
-                         sort_interval=sort_interval, mcc=tables, seed=1000 + rank, **GRAPH_OPTS)
+                         sort_interval=sort_interval, mcc=tables, seed=1000 + rank, **opts)
 
 
 def gen_arrays(w, rank):
@@ -303,6 +306,28 @@ def run_ours(args, world, rank, local):
                                 "push_frac_of_peak": round((0.5 * (m0 + m1) * BYTES_PER_PARTICLE + G * BYTES_PER_NODE)
                                                            / (p2 / 1e3) / 1e9 / peak, 4),
                                 "mg_cycles_per_step": prof2["mg_cycles"] / args.steps}
+        sim.close()
+        del sim
+        torch.cuda.empty_cache()
+
+    if not args.no_dst and args.mg_launch != "dst":
+        # the same workload with the field solved by sine transforms (the
+        # reference's FFT path, src/FFT.py:10-64): exact to FP64 round-off,
+        # no V-cycles; the headline stays on the multigrid
+        sim = make_sim(w, rank, args.sort_interval, mcc=True, mg_launch="dst")
+        for s, a in enumerate(arrays):
+            sim.load(s, *a)
+        sim.init()
+        sim.step(args.warmup)
+        ms3, prof3, _, m0, m1 = time_steps(sim, args.steps, world)
+        t3 = torch.tensor([ms3], device="cuda", dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(t3, op=dist.ReduceOp.MAX)
+        out["dst_solve"] = {"value": world * 0.5 * (m0 + m1) * args.steps / (float(t3.item()) / 1e3),
+                            "ms_per_step": float(t3.item()) / args.steps,
+                            "solve_ms_per_step": round(prof3["solve"]["ms"] / args.steps, 4),
+                            "rel_res": sim.counters()["last_rel_res"],
+                            "solver": sim.mg_effective_launch()}
         sim.close()
         del sim
         torch.cuda.empty_cache()

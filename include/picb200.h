@@ -128,8 +128,12 @@ typedef enum pic_mg_launch_mode {
     PIC_MG_PERSISTENT = 0, /* one cooperative kernel per solve; phases separated by grid barriers */
     PIC_MG_HOST_LOOP = 1,  /* one launch per kernel, convergence tested on the host each cycle */
     PIC_MG_GRAPH_LOOP = 2, /* one launch per kernel inside a CUDA-graph conditional WHILE node */
-    PIC_MG_CLUSTER = 3     /* one launch of a single thread-block cluster per solve (FP32 levels whose
+    PIC_MG_CLUSTER = 3,    /* one launch of a single thread-block cluster per solve (FP32 levels whose
                               row bands fit in shared memory; otherwise the graph loop) */
+    PIC_MG_DST = 4         /* no V-cycles: the direct solve by sine transforms of src/FFT.py:10-64
+                              (FP64, three kernels, then the FP64 residual for pic_mg_info), for
+                              Cartesian grids of 2^q + 1 nodes (q <= 11) whose Dirichlet nodes are
+                              exactly the four edges; otherwise the graph loop */
 } pic_mg_launch_mode;
 
 /* Geometry of the grid.  PIC_GEOM_RZ is axisymmetric r-z (the reference's
@@ -378,6 +382,9 @@ typedef struct pic_sim_diag {
     double div_error_l2;                    /* V/m^2: || div E - rho/eps0 || over the nodes */
 } pic_sim_diag;
 int pic_sim_diagnostics(pic_sim* sim, pic_sim_diag* out, void* stream);
+/* The launch mode its Poisson solves use (pic_mg_effective_launch_mode of
+ * the simulation's solver: PIC_MG_DST or the graph loop it falls back to). */
+int pic_sim_solver_mode(pic_sim* sim, int* mode);
 /* Kernel launches issued by this object since creation (all phases). */
 long long pic_sim_kernel_launches(pic_sim* sim);
 

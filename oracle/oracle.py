@@ -340,6 +340,31 @@ def ref_cylindrical_laplacian(m, n, dz, dr):
     return A
 
 
+def poisson_fft_dirichlet(f, g, dx):
+    """The reference's poisson_fft_dirichlet (src/FFT.py:10-64) restated in
+    numpy/scipy: lap(phi) = f on a square-celled grid, phi = g on the four
+    edges.  The edge values enter through f - lap(phi_g) (phi_g = g on the
+    edges, 0 inside), the interior is solved with orthonormal DST-I in both
+    directions and the 5-point eigenvalues.  f, g: 2D arrays [rows, columns]."""
+    from scipy.fft import dstn, idstn
+
+    f = np.asarray(f, np.float64)
+    g = np.asarray(g, np.float64)
+    phi_g = np.zeros_like(f)
+    phi_g[0, :], phi_g[-1, :], phi_g[:, 0], phi_g[:, -1] = g[0, :], g[-1, :], g[:, 0], g[:, -1]
+    lap = np.zeros_like(f)
+    lap[1:-1, 1:-1] = (-4 * phi_g[1:-1, 1:-1] + phi_g[2:, 1:-1] + phi_g[:-2, 1:-1] + phi_g[1:-1, 2:]
+                       + phi_g[1:-1, :-2]) / dx ** 2
+    f_hat = dstn((f - lap)[1:-1, 1:-1], type=1, norm="ortho")
+    nx, ny = f_hat.shape
+    i = np.arange(1, nx + 1).reshape(-1, 1)
+    j = np.arange(1, ny + 1).reshape(1, -1)
+    denom = (2 * (np.cos(np.pi * i / (nx + 1)) - 1) + 2 * (np.cos(np.pi * j / (ny + 1)) - 1)) / dx ** 2
+    phi = phi_g.copy()
+    phi[1:-1, 1:-1] += idstn(f_hat / denom, type=1, norm="ortho")
+    return phi
+
+
 def residual_f64(phi, f, dirichlet, m, n, dx, dy, want_r=False):
     r = np.zeros(m * n) if want_r else None
     s = lib().or_residual_f64(np.ascontiguousarray(phi, np.float64), np.ascontiguousarray(f, np.float64),

@@ -40,8 +40,9 @@ PIC_MG_PERSISTENT = 0
 PIC_MG_HOST_LOOP = 1
 PIC_MG_GRAPH_LOOP = 2
 PIC_MG_CLUSTER = 3
+PIC_MG_DST = 4
 MG_LAUNCH_MODES = {"persistent": PIC_MG_PERSISTENT, "host": PIC_MG_HOST_LOOP, "graph": PIC_MG_GRAPH_LOOP,
-                   "cluster": PIC_MG_CLUSTER}
+                   "cluster": PIC_MG_CLUSTER, "dst": PIC_MG_DST}
 
 PIC_ELASTIC = 0
 PIC_EXCITATION = 1
@@ -141,6 +142,7 @@ SIGNATURES = {
     "pic_update_E": [_vp, _vp, _vp, _i, _i, _d, _d, _vp],
     "pic_form_rhs": [_vp, _vp, _d, _vp, _i, _i, _vp],
     "pic_update_E_rz": [_vp, _vp, _vp, _i, _i, _d, _d, _vp],
+    "pic_sim_solver_mode": [_vp, C.POINTER(_i)],
     "pic_rz_density": [_vp, _i, _i, _d, _vp],
     "pic_update_R_rz": [_vp, _vp, _vp, _vp, _vp, _i, _f, _f, _vp],
     "pic_mg_create": [_i, _i, _d, _d, _vp, C.POINTER(MgOptions), C.POINTER(_vp)],

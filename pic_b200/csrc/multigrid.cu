@@ -1218,12 +1218,18 @@ struct CoarseLayout {
     uint4* mimg = nullptr;
 };
 
+struct DstPlan;
+int dst_create(int nx, int ny, double dx, double dy, DstPlan** out);
+void dst_destroy(DstPlan* P);
+int dst_launch(DstPlan* P, double* phi, const double* f, cudaStream_t st);
+
 struct MgImpl {
     int precision = PIC_MG_MIXED;
     int nx = 0, ny = 0, L = 0, Lc = 0;
     double dx = 0, dy = 0;
     bool rz = false;          // r-z geometry (PIC_GEOM_RZ)
     double* rz0 = nullptr;    // level-0 row coefficients in FP64 (r-z)
+    DstPlan* dst = nullptr;   // PIC_MG_DST: the sine-transform solve
     pic_mg_options o{};
     std::vector<LevelDev<float>> lf;
     std::vector<LevelDev<double>> ld;
@@ -1530,6 +1536,7 @@ static void mg_release(pic_mg* mg) {
     if (M.exec) cudaGraphExecDestroy(M.exec);
     if (M.side) cudaStreamDestroy(M.side);
     if (M.cap) cudaStreamDestroy(M.cap);
+    if (M.dst) dst_destroy(M.dst);
     for (void* p : M.allocs) cudaFree(p);
     delete mg;
 }
@@ -1562,7 +1569,7 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
         return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: unknown precision %d", M.o.precision));
     if (M.o.pre_sweeps > kMgMaxSweeps || M.o.post_sweeps > kMgMaxSweeps)
         return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: at most 8 pre/post sweeps"));
-    if (M.o.launch_mode < PIC_MG_PERSISTENT || M.o.launch_mode > PIC_MG_CLUSTER)
+    if (M.o.launch_mode < PIC_MG_PERSISTENT || M.o.launch_mode > PIC_MG_DST)
         return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: unknown launch mode %d", M.o.launch_mode));
     if (M.o.geometry != PIC_GEOM_CARTESIAN && M.o.geometry != PIC_GEOM_RZ)
         return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: unknown geometry %d", M.o.geometry));
@@ -1671,6 +1678,21 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
                                          : alloc_levels(M, M.ld, masks, nxs, nys);
     if (st == PIC_OK) st = M.precision == PIC_MG_MIXED ? configure_kernels<float>(M) : configure_kernels<double>(M);
     if (st == PIC_OK && M.o.launch_mode == PIC_MG_CLUSTER) st = configure_cluster(M, nxs, nys);
+    if (st == PIC_OK && M.o.launch_mode == PIC_MG_DST) {
+        // the sine-transform solve applies to Cartesian grids of 2^q + 1 nodes
+        // whose Dirichlet nodes are the edges alone; otherwise the graph loop
+        bool edges_only = !M.rz;
+        for (int j = 1; j < ny - 1 && edges_only; ++j)
+            for (int i = 1; i < nx - 1; ++i)
+                if (masks[0][size_t(j) * nx + i]) {
+                    edges_only = false;
+                    break;
+                }
+        const bool pow2 = nx - 1 >= 4 && ny - 1 >= 4 && nx - 1 <= 2048 && ny - 1 <= 2048 &&
+                          ((nx - 1) & (nx - 2)) == 0 && ((ny - 1) & (ny - 2)) == 0;
+        if (edges_only && pow2) st = dst_create(nx, ny, dx, dy, &M.dst);
+        if (st == PIC_OK && !M.dst) M.o.launch_mode = PIC_MG_GRAPH_LOOP;
+    }
     if (st != PIC_OK) return bail(st);
     M.grd0 = dim3(div_up(nx, M.blk0.x), div_up(ny, M.blk0.y * kR0Rows));
     // block partials of the residual norm: one pair per block of the level-0
@@ -1849,7 +1871,17 @@ static int launch_cluster(MgImpl& M, double* phi, const double* f, double tol, i
 
 // Appends the whole solve to a capture in progress on `st`: the persistent or
 // cluster kernel, or the residual and a WHILE node over V-cycles.
+// The sine-transform solve, then the FP64 residual and its norms for pic_mg_info.
+static int launch_dst(MgImpl& M, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
+    PIC_TRY(dst_launch(M.dst, phi, f, st));
+    if (M.precision == PIC_MG_MIXED) launch_r0(M, M.lf, phi, f, tol, max_cycles, 1, cudaGraphConditionalHandle{}, 0, st);
+    else launch_r0(M, M.ld, phi, f, tol, max_cycles, 1, cudaGraphConditionalHandle{}, 0, st);
+    PIC_LAUNCH_CHECK();
+    return PIC_OK;
+}
+
 int mg_capture(MgImpl& M, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
+    if (M.dst) return launch_dst(M, phi, f, tol, max_cycles, st);
     if (M.o.launch_mode == PIC_MG_CLUSTER && M.cluster_ok) return launch_cluster(M, phi, f, tol, max_cycles, st);
     if (M.o.launch_mode == PIC_MG_PERSISTENT)
         return M.precision == PIC_MG_MIXED ? launch_persistent(M, M.lf, phi, f, tol, max_cycles, st)
@@ -1935,6 +1967,7 @@ static int solve_eager(MgImpl& M, std::vector<LevelDev<T>>& lv, double* phi, con
 }
 
 int mg_launch(MgImpl& M, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
+    if (M.dst) return launch_dst(M, phi, f, tol, max_cycles, st);
     if (M.o.launch_mode == PIC_MG_CLUSTER && M.cluster_ok) return launch_cluster(M, phi, f, tol, max_cycles, st);
     if (M.o.launch_mode == PIC_MG_PERSISTENT)
         return M.precision == PIC_MG_MIXED ? launch_persistent(M, M.lf, phi, f, tol, max_cycles, st)
@@ -1954,7 +1987,7 @@ int mg_solve(MgImpl& M, double* phi, const double* f, double tol, int max_cycles
     pic_mg_info loc{};
     PIC_TRY(mg_read_info(M, &loc));
     const bool one_kernel = M.o.launch_mode == PIC_MG_PERSISTENT || (M.o.launch_mode == PIC_MG_CLUSTER && M.cluster_ok);
-    M.launches += 1 + (one_kernel ? 0 : (long long)(loc.cycles) * M.body_launches);
+    M.launches += M.dst ? 4 : 1 + (one_kernel ? 0 : (long long)(loc.cycles) * M.body_launches);
     if (info) *info = loc;
     if (!loc.converged)
         return fail(PIC_ERR_NOT_CONVERGED, "multigrid: relative residual %.3e after %d cycles (tol %.1e)", loc.rel_res,
@@ -1966,9 +1999,13 @@ long long mg_launches(pic_mg* mg) { return mg ? mg->m.launches : 0; }
 int mg_body_launches(pic_mg* mg) {
     if (!mg) return 0;
     const MgImpl& M = mg->m;
-    const bool one_kernel = M.o.launch_mode == PIC_MG_PERSISTENT || (M.o.launch_mode == PIC_MG_CLUSTER && M.cluster_ok);
+    const bool one_kernel = M.dst || M.o.launch_mode == PIC_MG_PERSISTENT ||
+                            (M.o.launch_mode == PIC_MG_CLUSTER && M.cluster_ok);
     return one_kernel ? 0 : M.body_launches;
 }
+// Kernels a solve runs besides its V-cycles: the residual, or the three
+// sine-transform kernels and the residual.
+int mg_fixed_launches(pic_mg* mg) { return mg && mg->m.dst ? 4 : 1; }
 int mg_capture_into(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
     return mg_capture(mg->m, phi, f, tol, max_cycles, st);
 }
@@ -1996,6 +2033,7 @@ int pic_mg_effective_launch_mode(pic_mg* mg, int* mode) {
     if (!mg || !mode) return fail(PIC_ERR_BAD_ARG, "pic_mg_effective_launch_mode: bad arguments");
     const MgImpl& M = mg->m;
     *mode = (M.o.launch_mode == PIC_MG_CLUSTER && !M.cluster_ok) ? int(PIC_MG_GRAPH_LOOP) : M.o.launch_mode;
+    if (M.dst) *mode = PIC_MG_DST;
     return PIC_OK;
 }
 

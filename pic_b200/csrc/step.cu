@@ -35,6 +35,7 @@ int launch_form_rhs(const float* rho, const uint8_t* dirichlet, double eps0, dou
                     double* phi, double* phi_prev, long G, cudaStream_t st, const double* rowf, int nx);
 int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const pic_mg_options* opts, pic_mg** out);
 int mg_body_launches(pic_mg* mg);
+int mg_fixed_launches(pic_mg* mg);
 long long mg_total_cycles(pic_mg* mg);
 int mg_capture_into(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st);
 int mg_launch_graph(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st);
@@ -1488,12 +1489,18 @@ int pic_sim_read_counters(pic_sim* sim, pic_sim_counters* out, void* stream) {
     return PIC_OK;
 }
 
+int pic_sim_solver_mode(pic_sim* sim, int* mode) {
+    clear_error();
+    if (!sim || !mode) return fail(PIC_ERR_BAD_ARG, "pic_sim_solver_mode: bad arguments");
+    return pic_mg_effective_launch_mode(sim->s.mg, mode);
+}
+
 long long pic_sim_kernel_launches(pic_sim* sim) {
     if (!sim) return 0;
     SimImpl& S = sim->s;
     cudaDeviceSynchronize();
     // each solve runs its residual kernel plus `body` kernels per V-cycle
-    return S.launches + S.solves + mg_total_cycles(S.mg) * mg_body_launches(S.mg);
+    return S.launches + S.solves * mg_fixed_launches(S.mg) + mg_total_cycles(S.mg) * mg_body_launches(S.mg);
 }
 
 int pic_sim_set_profiling(pic_sim* sim, int enable) {

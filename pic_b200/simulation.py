@@ -162,6 +162,12 @@ class PICSimulation:
             "electrode_absorbed": [c.electrode_absorbed[s] for s in range(ns)],
         }
 
+    def mg_effective_launch(self) -> str:
+        """The launch mode of the field solves ("dst" where the sine-transform solve applies)."""
+        m = C.c_int()
+        _lib.call("pic_sim_solver_mode", self._h, C.byref(m))
+        return {v: k for k, v in _lib.MG_LAUNCH_MODES.items()}[m.value]
+
     def diagnostics(self) -> dict:
         """Kinetic energy and momentum per species, field energy and Gauss's law
         terms of the current state (pic_sim_diagnostics)."""
