@@ -382,6 +382,16 @@ typedef struct pic_sim_diag {
     double div_error_l2;                    /* V/m^2: || div E - rho/eps0 || over the nodes */
 } pic_sim_diag;
 int pic_sim_diagnostics(pic_sim* sim, pic_sim_diag* out, void* stream);
+/* The particle vertex buffer of the reference's renderer (Renderer.update_particles,
+ * src/Render.py:544-571, an OpenGL VBO written through CUDA interop) as a
+ * headless device buffer: d_out[capacity][3] float32 receives, for every live
+ * particle in species order and slot order, 2 (x - x_min)/(x_max - x_min) - 1,
+ * the same for y (positions in metres), and the species' type (index + 1).
+ * Dead slots are skipped by a stable compaction.  *count (host) receives the
+ * live particles; PIC_ERR_OUT_OF_CAPACITY if they exceed capacity (the
+ * first `capacity` are written).  Synchronises `stream`. */
+int pic_sim_particle_buffer(pic_sim* sim, float* d_out, int capacity, double x_min, double x_max, double y_min,
+                            double y_max, int* count, void* stream);
 /* The launch mode its Poisson solves use (pic_mg_effective_launch_mode of
  * the simulation's solver: PIC_MG_DST or the graph loop it falls back to). */
 int pic_sim_solver_mode(pic_sim* sim, int* mode);

@@ -696,6 +696,103 @@ __global__ void k_untile_all(SpeciesState* state, int nspecies, int* n_tiled) {
 
 // ---- host object -----------------------------------------------------------------
 
+// ---- headless particle buffer ---------------------------------------------------------
+//
+// The particle vertex buffer of the reference's renderer (src/Render.py:544-571,
+// an OpenGL VBO filled through CUDA interop) as a plain device buffer: for every
+// live particle, in species order and slot order, (x, y) normalised to [-1, 1]
+// over [x_min, x_max] x [y_min, y_max] and the species' type (index + 1), as
+// float32 triples.  Dead slots are dropped by a stable compaction: per 1024-slot
+// block a live count, one exclusive scan over all blocks, then each block writes
+// its live particles at its offset plus their rank among the block's live slots.
+
+constexpr int kRenderBlock = 1024;
+
+struct RenderArgs {
+    const SpeciesState* state;
+    int ns;
+    int first_block[PIC_MAX_SPECIES + 1];  // blocks of species s: [first_block[s], first_block[s+1])
+    int* counts;                           // [blocks + 1]: live slots per block, then exclusive offsets
+    float* out;                            // [capacity][3]
+    int capacity;
+    double dx, dy, x0, y0, wx, wy;         // x_ndc = 2 (x dx - x0) / wx - 1 (the reference's order)
+};
+
+__device__ __forceinline__ int render_species(const RenderArgs& R, int blk) {
+    int s = 0;
+    while (s + 1 < R.ns && blk >= R.first_block[s + 1]) ++s;
+    return s;
+}
+
+__global__ void __launch_bounds__(kRenderBlock) k_render_count(RenderArgs R) {
+    const int s = render_species(R, blockIdx.x);
+    const SpeciesState& S = R.state[s];
+    const int slot = (blockIdx.x - R.first_block[s]) * kRenderBlock + threadIdx.x;
+    const bool live = slot < S.count && is_live(S.cur[0][slot]);
+    const int n = __syncthreads_count(live);
+    if (threadIdx.x == 0) R.counts[blockIdx.x] = n;
+}
+
+// One block: exclusive offsets of the block counts in place, the total in counts[nb].
+__global__ void __launch_bounds__(1024) k_render_scan(int* counts, int nb) {
+    __shared__ int warp_tot[32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int base = 0; base < nb; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const int v = i < nb ? counts[i] : 0;
+        int x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_tot[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            int t = warp_tot[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, t, o);
+                if (lane >= o) t += y;
+            }
+            warp_tot[lane] = t;  // inclusive over warps
+        }
+        __syncthreads();
+        const int before = carry + (w ? warp_tot[w - 1] : 0) + x - v;
+        if (i < nb) counts[i] = before;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += warp_tot[31];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) counts[nb] = carry;
+}
+
+__global__ void __launch_bounds__(kRenderBlock) k_render_emit(RenderArgs R) {
+    __shared__ int warp_n[kRenderBlock / 32];
+    const int s = render_species(R, blockIdx.x);
+    const SpeciesState& S = R.state[s];
+    const int slot = (blockIdx.x - R.first_block[s]) * kRenderBlock + threadIdx.x;
+    const float x = slot < S.count ? S.cur[0][slot] : __int_as_float(0x7fc00000);
+    const bool live = is_live(x);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned bal = __ballot_sync(0xffffffffu, live);
+    if (lane == 0) warp_n[w] = __popc(bal);
+    __syncthreads();
+    int off = R.counts[blockIdx.x];
+    for (int q = 0; q < w; ++q) off += warp_n[q];
+    off += __popc(bal & ((1u << lane) - 1u));
+    if (live && off < R.capacity) {
+        const float y = S.cur[1][slot];
+        float* o = R.out + 3L * off;
+        o[0] = float(2.0 * (double(x) * R.dx - R.x0) / R.wx - 1.0);
+        o[1] = float(2.0 * (double(y) * R.dy - R.y0) / R.wy - 1.0);
+        o[2] = float(s + 1);
+    }
+}
+
 struct SimImpl {
     pic_sim_desc d{};
     int nx = 0, ny = 0, ns = 0;
@@ -709,6 +806,8 @@ struct SimImpl {
     unsigned* cbits[PIC_MAX_SPECIES]{};  // candidate bit per slot of each colliding species
     unsigned *vbits = nullptr, *hbits = nullptr;  // internal electrode edges
     double* diag = nullptr;                        // diagnostics scratch
+    int* render_counts = nullptr;                  // particle-buffer block counts (render_blocks + 1)
+    int render_blocks = 0;
     bool electrodes = false;
     bool rz = false;                               // r-z geometry (desc.mg.geometry)
     double* rowf = nullptr;  // r-z: per row dx*dy / V_j, deposit -> charge density (null: Cartesian)
@@ -1486,6 +1585,48 @@ int pic_sim_read_counters(pic_sim* sim, pic_sim_counters* out, void* stream) {
     out->last_cycles = S.last.cycles;
     out->last_rel_res = S.last.rel_res;
     out->steps = S.steps;
+    return PIC_OK;
+}
+
+int pic_sim_particle_buffer(pic_sim* sim, float* d_out, int capacity, double x_min, double x_max, double y_min,
+                            double y_max, int* count, void* stream) {
+    clear_error();
+    if (!sim || !count || capacity < 0 || (capacity > 0 && !d_out) || !(x_max > x_min) || !(y_max > y_min))
+        return fail(PIC_ERR_BAD_ARG, "pic_sim_particle_buffer: bad arguments");
+    SimImpl& S = sim->s;
+    cudaStream_t st = as_stream(stream);
+    RenderArgs R{};
+    R.state = S.d_state;
+    R.ns = S.ns;
+    int nb = 0;
+    for (int s = 0; s < S.ns; ++s) {
+        R.first_block[s] = nb;
+        nb += div_up(S.d.species[s].capacity, kRenderBlock);
+    }
+    R.first_block[S.ns] = nb;
+    if (!S.render_counts) {
+        PIC_TRY(dalloc(S, &S.render_counts, size_t(nb) + 1));
+        S.render_blocks = nb;
+    }
+    R.counts = S.render_counts;
+    R.out = d_out;
+    R.capacity = capacity;
+    R.dx = S.d.dx;
+    R.dy = S.d.dy;
+    R.x0 = x_min;
+    R.y0 = y_min;
+    R.wx = x_max - x_min;
+    R.wy = y_max - y_min;
+    k_render_count<<<nb, kRenderBlock, 0, st>>>(R);
+    k_render_scan<<<1, 1024, 0, st>>>(S.render_counts, nb);
+    k_render_emit<<<nb, kRenderBlock, 0, st>>>(R);
+    PIC_LAUNCH_CHECK();
+    PIC_CUDA(cudaMemcpyAsync(count, S.render_counts + nb, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PIC_CUDA(cudaStreamSynchronize(st));
+    S.launches += 3;
+    if (*count > capacity)
+        return fail(PIC_ERR_OUT_OF_CAPACITY, "pic_sim_particle_buffer: %d live particles, buffer holds %d", *count,
+                    capacity);
     return PIC_OK;
 }
 

@@ -162,6 +162,21 @@ class PICSimulation:
             "electrode_absorbed": [c.electrode_absorbed[s] for s in range(ns)],
         }
 
+    def particle_buffer(self, x_range=None, y_range=None, out=None):
+        """The renderer's particle vertex buffer (src/Render.py:544-571) as a
+        device tensor (n, 3) float32: positions normalised to [-1, 1] over the
+        ranges in metres (default: the grid), and the species type (index + 1),
+        live particles in species order.  `out` (capacity, 3) is reused when given."""
+        xr = x_range or (0.0, self.dx * (self.nx - 1))
+        yr = y_range or (0.0, self.dy * (self.ny - 1))
+        if out is None:
+            cap = sum(int(s["capacity"]) for s in self.species)
+            out = torch.empty((cap, 3), dtype=torch.float32, device="cuda")
+        n = C.c_int()
+        _lib.call("pic_sim_particle_buffer", self._h, out.data_ptr(), out.shape[0], float(xr[0]), float(xr[1]),
+                  float(yr[0]), float(yr[1]), C.byref(n), _lib.stream_ptr())
+        return out[: n.value]
+
     def mg_effective_launch(self) -> str:
         """The launch mode of the field solves ("dst" where the sine-transform solve applies)."""
         m = C.c_int()

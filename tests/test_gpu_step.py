@@ -288,3 +288,32 @@ def test_diagnostics_match_numpy():
     dey[-1, :] = (E[1][-1, :] - E[1][-2, :]) / dy
     err = np.sqrt(np.sum((dex + dey - rho.reshape(m, m) / Consts.eps0) ** 2))
     assert d["div_error_l2"] == pytest.approx(err, rel=1e-9)
+
+
+def test_particle_buffer_matches_numpy():
+    """The headless particle vertex buffer (the renderer's VBO, src/Render.py:544-571):
+    live particles in species order, normalised positions and species types,
+    bit-exact against numpy with the same FP64 arithmetic, after absorption has
+    left dead slots; a buffer that is too small raises."""
+    w = workloads.scaled(workloads.SMALL, n=50_000, left_V=80.0)
+    sim, _, _, _ = make_sim(w, 0)
+    sim.init()
+    sim.step(30)
+    sim.sync()
+    assert sum(sim.counters()["absorbed"]) > 0
+    xr, yr = (0.001, 0.011), (-0.002, 0.0128)
+    got = sim.particle_buffer(xr, yr).cpu().numpy()
+    want = []
+    for s in range(2):
+        x, y = (t.cpu().numpy().astype(np.float64) for t in sim.species_arrays(s)[:2])
+        live = np.isfinite(x)
+        xm, ym = x[live] * w.dx, y[live] * w.dx
+        want.append(np.stack([2.0 * (xm - xr[0]) / (xr[1] - xr[0]) - 1.0, 2.0 * (ym - yr[0]) / (yr[1] - yr[0]) - 1.0,
+                              np.full(xm.size, s + 1.0)], 1).astype(np.float32))
+    want = np.concatenate(want)
+    assert got.shape == want.shape
+    np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+    small = torch.empty((10, 3), dtype=torch.float32, device="cuda")
+    with pytest.raises(Exception):
+        sim.particle_buffer(xr, yr, out=small)
+    sim.close()
