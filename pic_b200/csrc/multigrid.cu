@@ -111,6 +111,15 @@ struct CoarseDesc {
 // multiply-shift, and every global load of a phase is issued before the first
 // one is used.
 
+// Programmatic dependent launch: the V-cycle is a chain of small dependent
+// kernels, launched with cudaLaunchAttributeProgrammaticStreamSerialization so
+// that each one is scheduled while its predecessor drains.  pdl_wait blocks
+// until the preceding grid has completed and its memory is visible (a no-op
+// for a launch without the attribute); pdl_trigger, after a CTA's last store,
+// lets the next grid launch.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 template <int S>
 struct DownGeom {
     static constexpr int H = 2 * S + 2, W = kMgTile + 2 * H;
@@ -263,7 +272,9 @@ __device__ void down_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, 
 template <class T, int S, bool CYL>
 __global__ void __launch_bounds__(kMgThreads) k_mg_down(LevelDev<T> F, LevelDev<T> Cc, T omega) {
     extern __shared__ __align__(16) unsigned char smem[];
+    pdl_wait();
     down_tile<T, S, CYL>(F, Cc, omega, blockIdx.x, blockIdx.y, smem);
+    pdl_trigger();
 }
 
 template <class T, int S, bool CYL = false>
@@ -347,7 +358,9 @@ template <class T, int S, bool CYL>
 __global__ void __launch_bounds__(kMgThreads) k_mg_up(LevelDev<T> F, LevelDev<T> Cc, T omega,
                                                       double* __restrict__ phi) {
     extern __shared__ __align__(16) unsigned char smem[];
+    pdl_wait();
     up_tile<T, S, CYL>(F, Cc, omega, phi, blockIdx.x, blockIdx.y, smem);
+    pdl_trigger();
 }
 
 // Runtime sweep counts (the persistent kernel) dispatched to the instances.
@@ -590,7 +603,9 @@ __device__ void coarse_vcycle(const CoarseDesc<T>& D, unsigned char* smem) {
 template <class T, bool CYL>
 __global__ void __launch_bounds__(kCoarseThreads) k_mg_coarse(CoarseDesc<T> D) {
     extern __shared__ __align__(16) unsigned char smem[];
+    pdl_wait();
     coarse_vcycle<T, CYL>(D, smem);
+    pdl_trigger();
 }
 
 // ---- FP64 residual, norms and the loop decision -----------------------------------
@@ -616,6 +631,7 @@ __global__ void __launch_bounds__(256) k_mg_r0(const double* __restrict__ phi, c
                                                const double* __restrict__ rz0) {
     // a 32 x 8 block covers 32 x 32 nodes, four rows per thread, every load
     // of a thread issued before the first is used
+    pdl_wait();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double r = 0.0, fv = 0.0;
     double pc[kR0Rows], pw[kR0Rows], pe[kR0Rows], ps[kR0Rows], pn[kR0Rows], pf[kR0Rows];
@@ -1719,17 +1735,36 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
     return PIC_OK;
 }
 
+// A launch that may start while the preceding kernel on the stream drains
+// (the kernel waits in pdl_wait before reading what that kernel wrote).
+template <class... KArgs, class... Args>
+static cudaError_t launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 // The FP64 residual and the loop decision (k_mg_r0) of either geometry.
 template <class T>
 static void launch_r0(MgImpl& M, const std::vector<LevelDev<T>>& lv, double* phi, const double* f, double tol,
                       int max_cycles, int initial, cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st) {
     const double cx = 1.0 / (M.dx * M.dx), cy = 1.0 / (M.dy * M.dy);
+    const double* nul = nullptr;
     if (M.rz)
-        k_mg_r0<T, true><<<M.grd0, M.blk0, 0, st>>>(phi, f, lv[0].mask, M.nx, M.ny, cx, cy, lv[0].g, M.N, tol * tol,
-                                                    max_cycles, initial, cond, use_cond, M.rz0);
+        launch_pdl(k_mg_r0<T, true>, M.grd0, M.blk0, 0, st, phi, f, lv[0].mask, M.nx, M.ny, cx, cy, lv[0].g, M.N,
+                   tol * tol, max_cycles, initial, cond, use_cond, (const double*)M.rz0);
     else
-        k_mg_r0<T, false><<<M.grd0, M.blk0, 0, st>>>(phi, f, lv[0].mask, M.nx, M.ny, cx, cy, lv[0].g, M.N, tol * tol,
-                                                     max_cycles, initial, cond, use_cond, nullptr);
+        launch_pdl(k_mg_r0<T, false>, M.grd0, M.blk0, 0, st, phi, f, lv[0].mask, M.nx, M.ny, cx, cy, lv[0].g, M.N,
+                   tol * tol, max_cycles, initial, cond, use_cond, nul);
 }
 
 // One V-cycle followed by the residual check, launched on stream st.
@@ -1744,17 +1779,17 @@ static int launch_cycle(MgImpl& M, std::vector<LevelDev<T>>& lv_in, double* phi,
     count = 0;
     for (int l = 0; l < M.Lc; ++l) {
         const dim3 g(div_up(lv[l].nx, kMgTile), div_up(lv[l].ny, kMgTile));
-        kdown<<<g, kMgThreads, down, st>>>(lv[l], lv[l + 1], omega);
+        launch_pdl(kdown, g, dim3(kMgThreads), down, st, lv[l], lv[l + 1], omega);
         ++count;
     }
     CoarseDesc<T> D{};
     fill_coarse(M, M.cl[0], lv, phi, D);
-    if (M.rz) k_mg_coarse<T, true><<<1, kCoarseThreads, M.cl[0].smem, st>>>(D);
-    else k_mg_coarse<T, false><<<1, kCoarseThreads, M.cl[0].smem, st>>>(D);
+    if (M.rz) launch_pdl(k_mg_coarse<T, true>, dim3(1), dim3(kCoarseThreads), M.cl[0].smem, st, D);
+    else launch_pdl(k_mg_coarse<T, false>, dim3(1), dim3(kCoarseThreads), M.cl[0].smem, st, D);
     ++count;
     for (int l = M.Lc - 1; l >= 0; --l) {
         const dim3 g(div_up(lv[l].nx, kMgTile), div_up(lv[l].ny, kMgTile));
-        kup<<<g, kMgThreads, up, st>>>(lv[l], lv[l + 1], omega, l == 0 ? phi : nullptr);
+        launch_pdl(kup, g, dim3(kMgThreads), up, st, lv[l], lv[l + 1], omega, l == 0 ? phi : (double*)nullptr);
         ++count;
     }
     launch_r0(M, lv, phi, f, tol, max_cycles, 0, cond, use_cond, st);
