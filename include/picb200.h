@@ -130,10 +130,13 @@ typedef enum pic_mg_launch_mode {
     PIC_MG_GRAPH_LOOP = 2, /* one launch per kernel inside a CUDA-graph conditional WHILE node */
     PIC_MG_CLUSTER = 3,    /* one launch of a single thread-block cluster per solve (FP32 levels whose
                               row bands fit in shared memory; otherwise the graph loop) */
-    PIC_MG_DST = 4         /* no V-cycles: the direct solve by sine transforms of src/FFT.py:10-64
+    PIC_MG_DST = 4,        /* no V-cycles: the direct solve by sine transforms of src/FFT.py:10-64
                               (FP64, three kernels, then the FP64 residual for pic_mg_info), for
                               Cartesian grids of 2^q + 1 nodes (q <= 11) whose Dirichlet nodes are
                               exactly the four edges; otherwise the graph loop */
+    PIC_MG_HYBRID = 5      /* the graph loop with the levels of at most 129^2 nodes of each V-cycle
+                              in one thread-block-cluster launch (FP32 Cartesian levels, grids
+                              larger than 129^2; otherwise the graph loop) */
 } pic_mg_launch_mode;
 
 /* Geometry of the grid.  PIC_GEOM_RZ is axisymmetric r-z (the reference's

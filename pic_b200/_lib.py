@@ -41,8 +41,9 @@ PIC_MG_HOST_LOOP = 1
 PIC_MG_GRAPH_LOOP = 2
 PIC_MG_CLUSTER = 3
 PIC_MG_DST = 4
+PIC_MG_HYBRID = 5
 MG_LAUNCH_MODES = {"persistent": PIC_MG_PERSISTENT, "host": PIC_MG_HOST_LOOP, "graph": PIC_MG_GRAPH_LOOP,
-                   "cluster": PIC_MG_CLUSTER, "dst": PIC_MG_DST}
+                   "cluster": PIC_MG_CLUSTER, "dst": PIC_MG_DST, "hybrid": PIC_MG_HYBRID}
 
 PIC_ELASTIC = 0
 PIC_EXCITATION = 1

@@ -29,6 +29,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -46,6 +47,7 @@ constexpr long kCoarseMaxNodes32 = 33L * 33L;    // FP32 levels at or below this
 constexpr long kCoarseMaxNodes64 = 33L * 33L;    // FP64 levels
 constexpr int kMgMaxLevels = 16;
 constexpr long kPersistCoarseMax = 33L * 33L;    // levels the persistent kernel's single block solves
+constexpr long kHybridBandMax = 129L * 129L;     // PIC_MG_HYBRID: levels at or below this size run in the cluster
 constexpr unsigned long long kBarrierPolls = 1ull << 24;  // a grid barrier gives up (error flag) after this
 
 // One level of the hierarchy.  The correction has two arrays: the down
@@ -921,6 +923,8 @@ constexpr int kBandBatch = 4;  // global loads a thread issues before the first 
 
 struct ClusterDesc {
     int L, Lb;  // levels; [0, Lb) in bands over the cluster, [Lb, L) in CTA 0
+    int Lt;     // tail: one V-cycle of levels [Lt, L), no residual and no loop (PIC_MG_HYBRID)
+    int tail;
     LevelDev<float> lv[kMgMaxLevels];
     CoarseDesc<float> coarse;
     const double* f;
@@ -1191,6 +1195,21 @@ __global__ void __launch_bounds__(kClusterThreads, 1) k_mg_cluster(ClusterDesc S
     __shared__ double s_part[2];
     cg::cluster_group cl = cg::this_cluster();
     const int rank = int(cl.block_rank()), parts = int(cl.num_blocks());
+    if (S.tail) {
+        // the coarse end of a V-cycle whose finer levels run in tile kernels:
+        // g of level Lt in, the correction of level Lt (its ec) out
+        for (int l = S.Lt; l < S.Lb; ++l) {
+            band_down(S.lv[l], S.lv[l + 1], S.omega, S.pre, rank, parts, smem);
+            cl.sync();
+        }
+        if (rank == 0) coarse_vcycle(S.coarse, smem);
+        cl.sync();
+        for (int l = S.Lb - 1; l >= S.Lt; --l) {
+            band_up(S.lv[l], S.lv[l + 1], S.omega, S.post, nullptr, rank, parts, smem);
+            cl.sync();
+        }
+        return;
+    }
     double r2 = 0.0, f2 = 0.0, dummy = 0.0;
     cluster_r0(S, rank, parts, s_part, r2, f2);
     const double ref = f2 > 0.0 ? f2 : 1.0;
@@ -1246,6 +1265,8 @@ struct MgImpl {
     bool rz = false;          // r-z geometry (PIC_GEOM_RZ)
     double* rz0 = nullptr;    // level-0 row coefficients in FP64 (r-z)
     DstPlan* dst = nullptr;   // PIC_MG_DST: the sine-transform solve
+    bool hybrid = false;      // PIC_MG_HYBRID: levels [Lt, L) in one cluster launch per cycle
+    int Lt = 0;
     pic_mg_options o{};
     std::vector<LevelDev<float>> lf;
     std::vector<LevelDev<double>> ld;
@@ -1499,13 +1520,13 @@ static void fill_coarse(const MgImpl& M, const CoarseLayout& C, const std::vecto
 // Picks the cluster size (16 CTAs where the device allows, else 8) whose
 // band phases fit in shared memory; leaves cluster_ok false (the graph loop
 // is used instead) for FP64 levels or bands that do not fit.
-static int configure_cluster(MgImpl& M, const std::vector<int>& nxs, const std::vector<int>& nys) {
+static int configure_cluster(MgImpl& M, const std::vector<int>& nxs, const std::vector<int>& nys, int first = 0) {
     M.cluster_ok = false;
     if (M.precision != PIC_MG_MIXED) return PIC_OK;
     const int pre = M.o.pre_sweeps, post = M.o.post_sweeps;
     for (int cs : {16, 8}) {
         size_t need = M.cl[1].smem;
-        for (int l = 0; l < M.Lp; ++l) {
+        for (int l = first; l < M.Lp; ++l) {
             const size_t per = size_t((nys[l] + cs - 1) / cs);
             const size_t Rd = per + 2 * size_t(2 * pre + 2), Ru = per + 4 * size_t(post);
             const size_t down = Rd * nxs[l] * (2 * sizeof(float) + 1);
@@ -1585,14 +1606,15 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
         return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: unknown precision %d", M.o.precision));
     if (M.o.pre_sweeps > kMgMaxSweeps || M.o.post_sweeps > kMgMaxSweeps)
         return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: at most 8 pre/post sweeps"));
-    if (M.o.launch_mode < PIC_MG_PERSISTENT || M.o.launch_mode > PIC_MG_DST)
+    if (M.o.launch_mode < PIC_MG_PERSISTENT || M.o.launch_mode > PIC_MG_HYBRID)
         return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: unknown launch mode %d", M.o.launch_mode));
     if (M.o.geometry != PIC_GEOM_CARTESIAN && M.o.geometry != PIC_GEOM_RZ)
         return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: unknown geometry %d", M.o.geometry));
     M.rz = M.o.geometry == PIC_GEOM_RZ;
     // r-z solves run in the graph or host loop (the persistent and cluster
     // kernels are Cartesian)
-    if (M.rz && (M.o.launch_mode == PIC_MG_PERSISTENT || M.o.launch_mode == PIC_MG_CLUSTER))
+    if (M.rz && (M.o.launch_mode == PIC_MG_PERSISTENT || M.o.launch_mode == PIC_MG_CLUSTER ||
+                 M.o.launch_mode == PIC_MG_HYBRID))
         M.o.launch_mode = PIC_MG_GRAPH_LOOP;
     M.precision = M.o.precision;
     M.nx = nx;
@@ -1694,6 +1716,17 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
                                          : alloc_levels(M, M.ld, masks, nxs, nys);
     if (st == PIC_OK) st = M.precision == PIC_MG_MIXED ? configure_kernels<float>(M) : configure_kernels<double>(M);
     if (st == PIC_OK && M.o.launch_mode == PIC_MG_CLUSTER) st = configure_cluster(M, nxs, nys);
+    if (st == PIC_OK && M.o.launch_mode == PIC_MG_HYBRID) {
+        // tile kernels for the levels above kHybridBandMax nodes, one cluster
+        // launch for the rest; FP32 Cartesian levels only, else the graph loop
+        M.Lt = 0;
+        while (M.Lt < M.L && long(nxs[M.Lt]) * nys[M.Lt] > kHybridBandMax) ++M.Lt;
+        if (M.precision == PIC_MG_MIXED && !M.rz && M.Lt >= 1 && M.Lt < M.Lp) {
+            st = configure_cluster(M, nxs, nys, M.Lt);
+            M.hybrid = st == PIC_OK && M.cluster_ok;
+        }
+        if (!M.hybrid) M.o.launch_mode = PIC_MG_GRAPH_LOOP;
+    }
     if (st == PIC_OK && M.o.launch_mode == PIC_MG_DST) {
         // the sine-transform solve applies to Cartesian grids of 2^q + 1 nodes
         // whose Dirichlet nodes are the edges alone; otherwise the graph loop
@@ -1735,6 +1768,8 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
     return PIC_OK;
 }
 
+static int launch_cluster_tail(MgImpl& M, const std::vector<LevelDev<float>>& lv, cudaStream_t st);
+
 // A launch that may start while the preceding kernel on the stream drains
 // (the kernel waits in pdl_wait before reading what that kernel wrote).
 template <class... KArgs, class... Args>
@@ -1771,23 +1806,36 @@ static void launch_r0(MgImpl& M, const std::vector<LevelDev<T>>& lv, double* phi
 template <class T>
 static int launch_cycle(MgImpl& M, std::vector<LevelDev<T>>& lv_in, double* phi, const double* f, double tol,
                         int max_cycles, cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st, int& count) {
-    const std::vector<LevelDev<T>> lv = with_corrections(lv_in, M.Lc);
+    // the hybrid cycle's coarse end starts at Lt (tiles above it); its
+    // cluster kernel's bands write eu like the tile up phases, its CTA 0 the
+    // levels from Lp
+    const bool hyb = std::is_same<T, float>::value && M.hybrid;
+    const int Ltile = hyb ? M.Lt : M.Lc;
+    const std::vector<LevelDev<T>> lv = with_corrections(lv_in, hyb ? M.Lp : M.Lc);
     const T omega = T(M.o.omega);
     const size_t down = down_smem<T>(M.o.pre_sweeps, M.rz), up = up_smem<T>(M.o.post_sweeps, M.rz);
     const DownKernel<T> kdown = M.rz ? down_kernel<T, true>(M.o.pre_sweeps) : down_kernel<T, false>(M.o.pre_sweeps);
     const UpKernel<T> kup = M.rz ? up_kernel<T, true>(M.o.post_sweeps) : up_kernel<T, false>(M.o.post_sweeps);
     count = 0;
-    for (int l = 0; l < M.Lc; ++l) {
+    for (int l = 0; l < Ltile; ++l) {
         const dim3 g(div_up(lv[l].nx, kMgTile), div_up(lv[l].ny, kMgTile));
         launch_pdl(kdown, g, dim3(kMgThreads), down, st, lv[l], lv[l + 1], omega);
         ++count;
     }
-    CoarseDesc<T> D{};
-    fill_coarse(M, M.cl[0], lv, phi, D);
-    if (M.rz) launch_pdl(k_mg_coarse<T, true>, dim3(1), dim3(kCoarseThreads), M.cl[0].smem, st, D);
-    else launch_pdl(k_mg_coarse<T, false>, dim3(1), dim3(kCoarseThreads), M.cl[0].smem, st, D);
-    ++count;
-    for (int l = M.Lc - 1; l >= 0; --l) {
+    if constexpr (std::is_same<T, float>::value) {
+        if (hyb) {
+            PIC_TRY(launch_cluster_tail(M, lv, st));
+            ++count;
+        }
+    }
+    if (!hyb) {
+        CoarseDesc<T> D{};
+        fill_coarse(M, M.cl[0], lv, phi, D);
+        if (M.rz) launch_pdl(k_mg_coarse<T, true>, dim3(1), dim3(kCoarseThreads), M.cl[0].smem, st, D);
+        else launch_pdl(k_mg_coarse<T, false>, dim3(1), dim3(kCoarseThreads), M.cl[0].smem, st, D);
+        ++count;
+    }
+    for (int l = Ltile - 1; l >= 0; --l) {
         const dim3 g(div_up(lv[l].nx, kMgTile), div_up(lv[l].ny, kMgTile));
         launch_pdl(kup, g, dim3(kMgThreads), up, st, lv[l], lv[l + 1], omega, l == 0 ? phi : (double*)nullptr);
         ++count;
@@ -1885,6 +1933,35 @@ static int launch_cluster(MgImpl& M, double* phi, const double* f, double tol, i
     S.N = M.N;
     S.tol2 = tol * tol;
     S.max_cycles = max_cycles;
+    S.omega = float(M.o.omega);
+    S.pre = M.o.pre_sweeps;
+    S.post = M.o.post_sweeps;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(M.cluster_size);
+    cfg.blockDim = dim3(kClusterThreads);
+    cfg.dynamicSmemBytes = M.cluster_smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = M.cluster_size;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    PIC_CUDA(cudaLaunchKernelEx(&cfg, k_mg_cluster, S));
+    return PIC_OK;
+}
+
+// The coarse end of a PIC_MG_HYBRID V-cycle: levels [Lt, Lp) in bands over the
+// cluster, [Lp, L) in its CTA 0, in one launch (lv: with eu corrections below Lp).
+static int launch_cluster_tail(MgImpl& M, const std::vector<LevelDev<float>>& lv, cudaStream_t st) {
+    ClusterDesc S{};
+    S.L = M.L;
+    S.Lb = M.Lp;
+    S.Lt = M.Lt;
+    S.tail = 1;
+    for (int l = 0; l < M.L; ++l) S.lv[l] = lv[l];
+    fill_coarse(M, M.cl[1], lv, nullptr, S.coarse);
     S.omega = float(M.o.omega);
     S.pre = M.o.pre_sweeps;
     S.post = M.o.post_sweeps;

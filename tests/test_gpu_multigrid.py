@@ -39,7 +39,7 @@ def manufactured(n):
     return h, f, exact
 
 
-@pytest.mark.parametrize("launch", ["persistent", "graph", "host", "cluster"])
+@pytest.mark.parametrize("launch", ["persistent", "graph", "host", "cluster", "hybrid"])
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
 @pytest.mark.parametrize("n", [17, 33, 65, 129, 257])
 def test_manufactured_solution(launch, precision, n):
@@ -93,7 +93,7 @@ def test_internal_electrodes_match_direct_solve():
     mask = edge_mask(n)
     mask[idx] = 1
     ref = direct_solve(n, h, idx, val, f)
-    for precision, launch in (("mixed", "graph"), ("fp64", "graph"), ("mixed", "cluster")):
+    for precision, launch in (("mixed", "graph"), ("fp64", "graph"), ("mixed", "cluster"), ("mixed", "hybrid")):
         mg = MultigridSolver(mask, n, n, h, precision=precision, launch=launch)
         phi0 = np.zeros(n * n)
         phi0[idx] = val
@@ -106,7 +106,7 @@ def test_internal_electrodes_match_direct_solve():
         np.testing.assert_allclose(phi.cpu().numpy(), ref, rtol=0, atol=1e-8 * np.abs(ref).max())
 
 
-@pytest.mark.parametrize("launch", ["graph", "persistent", "cluster"])
+@pytest.mark.parametrize("launch", ["graph", "persistent", "cluster", "hybrid"])
 def test_electrodes_on_odd_lines(launch):
     """Electrodes on lines that do not survive injection to the coarse grids
     (column 43 and row 77, both odd; column 85): the coarse grids keep them as
@@ -145,8 +145,10 @@ def test_residual_recomputed_on_cpu(n, tol):
     f[mask == 1] = 0
     phi0 = np.zeros(n * n)
     phi0.reshape(n, n)[1:-1, 0] = 100.0
-    for precision, launch in (("mixed", "graph"), ("fp64", "graph"), ("mixed", "cluster")):
+    for precision, launch in (("mixed", "graph"), ("fp64", "graph"), ("mixed", "cluster"), ("mixed", "hybrid")):
         mg = MultigridSolver(mask, n, n, h, precision=precision, launch=launch)
+        if launch == "hybrid":
+            assert mg.effective_launch() == "hybrid"
         if launch == "cluster":
             # the finest band of a 513^2 grid fits one CTA's shared memory; 1025^2 and up fall back
             assert mg.effective_launch() == ("cluster" if n <= 513 else "graph")
