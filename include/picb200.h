@@ -403,7 +403,7 @@ long long pic_sim_kernel_launches(pic_sim* sim);
 
 /* Per-phase device timing with CUDA events recorded on the launch stream. */
 enum {
-    PIC_PHASE_BUILD = 0, /* work items, step counter           */
+    PIC_PHASE_BUILD = 0, /* work items, step counter, candidates */
     PIC_PHASE_PUSH = 1,  /* the fused particle kernel           */
     PIC_PHASE_MERGE = 2, /* ionisation products                 */
     PIC_PHASE_RHS = 3,   /* rho -> f                            */

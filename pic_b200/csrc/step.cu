@@ -843,8 +843,14 @@ struct SimImpl {
     long long launches = 0;  // launches outside the multigrid loop
     long long solves = 0;    // multigrid solves issued (each runs 1 + cycles * body kernels)
     bool profiling = false;
-    cudaStream_t cap = nullptr;
+    cudaStream_t cap = nullptr, cap2 = nullptr;  // capture stream and the side branch of a captured step
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // g_sort_step: the step whose side branch sorts for the next step
     cudaGraphExec_t g_step = nullptr, g_sort_step = nullptr;
+    // the next particle pass is prepared (its sort, items and candidate bits
+    // done, the step counter advanced): set by a captured step, cleared by
+    // anything that changes the particle state on the host's behalf
+    bool prepared = false;
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
     std::vector<cudaEvent_t> event_pool;
     long long prof_cycles = 0;
@@ -931,21 +937,33 @@ static PushArgs push_args(SimImpl& S, int kick, int mcc, int drift, int deposit,
     return A;
 }
 
-static int particle_pass(SimImpl& S, cudaStream_t st, int kick, int mcc, int drift, int deposit, double kick_factor,
-                         int advance_step) {
+// The preparation of a particle pass: work items for the current particle
+// state (and the step counter, when advance_step), then, for a pass with
+// collisions, the null-collision candidate bits of that step.  It reads only
+// the particle state, so a captured step runs the next step's preparation
+// beside its own field solve.
+static int prepare_pass(SimImpl& S, cudaStream_t st, int mcc, int advance_step) {
     {
         PhaseTimer t(S, PIC_PHASE_BUILD, st);
         k_build_items<<<1, 256, 0, st>>>(S.d_state, S.ns, S.n_tiled, S.items, S.n_items, S.item_next, S.step_ctr,
                                          S.births.count, S.cand_count, advance_step);
-    }
-    const PushArgs A = push_args(S, kick, mcc, drift, deposit, kick_factor);
-    {
-        PhaseTimer t(S, PIC_PHASE_PUSH, st);
-        if (A.do_mcc) {
-            k_mcc_bits<<<div_up(S.cbits_segments, 256), 256, 0, st>>>(S.mcc_dev, S.ns, S.step_ctr, A.key, S.d_cbits,
+        if (mcc && S.have_mcc) {
+            const uint2 key = make_uint2(uint32_t(S.d.seed), uint32_t(S.d.seed >> 32));
+            k_mcc_bits<<<div_up(S.cbits_segments, 256), 256, 0, st>>>(S.mcc_dev, S.ns, S.step_ctr, key, S.d_cbits,
                                                                      S.d_nseg);
             S.launches += 1;
         }
+    }
+    S.launches += 1;
+    PIC_LAUNCH_CHECK();
+    return PIC_OK;
+}
+
+// The particle pass itself, once prepare_pass has run for it.
+static int run_pass(SimImpl& S, cudaStream_t st, int kick, int mcc, int drift, int deposit, double kick_factor) {
+    const PushArgs A = push_args(S, kick, mcc, drift, deposit, kick_factor);
+    {
+        PhaseTimer t(S, PIC_PHASE_PUSH, st);
         if (S.rz) k_push<true><<<S.push_grid, kPushThreads, S.push_smem, st>>>(A);
         else k_push<false><<<S.push_grid, kPushThreads, S.push_smem, st>>>(A);
     }
@@ -959,9 +977,15 @@ static int particle_pass(SimImpl& S, cudaStream_t st, int kick, int mcc, int dri
         }
         k_merge_births<<<64, 256, 0, st>>>(A);
     }
-    S.launches += 3;
+    S.launches += 2;
     PIC_LAUNCH_CHECK();
     return PIC_OK;
+}
+
+static int particle_pass(SimImpl& S, cudaStream_t st, int kick, int mcc, int drift, int deposit, double kick_factor,
+                         int advance_step) {
+    PIC_TRY(prepare_pass(S, st, mcc, advance_step));
+    return run_pass(S, st, kick, mcc, drift, deposit, kick_factor);
 }
 
 static int field_solve(SimImpl& S, cudaStream_t st, bool capturing) {
@@ -1008,17 +1032,28 @@ static int sort_all(SimImpl& S, cudaStream_t st) {
     return PIC_OK;
 }
 
-// The steady-state step (kick + MCC + drift + deposit, solve, E), optionally
-// preceded by the cell sort, captured once into a CUDA graph.
-static int capture_step(SimImpl& S, bool with_sort, cudaGraphExec_t* out) {
+// The steady-state step captured once into a CUDA graph: the particle pass
+// (kick + MCC + drift + deposit, prepared beforehand), then the field solve
+// (RHS, multigrid, E) on the capture stream and, on a side branch beside it,
+// the next step's preparation (its cell sort when sort_next, work items,
+// candidate bits), which reads only the particle state.
+static int capture_step(SimImpl& S, bool sort_next, cudaGraphExec_t* out) {
     const bool prof = S.profiling;
     S.profiling = false;
     const long long l0 = S.launches, s0 = S.solves;
     PIC_CUDA(cudaStreamBeginCapture(S.cap, cudaStreamCaptureModeThreadLocal));
-    int rc = PIC_OK;
-    if (with_sort) rc = sort_all(S, S.cap);
-    if (rc == PIC_OK) rc = particle_pass(S, S.cap, 1, 1, 1, 1, 1.0, 1);
+    int rc = run_pass(S, S.cap, 1, 1, 1, 1, 1.0);
+    bool forked = false;
+    if (rc == PIC_OK && cudaEventRecord(S.ev_fork, S.cap) == cudaSuccess &&
+        cudaStreamWaitEvent(S.cap2, S.ev_fork, 0) == cudaSuccess) {
+        forked = true;
+        if (sort_next) rc = sort_all(S, S.cap2);
+        if (rc == PIC_OK) rc = prepare_pass(S, S.cap2, 1, 1);
+        if (cudaEventRecord(S.ev_join, S.cap2) != cudaSuccess && rc == PIC_OK)
+            rc = fail(PIC_ERR_CUDA, "step capture: join event");
+    }
     if (rc == PIC_OK) rc = field_solve(S, S.cap, true);
+    if (forked) cudaStreamWaitEvent(S.cap, S.ev_join, 0);
     cudaGraph_t g = nullptr;
     const cudaError_t ec = cudaStreamEndCapture(S.cap, &g);
     S.profiling = prof;
@@ -1209,6 +1244,9 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
     PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_fn, kPushThreads, S.push_smem));
     S.push_grid = std::max(1, per_sm) * num_sms();
     PIC_CUDA(cudaStreamCreateWithFlags(&S.cap, cudaStreamNonBlocking));
+    PIC_CUDA(cudaStreamCreateWithFlags(&S.cap2, cudaStreamNonBlocking));
+    PIC_CUDA(cudaEventCreateWithFlags(&S.ev_fork, cudaEventDisableTiming));
+    PIC_CUDA(cudaEventCreateWithFlags(&S.ev_join, cudaEventDisableTiming));
     (void)st;
     return PIC_OK;
 }
@@ -1218,6 +1256,9 @@ static void sim_free(SimImpl& S) {
     if (S.g_sort_step) cudaGraphExecDestroy(S.g_sort_step);
     S.g_step = S.g_sort_step = nullptr;
     if (S.cap) cudaStreamDestroy(S.cap);
+    if (S.cap2) cudaStreamDestroy(S.cap2);
+    if (S.ev_fork) cudaEventDestroy(S.ev_fork);
+    if (S.ev_join) cudaEventDestroy(S.ev_join);
     S.cap = nullptr;
     for (auto& m : S.marks) {
         cudaEventDestroy(m.second.first);
@@ -1453,6 +1494,7 @@ int pic_sim_load_species(pic_sim* sim, int s, const float* x, const float* y, co
     if (!sim || s < 0 || s >= sim->s.ns || n < 0 || n > sim->s.d.species[s].capacity)
         return fail(PIC_ERR_BAD_ARG, "pic_sim_load_species: bad arguments");
     SimImpl& S = sim->s;
+    S.prepared = false;
     cudaStream_t st = as_stream(stream);
     PIC_CUDA(cudaStreamSynchronize(st));
     PIC_CUDA(cudaMemcpy(&S.h_state[s], S.d_state + s, sizeof(SpeciesState), cudaMemcpyDeviceToHost));
@@ -1474,6 +1516,7 @@ int pic_sim_init(pic_sim* sim, void* stream) {
     if (!sim) return fail(PIC_ERR_BAD_ARG, "pic_sim_init: sim is NULL");
     SimImpl& S = sim->s;
     cudaStream_t st = as_stream(stream);
+    S.prepared = false;
     if (S.d.sort_interval > 0) PIC_TRY(sort_all(S, st));
     PIC_TRY(particle_pass(S, st, 0, 0, 0, 1, 1.0, 0));
     PIC_TRY(field_solve(S, st, false));
@@ -1492,15 +1535,28 @@ int pic_sim_step(pic_sim* sim, int n_steps, void* stream) {
     for (int i = 0; i < n_steps; ++i) {
         const bool sort = S.d.sort_interval > 0 && S.steps % S.d.sort_interval == 0;
         if (S.d.use_graph && S.kick_pending && !S.profiling && mg_uses_graph(S.mg)) {
-            cudaGraphExec_t& g = sort ? S.g_sort_step : S.g_step;
-            if (!g) PIC_TRY(capture_step(S, sort, &g));
+            if (!S.prepared) {
+                if (sort) PIC_TRY(sort_all(S, st));
+                PIC_TRY(prepare_pass(S, st, 1, 1));
+            }
+            const bool sort_next = S.d.sort_interval > 0 && (S.steps + 1) % S.d.sort_interval == 0;
+            cudaGraphExec_t& g = sort_next ? S.g_sort_step : S.g_step;
+            if (!g) PIC_TRY(capture_step(S, sort_next, &g));
             PIC_CUDA(cudaGraphLaunch(g, st));
-            S.launches += 3 + (S.have_mcc ? 2 : 0) + 2 + (sort ? 1 + (long long)S.ns * (5 + 3 * S.sorter.passes) : 0);
+            S.launches +=
+                3 + (S.have_mcc ? 2 : 0) + 2 + (sort_next ? 1 + (long long)S.ns * (5 + 3 * S.sorter.passes) : 0);
             S.solves += 1;
+            S.prepared = true;
         } else {
-            if (sort) PIC_TRY(sort_all(S, st));
             const int k = S.kick_pending ? 1 : 0;
-            PIC_TRY(particle_pass(S, st, k, k, 1, 1, 1.0, 1));
+            if (S.prepared) {
+                // this step's sort, items and counter were done by the last captured step
+                PIC_TRY(run_pass(S, st, k, k, 1, 1, 1.0));
+                S.prepared = false;
+            } else {
+                if (sort) PIC_TRY(sort_all(S, st));
+                PIC_TRY(particle_pass(S, st, k, k, 1, 1, 1.0, 1));
+            }
             PIC_TRY(field_solve(S, st, false));
         }
         S.kick_pending = true;
@@ -1514,7 +1570,9 @@ int pic_sim_sync(pic_sim* sim, void* stream) {
     if (!sim) return fail(PIC_ERR_BAD_ARG, "pic_sim_sync: sim is NULL");
     SimImpl& S = sim->s;
     if (!S.kick_pending) return PIC_OK;
-    PIC_TRY(particle_pass(S, as_stream(stream), 1, 1, 0, 0, 1.0, 1));
+    // a prepared pass has its counter advanced already
+    PIC_TRY(particle_pass(S, as_stream(stream), 1, 1, 0, 0, 1.0, S.prepared ? 0 : 1));
+    S.prepared = false;
     S.kick_pending = false;
     return PIC_OK;
 }
@@ -1737,8 +1795,13 @@ int pic_ens_step(pic_ens* e, int n_steps, void* stream) {
     if (fresh) {
         for (SimImpl* S : E.m) {
             const int k = S->kick_pending ? 1 : 0;
-            if (S->d.sort_interval > 0 && S->steps % S->d.sort_interval == 0) PIC_TRY(sort_all(*S, st));
-            PIC_TRY(particle_pass(*S, st, k, k, 1, 1, 1.0, 1));
+            if (S->prepared) {
+                PIC_TRY(run_pass(*S, st, k, k, 1, 1, 1.0));
+            } else {
+                if (S->d.sort_interval > 0 && S->steps % S->d.sort_interval == 0) PIC_TRY(sort_all(*S, st));
+                PIC_TRY(particle_pass(*S, st, k, k, 1, 1, 1.0, 1));
+            }
+            S->prepared = false;
             PIC_TRY(field_solve(*S, st, false));
             S->kick_pending = true;
             ++S->steps;
@@ -1754,6 +1817,8 @@ int pic_ens_step(pic_ens* e, int n_steps, void* stream) {
     PIC_CUDA(cudaMemcpyAsync(E.d_ctl, &ctl, sizeof ctl, cudaMemcpyHostToDevice, st));
     PIC_CUDA(cudaStreamSynchronize(st));  // the host copies above read stack memory
     PIC_CUDA(cudaGraphLaunch(E.exec, st));
+    // the ensemble's body prepares each pass itself
+    for (SimImpl* S : E.m) S->prepared = false;
     for (SimImpl* S : E.m) {
         long long sorts = 0;
         if (S->d.sort_interval > 0)
