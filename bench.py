@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--sort-interval", type=int, default=80,
                     help="steps between cell sorts (80: the autotuner's choice for 513^2 shapes)")
     ap.add_argument("--particles", type=int, default=4_000_000, help="per species")
+    ap.add_argument("--tile", type=int, default=16, help="cells per side of the push's work tiles")
     ap.add_argument("--no-poisson", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -626,6 +627,7 @@ def main():
     GRAPH_OPTS["mg_launch"] = args.mg_launch
     GRAPH_OPTS["pre_sweeps"], GRAPH_OPTS["post_sweeps"] = args.mg_sweeps
     GRAPH_OPTS["omega"] = args.omega
+    GRAPH_OPTS["tile"] = args.tile
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, world, rank)

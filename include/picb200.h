@@ -197,6 +197,22 @@ int pic_mg_read_info(pic_mg* mg, double tol, pic_mg_info* info);
  * PIC_MG_GRAPH_LOOP where the cluster solve does not apply). */
 int pic_mg_effective_launch_mode(pic_mg* mg, int* mode);
 
+/* Solver(solver_type='cg' | 'gmres') (src/Solvers.py:245-258: cupyx cg and
+ * gmres on the 5-point Laplacian with Dirichlet rows): flexible
+ * preconditioned conjugate gradients for lap(phi) = f in FP64, Cartesian.
+ * The system is symmetric, so the solution is the one GMRES converges to.
+ * h_dirichlet: nx*ny, 1 = Dirichlet (the grid edges always are); precond: a
+ * pic_mg of the same grid and mask whose one V-cycle from zero
+ * preconditions each iteration (NULL: none).  pic_cg_solve keeps phi on the
+ * Dirichlet nodes, iterates until ||f - lap(phi)|| / ||f|| < tol over the free
+ * nodes or max_iter (info->cycles = iterations), synchronises `stream` once
+ * per dot product, and returns PIC_ERR_NOT_CONVERGED if tol is not reached. */
+typedef struct pic_cg pic_cg;
+int pic_cg_create(int nx, int ny, double dx, double dy, const uint8_t* h_dirichlet, pic_mg* precond, pic_cg** out);
+int pic_cg_solve(pic_cg* cg, double* d_phi, const double* d_f, double tol, int max_iter, pic_mg_info* info,
+                 void* stream);
+int pic_cg_destroy(pic_cg* cg);
+
 /* ------------------------------------------------------------------ */
 /* Cell sort (replaces Particles2D.sort_particles_sparse, src/Particles.py:550-632) */
 /* ------------------------------------------------------------------ */

@@ -144,6 +144,9 @@ SIGNATURES = {
     "pic_form_rhs": [_vp, _vp, _d, _vp, _i, _i, _vp],
     "pic_update_E_rz": [_vp, _vp, _vp, _i, _i, _d, _d, _vp],
     "pic_sim_solver_mode": [_vp, C.POINTER(_i)],
+    "pic_cg_create": [_i, _i, _d, _d, _vp, _vp, C.POINTER(_vp)],
+    "pic_cg_solve": [_vp, _vp, _vp, _d, _i, C.POINTER(MgInfo), _vp],
+    "pic_cg_destroy": [_vp],
     "pic_sim_particle_buffer": [_vp, _vp, _i, _d, _d, _d, _d, C.POINTER(_i), _vp],
     "pic_rz_density": [_vp, _i, _i, _d, _vp],
     "pic_update_R_rz": [_vp, _vp, _vp, _vp, _vp, _i, _f, _f, _vp],

@@ -2122,6 +2122,7 @@ int mg_capture_into(pic_mg* mg, double* phi, const double* f, double tol, int ma
     return mg_capture(mg->m, phi, f, tol, max_cycles, st);
 }
 bool mg_uses_graph(pic_mg* mg) { return mg->m.o.launch_mode != PIC_MG_HOST_LOOP; }
+bool mg_is_rz(pic_mg* mg) { return mg->m.rz; }
 int mg_launch_graph(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
     return mg_launch(mg->m, phi, f, tol, max_cycles, st);
 }

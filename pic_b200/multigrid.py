@@ -75,3 +75,41 @@ class MultigridSolver:
             _lib.check(rc, "pic_mg_solve")
         self.last_info = info
         return phi, (info.cycles, info.rel_res)
+
+
+class ConjugateGradientSolver:
+    """The 'cg' / 'gmres' branches of the reference's Solver (src/Solvers.py:245-258,
+    cupyx cg and gmres): flexible preconditioned conjugate gradients on the GPU
+    (pic_cg_*), FP64, each iteration preconditioned by one V-cycle of
+    `precond` (a MultigridSolver of the same grid and mask) when given.  The
+    Cartesian 5-point system is symmetric, so this is also the solution GMRES
+    converges to."""
+
+    def __init__(self, bc_mask, nx, ny, h, hy=None, precond: MultigridSolver | None = None):
+        self.nx, self.ny = int(nx), int(ny)
+        mask = np.ascontiguousarray(torch.as_tensor(bc_mask).cpu().numpy().reshape(-1) != 0, dtype=np.uint8)
+        self.precond = precond
+        self._h = C.c_void_p()
+        _lib.call("pic_cg_create", self.nx, self.ny, float(h), float(h if hy is None else hy), mask.ctypes.data,
+                  precond._h if precond is not None else None, C.byref(self._h))
+        self.last_info = None
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _lib.load().pic_cg_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def solve(self, phi, rho, tol=1e-5, max_iter=200, raise_on_fail=False):
+        """Solve lap(phi) = rho in place; returns (phi, (iterations, rel_res))."""
+        assert phi.dtype == torch.float64 and rho.dtype == torch.float64 and phi.is_cuda and rho.is_cuda
+        info = _lib.MgInfo()
+        rc = _lib.load().pic_cg_solve(self._h, _lib.ptr(phi), _lib.ptr(rho), float(tol), int(max_iter),
+                                      C.byref(info), _lib.stream_ptr())
+        if rc not in (_lib.PIC_OK, _lib.PIC_ERR_NOT_CONVERGED) or (raise_on_fail and rc != _lib.PIC_OK):
+            _lib.check(rc, "pic_cg_solve")
+        self.last_info = info
+        return phi, (info.cycles, info.rel_res)
