@@ -47,7 +47,8 @@ size_t diagnostics_scratch_doubles();
 bool mg_uses_graph(pic_mg* mg);
 
 constexpr int kPushThreads = 256;
-constexpr int kPushP = 5;  // particles per thread per chunk (odd: conflict-free blocked access to shared memory)
+constexpr int kPushP = 3;  // particles per thread per chunk (odd: conflict-free blocked access to shared memory;
+                           // 3 keeps a CTA at 45 KB of shared memory, so that four fit on an SM)
 constexpr int kChunk = kPushThreads * kPushP;
 constexpr int kBufStride = kChunk + 8;  // floats per array per buffer: room for the 16-byte alignment window
 constexpr int kUnitMax = 8160;          // particles per work unit (one E tile staging, one charge flush)
@@ -274,7 +275,7 @@ constexpr int kStages = 3;  // chunk buffers: one loading, one in work, one drai
 // RZ: r-z geometry (drift_rz); a separate instance, so that the Cartesian
 // pass carries none of it.
 template <bool RZ>
-__global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
+__global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
     extern __shared__ __align__(128) unsigned char smem[];
     float* bufs = reinterpret_cast<float*>(smem);  // [kStages][4][kBufStride]
     const int RW = A.rw;
@@ -348,12 +349,20 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push(PushArgs A) {
         // r-z: the azimuthal velocity is not staged; it is read and written in place
         float* const gvz = RZ ? A.state[s].cur[4] + b : nullptr;
         unsigned my_abs = 0, my_cand = 0, my_elec = 0;
+        // the candidate bits of this thread's slots: at most two words, each
+        // loaded only if one of the chunk's slots lies in it
+        const int s0 = b + tid * kPushP, s_last = min(s0 + kPushP, b + n) - 1;
+        unsigned cw0 = 0u, cw1 = 0u;
+        if (cbits && s0 <= s_last) {
+            cw0 = __ldg(cbits + (s0 >> 5));
+            if ((s_last >> 5) != (s0 >> 5)) cw1 = __ldg(cbits + (s_last >> 5));
+        }
 #pragma unroll
         for (int k = 0; k < kPushP; ++k) {
             const int l = tid * kPushP + k;
             if (l >= n) break;
             const int slot = b + l;
-            const bool candidate = cbits && ((__ldg(cbits + (slot >> 5)) >> (slot & 31)) & 1u);
+            const bool candidate = (((slot >> 5) == (s0 >> 5) ? cw0 : cw1) >> (slot & 31)) & 1u;
             float x = px[l], y = py[l];
             if (!is_live(x)) continue;
             float vx = pvx[l], vy = pvy[l];
