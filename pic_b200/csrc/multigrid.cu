@@ -115,10 +115,14 @@ struct CoarseDesc {
 
 // Programmatic dependent launch: the V-cycle is a chain of small dependent
 // kernels, launched with cudaLaunchAttributeProgrammaticStreamSerialization so
-// that each one is scheduled while its predecessor drains.  pdl_wait blocks
+// that each one is scheduled while its predecessor runs.  pdl_wait blocks
 // until the preceding grid has completed and its memory is visible (a no-op
-// for a launch without the attribute); pdl_trigger, after a CTA's last store,
-// lets the next grid launch.
+// for a launch without the attribute); every kernel triggers its successor
+// right after its own wait, so at most two grids of the chain are resident and
+// the code of a kernel before its wait may read anything written two or more
+// launches earlier (never what the kernel just before it writes).  The up
+// kernels load their whole fine tile (mask, g, e of their level, phi) there,
+// so only the coarse correction's load follows the wait.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
@@ -275,11 +279,11 @@ template <class T, int S, bool CYL>
 __global__ void __launch_bounds__(kMgThreads) k_mg_down(LevelDev<T> F, LevelDev<T> Cc, T omega) {
     extern __shared__ __align__(16) unsigned char smem[];
     pdl_wait();
-    down_tile<T, S, CYL>(F, Cc, omega, blockIdx.x, blockIdx.y, smem);
     pdl_trigger();
+    down_tile<T, S, CYL>(F, Cc, omega, blockIdx.x, blockIdx.y, smem);
 }
 
-template <class T, int S, bool CYL = false>
+template <class T, int S, bool CYL = false, bool PDL = false>
 __device__ void up_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, double* __restrict__ phi, int tx,
                         int ty, unsigned char* smem) {
     constexpr int H = UpGeom<S>::H, W = UpGeom<S>::W, CW = UpGeom<S>::CW;
@@ -294,16 +298,6 @@ __device__ void up_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, do
     const int ox = x0 - H, oy = y0 - H;
     const int cox = ox >> 1, coy = oy >> 1;  // floor for negative origins
     const int tid = threadIdx.x;
-    // every global load of this tile is issued up front: the coarse
-    // correction, phi of the core (level 0), then the fine tile
-    T cv[CIT];
-#pragma unroll
-    for (int it = 0; it < CIT; ++it) {
-        const int q = it * kMgThreads + tid;
-        const int I = cox + q % CW, J = coy + q / CW;
-        const bool in = q < CW * CW && I >= 0 && J >= 0 && I < Cc.nx && J < Cc.ny;
-        cv[it] = in ? Cc.ec[long(J) * Cc.nx + I] : T(0);
-    }
     double pv[OIT];
 #pragma unroll
     for (int it = 0; it < OIT; ++it) {
@@ -312,6 +306,18 @@ __device__ void up_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, do
         pv[it] = (phi && i < F.nx && j < F.ny) ? phi[long(j) * F.nx + i] : 0.0;
     }
     tile_load<T, W, true, CYL>(F, ox, oy, se, sg, sm, srz);
+    if constexpr (PDL) {
+        pdl_wait();
+        pdl_trigger();
+    }
+    T cv[CIT];
+#pragma unroll
+    for (int it = 0; it < CIT; ++it) {
+        const int q = it * kMgThreads + tid;
+        const int I = cox + q % CW, J = coy + q / CW;
+        const bool in = q < CW * CW && I >= 0 && J >= 0 && I < Cc.nx && J < Cc.ny;
+        cv[it] = in ? Cc.ec[long(J) * Cc.nx + I] : T(0);
+    }
 #pragma unroll
     for (int it = 0; it < CIT; ++it) {
         const int q = it * kMgThreads + tid;
@@ -360,9 +366,7 @@ template <class T, int S, bool CYL>
 __global__ void __launch_bounds__(kMgThreads) k_mg_up(LevelDev<T> F, LevelDev<T> Cc, T omega,
                                                       double* __restrict__ phi) {
     extern __shared__ __align__(16) unsigned char smem[];
-    pdl_wait();
-    up_tile<T, S, CYL>(F, Cc, omega, phi, blockIdx.x, blockIdx.y, smem);
-    pdl_trigger();
+    up_tile<T, S, CYL, true>(F, Cc, omega, phi, blockIdx.x, blockIdx.y, smem);
 }
 
 // Runtime sweep counts (the persistent kernel) dispatched to the instances.
@@ -606,8 +610,8 @@ template <class T, bool CYL>
 __global__ void __launch_bounds__(kCoarseThreads) k_mg_coarse(CoarseDesc<T> D) {
     extern __shared__ __align__(16) unsigned char smem[];
     pdl_wait();
-    coarse_vcycle<T, CYL>(D, smem);
     pdl_trigger();
+    coarse_vcycle<T, CYL>(D, smem);
 }
 
 // ---- FP64 residual, norms and the loop decision -----------------------------------
@@ -634,6 +638,7 @@ __global__ void __launch_bounds__(256) k_mg_r0(const double* __restrict__ phi, c
     // a 32 x 8 block covers 32 x 32 nodes, four rows per thread, every load
     // of a thread issued before the first is used
     pdl_wait();
+    pdl_trigger();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double r = 0.0, fv = 0.0;
     double pc[kR0Rows], pw[kR0Rows], pe[kR0Rows], ps[kR0Rows], pn[kR0Rows], pf[kR0Rows];
