@@ -614,6 +614,65 @@ __global__ void __launch_bounds__(kCoarseThreads) k_mg_coarse(CoarseDesc<T> D) {
     coarse_vcycle<T, CYL>(D, smem);
 }
 
+// ---- direct solve of the first coarse level ----------------------------------------
+//
+// The coarse end of a graph- or host-loop V-cycle: e = A^-1 g on the first
+// level of at most 33^2 nodes, A^-1 the inverse of that level's operator on its
+// free nodes (band LU at creation), instead of a V-cycle of the levels below
+// in one CTA.  One warp per row of the inverse, kDirectRows rows per CTA;
+// a warp's row never changes, so it is loaded before the wait, and only the
+// gather of g follows it.
+
+constexpr int kDirectMaxFree = 1120;              // free nodes of the level
+constexpr int kDirectCols = kDirectMaxFree / 32;  // entries of a row per lane
+constexpr int kDirectRows = 8;                    // rows (warps) per CTA
+constexpr int kDirectGather = (kDirectMaxFree + kDirectRows * 32 - 1) / (kDirectRows * 32);
+
+template <class T>
+struct DirectDesc {
+    const T* ainv;    // [n][n], row-major
+    const int* idx;   // the free node of each row
+    const int* zidx;  // the level's other nodes (their e is 0)
+    const T* g;       // right-hand side (every node of the level)
+    T* e;             // solution (every node of the level)
+    int n, nz;
+};
+
+template <class T>
+__global__ void __launch_bounds__(kDirectRows * 32) k_mg_direct(DirectDesc<T> D) {
+    __shared__ T gs[kDirectMaxFree];
+    const int lane = threadIdx.x & 31, row = blockIdx.x * kDirectRows + int(threadIdx.x >> 5);
+    T a[kDirectCols];
+#pragma unroll
+    for (int u = 0; u < kDirectCols; ++u) {
+        const int c = lane + 32 * u;
+        a[u] = (row < D.n && c < D.n) ? __ldg(D.ainv + long(row) * D.n + c) : T(0);
+    }
+    int gi[kDirectGather];
+#pragma unroll
+    for (int u = 0; u < kDirectGather; ++u) {
+        const int k = int(threadIdx.x) + u * kDirectRows * 32;
+        gi[u] = k < D.n ? __ldg(D.idx + k) : -1;
+    }
+    const int out = row < D.n ? __ldg(D.idx + row) : -1;
+    pdl_wait();
+    pdl_trigger();
+#pragma unroll
+    for (int u = 0; u < kDirectGather; ++u)
+        if (gi[u] >= 0) gs[threadIdx.x + u * kDirectRows * 32] = D.g[gi[u]];
+    if (blockIdx.x == 0)
+        for (int k = threadIdx.x; k < D.nz; k += blockDim.x) D.e[D.zidx[k]] = T(0);
+    __syncthreads();
+    T s = T(0);
+#pragma unroll
+    for (int u = 0; u < kDirectCols; ++u) {
+        const int c = lane + 32 * u;
+        if (c < D.n) s += a[u] * gs[c];
+    }
+    const double t = warp_sum(double(s));
+    if (lane == 0 && out >= 0) D.e[out] = T(t);
+}
+
 // ---- FP64 residual, norms and the loop decision -----------------------------------
 
 struct NormState {
@@ -1279,6 +1338,11 @@ struct MgImpl {
     double* ainv = nullptr;
     int* cidx = nullptr;
     int nfree_c = 0;
+    // direct solve of level Lc (graph and host loops; else the coarse kernel)
+    bool direct = false;
+    void* dinv = nullptr;  // [dn][dn] in the V-cycle's precision
+    int* didx = nullptr;   // dn free nodes, then dnz others
+    int dn = 0, dnz = 0;
     NormState N{};
     dim3 blk0{32, 8}, grd0;
     CoarseLayout cl[2];  // the coarse kernel's levels (from Lc) and the persistent/cluster ones (from Lp)
@@ -1413,6 +1477,121 @@ static bool invert(std::vector<double>& a, int n) {
     }
     a.swap(inv);
     return true;
+}
+
+// The dense operator of level l (spacings dx 2^l, dy 2^l) on its free nodes:
+// not Dirichlet, not on the grid edges (in r-z geometry the axis row is free).
+// idx lists the free nodes in row-major order; bw is the largest distance
+// between a row and the column of one of its couplings.  With more than
+// max_n free nodes only idx is filled.
+static std::vector<double> dense_operator(const MgImpl& M, int l, int nx, int ny, const std::vector<uint8_t>& mask,
+                                          std::vector<int>& idx, int& bw, int max_n) {
+    std::vector<int> where(size_t(nx) * ny, -1);
+    idx.clear();
+    for (int j = M.rz ? 0 : 1; j < ny - 1; ++j)
+        for (int i = 1; i < nx - 1; ++i)
+            if (!mask[size_t(j) * nx + i]) {
+                where[size_t(j) * nx + i] = int(idx.size());
+                idx.push_back(j * nx + i);
+            }
+    const int n = int(idx.size());
+    bw = 0;
+    if (n > max_n) return {};
+    const double hx = M.dx * double(1 << l), hy = M.dy * double(1 << l);
+    const double ccx = 1.0 / (hx * hx), ccy = 1.0 / (hy * hy);
+    const std::vector<double> rows = M.rz ? rz_rows(ny, hx, hy) : std::vector<double>();
+    std::vector<double> A(size_t(n) * n, 0.0);
+    for (int a = 0; a < n; ++a) {
+        const int k = idx[a], j = k / nx;
+        const double wn = M.rz ? rows[4 * j] : ccy, ws = M.rz ? rows[4 * j + 1] : ccy;
+        A[size_t(a) * n + a] = -(2.0 * ccx + wn + ws);
+        const int nb[4] = {k - 1, k + 1, j > 0 ? k - nx : -1, k + nx};
+        const double w[4] = {ccx, ccx, ws, wn};
+        for (int q = 0; q < 4; ++q) {
+            const int b = nb[q] >= 0 ? where[nb[q]] : -1;
+            if (b >= 0) {
+                A[size_t(a) * n + b] += w[q];
+                bw = std::max(bw, std::abs(b - a));
+            }
+        }
+    }
+    return A;
+}
+
+// Inverse of a band matrix (every coupling within bw of the diagonal) by LU
+// factorisation without pivoting, then one forward and one back substitution
+// per column of the identity: O(n bw^2 + n^2 bw).  The level operators are
+// M-matrices (weakly diagonally dominant, dominant on the rows next to a
+// Dirichlet node), for which elimination without pivoting is stable.
+static bool band_inverse(std::vector<double>& a, int n, int bw) {
+    auto A = [&](int r, int c) -> double& { return a[size_t(r) * n + c]; };
+    for (int k = 0; k < n; ++k) {
+        const double p = A(k, k);
+        if (!(std::fabs(p) > 1e-300)) return false;
+        const int last = std::min(n - 1, k + bw);
+        for (int r = k + 1; r <= last; ++r) {
+            const double m = A(r, k) / p;
+            if (m == 0.0) continue;
+            A(r, k) = m;
+            for (int c = k + 1; c <= last; ++c) A(r, c) -= m * A(k, c);
+        }
+    }
+    std::vector<double> inv(size_t(n) * n), x(n);
+    for (int col = 0; col < n; ++col) {
+        // L y = e_col (unit lower triangle; y is zero above col)
+        std::fill(x.begin(), x.end(), 0.0);
+        x[col] = 1.0;
+        for (int i = col + 1; i < n; ++i) {
+            double s = 0.0;
+            for (int k = std::max(col, i - bw); k < i; ++k) s += A(i, k) * x[k];
+            x[i] = -s;
+        }
+        // U x = y
+        for (int i = n - 1; i >= 0; --i) {
+            double s = x[i];
+            const int last = std::min(n - 1, i + bw);
+            for (int k = i + 1; k <= last; ++k) s -= A(i, k) * x[k];
+            x[i] = s / A(i, i);
+        }
+        for (int i = 0; i < n; ++i) inv[size_t(i) * n + col] = x[i];
+    }
+    a.swap(inv);
+    return true;
+}
+
+// The direct solve of level Lc (see k_mg_direct); left off (the coarse
+// V-cycle kernel runs) when the level has no free node or too many.
+static int configure_direct(MgImpl& M, const std::vector<int>& nxs, const std::vector<int>& nys,
+                            const std::vector<std::vector<uint8_t>>& masks) {
+    const int l = M.Lc, nx = nxs[l], ny = nys[l];
+    std::vector<int> idx;
+    int bw = 0;
+    std::vector<double> A = dense_operator(M, l, nx, ny, masks[l], idx, bw, kDirectMaxFree);
+    const int n = int(idx.size());
+    if (n == 0 || n > kDirectMaxFree) return PIC_OK;
+    if (!band_inverse(A, n, bw)) return fail(PIC_ERR_NUMERIC, "pic_mg_create: singular coarse system");
+    std::vector<char> fr(size_t(nx) * ny, 0);
+    for (int k : idx) fr[k] = 1;
+    std::vector<int> all(idx);
+    for (int k = 0; k < nx * ny; ++k)
+        if (!fr[k]) all.push_back(k);
+    const bool f32 = M.precision == PIC_MG_MIXED;
+    const size_t bytes = A.size() * (f32 ? sizeof(float) : sizeof(double));
+    PIC_CUDA(cudaMalloc(&M.dinv, bytes));
+    M.allocs.push_back(M.dinv);
+    if (f32) {
+        const std::vector<float> af(A.begin(), A.end());
+        PIC_CUDA(cudaMemcpy(M.dinv, af.data(), bytes, cudaMemcpyHostToDevice));
+    } else {
+        PIC_CUDA(cudaMemcpy(M.dinv, A.data(), bytes, cudaMemcpyHostToDevice));
+    }
+    PIC_CUDA(cudaMalloc(&M.didx, all.size() * sizeof(int)));
+    M.allocs.push_back(M.didx);
+    PIC_CUDA(cudaMemcpy(M.didx, all.data(), all.size() * sizeof(int), cudaMemcpyHostToDevice));
+    M.dn = n;
+    M.dnz = int(all.size()) - n;
+    M.direct = true;
+    return PIC_OK;
 }
 
 template <class T>
@@ -1669,33 +1848,13 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
                          ny, coarse_max));
     const int ncx = nxs.back(), ncy = nys.back();
     std::vector<int> idx;
-    std::vector<int> where(size_t(ncx) * ncy, -1);
-    for (int j = M.rz ? 0 : 1; j < ncy - 1; ++j)
-        for (int i = 1; i < ncx - 1; ++i)
-            if (!masks.back()[size_t(j) * ncx + i]) {
-                where[size_t(j) * ncx + i] = int(idx.size());
-                idx.push_back(j * ncx + i);
-            }
+    int bw = 0;
+    std::vector<double> A = dense_operator(M, M.L - 1, ncx, ncy, masks.back(), idx, bw, 4096);
     M.nfree_c = int(idx.size());
     if (M.nfree_c > 4096)
         return bail(fail(PIC_ERR_BAD_ARG, "pic_mg_create: coarsest level %dx%d has %d unknowns", ncx, ncy, M.nfree_c));
     if (M.nfree_c > 0) {
-        const double hx = dx * double(1 << (M.L - 1)), hy = dy * double(1 << (M.L - 1));
-        const double ccx = 1.0 / (hx * hx), ccy = 1.0 / (hy * hy);
-        const std::vector<double> rows = M.rz ? rz_rows(ncy, hx, hy) : std::vector<double>();
         const int n = M.nfree_c;
-        std::vector<double> A(size_t(n) * n, 0.0);
-        for (int a = 0; a < n; ++a) {
-            const int k = idx[a], j = k / ncx;
-            const double wn = M.rz ? rows[4 * j] : ccy, ws = M.rz ? rows[4 * j + 1] : ccy;
-            A[size_t(a) * n + a] = -(2.0 * ccx + wn + ws);
-            const int nb[4] = {k - 1, k + 1, j > 0 ? k - ncx : -1, k + ncx};
-            const double w[4] = {ccx, ccx, ws, wn};
-            for (int q = 0; q < 4; ++q) {
-                const int b = nb[q] >= 0 ? where[nb[q]] : -1;
-                if (b >= 0) A[size_t(a) * n + b] += w[q];
-            }
-        }
         if (!invert(A, n)) return bail(fail(PIC_ERR_NUMERIC, "pic_mg_create: singular coarsest system"));
         // padded to 16 bytes: the coarse kernel reads both in 16-byte words
         const size_t ab = (A.size() * sizeof(double) + 15) / 16 * 16, cb = (idx.size() * sizeof(int) + 15) / 16 * 16;
@@ -1747,6 +1906,9 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
         if (edges_only && pow2) st = dst_create(nx, ny, dx, dy, &M.dst);
         if (st == PIC_OK && !M.dst) M.o.launch_mode = PIC_MG_GRAPH_LOOP;
     }
+    if (st == PIC_OK && M.Lc >= 1 &&
+        (M.o.launch_mode == PIC_MG_GRAPH_LOOP || M.o.launch_mode == PIC_MG_HOST_LOOP))
+        st = configure_direct(M, nxs, nys, masks);
     if (st != PIC_OK) return bail(st);
     M.grd0 = dim3(div_up(nx, M.blk0.x), div_up(ny, M.blk0.y * kR0Rows));
     // block partials of the residual norm: one pair per block of the level-0
@@ -1833,7 +1995,12 @@ static int launch_cycle(MgImpl& M, std::vector<LevelDev<T>>& lv_in, double* phi,
             ++count;
         }
     }
-    if (!hyb) {
+    if (!hyb && M.direct) {
+        const DirectDesc<T> D{static_cast<const T*>(M.dinv), M.didx, M.didx + M.dn, lv[M.Lc].g, lv[M.Lc].e, M.dn,
+                              M.dnz};
+        launch_pdl(k_mg_direct<T>, dim3(div_up(M.dn, kDirectRows)), dim3(kDirectRows * 32), 0, st, D);
+        ++count;
+    } else if (!hyb) {
         CoarseDesc<T> D{};
         fill_coarse(M, M.cl[0], lv, phi, D);
         if (M.rz) launch_pdl(k_mg_coarse<T, true>, dim3(1), dim3(kCoarseThreads), M.cl[0].smem, st, D);
