@@ -72,6 +72,29 @@ struct LevelDev {
     const T* rz;
 };
 
+// The residual norm and the loop decision: block partials, the counter of
+// blocks finished, and the solve's state.
+struct NormState {
+    double* partial;   // [nblocks] r^2, then [nblocks] f^2
+    unsigned* done;    // blocks finished
+    double* norms;     // [||f||^2, ||r||^2]
+    int* converged;
+    int* cycles;       // V-cycles of the current solve
+    long long* total;  // V-cycles since creation
+};
+
+// The finest up phase fused with the FP64 residual (k_mg_up_res).
+struct ResArgs {
+    double* r64;        // the residual of phi, FP64, kept between cycles
+    const double* rz0;  // r-z: level-0 row coefficients in FP64, else null
+    double cx, cy;
+    NormState N;
+    double tol2;
+    int max_cycles;
+    cudaGraphConditionalHandle cond;
+    int use_cond;
+};
+
 // The levels as a launch mode uses them: up phases on the levels below
 // `first_coarse` (their final correction is eu), the coarse V-cycle from it.
 template <class T>
@@ -130,9 +153,11 @@ template <int S>
 struct DownGeom {
     static constexpr int H = 2 * S + 2, W = kMgTile + 2 * H;
 };
-template <int S>
+// RES: the finest up phase fused with the residual, one more halo row so that
+// e is final one node beyond the core.
+template <int S, bool RES = false>
 struct UpGeom {
-    static constexpr int H = 2 * S, W = kMgTile + 2 * H, CW = W / 2 + 2;
+    static constexpr int H = 2 * S + (RES ? 1 : 0), W = kMgTile + 2 * H, CW = W / 2 + 2;
 };
 
 // One red or black half-sweep over the nodes 1..W-2 of a W x W shared tile;
@@ -166,12 +191,14 @@ __device__ __forceinline__ void tile_half_sweep(T* __restrict__ se, const T* __r
 }
 
 // Loads level L over the W x W region at (ox, oy): mask (edges and outside
-// the grid count as Dirichlet; in r-z geometry the axis row is free), g, e
-// (zero, or the stored correction on free nodes) and, in r-z geometry, the
-// row coefficients of the W rows (zero outside the grid).
+// the grid count as Dirichlet; in r-z geometry the axis row is free), g (from
+// g64, the FP64 residual, when given), e (zero, or the stored correction on
+// free nodes) and, in r-z geometry, the row coefficients of the W rows (zero
+// outside the grid).
 template <class T, int W, bool LOAD_E, bool CYL>
 __device__ __forceinline__ void tile_load(const LevelDev<T>& L, int ox, int oy, T* __restrict__ se,
-                                          T* __restrict__ sg, uint8_t* __restrict__ sm, T* __restrict__ srz) {
+                                          T* __restrict__ sg, uint8_t* __restrict__ sm, T* __restrict__ srz,
+                                          const double* __restrict__ g64 = nullptr) {
     constexpr int N = W * W, IT = (N + kMgThreads - 1) / kMgThreads;
     uint8_t mk[IT];
     T gv[IT], ev[IT];
@@ -182,7 +209,7 @@ __device__ __forceinline__ void tile_load(const LevelDev<T>& L, int ox, int oy, 
         const bool in = q < N && i >= 0 && j >= 0 && i < L.nx && j < L.ny;
         const long k = long(j) * L.nx + i;
         mk[it] = in ? L.mask[k] : uint8_t(1);
-        gv[it] = in ? L.g[k] : T(0);
+        gv[it] = in ? (g64 ? T(g64[k]) : L.g[k]) : T(0);
         ev[it] = (LOAD_E && in) ? L.e[k] : T(0);
     }
     if constexpr (CYL) {
@@ -203,9 +230,12 @@ __device__ __forceinline__ void tile_load(const LevelDev<T>& L, int ox, int oy, 
     }
 }
 
+// g64 (level 0 of the graph and host loops): the right-hand side is the FP64
+// residual, and the tile stores its FP32 copy of the core to F.g for the up
+// phase of the same cycle.
 template <class T, int S, bool CYL = false>
 __device__ void down_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, int tx, int ty,
-                          unsigned char* smem) {
+                          unsigned char* smem, const double* __restrict__ g64 = nullptr) {
     constexpr int H = DownGeom<S>::H, W = DownGeom<S>::W, hx = kMgTile / 2;
     static_assert(hx * hx <= kMgThreads, "one coarse node per thread");
     T* se = reinterpret_cast<T*>(smem);
@@ -220,7 +250,7 @@ __device__ void down_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, 
     const bool own = tid < hx * hx && I < Cc.nx && J < Cc.ny;
     const long K = long(J) * Cc.nx + I;
     const bool cdir = own && (I == 0 || (!CYL && J == 0) || I == Cc.nx - 1 || J == Cc.ny - 1 || Cc.mask[K]);
-    tile_load<T, W, false, CYL>(F, ox, oy, se, sg, sm, srz);
+    tile_load<T, W, false, CYL>(F, ox, oy, se, sg, sm, srz, g64);
     __syncthreads();
     // global red nodes have (i + j) even; locally (li + lj + ox + oy) even
     const int par0 = (ox + oy) & 1;
@@ -234,7 +264,10 @@ __device__ void down_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, 
 #pragma unroll
     for (int q = tid; q < kMgTile * kMgTile; q += kMgThreads) {
         const int i = x0 + q % kMgTile, j = y0 + q / kMgTile;
-        if (i < F.nx && j < F.ny) F.e[long(j) * F.nx + i] = se[(H + q / kMgTile) * W + H + q % kMgTile];
+        if (i >= F.nx || j >= F.ny) continue;
+        const int lq = (H + q / kMgTile) * W + H + q % kMgTile;
+        F.e[long(j) * F.nx + i] = se[lq];
+        if (g64) F.g[long(j) * F.nx + i] = sg[lq];
     }
     // residual in place of g (each node reads only its own g)
     constexpr int IT = (W * W + kMgThreads - 1) / kMgThreads;
@@ -276,17 +309,21 @@ __device__ void down_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, 
 }
 
 template <class T, int S, bool CYL>
-__global__ void __launch_bounds__(kMgThreads) k_mg_down(LevelDev<T> F, LevelDev<T> Cc, T omega) {
+__global__ void __launch_bounds__(kMgThreads) k_mg_down(LevelDev<T> F, LevelDev<T> Cc, T omega,
+                                                        const double* __restrict__ g64) {
     extern __shared__ __align__(16) unsigned char smem[];
     pdl_wait();
     pdl_trigger();
-    down_tile<T, S, CYL>(F, Cc, omega, blockIdx.x, blockIdx.y, smem);
+    down_tile<T, S, CYL>(F, Cc, omega, blockIdx.x, blockIdx.y, smem, g64);
 }
 
-template <class T, int S, bool CYL = false, bool PDL = false>
-__device__ void up_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, double* __restrict__ phi, int tx,
-                        int ty, unsigned char* smem) {
-    constexpr int H = UpGeom<S>::H, W = UpGeom<S>::W, CW = UpGeom<S>::CW;
+// RES (level 0 only): also r -= A e in FP64 on the core's free nodes (R->r64,
+// the residual of phi before the cycle, becomes the residual after it);
+// returns the tile's sum of r^2 (0 without RES).
+template <class T, int S, bool CYL = false, bool PDL = false, bool RES = false>
+__device__ double up_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, double* __restrict__ phi, int tx,
+                          int ty, unsigned char* smem, const ResArgs* R = nullptr) {
+    constexpr int H = UpGeom<S, RES>::H, W = UpGeom<S, RES>::W, CW = UpGeom<S, RES>::CW;
     constexpr int CIT = (CW * CW + kMgThreads - 1) / kMgThreads;
     constexpr int OIT = (kMgTile * kMgTile + kMgThreads - 1) / kMgThreads;
     T* se = reinterpret_cast<T*>(smem);
@@ -298,12 +335,14 @@ __device__ void up_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, do
     const int ox = x0 - H, oy = y0 - H;
     const int cox = ox >> 1, coy = oy >> 1;  // floor for negative origins
     const int tid = threadIdx.x;
-    double pv[OIT];
+    double pv[OIT], rv[RES ? OIT : 1];
 #pragma unroll
     for (int it = 0; it < OIT; ++it) {
         const int q = it * kMgThreads + tid;
         const int i = x0 + q % kMgTile, j = y0 + q / kMgTile;
-        pv[it] = (phi && i < F.nx && j < F.ny) ? phi[long(j) * F.nx + i] : 0.0;
+        const bool in = q < kMgTile * kMgTile && i < F.nx && j < F.ny;
+        pv[it] = (phi && in) ? phi[long(j) * F.nx + i] : 0.0;
+        if constexpr (RES) rv[it] = in ? R->r64[long(j) * F.nx + i] : 0.0;
     }
     tile_load<T, W, true, CYL>(F, ox, oy, se, sg, sm, srz);
     if constexpr (PDL) {
@@ -349,17 +388,36 @@ __device__ void up_tile(const LevelDev<T>& F, const LevelDev<T>& Cc, T omega, do
             tile_half_sweep<T, W, CYL>(se, sg, sm, color ^ par0, F.cx, F.cy, F.inv_diag, omega, srz);
             __syncthreads();
         }
+    double r2 = 0.0;
 #pragma unroll
     for (int it = 0; it < OIT; ++it) {
         const int q = it * kMgThreads + tid;
         const int i = x0 + q % kMgTile, j = y0 + q / kMgTile;
         if (q >= kMgTile * kMgTile || i >= F.nx || j >= F.ny) continue;
         const long k = long(j) * F.nx + i;
-        const T v = se[(H + q / kMgTile) * W + H + q % kMgTile];
+        const int lq = (H + q / kMgTile) * W + H + q % kMgTile;
+        const T v = se[lq];
         if (phi) phi[k] = pv[it] + double(v);
         else F.ec[k] = v;
+        if constexpr (RES) {
+            if (!sm[lq]) {
+                // the change of the FP64 residual, f - A(phi + e) = r - A e, in
+                // the association of k_mg_r0's Laplacian
+                const double c = double(v), w = double(se[lq - 1]), e = double(se[lq + 1]);
+                const double sv = double(se[lq - W]), nv = double(se[lq + W]);
+                double lap;
+                if constexpr (CYL)
+                    lap = R->cx * ((w - c) + (e - c)) + R->rz0[4 * j] * (nv - c) + R->rz0[4 * j + 1] * (sv - c);
+                else
+                    lap = R->cx * ((w - c) + (e - c)) + R->cy * ((sv - c) + (nv - c));
+                const double r = rv[it] - lap;
+                R->r64[k] = r;
+                r2 += r * r;
+            }
+        }
     }
     __syncthreads();  // the caller may reuse the shared tile
+    return r2;
 }
 
 template <class T, int S, bool CYL>
@@ -367,6 +425,99 @@ __global__ void __launch_bounds__(kMgThreads) k_mg_up(LevelDev<T> F, LevelDev<T>
                                                       double* __restrict__ phi) {
     extern __shared__ __align__(16) unsigned char smem[];
     up_tile<T, S, CYL, true>(F, Cc, omega, phi, blockIdx.x, blockIdx.y, smem);
+}
+
+// Sums (a, b) over the grid: block partials into N.partial; the last block to
+// finish adds them in a fixed order (the same decision on every run) and
+// takes the loop decision: initial (first residual of a solve) records
+// ||f||^2 = b and zeroes the cycle count, else counts a V-cycle; converged
+// when ||r||^2 = a < tol2 ||f||^2; the WHILE node's condition (use_cond) is
+// to go on while neither converged nor at max_cycles.
+__device__ void norm_reduce_decide(double a, double b, const NormState& N, double tol2, int max_cycles, int initial,
+                                   cudaGraphConditionalHandle cond, int use_cond) {
+    __shared__ double ws[2][32];
+    __shared__ bool last;
+    const int t = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y, nw = nt >> 5;
+    const int lane = t & 31, w = t >> 5;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    if (lane == 0) {
+        ws[0][w] = a;
+        ws[1][w] = b;
+    }
+    __syncthreads();
+    const int nb = gridDim.x * gridDim.y, bid = blockIdx.y * gridDim.x + blockIdx.x;
+    if (w == 0) {
+        // the block's sums: a warp reduction of the warps' sums (lane 0's value)
+        double sa = lane < nw ? ws[0][lane] : 0.0, sb = lane < nw ? ws[1][lane] : 0.0;
+        sa = warp_sum(sa);
+        sb = warp_sum(sb);
+        if (lane == 0) {
+            N.partial[bid] = sa;
+            N.partial[nb + bid] = sb;
+            cuda::atomic_ref<unsigned, cuda::thread_scope_device> done(*N.done);
+            last = done.fetch_add(1u, cuda::memory_order_acq_rel) == unsigned(nb - 1);
+        }
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // the solve's state and every block partial, loaded together
+    int cyc = 0;
+    long long tot = 0;
+    double ref0 = 0.0;
+    if (t == 0) {
+        cyc = *reinterpret_cast<volatile int*>(N.cycles);
+        tot = *reinterpret_cast<volatile long long*>(N.total);
+        ref0 = *reinterpret_cast<volatile double*>(N.norms);
+    }
+    const volatile double* P = N.partial;
+    double sa = 0.0, sb = 0.0;
+    for (int q = t; q < nb; q += nt) {
+        sa += P[q];
+        sb += P[nb + q];
+    }
+    sa = warp_sum(sa);
+    sb = warp_sum(sb);
+    __syncthreads();
+    if (lane == 0) {
+        ws[0][w] = sa;
+        ws[1][w] = sb;
+    }
+    __syncthreads();
+    if (w == 0) {
+        double r2 = lane < nw ? ws[0][lane] : 0.0, f2 = lane < nw ? ws[1][lane] : 0.0;
+        r2 = warp_sum(r2);
+        f2 = warp_sum(f2);
+        if (lane == 0) {
+            if (initial) {
+                ref0 = f2;
+                N.norms[0] = f2;
+                cyc = 0;
+            } else {
+                cyc += 1;
+                *N.total = tot + 1;
+            }
+            *N.cycles = cyc;
+            N.norms[1] = r2;
+            const int conv = r2 < tol2 * (ref0 > 0.0 ? ref0 : 1.0);
+            *N.converged = conv;
+            const int cont = !conv && cyc < max_cycles;
+            if (use_cond) cudaGraphSetConditional(cond, cont ? 1u : 0u);
+            *N.done = 0u;
+        }
+    }
+}
+
+// The finest up phase of a graph- or host-loop V-cycle fused with the FP64
+// residual and the loop decision of k_mg_r0: phi += e, r -= A e on the core,
+// then the norm of r.
+template <class T, int S, bool CYL>
+__global__ void __launch_bounds__(kMgThreads) k_mg_up_res(LevelDev<T> F, LevelDev<T> Cc, T omega,
+                                                          double* __restrict__ phi, ResArgs R) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const double r2 = up_tile<T, S, CYL, true, true>(F, Cc, omega, phi, blockIdx.x, blockIdx.y, smem, &R);
+    norm_reduce_decide(r2, 0.0, R.N, R.tol2, R.max_cycles, 0, R.cond, R.use_cond);
 }
 
 // Runtime sweep counts (the persistent kernel) dispatched to the instances.
@@ -401,9 +552,11 @@ __device__ void up_tile_n(int post, const LevelDev<T>& F, const LevelDev<T>& Cc,
 }
 
 template <class T>
-using DownKernel = void (*)(LevelDev<T>, LevelDev<T>, T);
+using DownKernel = void (*)(LevelDev<T>, LevelDev<T>, T, const double*);
 template <class T>
 using UpKernel = void (*)(LevelDev<T>, LevelDev<T>, T, double*);
+template <class T>
+using UpResKernel = void (*)(LevelDev<T>, LevelDev<T>, T, double*, ResArgs);
 
 template <class T, bool CYL>
 static DownKernel<T> down_kernel(int s) {
@@ -422,6 +575,15 @@ static UpKernel<T> up_kernel(int s) {
     return k[s];
 }
 
+template <class T, bool CYL>
+static UpResKernel<T> up_res_kernel(int s) {
+    static const UpResKernel<T> k[kMgMaxSweeps + 1] = {
+        nullptr,                  k_mg_up_res<T, 1, CYL>, k_mg_up_res<T, 2, CYL>, k_mg_up_res<T, 3, CYL>,
+        k_mg_up_res<T, 4, CYL>,   k_mg_up_res<T, 5, CYL>, k_mg_up_res<T, 6, CYL>, k_mg_up_res<T, 7, CYL>,
+        k_mg_up_res<T, 8, CYL>};
+    return k[s];
+}
+
 template <class T>
 static size_t down_smem(int s, bool cyl = false) {
     const size_t W = kMgTile + 2 * (2 * s + 2);
@@ -429,8 +591,8 @@ static size_t down_smem(int s, bool cyl = false) {
 }
 
 template <class T>
-static size_t up_smem(int s, bool cyl = false) {
-    const size_t W = kMgTile + 2 * (2 * s), CW = W / 2 + 2;
+static size_t up_smem(int s, bool cyl = false, bool res = false) {
+    const size_t W = kMgTile + 2 * (2 * s + (res ? 1 : 0)), CW = W / 2 + 2;
     return W * W * (2 * sizeof(T) + 1) + CW * CW * sizeof(T) + (cyl ? 4 * W * sizeof(T) : 0);
 }
 
@@ -675,25 +837,18 @@ __global__ void __launch_bounds__(kDirectRows * 32) k_mg_direct(DirectDesc<T> D)
 
 // ---- FP64 residual, norms and the loop decision -----------------------------------
 
-struct NormState {
-    double* partial;   // [nblocks] r^2, then [nblocks] f^2
-    unsigned* done;    // blocks finished
-    double* norms;     // [||f||^2, ||r||^2]
-    int* converged;
-    int* cycles;       // V-cycles of the current solve
-    long long* total;  // V-cycles since creation
-};
 
 constexpr int kR0Rows = 4;  // rows per thread of the residual kernel
 
 // rz0: in r-z geometry the level-0 row coefficients in FP64 ({wN, wS, 1/diag,
-// D} per row, as LevelDev::rz), else null.
+// D} per row, as LevelDev::rz), else null.  The residual goes to g0 (the
+// V-cycle's precision) and, when given, to r64 in FP64.
 template <class T, bool CYL>
 __global__ void __launch_bounds__(256) k_mg_r0(const double* __restrict__ phi, const double* __restrict__ f,
                                                const uint8_t* __restrict__ mask, int nx, int ny, double cx, double cy,
                                                T* __restrict__ g0, NormState N, double tol2, int max_cycles,
                                                int initial, cudaGraphConditionalHandle cond, int use_cond,
-                                               const double* __restrict__ rz0) {
+                                               const double* __restrict__ rz0, double* __restrict__ r64) {
     // a 32 x 8 block covers 32 x 32 nodes, four rows per thread, every load
     // of a thread issued before the first is used
     pdl_wait();
@@ -732,67 +887,9 @@ __global__ void __launch_bounds__(256) k_mg_r0(const double* __restrict__ phi, c
         }
         r += ru * ru;
         g0[long(j) * nx + i] = T(ru);
+        if (r64) r64[long(j) * nx + i] = ru;
     }
-    __shared__ double ws[2][8];
-    __shared__ bool last;
-    const int t = threadIdx.y * blockDim.x + threadIdx.x;
-    double a = warp_sum(r), b = warp_sum(fv);
-    if ((t & 31) == 0) {
-        ws[0][t >> 5] = a;
-        ws[1][t >> 5] = b;
-    }
-    __syncthreads();
-    const int nb = gridDim.x * gridDim.y, bid = blockIdx.y * gridDim.x + blockIdx.x;
-    if (t == 0) {
-        double sa = 0.0, sb = 0.0;
-        for (int w = 0; w < 8; ++w) {
-            sa += ws[0][w];
-            sb += ws[1][w];
-        }
-        N.partial[bid] = sa;
-        N.partial[nb + bid] = sb;
-        __threadfence();
-        last = atomicAdd(N.done, 1u) == unsigned(nb - 1);
-    }
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    // deterministic sum of the block partials: fixed stride per thread, fixed tree
-    const volatile double* P = N.partial;
-    double sa = 0.0, sb = 0.0;
-    for (int q = t; q < nb; q += 256) {
-        sa += P[q];
-        sb += P[nb + q];
-    }
-    sa = warp_sum(sa);
-    sb = warp_sum(sb);
-    __syncthreads();
-    if ((t & 31) == 0) {
-        ws[0][t >> 5] = sa;
-        ws[1][t >> 5] = sb;
-    }
-    __syncthreads();
-    if (t == 0) {
-        double r2 = 0.0, f2 = 0.0;
-        for (int w = 0; w < 8; ++w) {
-            r2 += ws[0][w];
-            f2 += ws[1][w];
-        }
-        if (initial) {
-            N.norms[0] = f2;
-            *N.cycles = 0;
-        } else {
-            *N.cycles += 1;
-            *N.total += 1;
-        }
-        N.norms[1] = r2;
-        const double ref = N.norms[0] > 0.0 ? N.norms[0] : 1.0;
-        const int conv = r2 < tol2 * ref;
-        *N.converged = conv;
-        const int cont = !conv && *N.cycles < max_cycles;
-        if (use_cond) cudaGraphSetConditional(cond, cont ? 1u : 0u);
-        *N.done = 0u;
-    }
+    norm_reduce_decide(r, fv, N, tol2, max_cycles, initial, cond, use_cond);
 }
 
 // ---- persistent cooperative solve -------------------------------------------------
@@ -1343,6 +1440,7 @@ struct MgImpl {
     void* dinv = nullptr;  // [dn][dn] in the V-cycle's precision
     int* didx = nullptr;   // dn free nodes, then dnz others
     int dn = 0, dnz = 0;
+    double* r64 = nullptr;  // FP64 residual of phi between the cycles of a graph- or host-loop solve
     NormState N{};
     dim3 blk0{32, 8}, grd0;
     CoarseLayout cl[2];  // the coarse kernel's levels (from Lc) and the persistent/cluster ones (from Lp)
@@ -1597,17 +1695,20 @@ static int configure_direct(MgImpl& M, const std::vector<int>& nxs, const std::v
 template <class T>
 static int configure_kernels(MgImpl& M) {
     const size_t down = down_smem<T>(M.o.pre_sweeps, M.rz), up = up_smem<T>(M.o.post_sweeps, M.rz);
-    if (down > 227 * 1024 || up > 227 * 1024 || M.cl[0].smem > 227 * 1024 || M.cl[1].smem > 227 * 1024)
+    const size_t upr = up_smem<T>(M.o.post_sweeps, M.rz, true);
+    if (down > 227 * 1024 || upr > 227 * 1024 || M.cl[0].smem > 227 * 1024 || M.cl[1].smem > 227 * 1024)
         return fail(PIC_ERR_BAD_ARG, "multigrid: shared memory too large (sweeps %d/%d)", M.o.pre_sweeps,
                     M.o.post_sweeps);
     if (M.rz) {
         PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(down_kernel<T, true>(M.o.pre_sweeps)), down));
         PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(up_kernel<T, true>(M.o.post_sweeps)), up));
+        PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(up_res_kernel<T, true>(M.o.post_sweeps)), upr));
         PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(k_mg_coarse<T, true>), M.cl[0].smem));
         return PIC_OK;  // r-z solves use the graph and host loops only
     }
     PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(down_kernel<T, false>(M.o.pre_sweeps)), down));
     PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(up_kernel<T, false>(M.o.post_sweeps)), up));
+    PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(up_res_kernel<T, false>(M.o.post_sweeps)), upr));
     PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(k_mg_coarse<T, false>), M.cl[0].smem));
     M.solve_smem = std::max(std::max(down, up), M.cl[1].smem);
     PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(k_mg_solve<T>), M.solve_smem));
@@ -1912,11 +2013,17 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
     if (st != PIC_OK) return bail(st);
     M.grd0 = dim3(div_up(nx, M.blk0.x), div_up(ny, M.blk0.y * kR0Rows));
     // block partials of the residual norm: one pair per block of the level-0
-    // tiling (k_mg_r0) or of the persistent grid (k_mg_solve), whichever is larger
-    const int nb = std::max(int(M.grd0.x * M.grd0.y), M.solve_grid);
+    // tiling (k_mg_r0, k_mg_up_res) or of the persistent grid (k_mg_solve),
+    // whichever is larger
+    const int nb = std::max(std::max(int(M.grd0.x * M.grd0.y), div_up(nx, kMgTile) * div_up(ny, kMgTile)),
+                            M.solve_grid);
     if (cudaMalloc(&M.N.partial, sizeof(double) * 2 * nb) != cudaSuccess)
         return bail(fail(PIC_ERR_CUDA, "pic_mg_create: out of device memory"));
     M.allocs.push_back(M.N.partial);
+    if (cudaMalloc(&M.r64, sizeof(double) * size_t(nx) * ny) != cudaSuccess)
+        return bail(fail(PIC_ERR_CUDA, "pic_mg_create: out of device memory"));
+    M.allocs.push_back(M.r64);
+    cudaMemset(M.r64, 0, sizeof(double) * size_t(nx) * ny);
     char* small = nullptr;
     if (cudaMalloc(&small, 256) != cudaSuccess) return bail(fail(PIC_ERR_CUDA, "pic_mg_create: out of device memory"));
     M.allocs.push_back(small);
@@ -1963,13 +2070,17 @@ static void launch_r0(MgImpl& M, const std::vector<LevelDev<T>>& lv, double* phi
     const double* nul = nullptr;
     if (M.rz)
         launch_pdl(k_mg_r0<T, true>, M.grd0, M.blk0, 0, st, phi, f, lv[0].mask, M.nx, M.ny, cx, cy, lv[0].g, M.N,
-                   tol * tol, max_cycles, initial, cond, use_cond, (const double*)M.rz0);
+                   tol * tol, max_cycles, initial, cond, use_cond, (const double*)M.rz0, M.r64);
     else
         launch_pdl(k_mg_r0<T, false>, M.grd0, M.blk0, 0, st, phi, f, lv[0].mask, M.nx, M.ny, cx, cy, lv[0].g, M.N,
-                   tol * tol, max_cycles, initial, cond, use_cond, nul);
+                   tol * tol, max_cycles, initial, cond, use_cond, nul, M.r64);
 }
 
-// One V-cycle followed by the residual check, launched on stream st.
+// One V-cycle followed by the residual check, launched on stream st.  With
+// tile levels, the finest down phase reads the FP64 residual (r64, from
+// k_mg_r0 or the previous cycle) and the finest up phase updates it and takes
+// the loop decision (k_mg_up_res); a cycle of the coarse kernel alone ends
+// with k_mg_r0.
 template <class T>
 static int launch_cycle(MgImpl& M, std::vector<LevelDev<T>>& lv_in, double* phi, const double* f, double tol,
                         int max_cycles, cudaGraphConditionalHandle cond, int use_cond, cudaStream_t st, int& count) {
@@ -1986,7 +2097,8 @@ static int launch_cycle(MgImpl& M, std::vector<LevelDev<T>>& lv_in, double* phi,
     count = 0;
     for (int l = 0; l < Ltile; ++l) {
         const dim3 g(div_up(lv[l].nx, kMgTile), div_up(lv[l].ny, kMgTile));
-        launch_pdl(kdown, g, dim3(kMgThreads), down, st, lv[l], lv[l + 1], omega);
+        launch_pdl(kdown, g, dim3(kMgThreads), down, st, lv[l], lv[l + 1], omega,
+                   l == 0 ? (const double*)M.r64 : nullptr);
         ++count;
     }
     if constexpr (std::is_same<T, float>::value) {
@@ -2007,12 +2119,30 @@ static int launch_cycle(MgImpl& M, std::vector<LevelDev<T>>& lv_in, double* phi,
         else launch_pdl(k_mg_coarse<T, false>, dim3(1), dim3(kCoarseThreads), M.cl[0].smem, st, D);
         ++count;
     }
-    for (int l = Ltile - 1; l >= 0; --l) {
+    for (int l = Ltile - 1; l >= 1; --l) {
         const dim3 g(div_up(lv[l].nx, kMgTile), div_up(lv[l].ny, kMgTile));
-        launch_pdl(kup, g, dim3(kMgThreads), up, st, lv[l], lv[l + 1], omega, l == 0 ? phi : (double*)nullptr);
+        launch_pdl(kup, g, dim3(kMgThreads), up, st, lv[l], lv[l + 1], omega, (double*)nullptr);
         ++count;
     }
-    launch_r0(M, lv, phi, f, tol, max_cycles, 0, cond, use_cond, st);
+    if (Ltile >= 1) {
+        ResArgs R{};
+        R.r64 = M.r64;
+        R.rz0 = M.rz ? (const double*)M.rz0 : nullptr;
+        R.cx = 1.0 / (M.dx * M.dx);
+        R.cy = 1.0 / (M.dy * M.dy);
+        R.N = M.N;
+        R.tol2 = tol * tol;
+        R.max_cycles = max_cycles;
+        R.cond = cond;
+        R.use_cond = use_cond;
+        const UpResKernel<T> kres =
+            M.rz ? up_res_kernel<T, true>(M.o.post_sweeps) : up_res_kernel<T, false>(M.o.post_sweeps);
+        const dim3 g(div_up(lv[0].nx, kMgTile), div_up(lv[0].ny, kMgTile));
+        launch_pdl(kres, g, dim3(kMgThreads), up_smem<T>(M.o.post_sweeps, M.rz, true), st, lv[0], lv[1], omega, phi,
+                   R);
+    } else {
+        launch_r0(M, lv, phi, f, tol, max_cycles, 0, cond, use_cond, st);
+    }
     ++count;
     PIC_LAUNCH_CHECK();
     return PIC_OK;
