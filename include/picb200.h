@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define PIC_ABI_VERSION 2
+#define PIC_ABI_VERSION 3
 #define PIC_MAX_SPECIES 4
 #define PIC_MAX_PROCESSES 4
 
@@ -341,6 +341,9 @@ typedef struct pic_sim_desc {
     const pic_mcc_desc* mcc;    /* NULL: collisionless */
     unsigned long long seed;    /* Philox key */
     int use_graph;              /* capture the step in a CUDA graph */
+    int min_cycles;             /* V-cycles of a step's solve run before its first convergence test
+                                   (0: test after every cycle).  In the captured step they are chained
+                                   launches; each further cycle is an iteration of a WHILE node. */
 } pic_sim_desc;
 
 typedef struct pic_sim_counters {

@@ -41,7 +41,8 @@ namespace pic {
 
 int grid_blocks(long n, int threads);
 int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const pic_mg_options* opts, pic_mg** out);
-int mg_launch_graph(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st);
+int mg_launch_graph(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, int min_cycles,
+                    cudaStream_t st);
 const int* mg_device_converged(pic_mg* mg);
 
 struct AdSpecies {
@@ -444,7 +445,7 @@ static int field_of(AdjImpl& J, int state, double* Ex, double* Ey, cudaStream_t 
     k_ad_deposit<<<pb, 256, 0, st>>>(J.x, J.y, J.sp, J.death, state, J.n, J.d.nx, J.d.ny, J.S, 0, -1, J.rho);
     k_ad_rhs<<<gb, 256, 0, st>>>(J.rho, J.mask, -1.0 / J.d.eps0, J.f, J.G);
     PIC_LAUNCH_CHECK();
-    PIC_TRY(mg_launch_graph(J.mg, J.phi, J.f, J.d.tol, J.d.max_cycles, st));
+    PIC_TRY(mg_launch_graph(J.mg, J.phi, J.f, J.d.tol, J.d.max_cycles, 0, st));
     if (J.d.tol > 0) k_ad_track<<<1, 1, 0, st>>>(mg_device_converged(J.mg), J.failures);
     dim3 g;
     const int t = grid2(J, g);
@@ -535,7 +536,7 @@ static int field_adj(AdjImpl& J, cudaStream_t st) {
     k_ad_gradT<<<g, t, 0, st>>>(J.lEx, J.lEy, J.mask, J.lphi, J.fa, J.d.nx, J.d.ny, J.d.dx, J.d.dy);
     k_ad_zero2<<<grid_blocks(J.G, 256), 256, 0, st>>>(J.lEx, J.lEy, J.G);
     PIC_LAUNCH_CHECK();
-    PIC_TRY(mg_launch_graph(J.mga, J.mu, J.fa, J.d.tol, J.d.max_cycles, st));
+    PIC_TRY(mg_launch_graph(J.mga, J.mu, J.fa, J.d.tol, J.d.max_cycles, 0, st));
     if (J.d.tol > 0) k_ad_track<<<1, 1, 0, st>>>(mg_device_converged(J.mga), J.failures);
     if (J.d.nseg > 0)
         k_ad_dV<<<g, t, 0, st>>>(J.lphi, J.mu, J.mask, J.segid, J.d.nx, J.d.ny, 1.0 / (J.d.dx * J.d.dx),

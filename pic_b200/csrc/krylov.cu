@@ -16,7 +16,8 @@
 
 namespace pic {
 
-int mg_launch_graph(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st);
+int mg_launch_graph(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, int min_cycles,
+                    cudaStream_t st);
 bool mg_is_rz(pic_mg* mg);
 
 constexpr int kCgThreads = 256;
@@ -214,7 +215,7 @@ int pic_cg_solve(pic_cg* h, double* d_phi, const double* d_f, double tol, int ma
         if (C.mg) {
             k_cg_copy<<<gb, kCgThreads, 0, st>>>(C.z, C.r, C.free_, C.G, 1);
             PIC_LAUNCH_CHECK();
-            PIC_TRY(mg_launch_graph(C.mg, C.z, C.r, 1e-300, 1, st));
+            PIC_TRY(mg_launch_graph(C.mg, C.z, C.r, 1e-300, 1, 0, st));
         } else {
             k_cg_copy<<<gb, kCgThreads, 0, st>>>(C.z, C.r, C.free_, C.G, 0);
             PIC_LAUNCH_CHECK();

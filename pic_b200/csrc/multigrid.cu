@@ -1464,6 +1464,7 @@ struct MgImpl {
     const double* g_f = nullptr;
     double g_tol = 0;
     int g_max = -1;
+    int g_min = -1;
 };
 
 }  // namespace pic
@@ -2097,8 +2098,12 @@ static int launch_cycle(MgImpl& M, std::vector<LevelDev<T>>& lv_in, double* phi,
     count = 0;
     for (int l = 0; l < Ltile; ++l) {
         const dim3 g(div_up(lv[l].nx, kMgTile), div_up(lv[l].ny, kMgTile));
-        launch_pdl(kdown, g, dim3(kMgThreads), down, st, lv[l], lv[l + 1], omega,
-                   l == 0 ? (const double*)M.r64 : nullptr);
+        // the finest down phase waits for its predecessor to finish before it
+        // is placed: launched ahead, its CTAs would take the SMs its
+        // predecessor leaves free first, several to an SM (measured 8.5 us
+        // instead of 4.8 at 513^2)
+        if (l == 0) kdown<<<g, dim3(kMgThreads), down, st>>>(lv[0], lv[1], omega, (const double*)M.r64);
+        else launch_pdl(kdown, g, dim3(kMgThreads), down, st, lv[l], lv[l + 1], omega, (const double*)nullptr);
         ++count;
     }
     if constexpr (std::is_same<T, float>::value) {
@@ -2148,9 +2153,12 @@ static int launch_cycle(MgImpl& M, std::vector<LevelDev<T>>& lv_in, double* phi,
     return PIC_OK;
 }
 
+// min_cycles: V-cycles chained in the capturing graph itself before the WHILE
+// node, which only then tests for convergence (each iteration of a WHILE
+// node costs a launch of its body graph).
 template <class T>
 static int capture_solve(MgImpl& M, std::vector<LevelDev<T>>& lv, double* phi, const double* f, double tol,
-                         int max_cycles, cudaStream_t st) {
+                         int max_cycles, int min_cycles, cudaStream_t st) {
     cudaStreamCaptureStatus cs;
     cudaGraph_t g = nullptr;
     const cudaGraphNode_t* deps = nullptr;
@@ -2159,8 +2167,13 @@ static int capture_solve(MgImpl& M, std::vector<LevelDev<T>>& lv, double* phi, c
     if (cs != cudaStreamCaptureStatusActive) return fail(PIC_ERR_BAD_ARG, "multigrid: stream is not capturing");
     cudaGraphConditionalHandle h;
     PIC_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
-    launch_r0(M, lv, phi, f, tol, max_cycles, 1, h, 1, st);
+    const int K = std::max(0, std::min(min_cycles, max_cycles));
+    launch_r0(M, lv, phi, f, tol, max_cycles, 1, h, K == 0, st);
     PIC_LAUNCH_CHECK();
+    for (int k = 0; k < K; ++k) {
+        int count = 0;
+        PIC_TRY(launch_cycle(M, lv, phi, f, tol, max_cycles, h, k == K - 1, st, count));
+    }
     PIC_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
     cudaGraphNodeParams p{};
     p.type = cudaGraphNodeTypeConditional;
@@ -2294,7 +2307,7 @@ static int launch_dst(MgImpl& M, double* phi, const double* f, double tol, int m
     return PIC_OK;
 }
 
-int mg_capture(MgImpl& M, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
+int mg_capture(MgImpl& M, double* phi, const double* f, double tol, int max_cycles, int min_cycles, cudaStream_t st) {
     if (M.dst) return launch_dst(M, phi, f, tol, max_cycles, st);
     if (M.o.launch_mode == PIC_MG_CLUSTER && M.cluster_ok) return launch_cluster(M, phi, f, tol, max_cycles, st);
     if (M.o.launch_mode == PIC_MG_PERSISTENT)
@@ -2302,18 +2315,19 @@ int mg_capture(MgImpl& M, double* phi, const double* f, double tol, int max_cycl
                                            : launch_persistent(M, M.ld, phi, f, tol, max_cycles, st);
     if (M.o.launch_mode == PIC_MG_HOST_LOOP)
         return fail(PIC_ERR_BAD_ARG, "multigrid: the host-driven loop cannot be captured in a graph");
-    return M.precision == PIC_MG_MIXED ? capture_solve(M, M.lf, phi, f, tol, max_cycles, st)
-                                       : capture_solve(M, M.ld, phi, f, tol, max_cycles, st);
+    return M.precision == PIC_MG_MIXED ? capture_solve(M, M.lf, phi, f, tol, max_cycles, min_cycles, st)
+                                       : capture_solve(M, M.ld, phi, f, tol, max_cycles, min_cycles, st);
 }
 
-static int ensure_graph(MgImpl& M, double* phi, const double* f, double tol, int max_cycles) {
-    if (M.exec && M.g_phi == phi && M.g_f == f && M.g_tol == tol && M.g_max == max_cycles) return PIC_OK;
+static int ensure_graph(MgImpl& M, double* phi, const double* f, double tol, int max_cycles, int min_cycles) {
+    if (M.exec && M.g_phi == phi && M.g_f == f && M.g_tol == tol && M.g_max == max_cycles && M.g_min == min_cycles)
+        return PIC_OK;
     if (M.exec) {
         cudaGraphExecDestroy(M.exec);
         M.exec = nullptr;
     }
     PIC_CUDA(cudaStreamBeginCapture(M.cap, cudaStreamCaptureModeThreadLocal));
-    const int rc = mg_capture(M, phi, f, tol, max_cycles, M.cap);
+    const int rc = mg_capture(M, phi, f, tol, max_cycles, min_cycles, M.cap);
     cudaGraph_t g = nullptr;
     const cudaError_t ec = cudaStreamEndCapture(M.cap, &g);
     if (rc != PIC_OK) {
@@ -2328,6 +2342,7 @@ static int ensure_graph(MgImpl& M, double* phi, const double* f, double tol, int
     M.g_f = f;
     M.g_tol = tol;
     M.g_max = max_cycles;
+    M.g_min = min_cycles;
     return PIC_OK;
 }
 
@@ -2362,17 +2377,18 @@ long long mg_total_cycles(pic_mg* mg) {
 
 int mg_read_info(MgImpl& M, pic_mg_info* info);
 
-// Host-driven solve: one launch per kernel and a synchronisation per cycle.
+// Host-driven solve: one launch per kernel and a synchronisation per cycle
+// (the first min_cycles cycles run whatever the residual).
 template <class T>
 static int solve_eager(MgImpl& M, std::vector<LevelDev<T>>& lv, double* phi, const double* f, double tol,
-                       int max_cycles, cudaStream_t st) {
+                       int max_cycles, int min_cycles, cudaStream_t st) {
     launch_r0(M, lv, phi, f, tol, max_cycles, 1, cudaGraphConditionalHandle{}, 0, st);
     PIC_LAUNCH_CHECK();
     pic_mg_info info{};
     for (;;) {
         PIC_CUDA(cudaStreamSynchronize(st));
         PIC_TRY(mg_read_info(M, &info));
-        if (info.converged || info.cycles >= max_cycles) break;
+        if ((info.converged && info.cycles >= min_cycles) || info.cycles >= max_cycles) break;
         int count = 0;
         PIC_TRY(launch_cycle(M, lv, phi, f, tol, max_cycles, cudaGraphConditionalHandle{}, 0, st, count));
         M.body_launches = count;
@@ -2380,23 +2396,23 @@ static int solve_eager(MgImpl& M, std::vector<LevelDev<T>>& lv, double* phi, con
     return PIC_OK;
 }
 
-int mg_launch(MgImpl& M, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
+int mg_launch(MgImpl& M, double* phi, const double* f, double tol, int max_cycles, int min_cycles, cudaStream_t st) {
     if (M.dst) return launch_dst(M, phi, f, tol, max_cycles, st);
     if (M.o.launch_mode == PIC_MG_CLUSTER && M.cluster_ok) return launch_cluster(M, phi, f, tol, max_cycles, st);
     if (M.o.launch_mode == PIC_MG_PERSISTENT)
         return M.precision == PIC_MG_MIXED ? launch_persistent(M, M.lf, phi, f, tol, max_cycles, st)
                                            : launch_persistent(M, M.ld, phi, f, tol, max_cycles, st);
     if (M.o.launch_mode == PIC_MG_HOST_LOOP)
-        return M.precision == PIC_MG_MIXED ? solve_eager(M, M.lf, phi, f, tol, max_cycles, st)
-                                           : solve_eager(M, M.ld, phi, f, tol, max_cycles, st);
-    PIC_TRY(ensure_graph(M, phi, f, tol, max_cycles));
+        return M.precision == PIC_MG_MIXED ? solve_eager(M, M.lf, phi, f, tol, max_cycles, min_cycles, st)
+                                           : solve_eager(M, M.ld, phi, f, tol, max_cycles, min_cycles, st);
+    PIC_TRY(ensure_graph(M, phi, f, tol, max_cycles, min_cycles));
     PIC_CUDA(cudaGraphLaunch(M.exec, st));
     return PIC_OK;
 }
 
 int mg_solve(MgImpl& M, double* phi, const double* f, double tol, int max_cycles, pic_mg_info* info,
              cudaStream_t st) {
-    PIC_TRY(mg_launch(M, phi, f, tol, max_cycles, st));
+    PIC_TRY(mg_launch(M, phi, f, tol, max_cycles, 0, st));
     PIC_CUDA(cudaStreamSynchronize(st));
     pic_mg_info loc{};
     PIC_TRY(mg_read_info(M, &loc));
@@ -2420,13 +2436,15 @@ int mg_body_launches(pic_mg* mg) {
 // Kernels a solve runs besides its V-cycles: the residual, or the three
 // sine-transform kernels and the residual.
 int mg_fixed_launches(pic_mg* mg) { return mg && mg->m.dst ? 4 : 1; }
-int mg_capture_into(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
-    return mg_capture(mg->m, phi, f, tol, max_cycles, st);
+int mg_capture_into(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, int min_cycles,
+                    cudaStream_t st) {
+    return mg_capture(mg->m, phi, f, tol, max_cycles, min_cycles, st);
 }
 bool mg_uses_graph(pic_mg* mg) { return mg->m.o.launch_mode != PIC_MG_HOST_LOOP; }
 bool mg_is_rz(pic_mg* mg) { return mg->m.rz; }
-int mg_launch_graph(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st) {
-    return mg_launch(mg->m, phi, f, tol, max_cycles, st);
+int mg_launch_graph(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, int min_cycles,
+                    cudaStream_t st) {
+    return mg_launch(mg->m, phi, f, tol, max_cycles, min_cycles, st);
 }
 int mg_info(pic_mg* mg, pic_mg_info* info) { return mg_read_info(mg->m, info); }
 const int* mg_device_converged(pic_mg* mg) { return mg->m.N.converged; }
@@ -2471,7 +2489,7 @@ int pic_mg_solve_async(pic_mg* mg, double* d_phi, const double* d_f, double tol,
     clear_error();
     if (!mg || !d_phi || !d_f || !(tol > 0) || cycles < 0)
         return fail(PIC_ERR_BAD_ARG, "pic_mg_solve_async: bad arguments");
-    return mg_launch(mg->m, d_phi, d_f, tol, cycles, as_stream(stream));
+    return mg_launch(mg->m, d_phi, d_f, tol, cycles, 0, as_stream(stream));
 }
 
 int pic_mg_read_info(pic_mg* mg, double tol, pic_mg_info* info) {

@@ -37,8 +37,10 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
 int mg_body_launches(pic_mg* mg);
 int mg_fixed_launches(pic_mg* mg);
 long long mg_total_cycles(pic_mg* mg);
-int mg_capture_into(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st);
-int mg_launch_graph(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, cudaStream_t st);
+int mg_capture_into(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, int min_cycles,
+                    cudaStream_t st);
+int mg_launch_graph(pic_mg* mg, double* phi, const double* f, double tol, int max_cycles, int min_cycles,
+                    cudaStream_t st);
 int mg_info(pic_mg* mg, pic_mg_info* info);
 int diagnostics(const DiagSpecies* sp, const double* mass, const double* np2c, int ns, const double* phi,
                 const float* rho, const float* Ex, const float* Ey, int nx, int ny, double dx, double dy, double eps0,
@@ -1010,8 +1012,8 @@ static int field_solve(SimImpl& S, cudaStream_t st, bool capturing) {
     }
     {
         PhaseTimer t(S, PIC_PHASE_SOLVE, st);
-        if (capturing) PIC_TRY(mg_capture_into(S.mg, S.phi, S.f, S.d.tol, S.d.max_cycles, st));
-        else PIC_TRY(mg_launch_graph(S.mg, S.phi, S.f, S.d.tol, S.d.max_cycles, st));
+        if (capturing) PIC_TRY(mg_capture_into(S.mg, S.phi, S.f, S.d.tol, S.d.max_cycles, S.d.min_cycles, st));
+        else PIC_TRY(mg_launch_graph(S.mg, S.phi, S.f, S.d.tol, S.d.max_cycles, S.d.min_cycles, st));
     }
     if (!S.have_prev) {
         PIC_CUDA(cudaMemcpyAsync(S.phi_prev, S.phi, sizeof(double) * S.G, cudaMemcpyDeviceToDevice, st));
@@ -1085,7 +1087,8 @@ static int capture_step(SimImpl& S, bool sort_next, cudaGraphExec_t* out) {
 
 static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
     if (!d || d->nx < 3 || d->ny < 3 || !(d->dx > 0) || !(d->dy > 0) || !(d->dt > 0) || !(d->eps0 > 0) ||
-        d->nspecies < 1 || d->nspecies > PIC_MAX_SPECIES || !d->h_dirichlet || !(d->tol > 0) || d->max_cycles < 1)
+        d->nspecies < 1 || d->nspecies > PIC_MAX_SPECIES || !d->h_dirichlet || !(d->tol > 0) || d->max_cycles < 1 ||
+        d->min_cycles < 0)
         return fail(PIC_ERR_BAD_ARG, "pic_sim_create: bad descriptor");
     S.d = *d;
     if (S.d.tile <= 0) S.d.tile = 16;

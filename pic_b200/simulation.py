@@ -55,6 +55,11 @@ class PICSimulation:
 
     species: list of dicts with keys name, charge (C), mass (kg), np2c, capacity.
     dirichlet / phi_bc: node mask (1 = Dirichlet) and potentials, nx*ny.
+    min_cycles: V-cycles every step's field solve runs before it first tests
+    the residual against tol (then one at a time until converged); a solve from
+    the extrapolated potential of the last two steps needs at least two at the
+    tolerances of a PIC step, and cycles that are not tested cost no WHILE-node
+    iteration in the captured step.
     geometry: "cartesian", or "rz" for the axisymmetric r-z step (the
     reference's Grid.Cylindrical = 1): x axial, y radial (row 0 the axis, a
     free row), vx axial, vy radial, vz azimuthal; np2c counts real particles;
@@ -65,7 +70,7 @@ class PICSimulation:
     def __init__(self, nx, ny, dx, dy, dt, species, dirichlet, phi_bc=None, tol=1e-8, max_cycles=50,
                  precision="mixed", pre_sweeps=2, post_sweeps=2, omega=1.15, sort_interval=20, tile=16,
                  mcc: MccTables | None = None, seed=0, use_graph=False, eps0=Consts.eps0, mg_launch="graph",
-                 coarsest_max=9, geometry="cartesian"):
+                 coarsest_max=9, geometry="cartesian", min_cycles=2):
         self.nx, self.ny, self.dx, self.dy, self.dt = int(nx), int(ny), float(dx), float(dy), float(dt)
         self.species = list(species)
         self.geometry = geometry
@@ -91,6 +96,7 @@ class PICSimulation:
         d.mcc = C.cast(C.pointer(self._mcc_desc), C.c_void_p) if mcc is not None else None
         d.seed = int(seed)
         d.use_graph = int(use_graph)
+        d.min_cycles = int(min_cycles)
         self._desc = d
         self._h = C.c_void_p()
         _lib.call("pic_sim_create", C.byref(d), _lib.stream_ptr(), C.byref(self._h))
