@@ -193,6 +193,33 @@ __device__ __forceinline__ float u01_float(uint32_t x) {
     return __fadd_rn(__fmul_rn(float(x >> 8), 1.0f / 16777216.0f), 0.5f / 16777216.0f);
 }
 
+// ---- programmatic dependent launch -----------------------------------------------
+//
+// A kernel launched with launch_pdl may be scheduled while the kernel before
+// it on the stream still runs (once every CTA of that kernel has called
+// pdl_trigger, or exited).  pdl_wait blocks until that kernel has completed
+// and its memory is visible; both are no-ops for a launch without the
+// attribute.
+
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <class... KArgs, class... Args>
+static cudaError_t launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 // ---- block reductions -----------------------------------------------------------
 
 __device__ __forceinline__ double warp_sum(double v) {

@@ -146,8 +146,6 @@ struct CoarseDesc {
 // launches earlier (never what the kernel just before it writes).  The up
 // kernels load their whole fine tile (mask, g, e of their level, phi) there,
 // so only the coarse correction's load follows the wait.
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 template <int S>
 struct DownGeom {
@@ -2044,24 +2042,6 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
 }
 
 static int launch_cluster_tail(MgImpl& M, const std::vector<LevelDev<float>>& lv, cudaStream_t st);
-
-// A launch that may start while the preceding kernel on the stream drains
-// (the kernel waits in pdl_wait before reading what that kernel wrote).
-template <class... KArgs, class... Args>
-static cudaError_t launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
-                              Args... args) {
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = st;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k, args...);
-}
 
 // The FP64 residual and the loop decision (k_mg_r0) of either geometry.
 template <class T>

@@ -501,6 +501,7 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
 // The collision candidates of the pass: MCC, then the drift, absorption and
 // deposit the pass skipped for them (global atomics; a few per thousand).
 __global__ void __launch_bounds__(128) k_collide(PushArgs A) {
+    pdl_wait();
     const int nc = min(*A.cand_count, A.cand_cap);
     const uint32_t step = *A.step;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nc; i += gridDim.x * blockDim.x) {
@@ -557,6 +558,8 @@ __global__ void __launch_bounds__(128) k_collide(PushArgs A) {
 // Ionisation products: drift, absorb and deposit them (global atomics) and
 // append them to their species.
 __global__ void k_merge_births(PushArgs A) {
+    pdl_wait();
+    pdl_trigger();
     const int nb = min(*A.births.count, A.births.capacity);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
         const int s = A.births.species[i];
@@ -987,10 +990,10 @@ static int run_pass(SimImpl& S, cudaStream_t st, int kick, int mcc, int drift, i
         if (A.do_mcc) {
             // one thread per candidate: each is a long chain of dependent
             // table lookups and Philox rounds
-            k_collide<<<4 * num_sms(), 128, 0, st>>>(A);
+            launch_pdl(k_collide, dim3(4 * num_sms()), dim3(128), 0, st, A);
             S.launches += 1;
         }
-        k_merge_births<<<64, 256, 0, st>>>(A);
+        launch_pdl(k_merge_births, dim3(64), dim3(256), 0, st, A);
     }
     S.launches += 2;
     PIC_LAUNCH_CHECK();
@@ -1555,10 +1558,13 @@ int pic_sim_step(pic_sim* sim, int n_steps, void* stream) {
                 if (sort) PIC_TRY(sort_all(S, st));
                 PIC_TRY(prepare_pass(S, st, 1, 1));
             }
+            if (!S.g_step) {
+                // both graphs of the step are captured at the first captured step
+                PIC_TRY(capture_step(S, false, &S.g_step));
+                if (S.d.sort_interval > 0) PIC_TRY(capture_step(S, true, &S.g_sort_step));
+            }
             const bool sort_next = S.d.sort_interval > 0 && (S.steps + 1) % S.d.sort_interval == 0;
-            cudaGraphExec_t& g = sort_next ? S.g_sort_step : S.g_step;
-            if (!g) PIC_TRY(capture_step(S, sort_next, &g));
-            PIC_CUDA(cudaGraphLaunch(g, st));
+            PIC_CUDA(cudaGraphLaunch(sort_next ? S.g_sort_step : S.g_step, st));
             S.launches +=
                 3 + (S.have_mcc ? 2 : 0) + 2 + (sort_next ? 1 + (long long)S.ns * (5 + 3 * S.sorter.passes) : 0);
             S.solves += 1;
