@@ -142,7 +142,6 @@ __global__ void k_form_rhs(const float* __restrict__ rho, const uint8_t* __restr
                            double* __restrict__ f, float* __restrict__ rho_snapshot, float* __restrict__ rho_zero,
                            double* __restrict__ phi, double* __restrict__ phi_prev, long G,
                            const double* __restrict__ rowf, int nx) {
-    pdl_wait();
     for (long k = blockIdx.x * long(blockDim.x) + threadIdx.x; k < G; k += long(gridDim.x) * blockDim.x) {
         float r = rho[k];
         double rd = double(r);
@@ -201,8 +200,8 @@ int launch_update_E(const double* phi, float* Ex, float* Ey, float2* E2, int nx,
 
 int launch_form_rhs(const float* rho, const uint8_t* dirichlet, double eps0, double* f, float* snapshot,
                     float* zero, double* phi, double* phi_prev, long G, cudaStream_t st, const double* rowf, int nx) {
-    launch_pdl(k_form_rhs, dim3(grid_blocks(G, 256)), dim3(256), 0, st, rho, dirichlet, -1.0 / eps0, f, snapshot, zero,
-               phi, phi_prev, G, rowf, nx);
+    k_form_rhs<<<grid_blocks(G, 256), 256, 0, st>>>(rho, dirichlet, -1.0 / eps0, f, snapshot, zero, phi, phi_prev, G,
+                                                    rowf, nx);
     PIC_LAUNCH_CHECK();
     return PIC_OK;
 }

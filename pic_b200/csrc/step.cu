@@ -501,7 +501,6 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
 // The collision candidates of the pass: MCC, then the drift, absorption and
 // deposit the pass skipped for them (global atomics; a few per thousand).
 __global__ void __launch_bounds__(128) k_collide(PushArgs A) {
-    pdl_wait();
     const int nc = min(*A.cand_count, A.cand_cap);
     const uint32_t step = *A.step;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nc; i += gridDim.x * blockDim.x) {
@@ -558,8 +557,6 @@ __global__ void __launch_bounds__(128) k_collide(PushArgs A) {
 // Ionisation products: drift, absorb and deposit them (global atomics) and
 // append them to their species.
 __global__ void k_merge_births(PushArgs A) {
-    pdl_wait();
-    pdl_trigger();
     const int nb = min(*A.births.count, A.births.capacity);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
         const int s = A.births.species[i];
@@ -990,10 +987,10 @@ static int run_pass(SimImpl& S, cudaStream_t st, int kick, int mcc, int drift, i
         if (A.do_mcc) {
             // one thread per candidate: each is a long chain of dependent
             // table lookups and Philox rounds
-            launch_pdl(k_collide, dim3(4 * num_sms()), dim3(128), 0, st, A);
+            k_collide<<<4 * num_sms(), 128, 0, st>>>(A);
             S.launches += 1;
         }
-        launch_pdl(k_merge_births, dim3(64), dim3(256), 0, st, A);
+        k_merge_births<<<64, 256, 0, st>>>(A);
     }
     S.launches += 2;
     PIC_LAUNCH_CHECK();
