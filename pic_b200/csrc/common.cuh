@@ -159,6 +159,25 @@ __device__ __forceinline__ Cic cic_weights(float gx, float gy, int nx, int ny) {
     return c;
 }
 
+// cic_weights for a position already in [0, nx-1] x [0, ny-1], where the
+// clamp changes nothing: the same weights without it.
+__device__ __forceinline__ Cic cic_weights_in_domain(float gx, float gy, int nx, int ny) {
+    Cic c;
+    c.i0 = int(floorf(gx));
+    c.j0 = int(floorf(gy));
+    c.i1 = min(c.i0 + 1, nx - 1);
+    c.j1 = min(c.j0 + 1, ny - 1);
+    const float wx = __fsub_rn(gx, float(c.i0));
+    const float wy = __fsub_rn(gy, float(c.j0));
+    const float ux = __fsub_rn(1.0f, wx);
+    const float uy = __fsub_rn(1.0f, wy);
+    c.w00 = __fmul_rn(ux, uy);
+    c.w10 = __fmul_rn(wx, uy);
+    c.w01 = __fmul_rn(ux, wy);
+    c.w11 = __fmul_rn(wx, wy);
+    return c;
+}
+
 // Interpolated field value: ((w00*a + w10*b) + w01*c) + w11*d with the first
 // product rounded and the rest fused, in this order.
 __device__ __forceinline__ float cic_interp(const Cic& c, float a, float b, float cc, float d) {

@@ -278,8 +278,9 @@ constexpr int kStages = 3;  // chunk buffers: one loading, one in work, one drai
 // every thread; only the first chunk of a new unit is published through
 // shared memory, across the unit-end barrier.
 // RZ: r-z geometry (drift_rz); a separate instance, so that the Cartesian
-// pass carries none of it.
-template <bool RZ>
+// pass carries none of it.  FULL: kick, drift and deposit all on (the step's
+// pass), fixed at compile time.
+template <bool RZ, bool FULL>
 __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
     extern __shared__ __align__(128) unsigned char smem[];
     float* bufs = reinterpret_cast<float*>(smem);  // [kStages][4][kBufStride]
@@ -310,6 +311,9 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
     unsigned phases = 0u;  // expected parity of each stage's mbarrier
     int cur = 0, ox = 0, oy = 0;
     if (ch.valid && ch.tile >= 0) stage_tile(A, ch.tile, et, rt, ox, oy);
+    const bool do_kick = FULL || A.do_kick, do_drift = FULL || A.do_drift, do_deposit = FULL || A.do_deposit;
+    // the unit's absorbed, candidate and electrode counts of this thread
+    unsigned my_abs = 0, my_cand = 0, my_elec = 0;
     while (ch.valid) {
         const bool tiled = ch.tile >= 0;
         const int prv = cur == 0 ? kStages - 1 : cur - 1;
@@ -353,30 +357,30 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
         const unsigned* const cbits = (A.do_mcc && A.mcc->sp[s].nproc > 0) ? A.cbits[s] : nullptr;
         // r-z: the azimuthal velocity is not staged; it is read and written in place
         float* const gvz = RZ ? A.state[s].cur[4] + b : nullptr;
-        unsigned my_abs = 0, my_cand = 0, my_elec = 0;
-        // the candidate bits of this thread's slots: at most two words, each
-        // loaded only if one of the chunk's slots lies in it
+        // the candidate bits of this thread's slots (at most two words, each
+        // loaded only if one of the chunk's slots lies in it), as a 3-bit mask
         const int wt = tid - 32;  // particle lane (warp 0 has none)
         const int s0 = b + wt * kPushP, s_last = min(s0 + kPushP, b + n) - 1;
-        unsigned cw0 = 0u, cw1 = 0u;
+        unsigned cmask = 0u;
         if (wt >= 0 && cbits && s0 <= s_last) {
-            cw0 = __ldg(cbits + (s0 >> 5));
-            if ((s_last >> 5) != (s0 >> 5)) cw1 = __ldg(cbits + (s_last >> 5));
+            const unsigned cw0 = __ldg(cbits + (s0 >> 5));
+            const unsigned cw1 = (s_last >> 5) != (s0 >> 5) ? __ldg(cbits + (s_last >> 5)) : 0u;
+            cmask = __funnelshift_r(cw0, cw1, s0 & 31);
         }
+        const unsigned tw = unsigned(RW - 1);  // staged tile: local cell index in [0, RW-2]
 #pragma unroll
         for (int k = 0; k < kPushP; ++k) {
             const int l = wt * kPushP + k;
             if (wt < 0 || l >= n) break;
-            const int slot = b + l;
-            const bool candidate = (((slot >> 5) == (s0 >> 5) ? cw0 : cw1) >> (slot & 31)) & 1u;
+            const bool candidate = (cmask >> k) & 1u;
             float x = px[l], y = py[l];
             if (!is_live(x)) continue;
             float vx = pvx[l], vy = pvy[l];
-            if (A.do_kick) {
+            if (do_kick) {
                 const Cic c = cic_weights(x, y, A.nx, A.ny);
                 const int li = c.i0 - ox, lj = c.j0 - oy;
                 float2 e00, e10, e01, e11;
-                if (tiled && li >= 0 && lj >= 0 && li + 1 < RW && lj + 1 < RW) {
+                if (tiled && unsigned(li) < tw && unsigned(lj) < tw) {
                     const int q = lj * RW + li;
                     const int dq = c.i1 - c.i0, dr = (c.j1 - c.j0) * RW;
                     e00 = et[q];
@@ -404,7 +408,7 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
                 }
                 atomicAdd(A.ctr + kCtrCandOverflow, 1ull);
             }
-            if (A.do_drift) {
+            if (do_drift) {
                 const float x0 = x, y0 = y;
                 if constexpr (RZ) {
                     float vz = gvz[l];
@@ -428,10 +432,12 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
             py[l] = y;
             pvx[l] = vx;
             pvy[l] = vy;
-            if (A.do_deposit && is_live(x)) {
-                const Cic c = cic_weights(x, y, A.nx, A.ny);
+            if (do_deposit && is_live(x)) {
+                // after the drift's domain test a live position lies in
+                // [0, nx-1] x [0, ny-1], where cic_weights' clamp changes nothing
+                const Cic c = FULL ? cic_weights_in_domain(x, y, A.nx, A.ny) : cic_weights(x, y, A.nx, A.ny);
                 const int li = c.i0 - ox, lj = c.j0 - oy;
-                if (tiled && li >= 0 && lj >= 0 && li + 1 < RW && lj + 1 < RW) {
+                if (tiled && unsigned(li) < tw && unsigned(lj) < tw) {
                     const int q = lj * RW + li;
                     const int dq = c.i1 - c.i0, dr = (c.j1 - c.j0) * RW;
                     atomicAdd(rt + q, __float2uint_rn(__fmul_rn(c.w00, kFixScale)));
@@ -446,14 +452,6 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
                 }
             }
         }
-        my_abs = __reduce_add_sync(0xffffffffu, my_abs);
-        my_cand = __reduce_add_sync(0xffffffffu, my_cand);
-        my_elec = __reduce_add_sync(0xffffffffu, my_elec);
-        if ((tid & 31) == 0) {
-            if (my_abs) atomicAdd(&s_abs, my_abs);
-            if (my_cand) atomicAdd(&s_cand, my_cand);
-            if (my_elec) atomicAdd(&s_elec, my_elec);
-        }
         prev = ch;
         if (ch.e < ch.unit_e) {
             // the unit continues: every thread derives the next chunk itself
@@ -462,8 +460,17 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
             ch.first = 0;
         } else {
             // end of the unit: flush the charge tile and the counters
+            my_abs = __reduce_add_sync(0xffffffffu, my_abs);
+            my_cand = __reduce_add_sync(0xffffffffu, my_cand);
+            my_elec = __reduce_add_sync(0xffffffffu, my_elec);
+            if ((tid & 31) == 0) {
+                if (my_abs) atomicAdd(&s_abs, my_abs);
+                if (my_cand) atomicAdd(&s_cand, my_cand);
+                if (my_elec) atomicAdd(&s_elec, my_elec);
+            }
+            my_abs = my_cand = my_elec = 0u;
             __syncthreads();
-            if (tiled && A.do_deposit) {
+            if (tiled && do_deposit) {
                 for (int q = tid; q < RW * RW; q += kPushThreads) {
                     const unsigned sum = rt[q];
                     if (sum)
@@ -979,8 +986,14 @@ static int run_pass(SimImpl& S, cudaStream_t st, int kick, int mcc, int drift, i
     const PushArgs A = push_args(S, kick, mcc, drift, deposit, kick_factor);
     {
         PhaseTimer t(S, PIC_PHASE_PUSH, st);
-        if (S.rz) k_push<true><<<S.push_grid, kPushThreads, S.push_smem, st>>>(A);
-        else k_push<false><<<S.push_grid, kPushThreads, S.push_smem, st>>>(A);
+        const bool full = kick && drift && deposit;
+        if (S.rz) {
+            if (full) k_push<true, true><<<S.push_grid, kPushThreads, S.push_smem, st>>>(A);
+            else k_push<true, false><<<S.push_grid, kPushThreads, S.push_smem, st>>>(A);
+        } else {
+            if (full) k_push<false, true><<<S.push_grid, kPushThreads, S.push_smem, st>>>(A);
+            else k_push<false, false><<<S.push_grid, kPushThreads, S.push_smem, st>>>(A);
+        }
     }
     {
         PhaseTimer t(S, PIC_PHASE_MERGE, st);
@@ -1254,8 +1267,13 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
     // launch shape of the particle pass
     S.push_smem =
         sizeof(float) * kStages * 4 * kBufStride + size_t(S.rw) * S.rw * (sizeof(float2) + sizeof(unsigned));
-    const void* push_fn = S.rz ? reinterpret_cast<const void*>(k_push<true>) : reinterpret_cast<const void*>(k_push<false>);
-    PIC_TRY(raise_smem_limit(push_fn, S.push_smem));
+    const void* push_fns[4] = {reinterpret_cast<const void*>(k_push<false, false>),
+                               reinterpret_cast<const void*>(k_push<false, true>),
+                               reinterpret_cast<const void*>(k_push<true, false>),
+                               reinterpret_cast<const void*>(k_push<true, true>)};
+    for (const void* fn : push_fns) PIC_TRY(raise_smem_limit(fn, S.push_smem));
+    // the grid of the step's instance (the others run the same grid)
+    const void* push_fn = push_fns[S.rz ? 3 : 1];
     int per_sm = 0;
     PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_fn, kPushThreads, S.push_smem));
     S.push_grid = std::max(1, per_sm) * num_sms();
