@@ -425,6 +425,231 @@ __global__ void __launch_bounds__(kMgThreads) k_mg_up(LevelDev<T> F, LevelDev<T>
     up_tile<T, S, CYL, true>(F, Cc, omega, phi, blockIdx.x, blockIdx.y, smem);
 }
 
+// ---- two levels in one launch --------------------------------------------------
+//
+// The down phases of a fine level F and the next level C in one launch, and
+// the up phases of C and F in another (Cartesian levels above the direct
+// solve).  A CTA owns a 32 x 32 tile of F, that is a 16 x 16 tile of C, and
+// works both levels over halos wide enough that its C tile comes out exactly
+// as the separate launches give it: F is smoothed over a halo of HF nodes so
+// that F's residual is final where C's restriction over C's own smoothing halo
+// reads it.  The redundant halo work runs on SMs that the separate launches of
+// these small levels (25 and 9 CTAs at 513^2) leave idle.
+
+template <int S>
+struct Down2Geom {
+    static constexpr int HC = 2 * S + 2, WC = kMgTile / 2 + 2 * HC;  // C: as DownGeom
+    // F residual on 2HC + 1 nodes around the tile, e final one node further
+    static constexpr int HF = 2 * HC + 2 + 2 * S, WF = kMgTile + 2 * HF;
+};
+template <int S>
+struct Up2Geom {
+    static constexpr int HF = 2 * S, WF = kMgTile + 2 * HF, CWF = WF / 2 + 2;  // F: as UpGeom
+    // C final on F's prolongation window, smoothed over 2S more
+    static constexpr int WC = CWF + 4 * S, CWC = WC / 2 + 2;
+};
+
+// Full-weighting restriction of the residual held in `r` (a W x W tile at
+// (ox, oy) of the fine level, masked by `sm`) to coarse node (I, J).
+template <class T, int W>
+__device__ __forceinline__ T restrict_fw(const T* r, const uint8_t* sm, int I, int J, int ox, int oy) {
+    const int p = (2 * J - oy) * W + (2 * I - ox);
+    auto rv = [&](int o) { return sm[p + o] ? T(0) : r[p + o]; };
+    T v = T(0.25) * rv(0);
+    v += T(0.125) * (rv(-1) + rv(1) + rv(-W) + rv(W));
+    v += T(0.0625) * (rv(-W - 1) + rv(-W + 1) + rv(W - 1) + rv(W + 1));
+    return v;
+}
+
+// The residual g - A e in place of g on the interior of a W x W tile (each
+// node reads only its own g).
+template <class T, int W>
+__device__ __forceinline__ void tile_residual(const T* se, T* sg, const uint8_t* sm, T cx, T cy) {
+    constexpr int IT = (W * W + kMgThreads - 1) / kMgThreads;
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int q = it * kMgThreads + int(threadIdx.x);
+        if (q >= W * W) break;
+        const int li = q % W, lj = q / W;
+        if (li < 1 || lj < 1 || li > W - 2 || lj > W - 2 || sm[q]) continue;
+        const T c = se[q];
+        sg[q] = sg[q] - (cx * (se[q - 1] + se[q + 1] - T(2) * c) + cy * (se[q - W] + se[q + W] - T(2) * c));
+    }
+}
+
+template <class T, int S>
+__device__ void down2_tile(const LevelDev<T>& F, const LevelDev<T>& C, const LevelDev<T>& C2, T omega, int tx, int ty,
+                           unsigned char* smem) {
+    using G = Down2Geom<S>;
+    constexpr int WF = G::WF, WC = G::WC, HF = G::HF, HC = G::HC;
+    T* seF = reinterpret_cast<T*>(smem);
+    T* sgF = seF + WF * WF;
+    T* seC = sgF + WF * WF;
+    T* sgC = seC + WC * WC;
+    uint8_t* smF = reinterpret_cast<uint8_t*>(sgC + WC * WC);
+    uint8_t* smC = smF + WF * WF;
+    const int tid = threadIdx.x;
+    const int x0 = tx * kMgTile, y0 = ty * kMgTile, ox = x0 - HF, oy = y0 - HF;
+    const int cx0 = x0 / 2, cy0 = y0 / 2, cox = cx0 - HC, coy = cy0 - HC;
+    // C's mask over its region (edges and outside the grid Dirichlet)
+    constexpr int CIT = (WC * WC + kMgThreads - 1) / kMgThreads;
+    uint8_t cm[CIT];
+#pragma unroll
+    for (int it = 0; it < CIT; ++it) {
+        const int q = it * kMgThreads + tid;
+        const int I = cox + q % WC, J = coy + q / WC;
+        const bool in = q < WC * WC && I > 0 && J > 0 && I < C.nx - 1 && J < C.ny - 1;
+        cm[it] = in ? C.mask[long(J) * C.nx + I] : uint8_t(1);
+    }
+    tile_load<T, WF, false, false>(F, ox, oy, seF, sgF, smF, nullptr);
+    __syncthreads();
+    const int parF = (ox + oy) & 1;
+#pragma unroll 1
+    for (int s = 0; s < S; ++s)
+#pragma unroll
+        for (int color = 0; color < 2; ++color) {
+            tile_half_sweep<T, WF, false>(seF, sgF, smF, color ^ parF, F.cx, F.cy, F.inv_diag, omega, nullptr);
+            __syncthreads();
+        }
+    for (int q = tid; q < kMgTile * kMgTile; q += kMgThreads) {
+        const int i = x0 + q % kMgTile, j = y0 + q / kMgTile;
+        if (i < F.nx && j < F.ny) F.e[long(j) * F.nx + i] = seF[(HF + q / kMgTile) * WF + HF + q % kMgTile];
+    }
+    tile_residual<T, WF>(seF, sgF, smF, F.cx, F.cy);
+    __syncthreads();
+    // C over its region: g restricted from F, e from zero; C's own tile of g
+    // is kept for C's up phase
+#pragma unroll
+    for (int it = 0; it < CIT; ++it) {
+        const int q = it * kMgThreads + tid;
+        if (q >= WC * WC) break;
+        const int LI = q % WC, LJ = q / WC, I = cox + LI, J = coy + LJ;
+        const T g = cm[it] ? T(0) : restrict_fw<T, WF>(sgF, smF, I, J, ox, oy);
+        smC[q] = cm[it];
+        sgC[q] = g;
+        seC[q] = T(0);
+        if (LI >= HC && LJ >= HC && LI < HC + kMgTile / 2 && LJ < HC + kMgTile / 2 && I < C.nx && J < C.ny)
+            C.g[long(J) * C.nx + I] = g;
+    }
+    __syncthreads();
+    const int parC = (cox + coy) & 1;
+#pragma unroll 1
+    for (int s = 0; s < S; ++s)
+#pragma unroll
+        for (int color = 0; color < 2; ++color) {
+            tile_half_sweep<T, WC, false>(seC, sgC, smC, color ^ parC, C.cx, C.cy, C.inv_diag, omega, nullptr);
+            __syncthreads();
+        }
+    constexpr int hc = kMgTile / 2;
+    for (int q = tid; q < hc * hc; q += kMgThreads) {
+        const int I = cx0 + q % hc, J = cy0 + q / hc;
+        if (I < C.nx && J < C.ny) C.e[long(J) * C.nx + I] = seC[(HC + q / hc) * WC + HC + q % hc];
+    }
+    tile_residual<T, WC>(seC, sgC, smC, C.cx, C.cy);
+    __syncthreads();
+    // C's residual restricted to the C2 nodes of this tile
+    constexpr int h2 = kMgTile / 4;
+    if (tid < h2 * h2) {
+        const int I = cx0 / 2 + tid % h2, J = cy0 / 2 + tid / h2;
+        if (I < C2.nx && J < C2.ny) {
+            const long K = long(J) * C2.nx + I;
+            const bool dir = I == 0 || J == 0 || I == C2.nx - 1 || J == C2.ny - 1 || C2.mask[K];
+            C2.g[K] = dir ? T(0) : restrict_fw<T, WC>(sgC, smC, I, J, cox, coy);
+        }
+    }
+}
+
+template <class T, int S>
+__global__ void __launch_bounds__(kMgThreads) k_mg_down2(LevelDev<T> F, LevelDev<T> C, LevelDev<T> C2, T omega) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    pdl_wait();
+    pdl_trigger();
+    down2_tile<T, S>(F, C, C2, omega, blockIdx.x, blockIdx.y, smem);
+}
+
+// Bilinear prolongation of the coarse values `sc` (a CW-wide window at
+// (cox, coy) of the coarse level) added onto the free nodes of a W x W tile
+// at (ox, oy).
+template <class T, int W, int CW>
+__device__ __forceinline__ void tile_prolong(T* se, const uint8_t* sm, const T* sc, int ox, int oy, int cox, int coy) {
+    constexpr int IT = (W * W + kMgThreads - 1) / kMgThreads;
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int q = it * kMgThreads + int(threadIdx.x);
+        if (q >= W * W) break;
+        if (sm[q]) continue;
+        const int i = ox + q % W, j = oy + q / W;
+        const int c = ((j >> 1) - coy) * CW + ((i >> 1) - cox);
+        T v;
+        if (!(i & 1) && !(j & 1)) v = sc[c];
+        else if ((i & 1) && !(j & 1)) v = T(0.5) * (sc[c] + sc[c + 1]);
+        else if (!(i & 1) && (j & 1)) v = T(0.5) * (sc[c] + sc[c + CW]);
+        else v = T(0.25) * (sc[c] + sc[c + 1] + sc[c + CW] + sc[c + CW + 1]);
+        se[q] += v;
+    }
+}
+
+template <class T, int S>
+__device__ void up2_tile(const LevelDev<T>& F, const LevelDev<T>& C, const LevelDev<T>& C2, T omega, int tx, int ty,
+                         unsigned char* smem) {
+    using G = Up2Geom<S>;
+    constexpr int WF = G::WF, HF = G::HF, CWF = G::CWF, WC = G::WC, CWC = G::CWC;
+    T* seF = reinterpret_cast<T*>(smem);
+    T* sgF = seF + WF * WF;
+    T* seC = sgF + WF * WF;
+    T* sgC = seC + WC * WC;
+    T* sc2 = sgC + WC * WC;
+    uint8_t* smF = reinterpret_cast<uint8_t*>(sc2 + CWC * CWC);
+    uint8_t* smC = smF + WF * WF;
+    const int tid = threadIdx.x;
+    const int x0 = tx * kMgTile, y0 = ty * kMgTile, ox = x0 - HF, oy = y0 - HF;
+    const int fcx = ox >> 1, fcy = oy >> 1;                    // F's prolongation window on C
+    const int cox = fcx - 2 * S, coy = fcy - 2 * S;            // C's region
+    const int c2x = cox >> 1, c2y = coy >> 1;                  // C's prolongation window on C2
+    // every tile load is issued before the wait: F and C were written by the
+    // down phase two launches back; only C2's correction follows the wait
+    tile_load<T, WF, true, false>(F, ox, oy, seF, sgF, smF, nullptr);
+    tile_load<T, WC, true, false>(C, cox, coy, seC, sgC, smC, nullptr);
+    pdl_wait();
+    pdl_trigger();
+    for (int q = tid; q < CWC * CWC; q += kMgThreads) {
+        const int I = c2x + q % CWC, J = c2y + q / CWC;
+        sc2[q] = (I >= 0 && J >= 0 && I < C2.nx && J < C2.ny) ? C2.ec[long(J) * C2.nx + I] : T(0);
+    }
+    __syncthreads();
+    tile_prolong<T, WC, CWC>(seC, smC, sc2, cox, coy, c2x, c2y);
+    __syncthreads();
+    const int parC = (cox + coy) & 1;
+#pragma unroll 1
+    for (int s = 0; s < S; ++s)
+#pragma unroll
+        for (int color = 0; color < 2; ++color) {
+            tile_half_sweep<T, WC, false>(seC, sgC, smC, color ^ parC, C.cx, C.cy, C.inv_diag, omega, nullptr);
+            __syncthreads();
+        }
+    // F's prolongation window lies 2S inside C's region
+    tile_prolong<T, WF, WC>(seF, smF, seC, ox, oy, cox, coy);
+    __syncthreads();
+    const int parF = (ox + oy) & 1;
+#pragma unroll 1
+    for (int s = 0; s < S; ++s)
+#pragma unroll
+        for (int color = 0; color < 2; ++color) {
+            tile_half_sweep<T, WF, false>(seF, sgF, smF, color ^ parF, F.cx, F.cy, F.inv_diag, omega, nullptr);
+            __syncthreads();
+        }
+    for (int q = tid; q < kMgTile * kMgTile; q += kMgThreads) {
+        const int i = x0 + q % kMgTile, j = y0 + q / kMgTile;
+        if (i < F.nx && j < F.ny) F.ec[long(j) * F.nx + i] = seF[(HF + q / kMgTile) * WF + HF + q % kMgTile];
+    }
+}
+
+template <class T, int S>
+__global__ void __launch_bounds__(kMgThreads) k_mg_up2(LevelDev<T> F, LevelDev<T> C, LevelDev<T> C2, T omega) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    up2_tile<T, S>(F, C, C2, omega, blockIdx.x, blockIdx.y, smem);
+}
+
 // Sums (a, b) over the grid: block partials into N.partial; the last block to
 // finish adds them in a fixed order (the same decision on every run) and
 // takes the loop decision: initial (first residual of a solve) records
@@ -580,6 +805,37 @@ static UpResKernel<T> up_res_kernel(int s) {
         k_mg_up_res<T, 4, CYL>,   k_mg_up_res<T, 5, CYL>, k_mg_up_res<T, 6, CYL>, k_mg_up_res<T, 7, CYL>,
         k_mg_up_res<T, 8, CYL>};
     return k[s];
+}
+
+template <class T>
+using Fused2Kernel = void (*)(LevelDev<T>, LevelDev<T>, LevelDev<T>, T);
+
+template <class T>
+static Fused2Kernel<T> down2_kernel(int s) {
+    static const Fused2Kernel<T> k[kMgMaxSweeps + 1] = {
+        nullptr,           k_mg_down2<T, 1>, k_mg_down2<T, 2>, k_mg_down2<T, 3>, k_mg_down2<T, 4>,
+        k_mg_down2<T, 5>,  k_mg_down2<T, 6>, k_mg_down2<T, 7>, k_mg_down2<T, 8>};
+    return k[s];
+}
+
+template <class T>
+static Fused2Kernel<T> up2_kernel(int s) {
+    static const Fused2Kernel<T> k[kMgMaxSweeps + 1] = {
+        nullptr,         k_mg_up2<T, 1>, k_mg_up2<T, 2>, k_mg_up2<T, 3>, k_mg_up2<T, 4>,
+        k_mg_up2<T, 5>,  k_mg_up2<T, 6>, k_mg_up2<T, 7>, k_mg_up2<T, 8>};
+    return k[s];
+}
+
+template <class T>
+static size_t down2_smem(int s) {
+    const size_t HC = 2 * s + 2, WC = kMgTile / 2 + 2 * HC, HF = 2 * HC + 2 + 2 * s, WF = kMgTile + 2 * HF;
+    return (WF * WF + WC * WC) * (2 * sizeof(T) + 1);
+}
+
+template <class T>
+static size_t up2_smem(int s) {
+    const size_t WF = kMgTile + 4 * s, CWF = WF / 2 + 2, WC = CWF + 4 * s, CWC = WC / 2 + 2;
+    return (WF * WF + WC * WC) * (2 * sizeof(T) + 1) + CWC * CWC * sizeof(T);
 }
 
 template <class T>
@@ -1439,6 +1695,7 @@ struct MgImpl {
     int* didx = nullptr;   // dn free nodes, then dnz others
     int dn = 0, dnz = 0;
     double* r64 = nullptr;  // FP64 residual of phi between the cycles of a graph- or host-loop solve
+    bool fuse2 = false;     // levels Lc-2 and Lc-1 in one down and one up launch (k_mg_down2, k_mg_up2)
     NormState N{};
     dim3 blk0{32, 8}, grd0;
     CoarseLayout cl[2];  // the coarse kernel's levels (from Lc) and the persistent/cluster ones (from Lp)
@@ -1654,6 +1911,18 @@ static bool band_inverse(std::vector<double>& a, int n, int bw) {
     }
     a.swap(inv);
     return true;
+}
+
+// The two-level launches (k_mg_down2, k_mg_up2) for levels Lc-2 and Lc-1,
+// where their shared memory fits.
+template <class T>
+static int configure_fuse2(MgImpl& M) {
+    const size_t d = down2_smem<T>(M.o.pre_sweeps), u = up2_smem<T>(M.o.post_sweeps);
+    if (d > 227 * 1024 || u > 227 * 1024) return PIC_OK;
+    PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(down2_kernel<T>(M.o.pre_sweeps)), d));
+    PIC_TRY(raise_smem_limit(reinterpret_cast<const void*>(up2_kernel<T>(M.o.post_sweeps)), u));
+    M.fuse2 = true;
+    return PIC_OK;
 }
 
 // The direct solve of level Lc (see k_mg_direct); left off (the coarse
@@ -2009,6 +2278,8 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
     if (st == PIC_OK && M.Lc >= 1 &&
         (M.o.launch_mode == PIC_MG_GRAPH_LOOP || M.o.launch_mode == PIC_MG_HOST_LOOP))
         st = configure_direct(M, nxs, nys, masks);
+    if (st == PIC_OK && M.direct && !M.rz && M.Lc >= 3)
+        st = M.precision == PIC_MG_MIXED ? configure_fuse2<float>(M) : configure_fuse2<double>(M);
     if (st != PIC_OK) return bail(st);
     M.grd0 = dim3(div_up(nx, M.blk0.x), div_up(ny, M.blk0.y * kR0Rows));
     // block partials of the residual norm: one pair per block of the level-0
@@ -2076,7 +2347,10 @@ static int launch_cycle(MgImpl& M, std::vector<LevelDev<T>>& lv_in, double* phi,
     const DownKernel<T> kdown = M.rz ? down_kernel<T, true>(M.o.pre_sweeps) : down_kernel<T, false>(M.o.pre_sweeps);
     const UpKernel<T> kup = M.rz ? up_kernel<T, true>(M.o.post_sweeps) : up_kernel<T, false>(M.o.post_sweeps);
     count = 0;
-    for (int l = 0; l < Ltile; ++l) {
+    // levels Lc-2 and Lc-1 in one launch each way where that applies
+    const bool f2 = M.fuse2 && !hyb;
+    const int Lsingle = f2 ? Ltile - 2 : Ltile;
+    for (int l = 0; l < Lsingle; ++l) {
         const dim3 g(div_up(lv[l].nx, kMgTile), div_up(lv[l].ny, kMgTile));
         // the finest down phase waits for its predecessor to finish before it
         // is placed: launched ahead, its CTAs would take the SMs its
@@ -2084,6 +2358,13 @@ static int launch_cycle(MgImpl& M, std::vector<LevelDev<T>>& lv_in, double* phi,
         // instead of 4.8 at 513^2)
         if (l == 0) kdown<<<g, dim3(kMgThreads), down, st>>>(lv[0], lv[1], omega, (const double*)M.r64);
         else launch_pdl(kdown, g, dim3(kMgThreads), down, st, lv[l], lv[l + 1], omega, (const double*)nullptr);
+        ++count;
+    }
+    if (f2) {
+        const int l = Lsingle;
+        const dim3 g(div_up(lv[l].nx, kMgTile), div_up(lv[l].ny, kMgTile));
+        launch_pdl(down2_kernel<T>(M.o.pre_sweeps), g, dim3(kMgThreads), down2_smem<T>(M.o.pre_sweeps), st, lv[l],
+                   lv[l + 1], lv[l + 2], omega);
         ++count;
     }
     if constexpr (std::is_same<T, float>::value) {
@@ -2104,7 +2385,14 @@ static int launch_cycle(MgImpl& M, std::vector<LevelDev<T>>& lv_in, double* phi,
         else launch_pdl(k_mg_coarse<T, false>, dim3(1), dim3(kCoarseThreads), M.cl[0].smem, st, D);
         ++count;
     }
-    for (int l = Ltile - 1; l >= 1; --l) {
+    if (f2) {
+        const int l = Lsingle;
+        const dim3 g(div_up(lv[l].nx, kMgTile), div_up(lv[l].ny, kMgTile));
+        launch_pdl(up2_kernel<T>(M.o.post_sweeps), g, dim3(kMgThreads), up2_smem<T>(M.o.post_sweeps), st, lv[l],
+                   lv[l + 1], lv[l + 2], omega);
+        ++count;
+    }
+    for (int l = Lsingle - 1; l >= 1; --l) {
         const dim3 g(div_up(lv[l].nx, kMgTile), div_up(lv[l].ny, kMgTile));
         launch_pdl(kup, g, dim3(kMgThreads), up, st, lv[l], lv[l + 1], omega, (double*)nullptr);
         ++count;
