@@ -52,12 +52,22 @@ __global__ void k_upsweep(const uint32_t* __restrict__ keys, const int* __restri
     cta_range(n_dev[0], G, blockIdx.x, b, e);
     const int lane = threadIdx.x & 31;
     // keys are nearly sorted, so a warp's 32 digits are mostly equal: one
-    // shared-memory increment per distinct digit and warp
-    for (int base = b; base < e; base += blockDim.x) {
-        const int i = base + threadIdx.x;
-        const int d = i < e ? int((keys[i] >> shift) & 0xff) : kRadix;
-        const unsigned peers = __match_any_sync(0xffffffffu, d);
-        if (d < kRadix && lane == __ffs(peers) - 1) atomicAdd(&h[d], __popc(peers));
+    // shared-memory increment per distinct digit and warp.  A thread loads
+    // kSortIpt keys before it uses the first, so that the loads overlap.
+    for (int base = b; base < e; base += kSortSub) {
+        uint32_t k[kSortIpt];
+#pragma unroll
+        for (int it = 0; it < kSortIpt; ++it) {
+            const int i = base + it * kSortThreads + int(threadIdx.x);
+            k[it] = i < e ? __ldg(keys + i) : 0xffffffffu;
+        }
+#pragma unroll
+        for (int it = 0; it < kSortIpt; ++it) {
+            const int i = base + it * kSortThreads + int(threadIdx.x);
+            const int d = i < e ? int((k[it] >> shift) & 0xff) : kRadix;
+            const unsigned peers = __match_any_sync(0xffffffffu, d);
+            if (d < kRadix && lane == __ffs(peers) - 1) atomicAdd(&h[d], __popc(peers));
+        }
     }
     __syncthreads();
     for (int d = threadIdx.x; d < kRadix; d += blockDim.x) cnt[d * G + blockIdx.x] = h[d];
@@ -131,12 +141,18 @@ __global__ void __launch_bounds__(kSortThreads) k_downsweep(const uint32_t* __re
         __syncthreads();
         uint32_t key[kSortIpt], val[kSortIpt];
         int rank[kSortIpt];
+        // every load of the sub-tile issued before the ranking uses the first
 #pragma unroll
         for (int it = 0; it < kSortIpt; ++it) {
             const int idx = base + warp * (32 * kSortIpt) + it * 32 + lane;
             const bool valid = idx < e;
-            key[it] = valid ? kin[idx] : 0u;
-            val[it] = valid ? vin[idx] : 0u;
+            key[it] = valid ? __ldg(kin + idx) : 0u;
+            val[it] = valid ? __ldg(vin + idx) : 0u;
+        }
+#pragma unroll
+        for (int it = 0; it < kSortIpt; ++it) {
+            const int idx = base + warp * (32 * kSortIpt) + it * 32 + lane;
+            const bool valid = idx < e;
             const int d = valid ? int((key[it] >> shift) & 0xff) : kRadix;
             const unsigned peers = __match_any_sync(0xffffffffu, d);
             const int leader = __ffs(peers) - 1;

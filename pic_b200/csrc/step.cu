@@ -694,11 +694,21 @@ __global__ void k_sim_keys(const SpeciesState* __restrict__ state, int s, int nc
 __global__ void k_sim_gather(const SpeciesState* __restrict__ state, int s, const uint32_t* __restrict__ perm,
                              const int* __restrict__ n_dev) {
     const int n = n_dev[1];
+    // the arrays' pointers in registers (a store through alt could otherwise
+    // alias the state struct and force them to be reloaded per element)
     const SpeciesState& S = state[s];
+    const float *__restrict__ c0 = S.cur[0], *__restrict__ c1 = S.cur[1], *__restrict__ c2 = S.cur[2],
+                *__restrict__ c3 = S.cur[3], *__restrict__ c4 = S.cur[4];
+    float *__restrict__ a0 = S.alt[0], *__restrict__ a1 = S.alt[1], *__restrict__ a2 = S.alt[2],
+          *__restrict__ a3 = S.alt[3], *__restrict__ a4 = S.alt[4];
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const uint32_t src = perm[k];
-#pragma unroll
-        for (int c = 0; c < 5; ++c) S.alt[c][k] = S.cur[c][src];
+        const uint32_t p = __ldg(perm + k);
+        const float v0 = c0[p], v1 = c1[p], v2 = c2[p], v3 = c3[p], v4 = c4[p];
+        a0[k] = v0;
+        a1[k] = v1;
+        a2[k] = v2;
+        a3[k] = v3;
+        a4[k] = v4;
     }
 }
 
