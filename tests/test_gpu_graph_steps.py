@@ -70,3 +70,29 @@ def test_graph_steps_match_eager_steps(chunks):
     np.testing.assert_allclose(phi_g, phi_e, rtol=0, atol=1e-6 * np.abs(phi_e).max())
     for sim in (eager, graph):
         sim.close()
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_min_cycles_run_before_the_first_test(use_graph):
+    # tol 1e-4 from the extrapolated potential: one V-cycle suffices (the
+    # first cuts the residual of a PIC step about 500-fold); min_cycles=3
+    # runs three whatever the residual, and ends closer to the solution
+    w = workloads.scaled(workloads.SMALL, n=20_000)
+    mask, phi_bc = workloads.dirichlet(w)
+    got = {}
+    for mc in (0, 3):
+        sp_ = [dict(name="e", charge=-Consts.qe, mass=Consts.me, np2c=w.np2c(w.n_e), capacity=2 * w.n_e),
+               dict(name="i", charge=Consts.qe, mass=workloads.ION_MASS, np2c=w.np2c(w.n_i), capacity=2 * w.n_i)]
+        sim = PICSimulation(w.nodes, w.nodes, w.dx, w.dx, w.dt, sp_, mask, phi_bc, tol=1e-4, max_cycles=60,
+                            sort_interval=0, use_graph=use_graph, min_cycles=mc)
+        rng = np.random.Generator(np.random.Philox(w.seed))
+        for s, which in enumerate("ei"):
+            sim.load(s, *workloads.species_arrays(w, which, rng))
+        sim.init()
+        sim.step(4)
+        sim.sync()
+        c = sim.counters()
+        got[mc] = (c["last_cycles"], c["last_rel_res"])
+        sim.close()
+    assert got[0][0] < 3 and got[0][1] < 1e-4, got
+    assert got[3][0] == 3 and got[3][1] < got[0][1], got
