@@ -483,12 +483,11 @@ def run_e2e(w, arrays, args, world, rank):
     sim.step(args.steps)
     sim.sync()
     ev[3].record(stream)
-    # the device views first (each call synchronises the device), then every
-    # copy back to back on the stream
-    views = [sim.species_arrays(s) for s in range(2)]
-    phi_dev = sim.fields()[0]
-    outs = [[h[: v.numel()].copy_(v, non_blocking=True) for h, v in zip(host_out[s], views[s])] for s in range(2)]
-    phi = host_phi.copy_(phi_dev, non_blocking=True)
+    outs = []
+    for s in range(2):
+        views = sim.species_arrays(s)
+        outs.append([h[: v.numel()].copy_(v, non_blocking=True) for h, v in zip(host_out[s], views)])
+    phi = host_phi.copy_(sim.fields()[0], non_blocking=True)
     ev[4].record(stream)
     torch.cuda.synchronize()
     ms = ev[0].elapsed_time(ev[4])
