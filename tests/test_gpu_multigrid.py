@@ -206,3 +206,40 @@ def test_solves_are_deterministic_across_launch_modes(n):
                 ref = out
             assert out[0] == ref[0] and out[1] == ref[1]
             np.testing.assert_array_equal(out[2], ref[2])
+
+
+@pytest.mark.parametrize("shape", [(513, 129), (129, 513), (385, 193)])
+def test_rectangular_grids_with_electrodes_match_direct_solve(shape):
+    # rectangular and 3 * 2^k + 1 grids deep enough for the two-level launches
+    # and the direct coarse solve (first coarse levels 33 x 9, 9 x 33, 25 x 13),
+    # with an electrode on an odd grid line, against scipy's sparse LU
+    m, n = shape
+    h = 1e-3
+    rng = np.random.default_rng(12)
+    mask = np.zeros((n, m), np.uint8)
+    mask[0, :] = mask[-1, :] = mask[:, 0] = mask[:, -1] = 1
+    phi_bc = np.zeros((n, m))
+    phi_bc[1:-1, 0] = 30.0
+    el = (slice(n // 3, 2 * n // 3), 2 * (m // 5) + 1)  # a vertical electrode on an odd column
+    mask[el] = 1
+    phi_bc[el] = -20.0
+    mask, phi_bc = mask.reshape(-1), phi_bc.reshape(-1)
+    f = rng.normal(0, 1e5, m * n)
+    f[mask == 1] = 0.0
+    A = sp.lil_matrix((m * n, m * n))
+    b = f.copy()
+    for k in range(m * n):
+        if mask[k]:
+            A[k, k] = 1.0
+            b[k] = phi_bc[k]
+        else:
+            A[k, k] = -4.0 / h**2
+            for q in (k - 1, k + 1, k - m, k + m):
+                A[k, q] = 1.0 / h**2
+    ref = spla.spsolve(A.tocsr(), b)
+    for precision in ("mixed", "fp64"):
+        mg = MultigridSolver(mask, m, n, h, precision=precision)
+        phi, (cycles, rel) = mg.solve(torch.as_tensor(phi_bc.copy(), device=DEV), torch.as_tensor(f, device=DEV),
+                                      tol=1e-10, max_cycles=120)
+        assert rel < 1e-10, (precision, cycles, rel)
+        np.testing.assert_allclose(phi.cpu().numpy(), ref, rtol=0, atol=1e-8 * np.abs(ref).max(), err_msg=precision)
