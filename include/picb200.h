@@ -196,6 +196,13 @@ int pic_mg_read_info(pic_mg* mg, double tol, pic_mg_info* info);
 /* The launch mode solves actually use (PIC_MG_CLUSTER falls back to
  * PIC_MG_GRAPH_LOOP where the cluster solve does not apply). */
 int pic_mg_effective_launch_mode(pic_mg* mg, int* mode);
+/* Failure detection of the persistent solve (PIC_MG_PERSISTENT; the
+ * reference's host loop, src/multigrid.py:445-455, has no device wait to
+ * bound): polls a grid barrier makes before the solve gives up, sets a device
+ * error flag and returns, and the solve returns PIC_ERR_TIMEOUT (the flag is
+ * then cleared and the solver stays usable).  polls < 0 restores the default
+ * (2^24 polls, about a second). */
+int pic_mg_set_wait_limit(pic_mg* mg, long long polls);
 
 /* Solver(solver_type='cg' | 'gmres') (src/Solvers.py:245-258: cupyx cg and
  * gmres on the 5-point Laplacian with Dirichlet rows): flexible
@@ -229,7 +236,9 @@ int pic_sorter_destroy(pic_sorter* s);
  * order (bit-identical to a stable argsort of the keys), gathers the five
  * arrays into the *_out arrays, writes the live count to *d_count_out
  * (device int) and, if d_tile_start is not NULL, the first sorted slot of
- * each tile (ntiles+1 ints).  Deterministic. */
+ * each tile (ntiles+1 ints).  d_perm and the *_out arrays need room for n
+ * entries: only the first (live count) are written.  d_x_out may be NULL to
+ * get the permutation alone.  Deterministic. */
 int pic_sort(pic_sorter* s, const float* d_x, const float* d_y, const float* d_vx, const float* d_vy,
              const float* d_vz, int n, float* d_x_out, float* d_y_out, float* d_vx_out, float* d_vy_out,
              float* d_vz_out, uint32_t* d_perm, int* d_count_out, int* d_tile_start, void* stream);
@@ -381,6 +390,17 @@ int pic_sim_sync(pic_sim* sim, void* stream);
 
 /* Current device arrays of species s (the sort swaps buffers). */
 int pic_sim_species_arrays(pic_sim* sim, int s, float** x, float** y, float** vx, float** vy, float** vz);
+/* The reference's R / V read back to the host (src/Particles.py:283-326 keeps
+ * them as device arrays the caller copies): the slots in use of species s as
+ * five consecutive rows x, y, vx, vy, vz of *count floats each in h_out
+ * (page-locked memory for an asynchronous copy), in one device-to-host copy
+ * on `stream`.  *count (the slots in use, dead ones included) is read first,
+ * synchronously.  PIC_ERR_OUT_OF_CAPACITY if 5 * count > capacity. */
+int pic_sim_read_particles(pic_sim* sim, int s, float* h_out, long long capacity, int* count, void* stream);
+/* The cell sort of every species, now (the sort a step runs every
+ * sort_interval steps; Particles2D.sort_particles_sparse,
+ * src/Particles.py:550-632).  Asynchronous on `stream`. */
+int pic_sim_sort(pic_sim* sim, void* stream);
 /* Device pointers of phi (FP64), rho (float32, last deposit), Ex, Ey (float32). */
 int pic_sim_fields(pic_sim* sim, double** phi, float** rho, float** Ex, float** Ey);
 /* Synchronises `stream` and reads counters. */
@@ -438,6 +458,17 @@ typedef struct pic_sim_profile {
 } pic_sim_profile;
 /* enable = 1 starts recording (and clears what was recorded), 0 stops. */
 int pic_sim_set_profiling(pic_sim* sim, int enable);
+/* Failure detection of the particle pass (the reference's pass has no device
+ * wait to bound, src/Particles.py:359-410): polls a wait on a bulk copy into
+ * shared memory makes before the pass gives up its work unit and sets a
+ * device error flag (the copy in flight is still waited for, with the
+ * default limit, before the block exits).  The next pic_sim_read_counters
+ * returns PIC_ERR_TIMEOUT and clears the flag; the particle state of that pass
+ * is then incomplete and should be reloaded.  polls < 0 restores the default
+ * (2^24 polls); 0 gives up at the first wait.  The same limit goes to the
+ * simulation's multigrid (pic_mg_set_wait_limit).  Captured step graphs are
+ * re-captured with the new limit. */
+int pic_sim_set_wait_limit(pic_sim* sim, long long polls);
 /* Synchronises the device and sums the recorded intervals. */
 int pic_sim_read_profile(pic_sim* sim, pic_sim_profile* out);
 

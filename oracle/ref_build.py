@@ -16,7 +16,7 @@ Kernels taken, by the name given to RawKernel:
                        coarsen_bc_mask (:235-274)
     src/MCC.py         compute_speeds_and_energies (:7-30), interpolate_cross_sections (:32-83)
 ``#include`` lines inside the strings are dropped (the shim provides what they
-would).  Usage:  python oracle/ref_build.py [--reference DIR] [--out DIR]
+would).  Usage:  python oracle/ref_build.py [--reference DIR] [--out DIR]  (or set PIC_REFERENCE_DIR)
 """
 from __future__ import annotations
 
@@ -27,7 +27,9 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_REFERENCE = "/root/reference"
+# the reference tree: --reference DIR, else $PIC_REFERENCE_DIR, else the
+# container's read-only checkout
+DEFAULT_REFERENCE = os.environ.get("PIC_REFERENCE_DIR", "/root/reference")
 
 WANTED = {
     "src/Grid.py": ["update_density_direct_cartesian", "update_E"],

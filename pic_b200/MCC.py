@@ -14,6 +14,7 @@ come from Philox4x32-10 keyed by ``seed`` and a step counter.
 from __future__ import annotations
 
 import ctypes as C
+import hashlib
 
 import numpy as np
 import torch
@@ -145,7 +146,25 @@ class MccOperator:
             self._h = None
 
 
+# Operators of null_collision_method, keyed by what determines them: the
+# cross-section tables' contents (a digest, so that a new table object with
+# the same values reuses the operator and one with other values never does),
+# the gas, dt, the seed and the species' masses.  At most _MAX_OPERATORS are
+# kept, the least recently used dropped first.
 _operators: dict = {}
+_MAX_OPERATORS = 8
+
+
+def _operator_key(particles, density, cross_sections, dt, ionization, seed, gas_temperature, gas_mass, threshold):
+    h = hashlib.sha1()
+    for table in cross_sections:
+        for col in table:
+            h.update(b"none" if col is None else np.ascontiguousarray(col, dtype=np.float64).tobytes())
+            h.update(b"|")
+        h.update(b"||")
+    masses = tuple((s.mass, s.charge, s.collision_model) for s in particles.species)
+    return (h.hexdigest(), float(density), float(dt), bool(ionization), int(seed), float(gas_temperature),
+            float(gas_mass), float(threshold), masses)
 
 
 def null_collision_method(particles, density, cross_sections, dt, max_particles, IONIZATION=True, seed=0,
@@ -164,8 +183,9 @@ def null_collision_method(particles, density, cross_sections, dt, max_particles,
     ions = [k for k, s in enumerate(particles.species) if s.charge > 0]
     s_i = ions[0] if ions else s_e
     grid = log_grid()
-    key = (id(particles), float(density), float(dt), bool(IONIZATION), id(cross_sections))
-    op = _operators.get(key)
+    key = _operator_key(particles, density, cross_sections, dt, IONIZATION, seed, gas_temperature, gas_mass,
+                        ionization_threshold)
+    op = _operators.pop(key, None)
     if op is None:
         t = MccTables(grid, density, gas_temperature, gas_mass)
         t.add(s_e, ELASTIC, resample(*cross_sections[0], grid))
@@ -176,7 +196,9 @@ def null_collision_method(particles, density, cross_sections, dt, max_particles,
             t.add(s_e, IONIZATION, resample(e_ion, s_ion, grid), threshold=thr)
             t.set_products(s_e, s_e, s_i)
         op = MccOperator(t, [s.mass for s in particles.species], dt, seed=seed)
-        _operators[key] = op
+    _operators[key] = op  # most recently used last
+    while len(_operators) > _MAX_OPERATORS:
+        _operators.pop(next(iter(_operators)))
     sp = particles.species[s_e]
     op.apply(s_e, sp.x, sp.y, sp.vx, sp.vy, sp.vz, sp.n)
     species, bx, by, bvx, bvy, bvz = op.take_births()

@@ -156,6 +156,7 @@ SIGNATURES = {
     "pic_mg_solve_async": [_vp, _vp, _vp, _d, _i, _vp],
     "pic_mg_read_info": [_vp, _d, C.POINTER(MgInfo)],
     "pic_mg_effective_launch_mode": [_vp, C.POINTER(_i)],
+    "pic_mg_set_wait_limit": [_vp, C.c_longlong],
     "pic_sorter_create": [_i, _i, _i, _i, C.POINTER(_vp)],
     "pic_sorter_destroy": [_vp],
     "pic_sort": [_vp, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
@@ -172,10 +173,13 @@ SIGNATURES = {
     "pic_sim_sync": [_vp, _vp],
     "pic_sim_species_arrays": [_vp, _i, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)],
     "pic_sim_fields": [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)],
+    "pic_sim_read_particles": [_vp, _i, _vp, C.c_longlong, C.POINTER(_i), _vp],
+    "pic_sim_sort": [_vp, _vp],
     "pic_sim_read_counters": [_vp, C.POINTER(SimCounters), _vp],
     "pic_sim_diagnostics": [_vp, C.c_void_p, _vp],
     "pic_sim_kernel_launches": [_vp],
     "pic_sim_set_profiling": [_vp, _i],
+    "pic_sim_set_wait_limit": [_vp, C.c_longlong],
     "pic_sim_read_profile": [_vp, C.c_void_p],
     "pic_ens_create": [C.POINTER(_vp), _i, C.POINTER(_vp)],
     "pic_ens_destroy": [_vp],

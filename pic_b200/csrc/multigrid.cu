@@ -1155,10 +1155,11 @@ struct GridBar {
 };
 
 // Grid-wide barrier of a cooperative launch; false (and *error set) if it
-// did not complete within kBarrierPolls polls.  On a timeout the block also
-// records, in error[1..5], the barrier's sequence number, its block index and
-// the counter state it saw.
-__device__ __forceinline__ bool grid_barrier(GridBar* b, int* error, int seq) {
+// did not complete within `polls` polls (kBarrierPolls unless the solver's
+// wait limit was changed).  On a timeout the block also records, in
+// error[1..5], the barrier's sequence number, its block index and the counter
+// state it saw.
+__device__ __forceinline__ bool grid_barrier(GridBar* b, int* error, int seq, unsigned long long polls) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1173,7 +1174,7 @@ __device__ __forceinline__ bool grid_barrier(GridBar* b, int* error, int seq) {
         } else {
             unsigned long long k = 0;
             while (gen.load(cuda::memory_order_acquire) == g) {
-                if (++k > kBarrierPolls) {
+                if (++k > polls) {
                     ok = 0;
                     if (atomicExch(error, 1) == 0) {
                         error[1] = seq;
@@ -1209,6 +1210,7 @@ struct SolveDesc {
     int pre, post;
     GridBar* bar;
     int* error;
+    unsigned long long polls;  // grid-barrier wait limit
 };
 
 // FP64 residual of phi on level 0 (written to g0 as the next V-cycle's
@@ -1259,7 +1261,7 @@ __device__ bool r0_phase(const SolveDesc<T>& S, double& r2, double& f2, int& seq
         S.N.partial[blockIdx.x] = sa;
         S.N.partial[nb + blockIdx.x] = sb;
     }
-    if (!grid_barrier(S.bar, S.error, seq++)) return false;
+    if (!grid_barrier(S.bar, S.error, seq++, S.polls)) return false;
     const volatile double* P = S.N.partial;
     double sa = 0.0, sb = 0.0;
     for (int q = threadIdx.x; q < nb; q += blockDim.x) {
@@ -1300,15 +1302,15 @@ __global__ void __launch_bounds__(kMgThreads) k_mg_solve(SolveDesc<T> S) {
             const int tnx = (S.lv[l].nx + kMgTile - 1) / kMgTile, tny = (S.lv[l].ny + kMgTile - 1) / kMgTile;
             for (int t = blockIdx.x; t < tnx * tny; t += gridDim.x)
                 down_tile_n(S.pre, S.lv[l], S.lv[l + 1], S.omega, t % tnx, t / tnx, smem);
-            if (!grid_barrier(S.bar, S.error, seq++)) return;
+            if (!grid_barrier(S.bar, S.error, seq++, S.polls)) return;
         }
         if (blockIdx.x == 0) coarse_vcycle(S.coarse, smem);
-        if (!grid_barrier(S.bar, S.error, seq++)) return;
+        if (!grid_barrier(S.bar, S.error, seq++, S.polls)) return;
         for (int l = S.Lp - 1; l >= 0; --l) {
             const int tnx = (S.lv[l].nx + kMgTile - 1) / kMgTile, tny = (S.lv[l].ny + kMgTile - 1) / kMgTile;
             for (int t = blockIdx.x; t < tnx * tny; t += gridDim.x)
                 up_tile_n(S.post, S.lv[l], S.lv[l + 1], S.omega, l == 0 ? S.phi : nullptr, t % tnx, t / tnx, smem);
-            if (!grid_barrier(S.bar, S.error, seq++)) return;
+            if (!grid_barrier(S.bar, S.error, seq++, S.polls)) return;
         }
         if (!r0_phase(S, r2, dummy, seq)) return;
         ++cycles;
@@ -1712,6 +1714,7 @@ struct MgImpl {
     size_t cluster_smem = 0;
     GridBar* bar = nullptr;
     int* error = nullptr;
+    unsigned long long wait_polls = kBarrierPolls;  // grid-barrier wait limit of the persistent solve
     cudaStream_t side = nullptr;
     cudaStream_t cap = nullptr;
     // cached solve graph
@@ -2446,6 +2449,7 @@ static int launch_persistent(MgImpl& M, std::vector<LevelDev<T>>& lv_in, double*
     S.post = M.o.post_sweeps;
     S.bar = M.bar;
     S.error = M.error;
+    S.polls = M.wait_polls;
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(M.solve_grid);
     cfg.blockDim = dim3(kMgThreads);
@@ -2579,11 +2583,17 @@ int mg_read_info(MgImpl& M, pic_mg_info* info) {
     PIC_CUDA(cudaMemcpy(small, M.N.norms, sizeof small, cudaMemcpyDeviceToHost));
     int err[6];
     memcpy(err, small + 48, sizeof err);
-    if (err[0])
+    if (err[0]) {
+        // the solve gave up (no kernel of it is still running: the stream was
+        // synchronised): clear the flag and the barrier, so that the solver
+        // can be used again, and report the timeout
+        PIC_CUDA(cudaMemset(M.bar, 0, sizeof(GridBar)));
+        PIC_CUDA(cudaMemset(M.error, 0, 6 * sizeof(int)));
         return fail(PIC_ERR_TIMEOUT,
                     "multigrid: grid barrier %d of the persistent solve timed out (block %d saw count %d, "
                     "generation %d, waited on %d)",
                     err[1], err[2], err[3], err[4], err[5]);
+    }
     double norms[2];
     int conv, cycles;
     memcpy(norms, small, 16);
@@ -2718,6 +2728,13 @@ int pic_mg_solve_async(pic_mg* mg, double* d_phi, const double* d_f, double tol,
     if (!mg || !d_phi || !d_f || !(tol > 0) || cycles < 0)
         return fail(PIC_ERR_BAD_ARG, "pic_mg_solve_async: bad arguments");
     return mg_launch(mg->m, d_phi, d_f, tol, cycles, 0, as_stream(stream));
+}
+
+int pic_mg_set_wait_limit(pic_mg* mg, long long polls) {
+    clear_error();
+    if (!mg) return fail(PIC_ERR_BAD_ARG, "pic_mg_set_wait_limit: mg is NULL");
+    mg->m.wait_polls = polls < 0 ? kBarrierPolls : (unsigned long long)polls;
+    return PIC_OK;
 }
 
 int pic_mg_read_info(pic_mg* mg, double tol, pic_mg_info* info) {

@@ -8,8 +8,11 @@
 //   downsweep stable ranks inside each 4096-key sub-tile (warp match_any in
 //             index order), scattered to their global slots
 // Dead particles (NaN position) get the largest key and are dropped.
+#include <cuda.h>
+
 #include <algorithm>
 #include <atomic>
+#include <mutex>
 #include <vector>
 
 #include "sort_internal.cuh"
@@ -229,6 +232,13 @@ __global__ void k_gather5(const uint32_t* __restrict__ perm, const int* __restri
     }
 }
 
+// The permutation alone (no arrays gathered): its first *live entries.
+__global__ void k_copy_perm(const uint32_t* __restrict__ perm, const int* __restrict__ live,
+                            uint32_t* __restrict__ perm_out) {
+    const int n = *live;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) perm_out[k] = perm[k];
+}
+
 __global__ void k_set_n(int* n_dev, int n) {
     n_dev[0] = n;
     n_dev[1] = 0;
@@ -313,7 +323,7 @@ int sort_run(SortImpl& S, const int* d_n, const float* x, const float* y, const 
     if (xo) k_gather5<<<grid_blocks(cap, 256), 256, 0, st>>>(perm, S.n_dev + 1, x, y, vx, vy, vz, xo, yo, vxo, vyo,
                                                              vzo, perm_out);
     else if (perm_out)
-        PIC_CUDA(cudaMemcpyAsync(perm_out, perm, sizeof(uint32_t) * cap, cudaMemcpyDeviceToDevice, st));
+        k_copy_perm<<<grid_blocks(cap, 256), 256, 0, st>>>(perm, S.n_dev + 1, perm_out);
     PIC_LAUNCH_CHECK();
     return PIC_OK;
 }
@@ -325,7 +335,8 @@ int sort_run(SortImpl& S, const int* d_n, const float* x, const float* y, const 
 // kStaticSortBytes, which every GPU that loads the library holds until the
 // process exits.  Every call shares it: calls that overlap on the GPU race.
 // The first call on a device, with that device current, looks up the array's
-// address (cudaGetSymbolAddress) and caches it; that first call should come
+// address (cudaGetSymbolAddress) and caches it with the device's context (a
+// call after a device reset looks it up again); that first call should come
 // before any stream capture.
 constexpr int kStaticSortCtas = 256;  // upper bound of the radix passes' CTA count
 constexpr size_t kStaticSortKeyBytes = sizeof(uint32_t) * size_t(PIC_SORT_STATIC_MAX);
@@ -335,22 +346,54 @@ constexpr size_t kStaticSortBytes = 4 * kStaticSortKeyBytes + kStaticSortCntByte
 static __device__ __align__(256) unsigned char g_sort_scratch[kStaticSortBytes];
 
 constexpr int kStaticMaxDevices = 64;
-static std::atomic<unsigned char*> g_sort_scratch_ptr[kStaticMaxDevices];
 
-// Address of this device's scratch array (looked up once per device).
-static int static_scratch(unsigned char** out) {
+// Per device: the context the scratch address was looked up in, the address
+// and the device's SM count.  A device reset (cudaDeviceReset) gives the
+// device a new primary context in which the module, and the array, are
+// loaded anew: the address is then looked up again.
+struct StaticScratch {
+    CUcontext ctx = nullptr;
+    unsigned char* ptr = nullptr;
+    int sms = 0;
+};
+static StaticScratch g_sort_scratch_at[kStaticMaxDevices];
+static std::mutex g_sort_scratch_mu;
+
+// Address of the current device's scratch array and its SM count.
+static int static_scratch(unsigned char** out, int* sms) {
     int dev = 0;
     PIC_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kStaticMaxDevices)
         return fail(PIC_ERR_BAD_ARG, "pic_sort_static: device %d beyond the supported %d", dev, kStaticMaxDevices);
-    unsigned char* p = g_sort_scratch_ptr[dev].load(std::memory_order_acquire);
-    if (!p) {
+    PIC_CUDA(cudaFree(nullptr));  // makes the device's primary context current
+    // cuCtxGetCurrent through the runtime's entry-point lookup, so that the
+    // library does not link the driver library itself
+    using CtxGetCurrent = CUresult (*)(CUcontext*);
+    static CtxGetCurrent get_ctx = nullptr;
+    if (!get_ctx) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        PIC_CUDA(cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !fn)
+            return fail(PIC_ERR_CUDA, "pic_sort_static: cuCtxGetCurrent not found");
+        get_ctx = reinterpret_cast<CtxGetCurrent>(fn);
+    }
+    CUcontext ctx = nullptr;
+    if (get_ctx(&ctx) != CUDA_SUCCESS || !ctx)
+        return fail(PIC_ERR_CUDA, "pic_sort_static: no current context on device %d", dev);
+    std::lock_guard<std::mutex> lock(g_sort_scratch_mu);
+    StaticScratch& S = g_sort_scratch_at[dev];
+    if (S.ctx != ctx || !S.ptr) {
         void* addr = nullptr;
         PIC_CUDA(cudaGetSymbolAddress(&addr, g_sort_scratch));
-        p = static_cast<unsigned char*>(addr);
-        g_sort_scratch_ptr[dev].store(p, std::memory_order_release);
+        int n = 0;
+        PIC_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+        S.ctx = ctx;
+        S.ptr = static_cast<unsigned char*>(addr);
+        S.sms = n;
     }
-    *out = p;
+    *out = S.ptr;
+    *sms = S.sms;
     return PIC_OK;
 }
 
@@ -428,9 +471,10 @@ int pic_sort_static(const float* d_x, const float* d_y, const float* d_vx, const
     int bits = 0;
     while ((1ull << bits) <= nkeys) ++bits;
     S.passes = (bits + 7) / 8;
-    S.G = std::max(1, std::min(std::min(num_sms(), kStaticSortCtas), div_up(S.capacity, kSortSub)));
     unsigned char* base = nullptr;
-    PIC_TRY(static_scratch(&base));
+    int sms = 0;
+    PIC_TRY(static_scratch(&base, &sms));
+    S.G = std::max(1, std::min(std::min(sms, kStaticSortCtas), div_up(S.capacity, kSortSub)));
     S.k0 = reinterpret_cast<uint32_t*>(base);
     S.k1 = reinterpret_cast<uint32_t*>(base + kStaticSortKeyBytes);
     S.v0 = reinterpret_cast<uint32_t*>(base + 2 * kStaticSortKeyBytes);

@@ -106,6 +106,7 @@ struct PushArgs {
     int cand_cap;
     unsigned long long* ctr;
     int* error;  // set when a bounded wait gives up
+    unsigned long long wait_limit;  // polls of a chunk wait (kWaitLimit unless changed)
 };
 
 // ---- TMA bulk copies and mbarriers (inline PTX, no multicast) -------------------
@@ -141,9 +142,9 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* m, unsigned pa
     return ok != 0;
 }
 
-// Waits for the phase with the given parity; false after kWaitLimit polls.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* m, unsigned parity) {
-    for (unsigned long long k = 0; k < kWaitLimit; ++k)
+// Waits for the phase with the given parity; false after `limit` polls.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* m, unsigned parity, unsigned long long limit) {
+    for (unsigned long long k = 0; k < limit; ++k)
         if (mbar_try_wait(m, parity)) return true;
     return false;
 }
@@ -328,14 +329,14 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
         const int prv = cur == 0 ? kStages - 1 : cur - 1;
         const int nxt = cur == kStages - 1 ? 0 : cur + 1;
         const unsigned par = (phases >> cur) & 1u;
-        const bool ok = mbar_wait(&bar[cur], par);
+        const bool ok = mbar_wait(&bar[cur], par, A.wait_limit);
         phases ^= 1u << cur;
         if (__syncthreads_or(!ok)) {
             // give up on this launch: flag it, then wait (bounded) for the one
             // load in flight (the next chunk's load is issued only after a wait succeeds)
             if (tid == 0) {
                 atomicExch(A.error, 1);
-                mbar_wait(&bar[cur], par);
+                mbar_wait(&bar[cur], par, kWaitLimit);
             }
             __syncthreads();
             break;
@@ -871,6 +872,7 @@ struct SimImpl {
     BirthDev births{};
     unsigned long long* ctr = nullptr;
     int* error = nullptr;
+    unsigned long long wait_limit = kWaitLimit;  // polls of k_push's chunk waits
     float2* E2 = nullptr;
     float *Ex = nullptr, *Ey = nullptr, *rho_acc = nullptr, *rho_out = nullptr;
     double *phi = nullptr, *f = nullptr, *phi_prev = nullptr;
@@ -975,6 +977,7 @@ static PushArgs push_args(SimImpl& S, int kick, int mcc, int drift, int deposit,
     A.cand_cap = S.cand_cap;
     A.ctr = S.ctr;
     A.error = S.error;
+    A.wait_limit = S.wait_limit;
     return A;
 }
 
@@ -1645,6 +1648,40 @@ int pic_sim_species_arrays(pic_sim* sim, int s, float** x, float** y, float** vx
     return PIC_OK;
 }
 
+int pic_sim_read_particles(pic_sim* sim, int s, float* h_out, long long capacity, int* count, void* stream) {
+    clear_error();
+    if (!sim || s < 0 || s >= sim->s.ns || !h_out || !count || capacity < 0)
+        return fail(PIC_ERR_BAD_ARG, "pic_sim_read_particles: bad arguments");
+    SimImpl& S = sim->s;
+    cudaStream_t st = as_stream(stream);
+    PIC_CUDA(cudaStreamSynchronize(st));
+    PIC_CUDA(cudaMemcpy(&S.h_state[s], S.d_state + s, sizeof(SpeciesState), cudaMemcpyDeviceToHost));
+    const SpeciesState& H = S.h_state[s];
+    *count = H.count;
+    if (5LL * H.count > capacity)
+        return fail(PIC_ERR_OUT_OF_CAPACITY, "pic_sim_read_particles: %d slots need %lld floats, capacity %lld",
+                    H.count, 5LL * H.count, capacity);
+    if (H.count == 0) return PIC_OK;
+    // the five arrays share one allocation at a fixed stride: one 2D copy
+    const size_t w = sizeof(float) * size_t(H.count);
+    PIC_CUDA(cudaMemcpy2DAsync(h_out, w, H.cur[0], sizeof(float) * size_t(H.stride), w, 5, cudaMemcpyDeviceToHost,
+                               st));
+    return PIC_OK;
+}
+
+int pic_sim_sort(pic_sim* sim, void* stream) {
+    clear_error();
+    if (!sim) return fail(PIC_ERR_BAD_ARG, "pic_sim_sort: sim is NULL");
+    SimImpl& S = sim->s;
+    if (!S.have_sorter) return fail(PIC_ERR_BAD_ARG, "pic_sim_sort: the simulation was created without a sort");
+    cudaStream_t st = as_stream(stream);
+    PIC_TRY(sort_all(S, st));
+    // a pass prepared by the last captured step holds work items of the
+    // unsorted order: rebuild them for the same step (the counter stays)
+    if (S.prepared) PIC_TRY(prepare_pass(S, st, 1, 0));
+    return PIC_OK;
+}
+
 int pic_sim_fields(pic_sim* sim, double** phi, float** rho, float** Ex, float** Ey) {
     clear_error();
     if (!sim) return fail(PIC_ERR_BAD_ARG, "pic_sim_fields: sim is NULL");
@@ -1680,6 +1717,13 @@ int pic_sim_read_counters(pic_sim* sim, pic_sim_counters* out, void* stream) {
     if (!sim || !out) return fail(PIC_ERR_BAD_ARG, "pic_sim_read_counters: bad arguments");
     SimImpl& S = sim->s;
     PIC_CUDA(cudaStreamSynchronize(as_stream(stream)));
+    int err = 0;
+    PIC_CUDA(cudaMemcpy(&err, S.error, sizeof err, cudaMemcpyDeviceToHost));
+    if (err) {
+        PIC_CUDA(cudaMemset(S.error, 0, sizeof err));
+        return fail(PIC_ERR_TIMEOUT, "particle pass: a wait on a bulk copy into shared memory gave up after %llu polls",
+                    S.wait_limit);
+    }
     unsigned long long c[kCtrCount];
     PIC_CUDA(cudaMemcpy(c, S.ctr, sizeof c, cudaMemcpyDeviceToHost));
     SpeciesState hs[PIC_MAX_SPECIES];
@@ -1699,6 +1743,20 @@ int pic_sim_read_counters(pic_sim* sim, pic_sim_counters* out, void* stream) {
     out->last_cycles = S.last.cycles;
     out->last_rel_res = S.last.rel_res;
     out->steps = S.steps;
+    return PIC_OK;
+}
+
+int pic_sim_set_wait_limit(pic_sim* sim, long long polls) {
+    clear_error();
+    if (!sim) return fail(PIC_ERR_BAD_ARG, "pic_sim_set_wait_limit: sim is NULL");
+    SimImpl& S = sim->s;
+    PIC_CUDA(cudaDeviceSynchronize());
+    S.wait_limit = polls < 0 ? kWaitLimit : (unsigned long long)polls;
+    PIC_TRY(pic_mg_set_wait_limit(S.mg, polls));  // the persistent solve's grid barriers
+    // the captured steps hold the old limits in their kernel arguments
+    if (S.g_step) cudaGraphExecDestroy(S.g_step);
+    if (S.g_sort_step) cudaGraphExecDestroy(S.g_sort_step);
+    S.g_step = S.g_sort_step = nullptr;
     return PIC_OK;
 }
 

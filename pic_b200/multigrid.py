@@ -64,6 +64,11 @@ class MultigridSolver:
         _lib.call("pic_mg_effective_launch_mode", self._h, C.byref(m))
         return {v: k for k, v in _lib.MG_LAUNCH_MODES.items()}[m.value]
 
+    def set_wait_limit(self, polls=-1):
+        """Polls a grid barrier of the persistent solve makes before the solve
+        gives up with PIC_ERR_TIMEOUT (raised as PicError); -1 restores the default."""
+        _lib.call("pic_mg_set_wait_limit", self._h, int(polls))
+
     def solve(self, phi, rho, tol=1e-5, smooth_iter=5, solve_iter=20, max_cycles=50, raise_on_fail=False):
         """Solve lap(phi) = rho in place; returns (phi, (cycles, rel_res)) like src/multigrid.py:445-455.
         smooth_iter/solve_iter are accepted for signature compatibility."""

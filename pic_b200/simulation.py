@@ -207,6 +207,19 @@ class PICSimulation:
         n = self.counters()["count"][s]
         return tuple(device_view(p.value, n) for p in ptrs)
 
+    def read_particles(self, s, out):
+        """Copies the slots in use of species s to the host tensor `out`
+        (float32, page-locked for an asynchronous copy, at least 5 * count
+        values) as rows x, y, vx, vy, vz, in one copy on the current stream;
+        returns the (5, count) view of `out`."""
+        n = C.c_int()
+        _lib.call("pic_sim_read_particles", self._h, s, out.data_ptr(), out.numel(), C.byref(n), _lib.stream_ptr())
+        return out[: 5 * n.value].view(5, n.value)
+
+    def sort(self):
+        """The cell sort of every species now (what a step runs every sort_interval steps)."""
+        _lib.call("pic_sim_sort", self._h, _lib.stream_ptr())
+
     def fields(self):
         """Zero-copy views: phi (FP64), rho of the last deposit, Ex, Ey (float32), all nx*ny."""
         p = [C.c_void_p() for _ in range(4)]
@@ -218,6 +231,12 @@ class PICSimulation:
     def kernel_launches(self) -> int:
         """Kernel launches issued since creation."""
         return int(_lib.load().pic_sim_kernel_launches(self._h))
+
+    def set_wait_limit(self, polls=-1):
+        """Polls a bounded device wait (the particle pass's bulk copies, the
+        persistent solve's grid barriers) makes before it gives up; the next
+        counters() raises PicError(PIC_ERR_TIMEOUT).  -1 restores the default."""
+        _lib.call("pic_sim_set_wait_limit", self._h, int(polls))
 
     def set_profiling(self, on: bool):
         _lib.call("pic_sim_set_profiling", self._h, int(bool(on)))

@@ -6,20 +6,25 @@ This script keeps its non-zero entries (row, column, value) in
 lap_cylindrical_10x10.npz so that the CPU tests can pin the oracle's
 restatement of the builder without the reference tree.
 
-    python tests/golden/make_golden_lap.py
+    python tests/golden/make_golden_lap.py [--reference DIR]
+
+The reference tree is --reference DIR, else $PIC_REFERENCE_DIR, else the
+container's read-only checkout.
 """
 from __future__ import annotations
 
+import argparse
 import os
 
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SOURCE = "/root/reference/lap.txt"
 
 
 def main():
-    L = np.loadtxt(SOURCE)
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=os.environ.get("PIC_REFERENCE_DIR", "/root/reference"))
+    L = np.loadtxt(os.path.join(ap.parse_args().reference, "lap.txt"))
     rows, cols = np.nonzero(L)
     np.savez_compressed(os.path.join(HERE, "lap_cylindrical_10x10.npz"), shape=np.array(L.shape),
                         rows=rows.astype(np.int32), cols=cols.astype(np.int32), vals=L[rows, cols])

@@ -71,3 +71,33 @@ def test_sort_is_deterministic_and_handles_empty():
     k, perm, _, ts = run_sort(np.zeros(0, np.float32), np.zeros(0, np.float32), np.zeros(0, np.float32),
                               np.zeros(0, np.float32), np.zeros(0, np.float32), m, m, 16, capacity=16)
     assert k == 0 and np.all(ts == 0)
+
+
+def test_permutation_only_writes_the_live_entries():
+    """pic_sort with d_x_out NULL: the permutation alone, into a buffer sized
+    for n (not for the sorter's larger capacity); nothing past the live count
+    is written (a guard region after n keeps its fill)."""
+    rng = np.random.Generator(np.random.Philox(12))
+    m, tile, n, cap, guard = 129, 16, 50_000, 400_000, 4096
+    x = rng.uniform(0, m - 1, n).astype(np.float32)
+    y = rng.uniform(0, m - 1, n).astype(np.float32)
+    dead = rng.random(n) < 0.05
+    x[dead] = np.nan
+    s = _lib.C.c_void_p()
+    _lib.call("pic_sorter_create", cap, m, m, tile, _lib.C.byref(s))
+    try:
+        X, Y = torch.as_tensor(x, device=DEV), torch.as_tensor(y, device=DEV)
+        perm = torch.full((n + guard,), -7, dtype=torch.int32, device=DEV)
+        cnt = torch.zeros(1, dtype=torch.int32, device=DEV)
+        _lib.call("pic_sort", s, _lib.ptr(X), _lib.ptr(Y), None, None, None, n, None, None, None, None, None,
+                  _lib.ptr(perm), _lib.ptr(cnt), None, _lib.stream_ptr())
+        torch.cuda.synchronize()
+        k = int(cnt.item())
+        got = perm.cpu().numpy()
+    finally:
+        _lib.load().pic_sorter_destroy(s)
+    keys = O.sort_keys(x, y, m, m, tile)
+    ref = np.argsort(keys, kind="stable")[: int((~dead).sum())]
+    assert k == ref.size
+    np.testing.assert_array_equal(got[:k], ref.astype(np.int32))
+    assert np.all(got[k:] == -7)

@@ -10,11 +10,10 @@ the FP32 trajectories against the FP64 reference arithmetic after 20 steps
 """
 import numpy as np
 import pytest
-import scipy.sparse as sp
-import scipy.sparse.linalg as spla
 import torch
 
 from oracle import oracle as O
+from oracle.fp64_step import fp64_reference_run
 from pic_b200 import Consts, workloads
 from pic_b200.simulation import PICSimulation
 
@@ -112,56 +111,6 @@ def test_particle_passes_bit_exact(sort_interval):
     assert rc in (0, 3)
 
 
-def fp64_reference_run(w, arrays, steps):
-    """The reference's step in FP64 (metres), with absorption and a direct Poisson solve."""
-    m, dx = w.nodes, w.dx
-    mask, phi_bc = workloads.dirichlet(w)
-    size = m * m
-    off = np.ones(size)
-    off[m - 1::m] = 0
-    A = sp.diags([np.full(size, -4.0), off[:-1], off[:-1], np.ones(size - m), np.ones(size - m)], [0, 1, -1, m, -m],
-                 (size, size), format="lil") / dx**2
-    A = A.tolil()
-    for k in np.flatnonzero(mask):
-        A.rows[k] = [k]
-        A.data[k] = [1.0]
-    lu = spla.splu(A.tocsc())
-    q = [-Consts.qe, Consts.qe]
-    mass = [Consts.me, workloads.ION_MASS]
-    np2c = [w.np2c(w.n_e), w.np2c(w.n_i)]
-    P = [[a[0].astype(np.float64) * dx, a[1].astype(np.float64) * dx, a[2].astype(np.float64),
-          a[3].astype(np.float64)] for a in arrays]
-    L = dx * (m - 1)
-
-    def solve():
-        rho = np.zeros(size)
-        for s in range(2):
-            live = ~np.isnan(P[s][0])
-            O.deposit_f64(P[s][0][live], P[s][1][live], q[s] * np2c[s], dx, dx, m, m, rho=rho, floorf_quirk=False)
-        b = -rho / (dx * dx) / Consts.eps0
-        b[mask == 1] = phi_bc[mask == 1]
-        return O.update_E_f64(lu.solve(b), m, m, dx, dx)
-
-    def kick(ex, ey, factor):
-        for s in range(2):
-            live = ~np.isnan(P[s][0])
-            vx, vy = P[s][2][live].copy(), P[s][3][live].copy()
-            O.lib().or_update_V_f64(P[s][0][live].copy(), P[s][1][live].copy(), vx, vy, int(live.sum()), ex, ey,
-                                    w.dt * factor * q[s] / mass[s], dx, dx, m, m, 0)
-            P[s][2][live], P[s][3][live] = vx, vy
-
-    kick(*solve(), -0.5)
-    for _ in range(steps):
-        for s in range(2):
-            live = ~np.isnan(P[s][0])
-            x, y = P[s][0][live].copy(), P[s][1][live].copy()
-            O.lib().or_update_R_f64(x, y, P[s][2][live].copy(), P[s][3][live].copy(), len(x), w.dt)
-            O.lib().or_absorb_f64(x, y, len(x), L, L)
-            P[s][0][live], P[s][1][live] = x, y
-        kick(*solve(), 1.0)
-    return P
-
-
 def test_trajectories_against_fp64_reference():
     w = workloads.scaled(workloads.SMALL, n=20_000, left_V=20.0)
     steps = 20
@@ -169,7 +118,7 @@ def test_trajectories_against_fp64_reference():
     sim.init()
     sim.step(steps)
     sim.sync()
-    ref = fp64_reference_run(w, arrays, steps)
+    ref = fp64_reference_run(w, arrays, steps, [-Consts.qe, Consts.qe], [Consts.me, workloads.ION_MASS]).P
     worst = 0.0
     for s in range(2):
         got = host(sim, s)
