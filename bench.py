@@ -53,6 +53,8 @@ def parse():
                     help="steps between cell sorts (80: the autotuner's choice for 513^2 shapes)")
     ap.add_argument("--particles", type=int, default=4_000_000, help="per species")
     ap.add_argument("--tile", type=int, default=16, help="cells per side of the push's work tiles")
+    ap.add_argument("--push", default="warp", choices=["warp", "ring"],
+                    help="particle-pass streaming: per-warp bulk-copy pipelines (warp) or one ring per block (ring)")
     ap.add_argument("--no-poisson", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -300,7 +302,8 @@ def run_ours(args, world, rank, local):
     achieved = bytes_per_launch / (push_ms / 1e3) / 1e9
     peak, peak_kind = peak_hbm()
     traffic = ncu_traffic()
-    roofline = {"bound": "hbm", "kernel": "k_push", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+    roofline = {"bound": "hbm", "kernel": "k_push_warp" if args.push == "warp" else "k_push", "achieved": round(achieved, 1),
+                "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
                 "bytes_per_launch": bytes_per_launch, "ms_per_launch": round(push_ms, 5)}
     phases = {k: round(v["ms"] / args.steps, 4) for k, v in prof.items() if isinstance(v, dict)}
@@ -708,6 +711,7 @@ def main():
     GRAPH_OPTS["pre_sweeps"], GRAPH_OPTS["post_sweeps"] = args.mg_sweeps
     GRAPH_OPTS["omega"] = args.omega
     GRAPH_OPTS["tile"] = args.tile
+    GRAPH_OPTS["push_kernel"] = args.push
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, world, rank)

@@ -353,7 +353,15 @@ typedef struct pic_sim_desc {
     int min_cycles;             /* V-cycles of a step's solve run before its first convergence test
                                    (0: test after every cycle).  In the captured step they are chained
                                    launches; each further cycle is an iteration of a WHILE node. */
+    int push_kernel;            /* pic_push_kernel: how the particle pass streams the particles */
 } pic_sim_desc;
+
+/* The particle pass's two streaming schemes; both do the same arithmetic and
+ * give bit-identical particles and charge. */
+typedef enum pic_push_kernel {
+    PIC_PUSH_WARP = 0, /* each warp streams its own groups of particles through its own bulk-copy stages */
+    PIC_PUSH_RING = 1  /* the block streams chunks through one shared three-stage ring */
+} pic_push_kernel;
 
 typedef struct pic_sim_counters {
     unsigned long long absorbed[PIC_MAX_SPECIES];

@@ -95,7 +95,10 @@ class SimDesc(C.Structure):
                 ("eps0", C.c_double), ("nspecies", C.c_int), ("species", SpeciesDesc * PIC_MAX_SPECIES),
                 ("h_dirichlet", C.c_void_p), ("h_phi_bc", C.c_void_p), ("tol", C.c_double), ("max_cycles", C.c_int),
                 ("mg", MgOptions), ("sort_interval", C.c_int), ("tile", C.c_int), ("mcc", C.c_void_p),
-                ("seed", C.c_ulonglong), ("use_graph", C.c_int), ("min_cycles", C.c_int)]
+                ("seed", C.c_ulonglong), ("use_graph", C.c_int), ("min_cycles", C.c_int), ("push_kernel", C.c_int)]
+
+
+PUSH_KERNELS = {"warp": 0, "ring": 1}
 
 
 PIC_ADJ_MAX_SEGMENTS = 16

@@ -10,20 +10,30 @@
 // the coarsest level.  Dirichlet nodes (mask = 1, and the grid edges) carry a
 // zero correction; a coarse node is Dirichlet when its injected fine node is.
 //
-// Kernels per V-cycle (8 launches for a 513^2 grid):
-//   down(l)   l < Lc: 2*pre red/black half-sweeps on a 32x32 tile held in
-//             shared memory with a halo of 2*pre+2 nodes (the valid region
-//             shrinks by one node per half-sweep), then the residual and its
-//             full-weighting restriction to level l+1
-//   coarse    one CTA: the whole V-cycle of the levels that fit in shared
-//             memory (<= 33^2 nodes), down to the direct solve and back up
-//   up(l)     prolongation-add of level l+1 and 2*post half-sweeps on a tile
-//             with a halo of 2*post; on level 0 it adds e to phi instead of
-//             storing e
-//   r0        the FP64 residual, a deterministic norm (last-block reduction)
-//             and the loop decision
-// The loop is a CUDA-graph conditional WHILE node whose condition r0 sets,
-// so a solve issues no host synchronisation.
+// Kernels per V-cycle in the graph and host loops (7 launches for a 513^2
+// grid):
+//   down(l)     2*pre red/black half-sweeps on a 32x32 tile held in shared
+//               memory with a halo wide enough for them, then the residual
+//               and its full-weighting restriction to level l+1; on level 0
+//               the right-hand side is the FP64 residual r
+//   down2       the down phases of two levels (129^2 and 65^2 at 513^2) in
+//               one launch, over halos wide enough that the coarser level's
+//               tile equals what two launches give
+//   direct      e = A^-1 g on the first level of at most 33^2 nodes (the
+//               dense inverse of that level's operator on its free nodes,
+//               formed at creation), one warp per row
+//   up2         the up phases of the same two levels in one launch
+//   up(l)       prolongation-add of level l+1 and 2*post half-sweeps
+//   up_res      the finest up phase: phi += e, the FP64 residual updated on
+//               the tile (r -= A e), its norm (deterministic last-block
+//               reduction) and the loop decision
+//   r0          once per solve, before the first cycle: r = f - A phi in
+//               FP64, its norm and the first loop decision
+// The single-CTA coarse kernel (every level of at most 33^2 nodes in shared
+// memory, down to a dense solve) serves grids that small and the persistent
+// and cluster modes.  The loop is a CUDA-graph conditional WHILE node whose
+// condition up_res (r0 before the first cycle) sets, so a solve issues no
+// host synchronisation.
 #include <cooperative_groups.h>
 #include <cuda/atomic>
 

@@ -120,8 +120,10 @@ __device__ __forceinline__ double2 grad_node(const double* __restrict__ phi, int
     return make_double2(ex, ey);
 }
 
+// E2 (when given) is the interleaved (Ex, Ey) copy the particle pass
+// gathers from, with rows `ep` nodes apart.
 __global__ void k_update_E(const double* __restrict__ phi, float* __restrict__ Ex, float* __restrict__ Ey,
-                           float2* __restrict__ E2, int nx, int ny, double dx, double dy, int axis) {
+                           float2* __restrict__ E2, int ep, int nx, int ny, double dx, double dy, int axis) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
     if (i >= nx) return;
@@ -130,7 +132,7 @@ __global__ void k_update_E(const double* __restrict__ phi, float* __restrict__ E
     const float fx = float(e.x), fy = float(e.y);
     if (Ex) Ex[k] = fx;
     if (Ey) Ey[k] = fy;
-    if (E2) E2[k] = make_float2(fx, fy);
+    if (E2) E2[long(j) * ep + i] = make_float2(fx, fy);
 }
 
 // rho -> f = -rho/eps0 on free nodes.  With phi_prev given, also replaces the
@@ -190,10 +192,10 @@ int grid_blocks(long n, int threads) {
     return int(b);
 }
 
-int launch_update_E(const double* phi, float* Ex, float* Ey, float2* E2, int nx, int ny, double dx, double dy,
-                    cudaStream_t st, bool axis) {
+int launch_update_E(const double* phi, float* Ex, float* Ey, float2* E2, int ep, int nx, int ny, double dx,
+                    double dy, cudaStream_t st, bool axis) {
     dim3 grid(div_up(nx, 128), ny);
-    k_update_E<<<grid, 128, 0, st>>>(phi, Ex, Ey, E2, nx, ny, dx, dy, axis ? 1 : 0);
+    k_update_E<<<grid, 128, 0, st>>>(phi, Ex, Ey, E2, ep, nx, ny, dx, dy, axis ? 1 : 0);
     PIC_LAUNCH_CHECK();
     return PIC_OK;
 }
@@ -263,7 +265,7 @@ int pic_update_E(const double* d_phi, float* d_Ex, float* d_Ey, int nx, int ny, 
     clear_error();
     if (!d_phi || !d_Ex || !d_Ey || nx < 2 || ny < 2 || !(dx > 0) || !(dy > 0))
         return fail(PIC_ERR_BAD_ARG, "pic_update_E: bad arguments");
-    return launch_update_E(d_phi, d_Ex, d_Ey, nullptr, nx, ny, dx, dy, as_stream(stream), false);
+    return launch_update_E(d_phi, d_Ex, d_Ey, nullptr, nx, nx, ny, dx, dy, as_stream(stream), false);
 }
 
 int pic_update_E_rz(const double* d_phi, float* d_Ex, float* d_Ey, int nx, int ny, double dx, double dy,
@@ -271,7 +273,7 @@ int pic_update_E_rz(const double* d_phi, float* d_Ex, float* d_Ey, int nx, int n
     clear_error();
     if (!d_phi || !d_Ex || !d_Ey || nx < 2 || ny < 2 || !(dx > 0) || !(dy > 0))
         return fail(PIC_ERR_BAD_ARG, "pic_update_E_rz: bad arguments");
-    return launch_update_E(d_phi, d_Ex, d_Ey, nullptr, nx, ny, dx, dy, as_stream(stream), true);
+    return launch_update_E(d_phi, d_Ex, d_Ey, nullptr, nx, nx, ny, dx, dy, as_stream(stream), true);
 }
 
 int pic_rz_density(float* d_rho, int nx, int ny, double dy, void* stream) {

@@ -11,17 +11,21 @@
 // Particle pass: persistent CTAs take work items (species, tile, [begin,end))
 // from an atomic counter.  Items of sorted particles belong to one tile of
 // tile x tile cells: the CTA stages the tile's E field (with a halo) and a
-// charge accumulator in shared memory, processes its particles in a blocked
-// order (consecutive sorted particles per thread, so the deposit accumulates
-// in registers while the cell repeats) and flushes the charge tile once with
-// global atomics.  Particles that left the staged region since the last sort
-// gather from and deposit to global memory directly.  Particles born since
-// the last sort are processed as untiled items.
+// charge accumulator (2^-19 fixed point) in shared memory, pushes the item's
+// particles and flushes the charge tile once with global atomics.  Particles
+// that left the staged region since the last sort gather from and deposit to
+// global memory directly.  Particles born since the last sort are processed
+// as untiled items.  Two streaming schemes, bit-identical in their results:
+// k_push_warp (the default) gives every warp its own pipeline of bulk copies
+// and deposits with warp-aggregated atomics; k_push streams chunks through
+// one ring per block.
 #include <algorithm>
 #include <climits>
 #include <cmath>
 #include <cstddef>
 #include <vector>
+
+#include <cuda.h>
 
 #include "mcc_host.cuh"
 #include "sort_internal.cuh"
@@ -29,7 +33,7 @@
 namespace pic {
 
 int grid_blocks(long n, int threads);
-int launch_update_E(const double* phi, float* Ex, float* Ey, float2* E2, int nx, int ny, double dx, double dy,
+int launch_update_E(const double* phi, float* Ex, float* Ey, float2* E2, int ep, int nx, int ny, double dx, double dy,
                     cudaStream_t st, bool axis);
 int launch_form_rhs(const float* rho, const uint8_t* dirichlet, double eps0, double* f, float* snapshot, float* zero,
                     double* phi, double* phi_prev, long G, cudaStream_t st, const double* rowf, int nx);
@@ -83,7 +87,8 @@ struct SpeciesConst {
     float scale;       // q np2c / (dx dy)
 };
 
-struct PushArgs {
+struct alignas(64) PushArgs {
+    CUtensorMap emap;  // E (interleaved Ex, Ey as 8-byte elements, nx x ny, rows ep apart): the E tiles' bulk loads
     SpeciesState* state;
     SpeciesConst sp[PIC_MAX_SPECIES];
     const int4* items;
@@ -92,6 +97,8 @@ struct PushArgs {
     const float2* E;
     float* rho;
     int nx, ny, tile, tiles_x, rw;
+    int ep;  // row pitch of E in nodes (nx rounded up to even: 16-byte row strides for the tensor map)
+    int ew;  // row width of k_push_warp's E tile (rw rounded up to even)
     int do_kick, do_mcc, do_drift, do_deposit;
     const MccDev* mcc;  // device copy of the tables' descriptor
     uint2 key;
@@ -232,7 +239,7 @@ __device__ __forceinline__ void stage_tile(const PushArgs& A, int tile, float4* 
         const int gi = ox + q % RW, gj = oy + q / RW;
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
         if (gi >= 0 && gj >= 0 && gi < A.nx && gj < A.ny) {
-            const long k = long(gj) * A.nx + gi;
+            const long k = long(gj) * A.ep + gi;
             const float2 e0 = __ldg(A.E + k), e1 = __ldg(A.E + k + (gi + 1 < A.nx ? 1 : 0));
             v = make_float4(e0.x, e0.y, e1.x, e1.y);
         }
@@ -398,10 +405,10 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
                     e01 = make_float2(p1.x, p1.y);
                     e11 = make_float2(p1.z, p1.w);
                 } else {
-                    e00 = __ldg(A.E + long(c.j0) * A.nx + c.i0);
-                    e10 = __ldg(A.E + long(c.j0) * A.nx + c.i1);
-                    e01 = __ldg(A.E + long(c.j1) * A.nx + c.i0);
-                    e11 = __ldg(A.E + long(c.j1) * A.nx + c.i1);
+                    e00 = __ldg(A.E + long(c.j0) * A.ep + c.i0);
+                    e10 = __ldg(A.E + long(c.j0) * A.ep + c.i1);
+                    e01 = __ldg(A.E + long(c.j1) * A.ep + c.i0);
+                    e11 = __ldg(A.E + long(c.j1) * A.ep + c.i1);
                 }
                 vx = __fmaf_rn(C.kq, cic_interp(c, e00.x, e10.x, e01.x, e11.x), vx);
                 vy = __fmaf_rn(C.kq, cic_interp(c, e00.y, e10.y, e01.y, e11.y), vy);
@@ -513,6 +520,349 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
         store_chunk_edges(A, prev, bufs + prv * 4 * kBufStride, tid);
     }
     if (tid == 0) bulk_wait_all();
+}
+
+// ---- particle pass, per-warp pipeline --------------------------------------------
+//
+// The same work as k_push (same work units, E tile and charge tile per unit,
+// same per-particle arithmetic), streamed differently: every warp runs its
+// own pipeline of bulk copies instead of the CTA sharing one ring.  A unit's
+// slots are cut into groups of kWarpGroup particles, dealt round-robin to the
+// eight warps; lane 0 of each warp keeps up to kWarpStages - 1 of its groups
+// in flight (cp.async.bulk of x, y, vx, vy into the warp's own stage buffers,
+// completed on the warp's own mbarriers), running ahead into the next unit,
+// whose descriptor is claimed one unit early.  Lane l of a group handles the
+// particles l, l + 32, l + 64, ...: coalesced, conflict-free reads of the stage
+// and coalesced stores of the results straight to global memory.  The only
+// block barriers are the three per unit (E tile staged; deposits done; charge
+// tile flushed), so a warp waits only on its own copies.
+//
+// The charge tile is deposited with warp-aggregated atomics when DEPOSIT_AGG:
+// lanes whose particles fall in the same cell (sorted particles put runs of
+// consecutive lanes in one cell) sum their four fixed-point weights with
+// redux.sync over __match_any_sync's group, and the group's lowest lane adds
+// the sums.  Integer sums are exact, so the tile holds the same values either way.
+constexpr bool kDepositAgg = true;  // warp-aggregated charge-tile atomics in k_push_warp
+constexpr int kWarpGroup = 128;  // particles per group (four per lane)
+constexpr int kWarpStages = 3;   // stage buffers per warp
+constexpr int kPushWarps = kPushThreads / 32;
+
+struct UnitDesc {
+    int valid;
+    int s, tile, b, e;
+};
+
+__device__ __forceinline__ UnitDesc claim_unit(const PushArgs& A, int n_items) {
+    UnitDesc u;
+    const int it = atomicAdd(A.item_next, 1);
+    u.valid = it < n_items;
+    u.s = u.tile = u.b = u.e = 0;
+    if (u.valid) {
+        const int4 v = A.items[it];
+        u.s = v.x;
+        u.tile = v.y;
+        u.b = v.z;
+        u.e = v.w;
+    }
+    return u;
+}
+
+// Per-warp producer state (meaningful in lane 0): the next group to load is
+// the pj-th of this warp in unit pu; `issued` groups were loaded so far.
+struct WarpFeed {
+    int pu, pj, issued;
+};
+
+// Lane 0: loads this warp's next groups while stage buffers are free and the
+// units are known (the current one and the next).
+__device__ __forceinline__ void warp_feed(const PushArgs& A, const UnitDesc* units, int kcur, int consumed,
+                                          WarpFeed& f, int warp, float* wbuf, unsigned long long* wbar) {
+    while (f.issued - consumed < kWarpStages && f.pu <= kcur + 1) {
+        const UnitDesc& U = units[f.pu & 1];
+        if (!U.valid) return;
+        const int w0 = (U.b & ~3) + (f.pj * kPushWarps + warp) * kWarpGroup;
+        if (w0 >= U.e) {
+            ++f.pu;
+            f.pj = 0;
+            continue;
+        }
+        const int w1 = min(w0 + kWarpGroup, (U.e + 3) & ~3);
+        const int st = f.issued % kWarpStages;
+        const unsigned bytes = unsigned(w1 - w0) * 4u;
+        float* buf = wbuf + st * 4 * kWarpGroup;
+        unsigned long long* bar = wbar + st;
+        fence_proxy_async();  // the lanes' reads of this stage before the copy overwrites it
+        mbar_expect_tx(bar, 4u * bytes);
+        const SpeciesState& S = A.state[U.s];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) bulk_g2s(buf + k * kWarpGroup, S.cur[k] + w0, bytes, bar);
+        ++f.issued;
+        ++f.pj;
+    }
+}
+
+// The E tile of a unit: one bulk tensor load of the ew x RW nodes from
+// (ox, oy) (zero outside the grid) into `dst`, completed on `bar` (one thread).
+__device__ __forceinline__ void issue_etile(const PushArgs& A, int tile, float2* dst, unsigned long long* bar) {
+    const int ox = (tile % A.tiles_x) * A.tile - kHalo, oy = (tile / A.tiles_x) * A.tile - kHalo;
+    fence_proxy_async();  // the block's reads of this buffer (the unit before last) before the copy overwrites it
+    mbar_expect_tx(bar, unsigned(A.ew * A.rw) * unsigned(sizeof(float2)));
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<unsigned long long>(&A.emap)), "r"(ox), "r"(oy), "r"(smem_u32(bar))
+        : "memory");
+}
+
+template <bool RZ, bool FULL, bool DEPOSIT_AGG>
+__global__ void __launch_bounds__(kPushThreads, 3) k_push_warp(const __grid_constant__ PushArgs A) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    float* wbufs = reinterpret_cast<float*>(smem);  // [warp][stage][4][kWarpGroup]
+    const int RW = A.rw, EW = A.ew;
+    // two E tiles (the unit in work and the next one), 128-byte aligned
+    const int ebuf = ((EW * RW * int(sizeof(float2)) + 127) / 128) * 128;
+    unsigned char* ebase = smem + sizeof(float) * kPushWarps * kWarpStages * 4 * kWarpGroup;
+    unsigned* rt = reinterpret_cast<unsigned*>(ebase + 2 * ebuf);
+    __shared__ __align__(8) unsigned long long bars[kPushWarps * kWarpStages];
+    __shared__ __align__(8) unsigned long long ebars[2];
+    __shared__ UnitDesc units[2];
+    __shared__ unsigned s_abs, s_cand, s_elec;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int n_items = *A.n_items;
+    float* const wbuf = wbufs + warp * kWarpStages * 4 * kWarpGroup;
+    unsigned long long* const wbar = bars + warp * kWarpStages;
+    unsigned epend = 0u;  // thread 0: E-tile buffers with a load issued and not yet waited for
+    if (tid == 0) {
+        for (int k = 0; k < kPushWarps * kWarpStages; ++k) mbar_init(&bars[k], 1);
+        mbar_init(&ebars[0], 1);
+        mbar_init(&ebars[1], 1);
+        fence_mbar_init();
+        for (int b = 0; b < 2; ++b) {
+            units[b] = claim_unit(A, n_items);
+            if (units[b].valid && units[b].tile >= 0) {
+                issue_etile(A, units[b].tile, reinterpret_cast<float2*>(ebase + b * ebuf), &ebars[b]);
+                epend |= 1u << b;
+            }
+        }
+        s_abs = s_cand = s_elec = 0u;
+    }
+    for (int q = tid; q < RW * RW; q += kPushThreads) rt[q] = 0u;  // the flush zeroes it after every unit
+    __syncthreads();
+    const bool do_kick = FULL || A.do_kick, do_drift = FULL || A.do_drift, do_deposit = FULL || A.do_deposit;
+    WarpFeed feed{0, 0, 0};
+    int consumed = 0;
+    unsigned ephase = 0u;  // parity of each E buffer's next load
+    bool failed = false;
+    const unsigned tw = unsigned(RW - 1);  // staged tile: local cell index in [0, RW-2]
+    for (int kcur = 0;; ++kcur) {
+        const UnitDesc U = units[kcur & 1];
+        if (!U.valid) break;
+        const bool tiled = U.tile >= 0;
+        const int eb = kcur & 1;
+        const float2* const et = reinterpret_cast<const float2*>(ebase + eb * ebuf);
+        int ox = 0, oy = 0;
+        if (tiled) {
+            ox = (U.tile % A.tiles_x) * A.tile - kHalo;
+            oy = (U.tile / A.tiles_x) * A.tile - kHalo;
+            if (mbar_wait(&ebars[eb], (ephase >> eb) & 1u, A.wait_limit)) {
+                ephase ^= 1u << eb;
+                if (tid == 0) epend &= ~(1u << eb);
+            } else {
+                failed = true;  // the load stays pending (thread 0 waits for it before exiting)
+            }
+        }
+        if (lane == 0) warp_feed(A, units, kcur, consumed, feed, warp, wbuf, wbar);
+        const int s = U.s;
+        const SpeciesConst C = A.sp[s];
+        const SpeciesState& SS = A.state[s];
+        float* const gx = SS.cur[0];
+        float* const gy = SS.cur[1];
+        float* const gvx = SS.cur[2];
+        float* const gvy = SS.cur[3];
+        float* const gvz = SS.cur[4];
+        const unsigned* const cbits = (A.do_mcc && A.mcc->sp[s].nproc > 0) ? A.cbits[s] : nullptr;
+        unsigned my_abs = 0, my_cand = 0, my_elec = 0;
+        const int a0 = U.b & ~3;
+        for (int j = 0; !failed; ++j) {
+            const int w0 = a0 + (j * kPushWarps + warp) * kWarpGroup;
+            if (w0 >= U.e) break;
+            const int st = consumed % kWarpStages;
+            const unsigned par = unsigned(consumed / kWarpStages) & 1u;
+            if (!mbar_wait(&wbar[st], par, A.wait_limit)) {
+                failed = true;
+                break;
+            }
+            __syncwarp();
+            const float* const buf = wbuf + st * 4 * kWarpGroup;
+#pragma unroll
+            for (int m = 0; m < kWarpGroup / 32; ++m) {
+                const int l = lane + 32 * m;
+                const int p = w0 + l;
+                const bool mine = p >= U.b && p < U.e;
+                float x = buf[l], y = buf[kWarpGroup + l];
+                const bool live = mine && is_live(x);
+                float vx = buf[2 * kWarpGroup + l], vy = buf[3 * kWarpGroup + l];
+                bool dep = false;
+                if (live) {
+                    if (do_kick) {
+                        const Cic c = cic_weights(x, y, A.nx, A.ny);
+                        const int li = c.i0 - ox, lj = c.j0 - oy;
+                        float2 e00, e10, e01, e11;
+                        if (tiled && unsigned(li) < tw && unsigned(lj) < tw) {
+                            const int q = lj * EW + li, dq = c.i1 - c.i0, dr = (c.j1 - c.j0) * EW;
+                            e00 = et[q];
+                            e10 = et[q + dq];
+                            e01 = et[q + dr];
+                            e11 = et[q + dr + dq];
+                        } else {
+                            e00 = __ldg(A.E + long(c.j0) * A.ep + c.i0);
+                            e10 = __ldg(A.E + long(c.j0) * A.ep + c.i1);
+                            e01 = __ldg(A.E + long(c.j1) * A.ep + c.i0);
+                            e11 = __ldg(A.E + long(c.j1) * A.ep + c.i1);
+                        }
+                        vx = __fmaf_rn(C.kq, cic_interp(c, e00.x, e10.x, e01.x, e11.x), vx);
+                        vy = __fmaf_rn(C.kq, cic_interp(c, e00.y, e10.y, e01.y, e11.y), vy);
+                    }
+                    bool candidate = false;
+                    if (cbits) candidate = (__ldg(cbits + (p >> 5)) >> (p & 31)) & 1u;
+                    if (candidate) {
+                        // kicked but not moved: k_collide finishes it after this pass
+                        ++my_cand;
+                        const int slot = atomicAdd(A.cand_count, 1);
+                        if (slot < A.cand_cap) {
+                            A.cand[slot] = make_int2(s, p);
+                        } else {
+                            atomicAdd(A.ctr + kCtrCandOverflow, 1ull);
+                            candidate = false;
+                        }
+                    }
+                    if (candidate) {
+                        gvx[p] = vx;
+                        gvy[p] = vy;
+                    } else {
+                        if (do_drift) {
+                            const float x0 = x, y0 = y;
+                            if constexpr (RZ) {
+                                float vz = gvz[p];
+                                drift_rz(x, y, vx, vy, vz, C.dtdx, C.dtdy);
+                                gvz[p] = vz;
+                            } else {
+                                x = __fmaf_rn(vx, C.dtdx, x);
+                                y = __fmaf_rn(vy, C.dtdy, y);
+                            }
+                            if (!(x >= 0.0f && x <= float(A.nx - 1) && y >= 0.0f && y <= float(A.ny - 1))) {
+                                x = __int_as_float(0x7fc00000);
+                                y = x;
+                                ++my_abs;
+                            } else if (A.electrodes && hits_electrode(x0, y0, x, y, A.nx, A.ny, A.vbits, A.hbits)) {
+                                x = __int_as_float(0x7fc00000);
+                                y = x;
+                                ++my_elec;
+                            }
+                        }
+                        gx[p] = x;
+                        gy[p] = y;
+                        gvx[p] = vx;
+                        gvy[p] = vy;
+                        dep = do_deposit && is_live(x);
+                    }
+                }
+                // deposit: the fixed-point tile for positions inside it, global atomics otherwise
+                Cic c{};
+                int q = -1;
+                if (dep) {
+                    c = FULL ? cic_weights_in_domain(x, y, A.nx, A.ny) : cic_weights(x, y, A.nx, A.ny);
+                    const int li = c.i0 - ox, lj = c.j0 - oy;
+                    if (tiled && unsigned(li) < tw && unsigned(lj) < tw) {
+                        q = lj * RW + li;
+                    } else {
+                        atomicAdd(A.rho + long(c.j0) * A.nx + c.i0, __fmul_rn(C.scale, c.w00));
+                        atomicAdd(A.rho + long(c.j0) * A.nx + c.i1, __fmul_rn(C.scale, c.w10));
+                        atomicAdd(A.rho + long(c.j1) * A.nx + c.i0, __fmul_rn(C.scale, c.w01));
+                        atomicAdd(A.rho + long(c.j1) * A.nx + c.i1, __fmul_rn(C.scale, c.w11));
+                    }
+                }
+                const int dq = c.i1 - c.i0, dr = (c.j1 - c.j0) * RW;
+                unsigned f00 = 0, f10 = 0, f01 = 0, f11 = 0;
+                if (q >= 0) {
+                    f00 = __float2uint_rn(__fmul_rn(c.w00, kFixScale));
+                    f10 = __float2uint_rn(__fmul_rn(c.w10, kFixScale));
+                    f01 = __float2uint_rn(__fmul_rn(c.w01, kFixScale));
+                    f11 = __float2uint_rn(__fmul_rn(c.w11, kFixScale));
+                }
+                if constexpr (DEPOSIT_AGG) {
+                    // lanes of one cell (and one neighbour layout) sum their weights; -1 - lane
+                    // keys keep the lanes without a tile deposit apart
+                    const int key = q >= 0 ? (q | (dq << 20) | ((dr != 0) << 21)) : -1 - lane;
+                    const unsigned grp = __match_any_sync(0xffffffffu, key);
+                    if (q >= 0) {
+                        const unsigned s00 = __reduce_add_sync(grp, f00), s10 = __reduce_add_sync(grp, f10);
+                        const unsigned s01 = __reduce_add_sync(grp, f01), s11 = __reduce_add_sync(grp, f11);
+                        if (lane == __ffs(grp) - 1) {
+                            atomicAdd(rt + q, s00);
+                            atomicAdd(rt + q + dq, s10);
+                            atomicAdd(rt + q + dr, s01);
+                            atomicAdd(rt + q + dr + dq, s11);
+                        }
+                    }
+                } else if (q >= 0) {
+                    atomicAdd(rt + q, f00);
+                    atomicAdd(rt + q + dq, f10);
+                    atomicAdd(rt + q + dr, f01);
+                    atomicAdd(rt + q + dr + dq, f11);
+                }
+            }
+            __syncwarp();  // every lane is done with the stage before lane 0 reloads it
+            ++consumed;
+            if (lane == 0) warp_feed(A, units, kcur, consumed, feed, warp, wbuf, wbar);
+        }
+        my_abs = __reduce_add_sync(0xffffffffu, my_abs);
+        my_cand = __reduce_add_sync(0xffffffffu, my_cand);
+        my_elec = __reduce_add_sync(0xffffffffu, my_elec);
+        if (lane == 0) {
+            if (my_abs) atomicAdd(&s_abs, my_abs);
+            if (my_cand) atomicAdd(&s_cand, my_cand);
+            if (my_elec) atomicAdd(&s_elec, my_elec);
+        }
+        const bool abort = __syncthreads_or(failed);  // deposits and E-tile reads of the unit done
+        if (tiled && do_deposit) {
+            // flush, and leave the tile zeroed for the next unit
+            for (int q = tid; q < RW * RW; q += kPushThreads) {
+                const unsigned sum = rt[q];
+                if (sum) {
+                    atomicAdd(A.rho + long(oy + q / RW) * A.nx + ox + q % RW,
+                              __fmul_rn(C.scale, __fmul_rn(float(sum), kFixInv)));
+                    rt[q] = 0u;
+                }
+            }
+        }
+        if (tid == 0) {
+            if (s_abs) atomicAdd(A.ctr + kCtrAbsorbed + s, (unsigned long long)s_abs);
+            if (s_cand) atomicAdd(A.ctr + kCtrCandidates + s, (unsigned long long)s_cand);
+            if (s_elec) atomicAdd(A.ctr + kCtrElectrode + s, (unsigned long long)s_elec);
+            s_abs = s_cand = s_elec = 0u;
+            if (abort) {
+                atomicExch(A.error, 1);
+            } else {
+                // unit kcur + 2, and its E tile into the buffer this unit used
+                const UnitDesc nu = claim_unit(A, n_items);
+                units[kcur & 1] = nu;
+                if (nu.valid && nu.tile >= 0) {
+                    issue_etile(A, nu.tile, reinterpret_cast<float2*>(ebase + eb * ebuf), &ebars[eb]);
+                    epend |= 1u << eb;
+                }
+            }
+        }
+        __syncthreads();  // charge tile flushed; the unit after next published
+        if (abort) break;
+    }
+    // after a give-up, the copies still in flight (none otherwise): wait for them
+    if (lane == 0)
+        for (int c = consumed; c < feed.issued; ++c)
+            mbar_wait(&wbar[c % kWarpStages], unsigned(c / kWarpStages) & 1u, kWaitLimit);
+    if (tid == 0)
+        for (int b = 0; b < 2; ++b)
+            if (epend & (1u << b)) mbar_wait(&ebars[b], (ephase >> b) & 1u, kWaitLimit);
 }
 
 // The collision candidates of the pass: MCC, then the drift, absorption and
@@ -874,12 +1224,18 @@ struct SimImpl {
     int* error = nullptr;
     unsigned long long wait_limit = kWaitLimit;  // polls of k_push's chunk waits
     float2* E2 = nullptr;
+    int ep = 0;          // row pitch of E2 (nodes)
+    int ew = 0;          // row width of an E tile in k_push_warp's shared memory (rw rounded up to even)
+    CUtensorMap emap{};  // tiles of E2 for k_push_warp's bulk tensor loads
     float *Ex = nullptr, *Ey = nullptr, *rho_acc = nullptr, *rho_out = nullptr;
     double *phi = nullptr, *f = nullptr, *phi_prev = nullptr;
     bool have_prev = false;  // phi_prev holds the potential of the previous solve
     uint8_t* dirichlet = nullptr;
     int push_grid = 0;
     size_t push_smem = 0;
+    int push_kernel = PIC_PUSH_WARP;  // pic_push_kernel
+    int push_grid_w = 0;              // launch shape of k_push_warp
+    size_t push_smem_w = 0;
     int rw = 0;
     bool kick_pending = false;
     long long steps = 0;
@@ -900,6 +1256,36 @@ struct SimImpl {
     pic_mg_info last{};
     int last_status = PIC_OK;
 };
+
+// The tensor map of E2 for k_push_warp's E tiles: 8-byte elements (an
+// (Ex, Ey) pair), nx x ny with rows ep elements apart, boxes of ew x RW
+// elements (ew = RW rounded up to even, so that a box row is a multiple of 16
+// bytes), zero fill outside the grid.  cuTensorMapEncodeTiled comes through the runtime's
+// entry-point lookup, so the library does not link the driver library.
+static int encode_e_map(SimImpl& S) {
+    using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static Encode encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        PIC_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !fn) return fail(PIC_ERR_CUDA, "cuTensorMapEncodeTiled not found");
+        encode = reinterpret_cast<Encode>(fn);
+    }
+    if (S.ew > 256 || S.rw > 256)
+        return fail(PIC_ERR_BAD_ARG, "pic_sim_create: tile %d gives an E tile of %d nodes", S.d.tile, S.rw);
+    const cuuint64_t dims[2] = {cuuint64_t(S.nx), cuuint64_t(S.ny)};
+    const cuuint64_t strides[1] = {cuuint64_t(S.ep) * sizeof(float2)};
+    const cuuint32_t box[2] = {cuuint32_t(S.ew), cuuint32_t(S.rw)};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = encode(&S.emap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, S.E2, dims, strides, box, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(PIC_ERR_CUDA, "cuTensorMapEncodeTiled: error %d", int(r));
+    return PIC_OK;
+}
 
 template <class T>
 static int dalloc(SimImpl& S, T** p, size_t n) {
@@ -953,6 +1339,9 @@ static PushArgs push_args(SimImpl& S, int kick, int mcc, int drift, int deposit,
     A.n_items = S.n_items;
     A.item_next = S.item_next;
     A.E = S.E2;
+    A.ep = S.ep;
+    A.ew = S.ew;
+    A.emap = S.emap;
     A.rho = S.rho_acc;
     A.nx = S.nx;
     A.ny = S.ny;
@@ -1009,7 +1398,17 @@ static int run_pass(SimImpl& S, cudaStream_t st, int kick, int mcc, int drift, i
     {
         PhaseTimer t(S, PIC_PHASE_PUSH, st);
         const bool full = kick && drift && deposit;
-        if (S.rz) {
+        if (S.push_kernel == PIC_PUSH_WARP) {
+            const int g = S.push_grid_w;
+            const size_t sm = S.push_smem_w;
+            if (S.rz) {
+                if (full) k_push_warp<true, true, kDepositAgg><<<g, kPushThreads, sm, st>>>(A);
+                else k_push_warp<true, false, kDepositAgg><<<g, kPushThreads, sm, st>>>(A);
+            } else {
+                if (full) k_push_warp<false, true, kDepositAgg><<<g, kPushThreads, sm, st>>>(A);
+                else k_push_warp<false, false, kDepositAgg><<<g, kPushThreads, sm, st>>>(A);
+            }
+        } else if (S.rz) {
             if (full) k_push<true, true><<<S.push_grid, kPushThreads, S.push_smem, st>>>(A);
             else k_push<true, false><<<S.push_grid, kPushThreads, S.push_smem, st>>>(A);
         } else {
@@ -1056,7 +1455,7 @@ static int field_solve(SimImpl& S, cudaStream_t st, bool capturing) {
     }
     {
         PhaseTimer t(S, PIC_PHASE_EFIELD, st);
-        PIC_TRY(launch_update_E(S.phi, S.Ex, S.Ey, S.E2, S.nx, S.ny, S.d.dx, S.d.dy, st, S.rz));
+        PIC_TRY(launch_update_E(S.phi, S.Ex, S.Ey, S.E2, S.ep, S.nx, S.ny, S.d.dx, S.d.dy, st, S.rz));
     }
     S.launches += 2;
     S.solves += 1;
@@ -1132,6 +1531,7 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
     S.ns = d->nspecies;
     S.G = long(S.nx) * S.ny;
     S.rw = S.d.tile + 1 + 2 * kHalo;
+    S.ew = (S.rw + 1) & ~1;
     PIC_TRY(mg_create(S.nx, S.ny, d->dx, d->dy, d->h_dirichlet, &d->mg, &S.mg));
     if (d->mg.geometry == PIC_GEOM_RZ) {
         // r-z: deposits become densities with the node volumes of each row
@@ -1234,7 +1634,9 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
     PIC_TRY(dalloc(S, &S.ctr, size_t(kCtrCount)));
     PIC_TRY(dalloc(S, &S.error, 1));
     // fields
-    PIC_TRY(dalloc(S, &S.E2, size_t(S.G)));
+    S.ep = (S.nx + 1) & ~1;
+    PIC_TRY(dalloc(S, &S.E2, size_t(S.ep) * S.ny));
+    PIC_TRY(encode_e_map(S));
     PIC_TRY(dalloc(S, &S.Ex, size_t(S.G)));
     PIC_TRY(dalloc(S, &S.Ey, size_t(S.G)));
     PIC_TRY(dalloc(S, &S.rho_acc, size_t(S.G)));
@@ -1299,6 +1701,23 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
     int per_sm = 0;
     PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_fn, kPushThreads, S.push_smem));
     S.push_grid = std::max(1, per_sm) * num_sms();
+    if (d->push_kernel != PIC_PUSH_WARP && d->push_kernel != PIC_PUSH_RING)
+        return fail(PIC_ERR_BAD_ARG, "pic_sim_create: push_kernel %d", d->push_kernel);
+    // k_push_warp's E-tile loads start at x = tile * tx - 4, which the tensor
+    // copy needs even (16-byte aligned): an odd tile takes the ring kernel
+    S.push_kernel = (S.d.tile & 1) ? int(PIC_PUSH_RING) : d->push_kernel;
+    S.push_smem_w = sizeof(float) * kPushWarps * kWarpStages * 4 * kWarpGroup +
+                    2 * ((size_t(S.ew) * S.rw * sizeof(float2) + 127) / 128 * 128) +
+                    size_t(S.rw) * S.rw * sizeof(unsigned);
+    const void* warp_fns[4] = {reinterpret_cast<const void*>(k_push_warp<false, false, kDepositAgg>),
+                               reinterpret_cast<const void*>(k_push_warp<false, true, kDepositAgg>),
+                               reinterpret_cast<const void*>(k_push_warp<true, false, kDepositAgg>),
+                               reinterpret_cast<const void*>(k_push_warp<true, true, kDepositAgg>)};
+    for (const void* fn : warp_fns) PIC_TRY(raise_smem_limit(fn, S.push_smem_w));
+    per_sm = 0;
+    PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, warp_fns[S.rz ? 3 : 1], kPushThreads,
+                                                           S.push_smem_w));
+    S.push_grid_w = std::max(1, per_sm) * num_sms();
     PIC_CUDA(cudaStreamCreateWithFlags(&S.cap, cudaStreamNonBlocking));
     PIC_CUDA(cudaStreamCreateWithFlags(&S.cap2, cudaStreamNonBlocking));
     PIC_CUDA(cudaEventCreateWithFlags(&S.ev_fork, cudaEventDisableTiming));

@@ -76,7 +76,9 @@ def test_cartesian_dropin_classes_in_step_order():
     L = dx * (m - 1)
     dt = 1e-11
     tol = 1e-8
-    w = workloads.scaled(workloads.SMALL, n=n_per, left_V=20.0)
+    # 10 eV electrons: a tail above the 15.8 eV ionisation threshold, so that
+    # the products are exercised too
+    w = workloads.scaled(workloads.SMALL, n=n_per, left_V=20.0, Te=10.0)
     grid = Grid2D(m, m, L, L)
     parts = Particles2D(2 * n_per)
     parts.add_species("electrons", Consts.me, -Consts.qe, 0)  # collision model 0: takes part in MCC

@@ -130,7 +130,7 @@ def test_drop_in_operators_bit_exact():
     np.testing.assert_allclose(t.cpu().numpy(), want, rtol=2e-7)
 
 
-def make_rz_sim(w, seed=0):
+def make_rz_sim(w, seed=0, push_kernel="warp"):
     m = w.nodes
     mask = rz_mask(m, m)
     phi_bc = np.zeros(m * m)
@@ -141,7 +141,7 @@ def make_rz_sim(w, seed=0):
     sp_ = [dict(name="e", charge=-Consts.qe, mass=Consts.me, np2c=5e3, capacity=2 * w.n_e),
            dict(name="i", charge=Consts.qe, mass=workloads.ION_MASS, np2c=5e3, capacity=2 * w.n_i)]
     sim = PICSimulation(m, m, w.dx, w.dx, w.dt, sp_, mask, phi_bc, tol=w.tol, max_cycles=60, sort_interval=0,
-                        seed=seed, geometry="rz")
+                        seed=seed, geometry="rz", push_kernel=push_kernel)
     rng = np.random.Generator(np.random.Philox(w.seed))
     arrays = [list(workloads.species_arrays(w, "e", rng)), list(workloads.species_arrays(w, "i", rng))]
     for s, a in enumerate(arrays):
@@ -156,9 +156,10 @@ def assert_bits(a, b):
     np.testing.assert_array_equal(a[~np.isnan(a)].view(np.uint32), b[~np.isnan(b)].view(np.uint32))
 
 
-def test_fused_rz_step_bit_exact():
+@pytest.mark.parametrize("push_kernel", ["warp", "ring"])
+def test_fused_rz_step_bit_exact(push_kernel):
     w = workloads.scaled(workloads.SMALL, n=30_000)
-    sim, ref, mask = make_rz_sim(w)
+    sim, ref, mask = make_rz_sim(w, push_kernel=push_kernel)
     m = w.nodes
     kqs = [np.float32(-Consts.qe / Consts.me * w.dt), np.float32(Consts.qe / workloads.ION_MASS * w.dt)]
     dtdx = np.float32(w.dt / w.dx)

@@ -20,12 +20,12 @@ from pic_b200.simulation import PICSimulation
 pytestmark = pytest.mark.gpu
 
 
-def make_sim(w, sort_interval, mcc=None, cap_factor=2, seed=0):
+def make_sim(w, sort_interval, mcc=None, cap_factor=2, seed=0, push_kernel="warp"):
     mask, phi_bc = workloads.dirichlet(w)
     sp_ = [dict(name="e", charge=-Consts.qe, mass=Consts.me, np2c=w.np2c(w.n_e), capacity=cap_factor * w.n_e),
            dict(name="i", charge=Consts.qe, mass=workloads.ION_MASS, np2c=w.np2c(w.n_i), capacity=cap_factor * w.n_i)]
     sim = PICSimulation(w.nodes, w.nodes, w.dx, w.dx, w.dt, sp_, mask, phi_bc, tol=w.tol, max_cycles=60,
-                        sort_interval=sort_interval, mcc=mcc, seed=seed)
+                        sort_interval=sort_interval, mcc=mcc, seed=seed, push_kernel=push_kernel)
     rng = np.random.Generator(np.random.Philox(w.seed))
     arrays = [workloads.species_arrays(w, "e", rng), workloads.species_arrays(w, "i", rng)]
     for s, a in enumerate(arrays):
@@ -55,10 +55,11 @@ def assert_bits(a, b):
     np.testing.assert_array_equal(a[~np.isnan(a)].view(np.uint32), b[~np.isnan(b)].view(np.uint32))
 
 
+@pytest.mark.parametrize("push_kernel", ["warp", "ring"])
 @pytest.mark.parametrize("sort_interval", [0, 1])
-def test_particle_passes_bit_exact(sort_interval):
+def test_particle_passes_bit_exact(sort_interval, push_kernel):
     w = workloads.scaled(workloads.SMALL, n=30_000)
-    sim, arrays, mask, _ = make_sim(w, sort_interval)
+    sim, arrays, mask, _ = make_sim(w, sort_interval, push_kernel=push_kernel)
     kqs, dtdx = consts(w)
     m = w.nodes
     ref = [list(a) for a in arrays]
@@ -150,7 +151,8 @@ def test_fused_step_with_mcc_bookkeeping():
     assert 0 < c["born"][0] <= c["collisions"][0][2] and c["born"][1] <= c["collisions"][0][2]
 
 
-def test_internal_electrodes_collect_bit_exact():
+@pytest.mark.parametrize("push_kernel", ["warp", "ring"])
+def test_internal_electrodes_collect_bit_exact(push_kernel):
     """Cathode and anode lines inside the domain (the equipotentials of the
     reference's test.inp, at x = L/4 and 3L/4 from the bottom wall to half
     height): drifts that cross them are collected, bit-exact against the
@@ -170,7 +172,8 @@ def test_internal_electrodes_collect_bit_exact():
            dict(name="i", charge=Consts.qe, mass=workloads.ION_MASS, np2c=w.np2c(w.n_i), capacity=2 * w.n_i)]
     # dt 1e-10 s: 20 eV electrons move ~0.3 cells a step, many cross the lines
     dt = 1e-10
-    sim = PICSimulation(m, m, w.dx, w.dx, dt, sp_, mask, phi_bc, tol=w.tol, max_cycles=60, sort_interval=0)
+    sim = PICSimulation(m, m, w.dx, w.dx, dt, sp_, mask, phi_bc, tol=w.tol, max_cycles=60, sort_interval=0,
+                        push_kernel=push_kernel)
     rng = np.random.Generator(np.random.Philox(w.seed))
     ref = [list(workloads.species_arrays(w, "e", rng)), list(workloads.species_arrays(w, "i", rng))]
     for s, a in enumerate(ref):
