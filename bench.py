@@ -452,6 +452,8 @@ def run_adjoint():
     collisionless steps, checkpoints every 20; gradients of the final
     electron-density loss with respect to four wall potentials and a velocity
     perturbation amplitude, against central finite differences."""
+    import torch
+
     from pic_b200 import adjoint
 
     w = adjoint.AdjWorkload()
@@ -480,23 +482,35 @@ def run_adjoint():
         fd[f"h={h:g} V{', absorption frozen' if frozen else ''}"] = {
             "dV_fd": g, "dA_fd": gA, "max_rel_err_dV": err, "rel_err_dA": abs(dA - gA) / abs(gA)}
     prob.close()
-    # every solve a fixed 10 V-cycles: the solve map is smooth in V, so small
-    # steps isolate the adjoint's agreement from the solver's stopping point
+    # every solve a fixed 10 V-cycles and the absorption frozen: the map the
+    # adjoint differentiates (a smooth solve map, a fixed absorption mask);
+    # what is left between it and central differences is the CIC weights'
+    # kinks: particles that sit in different cells in the +h and -h runs
     fixed = adjoint.AdjWorkload(tol=0.0, max_cycles=10)
     prob, V0, A0, _ = adjoint.build(fixed)
     prob.forward(V0, A0)
     fdV, fdA = prob.backward()
     prob.freeze_absorption(True)
-    for h, hA in ((1e-4, 0.1), (1e-6, 0.01)):
-        g = []
+
+    def cells(pr):
+        x, y = pr.state()[:2]
+        return torch.floor(x).to(torch.int64) * 100000 + torch.floor(y).to(torch.int64)
+
+    for h, hA in ((1e-3, 1.0), (1e-4, 0.1), (1e-6, 0.01)):
+        g, kinks = [], []
         for q in range(4):
             e = np.zeros(4)
             e[q] = h
-            g.append((prob.forward(V0 + e, A0) - prob.forward(V0 - e, A0)) / (2 * h))
+            lp = prob.forward(V0 + e, A0)
+            cp = cells(prob).clone()
+            lm = prob.forward(V0 - e, A0)
+            kinks.append(int((cells(prob) != cp).sum()))
+            g.append((lp - lm) / (2 * h))
         gA = (prob.forward(V0, A0 + hA) - prob.forward(V0, A0 - hA)) / (2 * hA)
         err = max(abs(a - b) for a, b in zip(fdV, g)) / max(abs(b) for b in g)
         fd[f"h={h:g} V, absorption frozen, 10 V-cycles per solve"] = {
-            "dV_adjoint": list(fdV), "dV_fd": g, "dA_fd": gA, "max_rel_err_dV": err, "rel_err_dA": abs(fdA - gA) / abs(gA)}
+            "dV_adjoint": list(fdV), "dV_fd": g, "dA_fd": gA, "max_rel_err_dV": err, "rel_err_dA": abs(fdA - gA) / abs(gA),
+            "particles_in_other_cells_at_the_end": kinks, "within_1e-4": bool(err <= 1e-4 and abs(fdA - gA) <= 1e-4 * abs(gA))}
     prob.close()
     return {"workload": "257x257 nodes, 1e6 e- + 1e6 ions, 200 FP64 steps, checkpoints every 20, 4 wall electrodes",
             "loss": loss, "dV": list(dV), "dA": dA, "forward_ms": 1e3 * (t1 - t0), "backward_ms": 1e3 * (t2 - t1),
