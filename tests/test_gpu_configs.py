@@ -284,7 +284,11 @@ def test_mcc_workload_full_size_step_against_oracle():
         for k in (2, 3, 4):
             assert np.all(np.abs(got[k][:n][collided[s]] - a[k][collided[s]]) <= 2e-6 * speed + 1e-3)
         for k in (0, 1):
-            assert np.all(np.abs(got[k][:n][collided[s]] - a[k][collided[s]]) <= 2e-6 * speed * dtdx + 1e-4)
+            # a collided particle may also leave the domain (NaN in both)
+            g, r = got[k][:n][collided[s]], a[k][collided[s]]
+            np.testing.assert_array_equal(np.isnan(g), np.isnan(r))
+            ok = ~np.isnan(r)
+            assert np.all(np.abs(g[ok] - r[ok]) <= 2e-6 * speed[ok] * dtdx + 1e-4)
         # the products, as multisets per component (their slots follow atomic order)
         for k in range(5):
             g, r = np.sort(got[k][n:]), np.sort(born[s][k])
