@@ -53,7 +53,7 @@ def parse():
                     help="steps between cell sorts (80: the autotuner's choice for 513^2 shapes)")
     ap.add_argument("--particles", type=int, default=4_000_000, help="per species")
     ap.add_argument("--tile", type=int, default=16, help="cells per side of the push's work tiles")
-    ap.add_argument("--push", default="warp", choices=["warp", "ring"],
+    ap.add_argument("--push", default="warp", choices=["warp", "ring", "warp_atomic"],
                     help="particle-pass streaming: per-warp bulk-copy pipelines (warp) or one ring per block (ring)")
     ap.add_argument("--no-poisson", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -302,7 +302,7 @@ def run_ours(args, world, rank, local):
     achieved = bytes_per_launch / (push_ms / 1e3) / 1e9
     peak, peak_kind = peak_hbm()
     traffic = ncu_traffic()
-    roofline = {"bound": "hbm", "kernel": "k_push_warp" if args.push == "warp" else "k_push", "achieved": round(achieved, 1),
+    roofline = {"bound": "hbm", "kernel": "k_push" if args.push == "ring" else "k_push_warp", "achieved": round(achieved, 1),
                 "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
                 "bytes_per_launch": bytes_per_launch, "ms_per_launch": round(push_ms, 5)}

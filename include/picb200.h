@@ -359,8 +359,10 @@ typedef struct pic_sim_desc {
 /* The particle pass's two streaming schemes; both do the same arithmetic and
  * give bit-identical particles and charge. */
 typedef enum pic_push_kernel {
-    PIC_PUSH_WARP = 0, /* each warp streams its own groups of particles through its own bulk-copy stages */
-    PIC_PUSH_RING = 1  /* the block streams chunks through one shared three-stage ring */
+    PIC_PUSH_WARP = 0,       /* each warp streams its own groups of particles through its own stage buffers;
+                                charge deposited with warp-aggregated atomics */
+    PIC_PUSH_RING = 1,       /* the block streams chunks through one shared three-stage ring of bulk copies */
+    PIC_PUSH_WARP_ATOMIC = 2 /* as PIC_PUSH_WARP, with one charge-tile atomic per particle and node */
 } pic_push_kernel;
 
 typedef struct pic_sim_counters {

@@ -542,12 +542,12 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
 // consecutive lanes in one cell) sum their four fixed-point weights with
 // redux.sync over __match_any_sync's group, and the group's lowest lane adds
 // the sums.  Integer sums are exact, so the tile holds the same values either way.
-constexpr bool kDepositAgg = true;  // warp-aggregated charge-tile atomics in k_push_warp
 constexpr int kWarpGroup = 128;  // particles per group (four per lane)
 constexpr int kWarpStages = 3;   // stage buffers per warp
 constexpr int kPushWarps = kPushThreads / 32;
 
 struct UnitDesc {
+    const float* cur[4];  // x, y, vx, vy of the unit's species
     int valid;
     int s, tile, b, e;
 };
@@ -563,20 +563,35 @@ __device__ __forceinline__ UnitDesc claim_unit(const PushArgs& A, int n_items) {
         u.tile = v.y;
         u.b = v.z;
         u.e = v.w;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) u.cur[k] = A.state[u.s].cur[k];
     }
     return u;
 }
 
-// Per-warp producer state (meaningful in lane 0): the next group to load is
-// the pj-th of this warp in unit pu; `issued` groups were loaded so far.
+// Per-warp producer state (the same in every lane): the next group to load
+// is the pj-th of this warp in unit pu; `issued` groups were loaded so far.
 struct WarpFeed {
     int pu, pj, issued;
 };
 
-// Lane 0: loads this warp's next groups while stage buffers are free and the
-// units are known (the current one and the next).
-__device__ __forceinline__ void warp_feed(const PushArgs& A, const UnitDesc* units, int kcur, int consumed,
-                                          WarpFeed& f, int warp, float* wbuf, unsigned long long* wbar) {
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+// Waits until at most n (0..2) of this thread's copy groups are still in flight.
+__device__ __forceinline__ void cp_async_wait_pending(int n) {
+    if (n <= 0) asm volatile("cp.async.wait_group 0;" ::: "memory");
+    else if (n == 1) asm volatile("cp.async.wait_group 1;" ::: "memory");
+    else asm volatile("cp.async.wait_group 2;" ::: "memory");
+}
+
+// Every lane: loads this warp's next groups (each lane 16 bytes of each of
+// x, y, vx, vy: one asynchronous copy group per particle group) while stage
+// buffers are free and the units are known (the current one and the next).
+__device__ __forceinline__ void warp_feed(const UnitDesc* units, int kcur, int consumed, WarpFeed& f, int warp,
+                                          int lane, float* wbuf) {
     while (f.issued - consumed < kWarpStages && f.pu <= kcur + 1) {
         const UnitDesc& U = units[f.pu & 1];
         if (!U.valid) return;
@@ -587,15 +602,13 @@ __device__ __forceinline__ void warp_feed(const PushArgs& A, const UnitDesc* uni
             continue;
         }
         const int w1 = min(w0 + kWarpGroup, (U.e + 3) & ~3);
-        const int st = f.issued % kWarpStages;
-        const unsigned bytes = unsigned(w1 - w0) * 4u;
-        float* buf = wbuf + st * 4 * kWarpGroup;
-        unsigned long long* bar = wbar + st;
-        fence_proxy_async();  // the lanes' reads of this stage before the copy overwrites it
-        mbar_expect_tx(bar, 4u * bytes);
-        const SpeciesState& S = A.state[U.s];
+        float* buf = wbuf + (f.issued % kWarpStages) * 4 * kWarpGroup;
+        const int o = 4 * lane;
+        if (w0 + o < w1) {
 #pragma unroll
-        for (int k = 0; k < 4; ++k) bulk_g2s(buf + k * kWarpGroup, S.cur[k] + w0, bytes, bar);
+            for (int k = 0; k < 4; ++k) cp_async16(buf + k * kWarpGroup + o, U.cur[k] + w0 + o);
+        }
+        cp_async_commit();
         ++f.issued;
         ++f.pj;
     }
@@ -623,17 +636,14 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push_warp(const __grid_cons
     const int ebuf = ((EW * RW * int(sizeof(float2)) + 127) / 128) * 128;
     unsigned char* ebase = smem + sizeof(float) * kPushWarps * kWarpStages * 4 * kWarpGroup;
     unsigned* rt = reinterpret_cast<unsigned*>(ebase + 2 * ebuf);
-    __shared__ __align__(8) unsigned long long bars[kPushWarps * kWarpStages];
     __shared__ __align__(8) unsigned long long ebars[2];
     __shared__ UnitDesc units[2];
     __shared__ unsigned s_abs, s_cand, s_elec;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n_items = *A.n_items;
     float* const wbuf = wbufs + warp * kWarpStages * 4 * kWarpGroup;
-    unsigned long long* const wbar = bars + warp * kWarpStages;
     unsigned epend = 0u;  // thread 0: E-tile buffers with a load issued and not yet waited for
     if (tid == 0) {
-        for (int k = 0; k < kPushWarps * kWarpStages; ++k) mbar_init(&bars[k], 1);
         mbar_init(&ebars[0], 1);
         mbar_init(&ebars[1], 1);
         fence_mbar_init();
@@ -671,7 +681,7 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push_warp(const __grid_cons
                 failed = true;  // the load stays pending (thread 0 waits for it before exiting)
             }
         }
-        if (lane == 0) warp_feed(A, units, kcur, consumed, feed, warp, wbuf, wbar);
+        warp_feed(units, kcur, consumed, feed, warp, lane, wbuf);
         const int s = U.s;
         const SpeciesConst C = A.sp[s];
         const SpeciesState& SS = A.state[s];
@@ -687,12 +697,8 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push_warp(const __grid_cons
             const int w0 = a0 + (j * kPushWarps + warp) * kWarpGroup;
             if (w0 >= U.e) break;
             const int st = consumed % kWarpStages;
-            const unsigned par = unsigned(consumed / kWarpStages) & 1u;
-            if (!mbar_wait(&wbar[st], par, A.wait_limit)) {
-                failed = true;
-                break;
-            }
-            __syncwarp();
+            cp_async_wait_pending(feed.issued - consumed - 1);
+            __syncwarp();  // the other lanes' copies of this group are visible
             const float* const buf = wbuf + st * 4 * kWarpGroup;
 #pragma unroll
             for (int m = 0; m < kWarpGroup / 32; ++m) {
@@ -812,9 +818,9 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push_warp(const __grid_cons
                     atomicAdd(rt + q + dr + dq, f11);
                 }
             }
-            __syncwarp();  // every lane is done with the stage before lane 0 reloads it
+            __syncwarp();  // every lane is done with the stage before it is reloaded
             ++consumed;
-            if (lane == 0) warp_feed(A, units, kcur, consumed, feed, warp, wbuf, wbar);
+            warp_feed(units, kcur, consumed, feed, warp, lane, wbuf);
         }
         my_abs = __reduce_add_sync(0xffffffffu, my_abs);
         my_cand = __reduce_add_sync(0xffffffffu, my_cand);
@@ -857,9 +863,7 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push_warp(const __grid_cons
         if (abort) break;
     }
     // after a give-up, the copies still in flight (none otherwise): wait for them
-    if (lane == 0)
-        for (int c = consumed; c < feed.issued; ++c)
-            mbar_wait(&wbar[c % kWarpStages], unsigned(c / kWarpStages) & 1u, kWaitLimit);
+    cp_async_wait_all();
     if (tid == 0)
         for (int b = 0; b < 2; ++b)
             if (epend & (1u << b)) mbar_wait(&ebars[b], (ephase >> b) & 1u, kWaitLimit);
@@ -1398,15 +1402,26 @@ static int run_pass(SimImpl& S, cudaStream_t st, int kick, int mcc, int drift, i
     {
         PhaseTimer t(S, PIC_PHASE_PUSH, st);
         const bool full = kick && drift && deposit;
-        if (S.push_kernel == PIC_PUSH_WARP) {
+        if (S.push_kernel == PIC_PUSH_WARP || S.push_kernel == PIC_PUSH_WARP_ATOMIC) {
             const int g = S.push_grid_w;
             const size_t sm = S.push_smem_w;
+            const bool agg = S.push_kernel == PIC_PUSH_WARP;
             if (S.rz) {
-                if (full) k_push_warp<true, true, kDepositAgg><<<g, kPushThreads, sm, st>>>(A);
-                else k_push_warp<true, false, kDepositAgg><<<g, kPushThreads, sm, st>>>(A);
+                if (full) {
+                    if (agg) k_push_warp<true, true, true><<<g, kPushThreads, sm, st>>>(A);
+                    else k_push_warp<true, true, false><<<g, kPushThreads, sm, st>>>(A);
+                } else {
+                    if (agg) k_push_warp<true, false, true><<<g, kPushThreads, sm, st>>>(A);
+                    else k_push_warp<true, false, false><<<g, kPushThreads, sm, st>>>(A);
+                }
             } else {
-                if (full) k_push_warp<false, true, kDepositAgg><<<g, kPushThreads, sm, st>>>(A);
-                else k_push_warp<false, false, kDepositAgg><<<g, kPushThreads, sm, st>>>(A);
+                if (full) {
+                    if (agg) k_push_warp<false, true, true><<<g, kPushThreads, sm, st>>>(A);
+                    else k_push_warp<false, true, false><<<g, kPushThreads, sm, st>>>(A);
+                } else {
+                    if (agg) k_push_warp<false, false, true><<<g, kPushThreads, sm, st>>>(A);
+                    else k_push_warp<false, false, false><<<g, kPushThreads, sm, st>>>(A);
+                }
             }
         } else if (S.rz) {
             if (full) k_push<true, true><<<S.push_grid, kPushThreads, S.push_smem, st>>>(A);
@@ -1701,7 +1716,7 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
     int per_sm = 0;
     PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_fn, kPushThreads, S.push_smem));
     S.push_grid = std::max(1, per_sm) * num_sms();
-    if (d->push_kernel != PIC_PUSH_WARP && d->push_kernel != PIC_PUSH_RING)
+    if (d->push_kernel != PIC_PUSH_WARP && d->push_kernel != PIC_PUSH_RING && d->push_kernel != PIC_PUSH_WARP_ATOMIC)
         return fail(PIC_ERR_BAD_ARG, "pic_sim_create: push_kernel %d", d->push_kernel);
     // k_push_warp's E-tile loads start at x = tile * tx - 4, which the tensor
     // copy needs even (16-byte aligned): an odd tile takes the ring kernel
@@ -1709,10 +1724,14 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
     S.push_smem_w = sizeof(float) * kPushWarps * kWarpStages * 4 * kWarpGroup +
                     2 * ((size_t(S.ew) * S.rw * sizeof(float2) + 127) / 128 * 128) +
                     size_t(S.rw) * S.rw * sizeof(unsigned);
-    const void* warp_fns[4] = {reinterpret_cast<const void*>(k_push_warp<false, false, kDepositAgg>),
-                               reinterpret_cast<const void*>(k_push_warp<false, true, kDepositAgg>),
-                               reinterpret_cast<const void*>(k_push_warp<true, false, kDepositAgg>),
-                               reinterpret_cast<const void*>(k_push_warp<true, true, kDepositAgg>)};
+    const void* warp_fns[8] = {reinterpret_cast<const void*>(k_push_warp<false, false, true>),
+                               reinterpret_cast<const void*>(k_push_warp<false, true, true>),
+                               reinterpret_cast<const void*>(k_push_warp<true, false, true>),
+                               reinterpret_cast<const void*>(k_push_warp<true, true, true>),
+                               reinterpret_cast<const void*>(k_push_warp<false, false, false>),
+                               reinterpret_cast<const void*>(k_push_warp<false, true, false>),
+                               reinterpret_cast<const void*>(k_push_warp<true, false, false>),
+                               reinterpret_cast<const void*>(k_push_warp<true, true, false>)};
     for (const void* fn : warp_fns) PIC_TRY(raise_smem_limit(fn, S.push_smem_w));
     per_sm = 0;
     PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, warp_fns[S.rz ? 3 : 1], kPushThreads,

@@ -156,7 +156,7 @@ def assert_bits(a, b):
     np.testing.assert_array_equal(a[~np.isnan(a)].view(np.uint32), b[~np.isnan(b)].view(np.uint32))
 
 
-@pytest.mark.parametrize("push_kernel", ["warp", "ring"])
+@pytest.mark.parametrize("push_kernel", ["warp", "ring", "warp_atomic"])
 def test_fused_rz_step_bit_exact(push_kernel):
     w = workloads.scaled(workloads.SMALL, n=30_000)
     sim, ref, mask = make_rz_sim(w, push_kernel=push_kernel)
