@@ -53,8 +53,9 @@ def parse():
                     help="steps between cell sorts (80: the autotuner's choice for 513^2 shapes)")
     ap.add_argument("--particles", type=int, default=4_000_000, help="per species")
     ap.add_argument("--tile", type=int, default=16, help="cells per side of the push's work tiles")
-    ap.add_argument("--push", default="warp", choices=["warp", "ring", "warp_atomic"],
-                    help="particle-pass streaming: per-warp bulk-copy pipelines (warp) or one ring per block (ring)")
+    ap.add_argument("--push", default="ring", choices=["ring", "warp", "warp_agg"],
+                    help="particle-pass streaming: one ring of bulk copies per block (ring), per-warp pipelines "
+                         "(warp), per-warp pipelines with warp-aggregated deposit atomics (warp_agg)")
     ap.add_argument("--no-poisson", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

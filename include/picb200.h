@@ -356,13 +356,15 @@ typedef struct pic_sim_desc {
     int push_kernel;            /* pic_push_kernel: how the particle pass streams the particles */
 } pic_sim_desc;
 
-/* The particle pass's two streaming schemes; both do the same arithmetic and
- * give bit-identical particles and charge. */
+/* The particle pass's streaming schemes; all do the same arithmetic and give
+ * bit-identical particles and the same charge (integer tile sums). */
 typedef enum pic_push_kernel {
-    PIC_PUSH_WARP = 0,       /* each warp streams its own groups of particles through its own stage buffers;
-                                charge deposited with warp-aggregated atomics */
-    PIC_PUSH_RING = 1,       /* the block streams chunks through one shared three-stage ring of bulk copies */
-    PIC_PUSH_WARP_ATOMIC = 2 /* as PIC_PUSH_WARP, with one charge-tile atomic per particle and node */
+    PIC_PUSH_RING = 0,     /* the block streams chunks through one shared three-stage ring of bulk copies
+                              (the default: the fastest measured) */
+    PIC_PUSH_WARP = 1,     /* each warp streams its own groups of particles through its own stage buffers
+                              (asynchronous copies), E tiles by bulk tensor copies, one charge-tile atomic
+                              per particle and node */
+    PIC_PUSH_WARP_AGG = 2  /* as PIC_PUSH_WARP, the charge deposited with warp-aggregated atomics */
 } pic_push_kernel;
 
 typedef struct pic_sim_counters {

@@ -98,7 +98,7 @@ class SimDesc(C.Structure):
                 ("seed", C.c_ulonglong), ("use_graph", C.c_int), ("min_cycles", C.c_int), ("push_kernel", C.c_int)]
 
 
-PUSH_KERNELS = {"warp": 0, "ring": 1, "warp_atomic": 2}
+PUSH_KERNELS = {"ring": 0, "warp": 1, "warp_agg": 2}
 
 
 PIC_ADJ_MAX_SEGMENTS = 16

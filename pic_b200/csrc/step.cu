@@ -1237,7 +1237,7 @@ struct SimImpl {
     uint8_t* dirichlet = nullptr;
     int push_grid = 0;
     size_t push_smem = 0;
-    int push_kernel = PIC_PUSH_WARP;  // pic_push_kernel
+    int push_kernel = PIC_PUSH_RING;  // pic_push_kernel
     int push_grid_w = 0;              // launch shape of k_push_warp
     size_t push_smem_w = 0;
     int rw = 0;
@@ -1402,10 +1402,10 @@ static int run_pass(SimImpl& S, cudaStream_t st, int kick, int mcc, int drift, i
     {
         PhaseTimer t(S, PIC_PHASE_PUSH, st);
         const bool full = kick && drift && deposit;
-        if (S.push_kernel == PIC_PUSH_WARP || S.push_kernel == PIC_PUSH_WARP_ATOMIC) {
+        if (S.push_kernel == PIC_PUSH_WARP || S.push_kernel == PIC_PUSH_WARP_AGG) {
             const int g = S.push_grid_w;
             const size_t sm = S.push_smem_w;
-            const bool agg = S.push_kernel == PIC_PUSH_WARP;
+            const bool agg = S.push_kernel == PIC_PUSH_WARP_AGG;
             if (S.rz) {
                 if (full) {
                     if (agg) k_push_warp<true, true, true><<<g, kPushThreads, sm, st>>>(A);
@@ -1716,7 +1716,7 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
     int per_sm = 0;
     PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_fn, kPushThreads, S.push_smem));
     S.push_grid = std::max(1, per_sm) * num_sms();
-    if (d->push_kernel != PIC_PUSH_WARP && d->push_kernel != PIC_PUSH_RING && d->push_kernel != PIC_PUSH_WARP_ATOMIC)
+    if (d->push_kernel != PIC_PUSH_RING && d->push_kernel != PIC_PUSH_WARP && d->push_kernel != PIC_PUSH_WARP_AGG)
         return fail(PIC_ERR_BAD_ARG, "pic_sim_create: push_kernel %d", d->push_kernel);
     // k_push_warp's E-tile loads start at x = tile * tx - 4, which the tensor
     // copy needs even (16-byte aligned): an odd tile takes the ring kernel

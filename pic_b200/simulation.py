@@ -60,9 +60,11 @@ class PICSimulation:
     the extrapolated potential of the last two steps needs at least two at the
     tolerances of a PIC step, and cycles that are not tested cost no WHILE-node
     iteration in the captured step.
-    push_kernel: "warp" (every warp streams its own groups of particles through
-    its own bulk-copy stages) or "ring" (the block streams chunks through one
-    shared ring); the two give bit-identical results.
+    push_kernel: how the particle pass streams the particles, all with
+    bit-identical results: "ring" (the block streams chunks through one
+    shared ring of bulk copies; the fastest measured), "warp" (every warp
+    streams its own groups through its own stage buffers, E tiles by bulk
+    tensor copies) or "warp_agg" ("warp" with warp-aggregated deposit atomics).
     geometry: "cartesian", or "rz" for the axisymmetric r-z step (the
     reference's Grid.Cylindrical = 1): x axial, y radial (row 0 the axis, a
     free row), vx axial, vy radial, vz azimuthal; np2c counts real particles;
@@ -73,7 +75,7 @@ class PICSimulation:
     def __init__(self, nx, ny, dx, dy, dt, species, dirichlet, phi_bc=None, tol=1e-8, max_cycles=50,
                  precision="mixed", pre_sweeps=2, post_sweeps=2, omega=1.15, sort_interval=20, tile=16,
                  mcc: MccTables | None = None, seed=0, use_graph=False, eps0=Consts.eps0, mg_launch="graph",
-                 coarsest_max=9, geometry="cartesian", min_cycles=2, push_kernel="warp"):
+                 coarsest_max=9, geometry="cartesian", min_cycles=2, push_kernel="ring"):
         self.nx, self.ny, self.dx, self.dy, self.dt = int(nx), int(ny), float(dx), float(dy), float(dt)
         self.species = list(species)
         self.geometry = geometry

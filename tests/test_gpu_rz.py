@@ -130,7 +130,7 @@ def test_drop_in_operators_bit_exact():
     np.testing.assert_allclose(t.cpu().numpy(), want, rtol=2e-7)
 
 
-def make_rz_sim(w, seed=0, push_kernel="warp"):
+def make_rz_sim(w, seed=0, push_kernel="ring"):
     m = w.nodes
     mask = rz_mask(m, m)
     phi_bc = np.zeros(m * m)
@@ -156,7 +156,7 @@ def assert_bits(a, b):
     np.testing.assert_array_equal(a[~np.isnan(a)].view(np.uint32), b[~np.isnan(b)].view(np.uint32))
 
 
-@pytest.mark.parametrize("push_kernel", ["warp", "ring", "warp_atomic"])
+@pytest.mark.parametrize("push_kernel", ["ring", "warp", "warp_agg"])
 def test_fused_rz_step_bit_exact(push_kernel):
     w = workloads.scaled(workloads.SMALL, n=30_000)
     sim, ref, mask = make_rz_sim(w, push_kernel=push_kernel)

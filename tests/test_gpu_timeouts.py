@@ -9,10 +9,11 @@ the host reads the error flag.
     arrive before the last one give up; every later barrier then gives up too,
     so every block returns.  The same solver then converges with the default
     limit.
-  * The fused particle pass (chunks streamed into shared memory by bulk
-    copies, completed on mbarriers): with a limit of zero polls every block
-    gives up at its first chunk, after waiting (with the default limit) for the
-    copy in flight.  The simulation then steps normally once reloaded.
+  * The fused particle pass (chunks, or E tiles, streamed into shared memory
+    by bulk copies completed on mbarriers): with a limit of zero polls every
+    block gives up at its first wait, after waiting (with the default limit)
+    for the copies in flight.  The simulation then steps normally once
+    reloaded.
 """
 import numpy as np
 import pytest
@@ -46,13 +47,14 @@ def test_persistent_solve_barrier_timeout_is_reported():
     assert rel < 1e-10 and cycles > 0
 
 
-def test_particle_pass_wait_timeout_is_reported():
+@pytest.mark.parametrize("push_kernel", ["ring", "warp"])
+def test_particle_pass_wait_timeout_is_reported(push_kernel):
     w = workloads.scaled(workloads.SMALL, n=50_000)
     mask, phi_bc = workloads.dirichlet(w)
     sp = [dict(name="e", charge=-Consts.qe, mass=Consts.me, np2c=w.np2c(w.n_e), capacity=w.n_e),
           dict(name="i", charge=Consts.qe, mass=workloads.ION_MASS, np2c=w.np2c(w.n_i), capacity=w.n_i)]
     sim = PICSimulation(w.nodes, w.nodes, w.dx, w.dx, w.dt, sp, mask, phi_bc, tol=w.tol, sort_interval=10,
-                        use_graph=True)
+                        use_graph=True, push_kernel=push_kernel)
     rng = np.random.Generator(np.random.Philox(4))
     arrays = [workloads.species_arrays(w, "e", rng), workloads.species_arrays(w, "i", rng)]
     for s, a in enumerate(arrays):
