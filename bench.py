@@ -72,7 +72,7 @@ def parse():
                          "in one cluster launch per cycle)")
     ap.add_argument("--ensemble", type=int, default=0,
                     help="also time an ensemble of this many independent collisionless members (0: off)")
-    ap.add_argument("--ensemble-steps", type=int, default=100)
+    ap.add_argument("--ensemble-steps", type=int, default=500)
     ap.add_argument("--adjoint", action="store_true",
                     help="also time the differentiable workload (forward, adjoint, finite-difference check)")
     ap.add_argument("--tune-cache", default=os.path.join(ROOT, "pic_b200", "tuned_b200.json"),
@@ -433,9 +433,17 @@ def run_ensemble(args):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     n1 = ens.particle_count()
+    fused = ens.fused_pass
     ens.close()
     for sim in sims:
         sim.close()
+    # the particle arrays' compulsory bytes (32 B per particle-step) and the
+    # grids' (12 B per node) over the whole ensemble step: a lower bound of the
+    # step's traffic, whose time also holds every member's field solve
+    nodes = sum(w.nodes * w.nodes for w in ws)
+    step_bytes = 0.5 * (n0 + n1) * BYTES_PER_PARTICLE + nodes * BYTES_PER_NODE
+    peak, kind = peak_hbm()
+    gbs = step_bytes / (ms / args.ensemble_steps / 1e3) / 1e9
     picked = {}
     for ch in choices:
         k = (f"tile {ch.tile}, sort every {ch.sort_interval}, coarsest {ch.coarsest_max}, omega {ch.omega}, "
@@ -445,7 +453,11 @@ def run_ensemble(args):
     return {"members": len(ws), "particles": n0, "steps": args.ensemble_steps, "ms_per_step": ms / args.ensemble_steps,
             "value": 0.5 * (n0 + n1) * args.ensemble_steps / (ms / 1e3), "unit": UNIT,
             "sides": {str(k): sides.count(k) for k in ensemble.SIDES}, "tuned": picked,
-            "tune_s": round(tune_s, 1), "tune_measurements": tuner.measurements}
+            "tune_s": round(tune_s, 1), "tune_measurements": tuner.measurements,
+            "one_particle_pass_over_all_members": fused,
+            "hbm": {"bytes_per_step": step_bytes, "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
+                    "frac": round(gbs / peak, 4), "peak_source": kind,
+                    "counts": "particle and grid bytes over the whole ensemble step (field solves included)"}}
 
 
 def run_adjoint():

@@ -489,8 +489,11 @@ int pic_sim_read_profile(pic_sim* sim, pic_sim_profile* out);
 /* ------------------------------------------------------------------ */
 
 /* Many independent simulations stepped together: one CUDA graph holds a step
- * of every member as independent branches, and a conditional WHILE node
- * repeats it, so that n steps of the whole ensemble are one graph launch.
+ * of every member, and a conditional WHILE node repeats it, so that n steps
+ * of the whole ensemble are one graph launch.  Within a step every member's
+ * preparation (cell sort, work items) is an independent branch, then one
+ * persistent particle pass takes the work items of all members from one
+ * queue, then every member's field solve is an independent branch.
  * Each member's cell sort sits under a conditional IF node that fires when
  * the member's own step count is a multiple of its sort interval; each
  * member's multigrid loop is a nested conditional WHILE node.  Members may
@@ -508,6 +511,11 @@ int pic_ens_destroy(pic_ens* e);
  * which the graph does not hold, so while any member is fresh every member
  * takes its first of the n steps eagerly. */
 int pic_ens_step(pic_ens* e, int n_steps, void* stream);
+/* 1 when the members' particle passes run as one persistent launch whose
+ * work queue spans every member's work items (every member uses
+ * PIC_PUSH_RING and the same geometry), 0 when each member's pass is its own
+ * launch in its branch. */
+int pic_ens_fused_pass(pic_ens* e, int* fused);
 
 /* ------------------------------------------------------------------ */
 /* Hand-written adjoint of the collisionless step                      */

@@ -114,7 +114,20 @@ struct alignas(64) PushArgs {
     unsigned long long* ctr;
     int* error;  // set when a bounded wait gives up
     unsigned long long wait_limit;  // polls of a chunk wait (kWaitLimit unless changed)
+    // one pass over an ensemble's members (k_push<..., true>): the members'
+    // own arguments, and the first work item of each member in the pass's
+    // flat item numbering (nmembers + 1 entries, the last the total)
+    const PushArgs* members;
+    const int* member_items;
+    int nmembers;
 };
+
+// The arguments of member m: the pass's own unless it runs an ensemble.
+template <bool ENS>
+__device__ __forceinline__ const PushArgs& member(const PushArgs& A, int m) {
+    if constexpr (ENS) return A.members[m];
+    else return A;
+}
 
 // ---- TMA bulk copies and mbarriers (inline PTX, no multicast) -------------------
 
@@ -159,25 +172,29 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* m, unsigned parity
 // One chunk of a work unit, as the producer thread hands it to the CTA.
 struct ChunkDesc {
     int valid;
+    int m;              // ensemble member (0 outside an ensemble)
     int s, tile, b, e;  // species, tile (-1: untiled), slot range of the chunk
     int unit_e;         // end of the unit's slot range
     int first;          // first chunk of its unit
 };
 
 // Issues the bulk copies of slots [b, e) of species s into `buf` (one thread).
+template <bool ENS>
 __device__ __forceinline__ void issue_chunk(const PushArgs& A, const ChunkDesc& c, float* buf,
                                             unsigned long long* bar) {
     const int a0 = c.b & ~3, a1 = (c.e + 3) & ~3;
     const unsigned bytes = unsigned(a1 - a0) * 4u;
     // x, y, vx, vy: vz is touched only by collision candidates (k_collide)
     mbar_expect_tx(bar, 4u * bytes);
-    const SpeciesState& S = A.state[c.s];
+    const SpeciesState& S = member<ENS>(A, c.m).state[c.s];
 #pragma unroll
     for (int k = 0; k < 4; ++k) bulk_g2s(buf + k * kBufStride, S.cur[k] + a0, bytes, bar);
 }
 
 // The chunk after `c`: the rest of its unit, else the first chunk of a newly
-// claimed unit (one thread).
+// claimed unit (one thread).  In an ensemble pass the claimed number runs over
+// every member's items: the member is found in member_items.
+template <bool ENS>
 __device__ __forceinline__ ChunkDesc next_chunk(const PushArgs& A, const ChunkDesc& c, int n_items) {
     ChunkDesc d;
     if (c.valid && c.e < c.unit_e) {
@@ -187,10 +204,21 @@ __device__ __forceinline__ ChunkDesc next_chunk(const PushArgs& A, const ChunkDe
         d.first = 0;
         return d;
     }
-    const int it = atomicAdd(A.item_next, 1);
+    int it = atomicAdd(A.item_next, 1);
     d.valid = it < n_items;
     if (!d.valid) return d;
-    const int4 u = A.items[it];
+    d.m = 0;
+    if constexpr (ENS) {
+        int lo = 0, hi = A.nmembers - 1;  // the last member whose first item is <= it
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(A.member_items + mid) <= it) lo = mid;
+            else hi = mid - 1;
+        }
+        d.m = lo;
+        it -= __ldg(A.member_items + lo);
+    }
+    const int4 u = member<ENS>(A, d.m).items[it];
     d.s = u.x;
     d.tile = u.y;
     d.b = u.z;
@@ -264,16 +292,18 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 // array by bulk copies (one thread).  The slots outside it (fewer than 4 at
 // each end) belong to neighbouring units on other CTAs' copies and go by
 // plain stores (store_chunk_edges).
+template <bool ENS>
 __device__ __forceinline__ void store_chunk_bulk(const PushArgs& A, const ChunkDesc& c, const float* buf) {
     const int a0 = c.b & ~3, b4 = (c.b + 3) & ~3, e4 = c.e & ~3;
     if (e4 <= b4) return;
     const unsigned bytes = unsigned(e4 - b4) * 4u;
-    const SpeciesState& S = A.state[c.s];
+    const SpeciesState& S = member<ENS>(A, c.m).state[c.s];
     fence_proxy_async();  // the threads' shared-memory writes, visible to the bulk copy
 #pragma unroll
     for (int k = 0; k < 4; ++k) bulk_s2g(S.cur[k] + b4, buf + k * kBufStride + (b4 - a0), bytes);
 }
 
+template <bool ENS>
 __device__ __forceinline__ void store_chunk_edges(const PushArgs& A, const ChunkDesc& c, const float* buf, int tid) {
     if (tid >= 24) return;
     const int a0 = c.b & ~3, b4 = (c.b + 3) & ~3, e4 = c.e & ~3;
@@ -281,7 +311,7 @@ __device__ __forceinline__ void store_chunk_edges(const PushArgs& A, const Chunk
     const int slot = j < 3 ? c.b + j : max(e4, b4) + (j - 3);
     const int lim = j < 3 ? min(b4, c.e) : c.e;
     if (slot >= lim) return;
-    A.state[c.s].cur[k][slot] = buf[k * kBufStride + (slot - a0)];
+    member<ENS>(A, c.m).state[c.s].cur[k][slot] = buf[k * kBufStride + (slot - a0)];
 }
 
 constexpr int kStages = 3;  // chunk buffers: one loading, one in work, one draining to global memory
@@ -297,13 +327,15 @@ constexpr int kStages = 3;  // chunk buffers: one loading, one in work, one drai
 // RZ: r-z geometry (drift_rz); a separate instance, so that the Cartesian
 // pass carries none of it.  FULL: kick, drift and deposit all on (the step's
 // pass), fixed at compile time.
-template <bool RZ, bool FULL>
+template <bool RZ, bool FULL, bool ENS = false>
 __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
     extern __shared__ __align__(128) unsigned char smem[];
     float* bufs = reinterpret_cast<float*>(smem);  // [kStages][4][kBufStride]
-    const int RW = A.rw;
+    // the tile side of the unit in work: an ensemble's members may differ
+    // (A.rw is then their largest, which sizes shared memory)
+    int RW = A.rw;
     float4* et = reinterpret_cast<float4*>(bufs + kStages * 4 * kBufStride);
-    unsigned* rt = reinterpret_cast<unsigned*>(et + RW * RW);
+    unsigned* rt = reinterpret_cast<unsigned*>(et + A.rw * A.rw);
     __shared__ __align__(8) unsigned long long bar[kStages];
     __shared__ ChunkDesc s_ch[kStages];
     __shared__ unsigned s_abs, s_cand, s_elec;
@@ -317,9 +349,9 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
         s_elec = 0;
         ChunkDesc none;
         none.valid = 0;
-        const ChunkDesc c = next_chunk(A, none, n_items);
+        const ChunkDesc c = next_chunk<ENS>(A, none, n_items);
         s_ch[0] = c;
-        if (c.valid) issue_chunk(A, c, bufs, &bar[0]);
+        if (c.valid) issue_chunk<ENS>(A, c, bufs, &bar[0]);
     }
     __syncthreads();
     ChunkDesc ch = s_ch[0];
@@ -327,7 +359,10 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
     prev.valid = 0;
     unsigned phases = 0u;  // expected parity of each stage's mbarrier
     int cur = 0, ox = 0, oy = 0;
-    if (ch.valid && ch.tile >= 0) stage_tile(A, ch.tile, et, rt, ox, oy);
+    if (ch.valid && ch.tile >= 0) {
+        if constexpr (ENS) RW = member<ENS>(A, ch.m).rw;
+        stage_tile(member<ENS>(A, ch.m), ch.tile, et, rt, ox, oy);
+    }
     const bool do_kick = FULL || A.do_kick, do_drift = FULL || A.do_drift, do_deposit = FULL || A.do_deposit;
     // the unit's absorbed, candidate and electrode counts of this thread
     unsigned my_abs = 0, my_cand = 0, my_elec = 0;
@@ -352,28 +387,32 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
             // write back the previous chunk, then reuse the buffer of the one
             // before it (its store has been read) for the next chunk's load
             if (prev.valid) {
-                store_chunk_bulk(A, prev, bufs + prv * 4 * kBufStride);
+                store_chunk_bulk<ENS>(A, prev, bufs + prv * 4 * kBufStride);
                 bulk_commit();
             }
             bulk_wait_read1();
-            const ChunkDesc nc = next_chunk(A, ch, n_items);
+            const ChunkDesc nc = next_chunk<ENS>(A, ch, n_items);
             s_ch[nxt] = nc;
             if (nc.valid) {
                 fence_proxy_async();
-                issue_chunk(A, nc, bufs + nxt * 4 * kBufStride, &bar[nxt]);
+                issue_chunk<ENS>(A, nc, bufs + nxt * 4 * kBufStride, &bar[nxt]);
             }
         }
-        if (prev.valid) store_chunk_edges(A, prev, bufs + prv * 4 * kBufStride, tid);
+        if (prev.valid) store_chunk_edges<ENS>(A, prev, bufs + prv * 4 * kBufStride, tid);
+        const PushArgs& M = member<ENS>(A, ch.m);  // this chunk's simulation
         const int s = ch.s, b = ch.b, n = ch.e - ch.b;
         const int off = b & 3;
         float* const px = bufs + cur * 4 * kBufStride + off;
         float* const py = px + kBufStride;
         float* const pvx = py + kBufStride;
         float* const pvy = pvx + kBufStride;
-        const SpeciesConst C = A.sp[s];
-        const unsigned* const cbits = (A.do_mcc && A.mcc->sp[s].nproc > 0) ? A.cbits[s] : nullptr;
+        const SpeciesConst C = M.sp[s];
+        const unsigned* const cbits = (M.do_mcc && M.mcc->sp[s].nproc > 0) ? M.cbits[s] : nullptr;
         // r-z: the azimuthal velocity is not staged; it is read and written in place
-        float* const gvz = RZ ? A.state[s].cur[4] + b : nullptr;
+        float* const gvz = RZ ? M.state[s].cur[4] + b : nullptr;
+        const int nx = M.nx, ny = M.ny, ep = M.ep;
+        const float2* const E = M.E;
+        float* const rho = M.rho;
         // the candidate bits of this thread's slots (at most two words, each
         // loaded only if one of the chunk's slots lies in it), as a 3-bit mask
         const int wt = tid - 32;  // particle lane (warp 0 has none)
@@ -394,7 +433,7 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
             if (!is_live(x)) continue;
             float vx = pvx[l], vy = pvy[l];
             if (do_kick) {
-                const Cic c = cic_weights(x, y, A.nx, A.ny);
+                const Cic c = cic_weights(x, y, nx, ny);
                 const int li = c.i0 - ox, lj = c.j0 - oy;
                 float2 e00, e10, e01, e11;
                 if (tiled && unsigned(li) < tw && unsigned(lj) < tw) {
@@ -405,10 +444,10 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
                     e01 = make_float2(p1.x, p1.y);
                     e11 = make_float2(p1.z, p1.w);
                 } else {
-                    e00 = __ldg(A.E + long(c.j0) * A.ep + c.i0);
-                    e10 = __ldg(A.E + long(c.j0) * A.ep + c.i1);
-                    e01 = __ldg(A.E + long(c.j1) * A.ep + c.i0);
-                    e11 = __ldg(A.E + long(c.j1) * A.ep + c.i1);
+                    e00 = __ldg(E + long(c.j0) * ep + c.i0);
+                    e10 = __ldg(E + long(c.j0) * ep + c.i1);
+                    e01 = __ldg(E + long(c.j1) * ep + c.i0);
+                    e11 = __ldg(E + long(c.j1) * ep + c.i1);
                 }
                 vx = __fmaf_rn(C.kq, cic_interp(c, e00.x, e10.x, e01.x, e11.x), vx);
                 vy = __fmaf_rn(C.kq, cic_interp(c, e00.y, e10.y, e01.y, e11.y), vy);
@@ -416,14 +455,14 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
             if (candidate) {
                 // kicked but not moved: k_collide finishes it after this pass
                 ++my_cand;
-                const int slot = atomicAdd(A.cand_count, 1);
-                if (slot < A.cand_cap) {
-                    A.cand[slot] = make_int2(s, b + l);
+                const int slot = atomicAdd(M.cand_count, 1);
+                if (slot < M.cand_cap) {
+                    M.cand[slot] = make_int2(s, b + l);
                     pvx[l] = vx;
                     pvy[l] = vy;
                     continue;
                 }
-                atomicAdd(A.ctr + kCtrCandOverflow, 1ull);
+                atomicAdd(M.ctr + kCtrCandOverflow, 1ull);
             }
             if (do_drift) {
                 const float x0 = x, y0 = y;
@@ -435,11 +474,11 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
                     x = __fmaf_rn(vx, C.dtdx, x);
                     y = __fmaf_rn(vy, C.dtdy, y);
                 }
-                if (!(x >= 0.0f && x <= float(A.nx - 1) && y >= 0.0f && y <= float(A.ny - 1))) {
+                if (!(x >= 0.0f && x <= float(nx - 1) && y >= 0.0f && y <= float(ny - 1))) {
                     x = __int_as_float(0x7fc00000);
                     y = x;
                     ++my_abs;
-                } else if (A.electrodes && hits_electrode(x0, y0, x, y, A.nx, A.ny, A.vbits, A.hbits)) {
+                } else if (M.electrodes && hits_electrode(x0, y0, x, y, nx, ny, M.vbits, M.hbits)) {
                     x = __int_as_float(0x7fc00000);
                     y = x;
                     ++my_elec;
@@ -452,7 +491,7 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
             if (do_deposit && is_live(x)) {
                 // after the drift's domain test a live position lies in
                 // [0, nx-1] x [0, ny-1], where cic_weights' clamp changes nothing
-                const Cic c = FULL ? cic_weights_in_domain(x, y, A.nx, A.ny) : cic_weights(x, y, A.nx, A.ny);
+                const Cic c = FULL ? cic_weights_in_domain(x, y, nx, ny) : cic_weights(x, y, nx, ny);
                 const int li = c.i0 - ox, lj = c.j0 - oy;
                 if (tiled && unsigned(li) < tw && unsigned(lj) < tw) {
                     const int q = lj * RW + li;
@@ -462,10 +501,10 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
                     atomicAdd(rt + q + dr, __float2uint_rn(__fmul_rn(c.w01, kFixScale)));
                     atomicAdd(rt + q + dr + dq, __float2uint_rn(__fmul_rn(c.w11, kFixScale)));
                 } else {
-                    atomicAdd(A.rho + long(c.j0) * A.nx + c.i0, __fmul_rn(C.scale, c.w00));
-                    atomicAdd(A.rho + long(c.j0) * A.nx + c.i1, __fmul_rn(C.scale, c.w10));
-                    atomicAdd(A.rho + long(c.j1) * A.nx + c.i0, __fmul_rn(C.scale, c.w01));
-                    atomicAdd(A.rho + long(c.j1) * A.nx + c.i1, __fmul_rn(C.scale, c.w11));
+                    atomicAdd(rho + long(c.j0) * nx + c.i0, __fmul_rn(C.scale, c.w00));
+                    atomicAdd(rho + long(c.j0) * nx + c.i1, __fmul_rn(C.scale, c.w10));
+                    atomicAdd(rho + long(c.j1) * nx + c.i0, __fmul_rn(C.scale, c.w01));
+                    atomicAdd(rho + long(c.j1) * nx + c.i1, __fmul_rn(C.scale, c.w11));
                 }
             }
         }
@@ -491,21 +530,24 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
                 for (int q = tid; q < RW * RW; q += kPushThreads) {
                     const unsigned sum = rt[q];
                     if (sum)
-                        atomicAdd(A.rho + long(oy + q / RW) * A.nx + ox + q % RW,
+                        atomicAdd(rho + long(oy + q / RW) * nx + ox + q % RW,
                                   __fmul_rn(C.scale, __fmul_rn(float(sum), kFixInv)));
                 }
             }
             if (tid == 0) {
-                if (s_abs) atomicAdd(A.ctr + kCtrAbsorbed + s, (unsigned long long)s_abs);
-                if (s_cand) atomicAdd(A.ctr + kCtrCandidates + s, (unsigned long long)s_cand);
-                if (s_elec) atomicAdd(A.ctr + kCtrElectrode + s, (unsigned long long)s_elec);
+                if (s_abs) atomicAdd(M.ctr + kCtrAbsorbed + s, (unsigned long long)s_abs);
+                if (s_cand) atomicAdd(M.ctr + kCtrCandidates + s, (unsigned long long)s_cand);
+                if (s_elec) atomicAdd(M.ctr + kCtrElectrode + s, (unsigned long long)s_elec);
                 s_abs = 0;
                 s_cand = 0;
                 s_elec = 0;
             }
             __syncthreads();
             ch = s_ch[nxt];
-            if (ch.valid && ch.tile >= 0) stage_tile(A, ch.tile, et, rt, ox, oy);
+            if (ch.valid && ch.tile >= 0) {
+                if constexpr (ENS) RW = member<ENS>(A, ch.m).rw;
+                stage_tile(member<ENS>(A, ch.m), ch.tile, et, rt, ox, oy);
+            }
         }
         cur = nxt;
     }
@@ -514,10 +556,10 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
     if (prev.valid) {
         const int prv = cur == 0 ? kStages - 1 : cur - 1;
         if (tid == 0) {
-            store_chunk_bulk(A, prev, bufs + prv * 4 * kBufStride);
+            store_chunk_bulk<ENS>(A, prev, bufs + prv * 4 * kBufStride);
             bulk_commit();
         }
-        store_chunk_edges(A, prev, bufs + prv * 4 * kBufStride, tid);
+        store_chunk_edges<ENS>(A, prev, bufs + prv * 4 * kBufStride, tid);
     }
     if (tid == 0) bulk_wait_all();
 }
@@ -1397,6 +1439,8 @@ static int prepare_pass(SimImpl& S, cudaStream_t st, int mcc, int advance_step) 
 }
 
 // The particle pass itself, once prepare_pass has run for it.
+static int run_pass_tail(SimImpl& S, cudaStream_t st, const PushArgs& A);
+
 static int run_pass(SimImpl& S, cudaStream_t st, int kick, int mcc, int drift, int deposit, double kick_factor) {
     const PushArgs A = push_args(S, kick, mcc, drift, deposit, kick_factor);
     {
@@ -1431,6 +1475,13 @@ static int run_pass(SimImpl& S, cudaStream_t st, int kick, int mcc, int drift, i
             else k_push<false, false><<<S.push_grid, kPushThreads, S.push_smem, st>>>(A);
         }
     }
+    S.launches += 1;
+    return run_pass_tail(S, st, A);
+}
+
+// What follows a particle pass: the collision candidates (k_collide) and the
+// ionisation products (k_merge_births).
+static int run_pass_tail(SimImpl& S, cudaStream_t st, const PushArgs& A) {
     {
         PhaseTimer t(S, PIC_PHASE_MERGE, st);
         if (A.do_mcc) {
@@ -1441,7 +1492,7 @@ static int run_pass(SimImpl& S, cudaStream_t st, int kick, int mcc, int drift, i
         }
         k_merge_births<<<64, 256, 0, st>>>(A);
     }
-    S.launches += 2;
+    S.launches += 1;
     PIC_LAUNCH_CHECK();
     return PIC_OK;
 }
@@ -1794,6 +1845,18 @@ __global__ void k_ens_loop(EnsControl* c, cudaGraphConditionalHandle h) {
     cudaGraphSetConditional(h, c->remaining > 0 ? 1u : 0u);
 }
 
+// The flat numbering of every member's work items for one particle pass over
+// the ensemble, and its claim counter reset (one thread).
+__global__ void k_ens_items(const PushArgs* __restrict__ members, int n, int* member_items, int* next) {
+    int total = 0;
+    for (int m = 0; m < n; ++m) {
+        member_items[m] = total;
+        total += *members[m].n_items;
+    }
+    member_items[n] = total;
+    *next = 0;
+}
+
 struct EnsImpl {
     std::vector<SimImpl*> m;
     std::vector<cudaStream_t> branch, side;
@@ -1804,7 +1867,58 @@ struct EnsImpl {
     cudaGraphExec_t exec = nullptr;
     std::vector<long long> per_step_launches;  // per member, without the sort
     std::vector<long long> sort_launches;
+    // one particle pass over every member (when every member uses the ring
+    // pass and the same geometry): the members' arguments, the flat item
+    // numbering and its claim counter, the launch shape
+    bool fused = false;
+    bool rz = false;
+    PushArgs* d_members = nullptr;
+    int* d_member_items = nullptr;
+    int* d_next = nullptr;
+    int push_grid = 0;
+    size_t push_smem = 0;
+    int rw_max = 0;
 };
+
+// Decides whether the members' particle passes run as one launch, and sets it up.
+static int ens_setup_fused(EnsImpl& E) {
+    const int n = int(E.m.size());
+    E.fused = true;
+    E.rz = E.m[0]->rz;
+    E.rw_max = 0;
+    E.push_smem = 0;
+    for (SimImpl* S : E.m) {
+        if (S->push_kernel != PIC_PUSH_RING || S->rz != E.rz) E.fused = false;
+        E.rw_max = std::max(E.rw_max, S->rw);
+        E.push_smem = std::max(E.push_smem, S->push_smem);
+    }
+    if (!E.fused) return PIC_OK;
+    std::vector<PushArgs> h(n);
+    for (int i = 0; i < n; ++i) h[i] = push_args(*E.m[i], 1, 1, 1, 1, 1.0);
+    PIC_CUDA(cudaMalloc(&E.d_members, sizeof(PushArgs) * n));
+    PIC_CUDA(cudaMalloc(&E.d_member_items, sizeof(int) * (n + 1)));
+    PIC_CUDA(cudaMalloc(&E.d_next, sizeof(int)));
+    PIC_CUDA(cudaMemcpy(E.d_members, h.data(), sizeof(PushArgs) * n, cudaMemcpyHostToDevice));
+    const void* fn = E.rz ? reinterpret_cast<const void*>(k_push<true, true, true>)
+                          : reinterpret_cast<const void*>(k_push<false, true, true>);
+    PIC_TRY(raise_smem_limit(fn, E.push_smem));
+    int per_sm = 0;
+    PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kPushThreads, E.push_smem));
+    E.push_grid = std::max(1, per_sm) * num_sms();
+    return PIC_OK;
+}
+
+// The arguments of the fused pass: the members' own, through d_members.
+static PushArgs ens_push_args(const EnsImpl& E) {
+    PushArgs A = push_args(*E.m[0], 1, 1, 1, 1, 1.0);
+    A.members = E.d_members;
+    A.member_items = E.d_member_items;
+    A.nmembers = int(E.m.size());
+    A.n_items = E.d_member_items + E.m.size();
+    A.item_next = E.d_next;
+    A.rw = E.rw_max;
+    return A;
+}
 
 // Adds, to the graph that st is capturing into, a conditional IF node whose
 // body is the member's cell sort, and moves st past it.
@@ -1898,7 +2012,42 @@ static int ens_capture_body(EnsImpl& E) {
             break;
         }
         if (cudaEventRecord(E.ev[n], root) != cudaSuccess) rc = fail(PIC_ERR_CUDA, "ensemble: fork event");
-        for (int i = 0; i < n && rc == PIC_OK; ++i) {
+        if (E.fused) {
+            // every member's sort and preparation as a branch, one particle
+            // pass over all members, then every member's field solve as a branch
+            for (int i = 0; i < n && rc == PIC_OK; ++i) {
+                SimImpl& S = *E.m[i];
+                cudaStream_t st = E.branch[i];
+                if (cudaStreamWaitEvent(st, E.ev[n], 0) != cudaSuccess) rc = fail(PIC_ERR_CUDA, "ensemble: fork wait");
+                if (rc == PIC_OK && S.d.sort_interval > 0) rc = capture_sort_if(S, E.d_steps + i, st, E.side[i]);
+                if (rc == PIC_OK) rc = prepare_pass(S, st, 1, 1);
+                if (rc == PIC_OK &&
+                    (cudaEventRecord(E.ev[i], st) != cudaSuccess || cudaStreamWaitEvent(root, E.ev[i], 0) != cudaSuccess))
+                    rc = fail(PIC_ERR_CUDA, "ensemble: join of member %d", i);
+            }
+            if (rc == PIC_OK) {
+                k_ens_items<<<1, 1, 0, root>>>(E.d_members, n, E.d_member_items, E.d_next);
+                const PushArgs A = ens_push_args(E);
+                if (E.rz) k_push<true, true, true><<<E.push_grid, kPushThreads, E.push_smem, root>>>(A);
+                else k_push<false, true, true><<<E.push_grid, kPushThreads, E.push_smem, root>>>(A);
+                if (cudaGetLastError() != cudaSuccess || cudaEventRecord(E.ev[n], root) != cudaSuccess)
+                    rc = fail(PIC_ERR_CUDA, "ensemble: particle pass");
+            }
+            for (int i = 0; i < n && rc == PIC_OK; ++i) {
+                SimImpl& S = *E.m[i];
+                cudaStream_t st = E.branch[i];
+                if (cudaStreamWaitEvent(st, E.ev[n], 0) != cudaSuccess) rc = fail(PIC_ERR_CUDA, "ensemble: fork wait");
+                if (rc == PIC_OK) rc = run_pass_tail(S, st, push_args(S, 1, 1, 1, 1, 1.0));
+                if (rc == PIC_OK) rc = field_solve(S, st, true);
+                if (rc == PIC_OK) {
+                    k_ens_advance<<<1, 1, 0, st>>>(E.d_steps + i);
+                    if (cudaEventRecord(E.ev[i], st) != cudaSuccess ||
+                        cudaStreamWaitEvent(root, E.ev[i], 0) != cudaSuccess)
+                        rc = fail(PIC_ERR_CUDA, "ensemble: join of member %d", i);
+                }
+            }
+        }
+        for (int i = 0; i < n && rc == PIC_OK && !E.fused; ++i) {
             SimImpl& S = *E.m[i];
             cudaStream_t st = E.branch[i];
             if (cudaStreamWaitEvent(st, E.ev[n], 0) != cudaSuccess) rc = fail(PIC_ERR_CUDA, "ensemble: fork wait");
@@ -1941,8 +2090,14 @@ static void ens_free(EnsImpl& E) {
     E.cap = nullptr;
     if (E.d_steps) cudaFree(E.d_steps);
     if (E.d_ctl) cudaFree(E.d_ctl);
+    if (E.d_members) cudaFree(E.d_members);
+    if (E.d_member_items) cudaFree(E.d_member_items);
+    if (E.d_next) cudaFree(E.d_next);
     E.d_steps = nullptr;
     E.d_ctl = nullptr;
+    E.d_members = nullptr;
+    E.d_member_items = nullptr;
+    E.d_next = nullptr;
 }
 
 }  // namespace pic
@@ -2320,7 +2475,16 @@ int pic_ens_create(pic_sim* const* sims, int n, pic_ens** out) {
         cudaMalloc(&E.d_steps, sizeof(long long) * n) != cudaSuccess ||
         cudaMalloc(&E.d_ctl, sizeof(EnsControl)) != cudaSuccess)
         return bail(fail(PIC_ERR_CUDA, "pic_ens_create: out of device memory"));
+    const int rc = ens_setup_fused(E);
+    if (rc != PIC_OK) return bail(rc);
     *out = e;
+    return PIC_OK;
+}
+
+int pic_ens_fused_pass(pic_ens* e, int* fused) {
+    clear_error();
+    if (!e || !fused) return fail(PIC_ERR_BAD_ARG, "pic_ens_fused_pass: bad arguments");
+    *fused = e->e.fused ? 1 : 0;
     return PIC_OK;
 }
 
@@ -2375,8 +2539,11 @@ int pic_ens_step(pic_ens* e, int n_steps, void* stream) {
         long long sorts = 0;
         if (S->d.sort_interval > 0)
             for (long long k = S->steps; k < S->steps + n_steps; ++k) sorts += (k % S->d.sort_interval == 0);
-        // the step counter, the particle pass (3, plus the collisions), the RHS and E
-        S->launches += n_steps * (1LL + 3 + (S->have_mcc ? 2 : 0) + 2) +
+        // the step counter, the particle pass (3, plus the collisions), the RHS
+        // and E; a fused ensemble's one pass (and its item numbering) is
+        // counted with the first member
+        const long long pass = E.fused ? (S == E.m[0] ? 4 : 2) : 3;
+        S->launches += n_steps * (1LL + pass + (S->have_mcc ? 2 : 0) + 2) +
                        sorts * (1 + (long long)S->ns * (5 + 3 * S->sorter.passes));
         if (S->d.sort_interval > 0) S->launches += n_steps;  // the sort condition
         S->solves += n_steps;

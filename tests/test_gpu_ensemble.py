@@ -36,9 +36,9 @@ def _workloads():
     return out
 
 
-def _make(w, cfg):
+def _make(w, cfg, push_kernel="ring"):
     _, _, _, tile, K, cmax = cfg
-    sim = ensemble.member_simulation(w, tile=tile, sort_interval=K, coarsest_max=cmax)
+    sim = ensemble.member_simulation(w, tile=tile, sort_interval=K, coarsest_max=cmax, push_kernel=push_kernel)
     for s, a in enumerate(ensemble.member_arrays(w)):
         sim.load(s, *a)
     sim.init()
@@ -54,12 +54,17 @@ def _state(sim):
     return c, xs, phi
 
 
-@pytest.mark.parametrize("steps", [23])
-def test_ensemble_matches_members_stepped_alone(steps):
+@pytest.mark.parametrize("fused", [True, False])
+def test_ensemble_matches_members_stepped_alone(fused, steps=23):
+    """fused: every member on the ring pass, so that one particle pass spans all
+    members; otherwise one member takes the per-warp pass and every member's
+    pass is its own launch."""
     ws = _workloads()
-    together = [_make(w, cfg) for w, cfg in zip(ws, MEMBERS)]
-    alone = [_make(w, cfg) for w, cfg in zip(ws, MEMBERS)]
+    kinds = ["ring"] * len(MEMBERS) if fused else ["warp"] + ["ring"] * (len(MEMBERS) - 1)
+    together = [_make(w, cfg, k) for w, cfg, k in zip(ws, MEMBERS, kinds)]
+    alone = [_make(w, cfg, k) for w, cfg, k in zip(ws, MEMBERS, kinds)]
     ens = ensemble.Ensemble(together)
+    assert ens.fused_pass == fused
     ens.step(steps - 3)
     ens.step(3)  # a second launch of the same graph
     for sim in alone:
