@@ -73,6 +73,8 @@ def parse():
     ap.add_argument("--ensemble", type=int, default=0,
                     help="also time an ensemble of this many independent collisionless members (0: off)")
     ap.add_argument("--ensemble-steps", type=int, default=500)
+    ap.add_argument("--ensemble-branches", action="store_true",
+                    help="give every ensemble member's particle pass its own launch (not one pass over all)")
     ap.add_argument("--adjoint", action="store_true",
                     help="also time the differentiable workload (forward, adjoint, finite-difference check)")
     ap.add_argument("--tune-cache", default=os.path.join(ROOT, "pic_b200", "tuned_b200.json"),
@@ -423,6 +425,8 @@ def run_ensemble(args):
         sim.init()
         sims.append(sim)
     ens = ensemble.Ensemble(sims)
+    if args.ensemble_branches:
+        ens.fused_pass = False
     ens.step(3)
     torch.cuda.synchronize()
     n0 = ens.particle_count()
@@ -434,6 +438,22 @@ def run_ensemble(args):
     ms = e0.elapsed_time(e1)
     n1 = ens.particle_count()
     fused = ens.fused_pass
+    # the other step structure on the same members, for comparison: every
+    # member's pass in its own branch (or back to the one pass)
+    ens.fused_pass = not fused
+    other = None
+    if ens.fused_pass != fused:
+        ens.step(3)
+        torch.cuda.synchronize()
+        m0 = ens.particle_count()
+        e0.record()
+        ens.step(args.ensemble_steps)
+        e1.record()
+        torch.cuda.synchronize()
+        ms2 = e0.elapsed_time(e1)
+        m1 = ens.particle_count()
+        other = {"one_particle_pass_over_all_members": ens.fused_pass, "ms_per_step": ms2 / args.ensemble_steps,
+                 "value": 0.5 * (m0 + m1) * args.ensemble_steps / (ms2 / 1e3)}
     ens.close()
     for sim in sims:
         sim.close()
@@ -454,7 +474,7 @@ def run_ensemble(args):
             "value": 0.5 * (n0 + n1) * args.ensemble_steps / (ms / 1e3), "unit": UNIT,
             "sides": {str(k): sides.count(k) for k in ensemble.SIDES}, "tuned": picked,
             "tune_s": round(tune_s, 1), "tune_measurements": tuner.measurements,
-            "one_particle_pass_over_all_members": fused,
+            "one_particle_pass_over_all_members": fused, "other_structure": other,
             "hbm": {"bytes_per_step": step_bytes, "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
                     "frac": round(gbs / peak, 4), "peak_source": kind,
                     "counts": "particle and grid bytes over the whole ensemble step (field solves included)"}}

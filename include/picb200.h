@@ -516,6 +516,10 @@ int pic_ens_step(pic_ens* e, int n_steps, void* stream);
  * PIC_PUSH_RING and the same geometry), 0 when each member's pass is its own
  * launch in its branch. */
 int pic_ens_fused_pass(pic_ens* e, int* fused);
+/* fused = 0 gives every member's particle pass its own launch in its branch
+ * (so that a member's pass can overlap another member's field solve); 1
+ * restores the one pass over all members where it applies. */
+int pic_ens_set_fused_pass(pic_ens* e, int fused);
 
 /* ------------------------------------------------------------------ */
 /* Hand-written adjoint of the collisionless step                      */

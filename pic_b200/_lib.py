@@ -188,6 +188,7 @@ SIGNATURES = {
     "pic_ens_destroy": [_vp],
     "pic_ens_step": [_vp, _i, _vp],
     "pic_ens_fused_pass": [_vp, C.POINTER(_i)],
+    "pic_ens_set_fused_pass": [_vp, _i],
     "pic_adj_create": [_vp, C.POINTER(_vp)],
     "pic_adj_destroy": [_vp],
     "pic_adj_set_particles": [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp],

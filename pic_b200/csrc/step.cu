@@ -2481,6 +2481,21 @@ int pic_ens_create(pic_sim* const* sims, int n, pic_ens** out) {
     return PIC_OK;
 }
 
+int pic_ens_set_fused_pass(pic_ens* e, int fused) {
+    clear_error();
+    if (!e) return fail(PIC_ERR_BAD_ARG, "pic_ens_set_fused_pass: e is NULL");
+    EnsImpl& E = e->e;
+    const bool want = fused != 0 && E.d_members != nullptr;
+    if (want != E.fused && E.exec) {
+        // the step graph holds the other structure: capture it again at the next step
+        PIC_CUDA(cudaDeviceSynchronize());
+        cudaGraphExecDestroy(E.exec);
+        E.exec = nullptr;
+    }
+    E.fused = want;
+    return PIC_OK;
+}
+
 int pic_ens_fused_pass(pic_ens* e, int* fused) {
     clear_error();
     if (!e || !fused) return fail(PIC_ERR_BAD_ARG, "pic_ens_fused_pass: bad arguments");

@@ -74,6 +74,10 @@ class Ensemble:
         _lib.call("pic_ens_fused_pass", self._h, C.byref(f))
         return bool(f.value)
 
+    @fused_pass.setter
+    def fused_pass(self, on: bool):
+        _lib.call("pic_ens_set_fused_pass", self._h, int(bool(on)))
+
     def particle_count(self):
         return sum(sum(m.counters()["count"]) for m in self.members)
 
