@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--mg-sweeps", type=int, nargs=2, default=(2, 2), metavar=("PRE", "POST"),
                     help="red-black sweeps before and after each coarse-grid correction")
     ap.add_argument("--omega", type=float, default=1.15, help="smoother over-relaxation")
+    ap.add_argument("--coarse-fp32", action="store_true",
+                    help="the mixed multigrid's direct solve of its 33^2 level in FP32 (default FP64)")
     ap.add_argument("--mg-launch", default="graph", choices=["persistent", "host", "graph", "cluster", "dst", "hybrid"],
                     help="multigrid launch mode (host: one launch per kernel, for profilers; dst: the "
                          "sine-transform solve in place of the V-cycles; hybrid: the levels of at most 129^2 nodes "
@@ -757,6 +759,7 @@ def main():
     GRAPH_OPTS["mg_launch"] = args.mg_launch
     GRAPH_OPTS["pre_sweeps"], GRAPH_OPTS["post_sweeps"] = args.mg_sweeps
     GRAPH_OPTS["omega"] = args.omega
+    GRAPH_OPTS["coarse_fp32"] = args.coarse_fp32
     GRAPH_OPTS["tile"] = args.tile
     GRAPH_OPTS["push_kernel"] = args.push
     world, rank, local = dist_setup(args)

@@ -160,6 +160,8 @@ typedef struct pic_mg_options {
     int coarsest_max; /* coarsen while both node counts exceed this (default 9) */
     int launch_mode;  /* pic_mg_launch_mode (r-z solves use the graph or host loop) */
     int geometry;     /* pic_geometry (default 0: Cartesian) */
+    int coarse_fp32;  /* PIC_MG_MIXED: 1 keeps the direct solve of the first level of at most 33^2
+                         nodes (its inverse and products) in FP32; 0 (default) runs it in FP64 */
 } pic_mg_options;
 
 typedef struct pic_mg_info {
@@ -203,6 +205,16 @@ int pic_mg_effective_launch_mode(pic_mg* mg, int* mode);
  * then cleared and the solver stays usable).  polls < 0 restores the default
  * (2^24 polls, about a second). */
 int pic_mg_set_wait_limit(pic_mg* mg, long long polls);
+/* The shared-memory tile geometry the multigrid's tile kernels use for
+ * `sweeps` red-black sweeps (1..8), in nodes, as PIC_MG_GEOMETRY_VALUES ints:
+ * tile side; down phase halo and width; up phase halo, width and coarse
+ * window width; the same for the finest up phase with the residual; the
+ * two-level down launch's coarse halo and width and fine halo and width; the
+ * two-level up launch's fine halo, width and coarse window width, and its
+ * coarse width and coarse window width.  No counterpart in the reference (its
+ * kernels work on whole levels); the tests emulate the tiles with these. */
+#define PIC_MG_GEOMETRY_VALUES 18
+int pic_mg_tile_geometry(int sweeps, int* out);
 
 /* Solver(solver_type='cg' | 'gmres') (src/Solvers.py:245-258: cupyx cg and
  * gmres on the 5-point Laplacian with Dirichlet rows): flexible

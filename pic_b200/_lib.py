@@ -59,7 +59,7 @@ class PicError(RuntimeError):
 
 class MgOptions(C.Structure):
     _fields_ = [("precision", C.c_int), ("pre_sweeps", C.c_int), ("post_sweeps", C.c_int), ("omega", C.c_double),
-                ("coarsest_max", C.c_int), ("launch_mode", C.c_int), ("geometry", C.c_int)]
+                ("coarsest_max", C.c_int), ("launch_mode", C.c_int), ("geometry", C.c_int), ("coarse_fp32", C.c_int)]
 
 
 GEOMETRIES = {"cartesian": 0, "rz": 1}
@@ -97,6 +97,8 @@ class SimDesc(C.Structure):
                 ("mg", MgOptions), ("sort_interval", C.c_int), ("tile", C.c_int), ("mcc", C.c_void_p),
                 ("seed", C.c_ulonglong), ("use_graph", C.c_int), ("min_cycles", C.c_int), ("push_kernel", C.c_int)]
 
+
+PIC_MG_GEOMETRY_VALUES = 18
 
 PUSH_KERNELS = {"ring": 0, "warp": 1, "warp_agg": 2}
 
@@ -160,6 +162,7 @@ SIGNATURES = {
     "pic_mg_read_info": [_vp, _d, C.POINTER(MgInfo)],
     "pic_mg_effective_launch_mode": [_vp, C.POINTER(_i)],
     "pic_mg_set_wait_limit": [_vp, C.c_longlong],
+    "pic_mg_tile_geometry": [_i, _vp],
     "pic_sorter_create": [_i, _i, _i, _i, C.POINTER(_vp)],
     "pic_sorter_destroy": [_vp],
     "pic_sort": [_vp, _vp, _vp, _vp, _vp, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],

@@ -1057,7 +1057,7 @@ constexpr int kDirectGather = (kDirectMaxFree + kDirectRows * 32 - 1) / (kDirect
 
 template <class T>
 struct DirectDesc {
-    const T* ainv;    // [n][n], row-major
+    const void* ainv;  // [n][n], row-major, FP64 (a64) or in the V-cycle's precision
     const int* idx;   // the free node of each row
     const int* zidx;  // the level's other nodes (their e is 0)
     const T* g;       // right-hand side (every node of the level)
@@ -1065,15 +1065,18 @@ struct DirectDesc {
     int n, nz;
 };
 
-template <class T>
+// MT: the precision of the inverse and of the products (double: the solve
+// in FP64 whatever the V-cycle's precision).
+template <class T, class MT>
 __global__ void __launch_bounds__(kDirectRows * 32) k_mg_direct(DirectDesc<T> D) {
-    __shared__ T gs[kDirectMaxFree];
+    __shared__ MT gs[kDirectMaxFree];
     const int lane = threadIdx.x & 31, row = blockIdx.x * kDirectRows + int(threadIdx.x >> 5);
-    T a[kDirectCols];
+    const MT* __restrict__ ainv = static_cast<const MT*>(D.ainv);
+    MT a[kDirectCols];
 #pragma unroll
     for (int u = 0; u < kDirectCols; ++u) {
         const int c = lane + 32 * u;
-        a[u] = (row < D.n && c < D.n) ? __ldg(D.ainv + long(row) * D.n + c) : T(0);
+        a[u] = (row < D.n && c < D.n) ? __ldg(ainv + long(row) * D.n + c) : MT(0);
     }
     int gi[kDirectGather];
 #pragma unroll
@@ -1086,11 +1089,11 @@ __global__ void __launch_bounds__(kDirectRows * 32) k_mg_direct(DirectDesc<T> D)
     pdl_trigger();
 #pragma unroll
     for (int u = 0; u < kDirectGather; ++u)
-        if (gi[u] >= 0) gs[threadIdx.x + u * kDirectRows * 32] = D.g[gi[u]];
+        if (gi[u] >= 0) gs[threadIdx.x + u * kDirectRows * 32] = MT(D.g[gi[u]]);
     if (blockIdx.x == 0)
         for (int k = threadIdx.x; k < D.nz; k += blockDim.x) D.e[D.zidx[k]] = T(0);
     __syncthreads();
-    T s = T(0);
+    MT s = MT(0);
 #pragma unroll
     for (int u = 0; u < kDirectCols; ++u) {
         const int c = lane + 32 * u;
@@ -1704,7 +1707,8 @@ struct MgImpl {
     int nfree_c = 0;
     // direct solve of level Lc (graph and host loops; else the coarse kernel)
     bool direct = false;
-    void* dinv = nullptr;  // [dn][dn] in the V-cycle's precision
+    void* dinv = nullptr;  // [dn][dn], FP64 unless a mixed V-cycle asked for FP32 (pic_mg_options.coarse_fp32)
+    bool dinv64 = true;
     int* didx = nullptr;   // dn free nodes, then dnz others
     int dn = 0, dnz = 0;
     double* r64 = nullptr;  // FP64 residual of phi between the cycles of a graph- or host-loop solve
@@ -1914,7 +1918,9 @@ static int configure_direct(MgImpl& M, const std::vector<int>& nxs, const std::v
     std::vector<int> all(idx);
     for (int k = 0; k < nx * ny; ++k)
         if (!fr[k]) all.push_back(k);
-    const bool f32 = M.precision == PIC_MG_MIXED;
+    // the inverse in FP32 only for a mixed-precision V-cycle that asked for it
+    const bool f32 = M.precision == PIC_MG_MIXED && M.o.coarse_fp32;
+    M.dinv64 = !f32;
     const size_t bytes = A.size() * (f32 ? sizeof(float) : sizeof(double));
     PIC_CUDA(cudaMalloc(&M.dinv, bytes));
     M.allocs.push_back(M.dinv);
@@ -2123,6 +2129,7 @@ int mg_create(int nx, int ny, double dx, double dy, const uint8_t* h_mask, const
         if (opts->coarsest_max >= 3) M.o.coarsest_max = opts->coarsest_max;
         M.o.launch_mode = opts->launch_mode;
         M.o.geometry = opts->geometry;
+        M.o.coarse_fp32 = opts->coarse_fp32 ? 1 : 0;
     }
     auto bail = [&](int code) {
         mg_release(mg);
@@ -2347,9 +2354,9 @@ static int launch_cycle(MgImpl& M, std::vector<LevelDev<T>>& lv_in, double* phi,
         }
     }
     if (!hyb && M.direct) {
-        const DirectDesc<T> D{static_cast<const T*>(M.dinv), M.didx, M.didx + M.dn, lv[M.Lc].g, lv[M.Lc].e, M.dn,
-                              M.dnz};
-        launch_pdl(k_mg_direct<T>, dim3(div_up(M.dn, kDirectRows)), dim3(kDirectRows * 32), 0, st, D);
+        const DirectDesc<T> D{M.dinv, M.didx, M.didx + M.dn, lv[M.Lc].g, lv[M.Lc].e, M.dn, M.dnz};
+        if (M.dinv64) launch_pdl(k_mg_direct<T, double>, dim3(div_up(M.dn, kDirectRows)), dim3(kDirectRows * 32), 0, st, D);
+        else launch_pdl(k_mg_direct<T, T>, dim3(div_up(M.dn, kDirectRows)), dim3(kDirectRows * 32), 0, st, D);
         ++count;
     } else if (!hyb) {
         CoarseDesc<T> D{};
@@ -2697,6 +2704,20 @@ int mg_launch_graph(pic_mg* mg, double* phi, const double* f, double tol, int ma
 int mg_info(pic_mg* mg, pic_mg_info* info) { return mg_read_info(mg->m, info); }
 const int* mg_device_converged(pic_mg* mg) { return mg->m.N.converged; }
 
+// The tile geometry of S sweeps (pic_mg_tile_geometry).
+template <int S>
+int tile_geometry(int* out) {
+    const int g[] = {kMgTile,
+                     DownGeom<S>::H,      DownGeom<S>::W,
+                     UpGeom<S>::H,        UpGeom<S>::W,        UpGeom<S>::CW,
+                     UpGeom<S, true>::H,  UpGeom<S, true>::W,  UpGeom<S, true>::CW,
+                     Down2Geom<S>::HC,    Down2Geom<S>::WC,    Down2Geom<S>::HF,    Down2Geom<S>::WF,
+                     Up2Geom<S>::HF,      Up2Geom<S>::WF,      Up2Geom<S>::CWF,     Up2Geom<S>::WC,
+                     Up2Geom<S>::CWC};
+    static_assert(sizeof(g) / sizeof(g[0]) == PIC_MG_GEOMETRY_VALUES, "geometry table");
+    for (int k = 0; k < PIC_MG_GEOMETRY_VALUES; ++k) out[k] = g[k];
+    return PIC_OK;
+}
 }  // namespace pic
 
 using namespace pic;
@@ -2738,6 +2759,22 @@ int pic_mg_solve_async(pic_mg* mg, double* d_phi, const double* d_f, double tol,
     if (!mg || !d_phi || !d_f || !(tol > 0) || cycles < 0)
         return fail(PIC_ERR_BAD_ARG, "pic_mg_solve_async: bad arguments");
     return mg_launch(mg->m, d_phi, d_f, tol, cycles, 0, as_stream(stream));
+}
+
+int pic_mg_tile_geometry(int sweeps, int* out) {
+    clear_error();
+    if (!out) return fail(PIC_ERR_BAD_ARG, "pic_mg_tile_geometry: out is NULL");
+    switch (sweeps) {
+        case 1: return pic::tile_geometry<1>(out);
+        case 2: return tile_geometry<2>(out);
+        case 3: return tile_geometry<3>(out);
+        case 4: return tile_geometry<4>(out);
+        case 5: return tile_geometry<5>(out);
+        case 6: return tile_geometry<6>(out);
+        case 7: return tile_geometry<7>(out);
+        case 8: return tile_geometry<8>(out);
+        default: return fail(PIC_ERR_BAD_ARG, "pic_mg_tile_geometry: sweeps %d outside 1..8", sweeps);
+    }
 }
 
 int pic_mg_set_wait_limit(pic_mg* mg, long long polls) {

@@ -30,7 +30,7 @@ from . import _lib
 
 class MultigridSolver:
     def __init__(self, bc_mask, nx, ny, h, levels=4, omega=1.15, precision="mixed", pre_sweeps=2, post_sweeps=2,
-                 hy=None, launch="graph", geometry="cartesian"):
+                 hy=None, launch="graph", geometry="cartesian", coarse_fp32=False):
         self.nx, self.ny = int(nx), int(ny)
         self.h = float(h)
         self.hy = float(h if hy is None else hy)
@@ -42,7 +42,8 @@ class MultigridSolver:
         self.precision = precision
         self.geometry = geometry
         opts = _lib.MgOptions(_lib.PIC_MG_MIXED if precision == "mixed" else _lib.PIC_MG_FP64, pre_sweeps,
-                              post_sweeps, self.omega, 9, _lib.MG_LAUNCH_MODES[launch], _lib.GEOMETRIES[geometry])
+                              post_sweeps, self.omega, 9, _lib.MG_LAUNCH_MODES[launch], _lib.GEOMETRIES[geometry],
+                              int(bool(coarse_fp32)))
         self._h = C.c_void_p()
         _lib.call("pic_mg_create", self.nx, self.ny, self.h, self.hy, mask.ctypes.data, C.byref(opts),
                   C.byref(self._h))

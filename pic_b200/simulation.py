@@ -60,6 +60,8 @@ class PICSimulation:
     the extrapolated potential of the last two steps needs at least two at the
     tolerances of a PIC step, and cycles that are not tested cost no WHILE-node
     iteration in the captured step.
+    coarse_fp32: keep the mixed-precision V-cycle's direct solve of its first
+    level of at most 33^2 nodes in FP32 (default: FP64).
     push_kernel: how the particle pass streams the particles, all with
     bit-identical results: "ring" (the block streams chunks through one
     shared ring of bulk copies; the fastest measured), "warp" (every warp
@@ -75,7 +77,7 @@ class PICSimulation:
     def __init__(self, nx, ny, dx, dy, dt, species, dirichlet, phi_bc=None, tol=1e-8, max_cycles=50,
                  precision="mixed", pre_sweeps=2, post_sweeps=2, omega=1.15, sort_interval=20, tile=16,
                  mcc: MccTables | None = None, seed=0, use_graph=False, eps0=Consts.eps0, mg_launch="graph",
-                 coarsest_max=9, geometry="cartesian", min_cycles=2, push_kernel="ring"):
+                 coarsest_max=9, geometry="cartesian", min_cycles=2, push_kernel="ring", coarse_fp32=False):
         self.nx, self.ny, self.dx, self.dy, self.dt = int(nx), int(ny), float(dx), float(dy), float(dt)
         self.species = list(species)
         self.geometry = geometry
@@ -94,7 +96,7 @@ class PICSimulation:
         d.max_cycles = int(max_cycles)
         d.mg = _lib.MgOptions(_lib.PIC_MG_MIXED if precision == "mixed" else _lib.PIC_MG_FP64, pre_sweeps,
                               post_sweeps, omega, int(coarsest_max), _lib.MG_LAUNCH_MODES[mg_launch],
-                              _lib.GEOMETRIES[geometry])
+                              _lib.GEOMETRIES[geometry], int(bool(coarse_fp32)))
         d.sort_interval = int(sort_interval)
         d.tile = int(tile)
         self._mcc_desc = mcc.desc() if mcc is not None else None

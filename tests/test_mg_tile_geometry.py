@@ -18,6 +18,31 @@ import pytest
 TILE = 32
 
 
+def geometry(S):
+    """The tile geometry of the library's multigrid kernels for S sweeps (pic_mg_tile_geometry)."""
+    import ctypes
+
+    from pic_b200 import _lib
+
+    out = (ctypes.c_int * _lib.PIC_MG_GEOMETRY_VALUES)()
+    _lib.call("pic_mg_tile_geometry", S, out)
+    g = list(out)
+    assert g[0] == TILE
+    return {"down": g[1:3], "up": g[3:6], "up_res": g[6:9], "down2": g[9:13], "up2": g[13:18]}
+
+
+def test_geometry_is_the_library_s():
+    """The kernels' halos are what each phase needs: the down phase one node
+    per half-sweep plus two (residual and restriction), the up phase one per
+    half-sweep (one more with the residual update), and the two-level launches
+    as the emulations below require; these emulations use the library's values."""
+    for S in range(1, 9):
+        g = geometry(S)
+        assert g["down"] == [2 * S + 2, TILE + 2 * (2 * S + 2)]
+        assert g["up"][:2] == [2 * S, TILE + 4 * S] and g["up_res"][:2] == [2 * S + 1, TILE + 4 * S + 2]
+        assert g["down2"][0] == g["down"][0] and g["down2"][1] == TILE // 2 + 2 * g["down2"][0]
+
+
 def coarse_mask(mf, fx, fy):
     """pic_mg_create's rule: a coarse node is Dirichlet if its injected fine node
     is, or an internal Dirichlet node lies in its 3 x 3 fine neighbourhood."""
@@ -148,11 +173,8 @@ def test_two_level_down_tiles_match_the_levels(shape, S):
     for J in range(m2.shape[0]):
         for I in range(m2.shape[1]):
             g2[J, I] = 0.0 if d2[J, I] else restrict_at(rC, I, J, -1, -1)
-    # Down2Geom
-    HC = 2 * S + 2
-    WC = TILE // 2 + 2 * HC
-    HF = 2 * HC + 2 + 2 * S
-    WF = TILE + 2 * HF
+    # the two-level down launch's tile geometry, as the library's kernels use it
+    HC, WC, HF, WF = geometry(S)["down2"]
     tiles_x, tiles_y = -(-fx // TILE), -(-fy // TILE)
     for ty, tx in {(0, 0), (tiles_y - 1, tiles_x - 1), (0, tiles_x // 2), (tiles_y // 2, tiles_x // 2)}:
         x0, y0 = tx * TILE, ty * TILE
@@ -213,11 +235,7 @@ def test_two_level_up_tiles_match_the_levels(shape, S):
     prolong_add(eF, dF, np.pad(eC, ((0, 1), (0, 1))), 0, 0, 0, 0)
     sweeps(eF, gF, dF, 0, 0, cF, omega, S)
     # Up2Geom
-    HF = 2 * S
-    WF = TILE + 2 * HF
-    CWF = WF // 2 + 2
-    WC = CWF + 4 * S
-    CWC = WC // 2 + 2
+    HF, WF, CWF, WC, CWC = geometry(S)["up2"]
     tiles_x, tiles_y = -(-fx // TILE), -(-fy // TILE)
     for ty, tx in {(0, 0), (tiles_y - 1, tiles_x - 1), (0, tiles_x // 2), (tiles_y // 2, tiles_x // 2)}:
         x0, y0 = tx * TILE, ty * TILE
