@@ -57,6 +57,9 @@ def parse():
                     help="particle-pass streaming: one ring of bulk copies per block (ring), per-warp pipelines "
                          "(warp), per-warp pipelines with warp-aggregated deposit atomics (warp_agg)")
     ap.add_argument("--no-poisson", action="store_true")
+    ap.add_argument("--poisson-only", action="store_true",
+                    help="run only the large Poisson comparison (its multigrid in the --mg-launch mode when that "
+                         "is 'host', so that profilers see each kernel)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-collisionless", action="store_true")
@@ -632,7 +635,7 @@ def mg_bytes_per_solve(n, precision, cycles):
     return r0 + cycles * (fine + mid + direct)
 
 
-def run_poisson():
+def run_poisson(launch="graph"):
     """Large workload: deposit 64M + 64M particles on 2049^2 nodes, solve to 1e-10 from phi = 0."""
     import torch
 
@@ -672,7 +675,7 @@ def run_poisson():
     _lib.call("pic_form_rhs", _lib.ptr(rho), _lib.ptr(mask_t), Consts.eps0, _lib.ptr(f), n, n, _lib.stream_ptr())
     res = {"workload": "large: 2049x2049 nodes, 64M e- (half in a sigma=0.2L blob) + 64M ions, tol 1e-10, phi0 = 0"}
     for prec in ("mixed", "fp64"):
-        mg = MultigridSolver(mask, n, n, w.dx, precision=prec)
+        mg = MultigridSolver(mask, n, n, w.dx, precision=prec, launch=launch)
         phi = torch.zeros(G, dtype=torch.float64, device="cuda")
         mg.solve(phi, f, tol=1e-10, max_cycles=60)  # warm-up (allocations, caches)
         best = None
@@ -765,6 +768,13 @@ def main():
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.poisson_only:
+        import torch
+
+        torch.cuda.set_device(local)
+        if rank == 0:
+            print(json.dumps({"poisson": run_poisson("host" if args.mg_launch == "host" else "graph")}), flush=True)
         return
     run_ours(args, world, rank, local)
 
