@@ -128,6 +128,11 @@ __device__ __forceinline__ const PushArgs& member(const PushArgs& A, int m) {
     if constexpr (ENS) return A.members[m];
     else return A;
 }
+// A chunk's species field holds the species plus 256 x the ensemble member.
+template <bool ENS>
+__device__ __forceinline__ int chunk_species(int s) { return ENS ? (s & 0xff) : s; }
+template <bool ENS>
+__device__ __forceinline__ int chunk_member(int s) { return ENS ? (s >> 8) : 0; }
 
 // ---- TMA bulk copies and mbarriers (inline PTX, no multicast) -------------------
 
@@ -172,8 +177,7 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* m, unsigned parity
 // One chunk of a work unit, as the producer thread hands it to the CTA.
 struct ChunkDesc {
     int valid;
-    int m;              // ensemble member (0 outside an ensemble)
-    int s, tile, b, e;  // species, tile (-1: untiled), slot range of the chunk
+    int s, tile, b, e;  // species (+ 256 x the ensemble member), tile (-1: untiled), slot range of the chunk
     int unit_e;         // end of the unit's slot range
     int first;          // first chunk of its unit
 };
@@ -186,7 +190,7 @@ __device__ __forceinline__ void issue_chunk(const PushArgs& A, const ChunkDesc& 
     const unsigned bytes = unsigned(a1 - a0) * 4u;
     // x, y, vx, vy: vz is touched only by collision candidates (k_collide)
     mbar_expect_tx(bar, 4u * bytes);
-    const SpeciesState& S = member<ENS>(A, c.m).state[c.s];
+    const SpeciesState& S = member<ENS>(A, chunk_member<ENS>(c.s)).state[chunk_species<ENS>(c.s)];
 #pragma unroll
     for (int k = 0; k < 4; ++k) bulk_g2s(buf + k * kBufStride, S.cur[k] + a0, bytes, bar);
 }
@@ -207,7 +211,7 @@ __device__ __forceinline__ ChunkDesc next_chunk(const PushArgs& A, const ChunkDe
     int it = atomicAdd(A.item_next, 1);
     d.valid = it < n_items;
     if (!d.valid) return d;
-    d.m = 0;
+    int m = 0;
     if constexpr (ENS) {
         int lo = 0, hi = A.nmembers - 1;  // the last member whose first item is <= it
         while (lo < hi) {
@@ -215,11 +219,11 @@ __device__ __forceinline__ ChunkDesc next_chunk(const PushArgs& A, const ChunkDe
             if (__ldg(A.member_items + mid) <= it) lo = mid;
             else hi = mid - 1;
         }
-        d.m = lo;
+        m = lo;
         it -= __ldg(A.member_items + lo);
     }
-    const int4 u = member<ENS>(A, d.m).items[it];
-    d.s = u.x;
+    const int4 u = member<ENS>(A, m).items[it];
+    d.s = u.x + (m << 8);
     d.tile = u.y;
     d.b = u.z;
     d.unit_e = u.w;
@@ -297,7 +301,7 @@ __device__ __forceinline__ void store_chunk_bulk(const PushArgs& A, const ChunkD
     const int a0 = c.b & ~3, b4 = (c.b + 3) & ~3, e4 = c.e & ~3;
     if (e4 <= b4) return;
     const unsigned bytes = unsigned(e4 - b4) * 4u;
-    const SpeciesState& S = member<ENS>(A, c.m).state[c.s];
+    const SpeciesState& S = member<ENS>(A, chunk_member<ENS>(c.s)).state[chunk_species<ENS>(c.s)];
     fence_proxy_async();  // the threads' shared-memory writes, visible to the bulk copy
 #pragma unroll
     for (int k = 0; k < 4; ++k) bulk_s2g(S.cur[k] + b4, buf + k * kBufStride + (b4 - a0), bytes);
@@ -311,7 +315,7 @@ __device__ __forceinline__ void store_chunk_edges(const PushArgs& A, const Chunk
     const int slot = j < 3 ? c.b + j : max(e4, b4) + (j - 3);
     const int lim = j < 3 ? min(b4, c.e) : c.e;
     if (slot >= lim) return;
-    member<ENS>(A, c.m).state[c.s].cur[k][slot] = buf[k * kBufStride + (slot - a0)];
+    member<ENS>(A, chunk_member<ENS>(c.s)).state[chunk_species<ENS>(c.s)].cur[k][slot] = buf[k * kBufStride + (slot - a0)];
 }
 
 constexpr int kStages = 3;  // chunk buffers: one loading, one in work, one draining to global memory
@@ -360,8 +364,8 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
     unsigned phases = 0u;  // expected parity of each stage's mbarrier
     int cur = 0, ox = 0, oy = 0;
     if (ch.valid && ch.tile >= 0) {
-        if constexpr (ENS) RW = member<ENS>(A, ch.m).rw;
-        stage_tile(member<ENS>(A, ch.m), ch.tile, et, rt, ox, oy);
+        if constexpr (ENS) RW = member<ENS>(A, chunk_member<ENS>(ch.s)).rw;
+        stage_tile(member<ENS>(A, chunk_member<ENS>(ch.s)), ch.tile, et, rt, ox, oy);
     }
     const bool do_kick = FULL || A.do_kick, do_drift = FULL || A.do_drift, do_deposit = FULL || A.do_deposit;
     // the unit's absorbed, candidate and electrode counts of this thread
@@ -399,8 +403,8 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
             }
         }
         if (prev.valid) store_chunk_edges<ENS>(A, prev, bufs + prv * 4 * kBufStride, tid);
-        const PushArgs& M = member<ENS>(A, ch.m);  // this chunk's simulation
-        const int s = ch.s, b = ch.b, n = ch.e - ch.b;
+        const PushArgs& M = member<ENS>(A, chunk_member<ENS>(ch.s));  // this chunk's simulation
+        const int s = chunk_species<ENS>(ch.s), b = ch.b, n = ch.e - ch.b;
         const int off = b & 3;
         float* const px = bufs + cur * 4 * kBufStride + off;
         float* const py = px + kBufStride;
@@ -410,9 +414,6 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
         const unsigned* const cbits = (M.do_mcc && M.mcc->sp[s].nproc > 0) ? M.cbits[s] : nullptr;
         // r-z: the azimuthal velocity is not staged; it is read and written in place
         float* const gvz = RZ ? M.state[s].cur[4] + b : nullptr;
-        const int nx = M.nx, ny = M.ny, ep = M.ep;
-        const float2* const E = M.E;
-        float* const rho = M.rho;
         // the candidate bits of this thread's slots (at most two words, each
         // loaded only if one of the chunk's slots lies in it), as a 3-bit mask
         const int wt = tid - 32;  // particle lane (warp 0 has none)
@@ -433,7 +434,7 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
             if (!is_live(x)) continue;
             float vx = pvx[l], vy = pvy[l];
             if (do_kick) {
-                const Cic c = cic_weights(x, y, nx, ny);
+                const Cic c = cic_weights(x, y, M.nx, M.ny);
                 const int li = c.i0 - ox, lj = c.j0 - oy;
                 float2 e00, e10, e01, e11;
                 if (tiled && unsigned(li) < tw && unsigned(lj) < tw) {
@@ -444,10 +445,10 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
                     e01 = make_float2(p1.x, p1.y);
                     e11 = make_float2(p1.z, p1.w);
                 } else {
-                    e00 = __ldg(E + long(c.j0) * ep + c.i0);
-                    e10 = __ldg(E + long(c.j0) * ep + c.i1);
-                    e01 = __ldg(E + long(c.j1) * ep + c.i0);
-                    e11 = __ldg(E + long(c.j1) * ep + c.i1);
+                    e00 = __ldg(M.E + long(c.j0) * M.ep + c.i0);
+                    e10 = __ldg(M.E + long(c.j0) * M.ep + c.i1);
+                    e01 = __ldg(M.E + long(c.j1) * M.ep + c.i0);
+                    e11 = __ldg(M.E + long(c.j1) * M.ep + c.i1);
                 }
                 vx = __fmaf_rn(C.kq, cic_interp(c, e00.x, e10.x, e01.x, e11.x), vx);
                 vy = __fmaf_rn(C.kq, cic_interp(c, e00.y, e10.y, e01.y, e11.y), vy);
@@ -474,11 +475,11 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
                     x = __fmaf_rn(vx, C.dtdx, x);
                     y = __fmaf_rn(vy, C.dtdy, y);
                 }
-                if (!(x >= 0.0f && x <= float(nx - 1) && y >= 0.0f && y <= float(ny - 1))) {
+                if (!(x >= 0.0f && x <= float(M.nx - 1) && y >= 0.0f && y <= float(M.ny - 1))) {
                     x = __int_as_float(0x7fc00000);
                     y = x;
                     ++my_abs;
-                } else if (M.electrodes && hits_electrode(x0, y0, x, y, nx, ny, M.vbits, M.hbits)) {
+                } else if (M.electrodes && hits_electrode(x0, y0, x, y, M.nx, M.ny, M.vbits, M.hbits)) {
                     x = __int_as_float(0x7fc00000);
                     y = x;
                     ++my_elec;
@@ -491,7 +492,7 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
             if (do_deposit && is_live(x)) {
                 // after the drift's domain test a live position lies in
                 // [0, nx-1] x [0, ny-1], where cic_weights' clamp changes nothing
-                const Cic c = FULL ? cic_weights_in_domain(x, y, nx, ny) : cic_weights(x, y, nx, ny);
+                const Cic c = FULL ? cic_weights_in_domain(x, y, M.nx, M.ny) : cic_weights(x, y, M.nx, M.ny);
                 const int li = c.i0 - ox, lj = c.j0 - oy;
                 if (tiled && unsigned(li) < tw && unsigned(lj) < tw) {
                     const int q = lj * RW + li;
@@ -501,10 +502,10 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
                     atomicAdd(rt + q + dr, __float2uint_rn(__fmul_rn(c.w01, kFixScale)));
                     atomicAdd(rt + q + dr + dq, __float2uint_rn(__fmul_rn(c.w11, kFixScale)));
                 } else {
-                    atomicAdd(rho + long(c.j0) * nx + c.i0, __fmul_rn(C.scale, c.w00));
-                    atomicAdd(rho + long(c.j0) * nx + c.i1, __fmul_rn(C.scale, c.w10));
-                    atomicAdd(rho + long(c.j1) * nx + c.i0, __fmul_rn(C.scale, c.w01));
-                    atomicAdd(rho + long(c.j1) * nx + c.i1, __fmul_rn(C.scale, c.w11));
+                    atomicAdd(M.rho + long(c.j0) * M.nx + c.i0, __fmul_rn(C.scale, c.w00));
+                    atomicAdd(M.rho + long(c.j0) * M.nx + c.i1, __fmul_rn(C.scale, c.w10));
+                    atomicAdd(M.rho + long(c.j1) * M.nx + c.i0, __fmul_rn(C.scale, c.w01));
+                    atomicAdd(M.rho + long(c.j1) * M.nx + c.i1, __fmul_rn(C.scale, c.w11));
                 }
             }
         }
@@ -530,7 +531,7 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
                 for (int q = tid; q < RW * RW; q += kPushThreads) {
                     const unsigned sum = rt[q];
                     if (sum)
-                        atomicAdd(rho + long(oy + q / RW) * nx + ox + q % RW,
+                        atomicAdd(M.rho + long(oy + q / RW) * M.nx + ox + q % RW,
                                   __fmul_rn(C.scale, __fmul_rn(float(sum), kFixInv)));
                 }
             }
@@ -545,8 +546,8 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
             __syncthreads();
             ch = s_ch[nxt];
             if (ch.valid && ch.tile >= 0) {
-                if constexpr (ENS) RW = member<ENS>(A, ch.m).rw;
-                stage_tile(member<ENS>(A, ch.m), ch.tile, et, rt, ox, oy);
+                if constexpr (ENS) RW = member<ENS>(A, chunk_member<ENS>(ch.s)).rw;
+                stage_tile(member<ENS>(A, chunk_member<ENS>(ch.s)), ch.tile, et, rt, ox, oy);
             }
         }
         cur = nxt;
