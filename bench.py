@@ -53,7 +53,7 @@ def parse():
                     help="steps between cell sorts (80: the autotuner's choice for 513^2 shapes)")
     ap.add_argument("--particles", type=int, default=4_000_000, help="per species")
     ap.add_argument("--tile", type=int, default=16, help="cells per side of the push's work tiles")
-    ap.add_argument("--push", default="ring", choices=["ring", "warp", "warp_agg"],
+    ap.add_argument("--push", default="ring", choices=["ring", "warp", "warp_agg", "pipe"],
                     help="particle-pass streaming: one ring of bulk copies per block (ring), per-warp pipelines "
                          "(warp), per-warp pipelines with warp-aggregated deposit atomics (warp_agg)")
     ap.add_argument("--no-poisson", action="store_true")
@@ -310,7 +310,7 @@ def run_ours(args, world, rank, local):
     achieved = bytes_per_launch / (push_ms / 1e3) / 1e9
     peak, peak_kind = peak_hbm()
     traffic = ncu_traffic()
-    roofline = {"bound": "hbm", "kernel": "k_push" if args.push == "ring" else "k_push_warp", "achieved": round(achieved, 1),
+    roofline = {"bound": "hbm", "kernel": {"ring": "k_push", "pipe": "k_push_pipe"}.get(args.push, "k_push_warp"), "achieved": round(achieved, 1),
                 "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
                 "bytes_per_launch": bytes_per_launch, "ms_per_launch": round(push_ms, 5)}

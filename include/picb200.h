@@ -376,7 +376,9 @@ typedef enum pic_push_kernel {
     PIC_PUSH_WARP = 1,     /* each warp streams its own groups of particles through its own stage buffers
                               (asynchronous copies), E tiles by bulk tensor copies, one charge-tile atomic
                               per particle and node */
-    PIC_PUSH_WARP_AGG = 2  /* as PIC_PUSH_WARP, the charge deposited with warp-aggregated atomics */
+    PIC_PUSH_WARP_AGG = 2, /* as PIC_PUSH_WARP, the charge deposited with warp-aggregated atomics */
+    PIC_PUSH_PIPE = 3      /* as PIC_PUSH_RING, with a producer warp and consumer warps that meet on
+                              mbarriers instead of one block barrier per chunk */
 } pic_push_kernel;
 
 typedef struct pic_sim_counters {

@@ -100,7 +100,7 @@ class SimDesc(C.Structure):
 
 PIC_MG_GEOMETRY_VALUES = 18
 
-PUSH_KERNELS = {"ring": 0, "warp": 1, "warp_agg": 2}
+PUSH_KERNELS = {"ring": 0, "warp": 1, "warp_agg": 2, "pipe": 3}
 
 
 PIC_ADJ_MAX_SEGMENTS = 16

@@ -565,6 +565,315 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
     if (tid == 0) bulk_wait_all();
 }
 
+// ---- particle pass, producer warp and consumer warps without block barriers ----------
+//
+// k_push_pipe: the work of k_push (same chunks, ring of three bulk-copied
+// buffers, E tile and charge tile per unit, same per-particle arithmetic, in
+// the same blocked order), with the per-chunk block barrier replaced by
+// mbarriers, so that the consumer warps never wait for one another inside a
+// unit:
+//   warp 0 (producer)   claims chunks, publishes each chunk's descriptor,
+//                       loads it (cp.async.bulk, completion on full[stage]),
+//                       waits for done[stage] (one arrival per consumer warp),
+//                       writes the chunk back (bulk stores, ragged edges by
+//                       plain stores) and reloads the buffer two chunks ahead;
+//                       past the last chunk it completes full[stage] with a
+//                       plain arrival, the end marker
+//   warps 1..7          wait full[stage], push their three particles each,
+//                       arrive on done[stage]; at the end of a unit they meet
+//                       on an mbarrier (cbar), flush the charge tile, stage
+//                       the next unit's E tile and meet again
+// Every wait is bounded: a thread whose wait gives up sets the error flag
+// and leaves; the others' waits on it then give up in turn.  The producer
+// waits, with the default limit, for every copy it started before it leaves.
+__device__ __forceinline__ void mbar_arrive(unsigned long long* m) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(m)) : "memory");
+}
+
+// stage_tile's E staging by the consumer threads (ctid in [0, nc)); the
+// charge tile is left as the last flush zeroed it.
+__device__ __forceinline__ void stage_etile_c(const PushArgs& A, int tile, float4* et, int& ox, int& oy, int ctid,
+                                              int nc) {
+    const int RW = A.rw;
+    ox = (tile % A.tiles_x) * A.tile - kHalo;
+    oy = (tile / A.tiles_x) * A.tile - kHalo;
+    for (int q = ctid; q < RW * RW; q += nc) {
+        const int gi = ox + q % RW, gj = oy + q / RW;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (gi >= 0 && gj >= 0 && gi < A.nx && gj < A.ny) {
+            const long k = long(gj) * A.ep + gi;
+            const float2 e0 = __ldg(A.E + k), e1 = __ldg(A.E + k + (gi + 1 < A.nx ? 1 : 0));
+            v = make_float4(e0.x, e0.y, e1.x, e1.y);
+        }
+        et[q] = v;
+    }
+}
+
+constexpr int kConsumerWarps = kPushThreads / 32 - 1;
+constexpr int kConsumers = kConsumerWarps * 32;
+
+// Consumer warps: arrive on cbar and wait for the phase (bounded).
+__device__ __forceinline__ bool consumer_meet(unsigned long long* cbar, unsigned& phase, unsigned long long limit) {
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) mbar_arrive(cbar);
+    const bool ok = mbar_wait(cbar, phase, limit);
+    phase ^= 1u;
+    return ok;
+}
+
+template <bool RZ, bool FULL>
+__global__ void __launch_bounds__(kPushThreads, 4) k_push_pipe(PushArgs A) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    float* bufs = reinterpret_cast<float*>(smem);  // [kStages][4][kBufStride]
+    const int RW = A.rw;
+    float4* et = reinterpret_cast<float4*>(bufs + kStages * 4 * kBufStride);
+    unsigned* rt = reinterpret_cast<unsigned*>(et + RW * RW);
+    __shared__ __align__(8) unsigned long long full[kStages], done[kStages], cbar;
+    __shared__ ChunkDesc s_ch[kStages];
+    __shared__ unsigned s_abs, s_cand, s_elec;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int n_items = *A.n_items;
+    for (int q = tid; q < RW * RW; q += kPushThreads) rt[q] = 0u;
+    if (tid == 0) {
+        for (int k = 0; k < kStages; ++k) {
+            mbar_init(&full[k], 1);
+            mbar_init(&done[k], kConsumerWarps);
+        }
+        mbar_init(&cbar, kConsumerWarps);
+        fence_mbar_init();
+        s_abs = s_cand = s_elec = 0u;
+        // the first two chunks
+        ChunkDesc none;
+        none.valid = 0;
+        for (int k = 0; k < 2; ++k) {
+            const ChunkDesc c = (k == 0 || s_ch[0].valid) ? next_chunk<false>(A, k ? s_ch[0] : none, n_items) : none;
+            s_ch[k] = c;
+            if (c.valid) issue_chunk<false>(A, c, bufs + k * 4 * kBufStride, &full[k]);
+            else mbar_arrive(&full[k]);  // the end marker
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+        // ---- producer ----
+        int j = 0;
+        bool ok = true;
+        for (;; ++j) {
+            const int st = j % kStages;
+            const ChunkDesc cj = s_ch[st];
+            if (!cj.valid) break;
+            // the consumers are done with chunk j: write it back
+            ok = mbar_wait(&done[st], unsigned(j / kStages) & 1u, A.wait_limit);
+            if (!ok) break;
+            float* const buf = bufs + st * 4 * kBufStride;
+            if (lane == 0) {
+                store_chunk_bulk<false>(A, cj, buf);
+                bulk_commit();
+            }
+            store_chunk_edges<false>(A, cj, buf, lane);
+            // chunk j + 2 into the buffer of chunk j - 1, once its store has read it
+            if (lane == 0) {
+                const int s2 = (j + 2) % kStages;
+                const ChunkDesc c1 = s_ch[(j + 1) % kStages];
+                ChunkDesc c2;
+                c2.valid = 0;
+                if (c1.valid) c2 = next_chunk<false>(A, c1, n_items);
+                bulk_wait_read1();
+                s_ch[s2] = c2;
+                if (c2.valid) {
+                    fence_proxy_async();
+                    issue_chunk<false>(A, c2, bufs + s2 * 4 * kBufStride, &full[s2]);
+                } else {
+                    mbar_arrive(&full[s2]);  // the end marker
+                }
+            }
+            __syncwarp();
+        }
+        if (lane == 0) {
+            if (!ok) {
+                atomicExch(A.error, 1);
+                // the loads started for chunks j and j + 1 (chunk j + 2's was not)
+                for (int k = 0; k <= 1; ++k) {
+                    const int c = j + k, st = c % kStages;
+                    if (s_ch[st].valid) mbar_wait(&full[st], unsigned(c / kStages) & 1u, kWaitLimit);
+                }
+            }
+            bulk_wait_all();
+        }
+        return;
+    }
+    // ---- consumers ----
+    const int ctid = tid - 32;
+    const bool do_kick = FULL || A.do_kick, do_drift = FULL || A.do_drift, do_deposit = FULL || A.do_deposit;
+    unsigned cphase = 0u;
+    int ox = 0, oy = 0;
+    if (!mbar_wait(&full[0], 0u, A.wait_limit)) {
+        atomicExch(A.error, 1);
+        return;
+    }
+    ChunkDesc ch = s_ch[0];
+    if (!ch.valid) return;
+    if (ch.tile >= 0) stage_etile_c(A, ch.tile, et, ox, oy, ctid, kConsumers);
+    if (!consumer_meet(&cbar, cphase, A.wait_limit)) {
+        atomicExch(A.error, 1);
+        return;
+    }
+    unsigned my_abs = 0, my_cand = 0, my_elec = 0;
+    const unsigned tw = unsigned(RW - 1);  // staged tile: local cell index in [0, RW-2]
+    for (int j = 0;; ++j) {
+        const int cur = j % kStages;
+        const bool tiled = ch.tile >= 0;
+        const int s = ch.s, b = ch.b, n = ch.e - ch.b;
+        const int off = b & 3;
+        float* const px = bufs + cur * 4 * kBufStride + off;
+        float* const py = px + kBufStride;
+        float* const pvx = py + kBufStride;
+        float* const pvy = pvx + kBufStride;
+        const SpeciesConst C = A.sp[s];
+        const unsigned* const cbits = (A.do_mcc && A.mcc->sp[s].nproc > 0) ? A.cbits[s] : nullptr;
+        float* const gvz = RZ ? A.state[s].cur[4] + b : nullptr;
+        const int s0 = b + ctid * kPushP, s_last = min(s0 + kPushP, b + n) - 1;
+        unsigned cmask = 0u;
+        if (cbits && s0 <= s_last) {
+            const unsigned cw0 = __ldg(cbits + (s0 >> 5));
+            const unsigned cw1 = (s_last >> 5) != (s0 >> 5) ? __ldg(cbits + (s_last >> 5)) : 0u;
+            cmask = __funnelshift_r(cw0, cw1, s0 & 31);
+        }
+#pragma unroll
+        for (int k = 0; k < kPushP; ++k) {
+            const int l = ctid * kPushP + k;
+            if (l >= n) break;
+            const bool candidate = (cmask >> k) & 1u;
+            float x = px[l], y = py[l];
+            if (!is_live(x)) continue;
+            float vx = pvx[l], vy = pvy[l];
+            if (do_kick) {
+                const Cic c = cic_weights(x, y, A.nx, A.ny);
+                const int li = c.i0 - ox, lj = c.j0 - oy;
+                float2 e00, e10, e01, e11;
+                if (tiled && unsigned(li) < tw && unsigned(lj) < tw) {
+                    const int q = lj * RW + li;
+                    const float4 p0 = et[q], p1 = et[q + (c.j1 - c.j0) * RW];
+                    e00 = make_float2(p0.x, p0.y);
+                    e10 = make_float2(p0.z, p0.w);
+                    e01 = make_float2(p1.x, p1.y);
+                    e11 = make_float2(p1.z, p1.w);
+                } else {
+                    e00 = __ldg(A.E + long(c.j0) * A.ep + c.i0);
+                    e10 = __ldg(A.E + long(c.j0) * A.ep + c.i1);
+                    e01 = __ldg(A.E + long(c.j1) * A.ep + c.i0);
+                    e11 = __ldg(A.E + long(c.j1) * A.ep + c.i1);
+                }
+                vx = __fmaf_rn(C.kq, cic_interp(c, e00.x, e10.x, e01.x, e11.x), vx);
+                vy = __fmaf_rn(C.kq, cic_interp(c, e00.y, e10.y, e01.y, e11.y), vy);
+            }
+            if (candidate) {
+                // kicked but not moved: k_collide finishes it after this pass
+                ++my_cand;
+                const int slot = atomicAdd(A.cand_count, 1);
+                if (slot < A.cand_cap) {
+                    A.cand[slot] = make_int2(s, b + l);
+                    pvx[l] = vx;
+                    pvy[l] = vy;
+                    continue;
+                }
+                atomicAdd(A.ctr + kCtrCandOverflow, 1ull);
+            }
+            if (do_drift) {
+                const float x0 = x, y0 = y;
+                if constexpr (RZ) {
+                    float vz = gvz[l];
+                    drift_rz(x, y, vx, vy, vz, C.dtdx, C.dtdy);
+                    gvz[l] = vz;
+                } else {
+                    x = __fmaf_rn(vx, C.dtdx, x);
+                    y = __fmaf_rn(vy, C.dtdy, y);
+                }
+                if (!(x >= 0.0f && x <= float(A.nx - 1) && y >= 0.0f && y <= float(A.ny - 1))) {
+                    x = __int_as_float(0x7fc00000);
+                    y = x;
+                    ++my_abs;
+                } else if (A.electrodes && hits_electrode(x0, y0, x, y, A.nx, A.ny, A.vbits, A.hbits)) {
+                    x = __int_as_float(0x7fc00000);
+                    y = x;
+                    ++my_elec;
+                }
+            }
+            px[l] = x;
+            py[l] = y;
+            pvx[l] = vx;
+            pvy[l] = vy;
+            if (do_deposit && is_live(x)) {
+                const Cic c = FULL ? cic_weights_in_domain(x, y, A.nx, A.ny) : cic_weights(x, y, A.nx, A.ny);
+                const int li = c.i0 - ox, lj = c.j0 - oy;
+                if (tiled && unsigned(li) < tw && unsigned(lj) < tw) {
+                    const int q = lj * RW + li;
+                    const int dq = c.i1 - c.i0, dr = (c.j1 - c.j0) * RW;
+                    atomicAdd(rt + q, __float2uint_rn(__fmul_rn(c.w00, kFixScale)));
+                    atomicAdd(rt + q + dq, __float2uint_rn(__fmul_rn(c.w10, kFixScale)));
+                    atomicAdd(rt + q + dr, __float2uint_rn(__fmul_rn(c.w01, kFixScale)));
+                    atomicAdd(rt + q + dr + dq, __float2uint_rn(__fmul_rn(c.w11, kFixScale)));
+                } else {
+                    atomicAdd(A.rho + long(c.j0) * A.nx + c.i0, __fmul_rn(C.scale, c.w00));
+                    atomicAdd(A.rho + long(c.j0) * A.nx + c.i1, __fmul_rn(C.scale, c.w10));
+                    atomicAdd(A.rho + long(c.j1) * A.nx + c.i0, __fmul_rn(C.scale, c.w01));
+                    atomicAdd(A.rho + long(c.j1) * A.nx + c.i1, __fmul_rn(C.scale, c.w11));
+                }
+            }
+        }
+        // this warp is done with chunk j (its results are in the buffer)
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&done[cur]);
+        const bool unit_end = ch.e == ch.unit_e;
+        const int nst = (j + 1) % kStages;
+        if (!mbar_wait(&full[nst], unsigned((j + 1) / kStages) & 1u, A.wait_limit)) {
+            atomicExch(A.error, 1);
+            return;
+        }
+        const ChunkDesc nc = s_ch[nst];
+        if (unit_end) {
+            // the unit's deposits and counters are complete once every consumer has met
+            my_abs = __reduce_add_sync(0xffffffffu, my_abs);
+            my_cand = __reduce_add_sync(0xffffffffu, my_cand);
+            my_elec = __reduce_add_sync(0xffffffffu, my_elec);
+            if (lane == 0) {
+                if (my_abs) atomicAdd(&s_abs, my_abs);
+                if (my_cand) atomicAdd(&s_cand, my_cand);
+                if (my_elec) atomicAdd(&s_elec, my_elec);
+            }
+            my_abs = my_cand = my_elec = 0u;
+            if (!consumer_meet(&cbar, cphase, A.wait_limit)) {
+                atomicExch(A.error, 1);
+                return;
+            }
+            if (tiled && do_deposit) {
+                // flush, and leave the tile zeroed for the next unit
+                for (int q = ctid; q < RW * RW; q += kConsumers) {
+                    const unsigned sum = rt[q];
+                    if (sum) {
+                        atomicAdd(A.rho + long(oy + q / RW) * A.nx + ox + q % RW,
+                                  __fmul_rn(C.scale, __fmul_rn(float(sum), kFixInv)));
+                        rt[q] = 0u;
+                    }
+                }
+            }
+            if (ctid == 0) {
+                if (s_abs) atomicAdd(A.ctr + kCtrAbsorbed + s, (unsigned long long)s_abs);
+                if (s_cand) atomicAdd(A.ctr + kCtrCandidates + s, (unsigned long long)s_cand);
+                if (s_elec) atomicAdd(A.ctr + kCtrElectrode + s, (unsigned long long)s_elec);
+                s_abs = s_cand = s_elec = 0u;
+            }
+            // every E-tile read of this unit is done: stage the next unit's
+            if (nc.valid && nc.tile >= 0) stage_etile_c(A, nc.tile, et, ox, oy, ctid, kConsumers);
+            if (!consumer_meet(&cbar, cphase, A.wait_limit)) {
+                atomicExch(A.error, 1);
+                return;
+            }
+        }
+        if (!nc.valid) return;
+        ch = nc;
+    }
+}
+
 // ---- particle pass, per-warp pipeline --------------------------------------------
 //
 // The same work as k_push (same work units, E tile and charge tile per unit,
@@ -1468,6 +1777,14 @@ static int run_pass(SimImpl& S, cudaStream_t st, int kick, int mcc, int drift, i
                     else k_push_warp<false, false, false><<<g, kPushThreads, sm, st>>>(A);
                 }
             }
+        } else if (S.push_kernel == PIC_PUSH_PIPE) {
+            if (S.rz) {
+                if (full) k_push_pipe<true, true><<<S.push_grid, kPushThreads, S.push_smem, st>>>(A);
+                else k_push_pipe<true, false><<<S.push_grid, kPushThreads, S.push_smem, st>>>(A);
+            } else {
+                if (full) k_push_pipe<false, true><<<S.push_grid, kPushThreads, S.push_smem, st>>>(A);
+                else k_push_pipe<false, false><<<S.push_grid, kPushThreads, S.push_smem, st>>>(A);
+            }
         } else if (S.rz) {
             if (full) k_push<true, true><<<S.push_grid, kPushThreads, S.push_smem, st>>>(A);
             else k_push<true, false><<<S.push_grid, kPushThreads, S.push_smem, st>>>(A);
@@ -1763,12 +2080,18 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
                                reinterpret_cast<const void*>(k_push<true, false>),
                                reinterpret_cast<const void*>(k_push<true, true>)};
     for (const void* fn : push_fns) PIC_TRY(raise_smem_limit(fn, S.push_smem));
+    const void* pipe_fns[4] = {reinterpret_cast<const void*>(k_push_pipe<false, false>),
+                               reinterpret_cast<const void*>(k_push_pipe<false, true>),
+                               reinterpret_cast<const void*>(k_push_pipe<true, false>),
+                               reinterpret_cast<const void*>(k_push_pipe<true, true>)};
+    for (const void* fn : pipe_fns) PIC_TRY(raise_smem_limit(fn, S.push_smem));
     // the grid of the step's instance (the others run the same grid)
     const void* push_fn = push_fns[S.rz ? 3 : 1];
     int per_sm = 0;
     PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_fn, kPushThreads, S.push_smem));
     S.push_grid = std::max(1, per_sm) * num_sms();
-    if (d->push_kernel != PIC_PUSH_RING && d->push_kernel != PIC_PUSH_WARP && d->push_kernel != PIC_PUSH_WARP_AGG)
+    if (d->push_kernel != PIC_PUSH_RING && d->push_kernel != PIC_PUSH_WARP && d->push_kernel != PIC_PUSH_WARP_AGG &&
+        d->push_kernel != PIC_PUSH_PIPE)
         return fail(PIC_ERR_BAD_ARG, "pic_sim_create: push_kernel %d", d->push_kernel);
     // k_push_warp's E-tile loads start at x = tile * tx - 4, which the tensor
     // copy needs even (16-byte aligned): an odd tile takes the ring kernel

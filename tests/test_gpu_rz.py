@@ -156,7 +156,7 @@ def assert_bits(a, b):
     np.testing.assert_array_equal(a[~np.isnan(a)].view(np.uint32), b[~np.isnan(b)].view(np.uint32))
 
 
-@pytest.mark.parametrize("push_kernel", ["ring", "warp", "warp_agg"])
+@pytest.mark.parametrize("push_kernel", ["ring", "warp", "warp_agg", "pipe"])
 def test_fused_rz_step_bit_exact(push_kernel):
     w = workloads.scaled(workloads.SMALL, n=30_000)
     sim, ref, mask = make_rz_sim(w, push_kernel=push_kernel)

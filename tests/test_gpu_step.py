@@ -55,7 +55,7 @@ def assert_bits(a, b):
     np.testing.assert_array_equal(a[~np.isnan(a)].view(np.uint32), b[~np.isnan(b)].view(np.uint32))
 
 
-@pytest.mark.parametrize("push_kernel", ["ring", "warp", "warp_agg"])
+@pytest.mark.parametrize("push_kernel", ["ring", "warp", "warp_agg", "pipe"])
 @pytest.mark.parametrize("sort_interval", [0, 1])
 def test_particle_passes_bit_exact(sort_interval, push_kernel):
     w = workloads.scaled(workloads.SMALL, n=30_000)
@@ -151,7 +151,7 @@ def test_fused_step_with_mcc_bookkeeping():
     assert 0 < c["born"][0] <= c["collisions"][0][2] and c["born"][1] <= c["collisions"][0][2]
 
 
-@pytest.mark.parametrize("push_kernel", ["ring", "warp", "warp_agg"])
+@pytest.mark.parametrize("push_kernel", ["ring", "warp", "warp_agg", "pipe"])
 def test_internal_electrodes_collect_bit_exact(push_kernel):
     """Cathode and anode lines inside the domain (the equipotentials of the
     reference's test.inp, at x = L/4 and 3L/4 from the bottom wall to half

@@ -47,7 +47,7 @@ def test_persistent_solve_barrier_timeout_is_reported():
     assert rel < 1e-10 and cycles > 0
 
 
-@pytest.mark.parametrize("push_kernel", ["ring", "warp"])
+@pytest.mark.parametrize("push_kernel", ["ring", "warp", "pipe"])
 def test_particle_pass_wait_timeout_is_reported(push_kernel):
     w = workloads.scaled(workloads.SMALL, n=50_000)
     mask, phi_bc = workloads.dirichlet(w)
