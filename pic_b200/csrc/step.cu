@@ -103,7 +103,6 @@ struct alignas(64) PushArgs {
     const MccDev* mcc;  // device copy of the tables' descriptor
     uint2 key;
     const uint32_t* step;
-    BirthDev births;
     const unsigned* cbits[PIC_MAX_SPECIES];  // null-collision candidate bit per slot (k_mcc_bits), or null
     const unsigned *vbits, *hbits;           // internal electrode edges (hits_electrode), when `electrodes`
     int electrodes;
@@ -1221,8 +1220,49 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push_warp(const __grid_cons
             if (epend & (1u << b)) mbar_wait(&ebars[b], (ephase >> b) & 1u, kWaitLimit);
 }
 
+// An ionisation product of this step's collisions, born at (x, y): its first
+// drift with its own velocity, then, unless that takes it out of the domain
+// or onto an electrode (it is then never stored), its slot at the end of its
+// species and its deposit (global atomics).
+__device__ __forceinline__ void place_product(const PushArgs& A, int s, float x, float y, float vx, float vy,
+                                              float vz) {
+    const SpeciesConst C = A.sp[s];
+    if (A.do_drift) {
+        const float x0 = x, y0 = y;
+        if (A.rz) {
+            drift_rz(x, y, vx, vy, vz, C.dtdx, C.dtdy);
+        } else {
+            x = __fmaf_rn(vx, C.dtdx, x);
+            y = __fmaf_rn(vy, C.dtdy, y);
+        }
+        if (!(x >= 0.0f && x <= float(A.nx - 1) && y >= 0.0f && y <= float(A.ny - 1))) return;
+        if (A.electrodes && hits_electrode(x0, y0, x, y, A.nx, A.ny, A.vbits, A.hbits)) return;
+    }
+    SpeciesState& S = A.state[s];
+    const int slot = atomicAdd(&S.count, 1);
+    if (slot >= S.capacity) {
+        atomicSub(&S.count, 1);
+        atomicAdd(A.ctr + kCtrDropped, 1ull);
+        return;
+    }
+    S.cur[0][slot] = x;
+    S.cur[1][slot] = y;
+    S.cur[2][slot] = vx;
+    S.cur[3][slot] = vy;
+    S.cur[4][slot] = vz;
+    atomicAdd(A.ctr + kCtrBorn + s, 1ull);
+    if (A.do_deposit) {
+        const Cic c = cic_weights(x, y, A.nx, A.ny);
+        atomicAdd(A.rho + long(c.j0) * A.nx + c.i0, __fmul_rn(C.scale, c.w00));
+        atomicAdd(A.rho + long(c.j0) * A.nx + c.i1, __fmul_rn(C.scale, c.w10));
+        atomicAdd(A.rho + long(c.j1) * A.nx + c.i0, __fmul_rn(C.scale, c.w01));
+        atomicAdd(A.rho + long(c.j1) * A.nx + c.i1, __fmul_rn(C.scale, c.w11));
+    }
+}
+
 // The collision candidates of the pass: MCC, then the drift, absorption and
-// deposit the pass skipped for them (global atomics; a few per thousand).
+// deposit the pass skipped for them (global atomics; a few per thousand), and
+// the ionisation products they create.
 __global__ void __launch_bounds__(128) k_collide(PushArgs A) {
     const int nc = min(*A.cand_count, A.cand_cap);
     const uint32_t step = *A.step;
@@ -1238,10 +1278,10 @@ __global__ void __launch_bounds__(128) k_collide(PushArgs A) {
         if (o.proc >= 0) {
             atomicAdd(A.ctr + kCtrCollisions + s * PIC_MAX_PROCESSES + o.proc, 1ull);
             if (o.born) {
+                // born at the parent's position before its drift
                 const MccSpeciesDev& M = A.mcc->sp[s];
-                const bool ok_e = birth_push(A.births, M.born_e, x, y, o.be[0], o.be[1], o.be[2]);
-                const bool ok_i = birth_push(A.births, M.born_i, x, y, o.bi[0], o.bi[1], o.bi[2]);
-                if (!ok_e || !ok_i) atomicAdd(A.ctr + kCtrDropped, 1ull);
+                place_product(A, M.born_e, x, y, o.be[0], o.be[1], o.be[2]);
+                place_product(A, M.born_i, x, y, o.bi[0], o.bi[1], o.bi[2]);
             }
         }
         if (A.do_drift) {
@@ -1277,55 +1317,10 @@ __global__ void __launch_bounds__(128) k_collide(PushArgs A) {
     }
 }
 
-// Ionisation products: drift, absorb and deposit them (global atomics) and
-// append them to their species.
-__global__ void k_merge_births(PushArgs A) {
-    const int nb = min(*A.births.count, A.births.capacity);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) {
-        const int s = A.births.species[i];
-        const SpeciesConst C = A.sp[s];
-        float x = A.births.x[i], y = A.births.y[i];
-        float vx = A.births.vx[i], vy = A.births.vy[i], vz = A.births.vz[i];
-        if (A.do_drift) {
-            const float x0 = x, y0 = y;
-            if (A.rz) {
-                drift_rz(x, y, vx, vy, vz, C.dtdx, C.dtdy);
-            } else {
-                x = __fmaf_rn(vx, C.dtdx, x);
-                y = __fmaf_rn(vy, C.dtdy, y);
-            }
-            // a product that leaves the domain or reaches an electrode in its
-            // first drift is never stored
-            if (!(x >= 0.0f && x <= float(A.nx - 1) && y >= 0.0f && y <= float(A.ny - 1))) continue;
-            if (A.electrodes && hits_electrode(x0, y0, x, y, A.nx, A.ny, A.vbits, A.hbits)) continue;
-        }
-        SpeciesState& S = A.state[s];
-        const int slot = atomicAdd(&S.count, 1);
-        if (slot >= S.capacity) {
-            atomicSub(&S.count, 1);
-            atomicAdd(A.ctr + kCtrDropped, 1ull);
-            continue;
-        }
-        S.cur[0][slot] = x;
-        S.cur[1][slot] = y;
-        S.cur[2][slot] = vx;
-        S.cur[3][slot] = vy;
-        S.cur[4][slot] = vz;
-        atomicAdd(A.ctr + kCtrBorn + s, 1ull);
-        if (A.do_deposit) {
-            const Cic c = cic_weights(x, y, A.nx, A.ny);
-            atomicAdd(A.rho + long(c.j0) * A.nx + c.i0, __fmul_rn(C.scale, c.w00));
-            atomicAdd(A.rho + long(c.j0) * A.nx + c.i1, __fmul_rn(C.scale, c.w10));
-            atomicAdd(A.rho + long(c.j1) * A.nx + c.i0, __fmul_rn(C.scale, c.w01));
-            atomicAdd(A.rho + long(c.j1) * A.nx + c.i1, __fmul_rn(C.scale, c.w11));
-        }
-    }
-}
-
 // Per step: untiled items for slots past the last sort, item counter reset,
-// RNG step advance, birth buffer reset.
+// RNG step advance, collision candidate list reset.
 __global__ void k_build_items(SpeciesState* state, int nspecies, const int* n_tiled, int4* items, int* n_items,
-                              int* item_next, uint32_t* step, int* birth_count, int* cand_count, int advance_step) {
+                              int* item_next, uint32_t* step, int* cand_count, int advance_step) {
     __shared__ int off[PIC_MAX_SPECIES + 1];
     if (threadIdx.x == 0) {
         int o = *n_tiled;
@@ -1337,7 +1332,6 @@ __global__ void k_build_items(SpeciesState* state, int nspecies, const int* n_ti
         off[nspecies] = o;
         *n_items = o;
         *item_next = 0;
-        *birth_count = 0;
         *cand_count = 0;
         if (advance_step) *step += 1u;
     }
@@ -1575,7 +1569,6 @@ struct SimImpl {
     int *n_items = nullptr, *item_next = nullptr, *n_tiled = nullptr;
     uint32_t* step_ctr = nullptr;
     int* tile_start = nullptr;
-    BirthDev births{};
     unsigned long long* ctr = nullptr;
     int* error = nullptr;
     unsigned long long wait_limit = kWaitLimit;  // polls of k_push's chunk waits
@@ -1711,7 +1704,6 @@ static PushArgs push_args(SimImpl& S, int kick, int mcc, int drift, int deposit,
     A.mcc = S.mcc_dev;
     A.key = make_uint2(uint32_t(S.d.seed), uint32_t(S.d.seed >> 32));
     A.step = S.step_ctr;
-    A.births = S.births;
     for (int s = 0; s < S.ns; ++s) A.cbits[s] = S.cbits[s];
     A.vbits = S.vbits;
     A.hbits = S.hbits;
@@ -1735,7 +1727,7 @@ static int prepare_pass(SimImpl& S, cudaStream_t st, int mcc, int advance_step) 
     {
         PhaseTimer t(S, PIC_PHASE_BUILD, st);
         k_build_items<<<1, 256, 0, st>>>(S.d_state, S.ns, S.n_tiled, S.items, S.n_items, S.item_next, S.step_ctr,
-                                         S.births.count, S.cand_count, advance_step);
+                                         S.cand_count, advance_step);
         if (mcc && S.have_mcc) {
             const uint2 key = make_uint2(uint32_t(S.d.seed), uint32_t(S.d.seed >> 32));
             k_mcc_bits<<<div_up(S.cbits_segments, 256), 256, 0, st>>>(S.mcc_dev, S.ns, S.step_ctr, key, S.d_cbits,
@@ -1797,20 +1789,16 @@ static int run_pass(SimImpl& S, cudaStream_t st, int kick, int mcc, int drift, i
     return run_pass_tail(S, st, A);
 }
 
-// What follows a particle pass: the collision candidates (k_collide) and the
-// ionisation products (k_merge_births).
+// What follows a particle pass with collisions: the collision candidates and
+// their ionisation products (k_collide).
 static int run_pass_tail(SimImpl& S, cudaStream_t st, const PushArgs& A) {
-    {
+    if (A.do_mcc) {
         PhaseTimer t(S, PIC_PHASE_MERGE, st);
-        if (A.do_mcc) {
-            // one thread per candidate: each is a long chain of dependent
-            // table lookups and Philox rounds
-            k_collide<<<4 * num_sms(), 128, 0, st>>>(A);
-            S.launches += 1;
-        }
-        k_merge_births<<<64, 256, 0, st>>>(A);
+        // one thread per candidate: each is a long chain of dependent
+        // table lookups and Philox rounds
+        k_collide<<<4 * num_sms(), 128, 0, st>>>(A);
+        S.launches += 1;
     }
-    S.launches += 1;
     PIC_LAUNCH_CHECK();
     return PIC_OK;
 }
@@ -1982,17 +1970,6 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
     PIC_TRY(dalloc(S, &S.n_tiled, 1));
     PIC_TRY(dalloc(S, &S.step_ctr, 1));
     PIC_TRY(dalloc(S, &S.tile_start, size_t(S.ns) * (S.sorter.ntiles + 1)));
-    // births
-    int bcap = 1 << 16;
-    for (int s = 0; s < S.ns; ++s) bcap = std::max(bcap, d->species[s].capacity / 64);
-    S.births.capacity = bcap;
-    PIC_TRY(dalloc(S, &S.births.x, size_t(bcap)));
-    PIC_TRY(dalloc(S, &S.births.y, size_t(bcap)));
-    PIC_TRY(dalloc(S, &S.births.vx, size_t(bcap)));
-    PIC_TRY(dalloc(S, &S.births.vy, size_t(bcap)));
-    PIC_TRY(dalloc(S, &S.births.vz, size_t(bcap)));
-    PIC_TRY(dalloc(S, &S.births.species, size_t(bcap)));
-    PIC_TRY(dalloc(S, &S.births.count, 1));
     // candidates per pass: P_null N on average (binomial); eight times the mean plus a margin
     double expect = 0.0;
     if (S.have_mcc)
@@ -2519,8 +2496,9 @@ int pic_sim_step(pic_sim* sim, int n_steps, void* stream) {
             }
             const bool sort_next = S.d.sort_interval > 0 && (S.steps + 1) % S.d.sort_interval == 0;
             PIC_CUDA(cudaGraphLaunch(sort_next ? S.g_sort_step : S.g_step, st));
+            // items and the pass (with collisions: candidate bits and k_collide), the RHS and E
             S.launches +=
-                3 + (S.have_mcc ? 2 : 0) + 2 + (sort_next ? 1 + (long long)S.ns * (5 + 3 * S.sorter.passes) : 0);
+                2 + (S.have_mcc ? 2 : 0) + 2 + (sort_next ? 1 + (long long)S.ns * (5 + 3 * S.sorter.passes) : 0);
             S.solves += 1;
             S.prepared = true;
         } else {
@@ -2878,10 +2856,10 @@ int pic_ens_step(pic_ens* e, int n_steps, void* stream) {
         long long sorts = 0;
         if (S->d.sort_interval > 0)
             for (long long k = S->steps; k < S->steps + n_steps; ++k) sorts += (k % S->d.sort_interval == 0);
-        // the step counter, the particle pass (3, plus the collisions), the RHS
-        // and E; a fused ensemble's one pass (and its item numbering) is
-        // counted with the first member
-        const long long pass = E.fused ? (S == E.m[0] ? 4 : 2) : 3;
+        // the step counter, the particle pass (items and the pass, plus the
+        // collisions), the RHS and E; a fused ensemble's one pass (and its item
+        // numbering) is counted with the first member
+        const long long pass = E.fused ? (S == E.m[0] ? 3 : 1) : 2;
         S->launches += n_steps * (1LL + pass + (S->have_mcc ? 2 : 0) + 2) +
                        sorts * (1 + (long long)S->ns * (5 + 3 * S->sorter.passes));
         if (S->d.sort_interval > 0) S->launches += n_steps;  // the sort condition
