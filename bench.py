@@ -80,6 +80,9 @@ def parse():
     ap.add_argument("--ensemble-steps", type=int, default=500)
     ap.add_argument("--ensemble-branches", action="store_true",
                     help="give every ensemble member's particle pass its own launch (not one pass over all)")
+    ap.add_argument("--large-step", action="store_true",
+                    help="also time the large workload as a PIC step: 2049^2 nodes, 64M + 64M particles, multigrid to "
+                         "1e-10, mixed precision against plain FP64, 200 steps")
     ap.add_argument("--adjoint", action="store_true",
                     help="also time the differentiable workload (forward, adjoint, finite-difference check)")
     ap.add_argument("--tune-cache", default=os.path.join(ROOT, "pic_b200", "tuned_b200.json"),
@@ -397,6 +400,8 @@ def run_ours(args, world, rank, local):
         out["poisson"] = run_poisson()
     if args.ensemble > 0 and rank == 0:
         out["ensemble"] = run_ensemble(args)
+    if args.large_step and rank == 0:
+        out["large_step"] = run_large_step()
     if args.adjoint and rank == 0:
         out["adjoint"] = run_adjoint()
     if not args.no_cpu_baseline and rank == 0 and world == 1:
@@ -483,6 +488,86 @@ def run_ensemble(args):
             "hbm": {"bytes_per_step": step_bytes, "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
                     "frac": round(gbs / peak, 4), "peak_source": kind,
                     "counts": "particle and grid bytes over the whole ensemble step (field solves included)"}}
+
+
+def large_species_on_device(w, which, gen):
+    """The large workload's particles, drawn on the device (seeded): ions
+    uniform; electrons half in a Gaussian blob (sigma 0.2 L, re-drawn until
+    inside the domain) and half uniform; Maxwellian velocities."""
+    import torch
+
+    from pic_b200 import Consts, workloads
+
+    n = w.n_e if which == "e" else w.n_i
+    top = float(w.nodes - 1)
+    hi = float(np.nextafter(np.float32(top), np.float32(0)))
+    x = torch.rand(n, generator=gen, device="cuda") * top
+    y = torch.rand(n, generator=gen, device="cuda") * top
+    if which == "e":
+        h = n // 2
+        c, sig = 0.5 * top, 0.2 * top
+        bx = torch.randn(h, generator=gen, device="cuda") * sig + c
+        by = torch.randn(h, generator=gen, device="cuda") * sig + c
+        for _ in range(64):
+            bad = (bx < 0) | (bx >= top) | (by < 0) | (by >= top)
+            k = int(bad.sum())
+            if k == 0:
+                break
+            bx[bad] = torch.randn(k, generator=gen, device="cuda") * sig + c
+            by[bad] = torch.randn(k, generator=gen, device="cuda") * sig + c
+        x[:h], y[:h] = bx, by
+    x.clamp_(0.0, hi)
+    y.clamp_(0.0, hi)
+    mass = Consts.me if which == "e" else workloads.ION_MASS
+    vth = float(np.sqrt((w.Te if which == "e" else w.Ti) * Consts.qe / mass))
+    v = [torch.randn(n, generator=gen, device="cuda") * vth for _ in range(3)]
+    return x, y, v[0], v[1], v[2]
+
+
+def run_large_step(steps=200):
+    """The large workload as a fused PIC step: 2049^2 nodes, 64M + 64M
+    particles, collisionless, multigrid to a 1e-10 relative residual every
+    step, the cell sort every 80 steps; once with the mixed-precision
+    multigrid and once with the plain FP64 one, on the same inputs."""
+    import torch
+
+    from pic_b200 import Consts, workloads
+    from pic_b200.simulation import PICSimulation
+
+    w = workloads.LARGE
+    mask, phi_bc = workloads.dirichlet(w)
+    species = [dict(name="e", charge=-Consts.qe, mass=Consts.me, np2c=w.np2c(w.n_e), capacity=int(w.n_e * 1.05)),
+               dict(name="i", charge=Consts.qe, mass=workloads.ION_MASS, np2c=w.np2c(w.n_i),
+                    capacity=int(w.n_i * 1.05))]
+    res = {"workload": "large: 2049x2049 nodes, 64M e- (half in a sigma=0.2L blob) + 64M ions, collisionless, "
+                       f"multigrid tol 1e-10 every step, sort every 80 steps, {steps} timed steps after 3"}
+    for prec in ("mixed", "fp64"):
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(7)
+        sim = PICSimulation(w.nodes, w.nodes, w.dx, w.dx, w.dt, species, mask, phi_bc, tol=w.tol, max_cycles=60,
+                            precision=prec, sort_interval=80, use_graph=True)
+        for s, which in enumerate(("e", "i")):
+            sim.load(s, *large_species_on_device(w, which, gen))
+        torch.cuda.empty_cache()
+        sim.init()
+        sim.step(3)
+        torch.cuda.synchronize()
+        n0 = sum(sim.counters()["count"])
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sim.step(steps)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        c = sim.counters()
+        res[prec] = {"ms_per_step": ms / steps, "value": 0.5 * (n0 + sum(c["count"])) * steps / (ms / 1e3),
+                     "unit": UNIT, "last_cycles": c["last_cycles"], "last_rel_res": c["last_rel_res"],
+                     "absorbed": c["absorbed"]}
+        sim.close()
+        del sim
+        torch.cuda.empty_cache()
+    res["speedup_mixed_vs_fp64"] = round(res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"], 3)
+    return res
 
 
 def run_adjoint():

@@ -314,3 +314,39 @@ def check_fields_loose_collided(sim, w, mask, full, collided, n_before):
             a[k][n:] = got[k][n:]
         fixed.append(a)
     check_fields(sim, w, mask, fixed, "step 2")
+
+
+def test_large_workload_grid_steps_against_oracle():
+    """The large workload's grid and tolerance (2049^2 nodes, the electrons half
+    in a Gaussian blob of sigma 0.2 L, multigrid to a 1e-10 relative residual),
+    as a fused PIC step with 4M + 4M particles (the particle passes do not
+    depend on the count; the bench times the full 64M + 64M): init and two
+    steps bit-exact against the oracle, phi's FP64 residual below 1e-10 every
+    time, rho within the deposit tolerance."""
+    w = workloads.scaled(workloads.LARGE, n=4_000_000)
+    assert (w.nodes, w.tol, w.blob) == (2049, 1e-10, True)
+    m = w.nodes
+    sim, arrays, mask, _ = build(w, 80, cap_factor=1.25)
+    kq = [np.float32(CHARGES[s] / MASSES[s] * w.dt) for s in range(2)]
+    dtdx = np.float32(w.dt / w.dx)
+    ref = [oracle_sort([a.copy() for a in sp], m) for sp in arrays]
+    assert sim.init() == 0
+    _, _, Ex0, Ey0 = check_fields(sim, w, mask, ref, "init")
+    for s in range(2):
+        O.kick_f32(ref[s][0], ref[s][1], ref[s][2], ref[s][3], Ex0, Ey0, np.float32(np.float64(kq[s]) * -0.5), m, m)
+    E_prev = None
+    absorbed = [0, 0]
+    for i in range(2):
+        assert sim.step(1) == 0
+        for s in range(2):
+            if i > 0:
+                O.kick_f32(ref[s][0], ref[s][1], ref[s][2], ref[s][3], E_prev[0], E_prev[1], kq[s], m, m)
+            absorbed[s] += O.drift_absorb_f32(ref[s][0], ref[s][1], ref[s][2], ref[s][3], dtdx, dtdx, m, m)
+        assert sim.counters()["absorbed"] == absorbed
+        for s in range(2):
+            got = host(sim, s)
+            for k in range(5):
+                assert_bits(got[k], ref[s][k], f"step {i + 1} species {s} array {k}")
+        _, _, Ex, Ey = check_fields(sim, w, mask, ref, f"step {i + 1}")
+        E_prev = (Ex, Ey)
+    sim.close()
