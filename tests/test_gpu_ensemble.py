@@ -97,3 +97,59 @@ def test_ensemble_rejects_eager_members_and_duplicates():
         ensemble.Ensemble([g, g])
     sim.close()
     g.close()
+
+
+def test_ensemble_with_collisions_matches_members_stepped_alone():
+    """Members with null-collision MCC (the MCC workload's tables, a denser gas
+    so that collisions and ionisation products occur every step) in the one
+    particle pass over all members, against the same members stepped alone.
+    The runs drift apart in the last bits (rho's global float atomics), and a
+    particle that then ends a step in another cell shifts the slots after the
+    next sort, and with them the Philox streams of the candidates: collision,
+    product and particle counts agree to within a few standard deviations, phi
+    and positions within the tolerances of the collisionless test."""
+    from pic_b200 import Consts
+    from pic_b200.simulation import PICSimulation
+
+    def make(i):
+        w = workloads.scaled(workloads.MCC, nodes=129 if i == 0 else 257, n=40_000 + 10_000 * i, gas_density=3e22,
+                             Te=8.0, seed=700 + i)
+        mask, phi_bc = workloads.dirichlet(w)
+        sp = [dict(name="e", charge=-Consts.qe, mass=Consts.me, np2c=w.np2c(w.n_e), capacity=2 * w.n_e),
+              dict(name="i", charge=Consts.qe, mass=workloads.ION_MASS, np2c=w.np2c(w.n_i), capacity=2 * w.n_i)]
+        sim = PICSimulation(w.nodes, w.nodes, w.dx, w.dx, w.dt, sp, mask, phi_bc, tol=w.tol, max_cycles=50,
+                            sort_interval=5, mcc=workloads.mcc_tables(w), seed=w.seed, use_graph=True)
+        for s, a in enumerate(ensemble.member_arrays(w)):
+            sim.load(s, *a)
+        sim.init()
+        return sim
+
+    together = [make(i) for i in range(2)]
+    alone = [make(i) for i in range(2)]
+    ens = ensemble.Ensemble(together)
+    assert ens.fused_pass
+    ens.step(12)
+    for sim in alone:
+        sim.step(12)
+    torch.cuda.synchronize()
+    for i, (a, b) in enumerate(zip(together, alone)):
+        ca, xa, pa = _state(a)
+        cb, xb, pb = _state(b)
+        assert sum(ca["collisions"][0]) > 0 and ca["born"][0] > 0, i
+        for s in range(2):
+            for k in range(4):
+                a_, b_ = ca["collisions"][s][k], cb["collisions"][s][k]
+                assert abs(a_ - b_) <= 3 * np.sqrt(b_) + 5, (i, s, k, a_, b_)
+            assert abs(ca["born"][s] - cb["born"][s]) <= 3 * np.sqrt(cb["born"][s]) + 5, i
+            assert abs(ca["count"][s] - cb["count"][s]) <= 3 * np.sqrt(cb["born"][s] + 1) + 5, i
+        scale = max(1.0, float(np.abs(pb).max()))
+        assert np.abs(pa - pb).max() <= 1e-4 * scale, i
+        for s in range(2):
+            # as multisets (a slot shift after a sort moves particles, not their positions)
+            ga, gb = np.sort(xa[s][np.isfinite(xa[s])]), np.sort(xb[s][np.isfinite(xb[s])])
+            n = min(ga.size, gb.size)
+            close = np.abs(ga[:n] - gb[:n]) <= 1e-3
+            assert close.mean() >= 0.99, (i, s, close.mean())
+    ens.close()
+    for sim in together + alone:
+        sim.close()
