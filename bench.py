@@ -12,7 +12,12 @@ steps with the state resident in HBM (particle arrays 8M x 20 B = 160 MB,
 larger than the 126 MB L2).  `e2e` times the public API from pinned host
 arrays: load, init, K steps, read back particles and phi.  `poisson` times
 the large workload's solve (2049^2, 64M + 64M particles, Gaussian blob) to a
-1e-10 relative residual, mixed precision against plain FP64.
+1e-10 relative residual, mixed precision against plain FP64.  On one GPU the
+line also carries the reference's other configurations: `large_step` (that
+workload as a PIC step for 200 steps, each multigrid), `ensemble` (64
+independent members of 129^2-513^2 nodes, 500 steps, one graph launch, one
+particle pass over all members per step) and `adjoint` (the differentiable
+257^2 workload: forward and backward cost, central finite differences).
 
 Multi-GPU (torchrun): independent replicas, one per GPU (the path does not
 shard); the time is the max over ranks and `value` sums all ranks' work.
@@ -75,16 +80,18 @@ def parse():
                     help="multigrid launch mode (host: one launch per kernel, for profilers; dst: the "
                          "sine-transform solve in place of the V-cycles; hybrid: the levels of at most 129^2 nodes "
                          "in one cluster launch per cycle)")
-    ap.add_argument("--ensemble", type=int, default=0,
-                    help="also time an ensemble of this many independent collisionless members (0: off)")
+    ap.add_argument("--ensemble", type=int, default=-1,
+                    help="also time an ensemble of this many independent collisionless members (0: off; default: "
+                         "64 on one GPU, off on several)")
     ap.add_argument("--ensemble-steps", type=int, default=500)
     ap.add_argument("--ensemble-branches", action="store_true",
                     help="give every ensemble member's particle pass its own launch (not one pass over all)")
-    ap.add_argument("--large-step", action="store_true",
-                    help="also time the large workload as a PIC step: 2049^2 nodes, 64M + 64M particles, multigrid to "
-                         "1e-10, mixed precision against plain FP64, 200 steps")
-    ap.add_argument("--adjoint", action="store_true",
-                    help="also time the differentiable workload (forward, adjoint, finite-difference check)")
+    ap.add_argument("--no-large-step", action="store_true",
+                    help="skip the large workload as a PIC step (2049^2 nodes, 64M + 64M particles, multigrid to "
+                         "1e-10, mixed precision against plain FP64, 200 steps; run on one GPU by default)")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the differentiable workload (forward, adjoint, finite-difference check; run on one GPU "
+                         "by default)")
     ap.add_argument("--tune-cache", default=os.path.join(ROOT, "pic_b200", "tuned_b200.json"),
                     help="autotuner results (read if present, written after tuning)")
     return ap.parse_args()
@@ -398,11 +405,14 @@ def run_ours(args, world, rank, local):
         out["e2e"] = run_e2e(w, arrays, args, world, rank)
     if not args.no_poisson and rank == 0:
         out["poisson"] = run_poisson()
-    if args.ensemble > 0 and rank == 0:
-        out["ensemble"] = run_ensemble(args)
-    if args.large_step and rank == 0:
+    # the other workloads of the reference's configuration list, on one GPU
+    # (a multi-GPU run times the replicated step only)
+    members = args.ensemble if args.ensemble >= 0 else (64 if world == 1 else 0)
+    if members > 0 and rank == 0:
+        out["ensemble"] = run_ensemble(args, members)
+    if not args.no_large_step and rank == 0 and world == 1:
         out["large_step"] = run_large_step()
-    if args.adjoint and rank == 0:
+    if not args.no_adjoint and rank == 0 and world == 1:
         out["adjoint"] = run_adjoint()
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         out["cpu_baseline"] = run_cpu_baseline(w, arrays, args.cpu_steps)
@@ -413,7 +423,7 @@ def run_ours(args, world, rank, local):
         dist.destroy_process_group()
 
 
-def run_ensemble(args):
+def run_ensemble(args, members):
     """Ensemble workload: members with grid sides from {129, 257, 513}, 1e5-2e6
     particles per species, Te 1-5 eV, left wall 0-200 V, collisionless; each
     member shape tuned by the autotuner; all members stepped by one graph
@@ -422,7 +432,7 @@ def run_ensemble(args):
 
     from pic_b200 import autotune, ensemble
 
-    ws = ensemble.ensemble_workloads(args.ensemble)
+    ws = ensemble.ensemble_workloads(members)
     tuner = autotune.Autotuner(cache_path=args.tune_cache)
     t0 = time.time()
     choices = tuner.tune_ensemble(ws)
