@@ -103,11 +103,13 @@ def test_ensemble_with_collisions_matches_members_stepped_alone():
     """Members with null-collision MCC (the MCC workload's tables, a denser gas
     so that collisions and ionisation products occur every step) in the one
     particle pass over all members, against the same members stepped alone.
-    The runs drift apart in the last bits (rho's global float atomics), and a
-    particle that then ends a step in another cell shifts the slots after the
-    next sort, and with them the Philox streams of the candidates: collision,
-    product and particle counts agree to within a few standard deviations, phi
-    and positions within the tolerances of the collisionless test."""
+    After two steps (one of them with collisions) the two are identical.  Then
+    the runs drift apart in the last bits (rho's global float atomics: the
+    candidates' and products' deposits), and a particle that ends a step in
+    another cell shifts the slots after the next sort, and with them the
+    Philox streams of the candidates: after twelve steps collision, product and
+    particle counts agree to within a few standard deviations, phi to 1e-3 of
+    its largest value and the positions as multisets to 1e-3 cells."""
     from pic_b200 import Consts
     from pic_b200.simulation import PICSimulation
 
@@ -128,9 +130,26 @@ def test_ensemble_with_collisions_matches_members_stepped_alone():
     alone = [make(i) for i in range(2)]
     ens = ensemble.Ensemble(together)
     assert ens.fused_pass
-    ens.step(12)
+    # two steps (the second kicks and collides, no sort between them): the
+    # same candidates and collisions, the particles that were there before
+    # bit for bit (the products' slots follow atomic order)
+    ens.step(2)
     for sim in alone:
-        sim.step(12)
+        sim.step(2)
+    torch.cuda.synchronize()
+    for i, (a, b) in enumerate(zip(together, alone)):
+        ca, cb = a.counters(), b.counters()
+        assert ca["collisions"] == cb["collisions"] and ca["born"] == cb["born"], i
+        assert ca["count"] == cb["count"] and ca["absorbed"] == cb["absorbed"], i
+        for s in range(2):
+            n = ca["count"][s] - ca["born"][s]
+            for k in range(5):
+                ga = a.species_arrays(s)[k][:n].cpu().numpy()
+                gb = b.species_arrays(s)[k][:n].cpu().numpy()
+                np.testing.assert_array_equal(ga.view(np.uint32), gb.view(np.uint32))
+    ens.step(10)
+    for sim in alone:
+        sim.step(10)
     torch.cuda.synchronize()
     for i, (a, b) in enumerate(zip(together, alone)):
         ca, xa, pa = _state(a)
@@ -142,8 +161,10 @@ def test_ensemble_with_collisions_matches_members_stepped_alone():
                 assert abs(a_ - b_) <= 3 * np.sqrt(b_) + 5, (i, s, k, a_, b_)
             assert abs(ca["born"][s] - cb["born"][s]) <= 3 * np.sqrt(cb["born"][s]) + 5, i
             assert abs(ca["count"][s] - cb["count"][s]) <= 3 * np.sqrt(cb["born"][s] + 1) + 5, i
+        # collided particles that differ between the runs change phi by a few
+        # particles' fields
         scale = max(1.0, float(np.abs(pb).max()))
-        assert np.abs(pa - pb).max() <= 1e-4 * scale, i
+        assert np.abs(pa - pb).max() <= 1e-3 * scale, i
         for s in range(2):
             # as multisets (a slot shift after a sort moves particles, not their positions)
             ga, gb = np.sort(xa[s][np.isfinite(xa[s])]), np.sort(xb[s][np.isfinite(xb[s])])
