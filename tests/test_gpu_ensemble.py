@@ -103,7 +103,8 @@ def test_ensemble_with_collisions_matches_members_stepped_alone():
     """Members with null-collision MCC (the MCC workload's tables, a denser gas
     so that collisions and ionisation products occur every step) in the one
     particle pass over all members, against the same members stepped alone.
-    After two steps (one of them with collisions) the two are identical.  Then
+    After two steps (one of them with collisions) the two agree to FP32
+    rounding, with the same candidates and collisions.  Then
     the runs drift apart in the last bits (rho's global float atomics: the
     candidates' and products' deposits), and a particle that ends a step in
     another cell shifts the slots after the next sort, and with them the
@@ -132,7 +133,9 @@ def test_ensemble_with_collisions_matches_members_stepped_alone():
     assert ens.fused_pass
     # two steps (the second kicks and collides, no sort between them): the
     # same candidates and collisions, the particles that were there before
-    # bit for bit (the products' slots follow atomic order)
+    # equal to FP32 rounding (the products' slots follow atomic order; the
+    # charge tiles' flush adds floats in atomic order, so E, and the kick, may
+    # differ in a last bit between any two runs)
     ens.step(2)
     for sim in alone:
         sim.step(2)
@@ -146,7 +149,7 @@ def test_ensemble_with_collisions_matches_members_stepped_alone():
             for k in range(5):
                 ga = a.species_arrays(s)[k][:n].cpu().numpy()
                 gb = b.species_arrays(s)[k][:n].cpu().numpy()
-                np.testing.assert_array_equal(ga.view(np.uint32), gb.view(np.uint32))
+                np.testing.assert_allclose(ga, gb, rtol=1e-6, atol=0, equal_nan=True)
     ens.step(10)
     for sim in alone:
         sim.step(10)
