@@ -658,11 +658,22 @@ def run_e2e(w, arrays, args, world, rank):
     pinned = [[torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in sp] for sp in arrays]
     sim = make_sim(w, rank, args.sort_interval, mcc=True)
     # read-back buffers (pinned, allocated before the timed region like the
-    # inputs): rows x, y, vx, vy, vz of each species, one copy per species
+    # inputs): rows x, y, vx, vy, vz of each species, one copy per array
     cap = [int(len(sp[0]) * 1.25) for sp in arrays]
     host_out = [torch.empty(5 * c, dtype=torch.float32).pin_memory() for c in cap]
     host_phi = torch.empty(w.nodes * w.nodes, dtype=torch.float64).pin_memory()
     stream = torch.cuda.current_stream()
+    # one untimed pass of the same calls first (args.warmup steps): the first
+    # copies into freshly pinned pages, the field views and the step's graph
+    # capture are one-time costs of a process, not of a run
+    for s, a in enumerate(pinned):
+        sim.load(s, *a)
+    sim.init()
+    sim.step(max(1, args.warmup))
+    sim.sync()
+    for s in range(2):
+        sim.read_particles(s, host_out[s])
+    host_phi.copy_(sim.fields()[0], non_blocking=True)
     outs = None
     if world > 1:
         dist.barrier()
@@ -696,7 +707,8 @@ def run_e2e(w, arrays, args, world, rank):
             "read_gbs": round(d2h / (phases["read"] / 1e3) / 1e9, 1) if phases["read"] > 0 else None,
             "load_gbs": round(h2d / (phases["load"] / 1e3) / 1e9, 1) if phases["load"] > 0 else None,
             "includes": "H2D of all particles from pinned host memory, init, "
-                        f"{args.steps} steps, D2H of particles (one copy per species) and phi into pinned host memory"}
+                        f"{args.steps} steps, D2H of particles (one copy per array) and phi into pinned host memory; "
+                        "after one untimed pass of the same calls"}
 
 
 def mg_levels(n, coarse_max=33):

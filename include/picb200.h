@@ -419,8 +419,8 @@ int pic_sim_species_arrays(pic_sim* sim, int s, float** x, float** y, float** vx
 /* The reference's R / V read back to the host (src/Particles.py:283-326 keeps
  * them as device arrays the caller copies): the slots in use of species s as
  * five consecutive rows x, y, vx, vy, vz of *count floats each in h_out
- * (page-locked memory for an asynchronous copy), in one device-to-host copy
- * on `stream`.  *count (the slots in use, dead ones included) is read first,
+ * (page-locked memory for an asynchronous copy), by device-to-host copies on
+ * `stream`.  *count (the slots in use, dead ones included) is read first,
  * synchronously.  PIC_ERR_OUT_OF_CAPACITY if 5 * count > capacity. */
 int pic_sim_read_particles(pic_sim* sim, int s, float* h_out, long long capacity, int* count, void* stream);
 /* The cell sort of every species, now (the sort a step runs every

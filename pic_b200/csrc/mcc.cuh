@@ -52,17 +52,39 @@ struct BirthDev {
     int capacity;
 };
 
-__device__ __forceinline__ float mcc_sigma(const MccDev& M, const float* __restrict__ S, float e) {
+// Where energy e falls on the shared log-spaced energy grid: below the first
+// point (lo), past the last (hi), or in bin j at fraction t.  Every process's
+// cross section is read at the same place, so a candidate locates it once.
+struct MccBin {
+    int j;
+    float t;
+    bool lo, hi;
+};
+
+__device__ __forceinline__ MccBin mcc_bin(const MccDev& M, float e) {
     const float* __restrict__ E = M.energy;
     const int ne = M.ne;
-    if (e <= E[0]) return S[0];
-    if (e >= E[ne - 1]) return S[ne - 1];
+    MccBin b;
+    b.j = 0;
+    b.t = 0.0f;
+    b.lo = e <= E[0];
+    b.hi = !b.lo && e >= E[ne - 1];
+    if (b.lo || b.hi) return b;
     int j = int(__fmul_rn(__fsub_rn(logf(e), M.log_e0), M.inv_log_ratio));
     j = max(0, min(j, ne - 2));
     while (j > 0 && e < E[j]) --j;
     while (j < ne - 2 && e >= E[j + 1]) ++j;
-    const float t = __fdiv_rn(__fsub_rn(e, E[j]), __fsub_rn(E[j + 1], E[j]));
-    return __fmaf_rn(t, __fsub_rn(S[j + 1], S[j]), S[j]);
+    b.j = j;
+    b.t = __fdiv_rn(__fsub_rn(e, E[j]), __fsub_rn(E[j + 1], E[j]));
+    return b;
+}
+
+// Cross section S (one row of the table) at the located energy: clamped to the
+// end values outside the grid, linear inside.
+__device__ __forceinline__ float mcc_sigma(const MccDev& M, const float* __restrict__ S, const MccBin& b) {
+    if (b.lo) return S[0];
+    if (b.hi) return S[M.ne - 1];
+    return __fmaf_rn(b.t, __fsub_rn(S[b.j + 1], S[b.j]), S[b.j]);
 }
 
 __device__ __forceinline__ void mcc_isotropic(float u_cos, float u_phi, float& dx, float& dy, float& dz) {
@@ -127,10 +149,11 @@ __device__ __forceinline__ MccOutcome mcc_collide(const MccDev& M, const MccSpec
     const float speed = __fsqrt_rn(v2);
     const float e = __fmul_rn(S.half_m_over_q, v2);
     const float target = __fmul_rn(u01_float(r0.x), S.nu_max);
+    const MccBin bin = mcc_bin(M, e);
     float acc = 0.0f;
     int proc = -1;
     for (int k = 0; k < S.nproc; ++k) {
-        const float sig = mcc_sigma(M, S.sigma + long(k) * M.ne, e);
+        const float sig = mcc_sigma(M, S.sigma + long(k) * M.ne, bin);
         acc = __fadd_rn(acc, __fmul_rn(__fmul_rn(M.gas_density, sig), speed));
         if (target < acc) {
             proc = k;

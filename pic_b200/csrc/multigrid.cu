@@ -604,7 +604,7 @@ template <class T, int S>
 __device__ void up2_tile(const LevelDev<T>& F, const LevelDev<T>& C, const LevelDev<T>& C2, T omega, int tx, int ty,
                          unsigned char* smem) {
     using G = Up2Geom<S>;
-    constexpr int WF = G::WF, HF = G::HF, CWF = G::CWF, WC = G::WC, CWC = G::CWC;
+    constexpr int WF = G::WF, HF = G::HF, WC = G::WC, CWC = G::CWC;
     T* seF = reinterpret_cast<T*>(smem);
     T* sgF = seF + WF * WF;
     T* seC = sgF + WF * WF;

@@ -15,10 +15,12 @@
 // particles and flushes the charge tile once with global atomics.  Particles
 // that left the staged region since the last sort gather from and deposit to
 // global memory directly.  Particles born since the last sort are processed
-// as untiled items.  Two streaming schemes, bit-identical in their results:
-// k_push_warp (the default) gives every warp its own pipeline of bulk copies
-// and deposits with warp-aggregated atomics; k_push streams chunks through
-// one ring per block.
+// as untiled items.  Null-collision candidates are kicked in the pass and
+// listed with their kicked state; k_collide finishes them (collision,
+// products, drift, deposit) after the pass.  k_push, one ring of bulk copies
+// per block, is the default (the fastest measured); three more streaming
+// schemes with the same per-particle arithmetic are kept as options
+// (k_push_pipe, k_push_warp with and without warp-aggregated deposits).
 #include <algorithm>
 #include <climits>
 #include <cmath>
@@ -107,7 +109,8 @@ struct alignas(64) PushArgs {
     const unsigned *vbits, *hbits;           // internal electrode edges (hits_electrode), when `electrodes`
     int electrodes;
     int rz;           // r-z geometry: drift_rz (y radial, vz azimuthal)
-    int2* cand;       // collision candidates (species, slot), processed by k_collide after the pass
+    int2* cand;          // collision candidates (species, slot), finished by k_collide after the pass
+    float4* cand_state;  // their kicked (x, y, vx, vy)
     int* cand_count;
     int cand_cap;
     unsigned long long* ctr;
@@ -187,7 +190,7 @@ __device__ __forceinline__ void issue_chunk(const PushArgs& A, const ChunkDesc& 
                                             unsigned long long* bar) {
     const int a0 = c.b & ~3, a1 = (c.e + 3) & ~3;
     const unsigned bytes = unsigned(a1 - a0) * 4u;
-    // x, y, vx, vy: vz is touched only by collision candidates (k_collide)
+    // x, y, vx, vy: vz is touched only by collision candidates (finish_candidate)
     mbar_expect_tx(bar, 4u * bytes);
     const SpeciesState& S = member<ENS>(A, chunk_member<ENS>(c.s)).state[chunk_species<ENS>(c.s)];
 #pragma unroll
@@ -317,6 +320,99 @@ __device__ __forceinline__ void store_chunk_edges(const PushArgs& A, const Chunk
     member<ENS>(A, chunk_member<ENS>(c.s)).state[chunk_species<ENS>(c.s)].cur[k][slot] = buf[k * kBufStride + (slot - a0)];
 }
 
+// An ionisation product of this step's collisions, born at (x, y): its first
+// drift with its own velocity, then, unless that takes it out of the domain
+// or onto an electrode (it is then never stored), its slot at the end of its
+// species and its deposit (global atomics).
+__device__ __forceinline__ void place_product(const PushArgs& A, int s, float x, float y, float vx, float vy,
+                                              float vz) {
+    const SpeciesConst C = A.sp[s];
+    if (A.do_drift) {
+        const float x0 = x, y0 = y;
+        if (A.rz) {
+            drift_rz(x, y, vx, vy, vz, C.dtdx, C.dtdy);
+        } else {
+            x = __fmaf_rn(vx, C.dtdx, x);
+            y = __fmaf_rn(vy, C.dtdy, y);
+        }
+        if (!(x >= 0.0f && x <= float(A.nx - 1) && y >= 0.0f && y <= float(A.ny - 1))) return;
+        if (A.electrodes && hits_electrode(x0, y0, x, y, A.nx, A.ny, A.vbits, A.hbits)) return;
+    }
+    SpeciesState& S = A.state[s];
+    const int slot = atomicAdd(&S.count, 1);
+    if (slot >= S.capacity) {
+        atomicSub(&S.count, 1);
+        atomicAdd(A.ctr + kCtrDropped, 1ull);
+        return;
+    }
+    S.cur[0][slot] = x;
+    S.cur[1][slot] = y;
+    S.cur[2][slot] = vx;
+    S.cur[3][slot] = vy;
+    S.cur[4][slot] = vz;
+    atomicAdd(A.ctr + kCtrBorn + s, 1ull);
+    if (A.do_deposit) {
+        const Cic c = cic_weights(x, y, A.nx, A.ny);
+        atomicAdd(A.rho + long(c.j0) * A.nx + c.i0, __fmul_rn(C.scale, c.w00));
+        atomicAdd(A.rho + long(c.j0) * A.nx + c.i1, __fmul_rn(C.scale, c.w10));
+        atomicAdd(A.rho + long(c.j1) * A.nx + c.i0, __fmul_rn(C.scale, c.w01));
+        atomicAdd(A.rho + long(c.j1) * A.nx + c.i1, __fmul_rn(C.scale, c.w11));
+    }
+}
+
+// The rest of a collision candidate's step, which the particle pass leaves
+// after its kick: the null-collision test and scattering (mcc_collide), the
+// ionisation products, then the drift, absorption and deposit (global
+// atomics; a few candidates per thousand particles).  (x, y, vx, vy) is the
+// kicked state; vz is read from the slot, which the pass does not touch.
+__device__ __forceinline__ void finish_candidate(const PushArgs& A, uint32_t step, int s, int p, float x, float y,
+                                                 float vx, float vy) {
+    const SpeciesState& S = A.state[s];
+    const SpeciesConst C = A.sp[s];
+    float vz = S.cur[4][p];
+    const MccOutcome o = mcc_collide(*A.mcc, A.mcc->sp[s], uint32_t(s), uint32_t(p), step, A.key, vx, vy, vz);
+    if (o.overflow) atomicAdd(A.ctr + kCtrOverflow, 1ull);
+    if (o.proc >= 0) {
+        atomicAdd(A.ctr + kCtrCollisions + s * PIC_MAX_PROCESSES + o.proc, 1ull);
+        if (o.born) {
+            // born at the parent's position before its drift
+            const MccSpeciesDev& M = A.mcc->sp[s];
+            place_product(A, M.born_e, x, y, o.be[0], o.be[1], o.be[2]);
+            place_product(A, M.born_i, x, y, o.bi[0], o.bi[1], o.bi[2]);
+        }
+    }
+    if (A.do_drift) {
+        const float x0 = x, y0 = y;
+        if (A.rz) {
+            drift_rz(x, y, vx, vy, vz, C.dtdx, C.dtdy);
+        } else {
+            x = __fmaf_rn(vx, C.dtdx, x);
+            y = __fmaf_rn(vy, C.dtdy, y);
+        }
+        if (!(x >= 0.0f && x <= float(A.nx - 1) && y >= 0.0f && y <= float(A.ny - 1))) {
+            x = __int_as_float(0x7fc00000);
+            y = x;
+            atomicAdd(A.ctr + kCtrAbsorbed + s, 1ull);
+        } else if (A.electrodes && hits_electrode(x0, y0, x, y, A.nx, A.ny, A.vbits, A.hbits)) {
+            x = __int_as_float(0x7fc00000);
+            y = x;
+            atomicAdd(A.ctr + kCtrElectrode + s, 1ull);
+        }
+    }
+    S.cur[0][p] = x;
+    S.cur[1][p] = y;
+    S.cur[2][p] = vx;
+    S.cur[3][p] = vy;
+    S.cur[4][p] = vz;
+    if (A.do_deposit && is_live(x)) {
+        const Cic w = cic_weights(x, y, A.nx, A.ny);
+        atomicAdd(A.rho + long(w.j0) * A.nx + w.i0, __fmul_rn(C.scale, w.w00));
+        atomicAdd(A.rho + long(w.j0) * A.nx + w.i1, __fmul_rn(C.scale, w.w10));
+        atomicAdd(A.rho + long(w.j1) * A.nx + w.i0, __fmul_rn(C.scale, w.w01));
+        atomicAdd(A.rho + long(w.j1) * A.nx + w.i1, __fmul_rn(C.scale, w.w11));
+    }
+}
+
 constexpr int kStages = 3;  // chunk buffers: one loading, one in work, one draining to global memory
 
 // Work units (species, tile, slot range) are claimed from an atomic counter
@@ -343,6 +439,9 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
     __shared__ ChunkDesc s_ch[kStages];
     __shared__ unsigned s_abs, s_cand, s_elec;
     const int tid = threadIdx.x;
+    // k_collide (launched as this pass's programmatic dependent) is placed as
+    // this grid's blocks retire, and waits for the whole pass
+    pdl_trigger();
     const int n_items = *A.n_items;
     if (tid == 0) {
         for (int k = 0; k < kStages; ++k) mbar_init(&bar[k], 1);
@@ -458,8 +557,7 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
                 const int slot = atomicAdd(M.cand_count, 1);
                 if (slot < M.cand_cap) {
                     M.cand[slot] = make_int2(s, b + l);
-                    pvx[l] = vx;
-                    pvy[l] = vy;
+                    M.cand_state[slot] = make_float4(x, y, vx, vy);
                     continue;
                 }
                 atomicAdd(M.ctr + kCtrCandOverflow, 1ull);
@@ -771,8 +869,7 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push_pipe(PushArgs A) {
                 const int slot = atomicAdd(A.cand_count, 1);
                 if (slot < A.cand_cap) {
                     A.cand[slot] = make_int2(s, b + l);
-                    pvx[l] = vx;
-                    pvy[l] = vy;
+                    A.cand_state[slot] = make_float4(x, y, vx, vy);
                     continue;
                 }
                 atomicAdd(A.ctr + kCtrCandOverflow, 1ull);
@@ -1088,6 +1185,7 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push_warp(const __grid_cons
                         const int slot = atomicAdd(A.cand_count, 1);
                         if (slot < A.cand_cap) {
                             A.cand[slot] = make_int2(s, p);
+                            A.cand_state[slot] = make_float4(x, y, vx, vy);
                         } else {
                             atomicAdd(A.ctr + kCtrCandOverflow, 1ull);
                             candidate = false;
@@ -1220,100 +1318,17 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push_warp(const __grid_cons
             if (epend & (1u << b)) mbar_wait(&ebars[b], (ephase >> b) & 1u, kWaitLimit);
 }
 
-// An ionisation product of this step's collisions, born at (x, y): its first
-// drift with its own velocity, then, unless that takes it out of the domain
-// or onto an electrode (it is then never stored), its slot at the end of its
-// species and its deposit (global atomics).
-__device__ __forceinline__ void place_product(const PushArgs& A, int s, float x, float y, float vx, float vy,
-                                              float vz) {
-    const SpeciesConst C = A.sp[s];
-    if (A.do_drift) {
-        const float x0 = x, y0 = y;
-        if (A.rz) {
-            drift_rz(x, y, vx, vy, vz, C.dtdx, C.dtdy);
-        } else {
-            x = __fmaf_rn(vx, C.dtdx, x);
-            y = __fmaf_rn(vy, C.dtdy, y);
-        }
-        if (!(x >= 0.0f && x <= float(A.nx - 1) && y >= 0.0f && y <= float(A.ny - 1))) return;
-        if (A.electrodes && hits_electrode(x0, y0, x, y, A.nx, A.ny, A.vbits, A.hbits)) return;
-    }
-    SpeciesState& S = A.state[s];
-    const int slot = atomicAdd(&S.count, 1);
-    if (slot >= S.capacity) {
-        atomicSub(&S.count, 1);
-        atomicAdd(A.ctr + kCtrDropped, 1ull);
-        return;
-    }
-    S.cur[0][slot] = x;
-    S.cur[1][slot] = y;
-    S.cur[2][slot] = vx;
-    S.cur[3][slot] = vy;
-    S.cur[4][slot] = vz;
-    atomicAdd(A.ctr + kCtrBorn + s, 1ull);
-    if (A.do_deposit) {
-        const Cic c = cic_weights(x, y, A.nx, A.ny);
-        atomicAdd(A.rho + long(c.j0) * A.nx + c.i0, __fmul_rn(C.scale, c.w00));
-        atomicAdd(A.rho + long(c.j0) * A.nx + c.i1, __fmul_rn(C.scale, c.w10));
-        atomicAdd(A.rho + long(c.j1) * A.nx + c.i0, __fmul_rn(C.scale, c.w01));
-        atomicAdd(A.rho + long(c.j1) * A.nx + c.i1, __fmul_rn(C.scale, c.w11));
-    }
-}
-
-// The collision candidates of the pass: MCC, then the drift, absorption and
-// deposit the pass skipped for them (global atomics; a few per thousand), and
-// the ionisation products they create.
+// The collision candidates of the pass, one thread each, with their kicked
+// state from the list.  Launched as the pass's programmatic dependent: the
+// blocks are placed while the pass ends and wait for its completion.
 __global__ void __launch_bounds__(128) k_collide(PushArgs A) {
+    pdl_wait();
     const int nc = min(*A.cand_count, A.cand_cap);
     const uint32_t step = *A.step;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nc; i += gridDim.x * blockDim.x) {
         const int2 c = A.cand[i];
-        const int s = c.x, p = c.y;
-        const SpeciesState& S = A.state[s];
-        const SpeciesConst C = A.sp[s];
-        float x = S.cur[0][p], y = S.cur[1][p];
-        float vx = S.cur[2][p], vy = S.cur[3][p], vz = S.cur[4][p];
-        const MccOutcome o = mcc_collide(*A.mcc, A.mcc->sp[s], uint32_t(s), uint32_t(p), step, A.key, vx, vy, vz);
-        if (o.overflow) atomicAdd(A.ctr + kCtrOverflow, 1ull);
-        if (o.proc >= 0) {
-            atomicAdd(A.ctr + kCtrCollisions + s * PIC_MAX_PROCESSES + o.proc, 1ull);
-            if (o.born) {
-                // born at the parent's position before its drift
-                const MccSpeciesDev& M = A.mcc->sp[s];
-                place_product(A, M.born_e, x, y, o.be[0], o.be[1], o.be[2]);
-                place_product(A, M.born_i, x, y, o.bi[0], o.bi[1], o.bi[2]);
-            }
-        }
-        if (A.do_drift) {
-            const float x0 = x, y0 = y;
-            if (A.rz) {
-                drift_rz(x, y, vx, vy, vz, C.dtdx, C.dtdy);
-            } else {
-                x = __fmaf_rn(vx, C.dtdx, x);
-                y = __fmaf_rn(vy, C.dtdy, y);
-            }
-            if (!(x >= 0.0f && x <= float(A.nx - 1) && y >= 0.0f && y <= float(A.ny - 1))) {
-                x = __int_as_float(0x7fc00000);
-                y = x;
-                atomicAdd(A.ctr + kCtrAbsorbed + s, 1ull);
-            } else if (A.electrodes && hits_electrode(x0, y0, x, y, A.nx, A.ny, A.vbits, A.hbits)) {
-                x = __int_as_float(0x7fc00000);
-                y = x;
-                atomicAdd(A.ctr + kCtrElectrode + s, 1ull);
-            }
-        }
-        S.cur[0][p] = x;
-        S.cur[1][p] = y;
-        S.cur[2][p] = vx;
-        S.cur[3][p] = vy;
-        S.cur[4][p] = vz;
-        if (A.do_deposit && is_live(x)) {
-            const Cic w = cic_weights(x, y, A.nx, A.ny);
-            atomicAdd(A.rho + long(w.j0) * A.nx + w.i0, __fmul_rn(C.scale, w.w00));
-            atomicAdd(A.rho + long(w.j0) * A.nx + w.i1, __fmul_rn(C.scale, w.w10));
-            atomicAdd(A.rho + long(w.j1) * A.nx + w.i0, __fmul_rn(C.scale, w.w01));
-            atomicAdd(A.rho + long(w.j1) * A.nx + w.i1, __fmul_rn(C.scale, w.w11));
-        }
+        const float4 v = A.cand_state[i];
+        finish_candidate(A, step, c.x, c.y, v.x, v.y, v.z, v.w);
     }
 }
 
@@ -1558,6 +1573,7 @@ struct SimImpl {
     int* d_nseg = nullptr;                // 256-slot segments per species (0: no collisions)
     int cbits_segments = 0;               // sum of d_nseg
     int2* cand = nullptr;       // collision candidates of one pass
+    float4* cand_state = nullptr;  // their kicked state
     int* cand_count = nullptr;
     int cand_cap = 0;
     std::vector<void*> allocs;
@@ -1710,6 +1726,7 @@ static PushArgs push_args(SimImpl& S, int kick, int mcc, int drift, int deposit,
     A.electrodes = S.electrodes ? 1 : 0;
     A.rz = S.rz ? 1 : 0;
     A.cand = S.cand;
+    A.cand_state = S.cand_state;
     A.cand_count = S.cand_count;
     A.cand_cap = S.cand_cap;
     A.ctr = S.ctr;
@@ -1796,7 +1813,7 @@ static int run_pass_tail(SimImpl& S, cudaStream_t st, const PushArgs& A) {
         PhaseTimer t(S, PIC_PHASE_MERGE, st);
         // one thread per candidate: each is a long chain of dependent
         // table lookups and Philox rounds
-        k_collide<<<4 * num_sms(), 128, 0, st>>>(A);
+        PIC_CUDA(launch_pdl(k_collide, dim3(4 * num_sms()), dim3(128), 0, st, A));
         S.launches += 1;
     }
     PIC_LAUNCH_CHECK();
@@ -1976,6 +1993,7 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
         for (int s = 0; s < S.ns; ++s) expect += S.mcc.p_null[s] * d->species[s].capacity;
     S.cand_cap = int(std::min(2.0e9, 8.0 * expect + 65536.0));
     PIC_TRY(dalloc(S, &S.cand, size_t(S.cand_cap)));
+    PIC_TRY(dalloc(S, &S.cand_state, size_t(S.cand_cap)));
     // candidate bit masks, one bit per slot of every colliding species
     {
         int nseg[PIC_MAX_SPECIES] = {};
@@ -2557,10 +2575,10 @@ int pic_sim_read_particles(pic_sim* sim, int s, float* h_out, long long capacity
         return fail(PIC_ERR_OUT_OF_CAPACITY, "pic_sim_read_particles: %d slots need %lld floats, capacity %lld",
                     H.count, 5LL * H.count, capacity);
     if (H.count == 0) return PIC_OK;
-    // the five arrays share one allocation at a fixed stride: one 2D copy
+    // one contiguous copy per array
     const size_t w = sizeof(float) * size_t(H.count);
-    PIC_CUDA(cudaMemcpy2DAsync(h_out, w, H.cur[0], sizeof(float) * size_t(H.stride), w, 5, cudaMemcpyDeviceToHost,
-                               st));
+    for (int c = 0; c < 5; ++c)
+        PIC_CUDA(cudaMemcpyAsync(h_out + size_t(c) * H.count, H.cur[c], w, cudaMemcpyDeviceToHost, st));
     return PIC_OK;
 }
 

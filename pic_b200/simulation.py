@@ -218,8 +218,8 @@ class PICSimulation:
     def read_particles(self, s, out):
         """Copies the slots in use of species s to the host tensor `out`
         (float32, page-locked for an asynchronous copy, at least 5 * count
-        values) as rows x, y, vx, vy, vz, in one copy on the current stream;
-        returns the (5, count) view of `out`."""
+        values) as rows x, y, vx, vy, vz, one copy per array on the current
+        stream; returns the (5, count) view of `out`."""
         n = C.c_int()
         _lib.call("pic_sim_read_particles", self._h, s, out.data_ptr(), out.numel(), C.byref(n), _lib.stream_ptr())
         return out[: 5 * n.value].view(5, n.value)
