@@ -439,9 +439,6 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
     __shared__ ChunkDesc s_ch[kStages];
     __shared__ unsigned s_abs, s_cand, s_elec;
     const int tid = threadIdx.x;
-    // k_collide (launched as this pass's programmatic dependent) is placed as
-    // this grid's blocks retire, and waits for the whole pass
-    pdl_trigger();
     const int n_items = *A.n_items;
     if (tid == 0) {
         for (int k = 0; k < kStages; ++k) mbar_init(&bar[k], 1);
@@ -1319,10 +1316,8 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push_warp(const __grid_cons
 }
 
 // The collision candidates of the pass, one thread each, with their kicked
-// state from the list.  Launched as the pass's programmatic dependent: the
-// blocks are placed while the pass ends and wait for its completion.
+// state from the list.
 __global__ void __launch_bounds__(128) k_collide(PushArgs A) {
-    pdl_wait();
     const int nc = min(*A.cand_count, A.cand_cap);
     const uint32_t step = *A.step;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nc; i += gridDim.x * blockDim.x) {
@@ -1813,7 +1808,7 @@ static int run_pass_tail(SimImpl& S, cudaStream_t st, const PushArgs& A) {
         PhaseTimer t(S, PIC_PHASE_MERGE, st);
         // one thread per candidate: each is a long chain of dependent
         // table lookups and Philox rounds
-        PIC_CUDA(launch_pdl(k_collide, dim3(4 * num_sms()), dim3(128), 0, st, A));
+        k_collide<<<4 * num_sms(), 128, 0, st>>>(A);
         S.launches += 1;
     }
     PIC_LAUNCH_CHECK();
