@@ -47,6 +47,22 @@ BYTES_PER_PARTICLE = 32.0  # x, y, vx, vy float32, read and written by the fused
 BYTES_PER_NODE = 12.0      # E (float2) read, charge (float) written
 
 
+def sort_passes(nodes, tile=16, digit_max=10):
+    """Radix passes of the cell sort of an nodes x nodes grid: tile-major cell
+    keys plus the dead key, in digits of at most digit_max bits."""
+    tiles = -(-(nodes - 1) // tile)
+    bits = (tiles * tiles * tile * tile).bit_length()
+    return -(-bits // digit_max)
+
+
+def sort_bytes_per_particle(passes):
+    """Compulsory bytes of one cell sort per particle: keys from x, y (8 B
+    read, key and slot 8 B written), each pass's histogram (4 B) and scatter
+    (8 B read, 8 B written), the tile starts (4 B), and the gather of the five
+    arrays through the permutation (4 B + 20 B read, 20 B written)."""
+    return 16.0 + 20.0 * passes + 4.0 + 44.0
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -258,6 +274,14 @@ def window_start(warmup, K, interval):
     return warmup + (target - warmup) % interval
 
 
+def sort_roofline(sort_ms, particles, nodes, peak):
+    """HBM fraction of one cell sort of every species (sort_bytes_per_particle)."""
+    passes = sort_passes(nodes)
+    b = particles * sort_bytes_per_particle(passes)
+    gbs = b / (sort_ms / 1e3) / 1e9
+    return {"passes": passes, "bytes": b, "achieved": round(gbs, 1), "unit": "GB/s", "frac": round(gbs / peak, 4)}
+
+
 def amortised_ms(ms_window, K, first_step, interval, sort_ms):
     """The window's time with the cell sort counted at its average rate: a
     sort every `interval` steps, whatever number of sorts the window held."""
@@ -347,6 +371,7 @@ def run_ours(args, world, rank, local):
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
         "ms_per_step_window": ms_window_max / args.steps, "sort_ms": round(sort_ms, 4),
         "sort_ms_amortised": round(sort_ms / args.sort_interval, 5) if args.sort_interval > 0 else 0.0,
+        "sort_roofline": sort_roofline(sort_ms, 0.5 * (n0 + n1), w.nodes, peak),
         "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 particles / f64 Poisson residual", "data": "synthetic (seeded Philox)",
         "config": {"workload": "mcc: 513x513 nodes (512^2 cells), dx 1e-4 m, "

@@ -1,13 +1,19 @@
 // Deterministic cell sort: the replacement of Particles2D.sort_particles_sparse
 // (src/Particles.py:550-632), whose atomic slot claims give a run-to-run
 // varying order.  Here the order is a stable least-significant-digit radix
-// sort of tile-major cell keys (8-bit digits; each pass is a stable counting
-// sort):
-//   upsweep   per-CTA digit histograms over a contiguous index range
-//   scan      one CTA: exclusive scan of the digit-major count table
-//   downsweep stable ranks inside each 4096-key sub-tile (warp match_any in
-//             index order), scattered to their global slots
-// Dead particles (NaN position) get the largest key and are dropped.
+// sort of tile-major cell keys, in as few passes of at most 10-bit digits as
+// the key width allows (19 bits at 513^2: two passes of 10 and 9 bits); each
+// pass is a stable counting sort over G CTAs (three per SM), each owning a
+// contiguous index range:
+//   upsweep    per-CTA digit histograms (one shared-memory increment per
+//              distinct digit and warp: the keys are nearly sorted)
+//   scan_rows  one CTA per digit: exclusive scan of that digit's counts over
+//              the CTAs, and the digit's total
+//   downsweep  the digits' bases (exclusive scan of the totals), then stable
+//              ranks inside each 4096-key sub-tile (warp match_any in index
+//              order), scattered to their global slots
+// then the first slot of every tile, from the sorted keys.  Dead particles
+// (NaN position) get the largest key and are dropped.
 #include <cuda.h>
 
 #include <algorithm>
@@ -23,7 +29,8 @@ constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortIpt = 16;
 constexpr int kSortSub = kSortThreads * kSortIpt;
-constexpr int kRadix = 256;
+constexpr int kRadixMax = 1 << kSortDigitMax;
+constexpr int kSortCtasPerSm = 3;  // the downsweep holds 80 registers a thread: three CTAs fit an SM
 
 __global__ void k_sort_keys(const float* __restrict__ x, const float* __restrict__ y, const int* __restrict__ n_dev,
                             int ncx, int ncy, int tile, int tiles_x, uint32_t dead_key, uint32_t* __restrict__ keys,
@@ -46,10 +53,13 @@ __device__ __forceinline__ void cta_range(int n, int G, int g, int& b, int& e) {
     e = min(n, b + per);
 }
 
-__global__ void k_upsweep(const uint32_t* __restrict__ keys, const int* __restrict__ n_dev, int shift, int G,
-                          int* __restrict__ cnt) {
-    __shared__ int h[kRadix];
-    for (int d = threadIdx.x; d < kRadix; d += blockDim.x) h[d] = 0;
+__global__ void __launch_bounds__(kSortThreads) k_upsweep(const uint32_t* __restrict__ keys,
+                                                          const int* __restrict__ n_dev, int shift, int bits, int G,
+                                                          int* __restrict__ cnt) {
+    __shared__ int h[kRadixMax];
+    const int radix = 1 << bits;
+    const uint32_t mask = uint32_t(radix - 1);
+    for (int d = threadIdx.x; d < radix; d += blockDim.x) h[d] = 0;
     __syncthreads();
     int b, e;
     cta_range(n_dev[0], G, blockIdx.x, b, e);
@@ -67,80 +77,110 @@ __global__ void k_upsweep(const uint32_t* __restrict__ keys, const int* __restri
 #pragma unroll
         for (int it = 0; it < kSortIpt; ++it) {
             const int i = base + it * kSortThreads + int(threadIdx.x);
-            const int d = i < e ? int((k[it] >> shift) & 0xff) : kRadix;
+            const int d = i < e ? int((k[it] >> shift) & mask) : kRadixMax;
             const unsigned peers = __match_any_sync(0xffffffffu, d);
-            if (d < kRadix && lane == __ffs(peers) - 1) atomicAdd(&h[d], __popc(peers));
+            if (d < kRadixMax && lane == __ffs(peers) - 1) atomicAdd(&h[d], __popc(peers));
         }
     }
     __syncthreads();
-    for (int d = threadIdx.x; d < kRadix; d += blockDim.x) cnt[d * G + blockIdx.x] = h[d];
+    for (int d = threadIdx.x; d < radix; d += blockDim.x) cnt[d * G + blockIdx.x] = h[d];
 }
 
-// Exclusive scan of cnt[0 .. total) in place, one CTA of 1024 threads: the
-// table is walked in coalesced tiles of 4096 counts (4 per thread), each
-// scanned by warp shuffles and carried into the next.
-__global__ void __launch_bounds__(1024) k_scan(int* __restrict__ cnt, int total) {
-    __shared__ int warp_tot[32];
-    __shared__ int carry;
+// Exclusive block scan of v (one value per thread, 256 threads); returns the
+// thread's prefix and leaves the block total in *total.
+__device__ __forceinline__ int block_exclusive_scan(int v, int* warp_tot, int* total) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    for (int base = 0; base < total; base += 4096) {
-        int v[4];
-        int sum = 0;
+    int incl = v;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int i = base + threadIdx.x * 4 + k;
-            v[k] = i < total ? cnt[i] : 0;
-            sum += v[k];
-        }
-        int incl = sum;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const int w = lane < kSortWarps ? warp_tot[lane] : 0;
+        int wi = w;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
+            const int t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += t;
         }
-        if (lane == 31) warp_tot[warp] = incl;
-        __syncthreads();
-        if (warp == 0) {
-            int w = warp_tot[lane];
-            int wi = w;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int t = __shfl_up_sync(0xffffffffu, wi, o);
-                if (lane >= o) wi += t;
-            }
-            warp_tot[lane] = wi - w;  // exclusive prefix of the warp totals
-        }
-        __syncthreads();
-        int run = carry + warp_tot[warp] + incl - sum;
+        if (lane < kSortWarps) warp_tot[lane] = wi - w;
+        if (lane == kSortWarps - 1) *total = wi;
+    }
+    __syncthreads();
+    const int r = warp_tot[warp] + incl - v;
+    __syncthreads();  // warp_tot may be reused
+    return r;
+}
+
+// One CTA per digit d: exclusive scan of cnt[d*G .. d*G+G) in place over the
+// CTAs, and the digit's total in tot[d].
+__global__ void __launch_bounds__(kSortThreads) k_scan_rows(int* __restrict__ cnt, int G, int* __restrict__ tot) {
+    __shared__ int warp_tot[kSortWarps];
+    __shared__ int total;
+    int* row = cnt + long(blockIdx.x) * G;
+    int carry = 0;
+    for (int base = 0; base < G; base += 4 * kSortThreads) {
+        int v[4], sum = 0;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            const int i = base + threadIdx.x * 4 + k;
-            if (i < total) cnt[i] = run;
+            const int i = base + int(threadIdx.x) * 4 + k;
+            v[k] = i < G ? row[i] : 0;
+            sum += v[k];
+        }
+        int run = carry + block_exclusive_scan(sum, warp_tot, &total);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int i = base + int(threadIdx.x) * 4 + k;
+            if (i < G) row[i] = run;
             run += v[k];
         }
-        __syncthreads();
-        if (threadIdx.x == 1023) carry = run;
+        carry += total;
         __syncthreads();
     }
+    if (threadIdx.x == 0) tot[blockIdx.x] = carry;
 }
 
 __global__ void __launch_bounds__(kSortThreads) k_downsweep(const uint32_t* __restrict__ kin,
                                                             const uint32_t* __restrict__ vin,
                                                             uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
-                                                            const int* __restrict__ n_dev, int shift, int G,
-                                                            const int* __restrict__ offs) {
-    __shared__ int running[kRadix];
-    __shared__ int wc[kSortWarps][kRadix];
-    __shared__ int subtotal[kRadix];
+                                                            const int* __restrict__ n_dev, int shift, int bits, int G,
+                                                            const int* __restrict__ offs,
+                                                            const int* __restrict__ tot) {
+    __shared__ int running[kRadixMax];
+    __shared__ int wc[kSortWarps][kRadixMax];
+    __shared__ int subtotal[kRadixMax];
+    __shared__ int warp_tot[kSortWarps];
+    __shared__ int total;
+    const int radix = 1 << bits;
+    const uint32_t mask = uint32_t(radix - 1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     int b, e;
     cta_range(n_dev[0], G, blockIdx.x, b, e);
-    for (int d = threadIdx.x; d < kRadix; d += blockDim.x) running[d] = offs[d * G + blockIdx.x];
+    {
+        // the digits' global bases: exclusive scan of the totals (each thread
+        // four consecutive digits), plus this CTA's offset within each digit
+        constexpr int kPer = kRadixMax / kSortThreads;
+        int v[kPer], sum = 0;
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            const int d = int(threadIdx.x) * kPer + k;
+            v[k] = d < radix ? tot[d] : 0;
+            sum += v[k];
+        }
+        int run = block_exclusive_scan(sum, warp_tot, &total);
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            const int d = int(threadIdx.x) * kPer + k;
+            if (d < radix) running[d] = run + offs[d * G + blockIdx.x];
+            run += v[k];
+        }
+    }
     for (int base = b; base < e; base += kSortSub) {
-        for (int q = threadIdx.x; q < kSortWarps * kRadix; q += blockDim.x) (&wc[0][0])[q] = 0;
+        for (int q = threadIdx.x; q < kSortWarps * radix; q += blockDim.x) wc[q >> bits][q & (radix - 1)] = 0;
         __syncthreads();
         uint32_t key[kSortIpt], val[kSortIpt];
         int rank[kSortIpt];
@@ -156,7 +196,7 @@ __global__ void __launch_bounds__(kSortThreads) k_downsweep(const uint32_t* __re
         for (int it = 0; it < kSortIpt; ++it) {
             const int idx = base + warp * (32 * kSortIpt) + it * 32 + lane;
             const bool valid = idx < e;
-            const int d = valid ? int((key[it] >> shift) & 0xff) : kRadix;
+            const int d = valid ? int((key[it] >> shift) & mask) : kRadixMax;
             const unsigned peers = __match_any_sync(0xffffffffu, d);
             const int leader = __ffs(peers) - 1;
             int basecnt = 0;
@@ -168,7 +208,7 @@ __global__ void __launch_bounds__(kSortThreads) k_downsweep(const uint32_t* __re
             rank[it] = valid ? basecnt + __popc(peers & lt) : -1;
         }
         __syncthreads();
-        for (int d = threadIdx.x; d < kRadix; d += blockDim.x) {
+        for (int d = threadIdx.x; d < radix; d += blockDim.x) {
             int run = 0;
 #pragma unroll
             for (int w = 0; w < kSortWarps; ++w) {
@@ -182,36 +222,30 @@ __global__ void __launch_bounds__(kSortThreads) k_downsweep(const uint32_t* __re
 #pragma unroll
         for (int it = 0; it < kSortIpt; ++it) {
             if (rank[it] < 0) continue;
-            const int d = int((key[it] >> shift) & 0xff);
+            const int d = int((key[it] >> shift) & mask);
             const int pos = running[d] + wc[warp][d] + rank[it];
             kout[pos] = key[it];
             vout[pos] = val[it];
         }
         __syncthreads();
-        for (int d = threadIdx.x; d < kRadix; d += blockDim.x) running[d] += subtotal[d];
+        for (int d = threadIdx.x; d < radix; d += blockDim.x) running[d] += subtotal[d];
         __syncthreads();
     }
 }
 
-// First sorted slot of each tile (lower bound of its first key) and the live count.
+// First sorted slot of each tile (the lower bound of its first key; empty
+// tiles get the next tile's start, the end the live count) and the live
+// count: position k writes the starts of the tiles after its predecessor's,
+// up to its own.
 __global__ void k_tile_starts(const uint32_t* __restrict__ keys, const int* __restrict__ live, int ntiles, int tt,
                               int* __restrict__ tile_start, int* __restrict__ count_out) {
     const int n = *live;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t <= ntiles; t += gridDim.x * blockDim.x) {
-        if (t == ntiles) {
-            if (tile_start) tile_start[t] = n;
-            if (count_out) *count_out = n;
-            continue;
-        }
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= n; k += gridDim.x * blockDim.x) {
+        if (k == n && count_out) *count_out = n;
         if (!tile_start) continue;
-        const uint32_t target = uint32_t(t) * uint32_t(tt);
-        int lo = 0, hi = n;
-        while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (keys[mid] < target) lo = mid + 1;
-            else hi = mid;
-        }
-        tile_start[t] = lo;
+        const int t1 = k < n ? int(keys[k] / uint32_t(tt)) : ntiles;
+        const int t0 = k > 0 ? int(keys[k - 1] / uint32_t(tt)) : -1;
+        for (int t = t0 + 1; t <= t1; ++t) tile_start[t] = k;
     }
 }
 
@@ -251,8 +285,7 @@ __global__ void k_copy_n(int* n_dev, const int* src) {
 
 int grid_blocks(long n, int threads);
 
-int sorter_create(int capacity, int nx, int ny, int tile, SortImpl* S) {
-    if (capacity < 1 || nx < 2 || ny < 2 || tile < 1) return fail(PIC_ERR_BAD_ARG, "pic_sorter_create: bad arguments");
+int sort_geometry(int capacity, int nx, int ny, int tile, int max_ctas, SortImpl* S) {
     S->capacity = capacity;
     S->nx = nx;
     S->ny = ny;
@@ -261,19 +294,33 @@ int sorter_create(int capacity, int nx, int ny, int tile, SortImpl* S) {
     S->tiles_y = (ny - 1 + tile - 1) / tile;
     S->ntiles = S->tiles_x * S->tiles_y;
     const unsigned long long nkeys = (unsigned long long)S->ntiles * tile * tile;
-    if (nkeys >= 0xffffffffull) return fail(PIC_ERR_BAD_ARG, "pic_sorter_create: grid too large for 32-bit keys");
+    if (nkeys >= 0xffffffffull) return fail(PIC_ERR_BAD_ARG, "cell sort: grid too large for 32-bit keys");
     S->dead_key = uint32_t(nkeys);
     int bits = 0;
     while ((1ull << bits) <= nkeys) ++bits;
-    S->passes = (bits + 7) / 8;
-    S->G = std::max(1, std::min(num_sms(), div_up(capacity, kSortSub)));
+    // the fewest passes of at most kSortDigitMax bits, the widths as even as possible
+    S->passes = (bits + kSortDigitMax - 1) / kSortDigitMax;
+    int rem = bits;
+    for (int p = 0; p < S->passes; ++p) {
+        S->digit[p] = (rem + (S->passes - p) - 1) / (S->passes - p);
+        rem -= S->digit[p];
+    }
+    S->G = std::max(1, std::min(max_ctas, div_up(capacity, kSortSub)));
+    return PIC_OK;
+}
+
+int sorter_create(int capacity, int nx, int ny, int tile, SortImpl* S) {
+    if (capacity < 1 || nx < 2 || ny < 2 || tile < 1) return fail(PIC_ERR_BAD_ARG, "pic_sorter_create: bad arguments");
+    PIC_TRY(sort_geometry(capacity, nx, ny, tile, kSortCtasPerSm * num_sms(), S));
     const size_t bytes = sizeof(uint32_t) * size_t(capacity);
     for (uint32_t** p : {&S->k0, &S->k1, &S->v0, &S->v1}) {
         PIC_CUDA(cudaMalloc(p, bytes));
         S->allocs.push_back(*p);
     }
-    PIC_CUDA(cudaMalloc(&S->cnt, sizeof(int) * kRadix * S->G));
+    PIC_CUDA(cudaMalloc(&S->cnt, sizeof(int) * kRadixMax * S->G));
     S->allocs.push_back(S->cnt);
+    PIC_CUDA(cudaMalloc(&S->tot, sizeof(int) * kRadixMax));
+    S->allocs.push_back(S->tot);
     PIC_CUDA(cudaMalloc(&S->n_dev, sizeof(int) * 2));
     S->allocs.push_back(S->n_dev);
     return PIC_OK;
@@ -289,16 +336,18 @@ void sorter_free(SortImpl* S) {
 // sorted source slots.
 int sort_passes(SortImpl& S, int* tile_start, int* count_out, const uint32_t** perm, cudaStream_t st) {
     uint32_t *ki = S.k0, *vi = S.v0, *ko = S.k1, *vo = S.v1;
+    int shift = 0;
     for (int p = 0; p < S.passes; ++p) {
-        const int shift = 8 * p;
-        k_upsweep<<<S.G, kSortThreads, 0, st>>>(ki, S.n_dev, shift, S.G, S.cnt);
-        k_scan<<<1, 1024, 0, st>>>(S.cnt, kRadix * S.G);
-        k_downsweep<<<S.G, kSortThreads, 0, st>>>(ki, vi, ko, vo, S.n_dev, shift, S.G, S.cnt);
+        const int w = S.digit[p];
+        k_upsweep<<<S.G, kSortThreads, 0, st>>>(ki, S.n_dev, shift, w, S.G, S.cnt);
+        k_scan_rows<<<1 << w, kSortThreads, 0, st>>>(S.cnt, S.G, S.tot);
+        k_downsweep<<<S.G, kSortThreads, 0, st>>>(ki, vi, ko, vo, S.n_dev, shift, w, S.G, S.cnt, S.tot);
         std::swap(ki, ko);
         std::swap(vi, vo);
+        shift += w;
     }
-    k_tile_starts<<<div_up(S.ntiles + 1, 256), 256, 0, st>>>(ki, S.n_dev + 1, S.ntiles, S.tile * S.tile, tile_start,
-                                                              count_out);
+    k_tile_starts<<<grid_blocks(long(S.capacity) + 1, 256), 256, 0, st>>>(ki, S.n_dev + 1, S.ntiles,
+                                                                           S.tile * S.tile, tile_start, count_out);
     *perm = vi;
     PIC_LAUNCH_CHECK();
     return PIC_OK;
@@ -340,8 +389,9 @@ int sort_run(SortImpl& S, const int* d_n, const float* x, const float* y, const 
 // before any stream capture.
 constexpr int kStaticSortCtas = 256;  // upper bound of the radix passes' CTA count
 constexpr size_t kStaticSortKeyBytes = sizeof(uint32_t) * size_t(PIC_SORT_STATIC_MAX);
-constexpr size_t kStaticSortCntBytes = sizeof(int) * size_t(kRadix) * kStaticSortCtas;
-constexpr size_t kStaticSortBytes = 4 * kStaticSortKeyBytes + kStaticSortCntBytes + 256;
+constexpr size_t kStaticSortCntBytes = sizeof(int) * size_t(kRadixMax) * kStaticSortCtas;
+constexpr size_t kStaticSortTotBytes = sizeof(int) * size_t(kRadixMax);
+constexpr size_t kStaticSortBytes = 4 * kStaticSortKeyBytes + kStaticSortCntBytes + kStaticSortTotBytes + 256;
 
 static __device__ __align__(256) unsigned char g_sort_scratch[kStaticSortBytes];
 
@@ -456,31 +506,19 @@ int pic_sort_static(const float* d_x, const float* d_y, const float* d_vx, const
         return fail(PIC_ERR_BAD_ARG, "pic_sort_static: bad arguments");
     if (d_x_out && (!d_y_out || !d_vx_out || !d_vy_out || !d_vx || !d_vy || (d_vz && !d_vz_out)))
         return fail(PIC_ERR_BAD_ARG, "pic_sort_static: output arrays incomplete");
-    // the same geometry and pass count as sorter_create, without its allocations
-    SortImpl S;
-    S.capacity = std::max(n, 1);
-    S.nx = nx;
-    S.ny = ny;
-    S.tile = tile;
-    S.tiles_x = (nx - 1 + tile - 1) / tile;
-    S.tiles_y = (ny - 1 + tile - 1) / tile;
-    S.ntiles = S.tiles_x * S.tiles_y;
-    const unsigned long long nkeys = (unsigned long long)S.ntiles * tile * tile;
-    if (nkeys >= 0xffffffffull) return fail(PIC_ERR_BAD_ARG, "pic_sort_static: grid too large for 32-bit keys");
-    S.dead_key = uint32_t(nkeys);
-    int bits = 0;
-    while ((1ull << bits) <= nkeys) ++bits;
-    S.passes = (bits + 7) / 8;
+    // the geometry and passes of sorter_create, without its allocations
     unsigned char* base = nullptr;
     int sms = 0;
     PIC_TRY(static_scratch(&base, &sms));
-    S.G = std::max(1, std::min(std::min(sms, kStaticSortCtas), div_up(S.capacity, kSortSub)));
+    SortImpl S;
+    PIC_TRY(sort_geometry(std::max(n, 1), nx, ny, tile, std::min(kSortCtasPerSm * sms, kStaticSortCtas), &S));
     S.k0 = reinterpret_cast<uint32_t*>(base);
     S.k1 = reinterpret_cast<uint32_t*>(base + kStaticSortKeyBytes);
     S.v0 = reinterpret_cast<uint32_t*>(base + 2 * kStaticSortKeyBytes);
     S.v1 = reinterpret_cast<uint32_t*>(base + 3 * kStaticSortKeyBytes);
     S.cnt = reinterpret_cast<int*>(base + 4 * kStaticSortKeyBytes);
-    S.n_dev = reinterpret_cast<int*>(base + 4 * kStaticSortKeyBytes + kStaticSortCntBytes);
+    S.tot = reinterpret_cast<int*>(base + 4 * kStaticSortKeyBytes + kStaticSortCntBytes);
+    S.n_dev = reinterpret_cast<int*>(base + 4 * kStaticSortKeyBytes + kStaticSortCntBytes + kStaticSortTotBytes);
     cudaStream_t st = as_stream(stream);
     // n_dev = {n, 0}: the live count starts at zero whatever the last call left
     k_set_n<<<1, 1, 0, st>>>(S.n_dev, n);

@@ -7,15 +7,24 @@
 
 namespace pic {
 
+constexpr int kSortDigitMax = 10;  // widest radix digit (bits)
+constexpr int kSortPassesMax = 4;  // 32-bit keys
+
 struct SortImpl {
     int capacity = 0, nx = 0, ny = 0, tile = 0, tiles_x = 0, tiles_y = 0, ntiles = 0;
     uint32_t dead_key = 0;
     int passes = 0, G = 0;
+    int digit[kSortPassesMax] = {};  // digit width of each pass (bits)
     uint32_t *k0 = nullptr, *k1 = nullptr, *v0 = nullptr, *v1 = nullptr;
-    int* cnt = nullptr;
+    int* cnt = nullptr;  // digit-major counts, (1 << kSortDigitMax) x G
+    int* tot = nullptr;  // digit totals, 1 << kSortDigitMax
     int* n_dev = nullptr;  // [0] = n (input slots), [1] = live count
     std::vector<void*> allocs;
 };
+
+// Tiles, dead key, passes and digit widths of a sort of `capacity` slots, and
+// its CTA count (at most max_ctas).
+int sort_geometry(int capacity, int nx, int ny, int tile, int max_ctas, SortImpl* S);
 
 int sorter_create(int capacity, int nx, int ny, int tile, SortImpl* S);
 void sorter_free(SortImpl* S);
