@@ -504,10 +504,12 @@ int pic_sim_read_profile(pic_sim* sim, pic_sim_profile* out);
 
 /* Many independent simulations stepped together: one CUDA graph holds a step
  * of every member, and a conditional WHILE node repeats it, so that n steps
- * of the whole ensemble are one graph launch.  Within a step every member's
- * preparation (cell sort, work items) is an independent branch, then one
- * persistent particle pass takes the work items of all members from one
- * queue, then every member's field solve is an independent branch.
+ * of the whole ensemble are one graph launch.  Within a step every member is
+ * an independent branch: its preparation (cell sort, work items), particle
+ * pass and field solve, so that one member's pass overlaps another's solve.
+ * Optionally (pic_ens_set_fused_pass) one persistent particle pass takes the
+ * work items of all members from one queue between the preparations and the
+ * solves.
  * Each member's cell sort sits under a conditional IF node that fires when
  * the member's own step count is a multiple of its sort interval; each
  * member's multigrid loop is a nested conditional WHILE node.  Members may
@@ -526,13 +528,13 @@ int pic_ens_destroy(pic_ens* e);
  * takes its first of the n steps eagerly. */
 int pic_ens_step(pic_ens* e, int n_steps, void* stream);
 /* 1 when the members' particle passes run as one persistent launch whose
- * work queue spans every member's work items (every member uses
- * PIC_PUSH_RING and the same geometry), 0 when each member's pass is its own
- * launch in its branch. */
+ * work queue spans every member's work items, 0 (the default) when each
+ * member's pass is its own launch in its branch. */
 int pic_ens_fused_pass(pic_ens* e, int* fused);
-/* fused = 0 gives every member's particle pass its own launch in its branch
- * (so that a member's pass can overlap another member's field solve); 1
- * restores the one pass over all members where it applies. */
+/* fused = 1 runs the members' particle passes as one launch over all members
+ * where that applies (every member uses PIC_PUSH_RING and the same
+ * geometry); 0 gives every member's pass its own launch in its branch (the
+ * default: a member's pass then overlaps another member's field solve). */
 int pic_ens_set_fused_pass(pic_ens* e, int fused);
 
 /* ------------------------------------------------------------------ */

@@ -7,7 +7,7 @@
 // contiguous index range:
 //   upsweep    per-CTA digit histograms (one shared-memory increment per
 //              distinct digit and warp: the keys are nearly sorted)
-//   scan_rows  one CTA per digit: exclusive scan of that digit's counts over
+//   scan_rows  one warp per digit: exclusive scan of that digit's counts over
 //              the CTAs, and the digit's total
 //   downsweep  the digits' bases (exclusive scan of the totals), then stable
 //              ranks inside each 4096-key sub-tile (warp match_any in index
@@ -115,32 +115,27 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* warp_tot, int* t
     return r;
 }
 
-// One CTA per digit d: exclusive scan of cnt[d*G .. d*G+G) in place over the
-// CTAs, and the digit's total in tot[d].
-__global__ void __launch_bounds__(kSortThreads) k_scan_rows(int* __restrict__ cnt, int G, int* __restrict__ tot) {
-    __shared__ int warp_tot[kSortWarps];
-    __shared__ int total;
-    int* row = cnt + long(blockIdx.x) * G;
+// One warp per digit d: exclusive scan of cnt[d*G .. d*G+G) in place over the
+// CTAs (32 counts at a time, carried), and the digit's total in tot[d].
+__global__ void __launch_bounds__(kSortThreads) k_scan_rows(int* __restrict__ cnt, int G, int radix,
+                                                            int* __restrict__ tot) {
+    const int d = blockIdx.x * kSortWarps + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (d >= radix) return;
+    int* row = cnt + long(d) * G;
     int carry = 0;
-    for (int base = 0; base < G; base += 4 * kSortThreads) {
-        int v[4], sum = 0;
+    for (int base = 0; base < G; base += 32) {
+        const int i = base + lane;
+        const int v = i < G ? row[i] : 0;
+        int incl = v;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int i = base + int(threadIdx.x) * 4 + k;
-            v[k] = i < G ? row[i] : 0;
-            sum += v[k];
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
         }
-        int run = carry + block_exclusive_scan(sum, warp_tot, &total);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int i = base + int(threadIdx.x) * 4 + k;
-            if (i < G) row[i] = run;
-            run += v[k];
-        }
-        carry += total;
-        __syncthreads();
+        if (i < G) row[i] = carry + incl - v;
+        carry += __shfl_sync(0xffffffffu, incl, 31);
     }
-    if (threadIdx.x == 0) tot[blockIdx.x] = carry;
+    if (lane == 0) tot[d] = carry;
 }
 
 __global__ void __launch_bounds__(kSortThreads) k_downsweep(const uint32_t* __restrict__ kin,
@@ -340,7 +335,7 @@ int sort_passes(SortImpl& S, int* tile_start, int* count_out, const uint32_t** p
     for (int p = 0; p < S.passes; ++p) {
         const int w = S.digit[p];
         k_upsweep<<<S.G, kSortThreads, 0, st>>>(ki, S.n_dev, shift, w, S.G, S.cnt);
-        k_scan_rows<<<1 << w, kSortThreads, 0, st>>>(S.cnt, S.G, S.tot);
+        k_scan_rows<<<div_up(1 << w, kSortWarps), kSortThreads, 0, st>>>(S.cnt, S.G, 1 << w, S.tot);
         k_downsweep<<<S.G, kSortThreads, 0, st>>>(ki, vi, ko, vo, S.n_dev, shift, w, S.G, S.cnt, S.tot);
         std::swap(ki, ko);
         std::swap(vi, vo);

@@ -2792,6 +2792,10 @@ int pic_ens_create(pic_sim* const* sims, int n, pic_ens** out) {
         return bail(fail(PIC_ERR_CUDA, "pic_ens_create: out of device memory"));
     const int rc = ens_setup_fused(E);
     if (rc != PIC_OK) return bail(rc);
+    // a pass per member by default: a member's pass then overlaps the other
+    // members' field solves (3.30 against 3.89 ms per step of the 64-member
+    // ensemble with one pass over all members, which ends before any solve)
+    E.fused = false;
     *out = e;
     return PIC_OK;
 }

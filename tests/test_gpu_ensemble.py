@@ -54,17 +54,20 @@ def _state(sim):
     return c, xs, phi
 
 
-@pytest.mark.parametrize("fused", [True, False])
-def test_ensemble_matches_members_stepped_alone(fused, steps=23):
-    """fused: every member on the ring pass, so that one particle pass spans all
-    members; otherwise one member takes the per-warp pass and every member's
-    pass is its own launch."""
+@pytest.mark.parametrize("structure", ["branches", "one_pass", "mixed_kernels"])
+def test_ensemble_matches_members_stepped_alone(structure, steps=23):
+    """branches (the default): every member's particle pass is its own launch in
+    its branch; one_pass: every member on the ring pass and one particle pass
+    spans all members; mixed_kernels: one member takes the per-warp pass, so
+    the one pass does not apply and the branches run."""
     ws = _workloads()
-    kinds = ["ring"] * len(MEMBERS) if fused else ["warp"] + ["ring"] * (len(MEMBERS) - 1)
+    kinds = ["warp"] + ["ring"] * (len(MEMBERS) - 1) if structure == "mixed_kernels" else ["ring"] * len(MEMBERS)
     together = [_make(w, cfg, k) for w, cfg, k in zip(ws, MEMBERS, kinds)]
     alone = [_make(w, cfg, k) for w, cfg, k in zip(ws, MEMBERS, kinds)]
     ens = ensemble.Ensemble(together)
-    assert ens.fused_pass == fused
+    assert not ens.fused_pass
+    ens.fused_pass = structure != "branches"
+    assert ens.fused_pass == (structure == "one_pass")
     ens.step(steps - 3)
     ens.step(3)  # a second launch of the same graph
     for sim in alone:
@@ -99,10 +102,12 @@ def test_ensemble_rejects_eager_members_and_duplicates():
     g.close()
 
 
-def test_ensemble_with_collisions_matches_members_stepped_alone():
+@pytest.mark.parametrize("one_pass", [True, False])
+def test_ensemble_with_collisions_matches_members_stepped_alone(one_pass):
     """Members with null-collision MCC (the MCC workload's tables, a denser gas
-    so that collisions and ionisation products occur every step) in the one
-    particle pass over all members, against the same members stepped alone.
+    so that collisions and ionisation products occur every step), in the one
+    particle pass over all members or in a pass per member, against the same
+    members stepped alone.
     After two steps (one of them with collisions) the two agree to FP32
     rounding, with the same candidates and collisions.  Then
     the runs drift apart in the last bits (rho's global float atomics: the
@@ -130,7 +135,8 @@ def test_ensemble_with_collisions_matches_members_stepped_alone():
     together = [make(i) for i in range(2)]
     alone = [make(i) for i in range(2)]
     ens = ensemble.Ensemble(together)
-    assert ens.fused_pass
+    ens.fused_pass = one_pass
+    assert ens.fused_pass == one_pass
     # two steps (the second kicks and collides, no sort between them): the
     # same candidates and collisions, the particles that were there before
     # equal to FP32 rounding (the products' slots follow atomic order; the
