@@ -62,6 +62,10 @@ constexpr int kPushP = 3;  // particles per thread per chunk (odd: conflict-free
 // wait on that bookkeeping (7 % faster than spreading the chunk over all warps).
 constexpr int kChunk = (kPushThreads - 32) * kPushP;
 constexpr int kBufStride = kChunk + 8;  // floats per array per buffer: room for the 16-byte alignment window
+// candidate-bit words staged with a chunk: its kChunk / 32 words, widened to
+// 16-byte boundaries at both ends
+constexpr int kCbWords = 32;
+static_assert(kChunk / 32 + 8 <= kCbWords, "a chunk's candidate words fit their stage");
 constexpr int kUnitMax = 8160;          // particles per work unit (one E tile staging, one charge flush)
 // The charge tile accumulates CIC weights as unsigned fixed point, 2^-19 per
 // unit: integer shared-memory atomics are native (float ones retry), the sum
@@ -184,17 +188,28 @@ struct ChunkDesc {
     int first;          // first chunk of its unit
 };
 
-// Issues the bulk copies of slots [b, e) of species s into `buf` (one thread).
+// The chunk's first candidate-bit word, rounded down to a 16-byte boundary.
+__device__ __forceinline__ int cb_word0(int b) { return (b >> 5) & ~3; }
+
+// Issues the bulk copies of slots [b, e) of species s into `buf` (one
+// thread), and, when `cbuf` is given and the species collides, the words of
+// its candidate bits that cover the slots into `cbuf`.
 template <bool ENS>
-__device__ __forceinline__ void issue_chunk(const PushArgs& A, const ChunkDesc& c, float* buf,
+__device__ __forceinline__ void issue_chunk(const PushArgs& A, const ChunkDesc& c, float* buf, unsigned* cbuf,
                                             unsigned long long* bar) {
     const int a0 = c.b & ~3, a1 = (c.e + 3) & ~3;
     const unsigned bytes = unsigned(a1 - a0) * 4u;
+    const PushArgs& M = member<ENS>(A, chunk_member<ENS>(c.s));
+    const int sp = chunk_species<ENS>(c.s);
+    const unsigned* const cb = (cbuf && M.do_mcc) ? M.cbits[sp] : nullptr;
+    const int w0 = cb_word0(c.b), w1 = (((c.e - 1) >> 5) + 4) & ~3;
+    const unsigned cbytes = cb ? unsigned(w1 - w0) * 4u : 0u;
     // x, y, vx, vy: vz is touched only by collision candidates (finish_candidate)
-    mbar_expect_tx(bar, 4u * bytes);
-    const SpeciesState& S = member<ENS>(A, chunk_member<ENS>(c.s)).state[chunk_species<ENS>(c.s)];
+    mbar_expect_tx(bar, 4u * bytes + cbytes);
+    const SpeciesState& S = M.state[sp];
 #pragma unroll
     for (int k = 0; k < 4; ++k) bulk_g2s(buf + k * kBufStride, S.cur[k] + a0, bytes, bar);
+    if (cb) bulk_g2s(cbuf, cb + w0, cbytes, bar);
 }
 
 // The chunk after `c`: the rest of its unit, else the first chunk of a newly
@@ -430,10 +445,11 @@ template <bool RZ, bool FULL, bool ENS = false>
 __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
     extern __shared__ __align__(128) unsigned char smem[];
     float* bufs = reinterpret_cast<float*>(smem);  // [kStages][4][kBufStride]
+    unsigned* cbs = reinterpret_cast<unsigned*>(bufs + kStages * 4 * kBufStride);  // [kStages][kCbWords]
     // the tile side of the unit in work: an ensemble's members may differ
     // (A.rw is then their largest, which sizes shared memory)
     int RW = A.rw;
-    float4* et = reinterpret_cast<float4*>(bufs + kStages * 4 * kBufStride);
+    float4* et = reinterpret_cast<float4*>(cbs + kStages * kCbWords);
     unsigned* rt = reinterpret_cast<unsigned*>(et + A.rw * A.rw);
     __shared__ __align__(8) unsigned long long bar[kStages];
     __shared__ ChunkDesc s_ch[kStages];
@@ -450,7 +466,7 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
         none.valid = 0;
         const ChunkDesc c = next_chunk<ENS>(A, none, n_items);
         s_ch[0] = c;
-        if (c.valid) issue_chunk<ENS>(A, c, bufs, &bar[0]);
+        if (c.valid) issue_chunk<ENS>(A, c, bufs, cbs, &bar[0]);
     }
     __syncthreads();
     ChunkDesc ch = s_ch[0];
@@ -494,7 +510,7 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
             s_ch[nxt] = nc;
             if (nc.valid) {
                 fence_proxy_async();
-                issue_chunk<ENS>(A, nc, bufs + nxt * 4 * kBufStride, &bar[nxt]);
+                issue_chunk<ENS>(A, nc, bufs + nxt * 4 * kBufStride, cbs + nxt * kCbWords, &bar[nxt]);
             }
         }
         if (prev.valid) store_chunk_edges<ENS>(A, prev, bufs + prv * 4 * kBufStride, tid);
@@ -506,17 +522,20 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
         float* const pvx = py + kBufStride;
         float* const pvy = pvx + kBufStride;
         const SpeciesConst C = M.sp[s];
-        const unsigned* const cbits = (M.do_mcc && M.mcc->sp[s].nproc > 0) ? M.cbits[s] : nullptr;
+        // the chunk's candidate-bit words, staged with it (a species without
+        // collision processes has no bits)
+        const unsigned* const cbw = (M.do_mcc && M.cbits[s]) ? cbs + cur * kCbWords : nullptr;
+        const int wb = cb_word0(b);
         // r-z: the azimuthal velocity is not staged; it is read and written in place
         float* const gvz = RZ ? M.state[s].cur[4] + b : nullptr;
-        // the candidate bits of this thread's slots (at most two words, each
-        // loaded only if one of the chunk's slots lies in it), as a 3-bit mask
+        // the candidate bits of this thread's slots (at most two words), as a
+        // 3-bit mask
         const int wt = tid - 32;  // particle lane (warp 0 has none)
         const int s0 = b + wt * kPushP, s_last = min(s0 + kPushP, b + n) - 1;
         unsigned cmask = 0u;
-        if (wt >= 0 && cbits && s0 <= s_last) {
-            const unsigned cw0 = __ldg(cbits + (s0 >> 5));
-            const unsigned cw1 = (s_last >> 5) != (s0 >> 5) ? __ldg(cbits + (s_last >> 5)) : 0u;
+        if (wt >= 0 && cbw && s0 <= s_last) {
+            const unsigned cw0 = cbw[(s0 >> 5) - wb];
+            const unsigned cw1 = (s_last >> 5) != (s0 >> 5) ? cbw[(s_last >> 5) - wb] : 0u;
             cmask = __funnelshift_r(cw0, cw1, s0 & 31);
         }
         const unsigned tw = unsigned(RW - 1);  // staged tile: local cell index in [0, RW-2]
@@ -742,7 +761,7 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push_pipe(PushArgs A) {
         for (int k = 0; k < 2; ++k) {
             const ChunkDesc c = (k == 0 || s_ch[0].valid) ? next_chunk<false>(A, k ? s_ch[0] : none, n_items) : none;
             s_ch[k] = c;
-            if (c.valid) issue_chunk<false>(A, c, bufs + k * 4 * kBufStride, &full[k]);
+            if (c.valid) issue_chunk<false>(A, c, bufs + k * 4 * kBufStride, nullptr, &full[k]);
             else mbar_arrive(&full[k]);  // the end marker
         }
     }
@@ -775,7 +794,7 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push_pipe(PushArgs A) {
                 s_ch[s2] = c2;
                 if (c2.valid) {
                     fence_proxy_async();
-                    issue_chunk<false>(A, c2, bufs + s2 * 4 * kBufStride, &full[s2]);
+                    issue_chunk<false>(A, c2, bufs + s2 * 4 * kBufStride, nullptr, &full[s2]);
                 } else {
                     mbar_arrive(&full[s2]);  // the end marker
                 }
@@ -823,7 +842,7 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push_pipe(PushArgs A) {
         float* const pvx = py + kBufStride;
         float* const pvy = pvx + kBufStride;
         const SpeciesConst C = A.sp[s];
-        const unsigned* const cbits = (A.do_mcc && A.mcc->sp[s].nproc > 0) ? A.cbits[s] : nullptr;
+        const unsigned* const cbits = A.do_mcc ? A.cbits[s] : nullptr;
         float* const gvz = RZ ? A.state[s].cur[4] + b : nullptr;
         const int s0 = b + ctid * kPushP, s_last = min(s0 + kPushP, b + n) - 1;
         unsigned cmask = 0u;
@@ -1135,7 +1154,7 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push_warp(const __grid_cons
         float* const gvx = SS.cur[2];
         float* const gvy = SS.cur[3];
         float* const gvz = SS.cur[4];
-        const unsigned* const cbits = (A.do_mcc && A.mcc->sp[s].nproc > 0) ? A.cbits[s] : nullptr;
+        const unsigned* const cbits = A.do_mcc ? A.cbits[s] : nullptr;
         unsigned my_abs = 0, my_cand = 0, my_elec = 0;
         const int a0 = U.b & ~3;
         for (int j = 0; !failed; ++j) {
@@ -2063,8 +2082,8 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
         PIC_CUDA(cudaMemcpy(S.phi, phi0.data(), sizeof(double) * S.G, cudaMemcpyHostToDevice));
     }
     // launch shape of the particle pass
-    S.push_smem =
-        sizeof(float) * kStages * 4 * kBufStride + size_t(S.rw) * S.rw * (sizeof(float4) + sizeof(unsigned));
+    S.push_smem = sizeof(float) * kStages * 4 * kBufStride + sizeof(unsigned) * kStages * kCbWords +
+                  size_t(S.rw) * S.rw * (sizeof(float4) + sizeof(unsigned));
     const void* push_fns[4] = {reinterpret_cast<const void*>(k_push<false, false>),
                                reinterpret_cast<const void*>(k_push<false, true>),
                                reinterpret_cast<const void*>(k_push<true, false>),
