@@ -66,6 +66,10 @@ constexpr int kBufStride = kChunk + 8;  // floats per array per buffer: room for
 // 16-byte boundaries at both ends
 constexpr int kCbWords = 32;
 static_assert(kChunk / 32 + 8 <= kCbWords, "a chunk's candidate words fit their stage");
+// collision candidates a k_push block lists in shared memory during a work
+// unit and appends to the global list at the unit's end (about P_null * 8160
+// per unit: 20 at the 513^2 workload's electrons); more go to it one by one
+constexpr int kCandUnit = 64;
 constexpr int kUnitMax = 8160;          // particles per work unit (one E tile staging, one charge flush)
 // The charge tile accumulates CIC weights as unsigned fixed point, 2^-19 per
 // unit: integer shared-memory atomics are native (float ones retry), the sum
@@ -454,6 +458,10 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
     __shared__ __align__(8) unsigned long long bar[kStages];
     __shared__ ChunkDesc s_ch[kStages];
     __shared__ unsigned s_abs, s_cand, s_elec;
+    // the unit's collision candidates: (species, slot) and kicked state
+    __shared__ int2 s_cidx[kCandUnit];
+    __shared__ float4 s_cst[kCandUnit];
+    __shared__ int s_nc, s_nflush, s_cbase;
     const int tid = threadIdx.x;
     const int n_items = *A.n_items;
     if (tid == 0) {
@@ -462,6 +470,7 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
         s_abs = 0;
         s_cand = 0;
         s_elec = 0;
+        s_nc = 0;
         ChunkDesc none;
         none.valid = 0;
         const ChunkDesc c = next_chunk<ENS>(A, none, n_items);
@@ -568,8 +577,15 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
                 vy = __fmaf_rn(C.kq, cic_interp(c, e00.y, e10.y, e01.y, e11.y), vy);
             }
             if (candidate) {
-                // kicked but not moved: k_collide finishes it after this pass
+                // kicked but not moved: listed here, appended to the global
+                // list at the unit's end; k_collide finishes it after this pass
                 ++my_cand;
+                const int k = atomicAdd(&s_nc, 1);
+                if (k < kCandUnit) {
+                    s_cidx[k] = make_int2(s, b + l);
+                    s_cst[k] = make_float4(x, y, vx, vy);
+                    continue;
+                }
                 const int slot = atomicAdd(M.cand_count, 1);
                 if (slot < M.cand_cap) {
                     M.cand[slot] = make_int2(s, b + l);
@@ -655,8 +671,24 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
                 s_abs = 0;
                 s_cand = 0;
                 s_elec = 0;
+                // the unit's listed candidates: one reservation in the global list
+                const int nl = min(s_nc, kCandUnit);
+                s_nflush = nl;
+                s_cbase = nl ? atomicAdd(M.cand_count, nl) : 0;
+                s_nc = 0;
             }
             __syncthreads();
+            // (the list is refilled only after the next chunk's barrier)
+            if (tid < s_nflush) {
+                const int slot = s_cbase + tid;
+                if (slot < M.cand_cap) {
+                    M.cand[slot] = s_cidx[tid];
+                    M.cand_state[slot] = s_cst[tid];
+                } else {
+                    // no room: the particle keeps its kick and is not moved this step
+                    atomicAdd(M.ctr + kCtrCandOverflow, 1ull);
+                }
+            }
             ch = s_ch[nxt];
             if (ch.valid && ch.tile >= 0) {
                 if constexpr (ENS) RW = member<ENS>(A, chunk_member<ENS>(ch.s)).rw;
