@@ -279,6 +279,24 @@ __global__ void __launch_bounds__(256) k_mcc_bits(const MccDev* __restrict__ M, 
     }
 }
 
+// Asynchronous copies into shared memory (cp.async), completed per thread.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+// 8 bytes, or zeros when `bytes` is 0 (the source is then not read)
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, unsigned bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+// Waits until at most n (0..2) of this thread's copy groups are still in flight.
+__device__ __forceinline__ void cp_async_wait_pending(int n) {
+    if (n <= 0) asm volatile("cp.async.wait_group 0;" ::: "memory");
+    else if (n == 1) asm volatile("cp.async.wait_group 1;" ::: "memory");
+    else asm volatile("cp.async.wait_group 2;" ::: "memory");
+}
+
 // Stages the E tile of a unit's tile and zeroes its charge tile.  The E tile
 // holds node pairs along x, et[q] = (E at node q, E at its east neighbour
 // i1 = min(i + 1, nx - 1)), so that a particle reads its four E values with
@@ -299,6 +317,26 @@ __device__ __forceinline__ void stage_tile(const PushArgs& A, int tile, float4* 
         et[q] = v;
         rt[q] = 0u;
     }
+}
+
+// stage_tile's E tile by asynchronous copies (two 8-byte copies per node
+// pair, zeros outside the grid), committed as one group; the charge tile is
+// left as the last flush zeroed it.  The caller waits (cp_async_wait_all)
+// and meets the block at a barrier before the tile is read.
+__device__ __forceinline__ void stage_etile_async(const PushArgs& A, int tile, float4* et, int& ox, int& oy) {
+    const int RW = A.rw;
+    ox = (tile % A.tiles_x) * A.tile - kHalo;
+    oy = (tile / A.tiles_x) * A.tile - kHalo;
+    for (int q = threadIdx.x; q < RW * RW; q += kPushThreads) {
+        const int gi = ox + q % RW, gj = oy + q / RW;
+        const bool in = gi >= 0 && gj >= 0 && gi < A.nx && gj < A.ny;
+        const float2* p0 = in ? A.E + long(gj) * A.ep + gi : A.E;
+        const float2* p1 = (in && gi + 1 < A.nx) ? p0 + 1 : p0;
+        float* d = reinterpret_cast<float*>(et + q);
+        cp_async8(d, p0, in ? 8u : 0u);
+        cp_async8(d + 2, p1, in ? 8u : 0u);
+    }
+    cp_async_commit();
 }
 
 // Bulk copies from shared memory back to global memory (one bulk group per
@@ -483,6 +521,8 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
     prev.valid = 0;
     unsigned phases = 0u;  // expected parity of each stage's mbarrier
     int cur = 0, ox = 0, oy = 0;
+    // the charge tile starts at zero (every flush zeroes what it read)
+    for (int q = tid; q < A.rw * A.rw; q += kPushThreads) rt[q] = 0u;
     if (ch.valid && ch.tile >= 0) {
         if constexpr (ENS) RW = member<ENS>(A, chunk_member<ENS>(ch.s)).rw;
         stage_tile(member<ENS>(A, chunk_member<ENS>(ch.s)), ch.tile, et, rt, ox, oy);
@@ -656,12 +696,20 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
             }
             my_abs = my_cand = my_elec = 0u;
             __syncthreads();
+            // every particle of the unit is done with the E tile: the next
+            // unit's tile is copied in while the charge tile is flushed
+            const ChunkDesc nch = s_ch[nxt];
+            int nox = ox, noy = oy;
+            if (nch.valid && nch.tile >= 0)
+                stage_etile_async(member<ENS>(A, chunk_member<ENS>(nch.s)), nch.tile, et, nox, noy);
             if (tiled && do_deposit) {
                 for (int q = tid; q < RW * RW; q += kPushThreads) {
                     const unsigned sum = rt[q];
-                    if (sum)
+                    if (sum) {
+                        rt[q] = 0u;
                         atomicAdd(M.rho + long(oy + q / RW) * M.nx + ox + q % RW,
                                   __fmul_rn(C.scale, __fmul_rn(float(sum), kFixInv)));
+                    }
                 }
             }
             if (tid == 0) {
@@ -677,6 +725,7 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
                 s_cbase = nl ? atomicAdd(M.cand_count, nl) : 0;
                 s_nc = 0;
             }
+            cp_async_wait_all();
             __syncthreads();
             // (the list is refilled only after the next chunk's barrier)
             if (tid < s_nflush) {
@@ -689,10 +738,11 @@ __global__ void __launch_bounds__(kPushThreads, 4) k_push(PushArgs A) {
                     atomicAdd(M.ctr + kCtrCandOverflow, 1ull);
                 }
             }
-            ch = s_ch[nxt];
+            ch = nch;
             if (ch.valid && ch.tile >= 0) {
                 if constexpr (ENS) RW = member<ENS>(A, chunk_member<ENS>(ch.s)).rw;
-                stage_tile(member<ENS>(A, chunk_member<ENS>(ch.s)), ch.tile, et, rt, ox, oy);
+                ox = nox;
+                oy = noy;
             }
         }
         cur = nxt;
@@ -1070,18 +1120,6 @@ __device__ __forceinline__ UnitDesc claim_unit(const PushArgs& A, int n_items) {
 struct WarpFeed {
     int pu, pj, issued;
 };
-
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-// Waits until at most n (0..2) of this thread's copy groups are still in flight.
-__device__ __forceinline__ void cp_async_wait_pending(int n) {
-    if (n <= 0) asm volatile("cp.async.wait_group 0;" ::: "memory");
-    else if (n == 1) asm volatile("cp.async.wait_group 1;" ::: "memory");
-    else asm volatile("cp.async.wait_group 2;" ::: "memory");
-}
 
 // Every lane: loads this warp's next groups (each lane 16 bytes of each of
 // x, y, vx, vy: one asynchronous copy group per particle group) while stage
