@@ -258,7 +258,7 @@ int pic_sort(pic_sorter* s, const float* d_x, const float* d_y, const float* d_v
 /* The cell sort of pic_sort without allocation.  No counterpart in the
  * reference: it serves callers that must not allocate device memory.  Its
  * scratch is a fixed device array sized for PIC_SORT_STATIC_MAX particles
- * (about 16 MiB, held by every GPU that loads the library until the process
+ * (about 17 MiB, held by every GPU that loads the library until the process
  * exits); n above that is rejected with PIC_ERR_BAD_ARG.  nx, ny and tile
  * are the arguments of pic_sorter_create; the rest, and the results, are
  * those of pic_sort.  Every call shares the array, which keeps the last
