@@ -34,8 +34,10 @@ def run_sort(x, y, vx, vy, vz, m, nn, tile, capacity=None):
         _lib.load().pic_sorter_destroy(s)
 
 
+# key widths: 9 bits (one radix pass), 15 (two), 19 (two of 10 and 9 bits),
+# 21 (three of 7), and a tile side that is not a power of two
 @pytest.mark.parametrize("m,nn,n,tile", [(17, 17, 1000, 4), (129, 129, 300_000, 16), (513, 513, 3_000_000, 16),
-                                         (65, 33, 50_000, 8)])
+                                         (65, 33, 50_000, 8), (1025, 1025, 2_000_000, 16), (200, 150, 100_000, 5)])
 def test_sort_is_stable_argsort(m, nn, n, tile):
     rng = np.random.Generator(np.random.Philox(7))
     x = rng.uniform(0, m - 1, n).astype(np.float32)
