@@ -26,6 +26,8 @@ int mcc_build(const pic_mcc_desc* d, int nspecies, const double* mass, double dt
     MccDev& M = H->dev;
     M = MccDev{};
     M.ne = ne;
+    M.e_lo = energy[0];
+    M.e_hi = energy[ne - 1];
     M.log_e0 = logf(energy[0]);
     M.inv_log_ratio = float(double(ne - 1) / std::log(double(energy[ne - 1]) / double(energy[0])));
     M.gas_density = float(d->gas_density);

@@ -39,6 +39,7 @@ struct MccSpeciesDev {
 struct MccDev {
     int ne;
     const float* energy;  // eV, log-spaced
+    float e_lo, e_hi;     // energy[0] and energy[ne - 1]
     float log_e0, inv_log_ratio;
     float gas_density;
     MccSpeciesDev sp[PIC_MAX_SPECIES];
@@ -67,15 +68,26 @@ __device__ __forceinline__ MccBin mcc_bin(const MccDev& M, float e) {
     MccBin b;
     b.j = 0;
     b.t = 0.0f;
-    b.lo = e <= E[0];
-    b.hi = !b.lo && e >= E[ne - 1];
+    b.lo = e <= M.e_lo;
+    b.hi = !b.lo && e >= M.e_hi;
     if (b.lo || b.hi) return b;
+    // the bin from the log-spaced grid, corrected (rarely) by the grid
+    // itself; both ends of the bin are loaded together
     int j = int(__fmul_rn(__fsub_rn(logf(e), M.log_e0), M.inv_log_ratio));
     j = max(0, min(j, ne - 2));
-    while (j > 0 && e < E[j]) --j;
-    while (j < ne - 2 && e >= E[j + 1]) ++j;
+    float a = E[j], c = E[j + 1];
+    while (j > 0 && e < a) {
+        --j;
+        c = a;
+        a = E[j];
+    }
+    while (j < ne - 2 && e >= c) {
+        ++j;
+        a = c;
+        c = E[j + 1];
+    }
     b.j = j;
-    b.t = __fdiv_rn(__fsub_rn(e, E[j]), __fsub_rn(E[j + 1], E[j]));
+    b.t = __fdiv_rn(__fsub_rn(e, a), __fsub_rn(c, a));
     return b;
 }
 
@@ -150,10 +162,18 @@ __device__ __forceinline__ MccOutcome mcc_collide(const MccDev& M, const MccSpec
     const float e = __fmul_rn(S.half_m_over_q, v2);
     const float target = __fmul_rn(u01_float(r0.x), S.nu_max);
     const MccBin bin = mcc_bin(M, e);
+    // every process's cross section at once (independent loads), then the
+    // cumulative test in process order
+    float sigs[PIC_MAX_PROCESSES];
+#pragma unroll
+    for (int k = 0; k < PIC_MAX_PROCESSES; ++k)
+        sigs[k] = k < S.nproc ? mcc_sigma(M, S.sigma + long(k) * M.ne, bin) : 0.0f;
     float acc = 0.0f;
     int proc = -1;
-    for (int k = 0; k < S.nproc; ++k) {
-        const float sig = mcc_sigma(M, S.sigma + long(k) * M.ne, bin);
+#pragma unroll
+    for (int k = 0; k < PIC_MAX_PROCESSES; ++k) {
+        if (k >= S.nproc) break;
+        const float sig = sigs[k];
         acc = __fadd_rn(acc, __fmul_rn(__fmul_rn(M.gas_density, sig), speed));
         if (target < acc) {
             proc = k;

@@ -422,18 +422,18 @@ __device__ __forceinline__ void place_product(const PushArgs& A, int s, float x,
 // ionisation products, then the drift, absorption and deposit (global
 // atomics; a few candidates per thousand particles).  (x, y, vx, vy) is the
 // kicked state; vz is read from the slot, which the pass does not touch.
-__device__ __forceinline__ void finish_candidate(const PushArgs& A, uint32_t step, int s, int p, float x, float y,
-                                                 float vx, float vy) {
+__device__ __forceinline__ void finish_candidate(const PushArgs& A, const MccDev& MC, uint32_t step, int s, int p,
+                                                 float x, float y, float vx, float vy) {
     const SpeciesState& S = A.state[s];
     const SpeciesConst C = A.sp[s];
     float vz = S.cur[4][p];
-    const MccOutcome o = mcc_collide(*A.mcc, A.mcc->sp[s], uint32_t(s), uint32_t(p), step, A.key, vx, vy, vz);
+    const MccOutcome o = mcc_collide(MC, MC.sp[s], uint32_t(s), uint32_t(p), step, A.key, vx, vy, vz);
     if (o.overflow) atomicAdd(A.ctr + kCtrOverflow, 1ull);
     if (o.proc >= 0) {
         atomicAdd(A.ctr + kCtrCollisions + s * PIC_MAX_PROCESSES + o.proc, 1ull);
         if (o.born) {
             // born at the parent's position before its drift
-            const MccSpeciesDev& M = A.mcc->sp[s];
+            const MccSpeciesDev& M = MC.sp[s];
             place_product(A, M.born_e, x, y, o.be[0], o.be[1], o.be[2]);
             place_product(A, M.born_i, x, y, o.bi[0], o.bi[1], o.bi[2]);
         }
@@ -1405,14 +1405,15 @@ __global__ void __launch_bounds__(kPushThreads, 3) k_push_warp(const __grid_cons
 }
 
 // The collision candidates of the pass, one thread each, with their kicked
-// state from the list.
-__global__ void __launch_bounds__(128) k_collide(PushArgs A) {
+// state from the list; the tables' descriptor is a kernel parameter (no
+// global load before the first table lookup).
+__global__ void __launch_bounds__(128) k_collide(PushArgs A, const __grid_constant__ MccDev MC) {
     const int nc = min(*A.cand_count, A.cand_cap);
     const uint32_t step = *A.step;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nc; i += gridDim.x * blockDim.x) {
         const int2 c = A.cand[i];
         const float4 v = A.cand_state[i];
-        finish_candidate(A, step, c.x, c.y, v.x, v.y, v.z, v.w);
+        finish_candidate(A, MC, step, c.x, c.y, v.x, v.y, v.z, v.w);
     }
 }
 
@@ -1897,7 +1898,7 @@ static int run_pass_tail(SimImpl& S, cudaStream_t st, const PushArgs& A) {
         PhaseTimer t(S, PIC_PHASE_MERGE, st);
         // one thread per candidate: each is a long chain of dependent
         // table lookups and Philox rounds
-        k_collide<<<4 * num_sms(), 128, 0, st>>>(A);
+        k_collide<<<4 * num_sms(), 128, 0, st>>>(A, S.mcc.dev);
         S.launches += 1;
     }
     PIC_LAUNCH_CHECK();
