@@ -1696,6 +1696,8 @@ struct SimImpl {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     // g_sort_step: the step whose side branch sorts for the next step
     cudaGraphExec_t g_step = nullptr, g_sort_step = nullptr;
+    cudaGraphExec_t g_sort = nullptr;  // the cell sort alone (init, pic_sim_sort)
+    long long sort_graph_launches = 0;
     // the next particle pass is prepared (its sort, items and candidate bits
     // done, the step counter advanced): set by a captured step, cleared by
     // anything that changes the particle state on the host's behalf
@@ -1955,6 +1957,33 @@ static int sort_all(SimImpl& S, cudaStream_t st) {
     return PIC_OK;
 }
 
+// sort_all as one graph launch (captured at the first call): its forty-odd
+// small launches are then enqueued by one call, so that the GPU does not wait
+// on the host between them.  Profiling launches them one by one.
+static int sort_all_graph(SimImpl& S, cudaStream_t st) {
+    if (S.profiling) return sort_all(S, st);
+    if (!S.g_sort) {
+        const long long l0 = S.launches;
+        PIC_CUDA(cudaStreamBeginCapture(S.cap, cudaStreamCaptureModeThreadLocal));
+        const int rc = sort_all(S, S.cap);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(S.cap, &g);
+        S.sort_graph_launches = S.launches - l0;
+        S.launches = l0;
+        if (rc != PIC_OK) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (ec != cudaSuccess) return fail(PIC_ERR_CUDA, "sort capture: %s", cudaGetErrorString(ec));
+        const cudaError_t ei = cudaGraphInstantiate(&S.g_sort, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) return fail(PIC_ERR_CUDA, "sort graph: %s", cudaGetErrorString(ei));
+    }
+    PIC_CUDA(cudaGraphLaunch(S.g_sort, st));
+    S.launches += S.sort_graph_launches;
+    return PIC_OK;
+}
+
 // The steady-state step captured once into a CUDA graph: the particle pass
 // (kick + MCC + drift + deposit, prepared beforehand), then the field solve
 // (RHS, multigrid, E) on the capture stream and, on a side branch beside it,
@@ -2203,7 +2232,8 @@ static int sim_create(const pic_sim_desc* d, cudaStream_t st, SimImpl& S) {
 static void sim_free(SimImpl& S) {
     if (S.g_step) cudaGraphExecDestroy(S.g_step);
     if (S.g_sort_step) cudaGraphExecDestroy(S.g_sort_step);
-    S.g_step = S.g_sort_step = nullptr;
+    if (S.g_sort) cudaGraphExecDestroy(S.g_sort);
+    S.g_step = S.g_sort_step = S.g_sort = nullptr;
     if (S.cap) cudaStreamDestroy(S.cap);
     if (S.cap2) cudaStreamDestroy(S.cap2);
     if (S.ev_fork) cudaEventDestroy(S.ev_fork);
@@ -2570,7 +2600,7 @@ int pic_sim_init(pic_sim* sim, void* stream) {
     SimImpl& S = sim->s;
     cudaStream_t st = as_stream(stream);
     S.prepared = false;
-    if (S.d.sort_interval > 0) PIC_TRY(sort_all(S, st));
+    if (S.d.sort_interval > 0) PIC_TRY(sort_all_graph(S, st));
     PIC_TRY(particle_pass(S, st, 0, 0, 0, 1, 1.0, 0));
     PIC_TRY(field_solve(S, st, false));
     PIC_TRY(particle_pass(S, st, 1, 0, 0, 0, -0.5, 0));
@@ -2589,7 +2619,7 @@ int pic_sim_step(pic_sim* sim, int n_steps, void* stream) {
         const bool sort = S.d.sort_interval > 0 && S.steps % S.d.sort_interval == 0;
         if (S.d.use_graph && S.kick_pending && !S.profiling && mg_uses_graph(S.mg)) {
             if (!S.prepared) {
-                if (sort) PIC_TRY(sort_all(S, st));
+                if (sort) PIC_TRY(sort_all_graph(S, st));
                 PIC_TRY(prepare_pass(S, st, 1, 1));
             }
             if (!S.g_step) {
@@ -2673,7 +2703,7 @@ int pic_sim_sort(pic_sim* sim, void* stream) {
     SimImpl& S = sim->s;
     if (!S.have_sorter) return fail(PIC_ERR_BAD_ARG, "pic_sim_sort: the simulation was created without a sort");
     cudaStream_t st = as_stream(stream);
-    PIC_TRY(sort_all(S, st));
+    PIC_TRY(sort_all_graph(S, st));
     // a pass prepared by the last captured step holds work items of the
     // unsorted order: rebuild them for the same step (the counter stays)
     if (S.prepared) PIC_TRY(prepare_pass(S, st, 1, 0));
