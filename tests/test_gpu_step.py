@@ -151,6 +151,45 @@ def test_fused_step_with_mcc_bookkeeping():
     assert 0 < c["born"][0] <= c["collisions"][0][2] and c["born"][1] <= c["collisions"][0][2]
 
 
+@pytest.mark.parametrize("push_kernel", ["ring", "pipe"])
+def test_fused_step_with_mcc_and_electrodes_bookkeeping(push_kernel):
+    """Null-collision MCC in a dense gas with internal electrode lines: the
+    collision candidates (finished after the pass) and their ionisation
+    products drift through the same electrode test as every other particle.
+    Every particle is accounted for: live = loaded - wall-absorbed -
+    electrode-collected + born, per species, with collections among the
+    candidates' drifts too."""
+    w = workloads.scaled(workloads.MCC, nodes=129, n=150_000, gas_density=3e22, Te=20.0)
+    m = w.nodes
+    mask2 = np.zeros((m, m), np.uint8)
+    mask2[0, :] = mask2[-1, :] = mask2[:, 0] = mask2[:, -1] = 1
+    phi2 = np.zeros((m, m))
+    xa, xb, top = (m - 1) // 4, 3 * (m - 1) // 4, (m - 1) // 2
+    mask2[0:top + 1, xa] = 1
+    mask2[0:top + 1, xb] = 1
+    phi2[1:top + 1, xa] = -5.0
+    phi2[1:top + 1, xb] = 5.0
+    sp_ = [dict(name="e", charge=-Consts.qe, mass=Consts.me, np2c=w.np2c(w.n_e), capacity=2 * w.n_e),
+           dict(name="i", charge=Consts.qe, mass=workloads.ION_MASS, np2c=w.np2c(w.n_i), capacity=2 * w.n_i)]
+    sim = PICSimulation(m, m, w.dx, w.dx, 1e-10, sp_, mask2.reshape(-1), phi2.reshape(-1), tol=w.tol,
+                        max_cycles=60, sort_interval=4, mcc=workloads.mcc_tables(w), seed=91, use_graph=True,
+                        push_kernel=push_kernel)
+    rng = np.random.Generator(np.random.Philox(w.seed))
+    for s, which in enumerate(("e", "i")):
+        sim.load(s, *workloads.species_arrays(w, which, rng))
+    sim.init()
+    sim.step(10)
+    sim.sync()
+    c = sim.counters()
+    assert sum(c["collisions"][0]) > 0 and c["born"][0] > 0
+    assert c["electrode_absorbed"][0] > 0
+    assert c["dropped_births"] == 0
+    for s, n0 in enumerate((w.n_e, w.n_i)):
+        live = int((~torch.isnan(sim.species_arrays(s)[0])).sum())
+        assert live == n0 - c["absorbed"][s] - c["electrode_absorbed"][s] + c["born"][s]
+    sim.close()
+
+
 @pytest.mark.parametrize("push_kernel", ["ring", "warp", "warp_agg", "pipe"])
 def test_internal_electrodes_collect_bit_exact(push_kernel):
     """Cathode and anode lines inside the domain (the equipotentials of the
