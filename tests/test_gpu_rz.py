@@ -130,7 +130,7 @@ def test_drop_in_operators_bit_exact():
     np.testing.assert_allclose(t.cpu().numpy(), want, rtol=2e-7)
 
 
-def make_rz_sim(w, seed=0, push_kernel="ring"):
+def make_rz_sim(w, seed=0, push_kernel="ring", mcc=None, sort_interval=0, use_graph=False):
     m = w.nodes
     mask = rz_mask(m, m)
     phi_bc = np.zeros(m * m)
@@ -140,8 +140,9 @@ def make_rz_sim(w, seed=0, push_kernel="ring"):
     phi_bc[sel] = -w.left_V if w.left_V else -20.0
     sp_ = [dict(name="e", charge=-Consts.qe, mass=Consts.me, np2c=5e3, capacity=2 * w.n_e),
            dict(name="i", charge=Consts.qe, mass=workloads.ION_MASS, np2c=5e3, capacity=2 * w.n_i)]
-    sim = PICSimulation(m, m, w.dx, w.dx, w.dt, sp_, mask, phi_bc, tol=w.tol, max_cycles=60, sort_interval=0,
-                        seed=seed, geometry="rz", push_kernel=push_kernel)
+    sim = PICSimulation(m, m, w.dx, w.dx, w.dt, sp_, mask, phi_bc, tol=w.tol, max_cycles=60,
+                        sort_interval=sort_interval, seed=seed, geometry="rz", push_kernel=push_kernel, mcc=mcc,
+                        use_graph=use_graph)
     rng = np.random.Generator(np.random.Philox(w.seed))
     arrays = [list(workloads.species_arrays(w, "e", rng)), list(workloads.species_arrays(w, "i", rng))]
     for s, a in enumerate(arrays):
@@ -212,6 +213,30 @@ def test_fused_rz_step_bit_exact(push_kernel):
     live = [np.isfinite(t.cpu().numpy()) for t in (sim.species_arrays(0)[0], sim.species_arrays(1)[0])]
     ys = [sim.species_arrays(s)[1].cpu().numpy()[live[s]] for s in range(2)]
     assert min(y.min() for y in ys) >= 0.0
+    sim.close()
+
+
+@pytest.mark.parametrize("push_kernel", ["ring", "warp"])
+def test_rz_step_with_mcc_bookkeeping(push_kernel):
+    """r-z geometry with null-collision MCC in a dense gas (the disk electrode
+    on the axis collecting too): the candidates keep their azimuthal velocity
+    through the pass and take the r-z drift after their collision, the
+    ionisation products too.  Every particle is accounted for, no live radius
+    is negative, and the azimuthal velocities stay finite."""
+    w = workloads.scaled(workloads.MCC, nodes=129, n=60_000, gas_density=3e22)
+    sim, _, _ = make_rz_sim(w, seed=5, push_kernel=push_kernel, mcc=workloads.mcc_tables(w), sort_interval=4,
+                            use_graph=True)
+    sim.init()
+    sim.step(10)
+    sim.sync()
+    c = sim.counters()
+    assert sum(c["collisions"][0]) > 0 and c["born"][0] > 0 and c["dropped_births"] == 0
+    for s, n0 in enumerate((w.n_e, w.n_i)):
+        x, y, vx, vy, vz = (t.cpu().numpy() for t in sim.species_arrays(s))
+        live = np.isfinite(x)
+        assert int(live.sum()) == n0 - c["absorbed"][s] - c["electrode_absorbed"][s] + c["born"][s]
+        assert y[live].min() >= 0.0
+        assert np.all(np.isfinite(vz[live]))
     sim.close()
 
 
