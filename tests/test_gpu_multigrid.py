@@ -243,3 +243,24 @@ def test_rectangular_grids_with_electrodes_match_direct_solve(shape):
                                       tol=1e-10, max_cycles=120)
         assert rel < 1e-10, (precision, cycles, rel)
         np.testing.assert_allclose(phi.cpu().numpy(), ref, rtol=0, atol=1e-8 * np.abs(ref).max(), err_msg=precision)
+
+
+@pytest.mark.parametrize("n", [257, 513])
+def test_coarse_solve_in_fp32_or_fp64(n):
+    """The mixed V-cycle's direct solve of its first level of at most 33^2
+    nodes runs in FP64 by default and in FP32 on request (coarse_fp32): both
+    reach the same tolerance on the manufactured problem, the FP32 one in at
+    most one more cycle, and agree with the exact discrete solution."""
+    h, f, exact = manufactured(n)
+    mask = edge_mask(n)
+    f[mask == 1] = 0.0
+    ft = torch.as_tensor(f, device=DEV)
+    res = {}
+    for c32 in (False, True):
+        mg = MultigridSolver(mask, n, n, h, precision="mixed", coarse_fp32=c32)
+        phi = torch.zeros(n * n, dtype=torch.float64, device=DEV)
+        phi, (cycles, rel) = mg.solve(phi, ft, tol=1e-11, max_cycles=40)
+        assert rel < 1e-11, (c32, cycles, rel)
+        np.testing.assert_allclose(phi.cpu().numpy(), exact, rtol=0, atol=1e-9 * np.abs(exact).max())
+        res[c32] = cycles
+    assert res[True] <= res[False] + 1, res
