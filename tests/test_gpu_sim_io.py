@@ -82,3 +82,26 @@ def test_sort_on_demand_orders_by_tile_and_keeps_every_particle():
         live = int(np.isfinite(host_arrays(sim, s)[0]).sum())
         assert live == before[s].shape[1] - (c["absorbed"][s] - absorbed0[s]) - int((~np.isfinite(before[s][0])).sum())
     sim.close()
+
+
+def test_read_particles_of_an_empty_species():
+    """A species with no particles loaded reads back as zero columns, and the
+    simulation steps with it."""
+    w = workloads.scaled(workloads.SMALL, n=20_000)
+    mask, phi_bc = workloads.dirichlet(w)
+    sp = [dict(name="e", charge=-Consts.qe, mass=Consts.me, np2c=w.np2c(w.n_e), capacity=2 * w.n_e),
+          dict(name="i", charge=Consts.qe, mass=workloads.ION_MASS, np2c=w.np2c(w.n_i), capacity=2 * w.n_i)]
+    sim = PICSimulation(w.nodes, w.nodes, w.dx, w.dx, w.dt, sp, mask, phi_bc, tol=w.tol, max_cycles=60,
+                        sort_interval=5, seed=3, use_graph=True)
+    rng = np.random.Generator(np.random.Philox(w.seed))
+    sim.load(0, *workloads.species_arrays(w, "e", rng))
+    empty = np.zeros(0, np.float32)
+    sim.load(1, empty, empty, empty, empty, empty)
+    sim.init()
+    sim.step(6)
+    sim.sync()
+    out = torch.empty(5 * 16, dtype=torch.float32).pin_memory()
+    got = sim.read_particles(1, out)
+    assert tuple(got.shape) == (5, 0)
+    assert sim.counters()["count"][1] == 0
+    sim.close()
