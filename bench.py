@@ -126,19 +126,52 @@ def dist_setup(args):
 # ---------------------------------------------------------------------------
 
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled during the timed
+    region, read only: through NVML in this process every half millisecond
+    (the timed windows last milliseconds), else nvidia-smi every 200 ms."""
 
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, index):
         self.index = index
-        self.rows = []
+        self.rows = []       # nvidia-smi rows
+        self.nvml_rows = []  # (sm MHz, max sm MHz, reason bits)
+        self.bits = {}
         self._stop = threading.Event()
+        self._ready = threading.Event()
         self._t = None
 
+    def _run_nvml(self):
+        import pynvml
+
+        pynvml.nvmlInit()
+        try:
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            self.bits = {"hw_slowdown": pynvml.nvmlClocksEventReasonHwSlowdown,
+                         "hw_thermal_slowdown": pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                         "sw_thermal_slowdown": pynvml.nvmlClocksEventReasonSwThermalSlowdown,
+                         "sw_power_cap": pynvml.nvmlClocksEventReasonSwPowerCap}
+            while True:
+                sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.nvml_rows.append((float(sm), float(mx), int(r)))
+                self._ready.set()
+                if self._stop.wait(0.0005):
+                    break
+        finally:
+            pynvml.nvmlShutdown()
+
     def _run(self):
+        try:
+            self._run_nvml()
+            return
+        except Exception:
+            pass
+        self._ready.set()
         while not self._stop.is_set():
             try:
                 out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
@@ -152,6 +185,7 @@ class ClockSampler:
     def __enter__(self):
         self._t = threading.Thread(target=self._run, daemon=True)
         self._t.start()
+        self._ready.wait(10)  # the first sample precedes the timed region
         return self
 
     def __exit__(self, *a):
@@ -160,15 +194,19 @@ class ClockSampler:
             self._t.join(timeout=10)
 
     def summary(self):
+        if self.nvml_rows:
+            sm = [r[0] for r in self.nvml_rows]
+            reasons = sorted({n for n in self.REASONS for r in self.nvml_rows if r[2] & self.bits[n]})
+            return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(r[1] for r in self.nvml_rows),
+                    "sm_min_mhz": min(sm), "reasons": reasons, "samples": len(self.nvml_rows), "source": "nvml"}
         if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
         mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 4 + k and "Active" in r[4 + k]
+        reasons = sorted({self.REASONS[k] for r in self.rows for k in range(4) if len(r) > 4 + k and "Active" in r[4 + k]
                           and "Not" not in r[4 + k]})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "reasons": reasons, "samples": len(self.rows), "source": "nvidia-smi"}
 
 
 # ---------------------------------------------------------------------------
