@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define PIC_ABI_VERSION 3
+#define PIC_ABI_VERSION 4
 #define PIC_MAX_SPECIES 4
 #define PIC_MAX_PROCESSES 4
 
@@ -396,6 +396,10 @@ typedef struct pic_sim_counters {
      * internal Dirichlet nodes, src/collisions.py:73-175 in the reference,
      * where the tracing exists but is unused) */
     unsigned long long electrode_absorbed[PIC_MAX_SPECIES];
+    /* collision candidates that found the candidate list full (sized at
+     * eight times the expected count plus 65536): they skipped their
+     * collision; nonzero only if the tables' bound was far off */
+    unsigned long long candidate_overflow;
 } pic_sim_counters;
 
 int pic_sim_create(const pic_sim_desc* desc, void* stream, pic_sim** out);

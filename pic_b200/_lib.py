@@ -129,7 +129,8 @@ class SimCounters(C.Structure):
                 ("collisions", (C.c_ulonglong * PIC_MAX_PROCESSES) * PIC_MAX_SPECIES),
                 ("null_candidates", C.c_ulonglong * PIC_MAX_SPECIES), ("born", C.c_ulonglong * PIC_MAX_SPECIES),
                 ("dropped_births", C.c_ulonglong), ("nu_overflow", C.c_ulonglong), ("count", C.c_int * PIC_MAX_SPECIES),
-                ("last_cycles", C.c_int), ("last_rel_res", C.c_double), ("steps", C.c_longlong), ("electrode_absorbed", C.c_ulonglong * PIC_MAX_SPECIES)]
+                ("last_cycles", C.c_int), ("last_rel_res", C.c_double), ("steps", C.c_longlong), ("electrode_absorbed", C.c_ulonglong * PIC_MAX_SPECIES),
+                ("candidate_overflow", C.c_ulonglong)]
 
 
 _vp = C.c_void_p

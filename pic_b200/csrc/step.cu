@@ -2767,6 +2767,7 @@ int pic_sim_read_counters(pic_sim* sim, pic_sim_counters* out, void* stream) {
     for (int s = 0; s < S.ns; ++s) out->electrode_absorbed[s] = c[kCtrElectrode + s];
     out->dropped_births = c[kCtrDropped];
     out->nu_overflow = c[kCtrOverflow];
+    out->candidate_overflow = c[kCtrCandOverflow];
     PIC_TRY(mg_info(S.mg, &S.last));
     out->last_cycles = S.last.cycles;
     out->last_rel_res = S.last.rel_res;

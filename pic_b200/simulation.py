@@ -174,6 +174,7 @@ class PICSimulation:
             "last_rel_res": c.last_rel_res,
             "steps": c.steps,
             "electrode_absorbed": [c.electrode_absorbed[s] for s in range(ns)],
+            "candidate_overflow": c.candidate_overflow,
         }
 
     def particle_buffer(self, x_range=None, y_range=None, out=None):

@@ -46,7 +46,7 @@ def test_python_binding_covers_the_header(libpath):
 
     assert set(declared_functions()) == set(_lib.SIGNATURES)
     lib = _lib.load()
-    assert lib.pic_abi_version() == 3
+    assert lib.pic_abi_version() == 4
     assert lib.pic_last_error() == b""
 
 

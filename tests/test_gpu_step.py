@@ -144,7 +144,7 @@ def test_fused_step_with_mcc_bookkeeping():
     sim.sync()
     c = sim.counters()
     assert sum(c["collisions"][0]) > 0 and c["collisions"][1][0] > 0
-    assert c["dropped_births"] == 0
+    assert c["dropped_births"] == 0 and c["candidate_overflow"] == 0
     for s in range(2):
         live = int((~torch.isnan(sim.species_arrays(s)[0])).sum())
         assert live == w.n_e - c["absorbed"][s] + c["born"][s]
@@ -183,7 +183,7 @@ def test_fused_step_with_mcc_and_electrodes_bookkeeping(push_kernel):
     c = sim.counters()
     assert sum(c["collisions"][0]) > 0 and c["born"][0] > 0
     assert c["electrode_absorbed"][0] > 0
-    assert c["dropped_births"] == 0
+    assert c["dropped_births"] == 0 and c["candidate_overflow"] == 0
     for s, n0 in enumerate((w.n_e, w.n_i)):
         live = int((~torch.isnan(sim.species_arrays(s)[0])).sum())
         assert live == n0 - c["absorbed"][s] - c["electrode_absorbed"][s] + c["born"][s]
